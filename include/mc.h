@@ -1,0 +1,175 @@
+/*
+ * libmc -- B200-native drift correction of dose-fractionated movies.
+ *
+ * C ABI of the frame-drift correction path of MotionCorr 1
+ * (dosefgpu_driftcorr, gepeng1983/motioncorr1exp, src-1125).  It replaces
+ * the reference's GPU layer (cufunc.h:16-47) and the body of
+ * CDFAlign::ThreadFunc_cuAlign (DFAlign.cu:456-1355): the caller reads the
+ * stack and writes the outputs, the library does everything in between on
+ * one GPU with hand-written sm_100a kernels (no cuFFT).
+ *
+ * Conventions
+ *   - every call returns MC_OK (0) or a negative MC_E_* code; mc_strerror()
+ *     and mc_last_error() describe it; nothing exits or installs handlers;
+ *   - the caller owns host buffers, a plan owns its device memory and its
+ *     CUDA stream; a plan is used by one host thread at a time and distinct
+ *     plans share no state;
+ *   - "position" p means frame nStart + p of the stack (0 <= p < nframe).
+ */
+#ifndef MC_H
+#define MC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC_VERSION 10000 /* 1.0.0 */
+
+enum {
+  MC_OK = 0,
+  MC_E_ARG = -1,      /* invalid argument / parameter combination */
+  MC_E_CUDA = -2,     /* CUDA runtime error (see mc_last_error) */
+  MC_E_NOMEM = -3,    /* device or host allocation failed */
+  MC_E_SIZE = -4,     /* geometry the kernels do not support */
+  MC_E_STATE = -5,    /* call out of order (e.g. pairs before forward) */
+  MC_E_NUMERIC = -6   /* singular least-squares system */
+};
+
+/* Alignment parameters: the fields of APARA (DFAlign.h:16-63) that act on the
+ * drift-correction path, plus -itr/-ith (DFAlign.h:75-76) and the added
+ * refinement switch.  Defaults: mc_default_params. */
+typedef struct mc_params {
+  int crop_offsetx;    /* -crx */
+  int crop_offsety;    /* -cry */
+  int crop_nsam;       /* -crd (0 = largest square) */
+  float bin;           /* -bin, clamped to [1, 2] */
+  int nStart;          /* -nst */
+  int nEnd;            /* -ned */
+  int nStartSum;       /* -nss */
+  int nEndSum;         /* -nes */
+  int GPUNum;          /* -gpu */
+  float bfactor;       /* -bft, pix^2 */
+  int CCPeakSearchDim; /* -pbx, 16..256 */
+  int FrameDistOffset; /* -fod */
+  int NoisePeakSize;   /* -nps */
+  float kiThresh;      /* -kit */
+  int bAlignToMid;     /* -atm */
+  int iter;            /* -itr */
+  float iterthres;     /* -ith */
+  int refine;          /* added: 0 = Fourier-upsampled peak only, 1 = + gradient refinement */
+} mc_params;
+
+typedef struct mc_plan mc_plan;
+
+typedef struct mc_info {
+  int nx, ny, nz, mode;  /* stack geometry and MRC pixel mode (0, 1, 2, 6) */
+  int nsam_unbin;        /* square crop side (verifyCropSize, func.cpp:80-103) */
+  int nsam;              /* binned side (DFAlign.cu:515) */
+  int nstart, nend, nframe;
+  int npairs;            /* frame pairs of OD_SetEquation_All (mfunc.h:64-84) */
+  int two_sets;          /* 1 when dark/gain references make hbuf != hbuf2 */
+  int prune_p, prune_q;  /* n = P*Q split of the pruned inverse transform */
+  size_t device_bytes;   /* device memory held by the plan */
+} mc_info;
+
+typedef struct mc_timings { /* device time of the last run, CUDA events */
+  float forward_ms, pairs_ms, solve_ms, iterate_ms, sum_ms, total_ms;
+} mc_timings;
+
+typedef void (*mc_log_fn)(const char* text, void* user);
+
+int mc_version(void);
+const char* mc_strerror(int code);
+/* Text of the last error of the calling thread ("" if none). */
+const char* mc_last_error(void);
+
+/* getDefaultPara (dosefgpu_driftcorr.cpp:8-58) plus itr=0, ith=0 (DFAlign.cu:15-16). */
+void mc_default_params(mc_params* p);
+
+/* VerifyPara frame-range repair and checks (dosefgpu_driftcorr.cpp:60-118)
+ * for a stack of nz frames.  Returns MC_E_ARG with the reference's abort text
+ * in mc_last_error() when the reference aborts. */
+int mc_verify_params(mc_params* p, int nz);
+
+/* Plan for one stack geometry: crop/bin (DFAlign.cu:500-530), frame range,
+ * device buffers, FFT plans.  Replaces initGPU, GPUMemAlloc, GPUFFTPlan,
+ * GPUIFFTPlan and MkPosList (cufunc.cu:30-65, 111-115, 202-215, 309-341). */
+int mc_plan_create(const mc_params* p, int nx, int ny, int nz, int mode, mc_plan** out);
+void mc_plan_destroy(mc_plan* plan);
+int mc_plan_info(const mc_plan* plan, mc_info* info);
+/* The plan's CUDA stream (cudaStream_t). */
+void* mc_plan_stream(mc_plan* plan);
+/* Log sink for the text ThreadFunc_cuAlign writes through TextOutput
+ * (DFAlign.cu:59-71); NULL disables. */
+void mc_plan_set_log(mc_plan* plan, mc_log_fn fn, void* user);
+
+/* Dark/gain references, nx*ny floats each, host memory, NULL = absent
+ * (DFAlign.cu:614-695): dark2/norm2 are the second frames of two-frame
+ * reference files; with a one-frame file pass NULL (then 0 / 1 are used). */
+int mc_plan_set_refs(mc_plan* plan, const float* dark, const float* dark2, const float* norm,
+                     const float* norm2);
+
+/* Copy raw frames (MRC pixel type of the plan's mode, nx*ny each) for
+ * positions [first, first+count) from host memory (pinned or pageable) or
+ * from device memory.  Replaces MRC::read2DIm_32bit + GPUMemH2D per frame
+ * (DFAlign.cu:713, 770, 795).  Host copies return once the source buffer
+ * may be reused; device copies are ordered on the plan stream. */
+int mc_plan_load_frames(mc_plan* plan, const void* frames, int first, int count);
+int mc_plan_load_frames_device(mc_plan* plan, const void* d_frames, int first, int count);
+
+/* Stages (each synchronous on return). */
+int mc_plan_forward(mc_plan* plan);         /* DFAlign.cu:710-824 */
+int mc_plan_pairs(mc_plan* plan);           /* DFAlign.cu:875-905 */
+int mc_plan_solve(mc_plan* plan);           /* DFAlign.cu:914-948 */
+int mc_plan_iterate(mc_plan* plan);         /* DFAlign.cu:950-1092 */
+int mc_plan_sum(mc_plan* plan, float* image_host); /* DFAlign.cu:1114-1292; image n*n or NULL */
+/* All stages in order. */
+int mc_plan_run(mc_plan* plan, float* image_host);
+
+/* Results. */
+int mc_plan_get_frame_shifts(const mc_plan* plan, double* xy);           /* 2*nframe, "Shift of Frame" */
+int mc_plan_get_pairs(const mc_plan* plan, int* ij, float* shift, float* cc, int* peak); /* 2P,2P,P,2P */
+int mc_plan_get_ki(const mc_plan* plan, double* ki1, int* nkept, int* kept, double* ki2);
+int mc_plan_get_frame_means(const mc_plan* plan, float* mean);           /* nframe */
+int mc_plan_get_spectrum(mc_plan* plan, int set, int pos, void* host);  /* (n/2+1)*n float2, [kx][ky] */
+int mc_plan_get_boxes(mc_plan* plan, float* host);                       /* npairs*pbx*pbx */
+int mc_plan_get_sum_shifts(const mc_plan* plan, double* xy, int* first, int* last);
+int mc_plan_get_timings(const mc_plan* plan, mc_timings* t);
+
+/* Per-kernel accounting of a plan: launches and algorithmic bytes are always
+ * counted; device time is recorded with one CUDA event pair per launch while
+ * profiling is on.  Kinds follow the kernels of the path. */
+enum {
+  MC_K_FWD_ROWS = 0,  /* decode + dark/gain + crop + row R2C */
+  MC_K_FWD_COLS = 1,  /* column FFT + Fourier-crop binning (k_rows_fft) */
+  MC_K_PAIR_COLS = 2, /* cross power x B-factor + pruned inverse along ky */
+  MC_K_PAIR_ROWS = 3, /* pruned C2R along kx onto the pbx window */
+  MC_K_PEAK = 4,      /* integer + x32 Fourier-upsampled peak */
+  MC_K_SHIFT_SUM = 5, /* phase-shift-and-accumulate (+ inverse columns) */
+  MC_K_C2R_ROWS = 6,  /* final C2R rows x 1/n^2 */
+  MC_KERNEL_KINDS = 7
+};
+void mc_plan_set_profiling(mc_plan* plan, int on);
+int mc_plan_reset_stats(mc_plan* plan);
+int mc_plan_kernel_stats(const mc_plan* plan, int kind, double* ms, long long* launches, double* bytes);
+const char* mc_kernel_name(int kind);
+
+/* Host-only drift solve of DFAlign.cu:914-948 on given pair measurements:
+ * lsSolver, residuals ki, OD_Threshold (mfunc.h:101-146), lsSolver again.
+ * ij: 2*npairs frame indices (i < j), shifts_xy: 2*npairs; outputs step_xy
+ * (2*(nframe-1) per-step shifts), ki1 (npairs), kept rows (ascending) and
+ * their second-round residuals ki2.  Any output may be NULL. */
+int mc_solve_pairs(int nframe, int npairs, const int* ij, const float* shifts_xy, float kithresh,
+                   double* step_xy, double* ki1, int* nkept, int* kept, double* ki2);
+
+/* Batched 1-D complex FFT of the library's engine on device memory
+ * (un-normalised; inverse = exp(+2 pi i)).  Stream may be NULL. */
+int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MC_H */

@@ -1,0 +1,286 @@
+"""Python mirror of the reference's alignment interface over libmc.
+
+``Params`` carries the APARA fields (DFAlign.h:16-63) under the reference's
+names; ``Plan`` wraps one mc_plan (one stack geometry on one GPU) and exposes
+the stages of CDFAlign::ThreadFunc_cuAlign (DFAlign.cu:456-1355).  Every
+call goes through the C ABI of libmc.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class Params:
+    """APARA with the defaults of getDefaultPara (dosefgpu_driftcorr.cpp:8-58)."""
+    crop_offsetx: int = 0
+    crop_offsety: int = 0
+    crop_nsam: int = 0
+    bin: float = 1.0
+    nStart: int = 0
+    nEnd: int = 0
+    nStartSum: int = 0
+    nEndSum: int = 0
+    GPUNum: int = 0
+    bfactor: float = 150.0
+    CCPeakSearchDim: int = 96
+    FrameDistOffset: int = 2
+    NoisePeakSize: int = 0
+    kiThresh: float = 1.0
+    bAlignToMid: int = 1
+    iter: int = 0
+    iterthres: float = 0.0
+    refine: int = 0
+
+    def to_c(self) -> L.McParams:
+        c = L.McParams()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+    @classmethod
+    def from_c(cls, c: L.McParams) -> "Params":
+        return cls(**{f.name: getattr(c, f.name) for f in fields(cls)})
+
+
+def default_params() -> Params:
+    c = L.McParams()
+    L.lib().mc_default_params(C.byref(c))
+    return Params.from_c(c)
+
+
+def verify_params(p: Params, nz: int) -> Params:
+    """VerifyPara (dosefgpu_driftcorr.cpp:60-118); raises McError on abort."""
+    c = p.to_c()
+    L.check(L.lib().mc_verify_params(C.byref(c), nz))
+    return Params.from_c(c)
+
+
+_WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2}
+KERNEL_KINDS = 7
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class Plan:
+    """One stack geometry on one GPU (mc_plan_create)."""
+
+    def __init__(self, params: Params, nx: int, ny: int, nz: int, mode: int,
+                 log: Optional[Callable[[str], None]] = None):
+        self._lib = L.lib()
+        h = C.c_void_p()
+        c = params.to_c()
+        L.check(self._lib.mc_plan_create(C.byref(c), nx, ny, nz, mode, C.byref(h)))
+        self._h = h
+        self.params = params
+        self._logcb = None
+        if log is not None:
+            self.set_log(log)
+        info = L.McInfo()
+        L.check(self._lib.mc_plan_info(self._h, C.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in L.McInfo._fields_}
+
+    # -- lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.mc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.mc_plan_stream(self._h) or 0)
+
+    @property
+    def nsam(self) -> int:
+        return self.info["nsam"]
+
+    @property
+    def nframe(self) -> int:
+        return self.info["nframe"]
+
+    @property
+    def npairs(self) -> int:
+        return self.info["npairs"]
+
+    def set_log(self, fn: Callable[[str], None]) -> None:
+        def _cb(text, _user):
+            fn(text.decode(errors="replace"))
+        self._logcb = L.LOG_FN(_cb)
+        self._lib.mc_plan_set_log(self._h, self._logcb, None)
+
+    # -- inputs
+    def set_refs(self, dark=None, dark2=None, norm=None, norm2=None) -> None:
+        keep = []
+
+        def p(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            keep.append(a)
+            return _ptr(a)
+        L.check(self._lib.mc_plan_set_refs(self._h, p(dark), p(dark2), p(norm), p(norm2)))
+        self.info["two_sets"] = int(dark is not None or norm is not None)
+
+    def load_frames(self, frames: np.ndarray, first: int = 0) -> None:
+        """Raw frames (count, ny, nx) in the plan's MRC pixel type, host memory."""
+        a = np.ascontiguousarray(frames)
+        if a.dtype.itemsize != _WORD_LENGTH[self.info["mode"]]:
+            raise ValueError(f"frames of {a.dtype} do not match MRC mode {self.info['mode']}")
+        count = a.shape[0] if a.ndim == 3 else 1
+        L.check(self._lib.mc_plan_load_frames(self._h, _ptr(a), first, count))
+        self._lib_keep = a  # the copy is asynchronous on the plan stream
+
+    def load_frames_device(self, dev_ptr: int, first: int, count: int) -> None:
+        L.check(self._lib.mc_plan_load_frames_device(self._h, C.c_void_p(dev_ptr), first, count))
+
+    # -- stages
+    def forward(self) -> None:
+        L.check(self._lib.mc_plan_forward(self._h))
+
+    def pairs(self) -> None:
+        L.check(self._lib.mc_plan_pairs(self._h))
+
+    def solve(self) -> None:
+        L.check(self._lib.mc_plan_solve(self._h))
+
+    def iterate(self) -> None:
+        L.check(self._lib.mc_plan_iterate(self._h))
+
+    def sum(self, want_image: bool = True) -> Optional[np.ndarray]:
+        img = np.empty((self.nsam, self.nsam), dtype=np.float32) if want_image else None
+        L.check(self._lib.mc_plan_sum(self._h, _ptr(img) if want_image else None))
+        return img
+
+    def run(self, want_image: bool = True, out: Optional[np.ndarray] = None) -> Optional[np.ndarray]:
+        img = out if out is not None else (np.empty((self.nsam, self.nsam), dtype=np.float32) if want_image else None)
+        L.check(self._lib.mc_plan_run(self._h, _ptr(img) if img is not None else None))
+        return img
+
+    # -- results
+    def frame_shifts(self) -> np.ndarray:
+        xy = np.empty((self.nframe, 2), dtype=np.float64)
+        L.check(self._lib.mc_plan_get_frame_shifts(self._h, _ptr(xy)))
+        return xy
+
+    def pair_results(self) -> dict:
+        P = self.npairs
+        ij = np.empty((P, 2), dtype=np.int32)
+        sh = np.empty((P, 2), dtype=np.float32)
+        cc = np.empty(P, dtype=np.float32)
+        pk = np.empty((P, 2), dtype=np.int32)
+        L.check(self._lib.mc_plan_get_pairs(self._h, _ptr(ij), _ptr(sh), _ptr(cc), _ptr(pk)))
+        return {"pairs": ij, "shift": sh, "cc": cc, "peak": pk}
+
+    def ki(self) -> dict:
+        P = self.npairs
+        ki1 = np.empty(P, dtype=np.float64)
+        kept = np.empty(P, dtype=np.int32)
+        ki2 = np.empty(P, dtype=np.float64)
+        nk = C.c_int()
+        L.check(self._lib.mc_plan_get_ki(self._h, _ptr(ki1), C.byref(nk), _ptr(kept), _ptr(ki2)))
+        return {"ki1": ki1, "kept": kept[: nk.value].copy(), "ki2": ki2[: nk.value].copy()}
+
+    def frame_means(self) -> np.ndarray:
+        m = np.empty(self.nframe, dtype=np.float32)
+        L.check(self._lib.mc_plan_get_frame_means(self._h, _ptr(m)))
+        return m
+
+    def spectrum(self, pos: int, set_: int = 0) -> np.ndarray:
+        """Half spectrum of position ``pos`` in the reference layout (ky rows, kx columns)."""
+        n = self.nsam
+        h = n // 2 + 1
+        s = np.empty((h, n), dtype=np.complex64)
+        L.check(self._lib.mc_plan_get_spectrum(self._h, set_, pos, _ptr(s)))
+        return s.T.copy()
+
+    def boxes(self) -> np.ndarray:
+        b = self.params.CCPeakSearchDim
+        out = np.empty((self.npairs, b, b), dtype=np.float32)
+        L.check(self._lib.mc_plan_get_boxes(self._h, _ptr(out)))
+        return out
+
+    def sum_shifts(self) -> tuple[np.ndarray, int, int]:
+        xy = np.empty((self.nframe, 2), dtype=np.float64)
+        f, l = C.c_int(), C.c_int()
+        L.check(self._lib.mc_plan_get_sum_shifts(self._h, _ptr(xy), C.byref(f), C.byref(l)))
+        return xy, f.value, l.value
+
+    def timings(self) -> dict:
+        t = L.McTimings()
+        L.check(self._lib.mc_plan_get_timings(self._h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in L.McTimings._fields_}
+
+    def set_profiling(self, on: bool) -> None:
+        self._lib.mc_plan_set_profiling(self._h, int(on))
+
+    def reset_stats(self) -> None:
+        L.check(self._lib.mc_plan_reset_stats(self._h))
+
+    def kernel_stats(self) -> dict:
+        """{kernel name: {"ms", "launches", "bytes"}} accumulated since reset."""
+        out = {}
+        for k in range(KERNEL_KINDS):
+            ms, n, b = C.c_double(), C.c_longlong(), C.c_double()
+            L.check(self._lib.mc_plan_kernel_stats(self._h, k, C.byref(ms), C.byref(n), C.byref(b)))
+            out[self._lib.mc_kernel_name(k).decode()] = {"ms": ms.value, "launches": n.value, "bytes": b.value}
+        return out
+
+
+def solve_pairs(nframe: int, pairs: np.ndarray, shifts: np.ndarray, kithresh: float = 1.0) -> dict:
+    """Host FP64 drift solve (mc_solve_pairs): lsSolver + OD_Threshold + lsSolver."""
+    ij = np.ascontiguousarray(pairs, dtype=np.int32)
+    sh = np.ascontiguousarray(shifts, dtype=np.float32)
+    P = ij.shape[0]
+    step = np.empty((nframe - 1, 2))
+    ki1 = np.empty(P)
+    kept = np.empty(P, dtype=np.int32)
+    ki2 = np.empty(P)
+    nk = C.c_int()
+    L.check(L.lib().mc_solve_pairs(nframe, P, _ptr(ij), _ptr(sh), kithresh, _ptr(step), _ptr(ki1),
+                                   C.byref(nk), _ptr(kept), _ptr(ki2)))
+    return {"step": step, "ki1": ki1, "kept": kept[: nk.value].copy(), "ki2": ki2[: nk.value].copy()}
+
+
+def fft1d(d_in: int, d_out: int, n: int, batch: int, inverse: bool, stream: int = 0) -> None:
+    """Engine transform on device pointers (tests)."""
+    L.check(L.lib().mc_fft1d(n, batch, int(inverse), C.c_void_p(d_in), C.c_void_p(d_out),
+                              C.c_void_p(stream) if stream else None))
+
+
+def align(frames: np.ndarray, mode: int, params: Params, nz: Optional[int] = None,
+          refs: Optional[dict] = None, log=None) -> dict:
+    """Whole path on a stack already in host memory: frames (nz, ny, nx) in
+    the file's pixel type.  Returns shifts, pair results and the sum."""
+    nf, ny, nx = frames.shape
+    nz = nz if nz is not None else nf
+    with Plan(params, nx, ny, nz, mode, log=log) as pl:
+        if refs:
+            pl.set_refs(**refs)
+        pl.load_frames(frames[pl.info["nstart"]: pl.info["nend"] + 1])
+        img = pl.run()
+        return {"image": img, "frame_shifts": pl.frame_shifts(), **pl.pair_results(), **pl.ki(),
+                "frame_mean": pl.frame_means(), "info": dict(pl.info), "timings": pl.timings()}

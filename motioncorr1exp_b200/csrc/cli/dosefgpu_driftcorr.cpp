@@ -1,0 +1,435 @@
+// dosefgpu_driftcorr: command-line drop-in for the reference program of the
+// same name (src-1125/dosefgpu_driftcorr.cpp).  Same flags, defaults,
+// clamping, abort messages, default output names, parameter log and
+// alignment log lines; the alignment itself runs in libmc (include/mc.h).
+#include <sys/stat.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mc.h"
+#include "mrc_file.h"
+
+namespace {
+
+struct Options {
+  mc_params p;
+  float xscale = 1.f, yscale = 1.f;  // -scx -scy (accepted, not applied)
+  int nEndSum2 = 0;                  // -2es (accepted, not applied)
+  int bSaveSubAreaCorrSum = 0, bSaveRawSum = 0, bSaveStackCorr = 0, bSaveCCmap = 0;
+  int bSaveLog = 1, bLogFSC = 0;
+  bool bSaveDisp = true;
+  int cdx = 0, cdy = 0;
+  std::string fnStack, fnRawsum, fnAlignsum, fnAlignsum2, fnStackCorr, fnCCmap, fnLog, fnDark, fnNorm;
+  std::string dispRawFFT, dispCorrSum, dispCorrFFT;
+};
+
+Options* g_opt = nullptr;
+
+// TextOutput (DFAlign.cu:59-71): stdout plus an append to the log file.
+void text_output(const char* s) {
+  printf("%s", s);
+  if (g_opt && g_opt->bSaveLog) {
+    FILE* fp = fopen(g_opt->fnLog.c_str(), "a");
+    if (fp) {
+      fprintf(fp, "%s", s);
+      fclose(fp);
+    }
+  }
+}
+
+void log_cb(const char* text, void*) { text_output(text); }
+
+// Message (DFAlign.cu:51-54)
+void message(const char* s) { printf("%s\n", s); }
+
+void usage() {
+  printf("Dose Fractionation Tool:\n");
+  printf("Drift correction\n\n");
+  printf("    Input: InputStack.mrc [OPTION VALUE] ...\n");
+  printf("          *Note: If not specify OPTION, the default value will be used.\n\n");
+  printf("           OPTION     VALUE(Default)    Introduction  \n");
+  printf("           -crx       0                 Image crop offset X\n");
+  printf("           -cry       0                 Image crop offset Y\n");
+  printf("           -crd       0                 Image crop dimension. If 0, use maximum size.\n");
+  printf("           -cdx/-cdy  0                 Crop dimension X/Y (square: the smaller is used).\n");
+  printf("           -bin       1.0               Float number between 1x and 2x. Bin stack before processing.\n");
+  printf("           -scx       1.0               Float number (>=1.0). Stretch image along X axis.\n");
+  printf("           -scy       1.0               Float number (>=1.0). Stretch image along Y axis.\n");
+  printf("           -nst       0                 First frame (0-base) used in alignment.\n");
+  printf("           -ned       0                 Last frame (0-base) used in alignment. If 0, use maximum value.\n");
+  printf("           -nss       0                 First frame (0-base) used for final sum.\n");
+  printf("           -nes       0                 Last frame (0-base) used for final sum. If 0,use maximum value.\n");
+  printf("           -2es       0                 Last frame (0-base) used for the second sum.\n");
+  printf("           -gpu       0                 GPU device ID.\n");
+  printf("           -bft       150               BFactor in pix^2.\n");
+  printf("           -pbx       96                Box dimension for searching CC peak.\n");
+  printf("           -fod       2                 Number of frame offset for frame comparision.\n");
+  printf("           -nps       0                 Radius of noise peak.\n");
+  printf("           -kit       1.0               Threshold of alignment error in pixel.\n");
+  printf("           -sub       0                 1: Save as sub-area corrected sum. 0: Not. \n");
+  printf("           -srs       0                 1: Save uncorrected sum. 0: Not.\n");
+  printf("           -ssc       0                 1: Save aligned stack. 0: Not.\n");
+  printf("           -scc       0                 1: Save CC Map. 0: Not.\n");
+  printf("           -slg       1                 1: Save Log. 0: Not.\n");
+  printf("           -atm       1                 1: Align to middle frame. 0: Not.\n");
+  printf("           -dsp       1                 1: Save quick results. 0: Not.\n");
+  printf("           -fsc       0                 1: Calculate and log FSC. 0: Not.\n");
+  printf("           -frs       FileName.mrc      Uncorrected sum\n");
+  printf("           -fcs       FileName.mrc      Corrected sum\n");
+  printf("           -2cs       FileName.mrc      Corrected second sum\n");
+  printf("           -fct       FileName.mrc      Corrected stack\n");
+  printf("           -fcm       FileName.mrc      CC map\n");
+  printf("           -flg       FileName.txt      Log file\n");
+  printf("           -fdk       FileName.mrc      Dark reference\n");
+  printf("           -fnm       FileName.mrc      Gain reference\n");
+  printf("           -itr       0                 Number of iteration for iterative alignment\n");
+  printf("           -ith       0.0               Convergence threshold for iterative alignment (RMSD shift)\n");
+  printf("           -ref       0                 1: gradient refinement of the sub-pixel shifts. 0: Not.\n");
+}
+
+int stack_nframe(const std::string& fn) {
+  if (!is_mrc(fn.c_str())) return 0;
+  MrcStack s;
+  if (s.open(fn.c_str()) <= 0) return 0;
+  return s.header().nz;
+}
+
+// VerifyPara (dosefgpu_driftcorr.cpp:60-118)
+bool verify_para(Options& o) {
+  const int nFrame = stack_nframe(o.fnStack);
+  if (nFrame <= 1) {
+    printf("Not a stack or wrong file. Abort\n");
+    return false;
+  }
+  mc_params& p = o.p;
+  if (p.nStart < 0) p.nStart = 0;
+  if (p.nEnd >= nFrame) p.nEnd = nFrame - 1;
+  if (p.nEnd <= p.nStart) p.nEnd = nFrame - 1;
+  if (p.nStartSum < p.nStart) p.nStartSum = p.nStart;
+  if (p.nEndSum > p.nEnd) p.nEndSum = p.nEnd;
+  if (p.nEndSum <= p.nStartSum) p.nEndSum = p.nEnd;
+  if (o.nEndSum2 > p.nEnd) o.nEndSum2 = p.nEnd;
+  if (o.nEndSum2 <= p.nStartSum) o.nEndSum2 = 0;
+  if (p.FrameDistOffset >= nFrame / 2 || p.FrameDistOffset < 0) {
+    printf("Frame distance offset is too big or less than 0. Abort\n");
+    return false;
+  }
+  if (o.nEndSum2 >= p.nEndSum) {
+    printf("Last frame # for the second sum image cannot be larger than or equal to that for the first sum image.\n");
+    return false;
+  }
+  return true;
+}
+
+// getPara (dosefgpu_driftcorr.cpp:121-515)
+bool get_para(int narg, char* argv[], Options& o) {
+  mc_default_params(&o.p);
+  mc_params& p = o.p;
+  o.fnStack = argv[1];
+  if (narg % 2 == 1) {
+    printf("Wrong number of arguments. Abort.\n");
+    return false;
+  }
+  bool dRaw = true, dAlign = true, dAlign2 = true, dStack = true, dCC = true, dLog = true;
+  for (int i = 2; i < narg; i++) {
+    const std::string opt = argv[i];
+    auto nexti = [&]() { return atoi(argv[++i]); };
+    auto nextf = [&]() { return (float)atof(argv[++i]); };
+    auto nexts = [&]() { return std::string(argv[++i]); };
+    if (opt == "-crx") { p.crop_offsetx = nexti(); continue; }
+    if (opt == "-cry") { p.crop_offsety = nexti(); continue; }
+    if (opt == "-crd") { p.crop_nsam = nexti(); continue; }
+    if (opt == "-cdx") { o.cdx = nexti(); continue; }
+    if (opt == "-cdy") { o.cdy = nexti(); continue; }
+    if (opt == "-bin") {
+      p.bin = nextf();
+      if (p.bin > 2.0001) {
+        printf("Larger than maximum binning 2. Set to 2.\n");
+        p.bin = 2.0;
+      } else if (p.bin < 0.9999) {
+        printf("Smaller than minimum binning 1. Set to 1.\n");
+        p.bin = 1.0;
+      }
+      continue;
+    }
+    if (opt == "-scx") {
+      o.xscale = nextf();
+      if (o.xscale < 1.0) {
+        printf("Stretching factor along X-axis needs to be >=1.0.\n");
+        return false;
+      }
+      continue;
+    }
+    if (opt == "-scy") {
+      o.yscale = nextf();
+      if (o.yscale < 1.0) {
+        printf("Stretching factor along Y-axis needs to be >=1.0.\n");
+        return false;
+      }
+      continue;
+    }
+    if (opt == "-nst") { p.nStart = nexti(); continue; }
+    if (opt == "-ned") { p.nEnd = nexti(); continue; }
+    if (opt == "-nss") { p.nStartSum = nexti(); continue; }
+    if (opt == "-nes") { p.nEndSum = nexti(); continue; }
+    if (opt == "-2es") { o.nEndSum2 = nexti(); continue; }
+    if (opt == "-gpu") { p.GPUNum = nexti(); continue; }
+    if (opt == "-bft") { p.bfactor = nextf(); continue; }
+    if (opt == "-pbx") { p.CCPeakSearchDim = nexti(); continue; }
+    if (opt == "-fod") { p.FrameDistOffset = nexti(); continue; }
+    if (opt == "-nps") { p.NoisePeakSize = nexti(); continue; }
+    if (opt == "-kit") { p.kiThresh = nextf(); continue; }
+    if (opt == "-sub") { o.bSaveSubAreaCorrSum = nexti() != 0; continue; }
+    if (opt == "-srs") { o.bSaveRawSum = nexti() != 0; continue; }
+    if (opt == "-ssc") { o.bSaveStackCorr = nexti() != 0; continue; }
+    if (opt == "-scc") { o.bSaveCCmap = nexti() != 0; continue; }
+    if (opt == "-slg") { o.bSaveLog = nexti() != 0; continue; }
+    if (opt == "-atm") { p.bAlignToMid = nexti() != 0; continue; }
+    if (opt == "-dsp") {
+      if (nexti() == 0) o.bSaveDisp = false;
+      continue;
+    }
+    if (opt == "-fsc") { o.bLogFSC = nexti() != 0; continue; }
+    if (opt == "-frs") { o.fnRawsum = nexts(); dRaw = false; continue; }
+    if (opt == "-fcs") { o.fnAlignsum = nexts(); dAlign = false; continue; }
+    if (opt == "-2cs") { o.fnAlignsum2 = nexts(); dAlign2 = false; continue; }
+    if (opt == "-fct") { o.fnStackCorr = nexts(); dStack = false; continue; }
+    if (opt == "-fcm") { o.fnCCmap = nexts(); dCC = false; continue; }
+    if (opt == "-flg") { o.fnLog = nexts(); dLog = false; continue; }
+    if (opt == "-fnm") { o.fnNorm = nexts(); continue; }
+    if (opt == "-fdk") { o.fnDark = nexts(); continue; }
+    if (opt == "-itr") { p.iter = nexti(); continue; }
+    if (opt == "-ith") { p.iterthres = nextf(); continue; }
+    if (opt == "-ref") { p.refine = nexti(); continue; }
+    printf("Undefined option: %s .Abort.\n", argv[i]);
+    return false;
+  }
+  if (o.cdx > 0 || o.cdy > 0) {
+    const int d = (o.cdx > 0 && o.cdy > 0) ? std::min(o.cdx, o.cdy) : std::max(o.cdx, o.cdy);
+    if (o.cdx > 0 && o.cdy > 0 && o.cdx != o.cdy)
+      printf("Warning: square crop only; using -cdx/-cdy %d.\n", d);
+    p.crop_nsam = d;
+  }
+  // default file names (dosefgpu_driftcorr.cpp:433-481)
+  std::string fnp = argv[1];
+  if (fnp.rfind('.') != std::string::npos) fnp = fnp.substr(0, fnp.rfind('.'));
+  if (p.bin > 1.0001) fnp += "_binned";
+  std::string path = ".", prefix;
+  if (fnp.rfind('/') == std::string::npos) prefix = fnp;
+  else prefix = fnp.substr(fnp.rfind('/') + 1);
+  if (dRaw) o.fnRawsum = prefix + "_SumRaw.mrc";
+  if (dAlign) o.fnAlignsum = prefix + "_SumCorr.mrc";
+  if (dAlign2) o.fnAlignsum2 = prefix + "_SumCorr2.mrc";
+  if (dStack) o.fnStackCorr = prefix + "_Corrected.mrc";
+  if (dCC) o.fnCCmap = prefix + "_CCMap.mrc";
+  if (dLog) o.fnLog = prefix + "_Log.txt";
+  if (o.bSaveDisp) {
+    const std::string d = path + "/dosef_quick/" + prefix;
+    o.dispRawFFT = d + "_RawFFT.mrc";
+    o.dispCorrSum = d + "_CorrSum.mrc";
+    o.dispCorrFFT = d + "_CorrFFT.mrc";
+  }
+  return verify_para(o);
+}
+
+// ShowPara (dosefgpu_driftcorr.cpp:517-579)
+void show_para(const Options& o) {
+  if (!o.bSaveLog) return;
+  FILE* fp = fopen(o.fnLog.c_str(), "w");
+  if (!fp) return;
+  const mc_params& p = o.p;
+  fprintf(fp, "******Parameter List******\n");
+  fprintf(fp, "Input:  %s\n", o.fnStack.c_str());
+  fprintf(fp, "  -crx  %d\n", p.crop_offsetx);
+  fprintf(fp, "  -cry  %d\n", p.crop_offsety);
+  fprintf(fp, "  -crd  %d\n", p.crop_nsam);
+  fprintf(fp, "  -bin  %f\n", p.bin);
+  fprintf(fp, "  -scx  %f\n", o.xscale);
+  fprintf(fp, "  -scy  %f\n", o.yscale);
+  fprintf(fp, "  -nst  %d\n", p.nStart);
+  fprintf(fp, "  -ned  %d\n", p.nEnd);
+  fprintf(fp, "  -nss  %d\n", p.nStartSum);
+  fprintf(fp, "  -nes  %d\n", p.nEndSum);
+  fprintf(fp, "  -2es  %d\n", o.nEndSum2);
+  fprintf(fp, "  -gpu  %d\n", p.GPUNum);
+  fprintf(fp, "  -bft  %f\n", p.bfactor);
+  fprintf(fp, "  -pbx  %d\n", p.CCPeakSearchDim);
+  fprintf(fp, "  -fod  %d\n", p.FrameDistOffset);
+  fprintf(fp, "  -nps  %d\n", p.NoisePeakSize);
+  fprintf(fp, "  -kit  %f\n", p.kiThresh);
+  fprintf(fp, "  -sub  %d\n", o.bSaveSubAreaCorrSum);
+  fprintf(fp, "  -srs  %d\n", o.bSaveRawSum);
+  fprintf(fp, "  -ssc  %d\n", o.bSaveStackCorr);
+  fprintf(fp, "  -scc  %d\n", o.bSaveCCmap);
+  fprintf(fp, "  -slg  %d\n", o.bSaveLog);
+  fprintf(fp, "  -atm  %d\n", p.bAlignToMid);
+  fprintf(fp, "  -dsp  %d\n", o.bSaveDisp ? 1 : 0);
+  fprintf(fp, "  -fsc  %d\n", o.bLogFSC);
+  fprintf(fp, "  -fcs  %s\n", o.fnAlignsum.c_str());
+  fprintf(fp, "  -2cs  %s\n", o.fnAlignsum2.c_str());
+  if (o.bSaveRawSum) fprintf(fp, "  -frs  %s\n", o.fnRawsum.c_str());
+  if (o.bSaveStackCorr) fprintf(fp, "  -fct  %s\n", o.fnStackCorr.c_str());
+  if (o.bSaveCCmap) fprintf(fp, "  -fcm  %s\n", o.fnCCmap.c_str());
+  if (o.bSaveLog) fprintf(fp, "  -flg  %s\n", o.fnLog.c_str());
+  if (o.bSaveDisp) {
+    fprintf(fp, "\nQuick results in dosef_quick folder:\n");
+    fprintf(fp, "UnCorrected FFT: %s \n", o.dispRawFFT.c_str());
+    fprintf(fp, "Corrected Sum:   %s \n", o.dispCorrSum.c_str());
+    fprintf(fp, "Corrected FFT:   %s \n", o.dispCorrFFT.c_str());
+  }
+  if (!o.fnDark.empty()) fprintf(fp, "  -fdk  %s\n", o.fnDark.c_str());
+  if (!o.fnNorm.empty()) fprintf(fp, "  -fnm  %s\n", o.fnNorm.c_str());
+  fprintf(fp, "  -itr  %d\n", p.iter);
+  fprintf(fp, "  -ith  %f\n", p.iterthres);
+  fprintf(fp, "******Parameter End******\n\n");
+  fclose(fp);
+}
+
+// Reads a one- or two-frame reference (DFAlign.cu:614-695).
+bool read_ref(const std::string& fn, const char* what, const char* plural, int nx, int ny, std::vector<float>& r1,
+              std::vector<float>& r2) {
+  char str[1024];
+  MrcStack s;
+  if (s.open(fn.c_str()) <= 0) {
+    snprintf(str, sizeof(str), "Error: Failed to open %s reference %s .", what, fn.c_str());
+    message(str);
+    return false;
+  }
+  if (nx != s.header().nx || ny != s.header().ny) {
+    snprintf(str, sizeof(str), "Error: Image dimension of %s reference %s differs from image stack .", what,
+             fn.c_str());
+    message(str);
+    return false;
+  }
+  r1.resize((size_t)nx * ny);
+  if (!s.read_frame_float(r1.data(), 0)) {
+    snprintf(str, sizeof(str), "Error: Failed to read %s reference %s .", what, fn.c_str());
+    message(str);
+    return false;
+  }
+  if (s.header().nz > 1) {
+    snprintf(str, sizeof(str), "Processing two %s references.", plural);
+    message(str);
+    r2.resize((size_t)nx * ny);
+    s.read_frame_float(r2.data(), 1);
+  } else {
+    snprintf(str, sizeof(str), "Processing single %s reference.", plural);
+    message(str);
+    r2.clear();
+  }
+  return true;
+}
+
+// ThreadFunc_cuAlign (DFAlign.cu:456-1355) around libmc.
+int run_align(Options& o) {
+  char str[2048];
+  const char* fn = o.fnStack.c_str();
+  if (starts_with_tiff(fn) || starts_with_gzip(fn)) {
+    message("Error: TIFF and MRC-gz stacks are not supported by this build; convert to MRC.");
+    return 1;
+  }
+  if (!is_mrc(fn)) {
+    message("Only MRC, MRC-gz, TIFF file formats are supported.");
+    return 1;
+  }
+  MrcStack stack;
+  if (stack.open(fn) <= 0) {
+    snprintf(str, sizeof(str), "Error: Failed to open stack %s .", fn);
+    message(str);
+    return 1;
+  }
+  const MrcHeader h = stack.header();
+  if (o.xscale > 1.0f || o.yscale > 1.0f) message("Warning: -scx/-scy stretching is not applied by this build.");
+  if (o.bSaveRawSum || o.bSaveStackCorr || o.bSaveCCmap || o.bLogFSC || o.nEndSum2 > 0 || o.bSaveSubAreaCorrSum)
+    message("Warning: -srs/-ssc/-scc/-fsc/-2es/-sub outputs are not produced by this build.");
+  mc_plan* plan = nullptr;
+  int rc = mc_plan_create(&o.p, h.nx, h.ny, h.nz, h.mode, &plan);
+  if (rc != MC_OK) {
+    snprintf(str, sizeof(str), "%s", mc_last_error());
+    message(str);
+    return 1;
+  }
+  mc_plan_set_log(plan, log_cb, nullptr);
+  mc_info info;
+  mc_plan_info(plan, &info);
+  std::vector<float> dark, dark2, norm, norm2;
+  if (!o.fnDark.empty() && !read_ref(o.fnDark, "dark", "dark", h.nx, h.ny, dark, dark2)) {
+    mc_plan_destroy(plan);
+    return 1;
+  }
+  if (!o.fnNorm.empty() && !read_ref(o.fnNorm, "gain", "norm", h.nx, h.ny, norm, norm2)) {
+    mc_plan_destroy(plan);
+    return 1;
+  }
+  if (!dark.empty() || !norm.empty()) {
+    rc = mc_plan_set_refs(plan, dark.empty() ? nullptr : dark.data(), dark2.empty() ? nullptr : dark2.data(),
+                          norm.empty() ? nullptr : norm.data(), norm2.empty() ? nullptr : norm2.data());
+    if (rc != MC_OK) {
+      message(mc_last_error());
+      mc_plan_destroy(plan);
+      return 1;
+    }
+  }
+  // frames nStart..nEnd, read in chunks and handed to the library
+  const size_t fb = stack.frame_bytes();
+  const int chunk = 8;
+  std::vector<unsigned char> buf(fb * chunk);
+  for (int f = 0; f < info.nframe; f += chunk) {
+    const int cnt = std::min(chunk, info.nframe - f);
+    const int got = stack.read_frames(buf.data(), info.nstart + f, cnt);
+    for (int k = got; k < cnt; k++) {
+      snprintf(str, sizeof(str), "Error when reading #%03d\n", info.nstart + f + k);
+      text_output(str);
+      std::memset(buf.data() + (size_t)k * fb, 0, fb);
+    }
+    rc = mc_plan_load_frames(plan, buf.data(), f, cnt);  // returns once buf may be reused
+    if (rc != MC_OK) {
+      message(mc_last_error());
+      mc_plan_destroy(plan);
+      return 1;
+    }
+  }
+  std::vector<float> image((size_t)info.nsam * info.nsam);
+  rc = mc_plan_run(plan, image.data());
+  if (rc != MC_OK) {
+    snprintf(str, sizeof(str), "Error: %s (%s)", mc_strerror(rc), mc_last_error());
+    message(str);
+    mc_plan_destroy(plan);
+    return 1;
+  }
+  MrcHeader oh;
+  if (!write_mrc_float(o.fnAlignsum.c_str(), image.data(), info.nsam, info.nsam, 1, &oh)) {
+    snprintf(str, sizeof(str), "Error: Failed to write %s\n", o.fnAlignsum.c_str());
+    text_output(str);
+    mc_plan_destroy(plan);
+    return 1;
+  }
+  snprintf(str, sizeof(str), "Mean=%f   Min=%f   Max=%f\n", oh.dmean, oh.dmin, oh.dmax);
+  text_output(str);
+  snprintf(str, sizeof(str), "Save Sum to: %s\n", o.fnAlignsum.c_str());
+  text_output(str);
+  text_output("Done.\n");
+  mc_plan_destroy(plan);
+  return 0;
+}
+
+}  // namespace
+
+int main(int narg, char* argv[]) {
+  if (narg == 1) {
+    usage();
+    return 0;
+  }
+  Options o;
+  g_opt = &o;
+  if (!get_para(narg, argv, o)) {
+    printf("Error: Have wrong parameters. Abort!\n");
+    return 1;
+  }
+  show_para(o);
+  return run_align(o);
+}

@@ -1,0 +1,150 @@
+// Kernel argument blocks and launchers of libmc.
+//
+// Spectrum layout in HBM: one frame's half spectrum is stored column-major,
+// spec[kx * ldn + ky] for kx in [0, n/2], ky in [0, n) (ky >= n/2 meaning
+// ky - n), ldn = n rounded up to a multiple of 4 complex (32 bytes).  Every
+// ky-column is contiguous, so the per-column work of the pair and sum stages
+// reads whole 29.7 KB columns (n = 3710) with unit stride.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fft_engine.cuh"
+
+namespace mc {
+
+// ---------------------------------------------------------------- forward --
+// Pass A: decode + dark/gain + crop + row R2C of length nu, keeping kx < hk,
+// written transposed: T[kx * ldt + y].
+struct FwdRowsArgs {
+  const void* frame;   // ny rows of nx pixels (MRC pixel type `mode`)
+  int mode;            // 0 int8, 1 int16, 2 float32, 6 uint16
+  int nx, ny;
+  int offx, offy, nu;  // square crop
+  int hk;              // kept kx columns (n/2 + 1)
+  const float* dark;   // nx*ny or null
+  const float* dark2;  // nx*ny or null (0 when dark given)
+  const float* norm;   // nx*ny or null
+  const float* norm2;  // nx*ny or null (1 when norm given)
+  int two_outputs;     // 1: refs make hbuf != hbuf2, row y -> (outA, outB)
+  float2* outA;
+  float2* outB;
+  int ldt;
+  FftPlan1D plan;      // length nu, forward
+  const float2* tw;    // nu twiddles exp(-2 pi i m / nu)
+};
+
+// Pass B and every other batched transform over contiguous rows:
+// out_row[i] = X[i] for i < keep_lo, X[i + n_in - n_out] otherwise.
+struct RowsFftArgs {
+  const float2* in;
+  long long ld_in;
+  float2* out;
+  long long ld_out;
+  int nrows;
+  int n_out;
+  int keep_lo;
+  float scale;
+  FftPlan1D plan;
+  const float2* tw;
+};
+
+// ------------------------------------------------------------------ pairs --
+// Column stage: for pair p and column kx,
+//   G[p][kx][m] = sum_ky c(ky) exp(+2 pi i ky y_m / n),  y_m = (ystart+m) mod n
+//   c(ky) = A[kx][ky] conj(B[kx][ky]) exp(mbf*(kx^2+ky^2)) / ((n/2+1) n)
+// evaluated with n = P*Q: Q-point inverse FFTs of the P stride-P subsequences
+// followed by a P-term sum per output.
+struct PairColsArgs {
+  const float2* specA;
+  long long strideA;   // elements between frames (0: one shared spectrum)
+  const float2* specB;
+  long long strideB;
+  const int2* pairs;   // (frame of A, frame of B)
+  int npairs;
+  int pairs_per_cta;
+  int n, ldn, H;
+  float mbf;           // -0.5*bfactor/n/n as float
+  float inv_size;      // 1 / ((n/2+1) n)
+  int P, Q;
+  FftPlan1D qplan;     // length Q
+  const float2* twQ;   // Q twiddles exp(-2 pi i m / Q)
+  const float2* twO;   // [P][box] exp(+2 pi i k1 y_m / n)
+  int box;
+  int ystart;
+  float2* G;           // [npairs][H][box]
+};
+
+// Row stage: box[p][yb][xb] = sum_kx Re(G[p][kx][yb] * h(kx) exp(+2 pi i kx x_xb / n))
+// with h = 1 at kx = 0, n/2 and 2 otherwise; cs[kx][xb] = h*(cos, sin).
+struct PairRowsArgs {
+  const float2* G;
+  int npairs, H, box;
+  const float2* cs;    // [H][box]
+  float* boxes;        // [npairs][box][box]
+};
+
+// Peak: integer argmax over the box, 16x16 sub-box, x32 Fourier upsampling,
+// argmax on the 512x512 grid (all in FP64).
+struct PeakArgs {
+  const float* boxes;
+  int npairs, box, n, nps;
+  const double* w16;   // [16][9] cosine-mask weights
+  float* shift;        // [npairs][2]
+  float* cc;           // [npairs]
+  int* peak;           // [npairs][2] integer box peak (x, y)
+};
+
+// -------------------------------------------------------------------- sum --
+// sum_f spec_f[kx][ky] * exp(+2 pi i (sx_f kx + sy_f ky) / n) over a frame list.
+// mode 0: write the sum spectrum out[kx*ld_out + ky].
+// mode 1: inverse FFT along ky and write transposed t2[y*ld_t2 + kx].
+struct ShiftSumArgs {
+  const float2* spec;
+  long long stride;
+  const int* frames;     // positions of the summed frames
+  const double2* shifts; // (sx, sy) per listed frame
+  const int* apply;      // 1 = multiply by the phase ramp, 0 = add unshifted
+  int nsum;
+  int n, ldn, H;
+  int mode;
+  float2* out;
+  long long ld_out;
+  FftPlan1D plan;        // length n (mode 1)
+  const float2* tw;
+};
+
+// C2R of rows y, y+1 packed as one complex inverse FFT: image[y][x] * scale.
+struct C2rRowsArgs {
+  const float2* t2;
+  long long ld_t2;
+  int n, H;
+  float scale;
+  float* image;          // n x n
+  FftPlan1D plan;        // length n
+  const float2* tw;
+};
+
+// Phase-ramp tables for the sum: ey[f][ky] = exp(+2 pi i sy_f ky_signed / n).
+struct RampArgs {
+  const double2* shifts;
+  int nsum, n;
+  float2* ey;            // [nsum][n]
+};
+
+cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st);
+cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st);
+cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st);
+cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st);
+cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
+// ey: scratch of nsum*n float2 for the per-frame ky phase ramps
+cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
+cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
+
+size_t fwd_rows_smem(int nu);
+size_t rows_fft_smem(int n, int rows_per_cta);
+size_t pair_cols_smem(int n, int P, int Q, int box);
+size_t shift_sum_smem(int n, int nsum);
+size_t c2r_rows_smem(int n);
+size_t peak_smem();
+
+}  // namespace mc

@@ -1,0 +1,615 @@
+// Hand-written sm_100a kernels of the drift-correction path.
+//
+//   k_fwd_rows    decode + dark/gain + crop + row R2C, transposed store    (DFAlign.cu:710-806)
+//   k_rows_fft    batched row FFTs: forward column pass with Fourier-crop binning
+//                 (cufunc.cu:162-176, 223-227) and the inverse passes
+//   k_pair_cols   cross-power x B-factor + pruned inverse FFT along ky     (cufunc.cu:343-370)
+//   k_pair_rows   pruned C2R along kx onto the pbx window                  (cufunc.cu:229-233, 404-407)
+//   k_peak        integer peak + x32 Fourier-upsampled sub-pixel peak     (cufunc.cu:396-497)
+//   k_shift_sum   phase-shift-and-accumulate (+ inverse column FFT)       (cufunc.cu:372-393)
+//   k_c2r_rows    final C2R rows x 1/n^2                                   (DFAlign.cu:1287-1292)
+#include <math.h>
+#include <stdint.h>
+#include "kernels.cuh"
+
+namespace mc {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ float load_pixel(const void* frame, int mode, long long idx) {
+  switch (mode) {
+    case 0: return (float)((const int8_t*)frame)[idx];
+    case 1: return (float)((const int16_t*)frame)[idx];
+    case 6: return (float)((const uint16_t*)frame)[idx];
+    default: return ((const float*)frame)[idx];
+  }
+}
+
+// exp(+/-2 pi i m / len) tables live in shared memory for the whole kernel.
+__device__ __forceinline__ void copy_table(float2* dst, const float2* __restrict__ src, int cnt) {
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = src[i];
+}
+
+}  // namespace
+
+// =========================================================== forward rows ==
+__global__ void __launch_bounds__(kThreads) k_fwd_rows(FwdRowsArgs a) {
+  extern __shared__ float2 sm[];
+  const int nu = a.nu;
+  float2* b0 = sm;
+  float2* b1 = sm + nu;
+  float2* tw = sm + 2 * nu;
+  copy_table(tw, a.tw, nu);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // rows handled by this CTA
+  int y0, y1;
+  if (a.two_outputs) {
+    y0 = blockIdx.x;
+    y1 = y0;
+  } else {
+    y0 = 2 * blockIdx.x;
+    y1 = y0 + 1;
+  }
+  const bool hasd = a.dark != nullptr, hasn = a.norm != nullptr;
+  const long long r0 = (long long)(a.offy + y0) * a.nx + a.offx;
+  const long long r1 = (long long)(a.offy + y1) * a.nx + a.offx;
+  for (int x = tid; x < nu; x += nth) {
+    float re, im;
+    if (a.two_outputs) {
+      const long long i0 = r0 + x;
+      const float raw = load_pixel(a.frame, a.mode, i0);
+      const float d1 = hasd ? a.dark[i0] : 0.f;
+      const float d2 = hasd ? (a.dark2 ? a.dark2[i0] : 0.f) : 0.f;
+      const float g1 = hasn ? a.norm[i0] : 1.f;
+      const float g2 = hasn ? (a.norm2 ? a.norm2[i0] : 1.f) : 1.f;
+      re = (raw - d1) * g1;  // hbuf   (DFAlign.cu:725)
+      im = (raw - d2) * g2;  // hbuf2  (DFAlign.cu:724)
+    } else {
+      re = load_pixel(a.frame, a.mode, r0 + x);
+      im = load_pixel(a.frame, a.mode, r1 + x);
+      if (hasd || hasn) {  // identical references: one spectrum per frame
+        const long long i0 = r0 + x, i1 = r1 + x;
+        re = (re - (hasd ? a.dark[i0] : 0.f)) * (hasn ? a.norm[i0] : 1.f);
+        im = (im - (hasd ? a.dark[i1] : 0.f)) * (hasn ? a.norm[i1] : 1.f);
+      }
+    }
+    b0[x] = make_float2(re, im);
+  }
+  __syncthreads();
+  float2* Z = fft_run<false, false>(b0, b1, a.plan, 1, nu, tw, tid, nth);
+  // split the two real transforms: X = (Z(k) + conj Z(-k))/2, Y = -i (Z(k) - conj Z(-k))/2
+  for (int k = tid; k < a.hk; k += nth) {
+    const float2 z = Z[k];
+    const float2 zc = Z[k == 0 ? 0 : nu - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    if (a.two_outputs) {
+      a.outA[(long long)k * a.ldt + y0] = X;
+      a.outB[(long long)k * a.ldt + y0] = Y;
+    } else {
+      float4* dst = reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0);
+      *dst = make_float4(X.x, X.y, Y.x, Y.y);
+    }
+  }
+}
+
+size_t fwd_rows_smem(int nu) { return (size_t)3 * nu * sizeof(float2); }
+
+cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st) {
+  const size_t smem = fwd_rows_smem(a.nu);
+  cudaError_t e = cudaFuncSetAttribute(k_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int grid = a.two_outputs ? a.nu : a.nu / 2;
+  k_fwd_rows<<<grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ========================================================= row transforms ==
+template <bool INV>
+__global__ void __launch_bounds__(kThreads) k_rows_fft(RowsFftArgs a, int rows_per_cta) {
+  extern __shared__ float2 sm[];
+  const int n = a.plan.n;
+  const int B = rows_per_cta;
+  float2* b0 = sm;
+  float2* b1 = sm + (size_t)B * n;
+  float2* tw = sm + (size_t)2 * B * n;
+  copy_table(tw, a.tw, n);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int row0 = blockIdx.x * B;
+  const int nb = min(B, a.nrows - row0);
+  for (int t = tid; t < B * n; t += nth) {
+    const int b = t / n, i = t - b * n;
+    b0[t] = (b < nb) ? a.in[(long long)(row0 + b) * a.ld_in + i] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* X = fft_run<INV, false>(b0, b1, a.plan, B, n, tw, tid, nth);
+  const int shift = n - a.n_out;
+  for (int t = tid; t < nb * a.n_out; t += nth) {
+    const int b = t / a.n_out, i = t - b * a.n_out;
+    const int src = (i < a.keep_lo) ? i : i + shift;
+    const float2 v = X[b * n + src];
+    a.out[(long long)(row0 + b) * a.ld_out + i] = make_float2(v.x * a.scale, v.y * a.scale);
+  }
+}
+
+size_t rows_fft_smem(int n, int rows_per_cta) {
+  return (size_t)(2 * rows_per_cta + 1) * n * sizeof(float2);
+}
+
+cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st) {
+  const size_t smem = rows_fft_smem(a.plan.n, rows_per_cta);
+  const int grid = (a.nrows + rows_per_cta - 1) / rows_per_cta;
+  cudaError_t e;
+  if (inverse) {
+    e = cudaFuncSetAttribute(k_rows_fft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_rows_fft<true><<<grid, kThreads, smem, st>>>(a, rows_per_cta);
+  } else {
+    e = cudaFuncSetAttribute(k_rows_fft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_rows_fft<false><<<grid, kThreads, smem, st>>>(a, rows_per_cta);
+  }
+  return cudaGetLastError();
+}
+
+// ============================================================ pair columns ==
+size_t pair_cols_smem(int n, int P, int Q, int box) {
+  return (size_t)2 * n * sizeof(float2)       // ping-pong
+         + (size_t)n * sizeof(float)          // B-factor column
+         + (size_t)Q * sizeof(float2)         // inner twiddles
+         + (size_t)P * box * sizeof(float2);  // outer twiddles
+}
+
+__global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, P = a.P, Q = a.Q, box = a.box;
+  float2* x0 = sm;
+  float2* x1 = sm + n;
+  float* wcol = reinterpret_cast<float*>(sm + 2 * n);
+  float2* twQ = reinterpret_cast<float2*>(wcol + n + (n & 1));  // keep 8-byte alignment
+  float2* twO = twQ + Q;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int kx = blockIdx.y;
+  copy_table(twQ, a.twQ, Q);
+  copy_table(twO, a.twO, P * box);
+  const int half = n / 2;
+  for (int ky = tid; ky < n; ky += nth) {
+    const int y = ky < half ? ky : ky - n;
+    const float r2 = (float)(kx * kx + y * y);
+    wcol[ky] = expf(a.mbf * r2) * a.inv_size;
+  }
+  __syncthreads();
+  const int p0 = blockIdx.x * a.pairs_per_cta;
+  const int p1 = min(p0 + a.pairs_per_cta, a.npairs);
+  const int nout = box * 2;  // two threads per output (k1 halves)
+  const int khalf = (P + 1) / 2;
+  for (int p = p0; p < p1; p++) {
+    const int2 pr = a.pairs[p];
+    const float2* ca = a.specA + (long long)pr.x * a.strideA + (long long)kx * a.ldn;
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    for (int ky = tid; ky < n; ky += nth) {
+      const float2 u = ca[ky], v = cb[ky];
+      x0[ky] = cscale(cmulc(u, v), wcol[ky]);
+    }
+    __syncthreads();
+    const float2* Y = fft_run<true, true>(x0, x1, a.qplan, P, 0, twQ, tid, nth);
+    for (int base = 0; base < nout; base += nth) {
+      const int o = base + tid;
+      const bool ok = o < nout;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = Y + (long long)P * r;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = twO[k * box + m];
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
+  const size_t smem = pair_cols_smem(a.n, a.P, a.Q, a.box) + 16;
+  cudaError_t e = cudaFuncSetAttribute(k_pair_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
+  k_pair_cols<<<grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// =============================================================== pair rows ==
+// 16x16 threads, each a 6x6 register tile of the 96x96 output block; kx in
+// chunks of 32 staged through shared memory.
+constexpr int kRowTile = 96;
+constexpr int kRowK = 16;
+
+__global__ void __launch_bounds__(kThreads) k_pair_rows(PairRowsArgs a) {
+  __shared__ float2 gs[kRowK][kRowTile];
+  __shared__ float2 cs[kRowK][kRowTile];
+  const int p = blockIdx.x;
+  const int box = a.box;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const float2* G = a.G + (long long)p * a.H * box;
+  for (int yb0 = 0; yb0 < box; yb0 += kRowTile) {
+    for (int xb0 = 0; xb0 < box; xb0 += kRowTile) {
+      float acc[6][6];
+#pragma unroll
+      for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) acc[i][j] = 0.f;
+      for (int k0 = 0; k0 < a.H; k0 += kRowK) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kRowK * kRowTile; t += blockDim.x) {
+          const int kk = t / kRowTile, c = t - kk * kRowTile;
+          const int kx = k0 + kk;
+          const bool okk = kx < a.H;
+          gs[kk][c] = (okk && yb0 + c < box) ? G[(long long)kx * box + yb0 + c] : make_float2(0.f, 0.f);
+          cs[kk][c] = (okk && xb0 + c < box) ? a.cs[(long long)kx * box + xb0 + c] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < kRowK; kk++) {
+          float2 g[6], c[6];
+#pragma unroll
+          for (int i = 0; i < 6; i++) g[i] = gs[kk][ty + 16 * i];
+#pragma unroll
+          for (int j = 0; j < 6; j++) c[j] = cs[kk][tx + 16 * j];
+#pragma unroll
+          for (int i = 0; i < 6; i++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) acc[i][j] = fmaf(g[i].x, c[j].x, fmaf(-g[i].y, c[j].y, acc[i][j]));
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        const int yb = yb0 + ty + 16 * i;
+        if (yb >= box) continue;
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          const int xb = xb0 + tx + 16 * j;
+          if (xb < box) a.boxes[((long long)p * box + yb) * box + xb] = acc[i][j];
+        }
+      }
+    }
+  }
+}
+
+cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st) {
+  k_pair_rows<<<a.npairs, kThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ==================================================================== peak ==
+constexpr int kSub = 16;
+constexpr int kPad = 512;
+constexpr int kUp = 32;
+
+struct PeakSmem {
+  double2 g1[kPad][8];     // column-inverse of the masked sub-box spectrum
+  double2 tw[kPad];        // exp(+2 pi i m / 512)
+  double2 s[kSub][9];      // masked 16x16 half spectrum
+  double2 rx[kSub][9];     // row transforms of the sub-box
+  double sub[kSub][kSub];
+  double rv[kThreads / 32];
+  int ri[kThreads / 32];
+  float fv[kThreads / 32];
+  int fi[kThreads / 32];
+  double f00;
+};
+
+size_t peak_smem() { return sizeof(PeakSmem); }
+
+// (v, i) beats (bv, bi): larger value, or equal value and earlier scan index.
+template <typename T>
+__device__ __forceinline__ bool better(T v, int i, T bv, int bi) {
+  return v > bv || (v == bv && i < bi);
+}
+
+__global__ void __launch_bounds__(kThreads) k_peak(PeakArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  PeakSmem& S = *reinterpret_cast<PeakSmem*>(smraw);
+  const int p = blockIdx.x;
+  const int box = a.box;
+  const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5;
+  const float* bm = a.boxes + (long long)p * box * box;
+  const int wnoise = a.nps - 1;
+  const int hb = box / 2;
+
+  // ---- integer peak (cufunc.cu:409-424): strict '>' from -1e9, y outer, x inner
+  float bv = -1e9f;
+  int bi = 0x7fffffff;
+  for (int idx = tid; idx < box * box; idx += nth) {
+    const int yy = idx / box, xx = idx - yy * box;
+    if (abs(xx - hb) <= wnoise && abs(yy - hb) <= wnoise) continue;
+    const float v = bm[idx];
+    if (v > -1e9f && better(v, idx, bv, bi)) {
+      bv = v;
+      bi = idx;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (better(ov, oi, bv, bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  if (lane == 0) {
+    S.fv[wid] = bv;
+    S.fi[wid] = bi;
+  }
+  __syncthreads();
+  bv = S.fv[0];
+  bi = S.fi[0];
+  for (int w = 1; w < nth / 32; w++)
+    if (better(S.fv[w], S.fi[w], bv, bi)) {
+      bv = S.fv[w];
+      bi = S.fi[w];
+    }
+  int ix = 0, iy = 0;
+  if (bi != 0x7fffffff) {
+    iy = bi / box;
+    ix = bi - iy * box;
+  }
+  int offx = ix - kSub / 2, offy = iy - kSub / 2;
+  if (offx + kSub > box) offx = box - kSub;
+  else if (offx < 0) offx = 0;
+  if (offy + kSub > box) offy = box - kSub;
+  else if (offy < 0) offy = 0;
+
+  // ---- sub-box, tables
+  for (int t = tid; t < kSub * kSub; t += nth) {
+    const int yy = t / kSub, xx = t - yy * kSub;
+    S.sub[yy][xx] = (double)bm[(offy + yy) * box + offx + xx];
+  }
+  for (int m = tid; m < kPad; m += nth) {
+    double sn, cn;
+    sincospi((double)m / (kPad / 2), &sn, &cn);
+    S.tw[m] = make_double2(cn, sn);
+  }
+  __syncthreads();
+  // R2C along x: rx[y][kx] = sum_x sub[y][x] exp(-2 pi i kx x / 16)
+  for (int t = tid; t < kSub * 9; t += nth) {
+    const int yy = t / 9, k = t - yy * 9;
+    double re = 0.0, im = 0.0;
+    for (int xx = 0; xx < kSub; xx++) {
+      const double2 w = S.tw[((k * xx) & (kSub - 1)) * (kPad / kSub)];
+      re += S.sub[yy][xx] * w.x;
+      im -= S.sub[yy][xx] * w.y;
+    }
+    S.rx[yy][k] = make_double2(re, im);
+  }
+  __syncthreads();
+  // along y, then the cosine mask (func.cpp:348-370)
+  for (int t = tid; t < kSub * 9; t += nth) {
+    const int j = t / 9, k = t - j * 9;
+    double re = 0.0, im = 0.0;
+    for (int yy = 0; yy < kSub; yy++) {
+      const double2 w = S.tw[((j * yy) & (kSub - 1)) * (kPad / kSub)];  // exp(+i..)
+      const double2 v = S.rx[yy][k];
+      re += v.x * w.x + v.y * w.y;  // v * conj(w)
+      im += v.y * w.x - v.x * w.y;
+    }
+    const double wt = a.w16[j * 9 + k];
+    S.s[j][k] = make_double2(re * wt, im * wt);
+  }
+  __syncthreads();
+  // zero-padded inverse along y: g1[Y][kx] = sum_j s[j][kx] exp(+2 pi i ky_j Y / 512)
+  for (int t = tid; t < kPad * 8; t += nth) {
+    const int Y = t >> 3, k = t & 7;
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < kSub; j++) {
+      const int ky = j < kSub / 2 ? j : j - kSub;
+      const double2 w = S.tw[(ky * Y) & (kPad - 1)];
+      const double2 v = S.s[j][k];
+      re += v.x * w.x - v.y * w.y;
+      im += v.x * w.y + v.y * w.x;
+    }
+    S.g1[Y][k] = make_double2(re, im);
+  }
+  __syncthreads();
+  // C2R along x on the 512 grid and the argmax (cufunc.cu:457-476)
+  const int ox = (hb - offx) * kUp, oy = (hb - offy) * kUp, wns = kUp * wnoise;
+  double best = -INFINITY;
+  int bidx = 0x7fffffff;
+  for (int X = tid; X < kPad; X += nth) {
+    double2 c[8];
+#pragma unroll
+    for (int k = 1; k < 8; k++) c[k] = S.tw[(k * X) & (kPad - 1)];
+    const bool xex = abs(X - ox) <= wns;
+    for (int Y = 0; Y < kPad; Y++) {
+      double f = S.g1[Y][0].x;
+#pragma unroll
+      for (int k = 1; k < 8; k++) {
+        const double2 g = S.g1[Y][k];
+        f += 2.0 * (g.x * c[k].x - g.y * c[k].y);
+      }
+      if (X == 0 && Y == 0) S.f00 = f;
+      if (xex && abs(Y - oy) <= wns) continue;
+      const int idx = Y * kPad + X;
+      if (better(f, idx, best, bidx)) {
+        best = f;
+        bidx = idx;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    if (better(ov, oi, best, bidx)) {
+      best = ov;
+      bidx = oi;
+    }
+  }
+  __syncthreads();
+  if (lane == 0) {
+    S.rv[wid] = best;
+    S.ri[wid] = bidx;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < nth / 32; w++)
+      if (better(S.rv[w], S.ri[w], best, bidx)) {
+        best = S.rv[w];
+        bidx = S.ri[w];
+      }
+    int sxp = 0, syp = 0;
+    double bestcc = S.f00;
+    if (bidx != 0x7fffffff && best > S.f00) {
+      sxp = bidx % kPad;
+      syp = bidx / kPad;
+      bestcc = best;
+    }
+    const float sx = (float)(offx + sxp / (double)kUp) - (float)hb;
+    const float sy = (float)(offy + syp / (double)kUp) - (float)hb;
+    a.shift[2 * p] = sx;
+    a.shift[2 * p + 1] = sy;
+    a.cc[p] = (float)(bestcc / a.n / a.n / kSub / kSub);
+    a.peak[2 * p] = ix;
+    a.peak[2 * p + 1] = iy;
+  }
+}
+
+cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st) {
+  const size_t smem = peak_smem();
+  cudaError_t e = cudaFuncSetAttribute(k_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_peak<<<a.npairs, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ============================================================== shift-sum ==
+size_t shift_sum_smem(int n, int nsum) {
+  return (size_t)3 * n * sizeof(float2) + (size_t)nsum * sizeof(float2);
+}
+
+__global__ void __launch_bounds__(kThreads) k_shift_sum(ShiftSumArgs a, const float2* __restrict__ ey) {
+  extern __shared__ float2 sm[];
+  const int n = a.n;
+  float2* acc = sm;
+  float2* b1 = sm + n;
+  float2* tw = sm + 2 * n;
+  float2* ex = sm + 3 * n;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int kx = blockIdx.x;
+  if (a.mode == 1) copy_table(tw, a.tw, n);
+  for (int f = tid; f < a.nsum; f += nth) {
+    double sn, cn;
+    // exp(+2 pi i sx kx / n), argument reduced in double
+    const double t = a.shifts[f].x * (double)kx / (double)n;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  for (int ky = tid; ky < n; ky += nth) acc[ky] = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int f = 0; f < a.nsum; f++) {
+    const float2* col = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
+    const float2 e = ex[f];
+    const float2* eyf = ey + (long long)f * n;
+    const bool ap = a.apply[f] != 0;
+    for (int ky = tid; ky < n; ky += nth) {
+      float2 v = col[ky];
+      if (ap) v = cmul(v, cmul(e, eyf[ky]));
+      acc[ky] = cadd(acc[ky], v);
+    }
+  }
+  __syncthreads();
+  if (a.mode == 0) {
+    for (int ky = tid; ky < n; ky += nth) a.out[(long long)kx * a.ld_out + ky] = acc[ky];
+    return;
+  }
+  float2* X = fft_run<true, false>(acc, b1, a.plan, 1, n, tw, tid, nth);
+  for (int y = tid; y < n; y += nth) a.out[(long long)y * a.ld_out + kx] = X[y];
+}
+
+__global__ void k_ramp(RampArgs a) {
+  const int f = blockIdx.y;
+  const double sy = a.shifts[f].y;
+  for (int ky = blockIdx.x * blockDim.x + threadIdx.x; ky < a.n; ky += gridDim.x * blockDim.x) {
+    const int y = ky < a.n / 2 ? ky : ky - a.n;
+    const double t = sy * (double)y / (double)a.n;
+    double sn, cn;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    a.ey[(long long)f * a.n + ky] = make_float2((float)cn, (float)sn);
+  }
+}
+
+cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st) {
+  RampArgs r;
+  r.shifts = a.shifts;
+  r.nsum = a.nsum;
+  r.n = a.n;
+  r.ey = ey;
+  dim3 g((a.n + 255) / 256, a.nsum);
+  k_ramp<<<g, 256, 0, st>>>(r);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = shift_sum_smem(a.n, a.nsum);
+  e = cudaFuncSetAttribute(k_shift_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_shift_sum<<<a.H, kThreads, smem, st>>>(a, ey);
+  return cudaGetLastError();
+}
+
+// ================================================================ C2R rows ==
+size_t c2r_rows_smem(int n) { return (size_t)3 * n * sizeof(float2); }
+
+__global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, H = a.H, half = n / 2;
+  float2* b0 = sm;
+  float2* b1 = sm + n;
+  float2* tw = sm + 2 * n;
+  copy_table(tw, a.tw, n);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const float2* g0 = a.t2 + (long long)y0 * a.ld_t2;
+  const float2* g1 = a.t2 + (long long)y1 * a.ld_t2;
+  for (int k = tid; k < n; k += nth) {
+    float2 u, v;
+    if (k <= half) {
+      u = g0[k];
+      v = g1[k];
+      if (k == 0 || k == half) {  // C2R uses only the real part of DC and Nyquist
+        u.y = 0.f;
+        v.y = 0.f;
+      }
+    } else {
+      u = g0[n - k];
+      v = g1[n - k];
+      u.y = -u.y;
+      v.y = -v.y;
+    }
+    b0[k] = make_float2(u.x - v.y, u.y + v.x);  // u + i v
+  }
+  (void)H;
+  __syncthreads();
+  float2* X = fft_run<true, false>(b0, b1, a.plan, 1, n, tw, tid, nth);
+  for (int x = tid; x < n; x += nth) {
+    const float2 z = X[x];
+    a.image[(long long)y0 * n + x] = z.x * a.scale;
+    a.image[(long long)y1 * n + x] = z.y * a.scale;
+  }
+}
+
+cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st) {
+  const size_t smem = c2r_rows_smem(a.n);
+  cudaError_t e = cudaFuncSetAttribute(k_c2r_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_c2r_rows<<<a.n / 2, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace mc

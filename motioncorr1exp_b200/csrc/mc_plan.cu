@@ -1,0 +1,1242 @@
+// Host orchestration and C ABI of libmc (include/mc.h).
+//
+// One plan = one stack geometry on one GPU.  The whole aligned frame range
+// stays resident in HBM: raw frames (file pixel type), their half spectra
+// (column-major, see kernels.cuh), the per-pair scratch and the sum buffers.
+// Per movie the host only solves the small FP64 least-squares system.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mc.h"
+#include "kernels.cuh"
+#include "lsq.h"
+
+using mc::cplx;
+using mc::FftPlan1D;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return set_err(MC_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                     __LINE__);                                                                    \
+  } while (0)
+
+#define CKR(expr)           \
+  do {                      \
+    int r_ = (expr);        \
+    if (r_ != MC_OK) return r_; \
+  } while (0)
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kPairBatch = 512;
+constexpr int kPairsPerCta = 32;
+
+inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+// ----------------------------------------------------------- FFT planning --
+const int kFixedRadices[] = {53, 13, 11, 7, 5, 3};
+
+std::vector<int> factor_radices(int n) {
+  std::vector<int> r;
+  int m = n;
+  for (int p : kFixedRadices)
+    while (m % p == 0) {
+      r.push_back(p);
+      m /= p;
+    }
+  int twos = 0;
+  while (m % 2 == 0) {
+    twos++;
+    m /= 2;
+  }
+  // remaining primes -> runtime-radix stages (placed first: no twiddles)
+  std::vector<int> generic;
+  for (int p = 3; (long long)p * p <= m; p += 2)
+    while (m % p == 0) {
+      generic.push_back(p);
+      m /= p;
+    }
+  if (m > 1) generic.push_back(m);
+  std::vector<int> pw;
+  while (twos >= 3) {
+    if (twos == 4) {
+      pw.push_back(4);
+      pw.push_back(4);
+      twos = 0;
+      break;
+    }
+    pw.push_back(8);
+    twos -= 3;
+  }
+  if (twos == 2) pw.push_back(4);
+  if (twos == 1) pw.push_back(2);
+  std::vector<int> out = generic;
+  out.insert(out.end(), r.begin(), r.end());
+  out.insert(out.end(), pw.begin(), pw.end());
+  return out;
+}
+
+bool make_plan(int n, FftPlan1D& p) {
+  std::vector<int> rad = factor_radices(n);
+  if ((int)rad.size() > mc::kMaxStages) return false;
+  p.n = n;
+  p.nst = (int)rad.size();
+  int ns = 1;
+  for (int s = 0; s < p.nst; s++) {
+    mc::FftStage& st = p.st[s];
+    st.R = rad[s];
+    st.Ns = ns;
+    st.tws = n / (ns * rad[s]);
+    st.nsdiv = mc::make_fastdiv((uint32_t)ns);
+    st.nqdiv = mc::make_fastdiv((uint32_t)(n / rad[s]));
+    ns *= rad[s];
+  }
+  return ns == n || n == 1;
+}
+
+// largest prime factor of n
+int max_prime(int n) {
+  int best = 1, m = n;
+  for (int p = 2; (long long)p * p <= m; p++)
+    while (m % p == 0) {
+      best = p;
+      m /= p;
+    }
+  return std::max(best, m);
+}
+
+double radix_cost(int r) {
+  switch (r) {
+    case 2: return 2.0;
+    case 4: return 2.5;
+    case 8: return 3.0;
+    case 3: return 3.0;
+    case 5: return 4.0;
+    case 7: return 5.0;
+    case 11: return 7.0;
+    case 13: return 8.0;
+    default: return (double)r;
+  }
+}
+
+// n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
+void choose_prune(int n, int box, int& P, int& Q) {
+  double best = 1e300;
+  P = n;
+  Q = 1;
+  for (int q = 1; q <= n; q++) {
+    if (n % q) continue;
+    const int p = n / q;
+    if ((long long)p * box > 8192) continue;  // outer table must fit in shared memory
+    if (q > 1 && max_prime(q) > 13) continue;
+    double c = 0.0;
+    if (q > 1) {
+      std::vector<int> rad = factor_radices(q);
+      for (size_t s = 0; s < rad.size(); s++) c += radix_cost(rad[s]) + (s ? 2.0 : 0.0);
+    }
+    const double cost = (double)n * c + 4.0 * box * p;
+    if (cost < best) {
+      best = cost;
+      P = p;
+      Q = q;
+    }
+  }
+}
+
+std::vector<float2> twiddles(int n, int sign) {
+  std::vector<float2> t(n);
+  for (int m = 0; m < n; m++) {
+    const double a = sign * 2.0 * kPi * (double)m / (double)n;
+    t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  return t;
+}
+
+int verify_crop_size(int nx, int ny, int offx, int offy, int nsamout, float fb) {
+  if (offx < 0 || offx >= nx || offy < 0 || offy >= ny || fb <= 0) return 0;
+  if (nsamout <= 0) nsamout = std::min(nx - offx, ny - offy);
+  if (nx - offx < nsamout) nsamout = nx - offx;
+  if (ny - offy < nsamout) nsamout = ny - offy;
+  if (std::fabs(fb - 1.0) < 0.0001) nsamout = nsamout / 2 * 2;
+  else if (std::fabs(fb - 2.0) < 0.0001) nsamout = nsamout / 4 * 4;
+  else nsamout = nsamout / 2 * 2;
+  return nsamout;
+}
+
+int word_length(int mode) {
+  switch (mode) {
+    case 0: return 1;
+    case 1: return 2;
+    case 2: return 4;
+    case 6: return 2;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+// ================================================================= plan ==
+struct mc_plan {
+  mc_params p{};
+  int nx = 0, ny = 0, nz = 0, mode = 0, wl = 0;
+  int nstart = 0, nend = 0, nframe = 0;
+  int nu = 0, n = 0, H = 0, ldn = 0, ldu = 0, ldt2 = 0;
+  int box = 0, ystart = 0, P = 1, Q = 1;
+  bool two_sets = false;
+  float binf = 1.f;
+  size_t frame_bytes = 0;
+  long long fstride = 0;  // complex elements per stored spectrum
+  size_t dev_bytes = 0;
+  cudaStream_t st = nullptr;
+  int device = 0;
+  mc_log_fn logfn = nullptr;
+  void* loguser = nullptr;
+
+  FftPlan1D plan_nu{}, plan_n{}, plan_q{};
+
+  // device memory
+  void* d_frames = nullptr;
+  float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
+  float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
+  float2 *d_tw_nu = nullptr, *d_tw_n = nullptr, *d_twQ = nullptr, *d_twO = nullptr, *d_cs = nullptr;
+  double* d_w16 = nullptr;
+  int2* d_pairs = nullptr;
+  float2* d_G = nullptr;
+  float* d_boxes = nullptr;
+  float *d_pshift = nullptr, *d_pcc = nullptr;
+  int* d_ppeak = nullptr;
+  float2 *d_sum = nullptr, *d_T2 = nullptr, *d_ey = nullptr;
+  float* d_image = nullptr;
+  int *d_sumframes = nullptr, *d_apply = nullptr;
+  double2* d_sumshift = nullptr;
+  int maxp = 0;
+  std::vector<void*> allocs;
+
+  // state
+  bool loaded_all = false, have_forward = false, have_pairs = false, have_solve = false, have_iter = false;
+  std::vector<char> loaded;
+
+  // results
+  std::vector<mc::PairIJ> pairs;
+  std::vector<float> pshift, pcc;
+  std::vector<int> ppeak;
+  std::vector<float> frame_mean;
+  std::vector<double> ki1, ki2;
+  std::vector<int> good;
+  std::vector<cplx> shift;        // per step (nframe-1)
+  std::vector<cplx> frame_shift;  // cumulative (nframe)
+  std::vector<cplx> sum_shift;
+  int sum_first = 0, sum_last = -1;
+  mc_timings tm{};
+  cudaEvent_t ev[8]{};
+
+  // per-kernel accounting: launches and algorithmic bytes always, device
+  // time (one event pair per launch) when profiling is on
+  bool profiling = false;
+  std::vector<cudaEvent_t> kpool;
+  struct KRec {
+    int kind, e0, e1;
+  };
+  std::vector<KRec> krec;
+  int kused = 0;
+  double kbytes[MC_KERNEL_KINDS] = {};
+  double kms[MC_KERNEL_KINDS] = {};
+  long long kcount[MC_KERNEL_KINDS] = {};
+
+  int kevent(cudaEvent_t* e) {
+    if (kused == (int)kpool.size()) {
+      cudaEvent_t x;
+      CK(cudaEventCreate(&x));
+      kpool.push_back(x);
+    }
+    *e = kpool[kused++];
+    return MC_OK;
+  }
+  int kstart(int kind, int* slot) {
+    *slot = -1;
+    if (!profiling) return MC_OK;
+    cudaEvent_t e;
+    CKR(kevent(&e));
+    CK(cudaEventRecord(e, st));
+    krec.push_back({kind, kused - 1, -1});
+    *slot = (int)krec.size() - 1;
+    return MC_OK;
+  }
+  int kstop(int kind, int slot, double bytes) {
+    kcount[kind]++;
+    kbytes[kind] += bytes;
+    if (slot < 0) return MC_OK;
+    cudaEvent_t e;
+    CKR(kevent(&e));
+    CK(cudaEventRecord(e, st));
+    krec[slot].e1 = kused - 1;
+    return MC_OK;
+  }
+  // after a stream synchronisation: fold the recorded launches into kms
+  int collect() {
+    for (const KRec& r : krec) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, kpool[r.e0], kpool[r.e1]));
+      kms[r.kind] += ms;
+    }
+    krec.clear();
+    kused = 0;
+    return MC_OK;
+  }
+
+  void log(const char* fmt, ...) {
+    if (!logfn) return;
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    logfn(buf, loguser);
+  }
+
+  template <typename T>
+  int alloc(T** ptr, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MC_E_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    allocs.push_back(q);
+    dev_bytes += bytes;
+    *ptr = (T*)q;
+    return MC_OK;
+  }
+
+  ~mc_plan() {
+    if (device >= 0) cudaSetDevice(device);
+    if (st) cudaStreamSynchronize(st);
+    for (void* q : allocs) cudaFree(q);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : kpool) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+// launch `call` as kernel kind `kind` moving `bytes` algorithmic bytes
+#define LAUNCH(pl, kind, bytes, call)        \
+  do {                                       \
+    int slot_;                               \
+    CKR((pl)->kstart((kind), &slot_));       \
+    CK(call);                                \
+    CKR((pl)->kstop((kind), slot_, (bytes))); \
+  } while (0)
+
+template <typename T>
+int upload(mc_plan* pl, T* dst, const std::vector<T>& src) {
+  CK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, pl->st));
+  return MC_OK;
+}
+
+float2* specA_at(mc_plan* pl, int f) { return pl->d_specA + (long long)f * pl->fstride; }
+float2* specB_at(mc_plan* pl, int f) { return pl->d_specB + (long long)f * pl->fstride; }
+
+// pair stage over an explicit list: (a-frame, b-frame) into a/b spectrum sets
+int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
+                  const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
+                  std::vector<int>& peak) {
+  const int np = (int)list.size();
+  shift.assign(2 * (size_t)np, 0.f);
+  cc.assign(np, 0.f);
+  peak.assign(2 * (size_t)np, 0);
+  std::vector<int2> pr(np);
+  for (int i = 0; i < np; i++) pr[i] = make_int2(list[i].first, list[i].second);
+  if (np > pl->maxp) return set_err(MC_E_STATE, "pair list larger than the plan's capacity");
+  CK(cudaMemcpyAsync(pl->d_pairs, pr.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, pl->st));
+  const float mbf = (float)(-0.5 * (double)pl->p.bfactor / pl->n / pl->n);
+  for (int p0 = 0; p0 < np; p0 += kPairBatch) {
+    const int nb = std::min(kPairBatch, np - p0);
+    mc::PairColsArgs a{};
+    a.specA = specA;
+    a.strideA = strideA;
+    a.specB = specB;
+    a.strideB = strideB;
+    a.pairs = pl->d_pairs + p0;
+    a.npairs = nb;
+    a.pairs_per_cta = kPairsPerCta;
+    a.n = pl->n;
+    a.ldn = pl->ldn;
+    a.H = pl->H;
+    a.mbf = mbf;
+    a.inv_size = (float)(1.0 / ((double)(pl->n / 2 + 1) * pl->n));
+    a.P = pl->P;
+    a.Q = pl->Q;
+    a.qplan = pl->plan_q;
+    a.twQ = pl->d_twQ;
+    a.twO = pl->d_twO;
+    a.box = pl->box;
+    a.ystart = pl->ystart;
+    a.G = pl->d_G;
+    // algorithmic bytes: every distinct spectrum the batch touches read once,
+    // the column-stage output written once
+    std::vector<char> seenA(pl->nframe + 1, 0), seenB(pl->nframe + 1, 0);
+    long long nspec = 0;
+    for (int i = p0; i < p0 + nb; i++) {
+      const int fa = strideA ? list[i].first : pl->nframe, fb = list[i].second;
+      if (!seenA[fa]) {
+        seenA[fa] = 1;
+        nspec++;
+      }
+      const bool same = (specA == specB && strideA == strideB && fa == fb);
+      if (!seenB[fb] && !(same && seenA[fb])) {
+        seenB[fb] = 1;
+        nspec++;
+      }
+    }
+    const double gbytes = (double)nb * pl->H * pl->box * sizeof(float2);
+    LAUNCH(pl, MC_K_PAIR_COLS, (double)nspec * pl->H * pl->n * sizeof(float2) + gbytes,
+           mc::launch_pair_cols(a, pl->st));
+    mc::PairRowsArgs r{};
+    r.G = pl->d_G;
+    r.npairs = nb;
+    r.H = pl->H;
+    r.box = pl->box;
+    r.cs = pl->d_cs;
+    r.boxes = pl->d_boxes + (long long)p0 * pl->box * pl->box;
+    LAUNCH(pl, MC_K_PAIR_ROWS,
+           gbytes + (double)pl->H * pl->box * sizeof(float2) + (double)nb * pl->box * pl->box * sizeof(float),
+           mc::launch_pair_rows(r, pl->st));
+  }
+  mc::PeakArgs k{};
+  k.boxes = pl->d_boxes;
+  k.npairs = np;
+  k.box = pl->box;
+  k.n = pl->n;
+  k.nps = pl->p.NoisePeakSize;
+  k.w16 = pl->d_w16;
+  k.shift = pl->d_pshift;
+  k.cc = pl->d_pcc;
+  k.peak = pl->d_ppeak;
+  LAUNCH(pl, MC_K_PEAK, (double)np * pl->box * pl->box * sizeof(float) + (double)np * 5 * sizeof(float),
+         mc::launch_peak(k, pl->st));
+  CK(cudaMemcpyAsync(shift.data(), pl->d_pshift, sizeof(float) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(cc.data(), pl->d_pcc, sizeof(float) * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(peak.data(), pl->d_ppeak, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  return pl->collect();
+}
+
+// sum of phase-shifted frames of set A; mode 0 -> d_sum spectrum, mode 1 -> image
+int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector<cplx>& shifts,
+                  const std::vector<int>& apply, int mode) {
+  const int ns = (int)frames.size();
+  std::vector<double2> sh(ns);
+  for (int i = 0; i < ns; i++) sh[i] = make_double2(shifts[i].real(), shifts[i].imag());
+  CK(cudaMemcpyAsync(pl->d_sumframes, frames.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_apply, apply.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_sumshift, sh.data(), sizeof(double2) * ns, cudaMemcpyHostToDevice, pl->st));
+  mc::ShiftSumArgs a{};
+  a.spec = pl->d_specA;
+  a.stride = pl->fstride;
+  a.frames = pl->d_sumframes;
+  a.shifts = pl->d_sumshift;
+  a.apply = pl->d_apply;
+  a.nsum = ns;
+  a.n = pl->n;
+  a.ldn = pl->ldn;
+  a.H = pl->H;
+  a.mode = mode;
+  a.plan = pl->plan_n;
+  a.tw = pl->d_tw_n;
+  if (mode == 0) {
+    a.out = pl->d_sum;
+    a.ld_out = pl->ldn;
+  } else {
+    a.out = pl->d_T2;
+    a.ld_out = pl->ldt2;
+  }
+  const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);
+  LAUNCH(pl, MC_K_SHIFT_SUM, (double)ns * spec_bytes + spec_bytes, mc::launch_shift_sum(a, pl->d_ey, pl->st));
+  if (mode == 1) {
+    mc::C2rRowsArgs c{};
+    c.t2 = pl->d_T2;
+    c.ld_t2 = pl->ldt2;
+    c.n = pl->n;
+    c.H = pl->H;
+    c.scale = (float)(1.0 / ((double)pl->n * pl->n));
+    c.image = pl->d_image;
+    c.plan = pl->plan_n;
+    c.tw = pl->d_tw_n;
+    LAUNCH(pl, MC_K_C2R_ROWS, spec_bytes + (double)pl->n * pl->n * sizeof(float), mc::launch_c2r_rows(c, pl->st));
+  }
+  return MC_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI ==
+extern "C" {
+
+int mc_version(void) { return MC_VERSION; }
+
+const char* mc_strerror(int code) {
+  switch (code) {
+    case MC_OK: return "ok";
+    case MC_E_ARG: return "invalid argument";
+    case MC_E_CUDA: return "CUDA error";
+    case MC_E_NOMEM: return "out of memory";
+    case MC_E_SIZE: return "unsupported size";
+    case MC_E_STATE: return "call out of order";
+    case MC_E_NUMERIC: return "singular least-squares system";
+    default: return "unknown error";
+  }
+}
+
+const char* mc_last_error(void) { return g_err.c_str(); }
+
+void mc_default_params(mc_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->bin = 1.0f;
+  p->bfactor = 150.f;
+  p->CCPeakSearchDim = 96;
+  p->FrameDistOffset = 2;
+  p->NoisePeakSize = 0;
+  p->kiThresh = 1.0f;
+  p->bAlignToMid = 1;
+  p->iter = 0;
+  p->iterthres = 0.f;
+  p->refine = 0;
+}
+
+int mc_verify_params(mc_params* p, int nz) {
+  if (!p) return set_err(MC_E_ARG, "null params");
+  if (nz <= 1) return set_err(MC_E_ARG, "Not a stack or wrong file. Abort");
+  if (p->nStart < 0) p->nStart = 0;
+  if (p->nEnd >= nz) p->nEnd = nz - 1;
+  if (p->nEnd <= p->nStart) p->nEnd = nz - 1;
+  if (p->nStartSum < p->nStart) p->nStartSum = p->nStart;
+  if (p->nEndSum > p->nEnd) p->nEndSum = p->nEnd;
+  if (p->nEndSum <= p->nStartSum) p->nEndSum = p->nEnd;
+  if (p->FrameDistOffset >= nz / 2 || p->FrameDistOffset < 0)
+    return set_err(MC_E_ARG, "Frame distance offset is too big or less than 0. Abort");
+  return MC_OK;
+}
+
+void* mc_plan_stream(mc_plan* pl) { return pl ? (void*)pl->st : nullptr; }
+
+void mc_plan_set_log(mc_plan* pl, mc_log_fn fn, void* user) {
+  if (!pl) return;
+  pl->logfn = fn;
+  pl->loguser = user;
+}
+
+void mc_plan_destroy(mc_plan* pl) { delete pl; }
+
+int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_plan** out) {
+  if (!pin || !out) return set_err(MC_E_ARG, "null argument");
+  *out = nullptr;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return set_err(MC_E_ARG, "bad stack size %d x %d x %d", nx, ny, nz);
+  if (word_length(mode) == 0) return set_err(MC_E_ARG, "unsupported MRC mode %d", mode);
+  mc_plan* pl = new mc_plan();
+  std::unique_ptr<mc_plan> guard(pl);
+  pl->p = *pin;
+  mc_params& p = pl->p;
+  // bin clamp of getPara (dosefgpu_driftcorr.cpp:174-190)
+  if (p.bin > 2.0001f) p.bin = 2.0f;
+  else if (p.bin < 0.9999f) p.bin = 1.0f;
+  pl->binf = p.bin;
+  pl->nx = nx;
+  pl->ny = ny;
+  pl->nz = nz;
+  pl->mode = mode;
+  pl->wl = word_length(mode);
+  pl->device = p.GPUNum;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (p.GPUNum < 0 || p.GPUNum >= ndev)
+    return set_err(MC_E_ARG, "GPU ID %d is out of range(%d). Abort.", p.GPUNum, ndev);
+  CK(cudaSetDevice(p.GPUNum));
+  // geometry (DFAlign.cu:500-530)
+  pl->nu = verify_crop_size(nx, ny, p.crop_offsetx, p.crop_offsety, p.crop_nsam, p.bin);
+  if (pl->nu <= 0) return set_err(MC_E_ARG, "Error: Wrong image Size.");
+  pl->n = (int)((float)pl->nu / p.bin) / 2 * 2;
+  if (pl->n < 16) return set_err(MC_E_SIZE, "binned size %d below 16", pl->n);
+  pl->nstart = std::max(p.nStart, 0);
+  pl->nend = std::min(p.nEnd, nz - 1);
+  pl->nframe = pl->nend - pl->nstart + 1;
+  if (pl->nframe < 2) return set_err(MC_E_ARG, "need at least two frames (nStart %d, nEnd %d)", pl->nstart, pl->nend);
+  pl->box = p.CCPeakSearchDim;
+  if (pl->box < 16 || pl->box > 256 || pl->box > pl->n)
+    return set_err(MC_E_SIZE, "-pbx %d outside [16, min(256, %d)]", pl->box, pl->n);
+  if (pl->nu > 9216) return set_err(MC_E_SIZE, "crop side %d above 9216", pl->nu);
+  pl->H = pl->n / 2 + 1;
+  pl->ldn = (int)round_up(pl->n, 4);
+  pl->ldu = (pl->nu == pl->n) ? pl->ldn : (int)round_up(pl->nu, 4);
+  pl->ldt2 = (int)round_up(pl->H, 4);
+  pl->fstride = (long long)pl->H * pl->ldn;
+  const int ori = (pl->n - pl->box) / 2;
+  pl->ystart = (ori + pl->n / 2) % pl->n;
+  if (!make_plan(pl->nu, pl->plan_nu) || !make_plan(pl->n, pl->plan_n))
+    return set_err(MC_E_SIZE, "no FFT plan for %d / %d", pl->nu, pl->n);
+  choose_prune(pl->n, pl->box, pl->P, pl->Q);
+  if (!make_plan(pl->Q, pl->plan_q)) return set_err(MC_E_SIZE, "no FFT plan for Q=%d", pl->Q);
+  if (mc::pair_cols_smem(pl->n, pl->P, pl->Q, pl->box) + 16 > 227 * 1024)
+    return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
+
+  CK(cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking));
+  for (auto& e : pl->ev) CK(cudaEventCreate(&e));
+
+  // pair list (mfunc.h:64-84)
+  int dist = pl->nframe / 2 - p.FrameDistOffset;
+  if (dist <= 0) dist = 1;
+  if (dist > pl->nframe / 2) dist = pl->nframe / 2;
+  for (int i = 0; i < pl->nframe; i++)
+    for (int j = i + dist; j < pl->nframe; j++) pl->pairs.push_back({i, j});
+  pl->maxp = std::max((int)pl->pairs.size(), pl->nframe);
+
+  // device buffers
+  pl->frame_bytes = (size_t)nx * ny * pl->wl;
+  CKR(pl->alloc(&pl->d_frames, pl->frame_bytes * pl->nframe));
+  CKR(pl->alloc(&pl->d_specA, sizeof(float2) * pl->fstride * pl->nframe));
+  pl->d_specB = pl->d_specA;
+  if (pl->nu != pl->n) CKR(pl->alloc(&pl->d_T, sizeof(float2) * (size_t)pl->H * pl->ldu));
+  CKR(pl->alloc(&pl->d_pairs, sizeof(int2) * pl->maxp));
+  CKR(pl->alloc(&pl->d_G, sizeof(float2) * (size_t)std::min(pl->maxp, kPairBatch) * pl->H * pl->box));
+  CKR(pl->alloc(&pl->d_boxes, sizeof(float) * (size_t)pl->maxp * pl->box * pl->box));
+  CKR(pl->alloc(&pl->d_pshift, sizeof(float) * 2 * pl->maxp));
+  CKR(pl->alloc(&pl->d_pcc, sizeof(float) * pl->maxp));
+  CKR(pl->alloc(&pl->d_ppeak, sizeof(int) * 2 * pl->maxp));
+  CKR(pl->alloc(&pl->d_sum, sizeof(float2) * pl->fstride));
+  CKR(pl->alloc(&pl->d_T2, sizeof(float2) * (size_t)pl->n * pl->ldt2));
+  CKR(pl->alloc(&pl->d_ey, sizeof(float2) * (size_t)pl->nframe * pl->n));
+  CKR(pl->alloc(&pl->d_image, sizeof(float) * (size_t)pl->n * pl->n));
+  CKR(pl->alloc(&pl->d_sumframes, sizeof(int) * pl->nframe));
+  CKR(pl->alloc(&pl->d_apply, sizeof(int) * pl->nframe));
+  CKR(pl->alloc(&pl->d_sumshift, sizeof(double2) * pl->nframe));
+
+  // tables
+  CKR(pl->alloc(&pl->d_tw_nu, sizeof(float2) * pl->nu));
+  CKR(upload(pl, pl->d_tw_nu, twiddles(pl->nu, -1)));
+  if (pl->nu == pl->n) {
+    pl->d_tw_n = pl->d_tw_nu;
+  } else {
+    CKR(pl->alloc(&pl->d_tw_n, sizeof(float2) * pl->n));
+    CKR(upload(pl, pl->d_tw_n, twiddles(pl->n, -1)));
+  }
+  CKR(pl->alloc(&pl->d_twQ, sizeof(float2) * pl->Q));
+  CKR(upload(pl, pl->d_twQ, twiddles(pl->Q, -1)));
+  {
+    std::vector<float2> two((size_t)pl->P * pl->box);
+    for (int k = 0; k < pl->P; k++)
+      for (int m = 0; m < pl->box; m++) {
+        const long long y = (pl->ystart + m) % pl->n;
+        const long long e = ((long long)k * y) % pl->n;
+        const double ang = 2.0 * kPi * (double)e / pl->n;
+        two[(size_t)k * pl->box + m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+      }
+    CKR(pl->alloc(&pl->d_twO, sizeof(float2) * two.size()));
+    CKR(upload(pl, pl->d_twO, two));
+    std::vector<float2> cs((size_t)pl->H * pl->box);
+    for (int k = 0; k < pl->H; k++) {
+      const double h = (k == 0 || k == pl->n / 2) ? 1.0 : 2.0;
+      for (int m = 0; m < pl->box; m++) {
+        const long long x = (pl->ystart + m) % pl->n;
+        const long long e = ((long long)k * x) % pl->n;
+        const double ang = 2.0 * kPi * (double)e / pl->n;
+        cs[(size_t)k * pl->box + m] = make_float2((float)(h * std::cos(ang)), (float)(h * std::sin(ang)));
+      }
+    }
+    CKR(pl->alloc(&pl->d_cs, sizeof(float2) * cs.size()));
+    CKR(upload(pl, pl->d_cs, cs));
+    // cosmask2d weights (func.cpp:348-370)
+    std::vector<double> w(16 * 9);
+    for (int j = 0; j < 16; j++) {
+      const int ky = j < 8 ? j : j - 16;
+      for (int i = 0; i < 9; i++) {
+        const int r = (int)std::sqrt((float)(i * i + ky * ky));
+        w[j * 9 + i] = r < 8 ? std::cos(r * kPi / 8.0) / 2 + 0.5 : 0.0;
+      }
+    }
+    CKR(pl->alloc(&pl->d_w16, sizeof(double) * w.size()));
+    CKR(upload(pl, pl->d_w16, w));
+  }
+  CK(cudaStreamSynchronize(pl->st));
+  pl->loaded.assign(pl->nframe, 0);
+  *out = guard.release();
+  return MC_OK;
+}
+
+int mc_plan_info(const mc_plan* pl, mc_info* i) {
+  if (!pl || !i) return set_err(MC_E_ARG, "null argument");
+  i->nx = pl->nx;
+  i->ny = pl->ny;
+  i->nz = pl->nz;
+  i->mode = pl->mode;
+  i->nsam_unbin = pl->nu;
+  i->nsam = pl->n;
+  i->nstart = pl->nstart;
+  i->nend = pl->nend;
+  i->nframe = pl->nframe;
+  i->npairs = (int)pl->pairs.size();
+  i->two_sets = pl->two_sets ? 1 : 0;
+  i->prune_p = pl->P;
+  i->prune_q = pl->Q;
+  i->device_bytes = pl->dev_bytes;
+  return MC_OK;
+}
+
+int mc_plan_set_refs(mc_plan* pl, const float* dark, const float* dark2, const float* norm, const float* norm2) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  CK(cudaSetDevice(pl->device));
+  const size_t bytes = sizeof(float) * (size_t)pl->nx * pl->ny;
+  auto put = [&](float** d, const float* h) -> int {
+    if (!h) {
+      *d = nullptr;
+      return MC_OK;
+    }
+    float* q = nullptr;
+    CKR(pl->alloc(&q, bytes));
+    CK(cudaMemcpyAsync(q, h, bytes, cudaMemcpyHostToDevice, pl->st));
+    *d = q;
+    return MC_OK;
+  };
+  if ((dark2 && !dark) || (norm2 && !norm)) return set_err(MC_E_ARG, "second reference without the first");
+  CKR(put(&pl->d_dark, dark));
+  CKR(put(&pl->d_dark2, dark2));
+  CKR(put(&pl->d_norm, norm));
+  CKR(put(&pl->d_norm2, norm2));
+  const bool two = dark || norm;
+  if (two && !pl->two_sets) {
+    CKR(pl->alloc(&pl->d_specB, sizeof(float2) * pl->fstride * pl->nframe));
+    pl->two_sets = true;
+  }
+  CK(cudaStreamSynchronize(pl->st));
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+static int load_frames(mc_plan* pl, const void* src, int first, int count, cudaMemcpyKind kind) {
+  if (!pl || !src) return set_err(MC_E_ARG, "null argument");
+  if (first < 0 || count < 0 || first + count > pl->nframe)
+    return set_err(MC_E_ARG, "frames [%d, %d) outside [0, %d)", first, first + count, pl->nframe);
+  CK(cudaSetDevice(pl->device));
+  CK(cudaMemcpyAsync((char*)pl->d_frames + (size_t)first * pl->frame_bytes, src, (size_t)count * pl->frame_bytes,
+                     kind, pl->st));
+  // the caller may reuse a host buffer as soon as this returns
+  if (kind == cudaMemcpyHostToDevice) CK(cudaStreamSynchronize(pl->st));
+  for (int i = first; i < first + count; i++) pl->loaded[i] = 1;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+int mc_plan_load_frames(mc_plan* pl, const void* frames, int first, int count) {
+  return load_frames(pl, frames, first, count, cudaMemcpyHostToDevice);
+}
+
+int mc_plan_load_frames_device(mc_plan* pl, const void* d_frames, int first, int count) {
+  return load_frames(pl, d_frames, first, count, cudaMemcpyDeviceToDevice);
+}
+
+int mc_plan_forward(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  for (int f = 0; f < pl->nframe; f++)
+    if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
+  CK(cudaSetDevice(pl->device));
+  CK(cudaEventRecord(pl->ev[0], pl->st));
+  const bool binned = pl->nu != pl->n;
+  for (int f = 0; f < pl->nframe; f++) {
+    mc::FwdRowsArgs a{};
+    a.frame = (const char*)pl->d_frames + (size_t)f * pl->frame_bytes;
+    a.mode = pl->mode;
+    a.nx = pl->nx;
+    a.ny = pl->ny;
+    a.offx = pl->p.crop_offsetx;
+    a.offy = pl->p.crop_offsety;
+    a.nu = pl->nu;
+    a.hk = pl->H;
+    a.dark = pl->d_dark;
+    a.dark2 = pl->d_dark2;
+    a.norm = pl->d_norm;
+    a.norm2 = pl->d_norm2;
+    a.two_outputs = pl->two_sets ? 1 : 0;
+    float2* TA = binned ? pl->d_T : specA_at(pl, f);
+    a.outA = TA;
+    a.ldt = binned ? pl->ldu : pl->ldn;
+    a.plan = pl->plan_nu;
+    a.tw = pl->d_tw_nu;
+    const int nrefs = (pl->d_dark ? 1 : 0) + (pl->d_dark2 ? 1 : 0) + (pl->d_norm ? 1 : 0) + (pl->d_norm2 ? 1 : 0);
+    const double crop_bytes = (double)pl->nu * pl->nu * (pl->wl + 4.0 * nrefs);
+    const double t_bytes = (double)pl->H * pl->nu * sizeof(float2);
+    const double s_bytes = (double)pl->H * pl->n * sizeof(float2);
+    float2* TB = nullptr;
+    if (pl->two_sets) TB = binned ? nullptr : specB_at(pl, f);
+    if (pl->two_sets && binned) {
+      // binned two-set case: set A, then set B, each through the scratch d_T
+      // with its references folded into the one-output row transform
+      for (int set = 0; set < 2; set++) {
+        mc::FwdRowsArgs b = a;
+        b.two_outputs = 0;
+        b.dark = set == 0 ? pl->d_dark : pl->d_dark2;
+        b.norm = set == 0 ? pl->d_norm : pl->d_norm2;
+        b.dark2 = nullptr;
+        b.norm2 = nullptr;
+        b.outA = pl->d_T;
+        LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes, mc::launch_fwd_rows(b, pl->st));
+        mc::RowsFftArgs c{};
+        c.in = pl->d_T;
+        c.ld_in = pl->ldu;
+        c.out = set == 0 ? specA_at(pl, f) : specB_at(pl, f);
+        c.ld_out = pl->ldn;
+        c.nrows = pl->H;
+        c.n_out = pl->n;
+        c.keep_lo = pl->n / 2;
+        c.scale = 1.f;
+        c.plan = pl->plan_nu;
+        c.tw = pl->d_tw_nu;
+        LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, pl->st));
+      }
+      continue;
+    }
+    a.outB = TB;
+    LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes * (pl->two_sets ? 2 : 1), mc::launch_fwd_rows(a, pl->st));
+    for (int set = 0; set < (pl->two_sets ? 2 : 1); set++) {
+      mc::RowsFftArgs c{};
+      c.in = set == 0 ? TA : TB;
+      c.ld_in = a.ldt;
+      c.out = set == 0 ? specA_at(pl, f) : specB_at(pl, f);
+      c.ld_out = pl->ldn;
+      c.nrows = pl->H;
+      c.n_out = pl->n;
+      c.keep_lo = binned ? pl->n / 2 : pl->n;
+      c.scale = 1.f;
+      c.plan = pl->plan_nu;
+      c.tw = pl->d_tw_nu;
+      LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, pl->st));
+    }
+  }
+  CK(cudaEventRecord(pl->ev[1], pl->st));
+  // per-frame mean: Re F(0,0) / n / n (DFAlign.cu:818)
+  std::vector<float2> dc(pl->nframe);
+  CK(cudaMemcpy2DAsync(dc.data(), sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
+                       pl->nframe, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CKR(pl->collect());
+  CK(cudaEventElapsedTime(&pl->tm.forward_ms, pl->ev[0], pl->ev[1]));
+  pl->frame_mean.resize(pl->nframe);
+  pl->log("\nRead stack:\n");
+  for (int f = 0; f < pl->nframe; f++) {
+    pl->frame_mean[f] = dc[f].x / pl->n / pl->n;
+    pl->log("......Read and sum frame #%03d   mean:%f\n", f + pl->nstart, pl->frame_mean[f]);
+  }
+  pl->have_forward = true;
+  pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+int mc_plan_pairs(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_forward) return set_err(MC_E_STATE, "pairs before forward");
+  CK(cudaSetDevice(pl->device));
+  CK(cudaEventRecord(pl->ev[2], pl->st));
+  CKR(run_pair_list(pl, pl->d_specA, pl->fstride, pl->d_specB, pl->fstride, pl->pairs, pl->pshift, pl->pcc,
+                    pl->ppeak));
+  CK(cudaEventRecord(pl->ev[3], pl->st));
+  CK(cudaEventSynchronize(pl->ev[3]));
+  CK(cudaEventElapsedTime(&pl->tm.pairs_ms, pl->ev[2], pl->ev[3]));
+  pl->log("\nCalculate relative drift between frames\n");
+  for (size_t j = 0; j < pl->pairs.size(); j++)
+    pl->log("......%03d Frame #%03d VS #%03d xy-shift: %8.4f %8.4f      CC:%f\n", (int)j,
+            pl->pairs[j].first + pl->nstart, pl->pairs[j].second + pl->nstart, pl->pshift[2 * j],
+            pl->pshift[2 * j + 1], pl->pcc[j]);
+  pl->have_pairs = true;
+  pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+int mc_plan_solve(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_pairs) return set_err(MC_E_STATE, "solve before pairs");
+  const int np = (int)pl->pairs.size();
+  const int ncol = pl->nframe - 1;
+  std::vector<cplx> b(np);
+  for (int j = 0; j < np; j++) b[j] = cplx(pl->pshift[2 * j], pl->pshift[2 * j + 1]);
+  std::vector<int> all(np);
+  for (int j = 0; j < np; j++) all[j] = j;
+  std::vector<cplx> s;
+  if (!mc::lsq_intervals(pl->pairs, all, ncol, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
+  pl->ki1 = mc::lsq_residuals(pl->pairs, all, b, s);
+  pl->log("\n......ki: First round \n");
+  double acc = 0;
+  for (int j = 0; j < np; j++) {
+    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4lf \n", j + pl->nstart, pl->pairs[j].first + pl->nstart,
+            pl->pairs[j].second + pl->nstart, pl->ki1[j]);
+    acc += pl->ki1[j];
+  }
+  pl->log("................................Average ki: %8.4lf \n\n", acc / np);
+  pl->good = mc::od_threshold(pl->pairs, pl->ki1, pl->nframe, (double)pl->p.kiThresh);
+  if (!mc::lsq_intervals(pl->pairs, pl->good, ncol, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
+  pl->ki2 = mc::lsq_residuals(pl->pairs, pl->good, b, s);
+  pl->log("......ki: Second round \n");
+  acc = 0;
+  for (size_t j = 0; j < pl->good.size(); j++) {
+    const auto& pr = pl->pairs[pl->good[j]];
+    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4f \n", (int)j + pl->nstart, pr.first + pl->nstart,
+            pr.second + pl->nstart, pl->ki2[j]);
+    acc += pl->ki2[j];
+  }
+  pl->log("................................Average ki: %8.4lf \n\n", acc / (double)pl->good.size());
+  pl->shift = s;
+  pl->have_solve = true;
+  pl->have_iter = false;
+  return MC_OK;
+}
+
+int mc_plan_iterate(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_solve) return set_err(MC_E_STATE, "iterate before solve");
+  CK(cudaSetDevice(pl->device));
+  const int nf = pl->nframe;
+  std::vector<cplx>& shift = pl->shift;
+  pl->log("Begin Iterative Alignment... \n");
+  std::vector<cplx> newshift(nf);
+  cplx all(0, 0);
+  newshift[0] = 0;
+  for (int j = 0; j < nf - 1; j++) {
+    newshift[j + 1] = all + shift[j];
+    all += shift[j];
+  }
+  std::vector<cplx> oldshift = newshift;
+  double rmsd = 0;
+  bool converged = false;
+  int j;
+  CK(cudaEventRecord(pl->ev[4], pl->st));
+  std::vector<mc::PairIJ> fl(nf);
+  for (int k = 0; k < nf; k++) fl[k] = {0, k};
+  std::vector<int> frames(nf), apply(nf, 1);
+  for (int k = 0; k < nf; k++) frames[k] = k;
+  const float ith = pl->p.iterthres;
+  for (j = 0; j < pl->p.iter && !converged; j++) {
+    pl->log("Iteration [%d/%d]\n", j, pl->p.iter);
+    std::vector<cplx> sh(nf);
+    for (int k = 0; k < nf; k++) sh[k] = -oldshift[k];
+    CKR(run_shift_sum(pl, frames, sh, apply, 0));
+    for (int k = 0; k < nf; k++)
+      pl->log("......Add Frame #%03d with xy shift: %8.4lf %8.4lf\n", k + pl->nstart, -oldshift[k].real(),
+              -oldshift[k].imag());
+    pl->log("Sum complete... \n");
+    std::vector<float> fs, fc;
+    std::vector<int> fp;
+    CKR(run_pair_list(pl, pl->d_sum, 0, pl->d_specA, pl->fstride, fl, fs, fc, fp));
+    double avgcc = 0;
+    for (int k = 0; k < nf; k++) {
+      newshift[k] = cplx(fs[2 * k], fs[2 * k + 1]);
+      avgcc += fc[k];
+      const cplx d = oldshift[k] - newshift[k];
+      pl->log("......%03d Frame #%03d VS <sum> xy-shift: %8.4f %8.4f (%8.4f %8.4f) CC:%f\n", k, k + pl->nstart,
+              fs[2 * k], fs[2 * k + 1], d.real(), d.imag(), fc[k]);
+    }
+    const cplx ref = newshift[0];
+    for (int k = 0; k < nf; k++) {
+      const cplx d = oldshift[k] - newshift[k];
+      oldshift[k] = newshift[k] - ref;
+      rmsd += d.real() * d.real() + d.imag() * d.imag();
+    }
+    pl->log("Average CC : %8.4f\n", avgcc / nf);
+    rmsd /= nf;
+    if (rmsd < (double)(ith * ith)) {
+      converged = true;
+      pl->log("Converged at iteration [%d/%d]\n", j, pl->p.iter);
+    }
+    pl->log("RMSD to <sum> : %8.4f  (%8.4f for convergence)\n", std::sqrt(rmsd), ith);
+  }
+  CK(cudaEventRecord(pl->ev[5], pl->st));
+  CK(cudaEventSynchronize(pl->ev[5]));
+  CK(cudaEventElapsedTime(&pl->tm.iterate_ms, pl->ev[4], pl->ev[5]));
+  pl->log("Final RMSD to <sum> : %8.4f at iteration [%d/%d]\n\nShifts (delta) after iterative aligment\n",
+          std::sqrt(rmsd), j - 1, pl->p.iter);
+  pl->log("...Frame #%03d xy-shift %8.4f %8.4f (%8.4f %8.4f)\n", 0, 0.0, 0.0, 0.0, 0.0);
+  all = 0;
+  for (int k = 0; k < nf - 1; k++) {
+    all += shift[k];
+    const cplx td = all - oldshift[k + 1];
+    pl->log("...Frame #%03d xy-shift %8.4f %8.4f (%8.4f %8.4f)\n", k + 1, oldshift[k + 1].real(),
+            oldshift[k + 1].imag(), td.real(), td.imag());
+    shift[k] = oldshift[k + 1] - oldshift[k];
+  }
+  pl->log("Final shift:\n");
+  pl->frame_shift.assign(nf, cplx(0, 0));
+  cplx total(0, 0);
+  pl->log("......Shift of Frame #%03d : %8.4f %8.4f\n", pl->nstart, total.real(), total.imag());
+  for (int k = 0; k < nf - 1; k++) {
+    total = total + shift[k];
+    pl->frame_shift[k + 1] = total;
+    pl->log("......Shift of Frame #%03d : %8.4f %8.4f\n", k + pl->nstart + 1, total.real(), total.imag());
+  }
+  pl->have_iter = true;
+  return MC_OK;
+}
+
+int mc_plan_sum(mc_plan* pl, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_iter) return set_err(MC_E_STATE, "sum before the shifts are final");
+  CK(cudaSetDevice(pl->device));
+  const int nf = pl->nframe;
+  const mc_params& p = pl->p;
+  int nss = p.nStartSum - pl->nstart;
+  int nes = p.nEndSum - pl->nstart;
+  if (nss <= 0) nss = 0;
+  if (nes <= nss || nes >= nf) nes = nf - 1;
+  pl->log("\nSum Frame #%03d - #%03d\n", nss + pl->nstart, nes + pl->nstart);
+  cplx mid(0, 0);
+  if (p.bAlignToMid) {
+    int ref = pl->nz / 2 + 1;
+    if (ref < pl->nstart) ref = pl->nstart;
+    // the reference reads past the shift vector when ref-nStart > nframe-1
+    const int lim = std::min(ref - pl->nstart, nf - 1);
+    for (int j = 0; j < lim; j++) mid += pl->shift[j];
+  }
+  cplx total(0, 0);
+  for (int j = 1; j < nss + 1; j++) total += pl->shift[j - 1];
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  pl->sum_shift.assign(nf, cplx(0, 0));
+  for (int k = nss; k <= nes; k++) {
+    if (k > nss) total += pl->shift[k - 1];
+    const cplx s = -total + mid;
+    frames.push_back(k);
+    sh.push_back(s);
+    apply.push_back((k == nss && !p.bAlignToMid) ? 0 : 1);
+    pl->sum_shift[k] = s;
+    pl->log("......Add Frame #%03d with xy shift: %8.4lf %8.4lf\n", k + pl->nstart, s.real(), s.imag());
+  }
+  pl->sum_first = nss;
+  pl->sum_last = nes;
+  CK(cudaEventRecord(pl->ev[6], pl->st));
+  CKR(run_shift_sum(pl, frames, sh, apply, 1));
+  CK(cudaEventRecord(pl->ev[7], pl->st));
+  if (image_host)
+    CK(cudaMemcpyAsync(image_host, pl->d_image, sizeof(float) * (size_t)pl->n * pl->n, cudaMemcpyDeviceToHost,
+                       pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CK(cudaEventElapsedTime(&pl->tm.sum_ms, pl->ev[6], pl->ev[7]));
+  CKR(pl->collect());
+  return MC_OK;
+}
+
+int mc_plan_run(mc_plan* pl, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  pl->log("Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", pl->nx, pl->ny, pl->nz, pl->mode);
+  pl->log("Crop Image: Offset(%d %d) RawDim(%d) BinnedDim(%d)\n", pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu,
+          pl->n);
+  CKR(mc_plan_forward(pl));
+  CKR(mc_plan_pairs(pl));
+  CKR(mc_plan_solve(pl));
+  CKR(mc_plan_iterate(pl));
+  CKR(mc_plan_sum(pl, image_host));
+  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.sum_ms;
+  return MC_OK;
+}
+
+int mc_plan_get_frame_shifts(const mc_plan* pl, double* xy) {
+  if (!pl || !xy) return set_err(MC_E_ARG, "null argument");
+  if (!pl->have_iter) return set_err(MC_E_STATE, "no final shifts yet");
+  for (int k = 0; k < pl->nframe; k++) {
+    xy[2 * k] = pl->frame_shift[k].real();
+    xy[2 * k + 1] = pl->frame_shift[k].imag();
+  }
+  return MC_OK;
+}
+
+int mc_plan_get_pairs(const mc_plan* pl, int* ij, float* shift, float* cc, int* peak) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_pairs) return set_err(MC_E_STATE, "no pair results yet");
+  const size_t np = pl->pairs.size();
+  for (size_t j = 0; j < np; j++) {
+    if (ij) {
+      ij[2 * j] = pl->pairs[j].first;
+      ij[2 * j + 1] = pl->pairs[j].second;
+    }
+    if (shift) {
+      shift[2 * j] = pl->pshift[2 * j];
+      shift[2 * j + 1] = pl->pshift[2 * j + 1];
+    }
+    if (cc) cc[j] = pl->pcc[j];
+    if (peak) {
+      peak[2 * j] = pl->ppeak[2 * j];
+      peak[2 * j + 1] = pl->ppeak[2 * j + 1];
+    }
+  }
+  return MC_OK;
+}
+
+int mc_plan_get_ki(const mc_plan* pl, double* ki1, int* nkept, int* kept, double* ki2) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_solve) return set_err(MC_E_STATE, "no solve yet");
+  if (ki1) std::copy(pl->ki1.begin(), pl->ki1.end(), ki1);
+  if (nkept) *nkept = (int)pl->good.size();
+  if (kept) std::copy(pl->good.begin(), pl->good.end(), kept);
+  if (ki2) std::copy(pl->ki2.begin(), pl->ki2.end(), ki2);
+  return MC_OK;
+}
+
+int mc_plan_get_frame_means(const mc_plan* pl, float* mean) {
+  if (!pl || !mean) return set_err(MC_E_ARG, "null argument");
+  if (!pl->have_forward) return set_err(MC_E_STATE, "no forward yet");
+  std::copy(pl->frame_mean.begin(), pl->frame_mean.end(), mean);
+  return MC_OK;
+}
+
+int mc_plan_get_spectrum(mc_plan* pl, int set, int pos, void* host) {
+  if (!pl || !host) return set_err(MC_E_ARG, "null argument");
+  if (!pl->have_forward) return set_err(MC_E_STATE, "no forward yet");
+  if (pos < 0 || pos >= pl->nframe || set < 0 || set > 1) return set_err(MC_E_ARG, "bad set/pos");
+  CK(cudaSetDevice(pl->device));
+  const float2* src = (set == 0 ? pl->d_specA : pl->d_specB) + (long long)pos * pl->fstride;
+  CK(cudaMemcpy2DAsync(host, sizeof(float2) * pl->n, src, sizeof(float2) * pl->ldn, sizeof(float2) * pl->n, pl->H,
+                       cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  return MC_OK;
+}
+
+int mc_plan_get_boxes(mc_plan* pl, float* host) {
+  if (!pl || !host) return set_err(MC_E_ARG, "null argument");
+  if (!pl->have_pairs) return set_err(MC_E_STATE, "no pair results yet");
+  CK(cudaSetDevice(pl->device));
+  CK(cudaMemcpyAsync(host, pl->d_boxes, sizeof(float) * pl->pairs.size() * pl->box * pl->box,
+                     cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  return MC_OK;
+}
+
+int mc_plan_get_sum_shifts(const mc_plan* pl, double* xy, int* first, int* last) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (xy)
+    for (int k = 0; k < pl->nframe; k++) {
+      xy[2 * k] = k < (int)pl->sum_shift.size() ? pl->sum_shift[k].real() : 0.0;
+      xy[2 * k + 1] = k < (int)pl->sum_shift.size() ? pl->sum_shift[k].imag() : 0.0;
+    }
+  if (first) *first = pl->sum_first;
+  if (last) *last = pl->sum_last;
+  return MC_OK;
+}
+
+int mc_plan_get_timings(const mc_plan* pl, mc_timings* t) {
+  if (!pl || !t) return set_err(MC_E_ARG, "null argument");
+  *t = pl->tm;
+  return MC_OK;
+}
+
+void mc_plan_set_profiling(mc_plan* pl, int on) {
+  if (pl) pl->profiling = on != 0;
+}
+
+int mc_plan_reset_stats(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  for (int k = 0; k < MC_KERNEL_KINDS; k++) {
+    pl->kms[k] = 0;
+    pl->kbytes[k] = 0;
+    pl->kcount[k] = 0;
+  }
+  return MC_OK;
+}
+
+int mc_plan_kernel_stats(const mc_plan* pl, int kind, double* ms, long long* launches, double* bytes) {
+  if (!pl || kind < 0 || kind >= MC_KERNEL_KINDS) return set_err(MC_E_ARG, "bad kernel kind");
+  if (ms) *ms = pl->kms[kind];
+  if (launches) *launches = pl->kcount[kind];
+  if (bytes) *bytes = pl->kbytes[kind];
+  return MC_OK;
+}
+
+const char* mc_kernel_name(int kind) {
+  static const char* names[MC_KERNEL_KINDS] = {"k_fwd_rows", "k_rows_fft", "k_pair_cols", "k_pair_rows",
+                                               "k_peak", "k_shift_sum", "k_c2r_rows"};
+  return (kind >= 0 && kind < MC_KERNEL_KINDS) ? names[kind] : "";
+}
+
+int mc_solve_pairs(int nframe, int npairs, const int* ij, const float* shifts_xy, float kithresh,
+                   double* step_xy, double* ki1, int* nkept, int* kept, double* ki2) {
+  if (nframe < 2 || npairs < 1 || !ij || !shifts_xy) return set_err(MC_E_ARG, "bad solve arguments");
+  std::vector<mc::PairIJ> rows(npairs);
+  std::vector<cplx> b(npairs);
+  std::vector<int> all(npairs);
+  for (int r = 0; r < npairs; r++) {
+    const int i = ij[2 * r], j = ij[2 * r + 1];
+    if (i < 0 || j <= i || j >= nframe) return set_err(MC_E_ARG, "pair %d (%d, %d) invalid", r, i, j);
+    rows[r] = {i, j};
+    b[r] = cplx(shifts_xy[2 * r], shifts_xy[2 * r + 1]);
+    all[r] = r;
+  }
+  std::vector<cplx> s;
+  if (!mc::lsq_intervals(rows, all, nframe - 1, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
+  const std::vector<double> k1 = mc::lsq_residuals(rows, all, b, s);
+  const std::vector<int> good = mc::od_threshold(rows, k1, nframe, (double)kithresh);
+  if (!mc::lsq_intervals(rows, good, nframe - 1, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
+  const std::vector<double> k2 = mc::lsq_residuals(rows, good, b, s);
+  if (step_xy)
+    for (int k = 0; k < nframe - 1; k++) {
+      step_xy[2 * k] = s[k].real();
+      step_xy[2 * k + 1] = s[k].imag();
+    }
+  if (ki1) std::copy(k1.begin(), k1.end(), ki1);
+  if (nkept) *nkept = (int)good.size();
+  if (kept) std::copy(good.begin(), good.end(), kept);
+  if (ki2) std::copy(k2.begin(), k2.end(), ki2);
+  return MC_OK;
+}
+
+int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void* stream) {
+  if (n < 1 || batch < 1 || !d_in || !d_out) return set_err(MC_E_ARG, "bad fft arguments");
+  if ((size_t)3 * n * sizeof(float2) > 227 * 1024) return set_err(MC_E_SIZE, "n=%d too large", n);
+  FftPlan1D p{};
+  if (!make_plan(n, p)) return set_err(MC_E_SIZE, "no FFT plan for %d", n);
+  float2* tw = nullptr;
+  CK(cudaMalloc(&tw, sizeof(float2) * n));
+  std::vector<float2> t = twiddles(n, -1);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(tw, t.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    mc::RowsFftArgs a{};
+    a.in = (const float2*)d_in;
+    a.ld_in = n;
+    a.out = (float2*)d_out;
+    a.ld_out = n;
+    a.nrows = batch;
+    a.n_out = n;
+    a.keep_lo = n;
+    a.scale = 1.f;
+    a.plan = p;
+    a.tw = tw;
+    e = mc::launch_rows_fft(a, inverse != 0, 1, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(tw);
+  if (e != cudaSuccess) return set_err(MC_E_CUDA, "mc_fft1d: %s", cudaGetErrorString(e));
+  return MC_OK;
+}
+
+}  // extern "C"

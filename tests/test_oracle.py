@@ -1,0 +1,256 @@
+"""Known-answer tests of the FP64 oracle (CPU only).
+
+The reference ships no tests or golden vectors for this path, so the oracle
+is pinned here by construction: brute-force DFTs, analytic peaks whose
+upsampled maximum sits exactly on the 1/32 grid, exactly consistent pair
+shifts, and the pair counts of the benchmark configurations.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import mc_oracle as O
+
+
+@pytest.mark.parametrize("nframe,fod,npairs", [(16, 2, 55), (40, 7, 378), (50, 2, 378), (60, 2, 528)])
+def test_pair_counts(nframe, fod, npairs):
+    assert len(O.pair_list(nframe, fod)) == npairs
+
+
+def test_pair_list_order_and_distance():
+    pairs = O.pair_list(10, 2)  # dist = 5 - 2 = 3
+    assert pairs[:3] == [(0, 3), (0, 4), (0, 5)]
+    assert all(j - i >= 3 for i, j in pairs)
+    # clamps of mfunc.h:71-73
+    assert O.pair_distance(10, 7) == 1
+    assert O.pair_distance(10, -3) == 5
+    assert O.pair_distance(2, 0) == 1
+
+
+@pytest.mark.parametrize("args,expect", [
+    ((3838, 3710, 0, 0, 0, 1.0), 3710),
+    ((7676, 7420, 0, 0, 0, 2.0), 7420),
+    ((101, 99, 0, 0, 0, 1.0), 98),
+    ((101, 99, 0, 0, 0, 2.0), 96),
+    ((100, 100, 10, 20, 0, 1.0), 80),
+    ((100, 100, 0, 0, 500, 1.0), 100),
+    ((100, 100, 0, 0, 33, 1.0), 32),
+    ((100, 100, 100, 0, 0, 1.0), 0),
+    ((100, 100, -1, 0, 0, 1.0), 0),
+    ((100, 100, 0, 0, 0, 1.5), 100),
+])
+def test_verify_crop_size(args, expect):
+    assert O.verify_crop_size(*args) == expect
+
+
+def test_binned_size():
+    assert O.binned_size(7420, 2.0) == 3710
+    assert O.binned_size(3710, 1.0) == 3710
+    assert O.binned_size(100, 1.5) == 66
+
+
+def test_forward_spectrum_bruteforce():
+    rng = np.random.default_rng(3)
+    img = rng.standard_normal((13, 15))
+    offx, offy, nu = 2, 1, 10
+    F = O.forward_spectrum(img, offx, offy, nu, nu)
+    crop = img[offy:offy + nu, offx:offx + nu]
+    y = np.arange(nu)
+    for ky in range(nu):
+        for kx in range(nu // 2 + 1):
+            ref = np.sum(crop * np.exp(-2j * np.pi * (kx * y[None, :] + ky * y[:, None]) / nu))
+            assert abs(F[ky, kx] - ref) < 1e-10
+    # Fourier crop keeps rows [0, n/2) and [nu - n/2, nu), columns [0, n/2]
+    Fb = O.forward_spectrum(img, offx, offy, nu, 6)
+    assert Fb.shape == (6, 4)
+    np.testing.assert_allclose(Fb[:3], F[:3, :4])
+    np.testing.assert_allclose(Fb[3:], F[7:, :4])
+
+
+def test_bfactor_mask_sign_and_decay():
+    n = 8
+    z = O.bfactor_mask(n, 150.0)
+    assert z.shape == (8, 5)
+    m = float(np.float32(-0.5 * 150.0 / 64))
+    assert z[0, 0] == 1.0
+    assert z[0, 1] == pytest.approx(-math.exp(m))
+    assert z[7, 0] == pytest.approx(-math.exp(m))     # ky = -1
+    assert z[7, 1] == pytest.approx(math.exp(2 * m))  # x + y = 0: even
+
+
+def test_cc_map_bruteforce():
+    rng = np.random.default_rng(1)
+    n = 8
+    a = rng.standard_normal((n, n))
+    b = rng.standard_normal((n, n))
+    Fa, Fb = np.fft.rfft2(a), np.fft.rfft2(b)
+    mask = O.bfactor_mask(n, 40.0)
+    got = O.cc_map(Fa, Fb, mask, n)
+    # full-plane inverse DFT of the Hermitian-extended cross power, un-normalised
+    size = (n // 2 + 1) * n
+    Ffa, Ffb = np.fft.fft2(a), np.fft.fft2(b)
+    k = np.arange(n)
+    ks = np.where(k < n // 2, k, k - n)
+    mfull = np.zeros((n, n))
+    for ky in range(n):
+        for kx in range(n):
+            x, y = ks[kx], ks[ky]
+            mfull[ky, kx] = (1 if (x + y) % 2 == 0 else -1) * math.exp(
+                float(np.float32(-0.5 * 40.0 / n / n)) * (x * x + y * y))
+    C = Ffa * np.conj(Ffb) * mfull / size
+    ref = np.real(np.fft.ifft2(C)) * n * n
+    np.testing.assert_allclose(got, ref, atol=1e-9)
+
+
+def test_integer_peak_ties_and_exclusion():
+    box = np.zeros((20, 20))
+    box[5, 7] = 3.0
+    box[5, 9] = 3.0     # same row, later column
+    box[9, 2] = 3.0     # later row
+    assert O.integer_peak(box, 0) == (7, 5)
+    # exclusion |i-10|<=wNoise && |j-10|<=wNoise with wNoise = nps-1
+    box = np.zeros((20, 20))
+    box[10, 10] = 9.0
+    box[2, 3] = 1.0
+    assert O.integer_peak(box, 0) == (10, 10)
+    assert O.integer_peak(box, 1) == (3, 2)
+    # nothing above -1e9 -> (0, 0)
+    assert O.integer_peak(np.full((20, 20), -2e9), 0) == (0, 0)
+
+
+def _bump_box(box, cx, cy, dx, dy, fill=-50.0):
+    """16-periodic band-limited bump centred at (cx+dx, cy+dy), written into the
+    16x16 window [cx-8, cx+8) x [cy-8, cy+8) of a box filled with ``fill``."""
+    b = np.full((box, box), fill)
+    ys, xs = np.mgrid[cy - 8:cy + 8, cx - 8:cx + 8]
+    f = np.zeros_like(xs, dtype=np.float64)
+    for ky in range(-7, 8):
+        for kx in range(-7, 8):
+            if kx * kx + ky * ky < 49:
+                c = math.exp(-(kx * kx + ky * ky) / 8.0)
+                f += c * np.cos(2 * math.pi * (kx * (xs - cx - dx) + ky * (ys - cy - dy)) / 16.0)
+    b[cy - 8:cy + 8, cx - 8:cx + 8] = f
+    return b
+
+
+@pytest.mark.parametrize("a,b", [(0, 0), (5, -3), (-12, 12), (11, 7), (-1, -9)])
+def test_find_shift_known_subpixel(a, b):
+    box, n = 96, 512
+    cx, cy = 50, 45
+    bm = _bump_box(box, cx, cy, a / 32.0, b / 32.0)
+    sx, sy, cc, ix, iy = O.find_shift(bm, n, 0)
+    assert (ix, iy) == (cx, cy)
+    assert sx == cx - box // 2 + a / 32.0
+    assert sy == cy - box // 2 + b / 32.0
+
+
+def test_find_shift_subbox_clamped_at_edge():
+    box, n = 96, 512
+    bm = np.full((box, box), -5.0)
+    bm[2, 93] = 10.0
+    sx, sy, cc, ix, iy = O.find_shift(bm, n, 0)
+    assert (ix, iy) == (93, 2)
+    # sub-box clamped to [80, 96) x [0, 16): the result stays inside it
+    assert 80 - 48 <= sx < 96 - 48 and -48 <= sy < 16 - 48
+
+
+def test_lsq_and_threshold_exact_and_outlier():
+    nframe = 12
+    pairs = O.pair_list(nframe, 2)
+    A = O.design_matrix(pairs, nframe)
+    rng = np.random.default_rng(5)
+    steps = rng.normal(0, 1, nframe - 1) + 1j * rng.normal(0, 1, nframe - 1)
+    b = A @ steps
+    s = O.lsq(A, b)
+    np.testing.assert_allclose(s, steps, atol=1e-10)
+    ki = np.abs(A @ s - b)
+    good = O.od_threshold(A, b, ki, 1.0)
+    assert good == list(range(len(pairs)))
+    b2 = b.copy()
+    b2[7] += 6.0
+    s2 = O.lsq(A, b2)
+    ki2 = np.abs(A @ s2 - b2)
+    good2 = O.od_threshold(A, b2, ki2, 1.0)
+    assert 7 not in good2
+    s3 = O.lsq(A[good2], b2[good2])
+    np.testing.assert_allclose(s3, steps, atol=1e-9)
+
+
+def test_threshold_grows_until_full_rank():
+    # two frames, every residual above threshold: keep cols rows, rank is full
+    nframe = 6
+    pairs = O.pair_list(nframe, 0)      # dist 3
+    A = O.design_matrix(pairs, nframe)
+    ki = np.full(len(pairs), 5.0)
+    good = O.od_threshold(A, np.zeros(len(pairs)), ki, 1.0)
+    assert np.linalg.matrix_rank(A[good]) == nframe - 1
+    assert len(good) >= nframe - 1
+
+
+def _periodic_movie(n, shifts, seed=0):
+    rng = np.random.default_rng(seed)
+    F = np.fft.rfft2(rng.standard_normal((n, n)))
+    ky = np.fft.fftfreq(n)[:, None]
+    kx = np.fft.rfftfreq(n)[None, :]
+    F[np.sqrt(kx ** 2 + ky ** 2) > 0.15] = 0
+    base = np.fft.irfft2(F, s=(n, n))
+    base = 10 + 3 * base / base.std()
+    return np.stack([np.roll(base, (dy, dx), axis=(0, 1)) for dx, dy in shifts]).astype(np.float32)
+
+
+def test_align_movie_integer_shifts_exact():
+    shifts = [(0, 0), (1, 0), (2, -1), (4, -1), (5, -2), (7, -2), (8, -3), (9, -3)]
+    frames = _periodic_movie(128, shifts)
+    p = O.verify_para(O.Params(CCPeakSearchDim=48, FrameDistOffset=2), len(shifts))
+    r = O.align_movie(frames, 2, p)
+    for (i, j), s in zip(r.pairs, r.pair_shift):
+        dx = shifts[j][0] - shifts[i][0]
+        dy = shifts[j][1] - shifts[i][1]
+        assert (s.real, s.imag) == (float(-dx), float(-dy))
+    fs = np.stack([r.frame_shift.real, r.frame_shift.imag], 1)
+    np.testing.assert_allclose(fs, -np.array(shifts, dtype=float), atol=1e-9)
+    assert r.goodlist == list(range(len(r.pairs)))
+
+
+def test_align_movie_sum_is_shifted_average():
+    # with exact integer shifts the aligned sum equals nframe copies of the
+    # frame that the middle-frame reference lands on
+    shifts = [(0, 0), (2, 1), (3, 3), (5, 4), (6, 6), (8, 7)]
+    frames = _periodic_movie(96, shifts, seed=2)
+    p = O.verify_para(O.Params(CCPeakSearchDim=32, FrameDistOffset=1), len(shifts))
+    r = O.align_movie(frames, 2, p)
+    ref = len(shifts) // 2 + 1      # RefFrame = nz/2+1
+    expect = frames[ref].astype(np.float64) * len(shifts)
+    np.testing.assert_allclose(r.image, expect, rtol=1e-9, atol=1e-6)
+
+
+def test_iterative_realignment_keeps_exact_solution():
+    shifts = [(0, 0), (1, 1), (3, 1), (4, 2), (6, 3), (7, 3), (9, 4), (10, 5)]
+    frames = _periodic_movie(128, shifts, seed=4)
+    p = O.verify_para(O.Params(CCPeakSearchDim=48, iter=3, iterthres=0.001), len(shifts))
+    r = O.align_movie(frames, 2, p)
+    fs = np.stack([r.frame_shift.real, r.frame_shift.imag], 1)
+    np.testing.assert_allclose(fs, -np.array(shifts, dtype=float), atol=1e-9)
+    assert r.iter_log and r.iter_log[-1]["converged"]
+
+
+def test_apply_refs_two_reference_scheme():
+    raw = np.arange(12, dtype=np.float64).reshape(3, 4)
+    dark = np.full((3, 4), 1.0)
+    norm = np.full((3, 4), 2.0)
+    a, b = O.apply_refs(raw, dark=dark, norm=norm)
+    np.testing.assert_array_equal(a, (raw - 1) * 2)
+    np.testing.assert_array_equal(b, raw)                 # dark2 = 0, norm2 = 1
+    a, b = O.apply_refs(raw, dark=dark, dark2=dark * 3)
+    np.testing.assert_array_equal(b, raw - 3)
+    a, b = O.apply_refs(raw)
+    assert a is b
+
+
+def test_decode_modes():
+    raw = np.array([0, 127, 128, 255], dtype=np.uint8)
+    np.testing.assert_array_equal(O.decode_frame(raw, 0), [0, 127, -128, -1])   # signed char
+    u16 = np.array([0, 40000], dtype=np.uint16)
+    np.testing.assert_array_equal(O.decode_frame(u16, 6), [0, 40000])
+    np.testing.assert_array_equal(O.decode_frame(u16.view(np.int16), 1), [0, 40000 - 65536])
