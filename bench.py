@@ -73,7 +73,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -181,7 +181,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    nx, ny, nz = 3838, 3710, 40
+    nx, ny, nz = 3838, 3710, args.frames
     frames, truth = synth.make_movie_torch(nx, ny, nz, mean=1.2, seed=args.seed + rank, dtype="u8",
                                            kind="linear", speed=0.3, rw_sigma=0.5, device=f"cuda:{local}")
     host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
@@ -263,7 +263,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "nsam": plan.nsam, "pairs": plan.npairs,
+                "config": {"workload": WORKLOAD if nz == 40 else f"profiling case: {nz} frames, else as c2",
+                           "nsam": plan.nsam, "pairs": plan.npairs,
                            "l2": "inputs larger than L2 (570 MB frames, 2.2 GB spectra per movie), no flush",
                            "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.numel()),
@@ -293,6 +294,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--frames", type=int, default=40,
+                    help="movie length; 40 is the benchmark workload, fewer only for profiling captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

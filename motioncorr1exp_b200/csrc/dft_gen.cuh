@@ -1209,4 +1209,880 @@ template <bool INV> __device__ __forceinline__ void dft_r53(float2* v) {
     }
   }
 }
+constexpr int kSplit53 = 3;
+template <bool INV, typename St>
+__device__ __forceinline__ void dft_r53_part(const float2* v, int part, St&& st) {
+  const float2 x0 = v[0];
+  const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
+  const float2 d1 = make_float2(v[1].x - v[52].x, v[1].y - v[52].y);
+  const float2 s2 = make_float2(v[2].x + v[51].x, v[2].y + v[51].y);
+  const float2 d2 = make_float2(v[2].x - v[51].x, v[2].y - v[51].y);
+  const float2 s3 = make_float2(v[3].x + v[50].x, v[3].y + v[50].y);
+  const float2 d3 = make_float2(v[3].x - v[50].x, v[3].y - v[50].y);
+  const float2 s4 = make_float2(v[4].x + v[49].x, v[4].y + v[49].y);
+  const float2 d4 = make_float2(v[4].x - v[49].x, v[4].y - v[49].y);
+  const float2 s5 = make_float2(v[5].x + v[48].x, v[5].y + v[48].y);
+  const float2 d5 = make_float2(v[5].x - v[48].x, v[5].y - v[48].y);
+  const float2 s6 = make_float2(v[6].x + v[47].x, v[6].y + v[47].y);
+  const float2 d6 = make_float2(v[6].x - v[47].x, v[6].y - v[47].y);
+  const float2 s7 = make_float2(v[7].x + v[46].x, v[7].y + v[46].y);
+  const float2 d7 = make_float2(v[7].x - v[46].x, v[7].y - v[46].y);
+  const float2 s8 = make_float2(v[8].x + v[45].x, v[8].y + v[45].y);
+  const float2 d8 = make_float2(v[8].x - v[45].x, v[8].y - v[45].y);
+  const float2 s9 = make_float2(v[9].x + v[44].x, v[9].y + v[44].y);
+  const float2 d9 = make_float2(v[9].x - v[44].x, v[9].y - v[44].y);
+  const float2 s10 = make_float2(v[10].x + v[43].x, v[10].y + v[43].y);
+  const float2 d10 = make_float2(v[10].x - v[43].x, v[10].y - v[43].y);
+  const float2 s11 = make_float2(v[11].x + v[42].x, v[11].y + v[42].y);
+  const float2 d11 = make_float2(v[11].x - v[42].x, v[11].y - v[42].y);
+  const float2 s12 = make_float2(v[12].x + v[41].x, v[12].y + v[41].y);
+  const float2 d12 = make_float2(v[12].x - v[41].x, v[12].y - v[41].y);
+  const float2 s13 = make_float2(v[13].x + v[40].x, v[13].y + v[40].y);
+  const float2 d13 = make_float2(v[13].x - v[40].x, v[13].y - v[40].y);
+  const float2 s14 = make_float2(v[14].x + v[39].x, v[14].y + v[39].y);
+  const float2 d14 = make_float2(v[14].x - v[39].x, v[14].y - v[39].y);
+  const float2 s15 = make_float2(v[15].x + v[38].x, v[15].y + v[38].y);
+  const float2 d15 = make_float2(v[15].x - v[38].x, v[15].y - v[38].y);
+  const float2 s16 = make_float2(v[16].x + v[37].x, v[16].y + v[37].y);
+  const float2 d16 = make_float2(v[16].x - v[37].x, v[16].y - v[37].y);
+  const float2 s17 = make_float2(v[17].x + v[36].x, v[17].y + v[36].y);
+  const float2 d17 = make_float2(v[17].x - v[36].x, v[17].y - v[36].y);
+  const float2 s18 = make_float2(v[18].x + v[35].x, v[18].y + v[35].y);
+  const float2 d18 = make_float2(v[18].x - v[35].x, v[18].y - v[35].y);
+  const float2 s19 = make_float2(v[19].x + v[34].x, v[19].y + v[34].y);
+  const float2 d19 = make_float2(v[19].x - v[34].x, v[19].y - v[34].y);
+  const float2 s20 = make_float2(v[20].x + v[33].x, v[20].y + v[33].y);
+  const float2 d20 = make_float2(v[20].x - v[33].x, v[20].y - v[33].y);
+  const float2 s21 = make_float2(v[21].x + v[32].x, v[21].y + v[32].y);
+  const float2 d21 = make_float2(v[21].x - v[32].x, v[21].y - v[32].y);
+  const float2 s22 = make_float2(v[22].x + v[31].x, v[22].y + v[31].y);
+  const float2 d22 = make_float2(v[22].x - v[31].x, v[22].y - v[31].y);
+  const float2 s23 = make_float2(v[23].x + v[30].x, v[23].y + v[30].y);
+  const float2 d23 = make_float2(v[23].x - v[30].x, v[23].y - v[30].y);
+  const float2 s24 = make_float2(v[24].x + v[29].x, v[24].y + v[29].y);
+  const float2 d24 = make_float2(v[24].x - v[29].x, v[24].y - v[29].y);
+  const float2 s25 = make_float2(v[25].x + v[28].x, v[25].y + v[28].y);
+  const float2 d25 = make_float2(v[25].x - v[28].x, v[25].y - v[28].y);
+  const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
+  const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
+  if (part == 0) st(0, make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y)));
+  switch (part) {
+  case 0: {
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.9929810762405396f, ar); ai = fmaf(s1.y, 0.9929810762405396f, ai); br = fmaf(d1.x, 0.11827316880226135f, br); bi = fmaf(d1.y, 0.11827316880226135f, bi);
+      ar = fmaf(s2.x, 0.9720228910446167f, ar); ai = fmaf(s2.y, 0.9720228910446167f, ai); br = fmaf(d2.x, 0.2348860502243042f, br); bi = fmaf(d2.y, 0.2348860502243042f, bi);
+      ar = fmaf(s3.x, 0.9374196529388428f, ar); ai = fmaf(s3.y, 0.9374196529388428f, ai); br = fmaf(d3.x, 0.3482016324996948f, br); bi = fmaf(d3.y, 0.3482016324996948f, bi);
+      ar = fmaf(s4.x, 0.8896570801734924f, ar); ai = fmaf(s4.y, 0.8896570801734924f, ai); br = fmaf(d4.x, 0.4566292464733124f, br); bi = fmaf(d4.y, 0.4566292464733124f, bi);
+      ar = fmaf(s5.x, 0.829405665397644f, ar); ai = fmaf(s5.y, 0.829405665397644f, ai); br = fmaf(d5.x, 0.5586467385292053f, br); bi = fmaf(d5.y, 0.5586467385292053f, bi);
+      ar = fmaf(s6.x, 0.7575112581253052f, ar); ai = fmaf(s6.y, 0.7575112581253052f, ai); br = fmaf(d6.x, 0.6528221368789673f, br); bi = fmaf(d6.y, 0.6528221368789673f, bi);
+      ar = fmaf(s7.x, 0.674983024597168f, ar); ai = fmaf(s7.y, 0.674983024597168f, ai); br = fmaf(d7.x, 0.7378332614898682f, br); bi = fmaf(d7.y, 0.7378332614898682f, bi);
+      ar = fmaf(s8.x, 0.5829795002937317f, ar); ai = fmaf(s8.y, 0.5829795002937317f, ai); br = fmaf(d8.x, 0.8124868869781494f, br); bi = fmaf(d8.y, 0.8124868869781494f, bi);
+      ar = fmaf(s9.x, 0.4827921986579895f, ar); ai = fmaf(s9.y, 0.4827921986579895f, ai); br = fmaf(d9.x, 0.8757349252700806f, br); bi = fmaf(d9.y, 0.8757349252700806f, bi);
+      ar = fmaf(s10.x, 0.3758275806903839f, ar); ai = fmaf(s10.y, 0.3758275806903839f, ai); br = fmaf(d10.x, 0.926689624786377f, br); bi = fmaf(d10.y, 0.926689624786377f, bi);
+      ar = fmaf(s11.x, 0.26358717679977417f, ar); ai = fmaf(s11.y, 0.26358717679977417f, ai); br = fmaf(d11.x, 0.9646356105804443f, br); bi = fmaf(d11.y, 0.9646356105804443f, bi);
+      ar = fmaf(s12.x, 0.14764656126499176f, ar); ai = fmaf(s12.y, 0.14764656126499176f, ai); br = fmaf(d12.x, 0.989040195941925f, br); bi = fmaf(d12.y, 0.989040195941925f, bi);
+      ar = fmaf(s13.x, 0.029633328318595886f, ar); ai = fmaf(s13.y, 0.029633328318595886f, ai); br = fmaf(d13.x, 0.9995608329772949f, br); bi = fmaf(d13.y, 0.9995608329772949f, bi);
+      ar = fmaf(s14.x, -0.08879589289426804f, ar); ai = fmaf(s14.y, -0.08879589289426804f, ai); br = fmaf(d14.x, 0.9960498213768005f, br); bi = fmaf(d14.y, 0.9960498213768005f, bi);
+      ar = fmaf(s15.x, -0.2059786170721054f, ar); ai = fmaf(s15.y, -0.2059786170721054f, ai); br = fmaf(d15.x, 0.9785565137863159f, br); bi = fmaf(d15.y, 0.9785565137863159f, bi);
+      ar = fmaf(s16.x, -0.3202698528766632f, ar); ai = fmaf(s16.y, -0.3202698528766632f, ai); br = fmaf(d16.x, 0.9473263621330261f, br); bi = fmaf(d16.y, 0.9473263621330261f, bi);
+      ar = fmaf(s17.x, -0.43006521463394165f, ar); ai = fmaf(s17.y, -0.43006521463394165f, ai); br = fmaf(d17.x, 0.9027978181838989f, br); bi = fmaf(d17.y, 0.9027978181838989f, bi);
+      ar = fmaf(s18.x, -0.5338233709335327f, ar); ai = fmaf(s18.y, -0.5338233709335327f, ai); br = fmaf(d18.x, 0.8455960154533386f, br); bi = fmaf(d18.y, 0.8455960154533386f, bi);
+      ar = fmaf(s19.x, -0.6300878524780273f, ar); ai = fmaf(s19.y, -0.6300878524780273f, ai); br = fmaf(d19.x, 0.7765238881111145f, br); bi = fmaf(d19.y, 0.7765238881111145f, bi);
+      ar = fmaf(s20.x, -0.7175072431564331f, ar); ai = fmaf(s20.y, -0.7175072431564331f, ai); br = fmaf(d20.x, 0.6965510249137878f, br); bi = fmaf(d20.y, 0.6965510249137878f, bi);
+      ar = fmaf(s21.x, -0.794854462146759f, ar); ai = fmaf(s21.y, -0.794854462146759f, ai); br = fmaf(d21.x, 0.6068001389503479f, br); bi = fmaf(d21.y, 0.6068001389503479f, bi);
+      ar = fmaf(s22.x, -0.8610436320304871f, ar); ai = fmaf(s22.y, -0.8610436320304871f, ai); br = fmaf(d22.x, 0.5085310935974121f, br); bi = fmaf(d22.y, 0.5085310935974121f, bi);
+      ar = fmaf(s23.x, -0.9151456356048584f, ar); ai = fmaf(s23.y, -0.9151456356048584f, ai); br = fmaf(d23.x, 0.4031234383583069f, br); bi = fmaf(d23.y, 0.4031234383583069f, bi);
+      ar = fmaf(s24.x, -0.956400990486145f, ar); ai = fmaf(s24.y, -0.956400990486145f, ai); br = fmaf(d24.x, 0.29205676913261414f, br); bi = fmaf(d24.y, 0.29205676913261414f, bi);
+      ar = fmaf(s25.x, -0.9842305779457092f, ar); ai = fmaf(s25.y, -0.9842305779457092f, ai); br = fmaf(d25.x, 0.1768902689218521f, br); bi = fmaf(d25.y, 0.1768902689218521f, bi);
+      ar = fmaf(s26.x, -0.9982437491416931f, ar); ai = fmaf(s26.y, -0.9982437491416931f, ai); br = fmaf(d26.x, 0.05924062803387642f, br); bi = fmaf(d26.y, 0.05924062803387642f, bi);
+      if (!INV) { st(1, make_float2(ar + bi, ai - br)); st(52, make_float2(ar - bi, ai + br)); }
+      else { st(1, make_float2(ar - bi, ai + br)); st(52, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.9720228910446167f, ar); ai = fmaf(s1.y, 0.9720228910446167f, ai); br = fmaf(d1.x, 0.2348860502243042f, br); bi = fmaf(d1.y, 0.2348860502243042f, bi);
+      ar = fmaf(s2.x, 0.8896570801734924f, ar); ai = fmaf(s2.y, 0.8896570801734924f, ai); br = fmaf(d2.x, 0.4566292464733124f, br); bi = fmaf(d2.y, 0.4566292464733124f, bi);
+      ar = fmaf(s3.x, 0.7575112581253052f, ar); ai = fmaf(s3.y, 0.7575112581253052f, ai); br = fmaf(d3.x, 0.6528221368789673f, br); bi = fmaf(d3.y, 0.6528221368789673f, bi);
+      ar = fmaf(s4.x, 0.5829795002937317f, ar); ai = fmaf(s4.y, 0.5829795002937317f, ai); br = fmaf(d4.x, 0.8124868869781494f, br); bi = fmaf(d4.y, 0.8124868869781494f, bi);
+      ar = fmaf(s5.x, 0.3758275806903839f, ar); ai = fmaf(s5.y, 0.3758275806903839f, ai); br = fmaf(d5.x, 0.926689624786377f, br); bi = fmaf(d5.y, 0.926689624786377f, bi);
+      ar = fmaf(s6.x, 0.14764656126499176f, ar); ai = fmaf(s6.y, 0.14764656126499176f, ai); br = fmaf(d6.x, 0.989040195941925f, br); bi = fmaf(d6.y, 0.989040195941925f, bi);
+      ar = fmaf(s7.x, -0.08879589289426804f, ar); ai = fmaf(s7.y, -0.08879589289426804f, ai); br = fmaf(d7.x, 0.9960498213768005f, br); bi = fmaf(d7.y, 0.9960498213768005f, bi);
+      ar = fmaf(s8.x, -0.3202698528766632f, ar); ai = fmaf(s8.y, -0.3202698528766632f, ai); br = fmaf(d8.x, 0.9473263621330261f, br); bi = fmaf(d8.y, 0.9473263621330261f, bi);
+      ar = fmaf(s9.x, -0.5338233709335327f, ar); ai = fmaf(s9.y, -0.5338233709335327f, ai); br = fmaf(d9.x, 0.8455960154533386f, br); bi = fmaf(d9.y, 0.8455960154533386f, bi);
+      ar = fmaf(s10.x, -0.7175072431564331f, ar); ai = fmaf(s10.y, -0.7175072431564331f, ai); br = fmaf(d10.x, 0.6965510249137878f, br); bi = fmaf(d10.y, 0.6965510249137878f, bi);
+      ar = fmaf(s11.x, -0.8610436320304871f, ar); ai = fmaf(s11.y, -0.8610436320304871f, ai); br = fmaf(d11.x, 0.5085310935974121f, br); bi = fmaf(d11.y, 0.5085310935974121f, bi);
+      ar = fmaf(s12.x, -0.956400990486145f, ar); ai = fmaf(s12.y, -0.956400990486145f, ai); br = fmaf(d12.x, 0.29205676913261414f, br); bi = fmaf(d12.y, 0.29205676913261414f, bi);
+      ar = fmaf(s13.x, -0.9982437491416931f, ar); ai = fmaf(s13.y, -0.9982437491416931f, ai); br = fmaf(d13.x, 0.05924062803387642f, br); bi = fmaf(d13.y, 0.05924062803387642f, bi);
+      ar = fmaf(s14.x, -0.9842305779457092f, ar); ai = fmaf(s14.y, -0.9842305779457092f, ai); br = fmaf(d14.x, -0.1768902689218521f, br); bi = fmaf(d14.y, -0.1768902689218521f, bi);
+      ar = fmaf(s15.x, -0.9151456356048584f, ar); ai = fmaf(s15.y, -0.9151456356048584f, ai); br = fmaf(d15.x, -0.4031234383583069f, br); bi = fmaf(d15.y, -0.4031234383583069f, bi);
+      ar = fmaf(s16.x, -0.794854462146759f, ar); ai = fmaf(s16.y, -0.794854462146759f, ai); br = fmaf(d16.x, -0.6068001389503479f, br); bi = fmaf(d16.y, -0.6068001389503479f, bi);
+      ar = fmaf(s17.x, -0.6300878524780273f, ar); ai = fmaf(s17.y, -0.6300878524780273f, ai); br = fmaf(d17.x, -0.7765238881111145f, br); bi = fmaf(d17.y, -0.7765238881111145f, bi);
+      ar = fmaf(s18.x, -0.43006521463394165f, ar); ai = fmaf(s18.y, -0.43006521463394165f, ai); br = fmaf(d18.x, -0.9027978181838989f, br); bi = fmaf(d18.y, -0.9027978181838989f, bi);
+      ar = fmaf(s19.x, -0.2059786170721054f, ar); ai = fmaf(s19.y, -0.2059786170721054f, ai); br = fmaf(d19.x, -0.9785565137863159f, br); bi = fmaf(d19.y, -0.9785565137863159f, bi);
+      ar = fmaf(s20.x, 0.029633328318595886f, ar); ai = fmaf(s20.y, 0.029633328318595886f, ai); br = fmaf(d20.x, -0.9995608329772949f, br); bi = fmaf(d20.y, -0.9995608329772949f, bi);
+      ar = fmaf(s21.x, 0.26358717679977417f, ar); ai = fmaf(s21.y, 0.26358717679977417f, ai); br = fmaf(d21.x, -0.9646356105804443f, br); bi = fmaf(d21.y, -0.9646356105804443f, bi);
+      ar = fmaf(s22.x, 0.4827921986579895f, ar); ai = fmaf(s22.y, 0.4827921986579895f, ai); br = fmaf(d22.x, -0.8757349252700806f, br); bi = fmaf(d22.y, -0.8757349252700806f, bi);
+      ar = fmaf(s23.x, 0.674983024597168f, ar); ai = fmaf(s23.y, 0.674983024597168f, ai); br = fmaf(d23.x, -0.7378332614898682f, br); bi = fmaf(d23.y, -0.7378332614898682f, bi);
+      ar = fmaf(s24.x, 0.829405665397644f, ar); ai = fmaf(s24.y, 0.829405665397644f, ai); br = fmaf(d24.x, -0.5586467385292053f, br); bi = fmaf(d24.y, -0.5586467385292053f, bi);
+      ar = fmaf(s25.x, 0.9374196529388428f, ar); ai = fmaf(s25.y, 0.9374196529388428f, ai); br = fmaf(d25.x, -0.3482016324996948f, br); bi = fmaf(d25.y, -0.3482016324996948f, bi);
+      ar = fmaf(s26.x, 0.9929810762405396f, ar); ai = fmaf(s26.y, 0.9929810762405396f, ai); br = fmaf(d26.x, -0.11827316880226135f, br); bi = fmaf(d26.y, -0.11827316880226135f, bi);
+      if (!INV) { st(2, make_float2(ar + bi, ai - br)); st(51, make_float2(ar - bi, ai + br)); }
+      else { st(2, make_float2(ar - bi, ai + br)); st(51, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.9374196529388428f, ar); ai = fmaf(s1.y, 0.9374196529388428f, ai); br = fmaf(d1.x, 0.3482016324996948f, br); bi = fmaf(d1.y, 0.3482016324996948f, bi);
+      ar = fmaf(s2.x, 0.7575112581253052f, ar); ai = fmaf(s2.y, 0.7575112581253052f, ai); br = fmaf(d2.x, 0.6528221368789673f, br); bi = fmaf(d2.y, 0.6528221368789673f, bi);
+      ar = fmaf(s3.x, 0.4827921986579895f, ar); ai = fmaf(s3.y, 0.4827921986579895f, ai); br = fmaf(d3.x, 0.8757349252700806f, br); bi = fmaf(d3.y, 0.8757349252700806f, bi);
+      ar = fmaf(s4.x, 0.14764656126499176f, ar); ai = fmaf(s4.y, 0.14764656126499176f, ai); br = fmaf(d4.x, 0.989040195941925f, br); bi = fmaf(d4.y, 0.989040195941925f, bi);
+      ar = fmaf(s5.x, -0.2059786170721054f, ar); ai = fmaf(s5.y, -0.2059786170721054f, ai); br = fmaf(d5.x, 0.9785565137863159f, br); bi = fmaf(d5.y, 0.9785565137863159f, bi);
+      ar = fmaf(s6.x, -0.5338233709335327f, ar); ai = fmaf(s6.y, -0.5338233709335327f, ai); br = fmaf(d6.x, 0.8455960154533386f, br); bi = fmaf(d6.y, 0.8455960154533386f, bi);
+      ar = fmaf(s7.x, -0.794854462146759f, ar); ai = fmaf(s7.y, -0.794854462146759f, ai); br = fmaf(d7.x, 0.6068001389503479f, br); bi = fmaf(d7.y, 0.6068001389503479f, bi);
+      ar = fmaf(s8.x, -0.956400990486145f, ar); ai = fmaf(s8.y, -0.956400990486145f, ai); br = fmaf(d8.x, 0.29205676913261414f, br); bi = fmaf(d8.y, 0.29205676913261414f, bi);
+      ar = fmaf(s9.x, -0.9982437491416931f, ar); ai = fmaf(s9.y, -0.9982437491416931f, ai); br = fmaf(d9.x, -0.05924062803387642f, br); bi = fmaf(d9.y, -0.05924062803387642f, bi);
+      ar = fmaf(s10.x, -0.9151456356048584f, ar); ai = fmaf(s10.y, -0.9151456356048584f, ai); br = fmaf(d10.x, -0.4031234383583069f, br); bi = fmaf(d10.y, -0.4031234383583069f, bi);
+      ar = fmaf(s11.x, -0.7175072431564331f, ar); ai = fmaf(s11.y, -0.7175072431564331f, ai); br = fmaf(d11.x, -0.6965510249137878f, br); bi = fmaf(d11.y, -0.6965510249137878f, bi);
+      ar = fmaf(s12.x, -0.43006521463394165f, ar); ai = fmaf(s12.y, -0.43006521463394165f, ai); br = fmaf(d12.x, -0.9027978181838989f, br); bi = fmaf(d12.y, -0.9027978181838989f, bi);
+      ar = fmaf(s13.x, -0.08879589289426804f, ar); ai = fmaf(s13.y, -0.08879589289426804f, ai); br = fmaf(d13.x, -0.9960498213768005f, br); bi = fmaf(d13.y, -0.9960498213768005f, bi);
+      ar = fmaf(s14.x, 0.26358717679977417f, ar); ai = fmaf(s14.y, 0.26358717679977417f, ai); br = fmaf(d14.x, -0.9646356105804443f, br); bi = fmaf(d14.y, -0.9646356105804443f, bi);
+      ar = fmaf(s15.x, 0.5829795002937317f, ar); ai = fmaf(s15.y, 0.5829795002937317f, ai); br = fmaf(d15.x, -0.8124868869781494f, br); bi = fmaf(d15.y, -0.8124868869781494f, bi);
+      ar = fmaf(s16.x, 0.829405665397644f, ar); ai = fmaf(s16.y, 0.829405665397644f, ai); br = fmaf(d16.x, -0.5586467385292053f, br); bi = fmaf(d16.y, -0.5586467385292053f, bi);
+      ar = fmaf(s17.x, 0.9720228910446167f, ar); ai = fmaf(s17.y, 0.9720228910446167f, ai); br = fmaf(d17.x, -0.2348860502243042f, br); bi = fmaf(d17.y, -0.2348860502243042f, bi);
+      ar = fmaf(s18.x, 0.9929810762405396f, ar); ai = fmaf(s18.y, 0.9929810762405396f, ai); br = fmaf(d18.x, 0.11827316880226135f, br); bi = fmaf(d18.y, 0.11827316880226135f, bi);
+      ar = fmaf(s19.x, 0.8896570801734924f, ar); ai = fmaf(s19.y, 0.8896570801734924f, ai); br = fmaf(d19.x, 0.4566292464733124f, br); bi = fmaf(d19.y, 0.4566292464733124f, bi);
+      ar = fmaf(s20.x, 0.674983024597168f, ar); ai = fmaf(s20.y, 0.674983024597168f, ai); br = fmaf(d20.x, 0.7378332614898682f, br); bi = fmaf(d20.y, 0.7378332614898682f, bi);
+      ar = fmaf(s21.x, 0.3758275806903839f, ar); ai = fmaf(s21.y, 0.3758275806903839f, ai); br = fmaf(d21.x, 0.926689624786377f, br); bi = fmaf(d21.y, 0.926689624786377f, bi);
+      ar = fmaf(s22.x, 0.029633328318595886f, ar); ai = fmaf(s22.y, 0.029633328318595886f, ai); br = fmaf(d22.x, 0.9995608329772949f, br); bi = fmaf(d22.y, 0.9995608329772949f, bi);
+      ar = fmaf(s23.x, -0.3202698528766632f, ar); ai = fmaf(s23.y, -0.3202698528766632f, ai); br = fmaf(d23.x, 0.9473263621330261f, br); bi = fmaf(d23.y, 0.9473263621330261f, bi);
+      ar = fmaf(s24.x, -0.6300878524780273f, ar); ai = fmaf(s24.y, -0.6300878524780273f, ai); br = fmaf(d24.x, 0.7765238881111145f, br); bi = fmaf(d24.y, 0.7765238881111145f, bi);
+      ar = fmaf(s25.x, -0.8610436320304871f, ar); ai = fmaf(s25.y, -0.8610436320304871f, ai); br = fmaf(d25.x, 0.5085310935974121f, br); bi = fmaf(d25.y, 0.5085310935974121f, bi);
+      ar = fmaf(s26.x, -0.9842305779457092f, ar); ai = fmaf(s26.y, -0.9842305779457092f, ai); br = fmaf(d26.x, 0.1768902689218521f, br); bi = fmaf(d26.y, 0.1768902689218521f, bi);
+      if (!INV) { st(3, make_float2(ar + bi, ai - br)); st(50, make_float2(ar - bi, ai + br)); }
+      else { st(3, make_float2(ar - bi, ai + br)); st(50, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.8896570801734924f, ar); ai = fmaf(s1.y, 0.8896570801734924f, ai); br = fmaf(d1.x, 0.4566292464733124f, br); bi = fmaf(d1.y, 0.4566292464733124f, bi);
+      ar = fmaf(s2.x, 0.5829795002937317f, ar); ai = fmaf(s2.y, 0.5829795002937317f, ai); br = fmaf(d2.x, 0.8124868869781494f, br); bi = fmaf(d2.y, 0.8124868869781494f, bi);
+      ar = fmaf(s3.x, 0.14764656126499176f, ar); ai = fmaf(s3.y, 0.14764656126499176f, ai); br = fmaf(d3.x, 0.989040195941925f, br); bi = fmaf(d3.y, 0.989040195941925f, bi);
+      ar = fmaf(s4.x, -0.3202698528766632f, ar); ai = fmaf(s4.y, -0.3202698528766632f, ai); br = fmaf(d4.x, 0.9473263621330261f, br); bi = fmaf(d4.y, 0.9473263621330261f, bi);
+      ar = fmaf(s5.x, -0.7175072431564331f, ar); ai = fmaf(s5.y, -0.7175072431564331f, ai); br = fmaf(d5.x, 0.6965510249137878f, br); bi = fmaf(d5.y, 0.6965510249137878f, bi);
+      ar = fmaf(s6.x, -0.956400990486145f, ar); ai = fmaf(s6.y, -0.956400990486145f, ai); br = fmaf(d6.x, 0.29205676913261414f, br); bi = fmaf(d6.y, 0.29205676913261414f, bi);
+      ar = fmaf(s7.x, -0.9842305779457092f, ar); ai = fmaf(s7.y, -0.9842305779457092f, ai); br = fmaf(d7.x, -0.1768902689218521f, br); bi = fmaf(d7.y, -0.1768902689218521f, bi);
+      ar = fmaf(s8.x, -0.794854462146759f, ar); ai = fmaf(s8.y, -0.794854462146759f, ai); br = fmaf(d8.x, -0.6068001389503479f, br); bi = fmaf(d8.y, -0.6068001389503479f, bi);
+      ar = fmaf(s9.x, -0.43006521463394165f, ar); ai = fmaf(s9.y, -0.43006521463394165f, ai); br = fmaf(d9.x, -0.9027978181838989f, br); bi = fmaf(d9.y, -0.9027978181838989f, bi);
+      ar = fmaf(s10.x, 0.029633328318595886f, ar); ai = fmaf(s10.y, 0.029633328318595886f, ai); br = fmaf(d10.x, -0.9995608329772949f, br); bi = fmaf(d10.y, -0.9995608329772949f, bi);
+      ar = fmaf(s11.x, 0.4827921986579895f, ar); ai = fmaf(s11.y, 0.4827921986579895f, ai); br = fmaf(d11.x, -0.8757349252700806f, br); bi = fmaf(d11.y, -0.8757349252700806f, bi);
+      ar = fmaf(s12.x, 0.829405665397644f, ar); ai = fmaf(s12.y, 0.829405665397644f, ai); br = fmaf(d12.x, -0.5586467385292053f, br); bi = fmaf(d12.y, -0.5586467385292053f, bi);
+      ar = fmaf(s13.x, 0.9929810762405396f, ar); ai = fmaf(s13.y, 0.9929810762405396f, ai); br = fmaf(d13.x, -0.11827316880226135f, br); bi = fmaf(d13.y, -0.11827316880226135f, bi);
+      ar = fmaf(s14.x, 0.9374196529388428f, ar); ai = fmaf(s14.y, 0.9374196529388428f, ai); br = fmaf(d14.x, 0.3482016324996948f, br); bi = fmaf(d14.y, 0.3482016324996948f, bi);
+      ar = fmaf(s15.x, 0.674983024597168f, ar); ai = fmaf(s15.y, 0.674983024597168f, ai); br = fmaf(d15.x, 0.7378332614898682f, br); bi = fmaf(d15.y, 0.7378332614898682f, bi);
+      ar = fmaf(s16.x, 0.26358717679977417f, ar); ai = fmaf(s16.y, 0.26358717679977417f, ai); br = fmaf(d16.x, 0.9646356105804443f, br); bi = fmaf(d16.y, 0.9646356105804443f, bi);
+      ar = fmaf(s17.x, -0.2059786170721054f, ar); ai = fmaf(s17.y, -0.2059786170721054f, ai); br = fmaf(d17.x, 0.9785565137863159f, br); bi = fmaf(d17.y, 0.9785565137863159f, bi);
+      ar = fmaf(s18.x, -0.6300878524780273f, ar); ai = fmaf(s18.y, -0.6300878524780273f, ai); br = fmaf(d18.x, 0.7765238881111145f, br); bi = fmaf(d18.y, 0.7765238881111145f, bi);
+      ar = fmaf(s19.x, -0.9151456356048584f, ar); ai = fmaf(s19.y, -0.9151456356048584f, ai); br = fmaf(d19.x, 0.4031234383583069f, br); bi = fmaf(d19.y, 0.4031234383583069f, bi);
+      ar = fmaf(s20.x, -0.9982437491416931f, ar); ai = fmaf(s20.y, -0.9982437491416931f, ai); br = fmaf(d20.x, -0.05924062803387642f, br); bi = fmaf(d20.y, -0.05924062803387642f, bi);
+      ar = fmaf(s21.x, -0.8610436320304871f, ar); ai = fmaf(s21.y, -0.8610436320304871f, ai); br = fmaf(d21.x, -0.5085310935974121f, br); bi = fmaf(d21.y, -0.5085310935974121f, bi);
+      ar = fmaf(s22.x, -0.5338233709335327f, ar); ai = fmaf(s22.y, -0.5338233709335327f, ai); br = fmaf(d22.x, -0.8455960154533386f, br); bi = fmaf(d22.y, -0.8455960154533386f, bi);
+      ar = fmaf(s23.x, -0.08879589289426804f, ar); ai = fmaf(s23.y, -0.08879589289426804f, ai); br = fmaf(d23.x, -0.9960498213768005f, br); bi = fmaf(d23.y, -0.9960498213768005f, bi);
+      ar = fmaf(s24.x, 0.3758275806903839f, ar); ai = fmaf(s24.y, 0.3758275806903839f, ai); br = fmaf(d24.x, -0.926689624786377f, br); bi = fmaf(d24.y, -0.926689624786377f, bi);
+      ar = fmaf(s25.x, 0.7575112581253052f, ar); ai = fmaf(s25.y, 0.7575112581253052f, ai); br = fmaf(d25.x, -0.6528221368789673f, br); bi = fmaf(d25.y, -0.6528221368789673f, bi);
+      ar = fmaf(s26.x, 0.9720228910446167f, ar); ai = fmaf(s26.y, 0.9720228910446167f, ai); br = fmaf(d26.x, -0.2348860502243042f, br); bi = fmaf(d26.y, -0.2348860502243042f, bi);
+      if (!INV) { st(4, make_float2(ar + bi, ai - br)); st(49, make_float2(ar - bi, ai + br)); }
+      else { st(4, make_float2(ar - bi, ai + br)); st(49, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.829405665397644f, ar); ai = fmaf(s1.y, 0.829405665397644f, ai); br = fmaf(d1.x, 0.5586467385292053f, br); bi = fmaf(d1.y, 0.5586467385292053f, bi);
+      ar = fmaf(s2.x, 0.3758275806903839f, ar); ai = fmaf(s2.y, 0.3758275806903839f, ai); br = fmaf(d2.x, 0.926689624786377f, br); bi = fmaf(d2.y, 0.926689624786377f, bi);
+      ar = fmaf(s3.x, -0.2059786170721054f, ar); ai = fmaf(s3.y, -0.2059786170721054f, ai); br = fmaf(d3.x, 0.9785565137863159f, br); bi = fmaf(d3.y, 0.9785565137863159f, bi);
+      ar = fmaf(s4.x, -0.7175072431564331f, ar); ai = fmaf(s4.y, -0.7175072431564331f, ai); br = fmaf(d4.x, 0.6965510249137878f, br); bi = fmaf(d4.y, 0.6965510249137878f, bi);
+      ar = fmaf(s5.x, -0.9842305779457092f, ar); ai = fmaf(s5.y, -0.9842305779457092f, ai); br = fmaf(d5.x, 0.1768902689218521f, br); bi = fmaf(d5.y, 0.1768902689218521f, bi);
+      ar = fmaf(s6.x, -0.9151456356048584f, ar); ai = fmaf(s6.y, -0.9151456356048584f, ai); br = fmaf(d6.x, -0.4031234383583069f, br); bi = fmaf(d6.y, -0.4031234383583069f, bi);
+      ar = fmaf(s7.x, -0.5338233709335327f, ar); ai = fmaf(s7.y, -0.5338233709335327f, ai); br = fmaf(d7.x, -0.8455960154533386f, br); bi = fmaf(d7.y, -0.8455960154533386f, bi);
+      ar = fmaf(s8.x, 0.029633328318595886f, ar); ai = fmaf(s8.y, 0.029633328318595886f, ai); br = fmaf(d8.x, -0.9995608329772949f, br); bi = fmaf(d8.y, -0.9995608329772949f, bi);
+      ar = fmaf(s9.x, 0.5829795002937317f, ar); ai = fmaf(s9.y, 0.5829795002937317f, ai); br = fmaf(d9.x, -0.8124868869781494f, br); bi = fmaf(d9.y, -0.8124868869781494f, bi);
+      ar = fmaf(s10.x, 0.9374196529388428f, ar); ai = fmaf(s10.y, 0.9374196529388428f, ai); br = fmaf(d10.x, -0.3482016324996948f, br); bi = fmaf(d10.y, -0.3482016324996948f, bi);
+      ar = fmaf(s11.x, 0.9720228910446167f, ar); ai = fmaf(s11.y, 0.9720228910446167f, ai); br = fmaf(d11.x, 0.2348860502243042f, br); bi = fmaf(d11.y, 0.2348860502243042f, bi);
+      ar = fmaf(s12.x, 0.674983024597168f, ar); ai = fmaf(s12.y, 0.674983024597168f, ai); br = fmaf(d12.x, 0.7378332614898682f, br); bi = fmaf(d12.y, 0.7378332614898682f, bi);
+      ar = fmaf(s13.x, 0.14764656126499176f, ar); ai = fmaf(s13.y, 0.14764656126499176f, ai); br = fmaf(d13.x, 0.989040195941925f, br); bi = fmaf(d13.y, 0.989040195941925f, bi);
+      ar = fmaf(s14.x, -0.43006521463394165f, ar); ai = fmaf(s14.y, -0.43006521463394165f, ai); br = fmaf(d14.x, 0.9027978181838989f, br); bi = fmaf(d14.y, 0.9027978181838989f, bi);
+      ar = fmaf(s15.x, -0.8610436320304871f, ar); ai = fmaf(s15.y, -0.8610436320304871f, ai); br = fmaf(d15.x, 0.5085310935974121f, br); bi = fmaf(d15.y, 0.5085310935974121f, bi);
+      ar = fmaf(s16.x, -0.9982437491416931f, ar); ai = fmaf(s16.y, -0.9982437491416931f, ai); br = fmaf(d16.x, -0.05924062803387642f, br); bi = fmaf(d16.y, -0.05924062803387642f, bi);
+      ar = fmaf(s17.x, -0.794854462146759f, ar); ai = fmaf(s17.y, -0.794854462146759f, ai); br = fmaf(d17.x, -0.6068001389503479f, br); bi = fmaf(d17.y, -0.6068001389503479f, bi);
+      ar = fmaf(s18.x, -0.3202698528766632f, ar); ai = fmaf(s18.y, -0.3202698528766632f, ai); br = fmaf(d18.x, -0.9473263621330261f, br); bi = fmaf(d18.y, -0.9473263621330261f, bi);
+      ar = fmaf(s19.x, 0.26358717679977417f, ar); ai = fmaf(s19.y, 0.26358717679977417f, ai); br = fmaf(d19.x, -0.9646356105804443f, br); bi = fmaf(d19.y, -0.9646356105804443f, bi);
+      ar = fmaf(s20.x, 0.7575112581253052f, ar); ai = fmaf(s20.y, 0.7575112581253052f, ai); br = fmaf(d20.x, -0.6528221368789673f, br); bi = fmaf(d20.y, -0.6528221368789673f, bi);
+      ar = fmaf(s21.x, 0.9929810762405396f, ar); ai = fmaf(s21.y, 0.9929810762405396f, ai); br = fmaf(d21.x, -0.11827316880226135f, br); bi = fmaf(d21.y, -0.11827316880226135f, bi);
+      ar = fmaf(s22.x, 0.8896570801734924f, ar); ai = fmaf(s22.y, 0.8896570801734924f, ai); br = fmaf(d22.x, 0.4566292464733124f, br); bi = fmaf(d22.y, 0.4566292464733124f, bi);
+      ar = fmaf(s23.x, 0.4827921986579895f, ar); ai = fmaf(s23.y, 0.4827921986579895f, ai); br = fmaf(d23.x, 0.8757349252700806f, br); bi = fmaf(d23.y, 0.8757349252700806f, bi);
+      ar = fmaf(s24.x, -0.08879589289426804f, ar); ai = fmaf(s24.y, -0.08879589289426804f, ai); br = fmaf(d24.x, 0.9960498213768005f, br); bi = fmaf(d24.y, 0.9960498213768005f, bi);
+      ar = fmaf(s25.x, -0.6300878524780273f, ar); ai = fmaf(s25.y, -0.6300878524780273f, ai); br = fmaf(d25.x, 0.7765238881111145f, br); bi = fmaf(d25.y, 0.7765238881111145f, bi);
+      ar = fmaf(s26.x, -0.956400990486145f, ar); ai = fmaf(s26.y, -0.956400990486145f, ai); br = fmaf(d26.x, 0.29205676913261414f, br); bi = fmaf(d26.y, 0.29205676913261414f, bi);
+      if (!INV) { st(5, make_float2(ar + bi, ai - br)); st(48, make_float2(ar - bi, ai + br)); }
+      else { st(5, make_float2(ar - bi, ai + br)); st(48, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.7575112581253052f, ar); ai = fmaf(s1.y, 0.7575112581253052f, ai); br = fmaf(d1.x, 0.6528221368789673f, br); bi = fmaf(d1.y, 0.6528221368789673f, bi);
+      ar = fmaf(s2.x, 0.14764656126499176f, ar); ai = fmaf(s2.y, 0.14764656126499176f, ai); br = fmaf(d2.x, 0.989040195941925f, br); bi = fmaf(d2.y, 0.989040195941925f, bi);
+      ar = fmaf(s3.x, -0.5338233709335327f, ar); ai = fmaf(s3.y, -0.5338233709335327f, ai); br = fmaf(d3.x, 0.8455960154533386f, br); bi = fmaf(d3.y, 0.8455960154533386f, bi);
+      ar = fmaf(s4.x, -0.956400990486145f, ar); ai = fmaf(s4.y, -0.956400990486145f, ai); br = fmaf(d4.x, 0.29205676913261414f, br); bi = fmaf(d4.y, 0.29205676913261414f, bi);
+      ar = fmaf(s5.x, -0.9151456356048584f, ar); ai = fmaf(s5.y, -0.9151456356048584f, ai); br = fmaf(d5.x, -0.4031234383583069f, br); bi = fmaf(d5.y, -0.4031234383583069f, bi);
+      ar = fmaf(s6.x, -0.43006521463394165f, ar); ai = fmaf(s6.y, -0.43006521463394165f, ai); br = fmaf(d6.x, -0.9027978181838989f, br); bi = fmaf(d6.y, -0.9027978181838989f, bi);
+      ar = fmaf(s7.x, 0.26358717679977417f, ar); ai = fmaf(s7.y, 0.26358717679977417f, ai); br = fmaf(d7.x, -0.9646356105804443f, br); bi = fmaf(d7.y, -0.9646356105804443f, bi);
+      ar = fmaf(s8.x, 0.829405665397644f, ar); ai = fmaf(s8.y, 0.829405665397644f, ai); br = fmaf(d8.x, -0.5586467385292053f, br); bi = fmaf(d8.y, -0.5586467385292053f, bi);
+      ar = fmaf(s9.x, 0.9929810762405396f, ar); ai = fmaf(s9.y, 0.9929810762405396f, ai); br = fmaf(d9.x, 0.11827316880226135f, br); bi = fmaf(d9.y, 0.11827316880226135f, bi);
+      ar = fmaf(s10.x, 0.674983024597168f, ar); ai = fmaf(s10.y, 0.674983024597168f, ai); br = fmaf(d10.x, 0.7378332614898682f, br); bi = fmaf(d10.y, 0.7378332614898682f, bi);
+      ar = fmaf(s11.x, 0.029633328318595886f, ar); ai = fmaf(s11.y, 0.029633328318595886f, ai); br = fmaf(d11.x, 0.9995608329772949f, br); bi = fmaf(d11.y, 0.9995608329772949f, bi);
+      ar = fmaf(s12.x, -0.6300878524780273f, ar); ai = fmaf(s12.y, -0.6300878524780273f, ai); br = fmaf(d12.x, 0.7765238881111145f, br); bi = fmaf(d12.y, 0.7765238881111145f, bi);
+      ar = fmaf(s13.x, -0.9842305779457092f, ar); ai = fmaf(s13.y, -0.9842305779457092f, ai); br = fmaf(d13.x, 0.1768902689218521f, br); bi = fmaf(d13.y, 0.1768902689218521f, bi);
+      ar = fmaf(s14.x, -0.8610436320304871f, ar); ai = fmaf(s14.y, -0.8610436320304871f, ai); br = fmaf(d14.x, -0.5085310935974121f, br); bi = fmaf(d14.y, -0.5085310935974121f, bi);
+      ar = fmaf(s15.x, -0.3202698528766632f, ar); ai = fmaf(s15.y, -0.3202698528766632f, ai); br = fmaf(d15.x, -0.9473263621330261f, br); bi = fmaf(d15.y, -0.9473263621330261f, bi);
+      ar = fmaf(s16.x, 0.3758275806903839f, ar); ai = fmaf(s16.y, 0.3758275806903839f, ai); br = fmaf(d16.x, -0.926689624786377f, br); bi = fmaf(d16.y, -0.926689624786377f, bi);
+      ar = fmaf(s17.x, 0.8896570801734924f, ar); ai = fmaf(s17.y, 0.8896570801734924f, ai); br = fmaf(d17.x, -0.4566292464733124f, br); bi = fmaf(d17.y, -0.4566292464733124f, bi);
+      ar = fmaf(s18.x, 0.9720228910446167f, ar); ai = fmaf(s18.y, 0.9720228910446167f, ai); br = fmaf(d18.x, 0.2348860502243042f, br); bi = fmaf(d18.y, 0.2348860502243042f, bi);
+      ar = fmaf(s19.x, 0.5829795002937317f, ar); ai = fmaf(s19.y, 0.5829795002937317f, ai); br = fmaf(d19.x, 0.8124868869781494f, br); bi = fmaf(d19.y, 0.8124868869781494f, bi);
+      ar = fmaf(s20.x, -0.08879589289426804f, ar); ai = fmaf(s20.y, -0.08879589289426804f, ai); br = fmaf(d20.x, 0.9960498213768005f, br); bi = fmaf(d20.y, 0.9960498213768005f, bi);
+      ar = fmaf(s21.x, -0.7175072431564331f, ar); ai = fmaf(s21.y, -0.7175072431564331f, ai); br = fmaf(d21.x, 0.6965510249137878f, br); bi = fmaf(d21.y, 0.6965510249137878f, bi);
+      ar = fmaf(s22.x, -0.9982437491416931f, ar); ai = fmaf(s22.y, -0.9982437491416931f, ai); br = fmaf(d22.x, 0.05924062803387642f, br); bi = fmaf(d22.y, 0.05924062803387642f, bi);
+      ar = fmaf(s23.x, -0.794854462146759f, ar); ai = fmaf(s23.y, -0.794854462146759f, ai); br = fmaf(d23.x, -0.6068001389503479f, br); bi = fmaf(d23.y, -0.6068001389503479f, bi);
+      ar = fmaf(s24.x, -0.2059786170721054f, ar); ai = fmaf(s24.y, -0.2059786170721054f, ai); br = fmaf(d24.x, -0.9785565137863159f, br); bi = fmaf(d24.y, -0.9785565137863159f, bi);
+      ar = fmaf(s25.x, 0.4827921986579895f, ar); ai = fmaf(s25.y, 0.4827921986579895f, ai); br = fmaf(d25.x, -0.8757349252700806f, br); bi = fmaf(d25.y, -0.8757349252700806f, bi);
+      ar = fmaf(s26.x, 0.9374196529388428f, ar); ai = fmaf(s26.y, 0.9374196529388428f, ai); br = fmaf(d26.x, -0.3482016324996948f, br); bi = fmaf(d26.y, -0.3482016324996948f, bi);
+      if (!INV) { st(6, make_float2(ar + bi, ai - br)); st(47, make_float2(ar - bi, ai + br)); }
+      else { st(6, make_float2(ar - bi, ai + br)); st(47, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.674983024597168f, ar); ai = fmaf(s1.y, 0.674983024597168f, ai); br = fmaf(d1.x, 0.7378332614898682f, br); bi = fmaf(d1.y, 0.7378332614898682f, bi);
+      ar = fmaf(s2.x, -0.08879589289426804f, ar); ai = fmaf(s2.y, -0.08879589289426804f, ai); br = fmaf(d2.x, 0.9960498213768005f, br); bi = fmaf(d2.y, 0.9960498213768005f, bi);
+      ar = fmaf(s3.x, -0.794854462146759f, ar); ai = fmaf(s3.y, -0.794854462146759f, ai); br = fmaf(d3.x, 0.6068001389503479f, br); bi = fmaf(d3.y, 0.6068001389503479f, bi);
+      ar = fmaf(s4.x, -0.9842305779457092f, ar); ai = fmaf(s4.y, -0.9842305779457092f, ai); br = fmaf(d4.x, -0.1768902689218521f, br); bi = fmaf(d4.y, -0.1768902689218521f, bi);
+      ar = fmaf(s5.x, -0.5338233709335327f, ar); ai = fmaf(s5.y, -0.5338233709335327f, ai); br = fmaf(d5.x, -0.8455960154533386f, br); bi = fmaf(d5.y, -0.8455960154533386f, bi);
+      ar = fmaf(s6.x, 0.26358717679977417f, ar); ai = fmaf(s6.y, 0.26358717679977417f, ai); br = fmaf(d6.x, -0.9646356105804443f, br); bi = fmaf(d6.y, -0.9646356105804443f, bi);
+      ar = fmaf(s7.x, 0.8896570801734924f, ar); ai = fmaf(s7.y, 0.8896570801734924f, ai); br = fmaf(d7.x, -0.4566292464733124f, br); bi = fmaf(d7.y, -0.4566292464733124f, bi);
+      ar = fmaf(s8.x, 0.9374196529388428f, ar); ai = fmaf(s8.y, 0.9374196529388428f, ai); br = fmaf(d8.x, 0.3482016324996948f, br); bi = fmaf(d8.y, 0.3482016324996948f, bi);
+      ar = fmaf(s9.x, 0.3758275806903839f, ar); ai = fmaf(s9.y, 0.3758275806903839f, ai); br = fmaf(d9.x, 0.926689624786377f, br); bi = fmaf(d9.y, 0.926689624786377f, bi);
+      ar = fmaf(s10.x, -0.43006521463394165f, ar); ai = fmaf(s10.y, -0.43006521463394165f, ai); br = fmaf(d10.x, 0.9027978181838989f, br); bi = fmaf(d10.y, 0.9027978181838989f, bi);
+      ar = fmaf(s11.x, -0.956400990486145f, ar); ai = fmaf(s11.y, -0.956400990486145f, ai); br = fmaf(d11.x, 0.29205676913261414f, br); bi = fmaf(d11.y, 0.29205676913261414f, bi);
+      ar = fmaf(s12.x, -0.8610436320304871f, ar); ai = fmaf(s12.y, -0.8610436320304871f, ai); br = fmaf(d12.x, -0.5085310935974121f, br); bi = fmaf(d12.y, -0.5085310935974121f, bi);
+      ar = fmaf(s13.x, -0.2059786170721054f, ar); ai = fmaf(s13.y, -0.2059786170721054f, ai); br = fmaf(d13.x, -0.9785565137863159f, br); bi = fmaf(d13.y, -0.9785565137863159f, bi);
+      ar = fmaf(s14.x, 0.5829795002937317f, ar); ai = fmaf(s14.y, 0.5829795002937317f, ai); br = fmaf(d14.x, -0.8124868869781494f, br); bi = fmaf(d14.y, -0.8124868869781494f, bi);
+      ar = fmaf(s15.x, 0.9929810762405396f, ar); ai = fmaf(s15.y, 0.9929810762405396f, ai); br = fmaf(d15.x, -0.11827316880226135f, br); bi = fmaf(d15.y, -0.11827316880226135f, bi);
+      ar = fmaf(s16.x, 0.7575112581253052f, ar); ai = fmaf(s16.y, 0.7575112581253052f, ai); br = fmaf(d16.x, 0.6528221368789673f, br); bi = fmaf(d16.y, 0.6528221368789673f, bi);
+      ar = fmaf(s17.x, 0.029633328318595886f, ar); ai = fmaf(s17.y, 0.029633328318595886f, ai); br = fmaf(d17.x, 0.9995608329772949f, br); bi = fmaf(d17.y, 0.9995608329772949f, bi);
+      ar = fmaf(s18.x, -0.7175072431564331f, ar); ai = fmaf(s18.y, -0.7175072431564331f, ai); br = fmaf(d18.x, 0.6965510249137878f, br); bi = fmaf(d18.y, 0.6965510249137878f, bi);
+      ar = fmaf(s19.x, -0.9982437491416931f, ar); ai = fmaf(s19.y, -0.9982437491416931f, ai); br = fmaf(d19.x, -0.05924062803387642f, br); bi = fmaf(d19.y, -0.05924062803387642f, bi);
+      ar = fmaf(s20.x, -0.6300878524780273f, ar); ai = fmaf(s20.y, -0.6300878524780273f, ai); br = fmaf(d20.x, -0.7765238881111145f, br); bi = fmaf(d20.y, -0.7765238881111145f, bi);
+      ar = fmaf(s21.x, 0.14764656126499176f, ar); ai = fmaf(s21.y, 0.14764656126499176f, ai); br = fmaf(d21.x, -0.989040195941925f, br); bi = fmaf(d21.y, -0.989040195941925f, bi);
+      ar = fmaf(s22.x, 0.829405665397644f, ar); ai = fmaf(s22.y, 0.829405665397644f, ai); br = fmaf(d22.x, -0.5586467385292053f, br); bi = fmaf(d22.y, -0.5586467385292053f, bi);
+      ar = fmaf(s23.x, 0.9720228910446167f, ar); ai = fmaf(s23.y, 0.9720228910446167f, ai); br = fmaf(d23.x, 0.2348860502243042f, br); bi = fmaf(d23.y, 0.2348860502243042f, bi);
+      ar = fmaf(s24.x, 0.4827921986579895f, ar); ai = fmaf(s24.y, 0.4827921986579895f, ai); br = fmaf(d24.x, 0.8757349252700806f, br); bi = fmaf(d24.y, 0.8757349252700806f, bi);
+      ar = fmaf(s25.x, -0.3202698528766632f, ar); ai = fmaf(s25.y, -0.3202698528766632f, ai); br = fmaf(d25.x, 0.9473263621330261f, br); bi = fmaf(d25.y, 0.9473263621330261f, bi);
+      ar = fmaf(s26.x, -0.9151456356048584f, ar); ai = fmaf(s26.y, -0.9151456356048584f, ai); br = fmaf(d26.x, 0.4031234383583069f, br); bi = fmaf(d26.y, 0.4031234383583069f, bi);
+      if (!INV) { st(7, make_float2(ar + bi, ai - br)); st(46, make_float2(ar - bi, ai + br)); }
+      else { st(7, make_float2(ar - bi, ai + br)); st(46, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.5829795002937317f, ar); ai = fmaf(s1.y, 0.5829795002937317f, ai); br = fmaf(d1.x, 0.8124868869781494f, br); bi = fmaf(d1.y, 0.8124868869781494f, bi);
+      ar = fmaf(s2.x, -0.3202698528766632f, ar); ai = fmaf(s2.y, -0.3202698528766632f, ai); br = fmaf(d2.x, 0.9473263621330261f, br); bi = fmaf(d2.y, 0.9473263621330261f, bi);
+      ar = fmaf(s3.x, -0.956400990486145f, ar); ai = fmaf(s3.y, -0.956400990486145f, ai); br = fmaf(d3.x, 0.29205676913261414f, br); bi = fmaf(d3.y, 0.29205676913261414f, bi);
+      ar = fmaf(s4.x, -0.794854462146759f, ar); ai = fmaf(s4.y, -0.794854462146759f, ai); br = fmaf(d4.x, -0.6068001389503479f, br); bi = fmaf(d4.y, -0.6068001389503479f, bi);
+      ar = fmaf(s5.x, 0.029633328318595886f, ar); ai = fmaf(s5.y, 0.029633328318595886f, ai); br = fmaf(d5.x, -0.9995608329772949f, br); bi = fmaf(d5.y, -0.9995608329772949f, bi);
+      ar = fmaf(s6.x, 0.829405665397644f, ar); ai = fmaf(s6.y, 0.829405665397644f, ai); br = fmaf(d6.x, -0.5586467385292053f, br); bi = fmaf(d6.y, -0.5586467385292053f, bi);
+      ar = fmaf(s7.x, 0.9374196529388428f, ar); ai = fmaf(s7.y, 0.9374196529388428f, ai); br = fmaf(d7.x, 0.3482016324996948f, br); bi = fmaf(d7.y, 0.3482016324996948f, bi);
+      ar = fmaf(s8.x, 0.26358717679977417f, ar); ai = fmaf(s8.y, 0.26358717679977417f, ai); br = fmaf(d8.x, 0.9646356105804443f, br); bi = fmaf(d8.y, 0.9646356105804443f, bi);
+      ar = fmaf(s9.x, -0.6300878524780273f, ar); ai = fmaf(s9.y, -0.6300878524780273f, ai); br = fmaf(d9.x, 0.7765238881111145f, br); bi = fmaf(d9.y, 0.7765238881111145f, bi);
+      ar = fmaf(s10.x, -0.9982437491416931f, ar); ai = fmaf(s10.y, -0.9982437491416931f, ai); br = fmaf(d10.x, -0.05924062803387642f, br); bi = fmaf(d10.y, -0.05924062803387642f, bi);
+      ar = fmaf(s11.x, -0.5338233709335327f, ar); ai = fmaf(s11.y, -0.5338233709335327f, ai); br = fmaf(d11.x, -0.8455960154533386f, br); bi = fmaf(d11.y, -0.8455960154533386f, bi);
+      ar = fmaf(s12.x, 0.3758275806903839f, ar); ai = fmaf(s12.y, 0.3758275806903839f, ai); br = fmaf(d12.x, -0.926689624786377f, br); bi = fmaf(d12.y, -0.926689624786377f, bi);
+      ar = fmaf(s13.x, 0.9720228910446167f, ar); ai = fmaf(s13.y, 0.9720228910446167f, ai); br = fmaf(d13.x, -0.2348860502243042f, br); bi = fmaf(d13.y, -0.2348860502243042f, bi);
+      ar = fmaf(s14.x, 0.7575112581253052f, ar); ai = fmaf(s14.y, 0.7575112581253052f, ai); br = fmaf(d14.x, 0.6528221368789673f, br); bi = fmaf(d14.y, 0.6528221368789673f, bi);
+      ar = fmaf(s15.x, -0.08879589289426804f, ar); ai = fmaf(s15.y, -0.08879589289426804f, ai); br = fmaf(d15.x, 0.9960498213768005f, br); bi = fmaf(d15.y, 0.9960498213768005f, bi);
+      ar = fmaf(s16.x, -0.8610436320304871f, ar); ai = fmaf(s16.y, -0.8610436320304871f, ai); br = fmaf(d16.x, 0.5085310935974121f, br); bi = fmaf(d16.y, 0.5085310935974121f, bi);
+      ar = fmaf(s17.x, -0.9151456356048584f, ar); ai = fmaf(s17.y, -0.9151456356048584f, ai); br = fmaf(d17.x, -0.4031234383583069f, br); bi = fmaf(d17.y, -0.4031234383583069f, bi);
+      ar = fmaf(s18.x, -0.2059786170721054f, ar); ai = fmaf(s18.y, -0.2059786170721054f, ai); br = fmaf(d18.x, -0.9785565137863159f, br); bi = fmaf(d18.y, -0.9785565137863159f, bi);
+      ar = fmaf(s19.x, 0.674983024597168f, ar); ai = fmaf(s19.y, 0.674983024597168f, ai); br = fmaf(d19.x, -0.7378332614898682f, br); bi = fmaf(d19.y, -0.7378332614898682f, bi);
+      ar = fmaf(s20.x, 0.9929810762405396f, ar); ai = fmaf(s20.y, 0.9929810762405396f, ai); br = fmaf(d20.x, 0.11827316880226135f, br); bi = fmaf(d20.y, 0.11827316880226135f, bi);
+      ar = fmaf(s21.x, 0.4827921986579895f, ar); ai = fmaf(s21.y, 0.4827921986579895f, ai); br = fmaf(d21.x, 0.8757349252700806f, br); bi = fmaf(d21.y, 0.8757349252700806f, bi);
+      ar = fmaf(s22.x, -0.43006521463394165f, ar); ai = fmaf(s22.y, -0.43006521463394165f, ai); br = fmaf(d22.x, 0.9027978181838989f, br); bi = fmaf(d22.y, 0.9027978181838989f, bi);
+      ar = fmaf(s23.x, -0.9842305779457092f, ar); ai = fmaf(s23.y, -0.9842305779457092f, ai); br = fmaf(d23.x, 0.1768902689218521f, br); bi = fmaf(d23.y, 0.1768902689218521f, bi);
+      ar = fmaf(s24.x, -0.7175072431564331f, ar); ai = fmaf(s24.y, -0.7175072431564331f, ai); br = fmaf(d24.x, -0.6965510249137878f, br); bi = fmaf(d24.y, -0.6965510249137878f, bi);
+      ar = fmaf(s25.x, 0.14764656126499176f, ar); ai = fmaf(s25.y, 0.14764656126499176f, ai); br = fmaf(d25.x, -0.989040195941925f, br); bi = fmaf(d25.y, -0.989040195941925f, bi);
+      ar = fmaf(s26.x, 0.8896570801734924f, ar); ai = fmaf(s26.y, 0.8896570801734924f, ai); br = fmaf(d26.x, -0.4566292464733124f, br); bi = fmaf(d26.y, -0.4566292464733124f, bi);
+      if (!INV) { st(8, make_float2(ar + bi, ai - br)); st(45, make_float2(ar - bi, ai + br)); }
+      else { st(8, make_float2(ar - bi, ai + br)); st(45, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.4827921986579895f, ar); ai = fmaf(s1.y, 0.4827921986579895f, ai); br = fmaf(d1.x, 0.8757349252700806f, br); bi = fmaf(d1.y, 0.8757349252700806f, bi);
+      ar = fmaf(s2.x, -0.5338233709335327f, ar); ai = fmaf(s2.y, -0.5338233709335327f, ai); br = fmaf(d2.x, 0.8455960154533386f, br); bi = fmaf(d2.y, 0.8455960154533386f, bi);
+      ar = fmaf(s3.x, -0.9982437491416931f, ar); ai = fmaf(s3.y, -0.9982437491416931f, ai); br = fmaf(d3.x, -0.05924062803387642f, br); bi = fmaf(d3.y, -0.05924062803387642f, bi);
+      ar = fmaf(s4.x, -0.43006521463394165f, ar); ai = fmaf(s4.y, -0.43006521463394165f, ai); br = fmaf(d4.x, -0.9027978181838989f, br); bi = fmaf(d4.y, -0.9027978181838989f, bi);
+      ar = fmaf(s5.x, 0.5829795002937317f, ar); ai = fmaf(s5.y, 0.5829795002937317f, ai); br = fmaf(d5.x, -0.8124868869781494f, br); bi = fmaf(d5.y, -0.8124868869781494f, bi);
+      ar = fmaf(s6.x, 0.9929810762405396f, ar); ai = fmaf(s6.y, 0.9929810762405396f, ai); br = fmaf(d6.x, 0.11827316880226135f, br); bi = fmaf(d6.y, 0.11827316880226135f, bi);
+      ar = fmaf(s7.x, 0.3758275806903839f, ar); ai = fmaf(s7.y, 0.3758275806903839f, ai); br = fmaf(d7.x, 0.926689624786377f, br); bi = fmaf(d7.y, 0.926689624786377f, bi);
+      ar = fmaf(s8.x, -0.6300878524780273f, ar); ai = fmaf(s8.y, -0.6300878524780273f, ai); br = fmaf(d8.x, 0.7765238881111145f, br); bi = fmaf(d8.y, 0.7765238881111145f, bi);
+      ar = fmaf(s9.x, -0.9842305779457092f, ar); ai = fmaf(s9.y, -0.9842305779457092f, ai); br = fmaf(d9.x, -0.1768902689218521f, br); bi = fmaf(d9.y, -0.1768902689218521f, bi);
+      ar = fmaf(s10.x, -0.3202698528766632f, ar); ai = fmaf(s10.y, -0.3202698528766632f, ai); br = fmaf(d10.x, -0.9473263621330261f, br); bi = fmaf(d10.y, -0.9473263621330261f, bi);
+      ar = fmaf(s11.x, 0.674983024597168f, ar); ai = fmaf(s11.y, 0.674983024597168f, ai); br = fmaf(d11.x, -0.7378332614898682f, br); bi = fmaf(d11.y, -0.7378332614898682f, bi);
+      ar = fmaf(s12.x, 0.9720228910446167f, ar); ai = fmaf(s12.y, 0.9720228910446167f, ai); br = fmaf(d12.x, 0.2348860502243042f, br); bi = fmaf(d12.y, 0.2348860502243042f, bi);
+      ar = fmaf(s13.x, 0.26358717679977417f, ar); ai = fmaf(s13.y, 0.26358717679977417f, ai); br = fmaf(d13.x, 0.9646356105804443f, br); bi = fmaf(d13.y, 0.9646356105804443f, bi);
+      ar = fmaf(s14.x, -0.7175072431564331f, ar); ai = fmaf(s14.y, -0.7175072431564331f, ai); br = fmaf(d14.x, 0.6965510249137878f, br); bi = fmaf(d14.y, 0.6965510249137878f, bi);
+      ar = fmaf(s15.x, -0.956400990486145f, ar); ai = fmaf(s15.y, -0.956400990486145f, ai); br = fmaf(d15.x, -0.29205676913261414f, br); bi = fmaf(d15.y, -0.29205676913261414f, bi);
+      ar = fmaf(s16.x, -0.2059786170721054f, ar); ai = fmaf(s16.y, -0.2059786170721054f, ai); br = fmaf(d16.x, -0.9785565137863159f, br); bi = fmaf(d16.y, -0.9785565137863159f, bi);
+      ar = fmaf(s17.x, 0.7575112581253052f, ar); ai = fmaf(s17.y, 0.7575112581253052f, ai); br = fmaf(d17.x, -0.6528221368789673f, br); bi = fmaf(d17.y, -0.6528221368789673f, bi);
+      ar = fmaf(s18.x, 0.9374196529388428f, ar); ai = fmaf(s18.y, 0.9374196529388428f, ai); br = fmaf(d18.x, 0.3482016324996948f, br); bi = fmaf(d18.y, 0.3482016324996948f, bi);
+      ar = fmaf(s19.x, 0.14764656126499176f, ar); ai = fmaf(s19.y, 0.14764656126499176f, ai); br = fmaf(d19.x, 0.989040195941925f, br); bi = fmaf(d19.y, 0.989040195941925f, bi);
+      ar = fmaf(s20.x, -0.794854462146759f, ar); ai = fmaf(s20.y, -0.794854462146759f, ai); br = fmaf(d20.x, 0.6068001389503479f, br); bi = fmaf(d20.y, 0.6068001389503479f, bi);
+      ar = fmaf(s21.x, -0.9151456356048584f, ar); ai = fmaf(s21.y, -0.9151456356048584f, ai); br = fmaf(d21.x, -0.4031234383583069f, br); bi = fmaf(d21.y, -0.4031234383583069f, bi);
+      ar = fmaf(s22.x, -0.08879589289426804f, ar); ai = fmaf(s22.y, -0.08879589289426804f, ai); br = fmaf(d22.x, -0.9960498213768005f, br); bi = fmaf(d22.y, -0.9960498213768005f, bi);
+      ar = fmaf(s23.x, 0.829405665397644f, ar); ai = fmaf(s23.y, 0.829405665397644f, ai); br = fmaf(d23.x, -0.5586467385292053f, br); bi = fmaf(d23.y, -0.5586467385292053f, bi);
+      ar = fmaf(s24.x, 0.8896570801734924f, ar); ai = fmaf(s24.y, 0.8896570801734924f, ai); br = fmaf(d24.x, 0.4566292464733124f, br); bi = fmaf(d24.y, 0.4566292464733124f, bi);
+      ar = fmaf(s25.x, 0.029633328318595886f, ar); ai = fmaf(s25.y, 0.029633328318595886f, ai); br = fmaf(d25.x, 0.9995608329772949f, br); bi = fmaf(d25.y, 0.9995608329772949f, bi);
+      ar = fmaf(s26.x, -0.8610436320304871f, ar); ai = fmaf(s26.y, -0.8610436320304871f, ai); br = fmaf(d26.x, 0.5085310935974121f, br); bi = fmaf(d26.y, 0.5085310935974121f, bi);
+      if (!INV) { st(9, make_float2(ar + bi, ai - br)); st(44, make_float2(ar - bi, ai + br)); }
+      else { st(9, make_float2(ar - bi, ai + br)); st(44, make_float2(ar + bi, ai - br)); }
+    }
+    break;
+  }
+  case 1: {
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.3758275806903839f, ar); ai = fmaf(s1.y, 0.3758275806903839f, ai); br = fmaf(d1.x, 0.926689624786377f, br); bi = fmaf(d1.y, 0.926689624786377f, bi);
+      ar = fmaf(s2.x, -0.7175072431564331f, ar); ai = fmaf(s2.y, -0.7175072431564331f, ai); br = fmaf(d2.x, 0.6965510249137878f, br); bi = fmaf(d2.y, 0.6965510249137878f, bi);
+      ar = fmaf(s3.x, -0.9151456356048584f, ar); ai = fmaf(s3.y, -0.9151456356048584f, ai); br = fmaf(d3.x, -0.4031234383583069f, br); bi = fmaf(d3.y, -0.4031234383583069f, bi);
+      ar = fmaf(s4.x, 0.029633328318595886f, ar); ai = fmaf(s4.y, 0.029633328318595886f, ai); br = fmaf(d4.x, -0.9995608329772949f, br); bi = fmaf(d4.y, -0.9995608329772949f, bi);
+      ar = fmaf(s5.x, 0.9374196529388428f, ar); ai = fmaf(s5.y, 0.9374196529388428f, ai); br = fmaf(d5.x, -0.3482016324996948f, br); bi = fmaf(d5.y, -0.3482016324996948f, bi);
+      ar = fmaf(s6.x, 0.674983024597168f, ar); ai = fmaf(s6.y, 0.674983024597168f, ai); br = fmaf(d6.x, 0.7378332614898682f, br); bi = fmaf(d6.y, 0.7378332614898682f, bi);
+      ar = fmaf(s7.x, -0.43006521463394165f, ar); ai = fmaf(s7.y, -0.43006521463394165f, ai); br = fmaf(d7.x, 0.9027978181838989f, br); bi = fmaf(d7.y, 0.9027978181838989f, bi);
+      ar = fmaf(s8.x, -0.9982437491416931f, ar); ai = fmaf(s8.y, -0.9982437491416931f, ai); br = fmaf(d8.x, -0.05924062803387642f, br); bi = fmaf(d8.y, -0.05924062803387642f, bi);
+      ar = fmaf(s9.x, -0.3202698528766632f, ar); ai = fmaf(s9.y, -0.3202698528766632f, ai); br = fmaf(d9.x, -0.9473263621330261f, br); bi = fmaf(d9.y, -0.9473263621330261f, bi);
+      ar = fmaf(s10.x, 0.7575112581253052f, ar); ai = fmaf(s10.y, 0.7575112581253052f, ai); br = fmaf(d10.x, -0.6528221368789673f, br); bi = fmaf(d10.y, -0.6528221368789673f, bi);
+      ar = fmaf(s11.x, 0.8896570801734924f, ar); ai = fmaf(s11.y, 0.8896570801734924f, ai); br = fmaf(d11.x, 0.4566292464733124f, br); bi = fmaf(d11.y, 0.4566292464733124f, bi);
+      ar = fmaf(s12.x, -0.08879589289426804f, ar); ai = fmaf(s12.y, -0.08879589289426804f, ai); br = fmaf(d12.x, 0.9960498213768005f, br); bi = fmaf(d12.y, 0.9960498213768005f, bi);
+      ar = fmaf(s13.x, -0.956400990486145f, ar); ai = fmaf(s13.y, -0.956400990486145f, ai); br = fmaf(d13.x, 0.29205676913261414f, br); bi = fmaf(d13.y, 0.29205676913261414f, bi);
+      ar = fmaf(s14.x, -0.6300878524780273f, ar); ai = fmaf(s14.y, -0.6300878524780273f, ai); br = fmaf(d14.x, -0.7765238881111145f, br); bi = fmaf(d14.y, -0.7765238881111145f, bi);
+      ar = fmaf(s15.x, 0.4827921986579895f, ar); ai = fmaf(s15.y, 0.4827921986579895f, ai); br = fmaf(d15.x, -0.8757349252700806f, br); bi = fmaf(d15.y, -0.8757349252700806f, bi);
+      ar = fmaf(s16.x, 0.9929810762405396f, ar); ai = fmaf(s16.y, 0.9929810762405396f, ai); br = fmaf(d16.x, 0.11827316880226135f, br); bi = fmaf(d16.y, 0.11827316880226135f, bi);
+      ar = fmaf(s17.x, 0.26358717679977417f, ar); ai = fmaf(s17.y, 0.26358717679977417f, ai); br = fmaf(d17.x, 0.9646356105804443f, br); bi = fmaf(d17.y, 0.9646356105804443f, bi);
+      ar = fmaf(s18.x, -0.794854462146759f, ar); ai = fmaf(s18.y, -0.794854462146759f, ai); br = fmaf(d18.x, 0.6068001389503479f, br); bi = fmaf(d18.y, 0.6068001389503479f, bi);
+      ar = fmaf(s19.x, -0.8610436320304871f, ar); ai = fmaf(s19.y, -0.8610436320304871f, ai); br = fmaf(d19.x, -0.5085310935974121f, br); bi = fmaf(d19.y, -0.5085310935974121f, bi);
+      ar = fmaf(s20.x, 0.14764656126499176f, ar); ai = fmaf(s20.y, 0.14764656126499176f, ai); br = fmaf(d20.x, -0.989040195941925f, br); bi = fmaf(d20.y, -0.989040195941925f, bi);
+      ar = fmaf(s21.x, 0.9720228910446167f, ar); ai = fmaf(s21.y, 0.9720228910446167f, ai); br = fmaf(d21.x, -0.2348860502243042f, br); bi = fmaf(d21.y, -0.2348860502243042f, bi);
+      ar = fmaf(s22.x, 0.5829795002937317f, ar); ai = fmaf(s22.y, 0.5829795002937317f, ai); br = fmaf(d22.x, 0.8124868869781494f, br); bi = fmaf(d22.y, 0.8124868869781494f, bi);
+      ar = fmaf(s23.x, -0.5338233709335327f, ar); ai = fmaf(s23.y, -0.5338233709335327f, ai); br = fmaf(d23.x, 0.8455960154533386f, br); bi = fmaf(d23.y, 0.8455960154533386f, bi);
+      ar = fmaf(s24.x, -0.9842305779457092f, ar); ai = fmaf(s24.y, -0.9842305779457092f, ai); br = fmaf(d24.x, -0.1768902689218521f, br); bi = fmaf(d24.y, -0.1768902689218521f, bi);
+      ar = fmaf(s25.x, -0.2059786170721054f, ar); ai = fmaf(s25.y, -0.2059786170721054f, ai); br = fmaf(d25.x, -0.9785565137863159f, br); bi = fmaf(d25.y, -0.9785565137863159f, bi);
+      ar = fmaf(s26.x, 0.829405665397644f, ar); ai = fmaf(s26.y, 0.829405665397644f, ai); br = fmaf(d26.x, -0.5586467385292053f, br); bi = fmaf(d26.y, -0.5586467385292053f, bi);
+      if (!INV) { st(10, make_float2(ar + bi, ai - br)); st(43, make_float2(ar - bi, ai + br)); }
+      else { st(10, make_float2(ar - bi, ai + br)); st(43, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.26358717679977417f, ar); ai = fmaf(s1.y, 0.26358717679977417f, ai); br = fmaf(d1.x, 0.9646356105804443f, br); bi = fmaf(d1.y, 0.9646356105804443f, bi);
+      ar = fmaf(s2.x, -0.8610436320304871f, ar); ai = fmaf(s2.y, -0.8610436320304871f, ai); br = fmaf(d2.x, 0.5085310935974121f, br); bi = fmaf(d2.y, 0.5085310935974121f, bi);
+      ar = fmaf(s3.x, -0.7175072431564331f, ar); ai = fmaf(s3.y, -0.7175072431564331f, ai); br = fmaf(d3.x, -0.6965510249137878f, br); bi = fmaf(d3.y, -0.6965510249137878f, bi);
+      ar = fmaf(s4.x, 0.4827921986579895f, ar); ai = fmaf(s4.y, 0.4827921986579895f, ai); br = fmaf(d4.x, -0.8757349252700806f, br); bi = fmaf(d4.y, -0.8757349252700806f, bi);
+      ar = fmaf(s5.x, 0.9720228910446167f, ar); ai = fmaf(s5.y, 0.9720228910446167f, ai); br = fmaf(d5.x, 0.2348860502243042f, br); bi = fmaf(d5.y, 0.2348860502243042f, bi);
+      ar = fmaf(s6.x, 0.029633328318595886f, ar); ai = fmaf(s6.y, 0.029633328318595886f, ai); br = fmaf(d6.x, 0.9995608329772949f, br); bi = fmaf(d6.y, 0.9995608329772949f, bi);
+      ar = fmaf(s7.x, -0.956400990486145f, ar); ai = fmaf(s7.y, -0.956400990486145f, ai); br = fmaf(d7.x, 0.29205676913261414f, br); bi = fmaf(d7.y, 0.29205676913261414f, bi);
+      ar = fmaf(s8.x, -0.5338233709335327f, ar); ai = fmaf(s8.y, -0.5338233709335327f, ai); br = fmaf(d8.x, -0.8455960154533386f, br); bi = fmaf(d8.y, -0.8455960154533386f, bi);
+      ar = fmaf(s9.x, 0.674983024597168f, ar); ai = fmaf(s9.y, 0.674983024597168f, ai); br = fmaf(d9.x, -0.7378332614898682f, br); bi = fmaf(d9.y, -0.7378332614898682f, bi);
+      ar = fmaf(s10.x, 0.8896570801734924f, ar); ai = fmaf(s10.y, 0.8896570801734924f, ai); br = fmaf(d10.x, 0.4566292464733124f, br); bi = fmaf(d10.y, 0.4566292464733124f, bi);
+      ar = fmaf(s11.x, -0.2059786170721054f, ar); ai = fmaf(s11.y, -0.2059786170721054f, ai); br = fmaf(d11.x, 0.9785565137863159f, br); bi = fmaf(d11.y, 0.9785565137863159f, bi);
+      ar = fmaf(s12.x, -0.9982437491416931f, ar); ai = fmaf(s12.y, -0.9982437491416931f, ai); br = fmaf(d12.x, 0.05924062803387642f, br); bi = fmaf(d12.y, 0.05924062803387642f, bi);
+      ar = fmaf(s13.x, -0.3202698528766632f, ar); ai = fmaf(s13.y, -0.3202698528766632f, ai); br = fmaf(d13.x, -0.9473263621330261f, br); bi = fmaf(d13.y, -0.9473263621330261f, bi);
+      ar = fmaf(s14.x, 0.829405665397644f, ar); ai = fmaf(s14.y, 0.829405665397644f, ai); br = fmaf(d14.x, -0.5586467385292053f, br); bi = fmaf(d14.y, -0.5586467385292053f, bi);
+      ar = fmaf(s15.x, 0.7575112581253052f, ar); ai = fmaf(s15.y, 0.7575112581253052f, ai); br = fmaf(d15.x, 0.6528221368789673f, br); bi = fmaf(d15.y, 0.6528221368789673f, bi);
+      ar = fmaf(s16.x, -0.43006521463394165f, ar); ai = fmaf(s16.y, -0.43006521463394165f, ai); br = fmaf(d16.x, 0.9027978181838989f, br); bi = fmaf(d16.y, 0.9027978181838989f, bi);
+      ar = fmaf(s17.x, -0.9842305779457092f, ar); ai = fmaf(s17.y, -0.9842305779457092f, ai); br = fmaf(d17.x, -0.1768902689218521f, br); bi = fmaf(d17.y, -0.1768902689218521f, bi);
+      ar = fmaf(s18.x, -0.08879589289426804f, ar); ai = fmaf(s18.y, -0.08879589289426804f, ai); br = fmaf(d18.x, -0.9960498213768005f, br); bi = fmaf(d18.y, -0.9960498213768005f, bi);
+      ar = fmaf(s19.x, 0.9374196529388428f, ar); ai = fmaf(s19.y, 0.9374196529388428f, ai); br = fmaf(d19.x, -0.3482016324996948f, br); bi = fmaf(d19.y, -0.3482016324996948f, bi);
+      ar = fmaf(s20.x, 0.5829795002937317f, ar); ai = fmaf(s20.y, 0.5829795002937317f, ai); br = fmaf(d20.x, 0.8124868869781494f, br); bi = fmaf(d20.y, 0.8124868869781494f, bi);
+      ar = fmaf(s21.x, -0.6300878524780273f, ar); ai = fmaf(s21.y, -0.6300878524780273f, ai); br = fmaf(d21.x, 0.7765238881111145f, br); bi = fmaf(d21.y, 0.7765238881111145f, bi);
+      ar = fmaf(s22.x, -0.9151456356048584f, ar); ai = fmaf(s22.y, -0.9151456356048584f, ai); br = fmaf(d22.x, -0.4031234383583069f, br); bi = fmaf(d22.y, -0.4031234383583069f, bi);
+      ar = fmaf(s23.x, 0.14764656126499176f, ar); ai = fmaf(s23.y, 0.14764656126499176f, ai); br = fmaf(d23.x, -0.989040195941925f, br); bi = fmaf(d23.y, -0.989040195941925f, bi);
+      ar = fmaf(s24.x, 0.9929810762405396f, ar); ai = fmaf(s24.y, 0.9929810762405396f, ai); br = fmaf(d24.x, -0.11827316880226135f, br); bi = fmaf(d24.y, -0.11827316880226135f, bi);
+      ar = fmaf(s25.x, 0.3758275806903839f, ar); ai = fmaf(s25.y, 0.3758275806903839f, ai); br = fmaf(d25.x, 0.926689624786377f, br); bi = fmaf(d25.y, 0.926689624786377f, bi);
+      ar = fmaf(s26.x, -0.794854462146759f, ar); ai = fmaf(s26.y, -0.794854462146759f, ai); br = fmaf(d26.x, 0.6068001389503479f, br); bi = fmaf(d26.y, 0.6068001389503479f, bi);
+      if (!INV) { st(11, make_float2(ar + bi, ai - br)); st(42, make_float2(ar - bi, ai + br)); }
+      else { st(11, make_float2(ar - bi, ai + br)); st(42, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.14764656126499176f, ar); ai = fmaf(s1.y, 0.14764656126499176f, ai); br = fmaf(d1.x, 0.989040195941925f, br); bi = fmaf(d1.y, 0.989040195941925f, bi);
+      ar = fmaf(s2.x, -0.956400990486145f, ar); ai = fmaf(s2.y, -0.956400990486145f, ai); br = fmaf(d2.x, 0.29205676913261414f, br); bi = fmaf(d2.y, 0.29205676913261414f, bi);
+      ar = fmaf(s3.x, -0.43006521463394165f, ar); ai = fmaf(s3.y, -0.43006521463394165f, ai); br = fmaf(d3.x, -0.9027978181838989f, br); bi = fmaf(d3.y, -0.9027978181838989f, bi);
+      ar = fmaf(s4.x, 0.829405665397644f, ar); ai = fmaf(s4.y, 0.829405665397644f, ai); br = fmaf(d4.x, -0.5586467385292053f, br); bi = fmaf(d4.y, -0.5586467385292053f, bi);
+      ar = fmaf(s5.x, 0.674983024597168f, ar); ai = fmaf(s5.y, 0.674983024597168f, ai); br = fmaf(d5.x, 0.7378332614898682f, br); bi = fmaf(d5.y, 0.7378332614898682f, bi);
+      ar = fmaf(s6.x, -0.6300878524780273f, ar); ai = fmaf(s6.y, -0.6300878524780273f, ai); br = fmaf(d6.x, 0.7765238881111145f, br); bi = fmaf(d6.y, 0.7765238881111145f, bi);
+      ar = fmaf(s7.x, -0.8610436320304871f, ar); ai = fmaf(s7.y, -0.8610436320304871f, ai); br = fmaf(d7.x, -0.5085310935974121f, br); bi = fmaf(d7.y, -0.5085310935974121f, bi);
+      ar = fmaf(s8.x, 0.3758275806903839f, ar); ai = fmaf(s8.y, 0.3758275806903839f, ai); br = fmaf(d8.x, -0.926689624786377f, br); bi = fmaf(d8.y, -0.926689624786377f, bi);
+      ar = fmaf(s9.x, 0.9720228910446167f, ar); ai = fmaf(s9.y, 0.9720228910446167f, ai); br = fmaf(d9.x, 0.2348860502243042f, br); bi = fmaf(d9.y, 0.2348860502243042f, bi);
+      ar = fmaf(s10.x, -0.08879589289426804f, ar); ai = fmaf(s10.y, -0.08879589289426804f, ai); br = fmaf(d10.x, 0.9960498213768005f, br); bi = fmaf(d10.y, 0.9960498213768005f, bi);
+      ar = fmaf(s11.x, -0.9982437491416931f, ar); ai = fmaf(s11.y, -0.9982437491416931f, ai); br = fmaf(d11.x, 0.05924062803387642f, br); bi = fmaf(d11.y, 0.05924062803387642f, bi);
+      ar = fmaf(s12.x, -0.2059786170721054f, ar); ai = fmaf(s12.y, -0.2059786170721054f, ai); br = fmaf(d12.x, -0.9785565137863159f, br); bi = fmaf(d12.y, -0.9785565137863159f, bi);
+      ar = fmaf(s13.x, 0.9374196529388428f, ar); ai = fmaf(s13.y, 0.9374196529388428f, ai); br = fmaf(d13.x, -0.3482016324996948f, br); bi = fmaf(d13.y, -0.3482016324996948f, bi);
+      ar = fmaf(s14.x, 0.4827921986579895f, ar); ai = fmaf(s14.y, 0.4827921986579895f, ai); br = fmaf(d14.x, 0.8757349252700806f, br); bi = fmaf(d14.y, 0.8757349252700806f, bi);
+      ar = fmaf(s15.x, -0.794854462146759f, ar); ai = fmaf(s15.y, -0.794854462146759f, ai); br = fmaf(d15.x, 0.6068001389503479f, br); bi = fmaf(d15.y, 0.6068001389503479f, bi);
+      ar = fmaf(s16.x, -0.7175072431564331f, ar); ai = fmaf(s16.y, -0.7175072431564331f, ai); br = fmaf(d16.x, -0.6965510249137878f, br); bi = fmaf(d16.y, -0.6965510249137878f, bi);
+      ar = fmaf(s17.x, 0.5829795002937317f, ar); ai = fmaf(s17.y, 0.5829795002937317f, ai); br = fmaf(d17.x, -0.8124868869781494f, br); bi = fmaf(d17.y, -0.8124868869781494f, bi);
+      ar = fmaf(s18.x, 0.8896570801734924f, ar); ai = fmaf(s18.y, 0.8896570801734924f, ai); br = fmaf(d18.x, 0.4566292464733124f, br); bi = fmaf(d18.y, 0.4566292464733124f, bi);
+      ar = fmaf(s19.x, -0.3202698528766632f, ar); ai = fmaf(s19.y, -0.3202698528766632f, ai); br = fmaf(d19.x, 0.9473263621330261f, br); bi = fmaf(d19.y, 0.9473263621330261f, bi);
+      ar = fmaf(s20.x, -0.9842305779457092f, ar); ai = fmaf(s20.y, -0.9842305779457092f, ai); br = fmaf(d20.x, -0.1768902689218521f, br); bi = fmaf(d20.y, -0.1768902689218521f, bi);
+      ar = fmaf(s21.x, 0.029633328318595886f, ar); ai = fmaf(s21.y, 0.029633328318595886f, ai); br = fmaf(d21.x, -0.9995608329772949f, br); bi = fmaf(d21.y, -0.9995608329772949f, bi);
+      ar = fmaf(s22.x, 0.9929810762405396f, ar); ai = fmaf(s22.y, 0.9929810762405396f, ai); br = fmaf(d22.x, -0.11827316880226135f, br); bi = fmaf(d22.y, -0.11827316880226135f, bi);
+      ar = fmaf(s23.x, 0.26358717679977417f, ar); ai = fmaf(s23.y, 0.26358717679977417f, ai); br = fmaf(d23.x, 0.9646356105804443f, br); bi = fmaf(d23.y, 0.9646356105804443f, bi);
+      ar = fmaf(s24.x, -0.9151456356048584f, ar); ai = fmaf(s24.y, -0.9151456356048584f, ai); br = fmaf(d24.x, 0.4031234383583069f, br); bi = fmaf(d24.y, 0.4031234383583069f, bi);
+      ar = fmaf(s25.x, -0.5338233709335327f, ar); ai = fmaf(s25.y, -0.5338233709335327f, ai); br = fmaf(d25.x, -0.8455960154533386f, br); bi = fmaf(d25.y, -0.8455960154533386f, bi);
+      ar = fmaf(s26.x, 0.7575112581253052f, ar); ai = fmaf(s26.y, 0.7575112581253052f, ai); br = fmaf(d26.x, -0.6528221368789673f, br); bi = fmaf(d26.y, -0.6528221368789673f, bi);
+      if (!INV) { st(12, make_float2(ar + bi, ai - br)); st(41, make_float2(ar - bi, ai + br)); }
+      else { st(12, make_float2(ar - bi, ai + br)); st(41, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, 0.029633328318595886f, ar); ai = fmaf(s1.y, 0.029633328318595886f, ai); br = fmaf(d1.x, 0.9995608329772949f, br); bi = fmaf(d1.y, 0.9995608329772949f, bi);
+      ar = fmaf(s2.x, -0.9982437491416931f, ar); ai = fmaf(s2.y, -0.9982437491416931f, ai); br = fmaf(d2.x, 0.05924062803387642f, br); bi = fmaf(d2.y, 0.05924062803387642f, bi);
+      ar = fmaf(s3.x, -0.08879589289426804f, ar); ai = fmaf(s3.y, -0.08879589289426804f, ai); br = fmaf(d3.x, -0.9960498213768005f, br); bi = fmaf(d3.y, -0.9960498213768005f, bi);
+      ar = fmaf(s4.x, 0.9929810762405396f, ar); ai = fmaf(s4.y, 0.9929810762405396f, ai); br = fmaf(d4.x, -0.11827316880226135f, br); bi = fmaf(d4.y, -0.11827316880226135f, bi);
+      ar = fmaf(s5.x, 0.14764656126499176f, ar); ai = fmaf(s5.y, 0.14764656126499176f, ai); br = fmaf(d5.x, 0.989040195941925f, br); bi = fmaf(d5.y, 0.989040195941925f, bi);
+      ar = fmaf(s6.x, -0.9842305779457092f, ar); ai = fmaf(s6.y, -0.9842305779457092f, ai); br = fmaf(d6.x, 0.1768902689218521f, br); bi = fmaf(d6.y, 0.1768902689218521f, bi);
+      ar = fmaf(s7.x, -0.2059786170721054f, ar); ai = fmaf(s7.y, -0.2059786170721054f, ai); br = fmaf(d7.x, -0.9785565137863159f, br); bi = fmaf(d7.y, -0.9785565137863159f, bi);
+      ar = fmaf(s8.x, 0.9720228910446167f, ar); ai = fmaf(s8.y, 0.9720228910446167f, ai); br = fmaf(d8.x, -0.2348860502243042f, br); bi = fmaf(d8.y, -0.2348860502243042f, bi);
+      ar = fmaf(s9.x, 0.26358717679977417f, ar); ai = fmaf(s9.y, 0.26358717679977417f, ai); br = fmaf(d9.x, 0.9646356105804443f, br); bi = fmaf(d9.y, 0.9646356105804443f, bi);
+      ar = fmaf(s10.x, -0.956400990486145f, ar); ai = fmaf(s10.y, -0.956400990486145f, ai); br = fmaf(d10.x, 0.29205676913261414f, br); bi = fmaf(d10.y, 0.29205676913261414f, bi);
+      ar = fmaf(s11.x, -0.3202698528766632f, ar); ai = fmaf(s11.y, -0.3202698528766632f, ai); br = fmaf(d11.x, -0.9473263621330261f, br); bi = fmaf(d11.y, -0.9473263621330261f, bi);
+      ar = fmaf(s12.x, 0.9374196529388428f, ar); ai = fmaf(s12.y, 0.9374196529388428f, ai); br = fmaf(d12.x, -0.3482016324996948f, br); bi = fmaf(d12.y, -0.3482016324996948f, bi);
+      ar = fmaf(s13.x, 0.3758275806903839f, ar); ai = fmaf(s13.y, 0.3758275806903839f, ai); br = fmaf(d13.x, 0.926689624786377f, br); bi = fmaf(d13.y, 0.926689624786377f, bi);
+      ar = fmaf(s14.x, -0.9151456356048584f, ar); ai = fmaf(s14.y, -0.9151456356048584f, ai); br = fmaf(d14.x, 0.4031234383583069f, br); bi = fmaf(d14.y, 0.4031234383583069f, bi);
+      ar = fmaf(s15.x, -0.43006521463394165f, ar); ai = fmaf(s15.y, -0.43006521463394165f, ai); br = fmaf(d15.x, -0.9027978181838989f, br); bi = fmaf(d15.y, -0.9027978181838989f, bi);
+      ar = fmaf(s16.x, 0.8896570801734924f, ar); ai = fmaf(s16.y, 0.8896570801734924f, ai); br = fmaf(d16.x, -0.4566292464733124f, br); bi = fmaf(d16.y, -0.4566292464733124f, bi);
+      ar = fmaf(s17.x, 0.4827921986579895f, ar); ai = fmaf(s17.y, 0.4827921986579895f, ai); br = fmaf(d17.x, 0.8757349252700806f, br); bi = fmaf(d17.y, 0.8757349252700806f, bi);
+      ar = fmaf(s18.x, -0.8610436320304871f, ar); ai = fmaf(s18.y, -0.8610436320304871f, ai); br = fmaf(d18.x, 0.5085310935974121f, br); bi = fmaf(d18.y, 0.5085310935974121f, bi);
+      ar = fmaf(s19.x, -0.5338233709335327f, ar); ai = fmaf(s19.y, -0.5338233709335327f, ai); br = fmaf(d19.x, -0.8455960154533386f, br); bi = fmaf(d19.y, -0.8455960154533386f, bi);
+      ar = fmaf(s20.x, 0.829405665397644f, ar); ai = fmaf(s20.y, 0.829405665397644f, ai); br = fmaf(d20.x, -0.5586467385292053f, br); bi = fmaf(d20.y, -0.5586467385292053f, bi);
+      ar = fmaf(s21.x, 0.5829795002937317f, ar); ai = fmaf(s21.y, 0.5829795002937317f, ai); br = fmaf(d21.x, 0.8124868869781494f, br); bi = fmaf(d21.y, 0.8124868869781494f, bi);
+      ar = fmaf(s22.x, -0.794854462146759f, ar); ai = fmaf(s22.y, -0.794854462146759f, ai); br = fmaf(d22.x, 0.6068001389503479f, br); bi = fmaf(d22.y, 0.6068001389503479f, bi);
+      ar = fmaf(s23.x, -0.6300878524780273f, ar); ai = fmaf(s23.y, -0.6300878524780273f, ai); br = fmaf(d23.x, -0.7765238881111145f, br); bi = fmaf(d23.y, -0.7765238881111145f, bi);
+      ar = fmaf(s24.x, 0.7575112581253052f, ar); ai = fmaf(s24.y, 0.7575112581253052f, ai); br = fmaf(d24.x, -0.6528221368789673f, br); bi = fmaf(d24.y, -0.6528221368789673f, bi);
+      ar = fmaf(s25.x, 0.674983024597168f, ar); ai = fmaf(s25.y, 0.674983024597168f, ai); br = fmaf(d25.x, 0.7378332614898682f, br); bi = fmaf(d25.y, 0.7378332614898682f, bi);
+      ar = fmaf(s26.x, -0.7175072431564331f, ar); ai = fmaf(s26.y, -0.7175072431564331f, ai); br = fmaf(d26.x, 0.6965510249137878f, br); bi = fmaf(d26.y, 0.6965510249137878f, bi);
+      if (!INV) { st(13, make_float2(ar + bi, ai - br)); st(40, make_float2(ar - bi, ai + br)); }
+      else { st(13, make_float2(ar - bi, ai + br)); st(40, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.08879589289426804f, ar); ai = fmaf(s1.y, -0.08879589289426804f, ai); br = fmaf(d1.x, 0.9960498213768005f, br); bi = fmaf(d1.y, 0.9960498213768005f, bi);
+      ar = fmaf(s2.x, -0.9842305779457092f, ar); ai = fmaf(s2.y, -0.9842305779457092f, ai); br = fmaf(d2.x, -0.1768902689218521f, br); bi = fmaf(d2.y, -0.1768902689218521f, bi);
+      ar = fmaf(s3.x, 0.26358717679977417f, ar); ai = fmaf(s3.y, 0.26358717679977417f, ai); br = fmaf(d3.x, -0.9646356105804443f, br); bi = fmaf(d3.y, -0.9646356105804443f, bi);
+      ar = fmaf(s4.x, 0.9374196529388428f, ar); ai = fmaf(s4.y, 0.9374196529388428f, ai); br = fmaf(d4.x, 0.3482016324996948f, br); bi = fmaf(d4.y, 0.3482016324996948f, bi);
+      ar = fmaf(s5.x, -0.43006521463394165f, ar); ai = fmaf(s5.y, -0.43006521463394165f, ai); br = fmaf(d5.x, 0.9027978181838989f, br); bi = fmaf(d5.y, 0.9027978181838989f, bi);
+      ar = fmaf(s6.x, -0.8610436320304871f, ar); ai = fmaf(s6.y, -0.8610436320304871f, ai); br = fmaf(d6.x, -0.5085310935974121f, br); bi = fmaf(d6.y, -0.5085310935974121f, bi);
+      ar = fmaf(s7.x, 0.5829795002937317f, ar); ai = fmaf(s7.y, 0.5829795002937317f, ai); br = fmaf(d7.x, -0.8124868869781494f, br); bi = fmaf(d7.y, -0.8124868869781494f, bi);
+      ar = fmaf(s8.x, 0.7575112581253052f, ar); ai = fmaf(s8.y, 0.7575112581253052f, ai); br = fmaf(d8.x, 0.6528221368789673f, br); bi = fmaf(d8.y, 0.6528221368789673f, bi);
+      ar = fmaf(s9.x, -0.7175072431564331f, ar); ai = fmaf(s9.y, -0.7175072431564331f, ai); br = fmaf(d9.x, 0.6965510249137878f, br); bi = fmaf(d9.y, 0.6965510249137878f, bi);
+      ar = fmaf(s10.x, -0.6300878524780273f, ar); ai = fmaf(s10.y, -0.6300878524780273f, ai); br = fmaf(d10.x, -0.7765238881111145f, br); bi = fmaf(d10.y, -0.7765238881111145f, bi);
+      ar = fmaf(s11.x, 0.829405665397644f, ar); ai = fmaf(s11.y, 0.829405665397644f, ai); br = fmaf(d11.x, -0.5586467385292053f, br); bi = fmaf(d11.y, -0.5586467385292053f, bi);
+      ar = fmaf(s12.x, 0.4827921986579895f, ar); ai = fmaf(s12.y, 0.4827921986579895f, ai); br = fmaf(d12.x, 0.8757349252700806f, br); bi = fmaf(d12.y, 0.8757349252700806f, bi);
+      ar = fmaf(s13.x, -0.9151456356048584f, ar); ai = fmaf(s13.y, -0.9151456356048584f, ai); br = fmaf(d13.x, 0.4031234383583069f, br); bi = fmaf(d13.y, 0.4031234383583069f, bi);
+      ar = fmaf(s14.x, -0.3202698528766632f, ar); ai = fmaf(s14.y, -0.3202698528766632f, ai); br = fmaf(d14.x, -0.9473263621330261f, br); bi = fmaf(d14.y, -0.9473263621330261f, bi);
+      ar = fmaf(s15.x, 0.9720228910446167f, ar); ai = fmaf(s15.y, 0.9720228910446167f, ai); br = fmaf(d15.x, -0.2348860502243042f, br); bi = fmaf(d15.y, -0.2348860502243042f, bi);
+      ar = fmaf(s16.x, 0.14764656126499176f, ar); ai = fmaf(s16.y, 0.14764656126499176f, ai); br = fmaf(d16.x, 0.989040195941925f, br); bi = fmaf(d16.y, 0.989040195941925f, bi);
+      ar = fmaf(s17.x, -0.9982437491416931f, ar); ai = fmaf(s17.y, -0.9982437491416931f, ai); br = fmaf(d17.x, 0.05924062803387642f, br); bi = fmaf(d17.y, 0.05924062803387642f, bi);
+      ar = fmaf(s18.x, 0.029633328318595886f, ar); ai = fmaf(s18.y, 0.029633328318595886f, ai); br = fmaf(d18.x, -0.9995608329772949f, br); bi = fmaf(d18.y, -0.9995608329772949f, bi);
+      ar = fmaf(s19.x, 0.9929810762405396f, ar); ai = fmaf(s19.y, 0.9929810762405396f, ai); br = fmaf(d19.x, 0.11827316880226135f, br); bi = fmaf(d19.y, 0.11827316880226135f, bi);
+      ar = fmaf(s20.x, -0.2059786170721054f, ar); ai = fmaf(s20.y, -0.2059786170721054f, ai); br = fmaf(d20.x, 0.9785565137863159f, br); bi = fmaf(d20.y, 0.9785565137863159f, bi);
+      ar = fmaf(s21.x, -0.956400990486145f, ar); ai = fmaf(s21.y, -0.956400990486145f, ai); br = fmaf(d21.x, -0.29205676913261414f, br); bi = fmaf(d21.y, -0.29205676913261414f, bi);
+      ar = fmaf(s22.x, 0.3758275806903839f, ar); ai = fmaf(s22.y, 0.3758275806903839f, ai); br = fmaf(d22.x, -0.926689624786377f, br); bi = fmaf(d22.y, -0.926689624786377f, bi);
+      ar = fmaf(s23.x, 0.8896570801734924f, ar); ai = fmaf(s23.y, 0.8896570801734924f, ai); br = fmaf(d23.x, 0.4566292464733124f, br); bi = fmaf(d23.y, 0.4566292464733124f, bi);
+      ar = fmaf(s24.x, -0.5338233709335327f, ar); ai = fmaf(s24.y, -0.5338233709335327f, ai); br = fmaf(d24.x, 0.8455960154533386f, br); bi = fmaf(d24.y, 0.8455960154533386f, bi);
+      ar = fmaf(s25.x, -0.794854462146759f, ar); ai = fmaf(s25.y, -0.794854462146759f, ai); br = fmaf(d25.x, -0.6068001389503479f, br); bi = fmaf(d25.y, -0.6068001389503479f, bi);
+      ar = fmaf(s26.x, 0.674983024597168f, ar); ai = fmaf(s26.y, 0.674983024597168f, ai); br = fmaf(d26.x, -0.7378332614898682f, br); bi = fmaf(d26.y, -0.7378332614898682f, bi);
+      if (!INV) { st(14, make_float2(ar + bi, ai - br)); st(39, make_float2(ar - bi, ai + br)); }
+      else { st(14, make_float2(ar - bi, ai + br)); st(39, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.2059786170721054f, ar); ai = fmaf(s1.y, -0.2059786170721054f, ai); br = fmaf(d1.x, 0.9785565137863159f, br); bi = fmaf(d1.y, 0.9785565137863159f, bi);
+      ar = fmaf(s2.x, -0.9151456356048584f, ar); ai = fmaf(s2.y, -0.9151456356048584f, ai); br = fmaf(d2.x, -0.4031234383583069f, br); bi = fmaf(d2.y, -0.4031234383583069f, bi);
+      ar = fmaf(s3.x, 0.5829795002937317f, ar); ai = fmaf(s3.y, 0.5829795002937317f, ai); br = fmaf(d3.x, -0.8124868869781494f, br); bi = fmaf(d3.y, -0.8124868869781494f, bi);
+      ar = fmaf(s4.x, 0.674983024597168f, ar); ai = fmaf(s4.y, 0.674983024597168f, ai); br = fmaf(d4.x, 0.7378332614898682f, br); bi = fmaf(d4.y, 0.7378332614898682f, bi);
+      ar = fmaf(s5.x, -0.8610436320304871f, ar); ai = fmaf(s5.y, -0.8610436320304871f, ai); br = fmaf(d5.x, 0.5085310935974121f, br); bi = fmaf(d5.y, 0.5085310935974121f, bi);
+      ar = fmaf(s6.x, -0.3202698528766632f, ar); ai = fmaf(s6.y, -0.3202698528766632f, ai); br = fmaf(d6.x, -0.9473263621330261f, br); bi = fmaf(d6.y, -0.9473263621330261f, bi);
+      ar = fmaf(s7.x, 0.9929810762405396f, ar); ai = fmaf(s7.y, 0.9929810762405396f, ai); br = fmaf(d7.x, -0.11827316880226135f, br); bi = fmaf(d7.y, -0.11827316880226135f, bi);
+      ar = fmaf(s8.x, -0.08879589289426804f, ar); ai = fmaf(s8.y, -0.08879589289426804f, ai); br = fmaf(d8.x, 0.9960498213768005f, br); bi = fmaf(d8.y, 0.9960498213768005f, bi);
+      ar = fmaf(s9.x, -0.956400990486145f, ar); ai = fmaf(s9.y, -0.956400990486145f, ai); br = fmaf(d9.x, -0.29205676913261414f, br); bi = fmaf(d9.y, -0.29205676913261414f, bi);
+      ar = fmaf(s10.x, 0.4827921986579895f, ar); ai = fmaf(s10.y, 0.4827921986579895f, ai); br = fmaf(d10.x, -0.8757349252700806f, br); bi = fmaf(d10.y, -0.8757349252700806f, bi);
+      ar = fmaf(s11.x, 0.7575112581253052f, ar); ai = fmaf(s11.y, 0.7575112581253052f, ai); br = fmaf(d11.x, 0.6528221368789673f, br); bi = fmaf(d11.y, 0.6528221368789673f, bi);
+      ar = fmaf(s12.x, -0.794854462146759f, ar); ai = fmaf(s12.y, -0.794854462146759f, ai); br = fmaf(d12.x, 0.6068001389503479f, br); bi = fmaf(d12.y, 0.6068001389503479f, bi);
+      ar = fmaf(s13.x, -0.43006521463394165f, ar); ai = fmaf(s13.y, -0.43006521463394165f, ai); br = fmaf(d13.x, -0.9027978181838989f, br); bi = fmaf(d13.y, -0.9027978181838989f, bi);
+      ar = fmaf(s14.x, 0.9720228910446167f, ar); ai = fmaf(s14.y, 0.9720228910446167f, ai); br = fmaf(d14.x, -0.2348860502243042f, br); bi = fmaf(d14.y, -0.2348860502243042f, bi);
+      ar = fmaf(s15.x, 0.029633328318595886f, ar); ai = fmaf(s15.y, 0.029633328318595886f, ai); br = fmaf(d15.x, 0.9995608329772949f, br); bi = fmaf(d15.y, 0.9995608329772949f, bi);
+      ar = fmaf(s16.x, -0.9842305779457092f, ar); ai = fmaf(s16.y, -0.9842305779457092f, ai); br = fmaf(d16.x, -0.1768902689218521f, br); bi = fmaf(d16.y, -0.1768902689218521f, bi);
+      ar = fmaf(s17.x, 0.3758275806903839f, ar); ai = fmaf(s17.y, 0.3758275806903839f, ai); br = fmaf(d17.x, -0.926689624786377f, br); bi = fmaf(d17.y, -0.926689624786377f, bi);
+      ar = fmaf(s18.x, 0.829405665397644f, ar); ai = fmaf(s18.y, 0.829405665397644f, ai); br = fmaf(d18.x, 0.5586467385292053f, br); bi = fmaf(d18.y, 0.5586467385292053f, bi);
+      ar = fmaf(s19.x, -0.7175072431564331f, ar); ai = fmaf(s19.y, -0.7175072431564331f, ai); br = fmaf(d19.x, 0.6965510249137878f, br); bi = fmaf(d19.y, 0.6965510249137878f, bi);
+      ar = fmaf(s20.x, -0.5338233709335327f, ar); ai = fmaf(s20.y, -0.5338233709335327f, ai); br = fmaf(d20.x, -0.8455960154533386f, br); bi = fmaf(d20.y, -0.8455960154533386f, bi);
+      ar = fmaf(s21.x, 0.9374196529388428f, ar); ai = fmaf(s21.y, 0.9374196529388428f, ai); br = fmaf(d21.x, -0.3482016324996948f, br); bi = fmaf(d21.y, -0.3482016324996948f, bi);
+      ar = fmaf(s22.x, 0.14764656126499176f, ar); ai = fmaf(s22.y, 0.14764656126499176f, ai); br = fmaf(d22.x, 0.989040195941925f, br); bi = fmaf(d22.y, 0.989040195941925f, bi);
+      ar = fmaf(s23.x, -0.9982437491416931f, ar); ai = fmaf(s23.y, -0.9982437491416931f, ai); br = fmaf(d23.x, -0.05924062803387642f, br); bi = fmaf(d23.y, -0.05924062803387642f, bi);
+      ar = fmaf(s24.x, 0.26358717679977417f, ar); ai = fmaf(s24.y, 0.26358717679977417f, ai); br = fmaf(d24.x, -0.9646356105804443f, br); bi = fmaf(d24.y, -0.9646356105804443f, bi);
+      ar = fmaf(s25.x, 0.8896570801734924f, ar); ai = fmaf(s25.y, 0.8896570801734924f, ai); br = fmaf(d25.x, 0.4566292464733124f, br); bi = fmaf(d25.y, 0.4566292464733124f, bi);
+      ar = fmaf(s26.x, -0.6300878524780273f, ar); ai = fmaf(s26.y, -0.6300878524780273f, ai); br = fmaf(d26.x, 0.7765238881111145f, br); bi = fmaf(d26.y, 0.7765238881111145f, bi);
+      if (!INV) { st(15, make_float2(ar + bi, ai - br)); st(38, make_float2(ar - bi, ai + br)); }
+      else { st(15, make_float2(ar - bi, ai + br)); st(38, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.3202698528766632f, ar); ai = fmaf(s1.y, -0.3202698528766632f, ai); br = fmaf(d1.x, 0.9473263621330261f, br); bi = fmaf(d1.y, 0.9473263621330261f, bi);
+      ar = fmaf(s2.x, -0.794854462146759f, ar); ai = fmaf(s2.y, -0.794854462146759f, ai); br = fmaf(d2.x, -0.6068001389503479f, br); bi = fmaf(d2.y, -0.6068001389503479f, bi);
+      ar = fmaf(s3.x, 0.829405665397644f, ar); ai = fmaf(s3.y, 0.829405665397644f, ai); br = fmaf(d3.x, -0.5586467385292053f, br); bi = fmaf(d3.y, -0.5586467385292053f, bi);
+      ar = fmaf(s4.x, 0.26358717679977417f, ar); ai = fmaf(s4.y, 0.26358717679977417f, ai); br = fmaf(d4.x, 0.9646356105804443f, br); bi = fmaf(d4.y, 0.9646356105804443f, bi);
+      ar = fmaf(s5.x, -0.9982437491416931f, ar); ai = fmaf(s5.y, -0.9982437491416931f, ai); br = fmaf(d5.x, -0.05924062803387642f, br); bi = fmaf(d5.y, -0.05924062803387642f, bi);
+      ar = fmaf(s6.x, 0.3758275806903839f, ar); ai = fmaf(s6.y, 0.3758275806903839f, ai); br = fmaf(d6.x, -0.926689624786377f, br); bi = fmaf(d6.y, -0.926689624786377f, bi);
+      ar = fmaf(s7.x, 0.7575112581253052f, ar); ai = fmaf(s7.y, 0.7575112581253052f, ai); br = fmaf(d7.x, 0.6528221368789673f, br); bi = fmaf(d7.y, 0.6528221368789673f, bi);
+      ar = fmaf(s8.x, -0.8610436320304871f, ar); ai = fmaf(s8.y, -0.8610436320304871f, ai); br = fmaf(d8.x, 0.5085310935974121f, br); bi = fmaf(d8.y, 0.5085310935974121f, bi);
+      ar = fmaf(s9.x, -0.2059786170721054f, ar); ai = fmaf(s9.y, -0.2059786170721054f, ai); br = fmaf(d9.x, -0.9785565137863159f, br); bi = fmaf(d9.y, -0.9785565137863159f, bi);
+      ar = fmaf(s10.x, 0.9929810762405396f, ar); ai = fmaf(s10.y, 0.9929810762405396f, ai); br = fmaf(d10.x, 0.11827316880226135f, br); bi = fmaf(d10.y, 0.11827316880226135f, bi);
+      ar = fmaf(s11.x, -0.43006521463394165f, ar); ai = fmaf(s11.y, -0.43006521463394165f, ai); br = fmaf(d11.x, 0.9027978181838989f, br); bi = fmaf(d11.y, 0.9027978181838989f, bi);
+      ar = fmaf(s12.x, -0.7175072431564331f, ar); ai = fmaf(s12.y, -0.7175072431564331f, ai); br = fmaf(d12.x, -0.6965510249137878f, br); bi = fmaf(d12.y, -0.6965510249137878f, bi);
+      ar = fmaf(s13.x, 0.8896570801734924f, ar); ai = fmaf(s13.y, 0.8896570801734924f, ai); br = fmaf(d13.x, -0.4566292464733124f, br); bi = fmaf(d13.y, -0.4566292464733124f, bi);
+      ar = fmaf(s14.x, 0.14764656126499176f, ar); ai = fmaf(s14.y, 0.14764656126499176f, ai); br = fmaf(d14.x, 0.989040195941925f, br); bi = fmaf(d14.y, 0.989040195941925f, bi);
+      ar = fmaf(s15.x, -0.9842305779457092f, ar); ai = fmaf(s15.y, -0.9842305779457092f, ai); br = fmaf(d15.x, -0.1768902689218521f, br); bi = fmaf(d15.y, -0.1768902689218521f, bi);
+      ar = fmaf(s16.x, 0.4827921986579895f, ar); ai = fmaf(s16.y, 0.4827921986579895f, ai); br = fmaf(d16.x, -0.8757349252700806f, br); bi = fmaf(d16.y, -0.8757349252700806f, bi);
+      ar = fmaf(s17.x, 0.674983024597168f, ar); ai = fmaf(s17.y, 0.674983024597168f, ai); br = fmaf(d17.x, 0.7378332614898682f, br); bi = fmaf(d17.y, 0.7378332614898682f, bi);
+      ar = fmaf(s18.x, -0.9151456356048584f, ar); ai = fmaf(s18.y, -0.9151456356048584f, ai); br = fmaf(d18.x, 0.4031234383583069f, br); bi = fmaf(d18.y, 0.4031234383583069f, bi);
+      ar = fmaf(s19.x, -0.08879589289426804f, ar); ai = fmaf(s19.y, -0.08879589289426804f, ai); br = fmaf(d19.x, -0.9960498213768005f, br); bi = fmaf(d19.y, -0.9960498213768005f, bi);
+      ar = fmaf(s20.x, 0.9720228910446167f, ar); ai = fmaf(s20.y, 0.9720228910446167f, ai); br = fmaf(d20.x, 0.2348860502243042f, br); bi = fmaf(d20.y, 0.2348860502243042f, bi);
+      ar = fmaf(s21.x, -0.5338233709335327f, ar); ai = fmaf(s21.y, -0.5338233709335327f, ai); br = fmaf(d21.x, 0.8455960154533386f, br); bi = fmaf(d21.y, 0.8455960154533386f, bi);
+      ar = fmaf(s22.x, -0.6300878524780273f, ar); ai = fmaf(s22.y, -0.6300878524780273f, ai); br = fmaf(d22.x, -0.7765238881111145f, br); bi = fmaf(d22.y, -0.7765238881111145f, bi);
+      ar = fmaf(s23.x, 0.9374196529388428f, ar); ai = fmaf(s23.y, 0.9374196529388428f, ai); br = fmaf(d23.x, -0.3482016324996948f, br); bi = fmaf(d23.y, -0.3482016324996948f, bi);
+      ar = fmaf(s24.x, 0.029633328318595886f, ar); ai = fmaf(s24.y, 0.029633328318595886f, ai); br = fmaf(d24.x, 0.9995608329772949f, br); bi = fmaf(d24.y, 0.9995608329772949f, bi);
+      ar = fmaf(s25.x, -0.956400990486145f, ar); ai = fmaf(s25.y, -0.956400990486145f, ai); br = fmaf(d25.x, -0.29205676913261414f, br); bi = fmaf(d25.y, -0.29205676913261414f, bi);
+      ar = fmaf(s26.x, 0.5829795002937317f, ar); ai = fmaf(s26.y, 0.5829795002937317f, ai); br = fmaf(d26.x, -0.8124868869781494f, br); bi = fmaf(d26.y, -0.8124868869781494f, bi);
+      if (!INV) { st(16, make_float2(ar + bi, ai - br)); st(37, make_float2(ar - bi, ai + br)); }
+      else { st(16, make_float2(ar - bi, ai + br)); st(37, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.43006521463394165f, ar); ai = fmaf(s1.y, -0.43006521463394165f, ai); br = fmaf(d1.x, 0.9027978181838989f, br); bi = fmaf(d1.y, 0.9027978181838989f, bi);
+      ar = fmaf(s2.x, -0.6300878524780273f, ar); ai = fmaf(s2.y, -0.6300878524780273f, ai); br = fmaf(d2.x, -0.7765238881111145f, br); bi = fmaf(d2.y, -0.7765238881111145f, bi);
+      ar = fmaf(s3.x, 0.9720228910446167f, ar); ai = fmaf(s3.y, 0.9720228910446167f, ai); br = fmaf(d3.x, -0.2348860502243042f, br); bi = fmaf(d3.y, -0.2348860502243042f, bi);
+      ar = fmaf(s4.x, -0.2059786170721054f, ar); ai = fmaf(s4.y, -0.2059786170721054f, ai); br = fmaf(d4.x, 0.9785565137863159f, br); bi = fmaf(d4.y, 0.9785565137863159f, bi);
+      ar = fmaf(s5.x, -0.794854462146759f, ar); ai = fmaf(s5.y, -0.794854462146759f, ai); br = fmaf(d5.x, -0.6068001389503479f, br); bi = fmaf(d5.y, -0.6068001389503479f, bi);
+      ar = fmaf(s6.x, 0.8896570801734924f, ar); ai = fmaf(s6.y, 0.8896570801734924f, ai); br = fmaf(d6.x, -0.4566292464733124f, br); bi = fmaf(d6.y, -0.4566292464733124f, bi);
+      ar = fmaf(s7.x, 0.029633328318595886f, ar); ai = fmaf(s7.y, 0.029633328318595886f, ai); br = fmaf(d7.x, 0.9995608329772949f, br); bi = fmaf(d7.y, 0.9995608329772949f, bi);
+      ar = fmaf(s8.x, -0.9151456356048584f, ar); ai = fmaf(s8.y, -0.9151456356048584f, ai); br = fmaf(d8.x, -0.4031234383583069f, br); bi = fmaf(d8.y, -0.4031234383583069f, bi);
+      ar = fmaf(s9.x, 0.7575112581253052f, ar); ai = fmaf(s9.y, 0.7575112581253052f, ai); br = fmaf(d9.x, -0.6528221368789673f, br); bi = fmaf(d9.y, -0.6528221368789673f, bi);
+      ar = fmaf(s10.x, 0.26358717679977417f, ar); ai = fmaf(s10.y, 0.26358717679977417f, ai); br = fmaf(d10.x, 0.9646356105804443f, br); bi = fmaf(d10.y, 0.9646356105804443f, bi);
+      ar = fmaf(s11.x, -0.9842305779457092f, ar); ai = fmaf(s11.y, -0.9842305779457092f, ai); br = fmaf(d11.x, -0.1768902689218521f, br); bi = fmaf(d11.y, -0.1768902689218521f, bi);
+      ar = fmaf(s12.x, 0.5829795002937317f, ar); ai = fmaf(s12.y, 0.5829795002937317f, ai); br = fmaf(d12.x, -0.8124868869781494f, br); bi = fmaf(d12.y, -0.8124868869781494f, bi);
+      ar = fmaf(s13.x, 0.4827921986579895f, ar); ai = fmaf(s13.y, 0.4827921986579895f, ai); br = fmaf(d13.x, 0.8757349252700806f, br); bi = fmaf(d13.y, 0.8757349252700806f, bi);
+      ar = fmaf(s14.x, -0.9982437491416931f, ar); ai = fmaf(s14.y, -0.9982437491416931f, ai); br = fmaf(d14.x, 0.05924062803387642f, br); bi = fmaf(d14.y, 0.05924062803387642f, bi);
+      ar = fmaf(s15.x, 0.3758275806903839f, ar); ai = fmaf(s15.y, 0.3758275806903839f, ai); br = fmaf(d15.x, -0.926689624786377f, br); bi = fmaf(d15.y, -0.926689624786377f, bi);
+      ar = fmaf(s16.x, 0.674983024597168f, ar); ai = fmaf(s16.y, 0.674983024597168f, ai); br = fmaf(d16.x, 0.7378332614898682f, br); bi = fmaf(d16.y, 0.7378332614898682f, bi);
+      ar = fmaf(s17.x, -0.956400990486145f, ar); ai = fmaf(s17.y, -0.956400990486145f, ai); br = fmaf(d17.x, 0.29205676913261414f, br); bi = fmaf(d17.y, 0.29205676913261414f, bi);
+      ar = fmaf(s18.x, 0.14764656126499176f, ar); ai = fmaf(s18.y, 0.14764656126499176f, ai); br = fmaf(d18.x, -0.989040195941925f, br); bi = fmaf(d18.y, -0.989040195941925f, bi);
+      ar = fmaf(s19.x, 0.829405665397644f, ar); ai = fmaf(s19.y, 0.829405665397644f, ai); br = fmaf(d19.x, 0.5586467385292053f, br); bi = fmaf(d19.y, 0.5586467385292053f, bi);
+      ar = fmaf(s20.x, -0.8610436320304871f, ar); ai = fmaf(s20.y, -0.8610436320304871f, ai); br = fmaf(d20.x, 0.5085310935974121f, br); bi = fmaf(d20.y, 0.5085310935974121f, bi);
+      ar = fmaf(s21.x, -0.08879589289426804f, ar); ai = fmaf(s21.y, -0.08879589289426804f, ai); br = fmaf(d21.x, -0.9960498213768005f, br); bi = fmaf(d21.y, -0.9960498213768005f, bi);
+      ar = fmaf(s22.x, 0.9374196529388428f, ar); ai = fmaf(s22.y, 0.9374196529388428f, ai); br = fmaf(d22.x, 0.3482016324996948f, br); bi = fmaf(d22.y, 0.3482016324996948f, bi);
+      ar = fmaf(s23.x, -0.7175072431564331f, ar); ai = fmaf(s23.y, -0.7175072431564331f, ai); br = fmaf(d23.x, 0.6965510249137878f, br); bi = fmaf(d23.y, 0.6965510249137878f, bi);
+      ar = fmaf(s24.x, -0.3202698528766632f, ar); ai = fmaf(s24.y, -0.3202698528766632f, ai); br = fmaf(d24.x, -0.9473263621330261f, br); bi = fmaf(d24.y, -0.9473263621330261f, bi);
+      ar = fmaf(s25.x, 0.9929810762405396f, ar); ai = fmaf(s25.y, 0.9929810762405396f, ai); br = fmaf(d25.x, 0.11827316880226135f, br); bi = fmaf(d25.y, 0.11827316880226135f, bi);
+      ar = fmaf(s26.x, -0.5338233709335327f, ar); ai = fmaf(s26.y, -0.5338233709335327f, ai); br = fmaf(d26.x, 0.8455960154533386f, br); bi = fmaf(d26.y, 0.8455960154533386f, bi);
+      if (!INV) { st(17, make_float2(ar + bi, ai - br)); st(36, make_float2(ar - bi, ai + br)); }
+      else { st(17, make_float2(ar - bi, ai + br)); st(36, make_float2(ar + bi, ai - br)); }
+    }
+    break;
+  }
+  case 2: {
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.5338233709335327f, ar); ai = fmaf(s1.y, -0.5338233709335327f, ai); br = fmaf(d1.x, 0.8455960154533386f, br); bi = fmaf(d1.y, 0.8455960154533386f, bi);
+      ar = fmaf(s2.x, -0.43006521463394165f, ar); ai = fmaf(s2.y, -0.43006521463394165f, ai); br = fmaf(d2.x, -0.9027978181838989f, br); bi = fmaf(d2.y, -0.9027978181838989f, bi);
+      ar = fmaf(s3.x, 0.9929810762405396f, ar); ai = fmaf(s3.y, 0.9929810762405396f, ai); br = fmaf(d3.x, 0.11827316880226135f, br); bi = fmaf(d3.y, 0.11827316880226135f, bi);
+      ar = fmaf(s4.x, -0.6300878524780273f, ar); ai = fmaf(s4.y, -0.6300878524780273f, ai); br = fmaf(d4.x, 0.7765238881111145f, br); bi = fmaf(d4.y, 0.7765238881111145f, bi);
+      ar = fmaf(s5.x, -0.3202698528766632f, ar); ai = fmaf(s5.y, -0.3202698528766632f, ai); br = fmaf(d5.x, -0.9473263621330261f, br); bi = fmaf(d5.y, -0.9473263621330261f, bi);
+      ar = fmaf(s6.x, 0.9720228910446167f, ar); ai = fmaf(s6.y, 0.9720228910446167f, ai); br = fmaf(d6.x, 0.2348860502243042f, br); bi = fmaf(d6.y, 0.2348860502243042f, bi);
+      ar = fmaf(s7.x, -0.7175072431564331f, ar); ai = fmaf(s7.y, -0.7175072431564331f, ai); br = fmaf(d7.x, 0.6965510249137878f, br); bi = fmaf(d7.y, 0.6965510249137878f, bi);
+      ar = fmaf(s8.x, -0.2059786170721054f, ar); ai = fmaf(s8.y, -0.2059786170721054f, ai); br = fmaf(d8.x, -0.9785565137863159f, br); bi = fmaf(d8.y, -0.9785565137863159f, bi);
+      ar = fmaf(s9.x, 0.9374196529388428f, ar); ai = fmaf(s9.y, 0.9374196529388428f, ai); br = fmaf(d9.x, 0.3482016324996948f, br); bi = fmaf(d9.y, 0.3482016324996948f, bi);
+      ar = fmaf(s10.x, -0.794854462146759f, ar); ai = fmaf(s10.y, -0.794854462146759f, ai); br = fmaf(d10.x, 0.6068001389503479f, br); bi = fmaf(d10.y, 0.6068001389503479f, bi);
+      ar = fmaf(s11.x, -0.08879589289426804f, ar); ai = fmaf(s11.y, -0.08879589289426804f, ai); br = fmaf(d11.x, -0.9960498213768005f, br); bi = fmaf(d11.y, -0.9960498213768005f, bi);
+      ar = fmaf(s12.x, 0.8896570801734924f, ar); ai = fmaf(s12.y, 0.8896570801734924f, ai); br = fmaf(d12.x, 0.4566292464733124f, br); bi = fmaf(d12.y, 0.4566292464733124f, bi);
+      ar = fmaf(s13.x, -0.8610436320304871f, ar); ai = fmaf(s13.y, -0.8610436320304871f, ai); br = fmaf(d13.x, 0.5085310935974121f, br); bi = fmaf(d13.y, 0.5085310935974121f, bi);
+      ar = fmaf(s14.x, 0.029633328318595886f, ar); ai = fmaf(s14.y, 0.029633328318595886f, ai); br = fmaf(d14.x, -0.9995608329772949f, br); bi = fmaf(d14.y, -0.9995608329772949f, bi);
+      ar = fmaf(s15.x, 0.829405665397644f, ar); ai = fmaf(s15.y, 0.829405665397644f, ai); br = fmaf(d15.x, 0.5586467385292053f, br); bi = fmaf(d15.y, 0.5586467385292053f, bi);
+      ar = fmaf(s16.x, -0.9151456356048584f, ar); ai = fmaf(s16.y, -0.9151456356048584f, ai); br = fmaf(d16.x, 0.4031234383583069f, br); bi = fmaf(d16.y, 0.4031234383583069f, bi);
+      ar = fmaf(s17.x, 0.14764656126499176f, ar); ai = fmaf(s17.y, 0.14764656126499176f, ai); br = fmaf(d17.x, -0.989040195941925f, br); bi = fmaf(d17.y, -0.989040195941925f, bi);
+      ar = fmaf(s18.x, 0.7575112581253052f, ar); ai = fmaf(s18.y, 0.7575112581253052f, ai); br = fmaf(d18.x, 0.6528221368789673f, br); bi = fmaf(d18.y, 0.6528221368789673f, bi);
+      ar = fmaf(s19.x, -0.956400990486145f, ar); ai = fmaf(s19.y, -0.956400990486145f, ai); br = fmaf(d19.x, 0.29205676913261414f, br); bi = fmaf(d19.y, 0.29205676913261414f, bi);
+      ar = fmaf(s20.x, 0.26358717679977417f, ar); ai = fmaf(s20.y, 0.26358717679977417f, ai); br = fmaf(d20.x, -0.9646356105804443f, br); bi = fmaf(d20.y, -0.9646356105804443f, bi);
+      ar = fmaf(s21.x, 0.674983024597168f, ar); ai = fmaf(s21.y, 0.674983024597168f, ai); br = fmaf(d21.x, 0.7378332614898682f, br); bi = fmaf(d21.y, 0.7378332614898682f, bi);
+      ar = fmaf(s22.x, -0.9842305779457092f, ar); ai = fmaf(s22.y, -0.9842305779457092f, ai); br = fmaf(d22.x, 0.1768902689218521f, br); bi = fmaf(d22.y, 0.1768902689218521f, bi);
+      ar = fmaf(s23.x, 0.3758275806903839f, ar); ai = fmaf(s23.y, 0.3758275806903839f, ai); br = fmaf(d23.x, -0.926689624786377f, br); bi = fmaf(d23.y, -0.926689624786377f, bi);
+      ar = fmaf(s24.x, 0.5829795002937317f, ar); ai = fmaf(s24.y, 0.5829795002937317f, ai); br = fmaf(d24.x, 0.8124868869781494f, br); bi = fmaf(d24.y, 0.8124868869781494f, bi);
+      ar = fmaf(s25.x, -0.9982437491416931f, ar); ai = fmaf(s25.y, -0.9982437491416931f, ai); br = fmaf(d25.x, 0.05924062803387642f, br); bi = fmaf(d25.y, 0.05924062803387642f, bi);
+      ar = fmaf(s26.x, 0.4827921986579895f, ar); ai = fmaf(s26.y, 0.4827921986579895f, ai); br = fmaf(d26.x, -0.8757349252700806f, br); bi = fmaf(d26.y, -0.8757349252700806f, bi);
+      if (!INV) { st(18, make_float2(ar + bi, ai - br)); st(35, make_float2(ar - bi, ai + br)); }
+      else { st(18, make_float2(ar - bi, ai + br)); st(35, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.6300878524780273f, ar); ai = fmaf(s1.y, -0.6300878524780273f, ai); br = fmaf(d1.x, 0.7765238881111145f, br); bi = fmaf(d1.y, 0.7765238881111145f, bi);
+      ar = fmaf(s2.x, -0.2059786170721054f, ar); ai = fmaf(s2.y, -0.2059786170721054f, ai); br = fmaf(d2.x, -0.9785565137863159f, br); bi = fmaf(d2.y, -0.9785565137863159f, bi);
+      ar = fmaf(s3.x, 0.8896570801734924f, ar); ai = fmaf(s3.y, 0.8896570801734924f, ai); br = fmaf(d3.x, 0.4566292464733124f, br); bi = fmaf(d3.y, 0.4566292464733124f, bi);
+      ar = fmaf(s4.x, -0.9151456356048584f, ar); ai = fmaf(s4.y, -0.9151456356048584f, ai); br = fmaf(d4.x, 0.4031234383583069f, br); bi = fmaf(d4.y, 0.4031234383583069f, bi);
+      ar = fmaf(s5.x, 0.26358717679977417f, ar); ai = fmaf(s5.y, 0.26358717679977417f, ai); br = fmaf(d5.x, -0.9646356105804443f, br); bi = fmaf(d5.y, -0.9646356105804443f, bi);
+      ar = fmaf(s6.x, 0.5829795002937317f, ar); ai = fmaf(s6.y, 0.5829795002937317f, ai); br = fmaf(d6.x, 0.8124868869781494f, br); bi = fmaf(d6.y, 0.8124868869781494f, bi);
+      ar = fmaf(s7.x, -0.9982437491416931f, ar); ai = fmaf(s7.y, -0.9982437491416931f, ai); br = fmaf(d7.x, -0.05924062803387642f, br); bi = fmaf(d7.y, -0.05924062803387642f, bi);
+      ar = fmaf(s8.x, 0.674983024597168f, ar); ai = fmaf(s8.y, 0.674983024597168f, ai); br = fmaf(d8.x, -0.7378332614898682f, br); bi = fmaf(d8.y, -0.7378332614898682f, bi);
+      ar = fmaf(s9.x, 0.14764656126499176f, ar); ai = fmaf(s9.y, 0.14764656126499176f, ai); br = fmaf(d9.x, 0.989040195941925f, br); bi = fmaf(d9.y, 0.989040195941925f, bi);
+      ar = fmaf(s10.x, -0.8610436320304871f, ar); ai = fmaf(s10.y, -0.8610436320304871f, ai); br = fmaf(d10.x, -0.5085310935974121f, br); bi = fmaf(d10.y, -0.5085310935974121f, bi);
+      ar = fmaf(s11.x, 0.9374196529388428f, ar); ai = fmaf(s11.y, 0.9374196529388428f, ai); br = fmaf(d11.x, -0.3482016324996948f, br); bi = fmaf(d11.y, -0.3482016324996948f, bi);
+      ar = fmaf(s12.x, -0.3202698528766632f, ar); ai = fmaf(s12.y, -0.3202698528766632f, ai); br = fmaf(d12.x, 0.9473263621330261f, br); bi = fmaf(d12.y, 0.9473263621330261f, bi);
+      ar = fmaf(s13.x, -0.5338233709335327f, ar); ai = fmaf(s13.y, -0.5338233709335327f, ai); br = fmaf(d13.x, -0.8455960154533386f, br); bi = fmaf(d13.y, -0.8455960154533386f, bi);
+      ar = fmaf(s14.x, 0.9929810762405396f, ar); ai = fmaf(s14.y, 0.9929810762405396f, ai); br = fmaf(d14.x, 0.11827316880226135f, br); bi = fmaf(d14.y, 0.11827316880226135f, bi);
+      ar = fmaf(s15.x, -0.7175072431564331f, ar); ai = fmaf(s15.y, -0.7175072431564331f, ai); br = fmaf(d15.x, 0.6965510249137878f, br); bi = fmaf(d15.y, 0.6965510249137878f, bi);
+      ar = fmaf(s16.x, -0.08879589289426804f, ar); ai = fmaf(s16.y, -0.08879589289426804f, ai); br = fmaf(d16.x, -0.9960498213768005f, br); bi = fmaf(d16.y, -0.9960498213768005f, bi);
+      ar = fmaf(s17.x, 0.829405665397644f, ar); ai = fmaf(s17.y, 0.829405665397644f, ai); br = fmaf(d17.x, 0.5586467385292053f, br); bi = fmaf(d17.y, 0.5586467385292053f, bi);
+      ar = fmaf(s18.x, -0.956400990486145f, ar); ai = fmaf(s18.y, -0.956400990486145f, ai); br = fmaf(d18.x, 0.29205676913261414f, br); bi = fmaf(d18.y, 0.29205676913261414f, bi);
+      ar = fmaf(s19.x, 0.3758275806903839f, ar); ai = fmaf(s19.y, 0.3758275806903839f, ai); br = fmaf(d19.x, -0.926689624786377f, br); bi = fmaf(d19.y, -0.926689624786377f, bi);
+      ar = fmaf(s20.x, 0.4827921986579895f, ar); ai = fmaf(s20.y, 0.4827921986579895f, ai); br = fmaf(d20.x, 0.8757349252700806f, br); bi = fmaf(d20.y, 0.8757349252700806f, bi);
+      ar = fmaf(s21.x, -0.9842305779457092f, ar); ai = fmaf(s21.y, -0.9842305779457092f, ai); br = fmaf(d21.x, -0.1768902689218521f, br); bi = fmaf(d21.y, -0.1768902689218521f, bi);
+      ar = fmaf(s22.x, 0.7575112581253052f, ar); ai = fmaf(s22.y, 0.7575112581253052f, ai); br = fmaf(d22.x, -0.6528221368789673f, br); bi = fmaf(d22.y, -0.6528221368789673f, bi);
+      ar = fmaf(s23.x, 0.029633328318595886f, ar); ai = fmaf(s23.y, 0.029633328318595886f, ai); br = fmaf(d23.x, 0.9995608329772949f, br); bi = fmaf(d23.y, 0.9995608329772949f, bi);
+      ar = fmaf(s24.x, -0.794854462146759f, ar); ai = fmaf(s24.y, -0.794854462146759f, ai); br = fmaf(d24.x, -0.6068001389503479f, br); bi = fmaf(d24.y, -0.6068001389503479f, bi);
+      ar = fmaf(s25.x, 0.9720228910446167f, ar); ai = fmaf(s25.y, 0.9720228910446167f, ai); br = fmaf(d25.x, -0.2348860502243042f, br); bi = fmaf(d25.y, -0.2348860502243042f, bi);
+      ar = fmaf(s26.x, -0.43006521463394165f, ar); ai = fmaf(s26.y, -0.43006521463394165f, ai); br = fmaf(d26.x, 0.9027978181838989f, br); bi = fmaf(d26.y, 0.9027978181838989f, bi);
+      if (!INV) { st(19, make_float2(ar + bi, ai - br)); st(34, make_float2(ar - bi, ai + br)); }
+      else { st(19, make_float2(ar - bi, ai + br)); st(34, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.7175072431564331f, ar); ai = fmaf(s1.y, -0.7175072431564331f, ai); br = fmaf(d1.x, 0.6965510249137878f, br); bi = fmaf(d1.y, 0.6965510249137878f, bi);
+      ar = fmaf(s2.x, 0.029633328318595886f, ar); ai = fmaf(s2.y, 0.029633328318595886f, ai); br = fmaf(d2.x, -0.9995608329772949f, br); bi = fmaf(d2.y, -0.9995608329772949f, bi);
+      ar = fmaf(s3.x, 0.674983024597168f, ar); ai = fmaf(s3.y, 0.674983024597168f, ai); br = fmaf(d3.x, 0.7378332614898682f, br); bi = fmaf(d3.y, 0.7378332614898682f, bi);
+      ar = fmaf(s4.x, -0.9982437491416931f, ar); ai = fmaf(s4.y, -0.9982437491416931f, ai); br = fmaf(d4.x, -0.05924062803387642f, br); bi = fmaf(d4.y, -0.05924062803387642f, bi);
+      ar = fmaf(s5.x, 0.7575112581253052f, ar); ai = fmaf(s5.y, 0.7575112581253052f, ai); br = fmaf(d5.x, -0.6528221368789673f, br); bi = fmaf(d5.y, -0.6528221368789673f, bi);
+      ar = fmaf(s6.x, -0.08879589289426804f, ar); ai = fmaf(s6.y, -0.08879589289426804f, ai); br = fmaf(d6.x, 0.9960498213768005f, br); bi = fmaf(d6.y, 0.9960498213768005f, bi);
+      ar = fmaf(s7.x, -0.6300878524780273f, ar); ai = fmaf(s7.y, -0.6300878524780273f, ai); br = fmaf(d7.x, -0.7765238881111145f, br); bi = fmaf(d7.y, -0.7765238881111145f, bi);
+      ar = fmaf(s8.x, 0.9929810762405396f, ar); ai = fmaf(s8.y, 0.9929810762405396f, ai); br = fmaf(d8.x, 0.11827316880226135f, br); bi = fmaf(d8.y, 0.11827316880226135f, bi);
+      ar = fmaf(s9.x, -0.794854462146759f, ar); ai = fmaf(s9.y, -0.794854462146759f, ai); br = fmaf(d9.x, 0.6068001389503479f, br); bi = fmaf(d9.y, 0.6068001389503479f, bi);
+      ar = fmaf(s10.x, 0.14764656126499176f, ar); ai = fmaf(s10.y, 0.14764656126499176f, ai); br = fmaf(d10.x, -0.989040195941925f, br); bi = fmaf(d10.y, -0.989040195941925f, bi);
+      ar = fmaf(s11.x, 0.5829795002937317f, ar); ai = fmaf(s11.y, 0.5829795002937317f, ai); br = fmaf(d11.x, 0.8124868869781494f, br); bi = fmaf(d11.y, 0.8124868869781494f, bi);
+      ar = fmaf(s12.x, -0.9842305779457092f, ar); ai = fmaf(s12.y, -0.9842305779457092f, ai); br = fmaf(d12.x, -0.1768902689218521f, br); bi = fmaf(d12.y, -0.1768902689218521f, bi);
+      ar = fmaf(s13.x, 0.829405665397644f, ar); ai = fmaf(s13.y, 0.829405665397644f, ai); br = fmaf(d13.x, -0.5586467385292053f, br); bi = fmaf(d13.y, -0.5586467385292053f, bi);
+      ar = fmaf(s14.x, -0.2059786170721054f, ar); ai = fmaf(s14.y, -0.2059786170721054f, ai); br = fmaf(d14.x, 0.9785565137863159f, br); bi = fmaf(d14.y, 0.9785565137863159f, bi);
+      ar = fmaf(s15.x, -0.5338233709335327f, ar); ai = fmaf(s15.y, -0.5338233709335327f, ai); br = fmaf(d15.x, -0.8455960154533386f, br); bi = fmaf(d15.y, -0.8455960154533386f, bi);
+      ar = fmaf(s16.x, 0.9720228910446167f, ar); ai = fmaf(s16.y, 0.9720228910446167f, ai); br = fmaf(d16.x, 0.2348860502243042f, br); bi = fmaf(d16.y, 0.2348860502243042f, bi);
+      ar = fmaf(s17.x, -0.8610436320304871f, ar); ai = fmaf(s17.y, -0.8610436320304871f, ai); br = fmaf(d17.x, 0.5085310935974121f, br); bi = fmaf(d17.y, 0.5085310935974121f, bi);
+      ar = fmaf(s18.x, 0.26358717679977417f, ar); ai = fmaf(s18.y, 0.26358717679977417f, ai); br = fmaf(d18.x, -0.9646356105804443f, br); bi = fmaf(d18.y, -0.9646356105804443f, bi);
+      ar = fmaf(s19.x, 0.4827921986579895f, ar); ai = fmaf(s19.y, 0.4827921986579895f, ai); br = fmaf(d19.x, 0.8757349252700806f, br); bi = fmaf(d19.y, 0.8757349252700806f, bi);
+      ar = fmaf(s20.x, -0.956400990486145f, ar); ai = fmaf(s20.y, -0.956400990486145f, ai); br = fmaf(d20.x, -0.29205676913261414f, br); bi = fmaf(d20.y, -0.29205676913261414f, bi);
+      ar = fmaf(s21.x, 0.8896570801734924f, ar); ai = fmaf(s21.y, 0.8896570801734924f, ai); br = fmaf(d21.x, -0.4566292464733124f, br); bi = fmaf(d21.y, -0.4566292464733124f, bi);
+      ar = fmaf(s22.x, -0.3202698528766632f, ar); ai = fmaf(s22.y, -0.3202698528766632f, ai); br = fmaf(d22.x, 0.9473263621330261f, br); bi = fmaf(d22.y, 0.9473263621330261f, bi);
+      ar = fmaf(s23.x, -0.43006521463394165f, ar); ai = fmaf(s23.y, -0.43006521463394165f, ai); br = fmaf(d23.x, -0.9027978181838989f, br); bi = fmaf(d23.y, -0.9027978181838989f, bi);
+      ar = fmaf(s24.x, 0.9374196529388428f, ar); ai = fmaf(s24.y, 0.9374196529388428f, ai); br = fmaf(d24.x, 0.3482016324996948f, br); bi = fmaf(d24.y, 0.3482016324996948f, bi);
+      ar = fmaf(s25.x, -0.9151456356048584f, ar); ai = fmaf(s25.y, -0.9151456356048584f, ai); br = fmaf(d25.x, 0.4031234383583069f, br); bi = fmaf(d25.y, 0.4031234383583069f, bi);
+      ar = fmaf(s26.x, 0.3758275806903839f, ar); ai = fmaf(s26.y, 0.3758275806903839f, ai); br = fmaf(d26.x, -0.926689624786377f, br); bi = fmaf(d26.y, -0.926689624786377f, bi);
+      if (!INV) { st(20, make_float2(ar + bi, ai - br)); st(33, make_float2(ar - bi, ai + br)); }
+      else { st(20, make_float2(ar - bi, ai + br)); st(33, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.794854462146759f, ar); ai = fmaf(s1.y, -0.794854462146759f, ai); br = fmaf(d1.x, 0.6068001389503479f, br); bi = fmaf(d1.y, 0.6068001389503479f, bi);
+      ar = fmaf(s2.x, 0.26358717679977417f, ar); ai = fmaf(s2.y, 0.26358717679977417f, ai); br = fmaf(d2.x, -0.9646356105804443f, br); bi = fmaf(d2.y, -0.9646356105804443f, bi);
+      ar = fmaf(s3.x, 0.3758275806903839f, ar); ai = fmaf(s3.y, 0.3758275806903839f, ai); br = fmaf(d3.x, 0.926689624786377f, br); bi = fmaf(d3.y, 0.926689624786377f, bi);
+      ar = fmaf(s4.x, -0.8610436320304871f, ar); ai = fmaf(s4.y, -0.8610436320304871f, ai); br = fmaf(d4.x, -0.5085310935974121f, br); bi = fmaf(d4.y, -0.5085310935974121f, bi);
+      ar = fmaf(s5.x, 0.9929810762405396f, ar); ai = fmaf(s5.y, 0.9929810762405396f, ai); br = fmaf(d5.x, -0.11827316880226135f, br); bi = fmaf(d5.y, -0.11827316880226135f, bi);
+      ar = fmaf(s6.x, -0.7175072431564331f, ar); ai = fmaf(s6.y, -0.7175072431564331f, ai); br = fmaf(d6.x, 0.6965510249137878f, br); bi = fmaf(d6.y, 0.6965510249137878f, bi);
+      ar = fmaf(s7.x, 0.14764656126499176f, ar); ai = fmaf(s7.y, 0.14764656126499176f, ai); br = fmaf(d7.x, -0.989040195941925f, br); bi = fmaf(d7.y, -0.989040195941925f, bi);
+      ar = fmaf(s8.x, 0.4827921986579895f, ar); ai = fmaf(s8.y, 0.4827921986579895f, ai); br = fmaf(d8.x, 0.8757349252700806f, br); bi = fmaf(d8.y, 0.8757349252700806f, bi);
+      ar = fmaf(s9.x, -0.9151456356048584f, ar); ai = fmaf(s9.y, -0.9151456356048584f, ai); br = fmaf(d9.x, -0.4031234383583069f, br); bi = fmaf(d9.y, -0.4031234383583069f, bi);
+      ar = fmaf(s10.x, 0.9720228910446167f, ar); ai = fmaf(s10.y, 0.9720228910446167f, ai); br = fmaf(d10.x, -0.2348860502243042f, br); bi = fmaf(d10.y, -0.2348860502243042f, bi);
+      ar = fmaf(s11.x, -0.6300878524780273f, ar); ai = fmaf(s11.y, -0.6300878524780273f, ai); br = fmaf(d11.x, 0.7765238881111145f, br); bi = fmaf(d11.y, 0.7765238881111145f, bi);
+      ar = fmaf(s12.x, 0.029633328318595886f, ar); ai = fmaf(s12.y, 0.029633328318595886f, ai); br = fmaf(d12.x, -0.9995608329772949f, br); bi = fmaf(d12.y, -0.9995608329772949f, bi);
+      ar = fmaf(s13.x, 0.5829795002937317f, ar); ai = fmaf(s13.y, 0.5829795002937317f, ai); br = fmaf(d13.x, 0.8124868869781494f, br); bi = fmaf(d13.y, 0.8124868869781494f, bi);
+      ar = fmaf(s14.x, -0.956400990486145f, ar); ai = fmaf(s14.y, -0.956400990486145f, ai); br = fmaf(d14.x, -0.29205676913261414f, br); bi = fmaf(d14.y, -0.29205676913261414f, bi);
+      ar = fmaf(s15.x, 0.9374196529388428f, ar); ai = fmaf(s15.y, 0.9374196529388428f, ai); br = fmaf(d15.x, -0.3482016324996948f, br); bi = fmaf(d15.y, -0.3482016324996948f, bi);
+      ar = fmaf(s16.x, -0.5338233709335327f, ar); ai = fmaf(s16.y, -0.5338233709335327f, ai); br = fmaf(d16.x, 0.8455960154533386f, br); bi = fmaf(d16.y, 0.8455960154533386f, bi);
+      ar = fmaf(s17.x, -0.08879589289426804f, ar); ai = fmaf(s17.y, -0.08879589289426804f, ai); br = fmaf(d17.x, -0.9960498213768005f, br); bi = fmaf(d17.y, -0.9960498213768005f, bi);
+      ar = fmaf(s18.x, 0.674983024597168f, ar); ai = fmaf(s18.y, 0.674983024597168f, ai); br = fmaf(d18.x, 0.7378332614898682f, br); bi = fmaf(d18.y, 0.7378332614898682f, bi);
+      ar = fmaf(s19.x, -0.9842305779457092f, ar); ai = fmaf(s19.y, -0.9842305779457092f, ai); br = fmaf(d19.x, -0.1768902689218521f, br); bi = fmaf(d19.y, -0.1768902689218521f, bi);
+      ar = fmaf(s20.x, 0.8896570801734924f, ar); ai = fmaf(s20.y, 0.8896570801734924f, ai); br = fmaf(d20.x, -0.4566292464733124f, br); bi = fmaf(d20.y, -0.4566292464733124f, bi);
+      ar = fmaf(s21.x, -0.43006521463394165f, ar); ai = fmaf(s21.y, -0.43006521463394165f, ai); br = fmaf(d21.x, 0.9027978181838989f, br); bi = fmaf(d21.y, 0.9027978181838989f, bi);
+      ar = fmaf(s22.x, -0.2059786170721054f, ar); ai = fmaf(s22.y, -0.2059786170721054f, ai); br = fmaf(d22.x, -0.9785565137863159f, br); bi = fmaf(d22.y, -0.9785565137863159f, bi);
+      ar = fmaf(s23.x, 0.7575112581253052f, ar); ai = fmaf(s23.y, 0.7575112581253052f, ai); br = fmaf(d23.x, 0.6528221368789673f, br); bi = fmaf(d23.y, 0.6528221368789673f, bi);
+      ar = fmaf(s24.x, -0.9982437491416931f, ar); ai = fmaf(s24.y, -0.9982437491416931f, ai); br = fmaf(d24.x, -0.05924062803387642f, br); bi = fmaf(d24.y, -0.05924062803387642f, bi);
+      ar = fmaf(s25.x, 0.829405665397644f, ar); ai = fmaf(s25.y, 0.829405665397644f, ai); br = fmaf(d25.x, -0.5586467385292053f, br); bi = fmaf(d25.y, -0.5586467385292053f, bi);
+      ar = fmaf(s26.x, -0.3202698528766632f, ar); ai = fmaf(s26.y, -0.3202698528766632f, ai); br = fmaf(d26.x, 0.9473263621330261f, br); bi = fmaf(d26.y, 0.9473263621330261f, bi);
+      if (!INV) { st(21, make_float2(ar + bi, ai - br)); st(32, make_float2(ar - bi, ai + br)); }
+      else { st(21, make_float2(ar - bi, ai + br)); st(32, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.8610436320304871f, ar); ai = fmaf(s1.y, -0.8610436320304871f, ai); br = fmaf(d1.x, 0.5085310935974121f, br); bi = fmaf(d1.y, 0.5085310935974121f, bi);
+      ar = fmaf(s2.x, 0.4827921986579895f, ar); ai = fmaf(s2.y, 0.4827921986579895f, ai); br = fmaf(d2.x, -0.8757349252700806f, br); bi = fmaf(d2.y, -0.8757349252700806f, bi);
+      ar = fmaf(s3.x, 0.029633328318595886f, ar); ai = fmaf(s3.y, 0.029633328318595886f, ai); br = fmaf(d3.x, 0.9995608329772949f, br); bi = fmaf(d3.y, 0.9995608329772949f, bi);
+      ar = fmaf(s4.x, -0.5338233709335327f, ar); ai = fmaf(s4.y, -0.5338233709335327f, ai); br = fmaf(d4.x, -0.8455960154533386f, br); bi = fmaf(d4.y, -0.8455960154533386f, bi);
+      ar = fmaf(s5.x, 0.8896570801734924f, ar); ai = fmaf(s5.y, 0.8896570801734924f, ai); br = fmaf(d5.x, 0.4566292464733124f, br); bi = fmaf(d5.y, 0.4566292464733124f, bi);
+      ar = fmaf(s6.x, -0.9982437491416931f, ar); ai = fmaf(s6.y, -0.9982437491416931f, ai); br = fmaf(d6.x, 0.05924062803387642f, br); bi = fmaf(d6.y, 0.05924062803387642f, bi);
+      ar = fmaf(s7.x, 0.829405665397644f, ar); ai = fmaf(s7.y, 0.829405665397644f, ai); br = fmaf(d7.x, -0.5586467385292053f, br); bi = fmaf(d7.y, -0.5586467385292053f, bi);
+      ar = fmaf(s8.x, -0.43006521463394165f, ar); ai = fmaf(s8.y, -0.43006521463394165f, ai); br = fmaf(d8.x, 0.9027978181838989f, br); bi = fmaf(d8.y, 0.9027978181838989f, bi);
+      ar = fmaf(s9.x, -0.08879589289426804f, ar); ai = fmaf(s9.y, -0.08879589289426804f, ai); br = fmaf(d9.x, -0.9960498213768005f, br); bi = fmaf(d9.y, -0.9960498213768005f, bi);
+      ar = fmaf(s10.x, 0.5829795002937317f, ar); ai = fmaf(s10.y, 0.5829795002937317f, ai); br = fmaf(d10.x, 0.8124868869781494f, br); bi = fmaf(d10.y, 0.8124868869781494f, bi);
+      ar = fmaf(s11.x, -0.9151456356048584f, ar); ai = fmaf(s11.y, -0.9151456356048584f, ai); br = fmaf(d11.x, -0.4031234383583069f, br); bi = fmaf(d11.y, -0.4031234383583069f, bi);
+      ar = fmaf(s12.x, 0.9929810762405396f, ar); ai = fmaf(s12.y, 0.9929810762405396f, ai); br = fmaf(d12.x, -0.11827316880226135f, br); bi = fmaf(d12.y, -0.11827316880226135f, bi);
+      ar = fmaf(s13.x, -0.794854462146759f, ar); ai = fmaf(s13.y, -0.794854462146759f, ai); br = fmaf(d13.x, 0.6068001389503479f, br); bi = fmaf(d13.y, 0.6068001389503479f, bi);
+      ar = fmaf(s14.x, 0.3758275806903839f, ar); ai = fmaf(s14.y, 0.3758275806903839f, ai); br = fmaf(d14.x, -0.926689624786377f, br); bi = fmaf(d14.y, -0.926689624786377f, bi);
+      ar = fmaf(s15.x, 0.14764656126499176f, ar); ai = fmaf(s15.y, 0.14764656126499176f, ai); br = fmaf(d15.x, 0.989040195941925f, br); bi = fmaf(d15.y, 0.989040195941925f, bi);
+      ar = fmaf(s16.x, -0.6300878524780273f, ar); ai = fmaf(s16.y, -0.6300878524780273f, ai); br = fmaf(d16.x, -0.7765238881111145f, br); bi = fmaf(d16.y, -0.7765238881111145f, bi);
+      ar = fmaf(s17.x, 0.9374196529388428f, ar); ai = fmaf(s17.y, 0.9374196529388428f, ai); br = fmaf(d17.x, 0.3482016324996948f, br); bi = fmaf(d17.y, 0.3482016324996948f, bi);
+      ar = fmaf(s18.x, -0.9842305779457092f, ar); ai = fmaf(s18.y, -0.9842305779457092f, ai); br = fmaf(d18.x, 0.1768902689218521f, br); bi = fmaf(d18.y, 0.1768902689218521f, bi);
+      ar = fmaf(s19.x, 0.7575112581253052f, ar); ai = fmaf(s19.y, 0.7575112581253052f, ai); br = fmaf(d19.x, -0.6528221368789673f, br); bi = fmaf(d19.y, -0.6528221368789673f, bi);
+      ar = fmaf(s20.x, -0.3202698528766632f, ar); ai = fmaf(s20.y, -0.3202698528766632f, ai); br = fmaf(d20.x, 0.9473263621330261f, br); bi = fmaf(d20.y, 0.9473263621330261f, bi);
+      ar = fmaf(s21.x, -0.2059786170721054f, ar); ai = fmaf(s21.y, -0.2059786170721054f, ai); br = fmaf(d21.x, -0.9785565137863159f, br); bi = fmaf(d21.y, -0.9785565137863159f, bi);
+      ar = fmaf(s22.x, 0.674983024597168f, ar); ai = fmaf(s22.y, 0.674983024597168f, ai); br = fmaf(d22.x, 0.7378332614898682f, br); bi = fmaf(d22.y, 0.7378332614898682f, bi);
+      ar = fmaf(s23.x, -0.956400990486145f, ar); ai = fmaf(s23.y, -0.956400990486145f, ai); br = fmaf(d23.x, -0.29205676913261414f, br); bi = fmaf(d23.y, -0.29205676913261414f, bi);
+      ar = fmaf(s24.x, 0.9720228910446167f, ar); ai = fmaf(s24.y, 0.9720228910446167f, ai); br = fmaf(d24.x, -0.2348860502243042f, br); bi = fmaf(d24.y, -0.2348860502243042f, bi);
+      ar = fmaf(s25.x, -0.7175072431564331f, ar); ai = fmaf(s25.y, -0.7175072431564331f, ai); br = fmaf(d25.x, 0.6965510249137878f, br); bi = fmaf(d25.y, 0.6965510249137878f, bi);
+      ar = fmaf(s26.x, 0.26358717679977417f, ar); ai = fmaf(s26.y, 0.26358717679977417f, ai); br = fmaf(d26.x, -0.9646356105804443f, br); bi = fmaf(d26.y, -0.9646356105804443f, bi);
+      if (!INV) { st(22, make_float2(ar + bi, ai - br)); st(31, make_float2(ar - bi, ai + br)); }
+      else { st(22, make_float2(ar - bi, ai + br)); st(31, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.9151456356048584f, ar); ai = fmaf(s1.y, -0.9151456356048584f, ai); br = fmaf(d1.x, 0.4031234383583069f, br); bi = fmaf(d1.y, 0.4031234383583069f, bi);
+      ar = fmaf(s2.x, 0.674983024597168f, ar); ai = fmaf(s2.y, 0.674983024597168f, ai); br = fmaf(d2.x, -0.7378332614898682f, br); bi = fmaf(d2.y, -0.7378332614898682f, bi);
+      ar = fmaf(s3.x, -0.3202698528766632f, ar); ai = fmaf(s3.y, -0.3202698528766632f, ai); br = fmaf(d3.x, 0.9473263621330261f, br); bi = fmaf(d3.y, 0.9473263621330261f, bi);
+      ar = fmaf(s4.x, -0.08879589289426804f, ar); ai = fmaf(s4.y, -0.08879589289426804f, ai); br = fmaf(d4.x, -0.9960498213768005f, br); bi = fmaf(d4.y, -0.9960498213768005f, bi);
+      ar = fmaf(s5.x, 0.4827921986579895f, ar); ai = fmaf(s5.y, 0.4827921986579895f, ai); br = fmaf(d5.x, 0.8757349252700806f, br); bi = fmaf(d5.y, 0.8757349252700806f, bi);
+      ar = fmaf(s6.x, -0.794854462146759f, ar); ai = fmaf(s6.y, -0.794854462146759f, ai); br = fmaf(d6.x, -0.6068001389503479f, br); bi = fmaf(d6.y, -0.6068001389503479f, bi);
+      ar = fmaf(s7.x, 0.9720228910446167f, ar); ai = fmaf(s7.y, 0.9720228910446167f, ai); br = fmaf(d7.x, 0.2348860502243042f, br); bi = fmaf(d7.y, 0.2348860502243042f, bi);
+      ar = fmaf(s8.x, -0.9842305779457092f, ar); ai = fmaf(s8.y, -0.9842305779457092f, ai); br = fmaf(d8.x, 0.1768902689218521f, br); bi = fmaf(d8.y, 0.1768902689218521f, bi);
+      ar = fmaf(s9.x, 0.829405665397644f, ar); ai = fmaf(s9.y, 0.829405665397644f, ai); br = fmaf(d9.x, -0.5586467385292053f, br); bi = fmaf(d9.y, -0.5586467385292053f, bi);
+      ar = fmaf(s10.x, -0.5338233709335327f, ar); ai = fmaf(s10.y, -0.5338233709335327f, ai); br = fmaf(d10.x, 0.8455960154533386f, br); bi = fmaf(d10.y, 0.8455960154533386f, bi);
+      ar = fmaf(s11.x, 0.14764656126499176f, ar); ai = fmaf(s11.y, 0.14764656126499176f, ai); br = fmaf(d11.x, -0.989040195941925f, br); bi = fmaf(d11.y, -0.989040195941925f, bi);
+      ar = fmaf(s12.x, 0.26358717679977417f, ar); ai = fmaf(s12.y, 0.26358717679977417f, ai); br = fmaf(d12.x, 0.9646356105804443f, br); bi = fmaf(d12.y, 0.9646356105804443f, bi);
+      ar = fmaf(s13.x, -0.6300878524780273f, ar); ai = fmaf(s13.y, -0.6300878524780273f, ai); br = fmaf(d13.x, -0.7765238881111145f, br); bi = fmaf(d13.y, -0.7765238881111145f, bi);
+      ar = fmaf(s14.x, 0.8896570801734924f, ar); ai = fmaf(s14.y, 0.8896570801734924f, ai); br = fmaf(d14.x, 0.4566292464733124f, br); bi = fmaf(d14.y, 0.4566292464733124f, bi);
+      ar = fmaf(s15.x, -0.9982437491416931f, ar); ai = fmaf(s15.y, -0.9982437491416931f, ai); br = fmaf(d15.x, -0.05924062803387642f, br); bi = fmaf(d15.y, -0.05924062803387642f, bi);
+      ar = fmaf(s16.x, 0.9374196529388428f, ar); ai = fmaf(s16.y, 0.9374196529388428f, ai); br = fmaf(d16.x, -0.3482016324996948f, br); bi = fmaf(d16.y, -0.3482016324996948f, bi);
+      ar = fmaf(s17.x, -0.7175072431564331f, ar); ai = fmaf(s17.y, -0.7175072431564331f, ai); br = fmaf(d17.x, 0.6965510249137878f, br); bi = fmaf(d17.y, 0.6965510249137878f, bi);
+      ar = fmaf(s18.x, 0.3758275806903839f, ar); ai = fmaf(s18.y, 0.3758275806903839f, ai); br = fmaf(d18.x, -0.926689624786377f, br); bi = fmaf(d18.y, -0.926689624786377f, bi);
+      ar = fmaf(s19.x, 0.029633328318595886f, ar); ai = fmaf(s19.y, 0.029633328318595886f, ai); br = fmaf(d19.x, 0.9995608329772949f, br); bi = fmaf(d19.y, 0.9995608329772949f, bi);
+      ar = fmaf(s20.x, -0.43006521463394165f, ar); ai = fmaf(s20.y, -0.43006521463394165f, ai); br = fmaf(d20.x, -0.9027978181838989f, br); bi = fmaf(d20.y, -0.9027978181838989f, bi);
+      ar = fmaf(s21.x, 0.7575112581253052f, ar); ai = fmaf(s21.y, 0.7575112581253052f, ai); br = fmaf(d21.x, 0.6528221368789673f, br); bi = fmaf(d21.y, 0.6528221368789673f, bi);
+      ar = fmaf(s22.x, -0.956400990486145f, ar); ai = fmaf(s22.y, -0.956400990486145f, ai); br = fmaf(d22.x, -0.29205676913261414f, br); bi = fmaf(d22.y, -0.29205676913261414f, bi);
+      ar = fmaf(s23.x, 0.9929810762405396f, ar); ai = fmaf(s23.y, 0.9929810762405396f, ai); br = fmaf(d23.x, -0.11827316880226135f, br); bi = fmaf(d23.y, -0.11827316880226135f, bi);
+      ar = fmaf(s24.x, -0.8610436320304871f, ar); ai = fmaf(s24.y, -0.8610436320304871f, ai); br = fmaf(d24.x, 0.5085310935974121f, br); bi = fmaf(d24.y, 0.5085310935974121f, bi);
+      ar = fmaf(s25.x, 0.5829795002937317f, ar); ai = fmaf(s25.y, 0.5829795002937317f, ai); br = fmaf(d25.x, -0.8124868869781494f, br); bi = fmaf(d25.y, -0.8124868869781494f, bi);
+      ar = fmaf(s26.x, -0.2059786170721054f, ar); ai = fmaf(s26.y, -0.2059786170721054f, ai); br = fmaf(d26.x, 0.9785565137863159f, br); bi = fmaf(d26.y, 0.9785565137863159f, bi);
+      if (!INV) { st(23, make_float2(ar + bi, ai - br)); st(30, make_float2(ar - bi, ai + br)); }
+      else { st(23, make_float2(ar - bi, ai + br)); st(30, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.956400990486145f, ar); ai = fmaf(s1.y, -0.956400990486145f, ai); br = fmaf(d1.x, 0.29205676913261414f, br); bi = fmaf(d1.y, 0.29205676913261414f, bi);
+      ar = fmaf(s2.x, 0.829405665397644f, ar); ai = fmaf(s2.y, 0.829405665397644f, ai); br = fmaf(d2.x, -0.5586467385292053f, br); bi = fmaf(d2.y, -0.5586467385292053f, bi);
+      ar = fmaf(s3.x, -0.6300878524780273f, ar); ai = fmaf(s3.y, -0.6300878524780273f, ai); br = fmaf(d3.x, 0.7765238881111145f, br); bi = fmaf(d3.y, 0.7765238881111145f, bi);
+      ar = fmaf(s4.x, 0.3758275806903839f, ar); ai = fmaf(s4.y, 0.3758275806903839f, ai); br = fmaf(d4.x, -0.926689624786377f, br); bi = fmaf(d4.y, -0.926689624786377f, bi);
+      ar = fmaf(s5.x, -0.08879589289426804f, ar); ai = fmaf(s5.y, -0.08879589289426804f, ai); br = fmaf(d5.x, 0.9960498213768005f, br); bi = fmaf(d5.y, 0.9960498213768005f, bi);
+      ar = fmaf(s6.x, -0.2059786170721054f, ar); ai = fmaf(s6.y, -0.2059786170721054f, ai); br = fmaf(d6.x, -0.9785565137863159f, br); bi = fmaf(d6.y, -0.9785565137863159f, bi);
+      ar = fmaf(s7.x, 0.4827921986579895f, ar); ai = fmaf(s7.y, 0.4827921986579895f, ai); br = fmaf(d7.x, 0.8757349252700806f, br); bi = fmaf(d7.y, 0.8757349252700806f, bi);
+      ar = fmaf(s8.x, -0.7175072431564331f, ar); ai = fmaf(s8.y, -0.7175072431564331f, ai); br = fmaf(d8.x, -0.6965510249137878f, br); bi = fmaf(d8.y, -0.6965510249137878f, bi);
+      ar = fmaf(s9.x, 0.8896570801734924f, ar); ai = fmaf(s9.y, 0.8896570801734924f, ai); br = fmaf(d9.x, 0.4566292464733124f, br); bi = fmaf(d9.y, 0.4566292464733124f, bi);
+      ar = fmaf(s10.x, -0.9842305779457092f, ar); ai = fmaf(s10.y, -0.9842305779457092f, ai); br = fmaf(d10.x, -0.1768902689218521f, br); bi = fmaf(d10.y, -0.1768902689218521f, bi);
+      ar = fmaf(s11.x, 0.9929810762405396f, ar); ai = fmaf(s11.y, 0.9929810762405396f, ai); br = fmaf(d11.x, -0.11827316880226135f, br); bi = fmaf(d11.y, -0.11827316880226135f, bi);
+      ar = fmaf(s12.x, -0.9151456356048584f, ar); ai = fmaf(s12.y, -0.9151456356048584f, ai); br = fmaf(d12.x, 0.4031234383583069f, br); bi = fmaf(d12.y, 0.4031234383583069f, bi);
+      ar = fmaf(s13.x, 0.7575112581253052f, ar); ai = fmaf(s13.y, 0.7575112581253052f, ai); br = fmaf(d13.x, -0.6528221368789673f, br); bi = fmaf(d13.y, -0.6528221368789673f, bi);
+      ar = fmaf(s14.x, -0.5338233709335327f, ar); ai = fmaf(s14.y, -0.5338233709335327f, ai); br = fmaf(d14.x, 0.8455960154533386f, br); bi = fmaf(d14.y, 0.8455960154533386f, bi);
+      ar = fmaf(s15.x, 0.26358717679977417f, ar); ai = fmaf(s15.y, 0.26358717679977417f, ai); br = fmaf(d15.x, -0.9646356105804443f, br); bi = fmaf(d15.y, -0.9646356105804443f, bi);
+      ar = fmaf(s16.x, 0.029633328318595886f, ar); ai = fmaf(s16.y, 0.029633328318595886f, ai); br = fmaf(d16.x, 0.9995608329772949f, br); bi = fmaf(d16.y, 0.9995608329772949f, bi);
+      ar = fmaf(s17.x, -0.3202698528766632f, ar); ai = fmaf(s17.y, -0.3202698528766632f, ai); br = fmaf(d17.x, -0.9473263621330261f, br); bi = fmaf(d17.y, -0.9473263621330261f, bi);
+      ar = fmaf(s18.x, 0.5829795002937317f, ar); ai = fmaf(s18.y, 0.5829795002937317f, ai); br = fmaf(d18.x, 0.8124868869781494f, br); bi = fmaf(d18.y, 0.8124868869781494f, bi);
+      ar = fmaf(s19.x, -0.794854462146759f, ar); ai = fmaf(s19.y, -0.794854462146759f, ai); br = fmaf(d19.x, -0.6068001389503479f, br); bi = fmaf(d19.y, -0.6068001389503479f, bi);
+      ar = fmaf(s20.x, 0.9374196529388428f, ar); ai = fmaf(s20.y, 0.9374196529388428f, ai); br = fmaf(d20.x, 0.3482016324996948f, br); bi = fmaf(d20.y, 0.3482016324996948f, bi);
+      ar = fmaf(s21.x, -0.9982437491416931f, ar); ai = fmaf(s21.y, -0.9982437491416931f, ai); br = fmaf(d21.x, -0.05924062803387642f, br); bi = fmaf(d21.y, -0.05924062803387642f, bi);
+      ar = fmaf(s22.x, 0.9720228910446167f, ar); ai = fmaf(s22.y, 0.9720228910446167f, ai); br = fmaf(d22.x, -0.2348860502243042f, br); bi = fmaf(d22.y, -0.2348860502243042f, bi);
+      ar = fmaf(s23.x, -0.8610436320304871f, ar); ai = fmaf(s23.y, -0.8610436320304871f, ai); br = fmaf(d23.x, 0.5085310935974121f, br); bi = fmaf(d23.y, 0.5085310935974121f, bi);
+      ar = fmaf(s24.x, 0.674983024597168f, ar); ai = fmaf(s24.y, 0.674983024597168f, ai); br = fmaf(d24.x, -0.7378332614898682f, br); bi = fmaf(d24.y, -0.7378332614898682f, bi);
+      ar = fmaf(s25.x, -0.43006521463394165f, ar); ai = fmaf(s25.y, -0.43006521463394165f, ai); br = fmaf(d25.x, 0.9027978181838989f, br); bi = fmaf(d25.y, 0.9027978181838989f, bi);
+      ar = fmaf(s26.x, 0.14764656126499176f, ar); ai = fmaf(s26.y, 0.14764656126499176f, ai); br = fmaf(d26.x, -0.989040195941925f, br); bi = fmaf(d26.y, -0.989040195941925f, bi);
+      if (!INV) { st(24, make_float2(ar + bi, ai - br)); st(29, make_float2(ar - bi, ai + br)); }
+      else { st(24, make_float2(ar - bi, ai + br)); st(29, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.9842305779457092f, ar); ai = fmaf(s1.y, -0.9842305779457092f, ai); br = fmaf(d1.x, 0.1768902689218521f, br); bi = fmaf(d1.y, 0.1768902689218521f, bi);
+      ar = fmaf(s2.x, 0.9374196529388428f, ar); ai = fmaf(s2.y, 0.9374196529388428f, ai); br = fmaf(d2.x, -0.3482016324996948f, br); bi = fmaf(d2.y, -0.3482016324996948f, bi);
+      ar = fmaf(s3.x, -0.8610436320304871f, ar); ai = fmaf(s3.y, -0.8610436320304871f, ai); br = fmaf(d3.x, 0.5085310935974121f, br); bi = fmaf(d3.y, 0.5085310935974121f, bi);
+      ar = fmaf(s4.x, 0.7575112581253052f, ar); ai = fmaf(s4.y, 0.7575112581253052f, ai); br = fmaf(d4.x, -0.6528221368789673f, br); bi = fmaf(d4.y, -0.6528221368789673f, bi);
+      ar = fmaf(s5.x, -0.6300878524780273f, ar); ai = fmaf(s5.y, -0.6300878524780273f, ai); br = fmaf(d5.x, 0.7765238881111145f, br); bi = fmaf(d5.y, 0.7765238881111145f, bi);
+      ar = fmaf(s6.x, 0.4827921986579895f, ar); ai = fmaf(s6.y, 0.4827921986579895f, ai); br = fmaf(d6.x, -0.8757349252700806f, br); bi = fmaf(d6.y, -0.8757349252700806f, bi);
+      ar = fmaf(s7.x, -0.3202698528766632f, ar); ai = fmaf(s7.y, -0.3202698528766632f, ai); br = fmaf(d7.x, 0.9473263621330261f, br); bi = fmaf(d7.y, 0.9473263621330261f, bi);
+      ar = fmaf(s8.x, 0.14764656126499176f, ar); ai = fmaf(s8.y, 0.14764656126499176f, ai); br = fmaf(d8.x, -0.989040195941925f, br); bi = fmaf(d8.y, -0.989040195941925f, bi);
+      ar = fmaf(s9.x, 0.029633328318595886f, ar); ai = fmaf(s9.y, 0.029633328318595886f, ai); br = fmaf(d9.x, 0.9995608329772949f, br); bi = fmaf(d9.y, 0.9995608329772949f, bi);
+      ar = fmaf(s10.x, -0.2059786170721054f, ar); ai = fmaf(s10.y, -0.2059786170721054f, ai); br = fmaf(d10.x, -0.9785565137863159f, br); bi = fmaf(d10.y, -0.9785565137863159f, bi);
+      ar = fmaf(s11.x, 0.3758275806903839f, ar); ai = fmaf(s11.y, 0.3758275806903839f, ai); br = fmaf(d11.x, 0.926689624786377f, br); bi = fmaf(d11.y, 0.926689624786377f, bi);
+      ar = fmaf(s12.x, -0.5338233709335327f, ar); ai = fmaf(s12.y, -0.5338233709335327f, ai); br = fmaf(d12.x, -0.8455960154533386f, br); bi = fmaf(d12.y, -0.8455960154533386f, bi);
+      ar = fmaf(s13.x, 0.674983024597168f, ar); ai = fmaf(s13.y, 0.674983024597168f, ai); br = fmaf(d13.x, 0.7378332614898682f, br); bi = fmaf(d13.y, 0.7378332614898682f, bi);
+      ar = fmaf(s14.x, -0.794854462146759f, ar); ai = fmaf(s14.y, -0.794854462146759f, ai); br = fmaf(d14.x, -0.6068001389503479f, br); bi = fmaf(d14.y, -0.6068001389503479f, bi);
+      ar = fmaf(s15.x, 0.8896570801734924f, ar); ai = fmaf(s15.y, 0.8896570801734924f, ai); br = fmaf(d15.x, 0.4566292464733124f, br); bi = fmaf(d15.y, 0.4566292464733124f, bi);
+      ar = fmaf(s16.x, -0.956400990486145f, ar); ai = fmaf(s16.y, -0.956400990486145f, ai); br = fmaf(d16.x, -0.29205676913261414f, br); bi = fmaf(d16.y, -0.29205676913261414f, bi);
+      ar = fmaf(s17.x, 0.9929810762405396f, ar); ai = fmaf(s17.y, 0.9929810762405396f, ai); br = fmaf(d17.x, 0.11827316880226135f, br); bi = fmaf(d17.y, 0.11827316880226135f, bi);
+      ar = fmaf(s18.x, -0.9982437491416931f, ar); ai = fmaf(s18.y, -0.9982437491416931f, ai); br = fmaf(d18.x, 0.05924062803387642f, br); bi = fmaf(d18.y, 0.05924062803387642f, bi);
+      ar = fmaf(s19.x, 0.9720228910446167f, ar); ai = fmaf(s19.y, 0.9720228910446167f, ai); br = fmaf(d19.x, -0.2348860502243042f, br); bi = fmaf(d19.y, -0.2348860502243042f, bi);
+      ar = fmaf(s20.x, -0.9151456356048584f, ar); ai = fmaf(s20.y, -0.9151456356048584f, ai); br = fmaf(d20.x, 0.4031234383583069f, br); bi = fmaf(d20.y, 0.4031234383583069f, bi);
+      ar = fmaf(s21.x, 0.829405665397644f, ar); ai = fmaf(s21.y, 0.829405665397644f, ai); br = fmaf(d21.x, -0.5586467385292053f, br); bi = fmaf(d21.y, -0.5586467385292053f, bi);
+      ar = fmaf(s22.x, -0.7175072431564331f, ar); ai = fmaf(s22.y, -0.7175072431564331f, ai); br = fmaf(d22.x, 0.6965510249137878f, br); bi = fmaf(d22.y, 0.6965510249137878f, bi);
+      ar = fmaf(s23.x, 0.5829795002937317f, ar); ai = fmaf(s23.y, 0.5829795002937317f, ai); br = fmaf(d23.x, -0.8124868869781494f, br); bi = fmaf(d23.y, -0.8124868869781494f, bi);
+      ar = fmaf(s24.x, -0.43006521463394165f, ar); ai = fmaf(s24.y, -0.43006521463394165f, ai); br = fmaf(d24.x, 0.9027978181838989f, br); bi = fmaf(d24.y, 0.9027978181838989f, bi);
+      ar = fmaf(s25.x, 0.26358717679977417f, ar); ai = fmaf(s25.y, 0.26358717679977417f, ai); br = fmaf(d25.x, -0.9646356105804443f, br); bi = fmaf(d25.y, -0.9646356105804443f, bi);
+      ar = fmaf(s26.x, -0.08879589289426804f, ar); ai = fmaf(s26.y, -0.08879589289426804f, ai); br = fmaf(d26.x, 0.9960498213768005f, br); bi = fmaf(d26.y, 0.9960498213768005f, bi);
+      if (!INV) { st(25, make_float2(ar + bi, ai - br)); st(28, make_float2(ar - bi, ai + br)); }
+      else { st(25, make_float2(ar - bi, ai + br)); st(28, make_float2(ar + bi, ai - br)); }
+    }
+    {
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      ar = fmaf(s1.x, -0.9982437491416931f, ar); ai = fmaf(s1.y, -0.9982437491416931f, ai); br = fmaf(d1.x, 0.05924062803387642f, br); bi = fmaf(d1.y, 0.05924062803387642f, bi);
+      ar = fmaf(s2.x, 0.9929810762405396f, ar); ai = fmaf(s2.y, 0.9929810762405396f, ai); br = fmaf(d2.x, -0.11827316880226135f, br); bi = fmaf(d2.y, -0.11827316880226135f, bi);
+      ar = fmaf(s3.x, -0.9842305779457092f, ar); ai = fmaf(s3.y, -0.9842305779457092f, ai); br = fmaf(d3.x, 0.1768902689218521f, br); bi = fmaf(d3.y, 0.1768902689218521f, bi);
+      ar = fmaf(s4.x, 0.9720228910446167f, ar); ai = fmaf(s4.y, 0.9720228910446167f, ai); br = fmaf(d4.x, -0.2348860502243042f, br); bi = fmaf(d4.y, -0.2348860502243042f, bi);
+      ar = fmaf(s5.x, -0.956400990486145f, ar); ai = fmaf(s5.y, -0.956400990486145f, ai); br = fmaf(d5.x, 0.29205676913261414f, br); bi = fmaf(d5.y, 0.29205676913261414f, bi);
+      ar = fmaf(s6.x, 0.9374196529388428f, ar); ai = fmaf(s6.y, 0.9374196529388428f, ai); br = fmaf(d6.x, -0.3482016324996948f, br); bi = fmaf(d6.y, -0.3482016324996948f, bi);
+      ar = fmaf(s7.x, -0.9151456356048584f, ar); ai = fmaf(s7.y, -0.9151456356048584f, ai); br = fmaf(d7.x, 0.4031234383583069f, br); bi = fmaf(d7.y, 0.4031234383583069f, bi);
+      ar = fmaf(s8.x, 0.8896570801734924f, ar); ai = fmaf(s8.y, 0.8896570801734924f, ai); br = fmaf(d8.x, -0.4566292464733124f, br); bi = fmaf(d8.y, -0.4566292464733124f, bi);
+      ar = fmaf(s9.x, -0.8610436320304871f, ar); ai = fmaf(s9.y, -0.8610436320304871f, ai); br = fmaf(d9.x, 0.5085310935974121f, br); bi = fmaf(d9.y, 0.5085310935974121f, bi);
+      ar = fmaf(s10.x, 0.829405665397644f, ar); ai = fmaf(s10.y, 0.829405665397644f, ai); br = fmaf(d10.x, -0.5586467385292053f, br); bi = fmaf(d10.y, -0.5586467385292053f, bi);
+      ar = fmaf(s11.x, -0.794854462146759f, ar); ai = fmaf(s11.y, -0.794854462146759f, ai); br = fmaf(d11.x, 0.6068001389503479f, br); bi = fmaf(d11.y, 0.6068001389503479f, bi);
+      ar = fmaf(s12.x, 0.7575112581253052f, ar); ai = fmaf(s12.y, 0.7575112581253052f, ai); br = fmaf(d12.x, -0.6528221368789673f, br); bi = fmaf(d12.y, -0.6528221368789673f, bi);
+      ar = fmaf(s13.x, -0.7175072431564331f, ar); ai = fmaf(s13.y, -0.7175072431564331f, ai); br = fmaf(d13.x, 0.6965510249137878f, br); bi = fmaf(d13.y, 0.6965510249137878f, bi);
+      ar = fmaf(s14.x, 0.674983024597168f, ar); ai = fmaf(s14.y, 0.674983024597168f, ai); br = fmaf(d14.x, -0.7378332614898682f, br); bi = fmaf(d14.y, -0.7378332614898682f, bi);
+      ar = fmaf(s15.x, -0.6300878524780273f, ar); ai = fmaf(s15.y, -0.6300878524780273f, ai); br = fmaf(d15.x, 0.7765238881111145f, br); bi = fmaf(d15.y, 0.7765238881111145f, bi);
+      ar = fmaf(s16.x, 0.5829795002937317f, ar); ai = fmaf(s16.y, 0.5829795002937317f, ai); br = fmaf(d16.x, -0.8124868869781494f, br); bi = fmaf(d16.y, -0.8124868869781494f, bi);
+      ar = fmaf(s17.x, -0.5338233709335327f, ar); ai = fmaf(s17.y, -0.5338233709335327f, ai); br = fmaf(d17.x, 0.8455960154533386f, br); bi = fmaf(d17.y, 0.8455960154533386f, bi);
+      ar = fmaf(s18.x, 0.4827921986579895f, ar); ai = fmaf(s18.y, 0.4827921986579895f, ai); br = fmaf(d18.x, -0.8757349252700806f, br); bi = fmaf(d18.y, -0.8757349252700806f, bi);
+      ar = fmaf(s19.x, -0.43006521463394165f, ar); ai = fmaf(s19.y, -0.43006521463394165f, ai); br = fmaf(d19.x, 0.9027978181838989f, br); bi = fmaf(d19.y, 0.9027978181838989f, bi);
+      ar = fmaf(s20.x, 0.3758275806903839f, ar); ai = fmaf(s20.y, 0.3758275806903839f, ai); br = fmaf(d20.x, -0.926689624786377f, br); bi = fmaf(d20.y, -0.926689624786377f, bi);
+      ar = fmaf(s21.x, -0.3202698528766632f, ar); ai = fmaf(s21.y, -0.3202698528766632f, ai); br = fmaf(d21.x, 0.9473263621330261f, br); bi = fmaf(d21.y, 0.9473263621330261f, bi);
+      ar = fmaf(s22.x, 0.26358717679977417f, ar); ai = fmaf(s22.y, 0.26358717679977417f, ai); br = fmaf(d22.x, -0.9646356105804443f, br); bi = fmaf(d22.y, -0.9646356105804443f, bi);
+      ar = fmaf(s23.x, -0.2059786170721054f, ar); ai = fmaf(s23.y, -0.2059786170721054f, ai); br = fmaf(d23.x, 0.9785565137863159f, br); bi = fmaf(d23.y, 0.9785565137863159f, bi);
+      ar = fmaf(s24.x, 0.14764656126499176f, ar); ai = fmaf(s24.y, 0.14764656126499176f, ai); br = fmaf(d24.x, -0.989040195941925f, br); bi = fmaf(d24.y, -0.989040195941925f, bi);
+      ar = fmaf(s25.x, -0.08879589289426804f, ar); ai = fmaf(s25.y, -0.08879589289426804f, ai); br = fmaf(d25.x, 0.9960498213768005f, br); bi = fmaf(d25.y, 0.9960498213768005f, bi);
+      ar = fmaf(s26.x, 0.029633328318595886f, ar); ai = fmaf(s26.y, 0.029633328318595886f, ai); br = fmaf(d26.x, -0.9995608329772949f, br); bi = fmaf(d26.y, -0.9995608329772949f, bi);
+      if (!INV) { st(26, make_float2(ar + bi, ai - br)); st(27, make_float2(ar - bi, ai + br)); }
+      else { st(26, make_float2(ar - bi, ai + br)); st(27, make_float2(ar + bi, ai - br)); }
+    }
+    break;
+  }
+  default: break;
+  }
+}
 }  // namespace mc

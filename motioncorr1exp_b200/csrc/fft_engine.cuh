@@ -170,6 +170,49 @@ __device__ __forceinline__ void stage_fixed(const float2* __restrict__ src, floa
   }
 }
 
+// Radix-53 stage with every butterfly spread over kSplit53 threads: each
+// thread loads the 53 inputs and produces its share of the outputs.  The
+// stage has only n/53 butterflies per transform, so this keeps the CTA busy.
+template <bool INV, bool INTERLEAVED>
+__device__ __forceinline__ void stage_r53_split(const float2* __restrict__ src, float2* __restrict__ dst,
+                                                const FftStage& s, int B, FastDiv bdiv, int ld,
+                                                const float2* __restrict__ tw, int tid, int nth) {
+  constexpr int R = 53;
+  const int nq = (int)s.nqdiv.d;
+  const int total = nq * B * kSplit53;
+  const FastDiv sdiv = make_fastdiv((uint32_t)kSplit53);
+  for (int t = tid; t < total; t += nth) {
+    uint32_t jb, part;
+    fdivmod((uint32_t)t, sdiv, jb, part);
+    uint32_t j, b;
+    if (INTERLEAVED) fdivmod(jb, bdiv, j, b);
+    else fdivmod(jb, s.nqdiv, b, j);
+    uint32_t jq, jm;
+    fdivmod(j, s.nsdiv, jq, jm);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = (int)j + r * nq;
+      v[r] = INTERLEAVED ? src[b + B * i] : src[b * ld + i];
+    }
+    if (s.Ns > 1) {
+      const int step = (int)jm * s.tws;
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        float2 w = tw[r * step];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    const int base = (int)jq * s.Ns * R + (int)jm;
+    dft_r53_part<INV>(v, (int)part, [&](int r, float2 x) {
+      const int i = base + r * s.Ns;
+      if (INTERLEAVED) dst[b + B * i] = x;
+      else dst[b * ld + i] = x;
+    });
+  }
+}
+
 // Runtime-radix fallback: every output of every butterfly as a direct sum,
 //   X_k = sum_r src[j + r*n/R] * W_n^(r*((j mod Ns)*tws + k*n/R)).
 template <bool INV, bool INTERLEAVED>
@@ -225,7 +268,7 @@ __device__ float2* fft_run(float2* a, float2* b, const FftPlan1D& p, int B, int 
       case 8: stage_fixed<8, INV, INTERLEAVED>(a, b, s, B, bdiv, ld, tw, tid, nth); break;
       case 11: stage_fixed<11, INV, INTERLEAVED>(a, b, s, B, bdiv, ld, tw, tid, nth); break;
       case 13: stage_fixed<13, INV, INTERLEAVED>(a, b, s, B, bdiv, ld, tw, tid, nth); break;
-      case 53: stage_fixed<53, INV, INTERLEAVED>(a, b, s, B, bdiv, ld, tw, tid, nth); break;
+      case 53: stage_r53_split<INV, INTERLEAVED>(a, b, s, B, bdiv, ld, tw, tid, nth); break;
       default: stage_generic<INV, INTERLEAVED>(a, b, s, p.n, B, bdiv, ld, tw, tid, nth); break;
     }
     __syncthreads();

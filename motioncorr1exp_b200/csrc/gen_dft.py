@@ -56,17 +56,151 @@ def emit_odd(R: int) -> str:
     return "\n".join(L)
 
 
+def emit_odd_split(R: int, S: int) -> str:
+    """Radix-R butterfly whose outputs are split over S threads: part p
+    computes X_0 (p == 0) and the pairs (X_k, X_{R-k}) of its k-range, and
+    hands each output to st(index, value)."""
+    h = (R - 1) // 2
+    bounds = [round(i * h / S) for i in range(S + 1)]
+    L = [f"template <bool INV, typename St>",
+         f"__device__ __forceinline__ void dft_r{R}_part(const float2* v, int part, St&& st) {{",
+         "  const float2 x0 = v[0];"]
+    for n in range(1, h + 1):
+        L.append(f"  const float2 s{n} = make_float2(v[{n}].x + v[{R-n}].x, v[{n}].y + v[{R-n}].y);")
+        L.append(f"  const float2 d{n} = make_float2(v[{n}].x - v[{R-n}].x, v[{n}].y - v[{R-n}].y);")
+    sx = " + ".join([f"s{n}.x" for n in range(1, h + 1)])
+    sy = " + ".join([f"s{n}.y" for n in range(1, h + 1)])
+    L.append(f"  if (part == 0) st(0, make_float2(x0.x + ({sx}), x0.y + ({sy})));")
+    L.append("  switch (part) {")
+    for p in range(S):
+        L.append(f"  case {p}: {{")
+        for k in range(bounds[p] + 1, bounds[p + 1] + 1):
+            L.append("    {")
+            L.append("      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;")
+            for n in range(1, h + 1):
+                m = (n * k) % R
+                c = flit(math.cos(2.0 * math.pi * m / R))
+                s = flit(math.sin(2.0 * math.pi * m / R))
+                L.append(f"      ar = fmaf(s{n}.x, {c}, ar); ai = fmaf(s{n}.y, {c}, ai);"
+                         f" br = fmaf(d{n}.x, {s}, br); bi = fmaf(d{n}.y, {s}, bi);")
+            L.append(f"      if (!INV) {{ st({k}, make_float2(ar + bi, ai - br)); st({R-k}, make_float2(ar - bi, ai + br)); }}")
+            L.append(f"      else {{ st({k}, make_float2(ar - bi, ai + br)); st({R-k}, make_float2(ar + bi, ai - br)); }}")
+            L.append("    }")
+        L.append("    break;")
+        L.append("  }")
+    L.append("  default: break;")
+    L.append("  }")
+    L.append("}")
+    return "\n".join(L)
+
+
+def factor_codelet(q: int) -> list:
+    """Radix order used for register codelets: odd radices first, then 8/4/2."""
+    rad, m = [], q
+    for p in (7, 5, 3):
+        while m % p == 0:
+            rad.append(p)
+            m //= p
+    twos = 0
+    while m % 2 == 0:
+        twos += 1
+        m //= 2
+    if m != 1:
+        raise ValueError(f"{q} has a factor outside 2,3,5,7")
+    pw = []
+    while twos >= 3:
+        if twos == 4:
+            pw += [4, 4]
+            twos = 0
+            break
+        pw.append(8)
+        twos -= 3
+    if twos == 2:
+        pw.append(4)
+    if twos == 1:
+        pw.append(2)
+    return rad + pw
+
+
+def emit_codelet(q: int) -> str:
+    """In-register Stockham FFT of length q with every index and twiddle
+    resolved at generation time: fft_reg_q<INV>(float2 a[q]), result in a."""
+    radices = factor_codelet(q)
+    L = [f"template <bool INV> __device__ __forceinline__ void fft_reg_{q}(float2* a) {{",
+         f"  float2 b[{q}];"]
+    ns, src, dst = 1, "a", "b"
+    for R in radices:
+        nq = q // R
+        for j in range(nq):
+            jm, jq = j % ns, j // ns
+            L.append("  {")
+            L.append(f"    float2 x[{R}];")
+            for r in range(R):
+                L.append(f"    x[{r}] = {src}[{j + r * nq}];")
+            if ns > 1:
+                for r in range(1, R):
+                    e = (r * jm * (q // (ns * R))) % q
+                    if e == 0:
+                        continue
+                    if 4 * e == q:
+                        L.append(f"    x[{r}] = rot90<INV>(x[{r}]);")
+                        continue
+                    if 2 * e == q:
+                        L.append(f"    x[{r}] = make_float2(-x[{r}].x, -x[{r}].y);")
+                        continue
+                    if 4 * e == 3 * q:
+                        L.append(f"    x[{r}] = rot90<!INV>(x[{r}]);")
+                        continue
+                    c = flit(math.cos(2.0 * math.pi * e / q))
+                    s = flit(-math.sin(2.0 * math.pi * e / q))
+                    L.append(f"    x[{r}] = cmul(x[{r}], make_float2({c}, INV ? -({s}) : ({s})));")
+            L.append(f"    dft_any<{R}, INV>(x);")
+            base = jq * ns * R + jm
+            for r in range(R):
+                L.append(f"    {dst}[{base + r * ns}] = x[{r}];")
+            L.append("  }")
+        src, dst = dst, src
+        ns *= R
+    if src != "a":
+        L.append(f"#pragma unroll\n  for (int i = 0; i < {q}; i++) a[i] = b[i];")
+    L.append("}")
+    return "\n".join(L)
+
+
+CODELETS = [4, 8, 10, 12, 14, 16, 20, 24, 28, 30, 32, 35, 40, 48, 56, 60, 64, 70]
+SPLIT53 = 3
+
+
 def main() -> None:
+    which = sys.argv[1] if len(sys.argv) > 1 else "dft"
     out = []
     out.append("// Generated by gen_dft.py -- do not edit by hand.")
-    out.append("// Straight-line odd-radix DFT butterflies (symmetric direct form).")
-    out.append("#pragma once")
-    out.append("#include <cuda_runtime.h>")
-    out.append("namespace mc {")
-    out.append(f"constexpr int kGeneratedOddRadices[] = {{{', '.join(map(str, ODD_RADICES))}}};")
-    for R in ODD_RADICES:
-        out.append(emit_odd(R))
-    out.append("}  // namespace mc")
+    if which == "dft":
+        out.append("// Straight-line odd-radix DFT butterflies (symmetric direct form).")
+        out.append("#pragma once")
+        out.append("#include <cuda_runtime.h>")
+        out.append("namespace mc {")
+        out.append(f"constexpr int kGeneratedOddRadices[] = {{{', '.join(map(str, ODD_RADICES))}}};")
+        for R in ODD_RADICES:
+            out.append(emit_odd(R))
+        out.append(f"constexpr int kSplit53 = {SPLIT53};")
+        out.append(emit_odd_split(53, SPLIT53))
+        out.append("}  // namespace mc")
+    else:
+        out.append("// Register-resident FFT codelets (lengths with factors 2, 3, 5, 7).")
+        out.append("#pragma once")
+        out.append('#include "fft_engine.cuh"')
+        out.append("namespace mc {")
+        out.append(f"constexpr int kCodelets[] = {{{', '.join(map(str, CODELETS))}}};")
+        out.append(f"constexpr int kNumCodelets = {len(CODELETS)};")
+        for q in CODELETS:
+            out.append(emit_codelet(q))
+        out.append("template <int Q, bool INV> __device__ __forceinline__ void fft_reg(float2* a) {")
+        for i, q in enumerate(CODELETS):
+            kw = "if" if i == 0 else "else if"
+            out.append(f"  {kw} constexpr (Q == {q}) fft_reg_{q}<INV>(a);")
+        out.append("}")
+        out.append("}  // namespace mc")
     sys.stdout.write("\n".join(out) + "\n")
 
 

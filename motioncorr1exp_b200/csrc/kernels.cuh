@@ -140,6 +140,10 @@ cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 
+// true when the register-codelet column stage handles the split n = P*Q
+bool pair_cols_reg_supported(int P, int Q);
+size_t pair_cols_reg_smem(int n, int team);
+
 size_t fwd_rows_smem(int nu);
 size_t rows_fft_smem(int n, int rows_per_cta);
 size_t pair_cols_smem(int n, int P, int Q, int box);

@@ -11,6 +11,7 @@
 #include <math.h>
 #include <stdint.h>
 #include "kernels.cuh"
+#include "codelets_gen.cuh"
 
 namespace mc {
 
@@ -97,7 +98,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_rows(FwdRowsArgs a) {
 
 size_t fwd_rows_smem(int nu) { return (size_t)3 * nu * sizeof(float2); }
 
+bool two_level_split(int n, int& n1, int& n2);
+cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st);
+cudaError_t launch_rows_fft2l(const RowsFftArgs& a, bool inverse, cudaStream_t st);
+
 cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st) {
+  int n1, n2;
+  if (two_level_split(a.nu, n1, n2)) return launch_fwd_rows2l(a, st);
   const size_t smem = fwd_rows_smem(a.nu);
   cudaError_t e = cudaFuncSetAttribute(k_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -139,6 +146,8 @@ size_t rows_fft_smem(int n, int rows_per_cta) {
 }
 
 cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st) {
+  int n1, n2;
+  if (two_level_split(a.plan.n, n1, n2)) return launch_rows_fft2l(a, inverse, st);
   const size_t smem = rows_fft_smem(a.plan.n, rows_per_cta);
   const int grid = (a.nrows + rows_per_cta - 1) / rows_per_cta;
   cudaError_t e;
@@ -152,6 +161,179 @@ cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta
     k_rows_fft<false><<<grid, kThreads, smem, st>>>(a, rows_per_cta);
   }
   return cudaGetLastError();
+}
+
+// ================================================== two-level transforms ==
+// Length N = N1*N2 with n = n1 + N1*n2 and k = k2 + N2*k1:
+//   Y[n1][k2]      = W_N^(n1 k2) * sum_n2 x[n1 + N1 n2] W_N2^(n2 k2)   thread n1: N2-point codelet
+//   X[k2 + N2 k1]  = sum_n1 Y[n1][k2] W_N1^(n1 k1)                    thread k2: N1-point codelet
+// so a whole transform costs one shared-memory exchange.  N1 = 53 uses the
+// generated radix-53 butterfly.  One CTA (a team of `T2L` threads) per
+// transform; W_N comes from the global twiddle table through the L1.
+template <int N1, bool INV>
+__device__ __forceinline__ void fft_n1(float2* v) {
+  if constexpr (N1 == 53) dft_r53<INV>(v);
+  else fft_reg<N1, INV>(v);
+}
+
+template <int N1, int N2>
+struct TwoLevel {
+  static constexpr int N = N1 * N2;
+  static constexpr int T = ((N1 > N2 ? N1 : N2) + 31) / 32 * 32;
+
+  // step A + exchange + step B; load(i) gives x[i], store(k, X[k]) takes the
+  // result.  T >= N2, so each thread owns at most one k2 in step B; with
+  // SYNC_STORE the stores wait for every thread's step-B reads, which lets
+  // store() write back into ysm.
+  template <bool INV, bool SYNC_STORE, class Load, class Store>
+  __device__ static void run(float2* ysm, const float2* __restrict__ tw, Load&& load, Store&& store) {
+    static_assert(T >= N2, "one k2 per thread");
+    const int lt = threadIdx.x;
+    if (lt < N1) {
+      float2 x[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) x[n2] = load(lt + N1 * n2);
+      fft_reg<N2, INV>(x);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) {
+        float2 w = __ldg(tw + lt * k2);
+        if (INV) w.y = -w.y;
+        ysm[k2 * N1 + lt] = k2 ? cmul(x[k2], w) : x[k2];
+      }
+    }
+    __syncthreads();
+    const bool act = lt < N2;
+    float2 v[N1];
+    if (act) {
+#pragma unroll
+      for (int n1 = 0; n1 < N1; n1++) v[n1] = ysm[lt * N1 + n1];
+      fft_n1<N1, INV>(v);
+    }
+    if (SYNC_STORE) __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) store(lt + N2 * k1, v[k1]);
+    }
+  }
+};
+
+// Batched rows: out_row[i] = scale * X[i < keep_lo ? i : i + (n - n_out)].
+template <int N1, int N2, bool INV>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_rows_fft2l(RowsFftArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  __shared__ float2 ysm[TL::N];
+  const long long row = blockIdx.x;
+  const float2* in = a.in + row * a.ld_in;
+  float2* out = a.out + row * a.ld_out;
+  const int shift = TL::N - a.n_out, keep = a.keep_lo;
+  const float sc = a.scale;
+  TL::template run<INV, false>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
+                        [&](int k, float2 v) {
+                          int o;
+                          if (k < keep) o = k;
+                          else if (k >= keep + shift) o = k - shift;
+                          else return;
+                          out[o] = make_float2(v.x * sc, v.y * sc);
+                        });
+}
+
+// Forward rows: two image rows (or the two reference sets of one row) packed
+// as one complex transform, then split into the two real half spectra.
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_fwd_rows2l(FwdRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  __shared__ float2 ysm[N];
+  float2* zsm = ysm;  // the spectrum Z reuses the exchange buffer
+  int y0, y1;
+  if (a.two_outputs) {
+    y0 = blockIdx.x;
+    y1 = y0;
+  } else {
+    y0 = 2 * blockIdx.x;
+    y1 = y0 + 1;
+  }
+  const bool hasd = a.dark != nullptr, hasn = a.norm != nullptr;
+  const long long r0 = (long long)(a.offy + y0) * a.nx + a.offx;
+  const long long r1 = (long long)(a.offy + y1) * a.nx + a.offx;
+  TL::template run<false, true>(
+      ysm, a.tw,
+      [&](int x) {
+        if (a.two_outputs) {
+          const long long i0 = r0 + x;
+          const float raw = load_pixel(a.frame, a.mode, i0);
+          const float d1 = hasd ? a.dark[i0] : 0.f;
+          const float d2 = hasd ? (a.dark2 ? a.dark2[i0] : 0.f) : 0.f;
+          const float g1 = hasn ? a.norm[i0] : 1.f;
+          const float g2 = hasn ? (a.norm2 ? a.norm2[i0] : 1.f) : 1.f;
+          return make_float2((raw - d1) * g1, (raw - d2) * g2);
+        }
+        float re = load_pixel(a.frame, a.mode, r0 + x);
+        float im = load_pixel(a.frame, a.mode, r1 + x);
+        if (hasd || hasn) {
+          const long long i0 = r0 + x, i1 = r1 + x;
+          re = (re - (hasd ? a.dark[i0] : 0.f)) * (hasn ? a.norm[i0] : 1.f);
+          im = (im - (hasd ? a.dark[i1] : 0.f)) * (hasn ? a.norm[i1] : 1.f);
+        }
+        return make_float2(re, im);
+      },
+      [&](int k, float2 v) { zsm[k] = v; });
+  __syncthreads();
+  for (int k = threadIdx.x; k < a.hk; k += TL::T) {
+    const float2 z = zsm[k];
+    const float2 zc = zsm[k == 0 ? 0 : N - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    if (a.two_outputs) {
+      a.outA[(long long)k * a.ldt + y0] = X;
+      a.outB[(long long)k * a.ldt + y0] = Y;
+    } else {
+      *reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0) = make_float4(X.x, X.y, Y.x, Y.y);
+    }
+  }
+}
+
+// Two-level splits compiled in (N1, N2).
+#define MC_TWO_LEVEL_LIST(X) X(53, 70) X(64, 64) X(32, 64) X(32, 32) X(16, 16) X(16, 32)
+
+bool two_level_split(int n, int& n1, int& n2) {
+#define MC_TL_MATCH(A, B)      \
+  if (n == (A) * (B)) {        \
+    n1 = (A);                  \
+    n2 = (B);                  \
+    return true;               \
+  }
+  MC_TWO_LEVEL_LIST(MC_TL_MATCH)
+#undef MC_TL_MATCH
+  return false;
+}
+
+cudaError_t launch_rows_fft2l(const RowsFftArgs& a, bool inverse, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (!two_level_split(a.plan.n, n1, n2)) return cudaErrorInvalidValue;
+#define MC_TL_LAUNCH(A, B)                                                                   \
+  if (n1 == (A) && n2 == (B)) {                                                              \
+    if (inverse) k_rows_fft2l<A, B, true><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);         \
+    else k_rows_fft2l<A, B, false><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);                \
+    return cudaGetLastError();                                                               \
+  }
+  MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)
+#undef MC_TL_LAUNCH
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (!two_level_split(a.nu, n1, n2)) return cudaErrorInvalidValue;
+  const int grid = a.two_outputs ? a.nu : a.nu / 2;
+#define MC_TL_LAUNCH(A, B)                                            \
+  if (n1 == (A) && n2 == (B)) {                                       \
+    k_fwd_rows2l<A, B><<<grid, TwoLevel<A, B>::T, 0, st>>>(a);        \
+    return cudaGetLastError();                                        \
+  }
+  MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)
+#undef MC_TL_LAUNCH
+  return cudaErrorInvalidValue;
 }
 
 // ============================================================ pair columns ==
@@ -219,11 +401,119 @@ __global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
   }
 }
 
+// Register-codelet variant of the column stage (P <= 128, Q a codelet length).
+// A CTA of 128 threads owns one column kx; it is split into teams of `team`
+// threads (team = P rounded up to a warp multiple) and each team takes whole
+// pairs.  Thread k1 < P of a team gathers its stride-P subsequence
+// c(k1 + P*k2), k2 < Q, straight from the two spectra (coalesced over k1),
+// runs the Q-point inverse FFT in registers, and parks the result in shared
+// memory; the team then forms the pbx output rows as P-term sums.
+constexpr int kRegThreads = 128;
+
+__device__ __forceinline__ void team_barrier(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+size_t pair_cols_reg_smem(int n, int team) {
+  const int teams = kRegThreads / team;
+  return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)teams * n * sizeof(float2);
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kRegThreads) k_pair_cols_reg(PairColsArgs a, int team) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, P = a.P, box = a.box;
+  float* wcol = reinterpret_cast<float*>(sm);
+  const int teams = kRegThreads / team;
+  const int tid = threadIdx.x;
+  const int tm = tid / team, lt = tid - tm * team;
+  float2* Y = sm + (n + 1) / 2 + (size_t)tm * n;
+  const int kx = blockIdx.y;
+  const int half = n / 2;
+  for (int ky = tid; ky < n; ky += kRegThreads) {
+    const int y = ky < half ? ky : ky - n;
+    wcol[ky] = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+  }
+  __syncthreads();
+  const int p0 = blockIdx.x * a.pairs_per_cta;
+  const int p1 = min(p0 + a.pairs_per_cta, a.npairs);
+  const int khalf = (P + 1) / 2;
+  for (int p = p0 + tm; p < p1; p += teams) {
+    const int2 pr = a.pairs[p];
+    const float2* ca = a.specA + (long long)pr.x * a.strideA + (long long)kx * a.ldn;
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    if (lt < P) {
+      float2 x[Q];
+#pragma unroll
+      for (int k2 = 0; k2 < Q; k2++) {
+        const int ky = lt + P * k2;
+        x[k2] = cscale(cmulc(__ldg(ca + ky), __ldg(cb + ky)), wcol[ky]);
+      }
+      fft_reg<Q, true>(x);
+#pragma unroll
+      for (int r = 0; r < Q; r++) Y[lt + P * r] = x[r];
+    }
+    team_barrier(1 + tm, team);
+    for (int base = 0; base < 2 * box; base += team) {
+      const int o = base + lt;
+      const bool ok = o < 2 * box;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = Y + P * r;
+        const float2* tw = a.twO + m;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = __ldg(tw + k * box);
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    team_barrier(1 + tm, team);
+  }
+}
+
+bool pair_cols_reg_supported(int P, int Q) {
+  if (P < 1 || P > kRegThreads) return false;
+  for (int q : kCodelets)
+    if (q == Q) return true;
+  return false;
+}
+
+template <int Q>
+cudaError_t launch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_pair_cols_reg<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_pair_cols_reg<Q><<<grid, kRegThreads, smem, st>>>(a, team);
+  return cudaGetLastError();
+}
+
+template <int I = 0>
+cudaError_t dispatch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid, cudaStream_t st) {
+  if constexpr (I < kNumCodelets) {
+    constexpr int Q = kCodelets[I];
+    if (a.Q == Q) return launch_reg<Q>(a, team, smem, grid, st);
+    return dispatch_reg<I + 1>(a, team, smem, grid, st);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
+  dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
+  if (pair_cols_reg_supported(a.P, a.Q)) {
+    const int team = a.P <= 32 ? 32 : (a.P <= 64 ? 64 : 128);
+    return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);
+  }
   const size_t smem = pair_cols_smem(a.n, a.P, a.Q, a.box) + 16;
   cudaError_t e = cudaFuncSetAttribute(k_pair_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
   k_pair_cols<<<grid, kThreads, smem, st>>>(a);
   return cudaGetLastError();
 }

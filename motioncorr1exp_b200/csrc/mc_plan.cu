@@ -145,7 +145,24 @@ double radix_cost(int r) {
 
 // n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
 void choose_prune(int n, int box, int& P, int& Q) {
+  // first choice: a split the register-codelet kernel handles
   double best = 1e300;
+  P = 0;
+  Q = 0;
+  for (int q = 2; q <= n; q++) {
+    if (n % q || !mc::pair_cols_reg_supported(n / q, q)) continue;
+    std::vector<int> rad = factor_radices(q);
+    double c = 0.0;
+    for (size_t s = 0; s < rad.size(); s++) c += radix_cost(rad[s]) + (s ? 2.0 : 0.0);
+    const double cost = (double)n * c + 4.0 * box * (n / q);
+    if (cost < best) {
+      best = cost;
+      P = n / q;
+      Q = q;
+    }
+  }
+  if (P) return;
+  // otherwise the shared-memory kernel
   P = n;
   Q = 1;
   for (int q = 1; q <= n; q++) {
@@ -402,6 +419,8 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
     a.G = pl->d_G;
     // algorithmic bytes: every distinct spectrum the batch touches read once,
     // the column-stage output written once
+    // (a shared spectrum set counts once: A and B are the same buffers)
+    const bool one_set = specA == specB && strideA == strideB;
     std::vector<char> seenA(pl->nframe + 1, 0), seenB(pl->nframe + 1, 0);
     long long nspec = 0;
     for (int i = p0; i < p0 + nb; i++) {
@@ -410,9 +429,9 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
         seenA[fa] = 1;
         nspec++;
       }
-      const bool same = (specA == specB && strideA == strideB && fa == fb);
-      if (!seenB[fb] && !(same && seenA[fb])) {
-        seenB[fb] = 1;
+      char& sb = one_set ? seenA[fb] : seenB[fb];
+      if (!sb) {
+        sb = 1;
         nspec++;
       }
     }
@@ -604,8 +623,12 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
     return set_err(MC_E_SIZE, "no FFT plan for %d / %d", pl->nu, pl->n);
   choose_prune(pl->n, pl->box, pl->P, pl->Q);
   if (!make_plan(pl->Q, pl->plan_q)) return set_err(MC_E_SIZE, "no FFT plan for Q=%d", pl->Q);
-  if (mc::pair_cols_smem(pl->n, pl->P, pl->Q, pl->box) + 16 > 227 * 1024)
-    return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
+  {
+    const bool reg = mc::pair_cols_reg_supported(pl->P, pl->Q);
+    const int team = pl->P <= 32 ? 32 : (pl->P <= 64 ? 64 : 128);
+    const size_t need = reg ? mc::pair_cols_reg_smem(pl->n, team) : mc::pair_cols_smem(pl->n, pl->P, pl->Q, pl->box) + 16;
+    if (need > 227 * 1024) return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
+  }
 
   CK(cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking));
   for (auto& e : pl->ev) CK(cudaEventCreate(&e));

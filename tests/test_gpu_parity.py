@@ -127,7 +127,8 @@ def test_forward_matches_oracle(gpu, nx, ny, mode, offx, offy, crd, bin_):
         frames = rng.integers(0, 60000, (nz, ny, nx)).astype(np.uint16)
     else:
         frames = rng.normal(5, 2, (nz, ny, nx)).astype(np.float32)
-    p = api.verify_params(api.Params(crop_offsetx=offx, crop_offsety=offy, crop_nsam=crd, bin=bin_), nz)
+    p = api.verify_params(api.Params(crop_offsetx=offx, crop_offsety=offy, crop_nsam=crd, bin=bin_,
+                                      FrameDistOffset=0), nz)
     with api.Plan(p, nx, ny, nz, mode) as pl:
         pl.load_frames(frames)
         pl.forward()
@@ -153,7 +154,7 @@ def test_refs_two_spectrum_sets(gpu, two_frame_refs, bin_):
     if two_frame_refs:
         refs["dark2"] = rng.normal(1, 0.1, (ny, nx)).astype(np.float32)
         refs["norm2"] = rng.normal(1, 0.05, (ny, nx)).astype(np.float32)
-    p = api.verify_params(api.Params(bin=bin_), nz)
+    p = api.verify_params(api.Params(bin=bin_, FrameDistOffset=0), nz)
     with api.Plan(p, nx, ny, nz, 0) as pl:
         pl.set_refs(**refs)
         pl.load_frames(frames)
