@@ -128,6 +128,13 @@ int mc_plan_iterate(mc_plan* plan);         /* DFAlign.cu:950-1092 */
 int mc_plan_sum(mc_plan* plan, float* image_host); /* DFAlign.cu:1114-1292; image n*n or NULL */
 /* All stages in order. */
 int mc_plan_run(mc_plan* plan, float* image_host);
+/* All stages in order on frames in host memory (all positions, file pixel
+ * type): the upload runs in chunks on a second stream and overlaps the
+ * forward transforms of the chunks already resident (pinned memory for the
+ * overlap; pageable works but serialises).  Replaces the per-frame
+ * read/GPUMemH2D/GPUFFT2d sequence of DFAlign.cu:710-820 plus the rest of
+ * the path. */
+int mc_plan_run_host(mc_plan* plan, const void* frames, float* image_host);
 
 /* Results. */
 int mc_plan_get_frame_shifts(const mc_plan* plan, double* xy);           /* 2*nframe, "Shift of Frame" */

@@ -66,6 +66,7 @@ SIGNATURES = {
     "mc_plan_iterate": (C.c_int, [C.c_void_p]),
     "mc_plan_sum": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mc_plan_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mc_plan_run_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mc_plan_get_frame_shifts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mc_plan_get_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mc_plan_get_ki": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),

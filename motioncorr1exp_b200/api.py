@@ -180,6 +180,16 @@ class Plan:
         L.check(self._lib.mc_plan_run(self._h, _ptr(img) if img is not None else None))
         return img
 
+    def run_host(self, frames: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Whole path from host frames (all positions) with the upload
+        overlapped with the forward transforms (mc_plan_run_host)."""
+        a = np.ascontiguousarray(frames)
+        if a.dtype.itemsize != _WORD_LENGTH[self.info["mode"]] or a.shape[0] != self.nframe:
+            raise ValueError("frames must hold every position in the plan's pixel type")
+        img = out if out is not None else np.empty((self.nsam, self.nsam), dtype=np.float32)
+        L.check(self._lib.mc_plan_run_host(self._h, _ptr(a), _ptr(img)))
+        return img
+
     # -- results
     def frame_shifts(self) -> np.ndarray:
         xy = np.empty((self.nframe, 2), dtype=np.float64)

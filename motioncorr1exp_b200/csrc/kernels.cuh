@@ -143,6 +143,10 @@ cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 // true when the register-codelet column stage handles the split n = P*Q
 bool pair_cols_reg_supported(int P, int Q);
 size_t pair_cols_reg_smem(int n, int team);
+// grouped column stage: groups[g] = (first pair, count) of pairs sharing A
+size_t pair_cols_grp_smem(int n, int teams);
+cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,
+                                     cudaStream_t st);
 
 size_t fwd_rows_smem(int nu);
 size_t rows_fft_smem(int n, int rows_per_cta);

@@ -239,12 +239,45 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_rows_fft2l(RowsFftArgs 
 
 // Forward rows: two image rows (or the two reference sets of one row) packed
 // as one complex transform, then split into the two real half spectra.
+// Stage the two packed input rows of k_fwd_rows2l in shared memory: every
+// thread of the CTA issues independent typed loads of the raw pixels.
+template <typename Px>
+__device__ __forceinline__ void stage_rows(float2* xin, const FwdRowsArgs& a, long long r0, long long r1, int n,
+                                           int nth) {
+  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const bool hasd = a.dark != nullptr, hasn = a.norm != nullptr;
+  if (a.two_outputs) {
+#pragma unroll 4
+    for (int x = threadIdx.x; x < n; x += nth) {
+      const long long i0 = r0 + x;
+      const float raw = (float)f[i0];
+      const float d1 = hasd ? a.dark[i0] : 0.f;
+      const float d2 = hasd ? (a.dark2 ? a.dark2[i0] : 0.f) : 0.f;
+      const float g1 = hasn ? a.norm[i0] : 1.f;
+      const float g2 = hasn ? (a.norm2 ? a.norm2[i0] : 1.f) : 1.f;
+      xin[x] = make_float2((raw - d1) * g1, (raw - d2) * g2);  // hbuf, hbuf2 (DFAlign.cu:724-725)
+    }
+  } else if (hasd || hasn) {
+#pragma unroll 4
+    for (int x = threadIdx.x; x < n; x += nth) {
+      const long long i0 = r0 + x, i1 = r1 + x;
+      const float re = ((float)f[i0] - (hasd ? a.dark[i0] : 0.f)) * (hasn ? a.norm[i0] : 1.f);
+      const float im = ((float)f[i1] - (hasd ? a.dark[i1] : 0.f)) * (hasn ? a.norm[i1] : 1.f);
+      xin[x] = make_float2(re, im);
+    }
+  } else {
+#pragma unroll 8
+    for (int x = threadIdx.x; x < n; x += nth) xin[x] = make_float2((float)f[r0 + x], (float)f[r1 + x]);
+  }
+}
+
 template <int N1, int N2>
 __global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_fwd_rows2l(FwdRowsArgs a) {
   using TL = TwoLevel<N1, N2>;
   constexpr int N = TL::N;
-  __shared__ float2 ysm[N];
-  float2* zsm = ysm;  // the spectrum Z reuses the exchange buffer
+  extern __shared__ float2 dyn2l[];
+  float2* xin = dyn2l;      // packed input rows, later the spectrum Z
+  float2* ysm = dyn2l + N;  // exchange buffer
   int y0, y1;
   if (a.two_outputs) {
     y0 = blockIdx.x;
@@ -253,31 +286,18 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_fwd_rows2l(FwdRowsArgs 
     y0 = 2 * blockIdx.x;
     y1 = y0 + 1;
   }
-  const bool hasd = a.dark != nullptr, hasn = a.norm != nullptr;
   const long long r0 = (long long)(a.offy + y0) * a.nx + a.offx;
   const long long r1 = (long long)(a.offy + y1) * a.nx + a.offx;
+  switch (a.mode) {
+    case 0: stage_rows<int8_t>(xin, a, r0, r1, N, TL::T); break;
+    case 1: stage_rows<int16_t>(xin, a, r0, r1, N, TL::T); break;
+    case 6: stage_rows<uint16_t>(xin, a, r0, r1, N, TL::T); break;
+    default: stage_rows<float>(xin, a, r0, r1, N, TL::T); break;
+  }
+  __syncthreads();
+  float2* zsm = xin;  // step B stores land after every step-A read of xin
   TL::template run<false, true>(
-      ysm, a.tw,
-      [&](int x) {
-        if (a.two_outputs) {
-          const long long i0 = r0 + x;
-          const float raw = load_pixel(a.frame, a.mode, i0);
-          const float d1 = hasd ? a.dark[i0] : 0.f;
-          const float d2 = hasd ? (a.dark2 ? a.dark2[i0] : 0.f) : 0.f;
-          const float g1 = hasn ? a.norm[i0] : 1.f;
-          const float g2 = hasn ? (a.norm2 ? a.norm2[i0] : 1.f) : 1.f;
-          return make_float2((raw - d1) * g1, (raw - d2) * g2);
-        }
-        float re = load_pixel(a.frame, a.mode, r0 + x);
-        float im = load_pixel(a.frame, a.mode, r1 + x);
-        if (hasd || hasn) {
-          const long long i0 = r0 + x, i1 = r1 + x;
-          re = (re - (hasd ? a.dark[i0] : 0.f)) * (hasn ? a.norm[i0] : 1.f);
-          im = (im - (hasd ? a.dark[i1] : 0.f)) * (hasn ? a.norm[i1] : 1.f);
-        }
-        return make_float2(re, im);
-      },
-      [&](int k, float2 v) { zsm[k] = v; });
+      ysm, a.tw, [&](int x) { return xin[x]; }, [&](int k, float2 v) { zsm[k] = v; });
   __syncthreads();
   for (int k = threadIdx.x; k < a.hk; k += TL::T) {
     const float2 z = zsm[k];
@@ -326,10 +346,14 @@ cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
   int n1 = 0, n2 = 0;
   if (!two_level_split(a.nu, n1, n2)) return cudaErrorInvalidValue;
   const int grid = a.two_outputs ? a.nu : a.nu / 2;
-#define MC_TL_LAUNCH(A, B)                                            \
-  if (n1 == (A) && n2 == (B)) {                                       \
-    k_fwd_rows2l<A, B><<<grid, TwoLevel<A, B>::T, 0, st>>>(a);        \
-    return cudaGetLastError();                                        \
+#define MC_TL_LAUNCH(A, B)                                                                           \
+  if (n1 == (A) && n2 == (B)) {                                                                      \
+    const size_t smem = (size_t)2 * (A) * (B) * sizeof(float2);                                      \
+    cudaError_t e = cudaFuncSetAttribute(k_fwd_rows2l<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)smem);                                                 \
+    if (e != cudaSuccess) return e;                                                                  \
+    k_fwd_rows2l<A, B><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                                    \
+    return cudaGetLastError();                                                                       \
   }
   MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)
 #undef MC_TL_LAUNCH
@@ -477,6 +501,129 @@ __global__ void __launch_bounds__(kRegThreads) k_pair_cols_reg(PairColsArgs a, i
     }
     team_barrier(1 + tm, team);
   }
+}
+
+// ---- grouped variant: one CTA per (A frame group, column kx) -------------
+// The pairs of a batch come in groups that share their A spectrum (the
+// reference's i-major order).  The CTA stages A(kx,:) x B-factor once in
+// shared memory; each team double-buffers the B columns of its pairs with
+// 16-byte cp.async copies, so the copy of pair p+1 overlaps the transform of
+// pair p.  Thread k1 reads only positions k1 + P*k2 of the B buffer and
+// writes Y back to the same positions, so Y lives in the consumed buffer.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+size_t pair_cols_grp_smem(int n, int teams) { return (size_t)(1 + 2 * teams) * n * sizeof(float2); }
+
+template <int Q>
+__global__ void __launch_bounds__(kRegThreads) k_pair_cols_grp(PairColsArgs a, const int2* __restrict__ groups,
+                                                               int team) {
+  extern __shared__ float2 smg[];
+  const int n = a.n, P = a.P, box = a.box;
+  const int teams = kRegThreads / team;
+  const int tid = threadIdx.x;
+  const int tm = tid / team, lt = tid - tm * team;
+  float2* aw = smg;
+  float2* buf0 = smg + n + (size_t)2 * tm * n;
+  const int kx = blockIdx.y;
+  const int2 g = groups[blockIdx.x];  // (first pair, count)
+  const int half = n / 2;
+  const int2 pr0 = a.pairs[g.x];
+  const float2* ca = a.specA + (long long)pr0.x * a.strideA + (long long)kx * a.ldn;
+  for (int ky = tid; ky < n; ky += kRegThreads) {
+    const int y = ky < half ? ky : ky - n;
+    const float w = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+    aw[ky] = cscale(__ldg(ca + ky), w);
+  }
+  const int nchunk = n / 2;  // 16-byte chunks of a column (n is even)
+  auto fetch = [&](int q, float2* dst) {
+    const int2 pr = a.pairs[g.x + q];
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    for (int c = lt; c < nchunk; c += team) cp_async16(dst + 2 * c, cb + 2 * c);
+  };
+  int cur = 0;
+  if (tm < g.y) fetch(tm, buf0);
+  cp_async_commit();
+  __syncthreads();  // aw visible to every team
+  const int khalf = (P + 1) / 2;
+  for (int q = tm; q < g.y; q += teams) {
+    float2* bc = buf0 + (size_t)cur * n;
+    if (q + teams < g.y) fetch(q + teams, buf0 + (size_t)(cur ^ 1) * n);
+    cp_async_commit();
+    cp_async_wait<1>();
+    team_barrier(1 + tm, team);
+    if (lt < P) {
+      float2 x[Q];
+#pragma unroll
+      for (int k2 = 0; k2 < Q; k2++) {
+        const int ky = lt + P * k2;
+        x[k2] = cmulc(aw[ky], bc[ky]);
+      }
+      fft_reg<Q, true>(x);
+#pragma unroll
+      for (int r = 0; r < Q; r++) bc[lt + P * r] = x[r];
+    }
+    team_barrier(1 + tm, team);
+    const int p = g.x + q;
+    for (int base = 0; base < 2 * box; base += team) {
+      const int o = base + lt;
+      const bool ok = o < 2 * box;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = bc + P * r;
+        const float2* tw = a.twO + m;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = __ldg(tw + k * box);
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    team_barrier(1 + tm, team);  // buffer `cur` may now be refilled
+    cur ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+template <int Q>
+cudaError_t launch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
+  const size_t smem = pair_cols_grp_smem(a.n, kRegThreads / team);
+  cudaError_t e = cudaFuncSetAttribute(k_pair_cols_grp<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(ngroups, a.H);
+  k_pair_cols_grp<Q><<<grid, kRegThreads, smem, st>>>(a, groups, team);
+  return cudaGetLastError();
+}
+
+template <int I = 0>
+cudaError_t dispatch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
+  if constexpr (I < kNumCodelets) {
+    constexpr int Q = kCodelets[I];
+    if (a.Q == Q) return launch_grp<Q>(a, groups, ngroups, team, st);
+    return dispatch_grp<I + 1>(a, groups, ngroups, team, st);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,
+                                     cudaStream_t st) {
+  if (!pair_cols_reg_supported(a.P, a.Q) || (a.n & 1)) return cudaErrorInvalidValue;
+  return dispatch_grp(a, groups, ngroups, team, st);
 }
 
 bool pair_cols_reg_supported(int P, int Q) {
@@ -836,6 +983,66 @@ __global__ void k_ramp(RampArgs a) {
   }
 }
 
+// Two-level variant for columns of length N1*N2: each thread keeps the
+// running sums of its E = ceil(n/256) column elements in registers, so a
+// frame's column is requested with E independent loads per thread; the final
+// inverse along ky is the two-level transform.
+template <int N1, int N2>
+__global__ void __launch_bounds__(kThreads) k_shift_sum2l(ShiftSumArgs a, const float2* __restrict__ ey) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  constexpr int E = (N + kThreads - 1) / kThreads;
+  extern __shared__ float2 sm2l[];
+  float2* col = sm2l;         // accumulated column, then the step-A input
+  float2* ysm = sm2l + N;     // exchange buffer
+  float2* ex = sm2l + 2 * N;  // per-frame exp(+2 pi i sx kx / n)
+  const int tid = threadIdx.x;
+  const int kx = blockIdx.x;
+  for (int f = tid; f < a.nsum; f += kThreads) {
+    double sn, cn;
+    const double t = a.shifts[f].x * (double)kx / (double)N;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  __syncthreads();
+  float2 acc[E];
+#pragma unroll
+  for (int j = 0; j < E; j++) acc[j] = make_float2(0.f, 0.f);
+  for (int f = 0; f < a.nsum; f++) {
+    const float2* c = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
+    const float2* eyf = ey + (long long)f * N;
+    const float2 e = ex[f];
+    const bool ap = a.apply[f] != 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < N) {
+        float2 v = __ldg(c + ky);
+        if (ap) v = cmul(v, cmul(e, __ldg(eyf + ky)));
+        acc[j] = cadd(acc[j], v);
+      }
+    }
+  }
+  if (a.mode == 0) {
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < N) a.out[(long long)kx * a.ld_out + ky] = acc[j];
+    }
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int ky = tid + kThreads * j;
+    if (ky < N) col[ky] = acc[j];
+  }
+  __syncthreads();
+  float2* out = a.out;
+  const long long ld = a.ld_out;
+  TL::template run<true, false>(ysm, a.tw, [&](int i) { return col[i]; },
+                                [&](int k, float2 v) { out[(long long)k * ld + kx] = v; });
+}
+
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st) {
   RampArgs r;
   r.shifts = a.shifts;
@@ -846,6 +1053,19 @@ cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st)
   k_ramp<<<g, 256, 0, st>>>(r);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  int n1 = 0, n2 = 0;
+  if (two_level_split(a.n, n1, n2)) {
+    const size_t smem2 = (size_t)(2 * a.n + a.nsum) * sizeof(float2);
+#define MC_TL_SUM(A, B)                                                                                       \
+  if (n1 == (A) && n2 == (B)) {                                                                               \
+    e = cudaFuncSetAttribute(k_shift_sum2l<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);   \
+    if (e != cudaSuccess) return e;                                                                           \
+    k_shift_sum2l<A, B><<<a.H, kThreads, smem2, st>>>(a, ey);                                                 \
+    return cudaGetLastError();                                                                                \
+  }
+    MC_TWO_LEVEL_LIST(MC_TL_SUM)
+#undef MC_TL_SUM
+  }
   const size_t smem = shift_sum_smem(a.n, a.nsum);
   e = cudaFuncSetAttribute(k_shift_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -894,7 +1114,55 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
   }
 }
 
+// Two-level variant: rows y, y+1 packed as Z = G_y + i G_{y+1} with the
+// Hermitian extension formed in the load (real DC and Nyquist).
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_c2r_rows2l(C2rRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  __shared__ float2 ysm[N];
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const float2* g0 = a.t2 + (long long)y0 * a.ld_t2;
+  const float2* g1 = a.t2 + (long long)y1 * a.ld_t2;
+  float* i0 = a.image + (long long)y0 * N;
+  float* i1 = a.image + (long long)y1 * N;
+  const float sc = a.scale;
+  TL::template run<true, false>(
+      ysm, a.tw,
+      [&](int k) {
+        float2 u, v;
+        if (k <= N / 2) {
+          u = __ldg(g0 + k);
+          v = __ldg(g1 + k);
+          if (k == 0 || k == N / 2) {
+            u.y = 0.f;
+            v.y = 0.f;
+          }
+        } else {
+          u = __ldg(g0 + N - k);
+          v = __ldg(g1 + N - k);
+          u.y = -u.y;
+          v.y = -v.y;
+        }
+        return make_float2(u.x - v.y, u.y + v.x);
+      },
+      [&](int x, float2 z) {
+        i0[x] = z.x * sc;
+        i1[x] = z.y * sc;
+      });
+}
+
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (two_level_split(a.n, n1, n2)) {
+#define MC_TL_C2R(A, B)                                              \
+  if (n1 == (A) && n2 == (B)) {                                      \
+    k_c2r_rows2l<A, B><<<a.n / 2, TwoLevel<A, B>::T, 0, st>>>(a);    \
+    return cudaGetLastError();                                       \
+  }
+    MC_TWO_LEVEL_LIST(MC_TL_C2R)
+#undef MC_TL_C2R
+  }
   const size_t smem = c2r_rows_smem(a.n);
   cudaError_t e = cudaFuncSetAttribute(k_c2r_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -11,6 +11,7 @@
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -145,6 +146,15 @@ double radix_cost(int r) {
 
 // n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
 void choose_prune(int n, int box, int& P, int& Q) {
+  // MC_PRUNE_Q=<q> forces the split n = (n/q)*q when the codelet kernel takes it
+  if (const char* env = getenv("MC_PRUNE_Q")) {
+    const int q = atoi(env);
+    if (q > 1 && n % q == 0 && mc::pair_cols_reg_supported(n / q, q)) {
+      P = n / q;
+      Q = q;
+      return;
+    }
+  }
   // first choice: a split the register-codelet kernel handles
   double best = 1e300;
   P = 0;
@@ -229,6 +239,9 @@ struct mc_plan {
   long long fstride = 0;  // complex elements per stored spectrum
   size_t dev_bytes = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st_copy = nullptr;          // upload stream of mc_plan_run_host
+  std::vector<cudaEvent_t> chunk_ev;       // one per uploaded chunk
+  cudaEvent_t start_ev = nullptr;
   int device = 0;
   mc_log_fn logfn = nullptr;
   void* loguser = nullptr;
@@ -242,6 +255,8 @@ struct mc_plan {
   float2 *d_tw_nu = nullptr, *d_tw_n = nullptr, *d_twQ = nullptr, *d_twO = nullptr, *d_cs = nullptr;
   double* d_w16 = nullptr;
   int2* d_pairs = nullptr;
+  int2* d_groups = nullptr;
+  bool grouped = false;  // grouped (cp.async, A staged once) column stage
   float2* d_G = nullptr;
   float* d_boxes = nullptr;
   float *d_pshift = nullptr, *d_pcc = nullptr;
@@ -357,6 +372,12 @@ struct mc_plan {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& e : kpool) cudaEventDestroy(e);
+    for (auto& e : chunk_ev) cudaEventDestroy(e);
+    if (start_ev) cudaEventDestroy(start_ev);
+    if (st_copy) {
+      cudaStreamSynchronize(st_copy);
+      cudaStreamDestroy(st_copy);
+    }
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -436,8 +457,20 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
       }
     }
     const double gbytes = (double)nb * pl->H * pl->box * sizeof(float2);
-    LAUNCH(pl, MC_K_PAIR_COLS, (double)nspec * pl->H * pl->n * sizeof(float2) + gbytes,
-           mc::launch_pair_cols(a, pl->st));
+    const double cbytes = (double)nspec * pl->H * pl->n * sizeof(float2) + gbytes;
+    if (pl->grouped) {
+      // runs of consecutive pairs that share their A spectrum
+      std::vector<int2> groups;
+      for (int i = 0; i < nb; i++) {
+        if (i == 0 || list[p0 + i].first != list[p0 + i - 1].first) groups.push_back(make_int2(i, 0));
+        groups.back().y++;
+      }
+      CK(cudaMemcpyAsync(pl->d_groups, groups.data(), sizeof(int2) * groups.size(), cudaMemcpyHostToDevice, pl->st));
+      LAUNCH(pl, MC_K_PAIR_COLS, cbytes,
+             mc::launch_pair_cols_grouped(a, pl->d_groups, (int)groups.size(), pl->P <= 64 ? 64 : 128, pl->st));
+    } else {
+      LAUNCH(pl, MC_K_PAIR_COLS, cbytes, mc::launch_pair_cols(a, pl->st));
+    }
     mc::PairRowsArgs r{};
     r.G = pl->d_G;
     r.npairs = nb;
@@ -628,6 +661,13 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
     const int team = pl->P <= 32 ? 32 : (pl->P <= 64 ? 64 : 128);
     const size_t need = reg ? mc::pair_cols_reg_smem(pl->n, team) : mc::pair_cols_smem(pl->n, pl->P, pl->Q, pl->box) + 16;
     if (need > 227 * 1024) return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
+    // grouped variant: A column + two B buffers per team (teams = 128 / team)
+    const int gteam = pl->P <= 64 ? 64 : 128;
+    // measured slower than the ungrouped kernel at n = 3710 (1 CTA per SM:
+    // shared-memory bound), so it runs only when asked for
+    const char* env = getenv("MC_PAIR_KERNEL");
+    pl->grouped = reg && (pl->n % 2 == 0) && mc::pair_cols_grp_smem(pl->n, 128 / gteam) <= 227 * 1024 &&
+                  env && std::strcmp(env, "grp") == 0;
   }
 
   CK(cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking));
@@ -648,6 +688,7 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
   pl->d_specB = pl->d_specA;
   if (pl->nu != pl->n) CKR(pl->alloc(&pl->d_T, sizeof(float2) * (size_t)pl->H * pl->ldu));
   CKR(pl->alloc(&pl->d_pairs, sizeof(int2) * pl->maxp));
+  CKR(pl->alloc(&pl->d_groups, sizeof(int2) * pl->maxp));
   CKR(pl->alloc(&pl->d_G, sizeof(float2) * (size_t)std::min(pl->maxp, kPairBatch) * pl->H * pl->box));
   CKR(pl->alloc(&pl->d_boxes, sizeof(float) * (size_t)pl->maxp * pl->box * pl->box));
   CKR(pl->alloc(&pl->d_pshift, sizeof(float) * 2 * pl->maxp));
@@ -784,14 +825,16 @@ int mc_plan_load_frames_device(mc_plan* pl, const void* d_frames, int first, int
   return load_frames(pl, d_frames, first, count, cudaMemcpyDeviceToDevice);
 }
 
-int mc_plan_forward(mc_plan* pl) {
-  if (!pl) return set_err(MC_E_ARG, "null plan");
-  for (int f = 0; f < pl->nframe; f++)
-    if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
-  CK(cudaSetDevice(pl->device));
+}  // extern "C"
+
+// Forward transforms of every position.  With `waits`, the plan stream waits
+// for (*waits)[f / chunk] before the first frame of each chunk (pipelined
+// upload); the per-frame means are read back and logged at the end.
+static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
   CK(cudaEventRecord(pl->ev[0], pl->st));
   const bool binned = pl->nu != pl->n;
   for (int f = 0; f < pl->nframe; f++) {
+    if (waits && f % chunk == 0) CK(cudaStreamWaitEvent(pl->st, (*waits)[f / chunk], 0));
     mc::FwdRowsArgs a{};
     a.frame = (const char*)pl->d_frames + (size_t)f * pl->frame_bytes;
     a.mode = pl->mode;
@@ -877,6 +920,54 @@ int mc_plan_forward(mc_plan* pl) {
   }
   pl->have_forward = true;
   pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+extern "C" {
+
+int mc_plan_forward(mc_plan* pl) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  for (int f = 0; f < pl->nframe; f++)
+    if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
+  CK(cudaSetDevice(pl->device));
+  return forward_all(pl, nullptr, 1);
+}
+
+int mc_plan_run_host(mc_plan* pl, const void* frames, float* image_host) {
+  if (!pl || !frames) return set_err(MC_E_ARG, "null argument");
+  CK(cudaSetDevice(pl->device));
+  if (!pl->st_copy) CK(cudaStreamCreateWithFlags(&pl->st_copy, cudaStreamNonBlocking));
+  // chunks of frames: copy chunk c on the copy stream while the plan stream
+  // transforms the frames of chunks < c
+  const int chunk = 4;
+  const int nchunk = (pl->nframe + chunk - 1) / chunk;
+  while ((int)pl->chunk_ev.size() < nchunk) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    pl->chunk_ev.push_back(e);
+  }
+  // the copies start after everything already queued on the plan stream
+  // (earlier readers of d_frames, a caller's start event)
+  if (!pl->start_ev) CK(cudaEventCreateWithFlags(&pl->start_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(pl->start_ev, pl->st));
+  CK(cudaStreamWaitEvent(pl->st_copy, pl->start_ev, 0));
+  for (int c = 0; c < nchunk; c++) {
+    const int f0 = c * chunk, cnt = std::min(chunk, pl->nframe - f0);
+    CK(cudaMemcpyAsync((char*)pl->d_frames + (size_t)f0 * pl->frame_bytes,
+                       (const char*)frames + (size_t)f0 * pl->frame_bytes, (size_t)cnt * pl->frame_bytes,
+                       cudaMemcpyHostToDevice, pl->st_copy));
+    CK(cudaEventRecord(pl->chunk_ev[c], pl->st_copy));
+  }
+  for (int f = 0; f < pl->nframe; f++) pl->loaded[f] = 1;
+  pl->log("Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", pl->nx, pl->ny, pl->nz, pl->mode);
+  pl->log("Crop Image: Offset(%d %d) RawDim(%d) BinnedDim(%d)\n", pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu,
+          pl->n);
+  CKR(forward_all(pl, &pl->chunk_ev, chunk));
+  CKR(mc_plan_pairs(pl));
+  CKR(mc_plan_solve(pl));
+  CKR(mc_plan_iterate(pl));
+  CKR(mc_plan_sum(pl, image_host));
+  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.sum_ms;
   return MC_OK;
 }
 
