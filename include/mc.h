@@ -172,6 +172,24 @@ const char* mc_kernel_name(int kind);
 int mc_solve_pairs(int nframe, int npairs, const int* ij, const float* shifts_xy, float kithresh,
                    double* step_xy, double* ki1, int* nkept, int* kept, double* ki2);
 
+/* No counterpart in the reference.  For callers that must not allocate
+ * device memory -- code inside a detector's acquisition/streaming loop that
+ * owns a fixed, pre-reserved memory budget, or a host framework that forbids
+ * allocation once its own pool is set up: the pbx x pbx cross-correlation
+ * window of one frame pair (what GPUShiftCC + GPUIFFT2d + the FindShift box
+ * copy produce, cufunc.cu:343-407), computed with no cudaMalloc/cudaFree and
+ * no allocating library call.  Inputs: two half spectra already on the
+ * device in this library's layout (spec[kx*ldn + ky], kx <= n/2, ky < n);
+ * output: d_window, pbx*pbx floats on the device.  Intermediate data lives in
+ * a 5 MiB file-scope device array that every GPU loading libmc holds until
+ * exit.  Limits: n even in [16, 4096], pbx in [16, min(128, n)], n = P*Q with
+ * P <= 128 and Q a register-codelet length; larger problems return MC_E_SIZE.
+ * The first call on a device looks up the array's address on that device
+ * (make it before any stream capture).  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
+int mc_pair_window_static(const void* d_spec_a, const void* d_spec_b, int n, int ldn, int pbx, float bfactor,
+                          float* d_window, void* stream);
+
 /* Batched 1-D complex FFT of the library's engine on device memory
  * (un-normalised; inverse = exp(+2 pi i)).  Stream may be NULL. */
 int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void* stream);

@@ -82,6 +82,8 @@ SIGNATURES = {
     "mc_kernel_name": (C.c_char_p, [C.c_int]),
     "mc_solve_pairs": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                  C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
+    "mc_pair_window_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p,
+                                        C.c_void_p]),
     "mc_fft1d": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 

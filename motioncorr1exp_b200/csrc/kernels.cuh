@@ -140,6 +140,9 @@ cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 
+// Sets the calling thread's mc_last_error() text; returns `code`.
+int record_error(int code, const char* text);
+
 // true when the register-codelet column stage handles the split n = P*Q
 bool pair_cols_reg_supported(int P, int Q);
 size_t pair_cols_reg_smem(int n, int team);

@@ -38,6 +38,12 @@ int set_err(int code, const char* fmt, ...) {
   return code;
 }
 
+}  // namespace
+
+int mc::record_error(int code, const char* text) { return set_err(code, "%s", text); }
+
+namespace {
+
 #define CK(call)                                                                                   \
   do {                                                                                             \
     cudaError_t e_ = (call);                                                                       \
