@@ -169,9 +169,8 @@ def run_ours(args):
     import torch.distributed as dist
     from motioncorr1exp_b200 import api, synth
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from motioncorr1exp_b200 import dist as D
+    rank, world, local = D.world()
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -225,10 +224,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     stats = plan.kernel_stats()
     shifts = plan.frame_shifts()
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = D.max_over_ranks(ms)
 
     # ---- end-to-end through the public API from pinned host buffers
     for _ in range(max(1, args.warmup // 2)):
@@ -242,10 +238,7 @@ def run_ours(args):
     f1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    t2 = torch.tensor([f0.elapsed_time(f1)], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t2.item())
+    e2e_ms = D.max_over_ranks(f0.elapsed_time(f1))
 
     truth_rmse = float(np.sqrt(np.mean(np.sum((shifts + (truth - truth[0])) ** 2, axis=1))))
 

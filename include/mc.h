@@ -76,7 +76,7 @@ typedef struct mc_info {
 } mc_info;
 
 typedef struct mc_timings { /* device time of the last run, CUDA events */
-  float forward_ms, pairs_ms, solve_ms, iterate_ms, sum_ms, total_ms;
+  float forward_ms, pairs_ms, solve_ms, iterate_ms, sum_ms, total_ms, refine_ms;
 } mc_timings;
 
 typedef void (*mc_log_fn)(const char* text, void* user);
@@ -146,6 +146,19 @@ int mc_plan_get_boxes(mc_plan* plan, float* host);                       /* npai
 int mc_plan_get_sum_shifts(const mc_plan* plan, double* xy, int* first, int* last);
 int mc_plan_get_timings(const mc_plan* plan, mc_timings* t);
 
+/* Added method (no reference counterpart; replaces the 1/32-px grid peak of
+ * FindShift, cufunc.cu:457-481, as the final sub-pixel step).  Objective of
+ * the frame-to-sum correlation for sum shifts s_k (the shifts
+ * phase-shift-and-sum applies, s_k = -frameshift_k + const):
+ *   J = sum_w h w |S|^2,  S = sum_k F_k exp(+i w.s_k),  w = B-factor weight,
+ * its gradient dJ/ds_k (2*nframe) from the hand-written adjoint of the
+ * shift-and-sum (one pass reading every spectrum once) and the 2x2 Hessian
+ * blocks (3*nframe: xx, xy, yy).  Any output may be NULL. */
+int mc_plan_objective(mc_plan* plan, const double* shifts_xy, double* J, double* grad, double* hess);
+/* Block-Newton ascent of J from the peak-fit shifts (after mc_plan_iterate);
+ * updates the final shifts.  mc_plan_run calls it when params.refine = 1. */
+int mc_plan_refine(mc_plan* plan, int iterations);
+
 /* Per-kernel accounting of a plan: launches and algorithmic bytes are always
  * counted; device time is recorded with one CUDA event pair per launch while
  * profiling is on.  Kinds follow the kernels of the path. */
@@ -157,7 +170,8 @@ enum {
   MC_K_PEAK = 4,      /* integer + x32 Fourier-upsampled peak */
   MC_K_SHIFT_SUM = 5, /* phase-shift-and-accumulate (+ inverse columns) */
   MC_K_C2R_ROWS = 6,  /* final C2R rows x 1/n^2 */
-  MC_KERNEL_KINDS = 7
+  MC_K_OBJECTIVE = 7, /* adjoint of the shift-and-sum: objective, gradient, Hessian blocks */
+  MC_KERNEL_KINDS = 8
 };
 void mc_plan_set_profiling(mc_plan* plan, int on);
 int mc_plan_reset_stats(mc_plan* plan);

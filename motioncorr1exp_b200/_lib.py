@@ -40,7 +40,8 @@ class McInfo(C.Structure):
 
 class McTimings(C.Structure):
     _fields_ = [("forward_ms", C.c_float), ("pairs_ms", C.c_float), ("solve_ms", C.c_float),
-                ("iterate_ms", C.c_float), ("sum_ms", C.c_float), ("total_ms", C.c_float)]
+                ("iterate_ms", C.c_float), ("sum_ms", C.c_float), ("total_ms", C.c_float),
+                ("refine_ms", C.c_float)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
@@ -80,6 +81,8 @@ SIGNATURES = {
     "mc_plan_kernel_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_double)]),
     "mc_kernel_name": (C.c_char_p, [C.c_int]),
+    "mc_plan_objective": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_void_p]),
+    "mc_plan_refine": (C.c_int, [C.c_void_p, C.c_int]),
     "mc_solve_pairs": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                  C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
     "mc_pair_window_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p,

@@ -63,7 +63,7 @@ def verify_params(p: Params, nz: int) -> Params:
 
 
 _WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2}
-KERNEL_KINDS = 7
+KERNEL_KINDS = 8
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
@@ -243,6 +243,19 @@ class Plan:
         t = L.McTimings()
         L.check(self._lib.mc_plan_get_timings(self._h, C.byref(t)))
         return {f: getattr(t, f) for f, _ in L.McTimings._fields_}
+
+    def objective(self, shifts: np.ndarray) -> tuple[float, np.ndarray, np.ndarray]:
+        """Frame-to-sum objective J at sum shifts (nframe, 2), its gradient
+        (nframe, 2) from the adjoint kernel and the Hessian blocks (nframe, 3)."""
+        s = np.ascontiguousarray(shifts, dtype=np.float64).reshape(self.nframe, 2)
+        J = C.c_double()
+        g = np.empty((self.nframe, 2))
+        h = np.empty((self.nframe, 3))
+        L.check(self._lib.mc_plan_objective(self._h, _ptr(s), C.byref(J), _ptr(g), _ptr(h)))
+        return J.value, g, h
+
+    def refine(self, iterations: int = 4) -> None:
+        L.check(self._lib.mc_plan_refine(self._h, iterations))
 
     def set_profiling(self, on: bool) -> None:
         self._lib.mc_plan_set_profiling(self._h, int(on))

@@ -2085,4 +2085,121 @@ __device__ __forceinline__ void dft_r53_part(const float2* v, int part, St&& st)
   default: break;
   }
 }
+__constant__ float2 c_tw53[27][27] = {{{1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f}},
+  {{1.0f, 0.0f}, {0.9929810762405396f, 0.11827316880226135f}, {0.9720228910446167f, 0.2348860502243042f}, {0.9374196529388428f, 0.3482016324996948f}, {0.8896570801734924f, 0.4566292464733124f}, {0.829405665397644f, 0.5586467385292053f}, {0.7575112581253052f, 0.6528221368789673f}, {0.674983024597168f, 0.7378332614898682f}, {0.5829795002937317f, 0.8124868869781494f}, {0.4827921986579895f, 0.8757349252700806f}, {0.3758275806903839f, 0.926689624786377f}, {0.26358717679977417f, 0.9646356105804443f}, {0.14764656126499176f, 0.989040195941925f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.9842305779457092f, 0.1768902689218521f}, {-0.9982437491416931f, 0.05924062803387642f}},
+  {{1.0f, 0.0f}, {0.9720228910446167f, 0.2348860502243042f}, {0.8896570801734924f, 0.4566292464733124f}, {0.7575112581253052f, 0.6528221368789673f}, {0.5829795002937317f, 0.8124868869781494f}, {0.3758275806903839f, 0.926689624786377f}, {0.14764656126499176f, 0.989040195941925f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.9982437491416931f, 0.05924062803387642f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.794854462146759f, -0.6068001389503479f}, {-0.6300878524780273f, -0.7765238881111145f}, {-0.43006521463394165f, -0.9027978181838989f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.029633328318595886f, -0.9995608329772949f}, {0.26358717679977417f, -0.9646356105804443f}, {0.4827921986579895f, -0.8757349252700806f}, {0.674983024597168f, -0.7378332614898682f}, {0.829405665397644f, -0.5586467385292053f}, {0.9374196529388428f, -0.3482016324996948f}, {0.9929810762405396f, -0.11827316880226135f}},
+  {{1.0f, 0.0f}, {0.9374196529388428f, 0.3482016324996948f}, {0.7575112581253052f, 0.6528221368789673f}, {0.4827921986579895f, 0.8757349252700806f}, {0.14764656126499176f, 0.989040195941925f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.7175072431564331f, -0.6965510249137878f}, {-0.43006521463394165f, -0.9027978181838989f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.26358717679977417f, -0.9646356105804443f}, {0.5829795002937317f, -0.8124868869781494f}, {0.829405665397644f, -0.5586467385292053f}, {0.9720228910446167f, -0.2348860502243042f}, {0.9929810762405396f, 0.11827316880226135f}, {0.8896570801734924f, 0.4566292464733124f}, {0.674983024597168f, 0.7378332614898682f}, {0.3758275806903839f, 0.926689624786377f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.9842305779457092f, 0.1768902689218521f}},
+  {{1.0f, 0.0f}, {0.8896570801734924f, 0.4566292464733124f}, {0.5829795002937317f, 0.8124868869781494f}, {0.14764656126499176f, 0.989040195941925f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.794854462146759f, -0.6068001389503479f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.029633328318595886f, -0.9995608329772949f}, {0.4827921986579895f, -0.8757349252700806f}, {0.829405665397644f, -0.5586467385292053f}, {0.9929810762405396f, -0.11827316880226135f}, {0.9374196529388428f, 0.3482016324996948f}, {0.674983024597168f, 0.7378332614898682f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.8610436320304871f, -0.5085310935974121f}, {-0.5338233709335327f, -0.8455960154533386f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.3758275806903839f, -0.926689624786377f}, {0.7575112581253052f, -0.6528221368789673f}, {0.9720228910446167f, -0.2348860502243042f}},
+  {{1.0f, 0.0f}, {0.829405665397644f, 0.5586467385292053f}, {0.3758275806903839f, 0.926689624786377f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.9842305779457092f, 0.1768902689218521f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.029633328318595886f, -0.9995608329772949f}, {0.5829795002937317f, -0.8124868869781494f}, {0.9374196529388428f, -0.3482016324996948f}, {0.9720228910446167f, 0.2348860502243042f}, {0.674983024597168f, 0.7378332614898682f}, {0.14764656126499176f, 0.989040195941925f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.794854462146759f, -0.6068001389503479f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.26358717679977417f, -0.9646356105804443f}, {0.7575112581253052f, -0.6528221368789673f}, {0.9929810762405396f, -0.11827316880226135f}, {0.8896570801734924f, 0.4566292464733124f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.956400990486145f, 0.29205676913261414f}},
+  {{1.0f, 0.0f}, {0.7575112581253052f, 0.6528221368789673f}, {0.14764656126499176f, 0.989040195941925f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.26358717679977417f, -0.9646356105804443f}, {0.829405665397644f, -0.5586467385292053f}, {0.9929810762405396f, 0.11827316880226135f}, {0.674983024597168f, 0.7378332614898682f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.9842305779457092f, 0.1768902689218521f}, {-0.8610436320304871f, -0.5085310935974121f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.3758275806903839f, -0.926689624786377f}, {0.8896570801734924f, -0.4566292464733124f}, {0.9720228910446167f, 0.2348860502243042f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.9982437491416931f, 0.05924062803387642f}, {-0.794854462146759f, -0.6068001389503479f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.4827921986579895f, -0.8757349252700806f}, {0.9374196529388428f, -0.3482016324996948f}},
+  {{1.0f, 0.0f}, {0.674983024597168f, 0.7378332614898682f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.26358717679977417f, -0.9646356105804443f}, {0.8896570801734924f, -0.4566292464733124f}, {0.9374196529388428f, 0.3482016324996948f}, {0.3758275806903839f, 0.926689624786377f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.8610436320304871f, -0.5085310935974121f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.5829795002937317f, -0.8124868869781494f}, {0.9929810762405396f, -0.11827316880226135f}, {0.7575112581253052f, 0.6528221368789673f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.14764656126499176f, -0.989040195941925f}, {0.829405665397644f, -0.5586467385292053f}, {0.9720228910446167f, 0.2348860502243042f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.9151456356048584f, 0.4031234383583069f}},
+  {{1.0f, 0.0f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.794854462146759f, -0.6068001389503479f}, {0.029633328318595886f, -0.9995608329772949f}, {0.829405665397644f, -0.5586467385292053f}, {0.9374196529388428f, 0.3482016324996948f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.3758275806903839f, -0.926689624786377f}, {0.9720228910446167f, -0.2348860502243042f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.674983024597168f, -0.7378332614898682f}, {0.9929810762405396f, 0.11827316880226135f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.9842305779457092f, 0.1768902689218521f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.14764656126499176f, -0.989040195941925f}, {0.8896570801734924f, -0.4566292464733124f}},
+  {{1.0f, 0.0f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.5829795002937317f, -0.8124868869781494f}, {0.9929810762405396f, 0.11827316880226135f}, {0.3758275806903839f, 0.926689624786377f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.674983024597168f, -0.7378332614898682f}, {0.9720228910446167f, 0.2348860502243042f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.956400990486145f, -0.29205676913261414f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.7575112581253052f, -0.6528221368789673f}, {0.9374196529388428f, 0.3482016324996948f}, {0.14764656126499176f, 0.989040195941925f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.9151456356048584f, -0.4031234383583069f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.829405665397644f, -0.5586467385292053f}, {0.8896570801734924f, 0.4566292464733124f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.8610436320304871f, 0.5085310935974121f}},
+  {{1.0f, 0.0f}, {0.3758275806903839f, 0.926689624786377f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.029633328318595886f, -0.9995608329772949f}, {0.9374196529388428f, -0.3482016324996948f}, {0.674983024597168f, 0.7378332614898682f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.9982437491416931f, -0.05924062803387642f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.7575112581253052f, -0.6528221368789673f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.4827921986579895f, -0.8757349252700806f}, {0.9929810762405396f, 0.11827316880226135f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.8610436320304871f, -0.5085310935974121f}, {0.14764656126499176f, -0.989040195941925f}, {0.9720228910446167f, -0.2348860502243042f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.829405665397644f, -0.5586467385292053f}},
+  {{1.0f, 0.0f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.4827921986579895f, -0.8757349252700806f}, {0.9720228910446167f, 0.2348860502243042f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.674983024597168f, -0.7378332614898682f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.9982437491416931f, 0.05924062803387642f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.829405665397644f, -0.5586467385292053f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.9842305779457092f, -0.1768902689218521f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.9374196529388428f, -0.3482016324996948f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.14764656126499176f, -0.989040195941925f}, {0.9929810762405396f, -0.11827316880226135f}, {0.3758275806903839f, 0.926689624786377f}, {-0.794854462146759f, 0.6068001389503479f}},
+  {{1.0f, 0.0f}, {0.14764656126499176f, 0.989040195941925f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.829405665397644f, -0.5586467385292053f}, {0.674983024597168f, 0.7378332614898682f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.8610436320304871f, -0.5085310935974121f}, {0.3758275806903839f, -0.926689624786377f}, {0.9720228910446167f, 0.2348860502243042f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.9982437491416931f, 0.05924062803387642f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.9374196529388428f, -0.3482016324996948f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.5829795002937317f, -0.8124868869781494f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.029633328318595886f, -0.9995608329772949f}, {0.9929810762405396f, -0.11827316880226135f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.7575112581253052f, -0.6528221368789673f}},
+  {{1.0f, 0.0f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.9982437491416931f, 0.05924062803387642f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.9929810762405396f, -0.11827316880226135f}, {0.14764656126499176f, 0.989040195941925f}, {-0.9842305779457092f, 0.1768902689218521f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.9720228910446167f, -0.2348860502243042f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.956400990486145f, 0.29205676913261414f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.9374196529388428f, -0.3482016324996948f}, {0.3758275806903839f, 0.926689624786377f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.8896570801734924f, -0.4566292464733124f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.829405665397644f, -0.5586467385292053f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.7575112581253052f, -0.6528221368789673f}, {0.674983024597168f, 0.7378332614898682f}, {-0.7175072431564331f, 0.6965510249137878f}},
+  {{1.0f, 0.0f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.26358717679977417f, -0.9646356105804443f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.8610436320304871f, -0.5085310935974121f}, {0.5829795002937317f, -0.8124868869781494f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.829405665397644f, -0.5586467385292053f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.9720228910446167f, -0.2348860502243042f}, {0.14764656126499176f, 0.989040195941925f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.029633328318595886f, -0.9995608329772949f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.956400990486145f, -0.29205676913261414f}, {0.3758275806903839f, -0.926689624786377f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.794854462146759f, -0.6068001389503479f}, {0.674983024597168f, -0.7378332614898682f}},
+  {{1.0f, 0.0f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.5829795002937317f, -0.8124868869781494f}, {0.674983024597168f, 0.7378332614898682f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.956400990486145f, -0.29205676913261414f}, {0.4827921986579895f, -0.8757349252700806f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.9720228910446167f, -0.2348860502243042f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.3758275806903839f, -0.926689624786377f}, {0.829405665397644f, 0.5586467385292053f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.9374196529388428f, -0.3482016324996948f}, {0.14764656126499176f, 0.989040195941925f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.26358717679977417f, -0.9646356105804443f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.6300878524780273f, 0.7765238881111145f}},
+  {{1.0f, 0.0f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.794854462146759f, -0.6068001389503479f}, {0.829405665397644f, -0.5586467385292053f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.3758275806903839f, -0.926689624786377f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.8896570801734924f, -0.4566292464733124f}, {0.14764656126499176f, 0.989040195941925f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.4827921986579895f, -0.8757349252700806f}, {0.674983024597168f, 0.7378332614898682f}, {-0.9151456356048584f, 0.4031234383583069f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.9720228910446167f, 0.2348860502243042f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.9374196529388428f, -0.3482016324996948f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.956400990486145f, -0.29205676913261414f}, {0.5829795002937317f, -0.8124868869781494f}},
+  {{1.0f, 0.0f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.794854462146759f, -0.6068001389503479f}, {0.8896570801734924f, -0.4566292464733124f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.7575112581253052f, -0.6528221368789673f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.5829795002937317f, -0.8124868869781494f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.3758275806903839f, -0.926689624786377f}, {0.674983024597168f, 0.7378332614898682f}, {-0.956400990486145f, 0.29205676913261414f}, {0.14764656126499176f, -0.989040195941925f}, {0.829405665397644f, 0.5586467385292053f}, {-0.8610436320304871f, 0.5085310935974121f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.5338233709335327f, 0.8455960154533386f}},
+  {{1.0f, 0.0f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.9720228910446167f, 0.2348860502243042f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.794854462146759f, 0.6068001389503479f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.029633328318595886f, -0.9995608329772949f}, {0.829405665397644f, 0.5586467385292053f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.14764656126499176f, -0.989040195941925f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.956400990486145f, 0.29205676913261414f}, {0.26358717679977417f, -0.9646356105804443f}, {0.674983024597168f, 0.7378332614898682f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.3758275806903839f, -0.926689624786377f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.4827921986579895f, -0.8757349252700806f}},
+  {{1.0f, 0.0f}, {-0.6300878524780273f, 0.7765238881111145f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.26358717679977417f, -0.9646356105804443f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.674983024597168f, -0.7378332614898682f}, {0.14764656126499176f, 0.989040195941925f}, {-0.8610436320304871f, -0.5085310935974121f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.7175072431564331f, 0.6965510249137878f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.829405665397644f, 0.5586467385292053f}, {-0.956400990486145f, 0.29205676913261414f}, {0.3758275806903839f, -0.926689624786377f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.7575112581253052f, -0.6528221368789673f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.794854462146759f, -0.6068001389503479f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.43006521463394165f, 0.9027978181838989f}},
+  {{1.0f, 0.0f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.029633328318595886f, -0.9995608329772949f}, {0.674983024597168f, 0.7378332614898682f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.794854462146759f, 0.6068001389503479f}, {0.14764656126499176f, -0.989040195941925f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.829405665397644f, -0.5586467385292053f}, {-0.2059786170721054f, 0.9785565137863159f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.9720228910446167f, 0.2348860502243042f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.26358717679977417f, -0.9646356105804443f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.956400990486145f, -0.29205676913261414f}, {0.8896570801734924f, -0.4566292464733124f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.3758275806903839f, -0.926689624786377f}},
+  {{1.0f, 0.0f}, {-0.794854462146759f, 0.6068001389503479f}, {0.26358717679977417f, -0.9646356105804443f}, {0.3758275806903839f, 0.926689624786377f}, {-0.8610436320304871f, -0.5085310935974121f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.14764656126499176f, -0.989040195941925f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.029633328318595886f, -0.9995608329772949f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.5338233709335327f, 0.8455960154533386f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.674983024597168f, 0.7378332614898682f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.8896570801734924f, -0.4566292464733124f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.829405665397644f, -0.5586467385292053f}, {-0.3202698528766632f, 0.9473263621330261f}},
+  {{1.0f, 0.0f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.4827921986579895f, -0.8757349252700806f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.829405665397644f, -0.5586467385292053f}, {-0.43006521463394165f, 0.9027978181838989f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.9151456356048584f, -0.4031234383583069f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.794854462146759f, 0.6068001389503479f}, {0.3758275806903839f, -0.926689624786377f}, {0.14764656126499176f, 0.989040195941925f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.674983024597168f, 0.7378332614898682f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.26358717679977417f, -0.9646356105804443f}},
+  {{1.0f, 0.0f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.674983024597168f, -0.7378332614898682f}, {-0.3202698528766632f, 0.9473263621330261f}, {-0.08879589289426804f, -0.9960498213768005f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.794854462146759f, -0.6068001389503479f}, {0.9720228910446167f, 0.2348860502243042f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.829405665397644f, -0.5586467385292053f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.14764656126499176f, -0.989040195941925f}, {0.26358717679977417f, 0.9646356105804443f}, {-0.6300878524780273f, -0.7765238881111145f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.3758275806903839f, -0.926689624786377f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.43006521463394165f, -0.9027978181838989f}, {0.7575112581253052f, 0.6528221368789673f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.2059786170721054f, 0.9785565137863159f}},
+  {{1.0f, 0.0f}, {-0.956400990486145f, 0.29205676913261414f}, {0.829405665397644f, -0.5586467385292053f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.3758275806903839f, -0.926689624786377f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.26358717679977417f, -0.9646356105804443f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.794854462146759f, -0.6068001389503479f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.674983024597168f, -0.7378332614898682f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.14764656126499176f, -0.989040195941925f}},
+  {{1.0f, 0.0f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.14764656126499176f, -0.989040195941925f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.3758275806903839f, 0.926689624786377f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.674983024597168f, 0.7378332614898682f}, {-0.794854462146759f, -0.6068001389503479f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.829405665397644f, -0.5586467385292053f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.08879589289426804f, 0.9960498213768005f}},
+  {{1.0f, 0.0f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.956400990486145f, 0.29205676913261414f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.8896570801734924f, -0.4566292464733124f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.829405665397644f, -0.5586467385292053f}, {-0.794854462146759f, 0.6068001389503479f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.674983024597168f, -0.7378332614898682f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.3758275806903839f, -0.926689624786377f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.2059786170721054f, 0.9785565137863159f}, {0.14764656126499176f, -0.989040195941925f}, {-0.08879589289426804f, 0.9960498213768005f}, {0.029633328318595886f, -0.9995608329772949f}}};
+template <bool INV, typename St>
+__device__ __forceinline__ void dft_r53_compact(const float2* v, St&& st) {
+  const float2 x0 = v[0];
+  const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
+  const float2 d1 = make_float2(v[1].x - v[52].x, v[1].y - v[52].y);
+  const float2 s2 = make_float2(v[2].x + v[51].x, v[2].y + v[51].y);
+  const float2 d2 = make_float2(v[2].x - v[51].x, v[2].y - v[51].y);
+  const float2 s3 = make_float2(v[3].x + v[50].x, v[3].y + v[50].y);
+  const float2 d3 = make_float2(v[3].x - v[50].x, v[3].y - v[50].y);
+  const float2 s4 = make_float2(v[4].x + v[49].x, v[4].y + v[49].y);
+  const float2 d4 = make_float2(v[4].x - v[49].x, v[4].y - v[49].y);
+  const float2 s5 = make_float2(v[5].x + v[48].x, v[5].y + v[48].y);
+  const float2 d5 = make_float2(v[5].x - v[48].x, v[5].y - v[48].y);
+  const float2 s6 = make_float2(v[6].x + v[47].x, v[6].y + v[47].y);
+  const float2 d6 = make_float2(v[6].x - v[47].x, v[6].y - v[47].y);
+  const float2 s7 = make_float2(v[7].x + v[46].x, v[7].y + v[46].y);
+  const float2 d7 = make_float2(v[7].x - v[46].x, v[7].y - v[46].y);
+  const float2 s8 = make_float2(v[8].x + v[45].x, v[8].y + v[45].y);
+  const float2 d8 = make_float2(v[8].x - v[45].x, v[8].y - v[45].y);
+  const float2 s9 = make_float2(v[9].x + v[44].x, v[9].y + v[44].y);
+  const float2 d9 = make_float2(v[9].x - v[44].x, v[9].y - v[44].y);
+  const float2 s10 = make_float2(v[10].x + v[43].x, v[10].y + v[43].y);
+  const float2 d10 = make_float2(v[10].x - v[43].x, v[10].y - v[43].y);
+  const float2 s11 = make_float2(v[11].x + v[42].x, v[11].y + v[42].y);
+  const float2 d11 = make_float2(v[11].x - v[42].x, v[11].y - v[42].y);
+  const float2 s12 = make_float2(v[12].x + v[41].x, v[12].y + v[41].y);
+  const float2 d12 = make_float2(v[12].x - v[41].x, v[12].y - v[41].y);
+  const float2 s13 = make_float2(v[13].x + v[40].x, v[13].y + v[40].y);
+  const float2 d13 = make_float2(v[13].x - v[40].x, v[13].y - v[40].y);
+  const float2 s14 = make_float2(v[14].x + v[39].x, v[14].y + v[39].y);
+  const float2 d14 = make_float2(v[14].x - v[39].x, v[14].y - v[39].y);
+  const float2 s15 = make_float2(v[15].x + v[38].x, v[15].y + v[38].y);
+  const float2 d15 = make_float2(v[15].x - v[38].x, v[15].y - v[38].y);
+  const float2 s16 = make_float2(v[16].x + v[37].x, v[16].y + v[37].y);
+  const float2 d16 = make_float2(v[16].x - v[37].x, v[16].y - v[37].y);
+  const float2 s17 = make_float2(v[17].x + v[36].x, v[17].y + v[36].y);
+  const float2 d17 = make_float2(v[17].x - v[36].x, v[17].y - v[36].y);
+  const float2 s18 = make_float2(v[18].x + v[35].x, v[18].y + v[35].y);
+  const float2 d18 = make_float2(v[18].x - v[35].x, v[18].y - v[35].y);
+  const float2 s19 = make_float2(v[19].x + v[34].x, v[19].y + v[34].y);
+  const float2 d19 = make_float2(v[19].x - v[34].x, v[19].y - v[34].y);
+  const float2 s20 = make_float2(v[20].x + v[33].x, v[20].y + v[33].y);
+  const float2 d20 = make_float2(v[20].x - v[33].x, v[20].y - v[33].y);
+  const float2 s21 = make_float2(v[21].x + v[32].x, v[21].y + v[32].y);
+  const float2 d21 = make_float2(v[21].x - v[32].x, v[21].y - v[32].y);
+  const float2 s22 = make_float2(v[22].x + v[31].x, v[22].y + v[31].y);
+  const float2 d22 = make_float2(v[22].x - v[31].x, v[22].y - v[31].y);
+  const float2 s23 = make_float2(v[23].x + v[30].x, v[23].y + v[30].y);
+  const float2 d23 = make_float2(v[23].x - v[30].x, v[23].y - v[30].y);
+  const float2 s24 = make_float2(v[24].x + v[29].x, v[24].y + v[29].y);
+  const float2 d24 = make_float2(v[24].x - v[29].x, v[24].y - v[29].y);
+  const float2 s25 = make_float2(v[25].x + v[28].x, v[25].y + v[28].y);
+  const float2 d25 = make_float2(v[25].x - v[28].x, v[25].y - v[28].y);
+  const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
+  const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
+  st(0, make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y)));
+#pragma unroll 1
+  for (int k = 1; k <= 26; k++) {
+    const float2* t = c_tw53[k];
+    float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+    { const float2 c = t[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); }
+    { const float2 c = t[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); }
+    { const float2 c = t[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); }
+    { const float2 c = t[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); }
+    { const float2 c = t[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); }
+    { const float2 c = t[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); }
+    { const float2 c = t[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); }
+    { const float2 c = t[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); }
+    { const float2 c = t[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); }
+    { const float2 c = t[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); }
+    { const float2 c = t[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); }
+    { const float2 c = t[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); }
+    { const float2 c = t[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); }
+    { const float2 c = t[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); }
+    { const float2 c = t[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); }
+    { const float2 c = t[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); }
+    { const float2 c = t[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); }
+    { const float2 c = t[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); }
+    { const float2 c = t[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); }
+    { const float2 c = t[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); }
+    { const float2 c = t[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); }
+    { const float2 c = t[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); }
+    { const float2 c = t[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); }
+    { const float2 c = t[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); }
+    { const float2 c = t[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); }
+    { const float2 c = t[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); }
+    if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - k, make_float2(ar - bi, ai + br)); }
+    else { st(k, make_float2(ar - bi, ai + br)); st(53 - k, make_float2(ar + bi, ai - br)); }
+  }
+}
 }  // namespace mc

@@ -94,6 +94,43 @@ def emit_odd_split(R: int, S: int) -> str:
     return "\n".join(L)
 
 
+def emit_odd_compact(R: int) -> str:
+    """Radix-R DFT with a runtime loop over the (R-1)/2 output pairs: the
+    pairs' twiddles come from a __constant__ table (uniform index, broadcast),
+    so the code is ~h times smaller than the straight-line form; each output
+    goes to st(index, value) as soon as it is formed."""
+    h = (R - 1) // 2
+    rows = []
+    for k in range(h + 1):
+        row = []
+        for n in range(h + 1):
+            m = (n * k) % R
+            row.append(f"{{{flit(math.cos(2 * math.pi * m / R))}, {flit(math.sin(2 * math.pi * m / R))}}}")
+        rows.append("{" + ", ".join(row) + "}")
+    L = [f"__constant__ float2 c_tw{R}[{h + 1}][{h + 1}] = {{" + ",\n  ".join(rows) + "};",
+         f"template <bool INV, typename St>",
+         f"__device__ __forceinline__ void dft_r{R}_compact(const float2* v, St&& st) {{",
+         "  const float2 x0 = v[0];"]
+    for n in range(1, h + 1):
+        L.append(f"  const float2 s{n} = make_float2(v[{n}].x + v[{R-n}].x, v[{n}].y + v[{R-n}].y);")
+        L.append(f"  const float2 d{n} = make_float2(v[{n}].x - v[{R-n}].x, v[{n}].y - v[{R-n}].y);")
+    sx = " + ".join([f"s{n}.x" for n in range(1, h + 1)])
+    sy = " + ".join([f"s{n}.y" for n in range(1, h + 1)])
+    L.append(f"  st(0, make_float2(x0.x + ({sx}), x0.y + ({sy})));")
+    L.append("#pragma unroll 1")
+    L.append(f"  for (int k = 1; k <= {h}; k++) {{")
+    L.append(f"    const float2* t = c_tw{R}[k];")
+    L.append("    float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;")
+    for n in range(1, h + 1):
+        L.append(f"    {{ const float2 c = t[{n}]; ar = fmaf(s{n}.x, c.x, ar); ai = fmaf(s{n}.y, c.x, ai);"
+                 f" br = fmaf(d{n}.x, c.y, br); bi = fmaf(d{n}.y, c.y, bi); }}")
+    L.append(f"    if (!INV) {{ st(k, make_float2(ar + bi, ai - br)); st({R} - k, make_float2(ar - bi, ai + br)); }}")
+    L.append(f"    else {{ st(k, make_float2(ar - bi, ai + br)); st({R} - k, make_float2(ar + bi, ai - br)); }}")
+    L.append("  }")
+    L.append("}")
+    return "\n".join(L)
+
+
 def factor_codelet(q: int) -> list:
     """Radix order used for register codelets: odd radices first, then 8/4/2."""
     rad, m = [], q
@@ -185,6 +222,7 @@ def main() -> None:
             out.append(emit_odd(R))
         out.append(f"constexpr int kSplit53 = {SPLIT53};")
         out.append(emit_odd_split(53, SPLIT53))
+        out.append(emit_odd_compact(53))
         out.append("}  // namespace mc")
     else:
         out.append("// Register-resident FFT codelets (lengths with factors 2, 3, 5, 7).")

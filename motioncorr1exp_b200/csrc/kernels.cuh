@@ -131,6 +131,29 @@ struct RampArgs {
   float2* ey;            // [nsum][n]
 };
 
+// ---------------------------------------------------------------- adjoint --
+// Frame-to-sum objective of the gradient refinement, for sum shifts s_k:
+//   J = sum h w |S|^2,  S = sum_k F_k exp(+i w.s_k)   (S given, mode-0 sum)
+//   g_k = -2 sum h w w_vec Im(u_k),  H_k = -2 sum h w w_vec w_vec^T Re(u_k),
+//   u_k = conj(S - P_k) P_k,  P_k = F_k exp(+i w.s_k)
+// h = half-spectrum multiplicity, w = exp(mbf r^2).  One CTA per column kx
+// reads S and every frame's column once; FP64 partials per (kx, frame).
+struct ObjectiveArgs {
+  const float2* spec;
+  long long stride;
+  int nframes;
+  const float2* S;       // [kx][ky], pitch ldn
+  const double2* shifts; // per frame (sx, sy)
+  const float2* ey;      // [frame][ky] exp(+2 pi i sy ky / n) (k_ramp table)
+  int n, ldn, H;
+  float mbf;
+  double* partial;       // [H][nframes][5]: gx, gy, hxx, hxy, hyy (without the -2)
+  double* partialJ;      // [H]
+  double* out;           // [nframes][5] (with the -2) then J at out[5*nframes]
+};
+cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st);
+cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st);
+
 cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st);
 cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st);
 cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st);

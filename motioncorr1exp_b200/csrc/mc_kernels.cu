@@ -207,12 +207,17 @@ struct TwoLevel {
     if (act) {
 #pragma unroll
       for (int n1 = 0; n1 < N1; n1++) v[n1] = ysm[lt * N1 + n1];
-      fft_n1<N1, INV>(v);
     }
-    if (SYNC_STORE) __syncthreads();
-    if (act) {
+    if constexpr (N1 == 53 && !SYNC_STORE) {
+      // compact radix-53 DFT: small code, outputs stored as they are formed
+      if (act) dft_r53_compact<INV>(v, [&](int k1, float2 x) { store(lt + N2 * k1, x); });
+    } else {
+      if (act) fft_n1<N1, INV>(v);
+      if (SYNC_STORE) __syncthreads();
+      if (act) {
 #pragma unroll
-      for (int k1 = 0; k1 < N1; k1++) store(lt + N2 * k1, v[k1]);
+        for (int k1 = 0; k1 < N1; k1++) store(lt + N2 * k1, v[k1]);
+      }
     }
   }
 };
@@ -295,8 +300,10 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_fwd_rows2l(FwdRowsArgs 
     default: stage_rows<float>(xin, a, r0, r1, N, TL::T); break;
   }
   __syncthreads();
-  float2* zsm = xin;  // step B stores land after every step-A read of xin
-  TL::template run<false, true>(
+  // step B writes Z into xin: every step-A read of xin precedes the barrier
+  // between the steps, and step B reads only ysm
+  float2* zsm = xin;
+  TL::template run<false, false>(
       ysm, a.tw, [&](int x) { return xin[x]; }, [&](int k, float2 v) { zsm[k] = v; });
   __syncthreads();
   for (int k = threadIdx.x; k < a.hk; k += TL::T) {
@@ -1112,6 +1119,144 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
     a.image[(long long)y0 * n + x] = z.x * a.scale;
     a.image[(long long)y1 * n + x] = z.y * a.scale;
   }
+}
+
+// =============================================================== adjoint ==
+template <int E>
+__global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
+  extern __shared__ double smo[];
+  double* red = smo;                                                   // [warps][5]
+  float2* ex = reinterpret_cast<float2*>(smo + (kThreads / 32) * 5);  // [nframes]
+  const int n = a.n, half = n / 2;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int kx = blockIdx.x;
+  const float h = (kx == 0 || kx == half) ? 1.f : 2.f;
+  const float ox = 6.283185307179586f * (float)kx / (float)n;
+  for (int f = tid; f < a.nframes; f += kThreads) {
+    double sn, cn;
+    const double t = a.shifts[f].x * (double)kx / (double)n;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  float2 s[E];
+  float hw[E], oy[E];
+  double jsum = 0.0;
+  const float2* Scol = a.S + (long long)kx * a.ldn;
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int ky = tid + kThreads * j;
+    if (ky < n) {
+      const int y = ky < half ? ky : ky - n;
+      s[j] = __ldg(Scol + ky);
+      hw[j] = h * expf(a.mbf * (float)(kx * kx + y * y));
+      oy[j] = 6.283185307179586f * (float)y / (float)n;
+      jsum += (double)(hw[j] * (s[j].x * s[j].x + s[j].y * s[j].y));
+    } else {
+      s[j] = make_float2(0.f, 0.f);
+      hw[j] = 0.f;
+      oy[j] = 0.f;
+    }
+  }
+  __syncthreads();
+  // J partial
+  for (int o = 16; o > 0; o >>= 1) jsum += __shfl_xor_sync(0xffffffffu, jsum, o);
+  if (lane == 0) red[wid * 5] = jsum;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; w++) t += red[w * 5];
+    a.partialJ[kx] = t;
+  }
+  __syncthreads();
+  for (int f = 0; f < a.nframes; f++) {
+    const float2* c = a.spec + (long long)f * a.stride + (long long)kx * a.ldn;
+    const float2* eyf = a.ey + (long long)f * n;
+    const float2 e = ex[f];
+    double gx = 0, gy = 0, hxx = 0, hxy = 0, hyy = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < n) {
+        const float2 P = cmul(__ldg(c + ky), cmul(e, __ldg(eyf + ky)));
+        const float2 d = csub(s[j], P);
+        const float2 u = cmulc(P, d);  // conj(d) * P
+        const double wi = (double)(hw[j] * u.y), wr = (double)(hw[j] * u.x);
+        const double y = (double)oy[j];
+        gx += wi;
+        gy += wi * y;
+        hxx += wr;
+        hxy += wr * y;
+        hyy += wr * y * y;
+      }
+    }
+    // omega_x is constant over the column: apply it after the sums
+    double v[5] = {gx * ox, gy, hxx * ox * ox, hxy * ox, hyy};
+#pragma unroll
+    for (int q = 0; q < 5; q++)
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 5; q++) red[wid * 5 + q] = v[q];
+    __syncthreads();
+    if (tid < 5) {
+      double t = 0.0;
+      for (int w = 0; w < kThreads / 32; w++) t += red[w * 5 + tid];
+      a.partial[((long long)kx * a.nframes + f) * 5 + tid] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Column partials -> per-frame totals in a fixed order (deterministic).
+__global__ void k_objective_reduce(ObjectiveArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nv = a.nframes * 5;
+  if (t < nv) {
+    double acc = 0.0;
+    for (int kx = 0; kx < a.H; kx++) acc += a.partial[(long long)kx * nv + t];
+    a.out[t] = -2.0 * acc;
+  } else if (t == nv) {
+    double acc = 0.0;
+    for (int kx = 0; kx < a.H; kx++) acc += a.partialJ[kx];
+    a.out[nv] = acc;
+  }
+}
+
+cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st) {
+  RampArgs r;
+  r.shifts = shifts;
+  r.nsum = nsum;
+  r.n = n;
+  r.ey = ey;
+  dim3 g((n + 255) / 256, nsum);
+  k_ramp<<<g, 256, 0, st>>>(r);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (kThreads / 32) * 5 + sizeof(float2) * (size_t)a.nframes;
+  cudaError_t e;
+  const int E = (a.n + kThreads - 1) / kThreads;
+  if (E <= 8) {
+    e = cudaFuncSetAttribute(k_objective<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_objective<8><<<a.H, kThreads, smem, st>>>(a);
+  } else if (E <= 16) {
+    e = cudaFuncSetAttribute(k_objective<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_objective<16><<<a.H, kThreads, smem, st>>>(a);
+  } else if (E <= 36) {
+    e = cudaFuncSetAttribute(k_objective<36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_objective<36><<<a.H, kThreads, smem, st>>>(a);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nv = a.nframes * 5 + 1;
+  k_objective_reduce<<<(nv + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 // Two-level variant: rows y, y+1 packed as Z = G_y + i G_{y+1} with the

@@ -271,6 +271,8 @@ struct mc_plan {
   float* d_image = nullptr;
   int *d_sumframes = nullptr, *d_apply = nullptr;
   double2* d_sumshift = nullptr;
+  double* d_opart = nullptr;  // objective partials [H][nframe][5] + [H]
+  double* d_oout = nullptr;   // objective totals [nframe][5] + J
   int maxp = 0;
   std::vector<void*> allocs;
 
@@ -707,6 +709,8 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
   CKR(pl->alloc(&pl->d_sumframes, sizeof(int) * pl->nframe));
   CKR(pl->alloc(&pl->d_apply, sizeof(int) * pl->nframe));
   CKR(pl->alloc(&pl->d_sumshift, sizeof(double2) * pl->nframe));
+  CKR(pl->alloc(&pl->d_opart, sizeof(double) * ((size_t)pl->H * pl->nframe * 5 + pl->H)));
+  CKR(pl->alloc(&pl->d_oout, sizeof(double) * ((size_t)pl->nframe * 5 + 1)));
 
   // tables
   CKR(pl->alloc(&pl->d_tw_nu, sizeof(float2) * pl->nu));
@@ -972,8 +976,10 @@ int mc_plan_run_host(mc_plan* pl, const void* frames, float* image_host) {
   CKR(mc_plan_pairs(pl));
   CKR(mc_plan_solve(pl));
   CKR(mc_plan_iterate(pl));
+  pl->tm.refine_ms = 0.f;
+  if (pl->p.refine) CKR(mc_plan_refine(pl, 4));
   CKR(mc_plan_sum(pl, image_host));
-  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.sum_ms;
+  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.refine_ms + pl->tm.sum_ms;
   return MC_OK;
 }
 
@@ -1167,6 +1173,104 @@ int mc_plan_sum(mc_plan* pl, float* image_host) {
   return MC_OK;
 }
 
+// Objective of the gradient refinement at sum shifts s (2*nframe): J, its
+// gradient (2*nframe) and the 2x2 Hessian blocks (3*nframe: xx, xy, yy).
+// Pass 1 is the phase-shift-and-sum into d_sum, pass 2 the adjoint kernel.
+static int objective(mc_plan* pl, const std::vector<cplx>& s, double* J, double* grad, double* hess) {
+  const int nf = pl->nframe;
+  std::vector<int> frames(nf), apply(nf, 1);
+  for (int k = 0; k < nf; k++) frames[k] = k;
+  CKR(run_shift_sum(pl, frames, s, apply, 0));  // also leaves the ky ramps of s in d_ey
+  mc::ObjectiveArgs a{};
+  a.spec = pl->d_specA;
+  a.stride = pl->fstride;
+  a.nframes = nf;
+  a.S = pl->d_sum;
+  a.shifts = pl->d_sumshift;
+  a.ey = pl->d_ey;
+  a.n = pl->n;
+  a.ldn = pl->ldn;
+  a.H = pl->H;
+  a.mbf = (float)(-0.5 * (double)pl->p.bfactor / pl->n / pl->n);
+  a.partial = pl->d_opart;
+  a.partialJ = pl->d_opart + (size_t)pl->H * nf * 5;
+  a.out = pl->d_oout;
+  LAUNCH(pl, MC_K_OBJECTIVE, (double)(nf + 1) * pl->H * pl->n * sizeof(float2), mc::launch_objective(a, pl->st));
+  std::vector<double> out((size_t)nf * 5 + 1);
+  CK(cudaMemcpyAsync(out.data(), pl->d_oout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CKR(pl->collect());
+  if (J) *J = out[(size_t)nf * 5];
+  for (int k = 0; k < nf; k++) {
+    if (grad) {
+      grad[2 * k] = out[5 * k];
+      grad[2 * k + 1] = out[5 * k + 1];
+    }
+    if (hess) {
+      hess[3 * k] = out[5 * k + 2];
+      hess[3 * k + 1] = out[5 * k + 3];
+      hess[3 * k + 2] = out[5 * k + 4];
+    }
+  }
+  return MC_OK;
+}
+
+int mc_plan_objective(mc_plan* pl, const double* shifts_xy, double* J, double* grad, double* hess) {
+  if (!pl || !shifts_xy) return set_err(MC_E_ARG, "null argument");
+  if (!pl->have_forward) return set_err(MC_E_STATE, "objective before forward");
+  CK(cudaSetDevice(pl->device));
+  std::vector<cplx> s(pl->nframe);
+  for (int k = 0; k < pl->nframe; k++) s[k] = cplx(shifts_xy[2 * k], shifts_xy[2 * k + 1]);
+  return objective(pl, s, J, grad, hess);
+}
+
+// Block-Newton ascent of J over every frame's sum shift, starting from the
+// peak-fit solution; frame 0 stays the reference of the refined shifts.
+int mc_plan_refine(mc_plan* pl, int iterations) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_iter) return set_err(MC_E_STATE, "refine before the peak-fit shifts are final");
+  CK(cudaSetDevice(pl->device));
+  const int nf = pl->nframe;
+  std::vector<cplx> s(nf);
+  for (int k = 0; k < nf; k++) s[k] = -pl->frame_shift[k];
+  std::vector<double> g(2 * (size_t)nf), h(3 * (size_t)nf);
+  double J = 0.0, maxd = 0.0;
+  int it;
+  CK(cudaEventRecord(pl->ev[4], pl->st));
+  for (it = 0; it < iterations; it++) {
+    CKR(objective(pl, s, &J, g.data(), h.data()));
+    maxd = 0.0;
+    for (int k = 0; k < nf; k++) {
+      const double a = h[3 * k], b = h[3 * k + 1], c = h[3 * k + 2];
+      const double det = a * c - b * b;
+      if (!(a < 0.0 && det > 0.0)) continue;  // not at a local maximum in this frame: leave it
+      double dx = -(c * g[2 * k] - b * g[2 * k + 1]) / det;
+      double dy = -(-b * g[2 * k] + a * g[2 * k + 1]) / det;
+      const double len = std::sqrt(dx * dx + dy * dy);
+      if (len > 0.25) {  // trust region of a quarter pixel per step
+        dx *= 0.25 / len;
+        dy *= 0.25 / len;
+      }
+      s[k] += cplx(dx, dy);
+      maxd = std::max(maxd, std::sqrt(dx * dx + dy * dy));
+    }
+    if (maxd < 1e-4) {
+      it++;
+      break;
+    }
+  }
+  CK(cudaEventRecord(pl->ev[5], pl->st));
+  CK(cudaEventSynchronize(pl->ev[5]));
+  CK(cudaEventElapsedTime(&pl->tm.refine_ms, pl->ev[4], pl->ev[5]));
+  for (int k = 0; k < nf; k++) pl->frame_shift[k] = s[0] - s[k];
+  for (int k = 0; k < nf - 1; k++) pl->shift[k] = pl->frame_shift[k + 1] - pl->frame_shift[k];
+  pl->log("\nGradient refinement: %d Newton step(s), last max update %.5f px, objective %.6e\n", it, maxd, J);
+  for (int k = 0; k < nf; k++)
+    pl->log("......Refined shift of Frame #%03d : %8.4f %8.4f\n", k + pl->nstart, pl->frame_shift[k].real(),
+            pl->frame_shift[k].imag());
+  return MC_OK;
+}
+
 int mc_plan_run(mc_plan* pl, float* image_host) {
   if (!pl) return set_err(MC_E_ARG, "null plan");
   pl->log("Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", pl->nx, pl->ny, pl->nz, pl->mode);
@@ -1176,8 +1280,10 @@ int mc_plan_run(mc_plan* pl, float* image_host) {
   CKR(mc_plan_pairs(pl));
   CKR(mc_plan_solve(pl));
   CKR(mc_plan_iterate(pl));
+  pl->tm.refine_ms = 0.f;
+  if (pl->p.refine) CKR(mc_plan_refine(pl, 4));
   CKR(mc_plan_sum(pl, image_host));
-  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.sum_ms;
+  pl->tm.total_ms = pl->tm.forward_ms + pl->tm.pairs_ms + pl->tm.iterate_ms + pl->tm.refine_ms + pl->tm.sum_ms;
   return MC_OK;
 }
 
@@ -1294,7 +1400,7 @@ int mc_plan_kernel_stats(const mc_plan* pl, int kind, double* ms, long long* lau
 
 const char* mc_kernel_name(int kind) {
   static const char* names[MC_KERNEL_KINDS] = {"k_fwd_rows", "k_rows_fft", "k_pair_cols", "k_pair_rows",
-                                               "k_peak", "k_shift_sum", "k_c2r_rows"};
+                                               "k_peak", "k_shift_sum", "k_c2r_rows", "k_objective"};
   return (kind >= 0 && kind < MC_KERNEL_KINDS) ? names[kind] : "";
 }
 

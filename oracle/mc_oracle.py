@@ -367,6 +367,42 @@ def spectrum_to_image(Fsum: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
+# frame-to-sum objective of the added gradient refinement (no reference
+# counterpart: north-star method 3), FP64
+# ---------------------------------------------------------------------------
+def sum_objective(F: list, shifts: np.ndarray, bfactor: float):
+    """J(s) = sum_w h(kx) w(kx,ky) |S|^2 with S = sum_k F_k exp(+i w.s_k),
+    w the B-factor weight exp(-0.5*bft*r^2/n^2) and h the half-spectrum
+    multiplicity (1 at kx = 0, n/2; 2 otherwise).  Returns (J, grad (F, 2),
+    hess (F, 3) = (xx, xy, yy) diagonal 2x2 blocks) where, with
+    P_k = F_k exp(i w.s_k) and u_k = conj(S - P_k) P_k,
+        grad_k = -2 sum h w  w_vec Im(u_k),  hess_k = -2 sum h w w_vec w_vec^T Re(u_k).
+    """
+    n = F[0].shape[0]
+    ky = np.arange(n)
+    y = np.where(ky < n // 2, ky, ky - n)[:, None].astype(np.float64)
+    x = np.arange(n // 2 + 1)[None, :].astype(np.float64)
+    wgt = np.exp(-0.5 * float(bfactor) / n / n * (x * x + y * y))
+    h = np.where((x == 0) | (x == n // 2), 1.0, 2.0)
+    hw = h * wgt
+    ox = 2.0 * math.pi * x / n
+    oy = 2.0 * math.pi * y / n
+    P = [Fk * np.exp(1j * (ox * s[0] + oy * s[1])) for Fk, s in zip(F, shifts)]
+    S = np.sum(P, axis=0)
+    J = float(np.sum(hw * np.abs(S) ** 2))
+    grad = np.zeros((len(F), 2))
+    hess = np.zeros((len(F), 3))
+    for k, Pk in enumerate(P):
+        u = np.conj(S - Pk) * Pk
+        grad[k, 0] = -2.0 * np.sum(hw * ox * u.imag)
+        grad[k, 1] = -2.0 * np.sum(hw * oy * u.imag)
+        hess[k, 0] = -2.0 * np.sum(hw * ox * ox * u.real)
+        hess[k, 1] = -2.0 * np.sum(hw * ox * oy * u.real)
+        hess[k, 2] = -2.0 * np.sum(hw * oy * oy * u.real)
+    return J, grad, hess
+
+
+# ---------------------------------------------------------------------------
 # whole movie
 # ---------------------------------------------------------------------------
 @dataclass

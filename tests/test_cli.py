@@ -1,0 +1,97 @@
+"""dosefgpu_driftcorr CLI: flags, defaults, aborts and the parameter log of
+dosefgpu_driftcorr.cpp (CPU: every case here stops before the GPU), and a
+full run on a small stack (GPU)."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from motioncorr1exp_b200 import api, mrc, synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "motioncorr1exp_b200", "lib", "dosefgpu_driftcorr")
+
+
+def run(args, cwd):
+    r = subprocess.run([CLI] + args, cwd=cwd, capture_output=True, text=True, timeout=300)
+    return r.returncode, r.stdout + r.stderr
+
+
+@pytest.fixture
+def stack(tmp_path):
+    frames = np.random.default_rng(0).integers(0, 5, (6, 40, 48)).astype(np.uint8)
+    p = tmp_path / "movie.mrc"
+    mrc.write_stack(str(p), frames, 0)
+    return p
+
+
+def test_usage_without_arguments(tmp_path):
+    rc, out = run([], tmp_path)
+    assert rc == 0
+    assert "-fod       2" in out and "-bft       150" in out and "-pbx       96" in out
+
+
+@pytest.mark.parametrize("args,msg", [
+    (["-fod"], "Wrong number of arguments. Abort."),
+    (["-xyz", "1"], "Undefined option: -xyz .Abort."),
+    (["-fod", "3"], "Frame distance offset is too big or less than 0. Abort"),
+    (["-fod", "-1"], "Frame distance offset is too big or less than 0. Abort"),
+    (["-scx", "0.5"], "Stretching factor along X-axis needs to be >=1.0."),
+    (["-scy", "0.9"], "Stretching factor along Y-axis needs to be >=1.0."),
+    (["-2es", "5", "-nes", "4"], "Last frame # for the second sum image cannot be larger"),
+])
+def test_abort_messages(stack, args, msg):
+    rc, out = run([str(stack)] + args, stack.parent)
+    assert rc == 1
+    assert msg in out
+    assert "Error: Have wrong parameters. Abort!" in out
+
+
+def test_bin_clamp_messages(stack):
+    rc, out = run([str(stack), "-bin", "3", "-fod", "9"], stack.parent)
+    assert "Larger than maximum binning 2. Set to 2." in out
+    rc, out = run([str(stack), "-bin", "0.5", "-fod", "9"], stack.parent)
+    assert "Smaller than minimum binning 1. Set to 1." in out
+
+
+def test_not_a_stack(tmp_path):
+    p = tmp_path / "one.mrc"
+    mrc.write_stack(str(p), np.zeros((1, 8, 8), np.uint8), 0)
+    rc, out = run([str(p)], tmp_path)
+    assert rc == 1 and "Not a stack or wrong file. Abort" in out
+
+
+def test_parameter_log_and_default_names(stack, tmp_path):
+    # valid parameters: ShowPara writes the log before the alignment starts
+    subprocess.run([CLI, str(stack), "-fod", "1", "-bft", "120", "-nst", "1", "-dsp", "0"], cwd=tmp_path,
+                   capture_output=True, text=True, timeout=300)
+    log = (tmp_path / "movie_Log.txt").read_text()
+    assert log.startswith("******Parameter List******\n")
+    assert f"Input:  {stack}\n" in log
+    assert "  -bft  120.000000\n" in log
+    assert "  -fod  1\n" in log
+    assert "  -nst  1\n" in log
+    assert "  -ned  5\n" in log           # repaired by VerifyPara
+    assert "  -fcs  movie_SumCorr.mrc\n" in log
+    assert "  -dsp  0\n" in log
+    assert "******Parameter End******\n" in log
+
+
+@pytest.mark.gpu
+def test_cli_full_run_matches_api(gpu, tmp_path):
+    mv = synth.make_movie(200, 190, 8, mean=2.0, seed=4, dtype="u8", speed=0.8, rw_sigma=0.3)
+    p = tmp_path / "m.mrc"
+    mrc.write_stack(str(p), mv.frames, 0)
+    rc, out = run([str(p), "-pbx", "64", "-fod", "2", "-dsp", "0", "-fcs", "sum.mrc", "-flg", "log.txt"], tmp_path)
+    assert rc == 0, out
+    img = mrc.read_image(str(tmp_path / "sum.mrc"))
+    res = api.align(mv.frames, 0, api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2), 8))
+    np.testing.assert_allclose(img, res["image"], rtol=0, atol=1e-5 * np.abs(res["image"]).max())
+    log = (tmp_path / "log.txt").read_text()
+    got = [(float(a), float(b)) for a, b in re.findall(r"Shift of Frame #\d{3} : +(\S+) +(\S+)", log)]
+    np.testing.assert_allclose(np.array(got), np.round(res["frame_shifts"], 4), atol=1.1e-4)
+    assert "Save Sum to: sum.mrc" in log and "Done." in log
+    h = mrc.read_header(str(tmp_path / "sum.mrc"))
+    assert int(h["mode"]) == 2 and bytes(h["map"]) == b""

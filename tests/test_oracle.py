@@ -235,6 +235,29 @@ def test_iterative_realignment_keeps_exact_solution():
     assert r.iter_log and r.iter_log[-1]["converged"]
 
 
+def test_sum_objective_derivatives_by_finite_differences():
+    rng = np.random.default_rng(8)
+    n = 32
+    F = [np.fft.rfft2(rng.standard_normal((n, n))) for _ in range(4)]
+    s = rng.uniform(-1, 1, (4, 2))
+    J, g, h = O.sum_objective(F, s, 60.0)
+    eps = 1e-5
+    for k in range(4):
+        for c in range(2):
+            sp, sm = s.copy(), s.copy()
+            sp[k, c] += eps
+            sm[k, c] -= eps
+            Jp, gp, _ = O.sum_objective(F, sp, 60.0)
+            Jm, gm, _ = O.sum_objective(F, sm, 60.0)
+            assert (Jp - Jm) / (2 * eps) == pytest.approx(g[k, c], rel=1e-6, abs=1e-6 * abs(J))
+            # d grad_k / d s_k,c gives the Hessian block column c
+            dg = (gp[k] - gm[k]) / (2 * eps)
+            hc = [h[k, 0], h[k, 1]] if c == 0 else [h[k, 1], h[k, 2]]
+            np.testing.assert_allclose(dg, hc, rtol=1e-5, atol=1e-6 * np.abs(h).max())
+    # a common translation of every frame leaves J unchanged
+    assert O.sum_objective(F, s + 0.37, 60.0)[0] == pytest.approx(J, rel=1e-12)
+
+
 def test_apply_refs_two_reference_scheme():
     raw = np.arange(12, dtype=np.float64).reshape(3, 4)
     dark = np.full((3, 4), 1.0)
