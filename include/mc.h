@@ -208,6 +208,80 @@ int mc_pair_window_static(const void* d_spec_a, const void* d_spec_b, int n, int
  * (un-normalised; inverse = exp(+2 pi i)).  Stream may be NULL. */
 int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void* stream);
 
+/* ---------------------------------------------------------------- batching --
+ * No counterpart in the reference, which aligns one movie per process
+ * (dosefgpu_driftcorr.cpp:121-515).  These entry points serve many movies
+ * from one process without reallocating per movie. */
+
+/* Re-targets a plan at another frame range / stack depth of the same
+ * geometry (crop, bin, pbx, bft, nps and GPU must match the plan's; nStart,
+ * nEnd, nStartSum, nEndSum, fod, kit, atm, itr, ith and refine may change).
+ * The new range must fit the plan's capacity (mc_plan_create_capacity).
+ * Frames must be loaded or bound again afterwards. */
+int mc_plan_reframe(mc_plan* plan, const mc_params* p, int nz);
+
+/* mc_plan_create with device buffers sized for up to cap_frames aligned
+ * frames and cap_pairs frame pairs (0 = this run's counts). */
+int mc_plan_create_capacity(const mc_params* p, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                            mc_plan** out);
+
+/* Reads the run's frames (positions nStart..nEnd, nx*ny pixels each in the
+ * plan's MRC mode, back to back) in place from caller device memory on the
+ * plan's GPU instead of the plan's own frame buffer; the memory must stay
+ * valid and unchanged until the run returns.  NULL unbinds.  A later
+ * mc_plan_load_frames* or mc_plan_run_host switches back to the plan's
+ * buffer. */
+int mc_plan_bind_frames_device(mc_plan* plan, const void* d_frames);
+
+/* Pair-stage schedule for one binned side n, as chosen by the autotuner
+ * (motioncorr1exp_b200/autotune.py): process-wide, read by plans created
+ * afterwards. */
+typedef struct mc_schedule {
+  int n;             /* binned side the entry applies to */
+  int pair_q;        /* codelet length Q of the split n = P*Q (0 = built-in cost model) */
+  int pairs_per_cta; /* pairs per CTA of the pair column stage (0 = 32) */
+  int pair_variant;  /* 0 register codelets, 1 grouped cp.async (even n) */
+} mc_schedule;
+int mc_schedule_set(const mc_schedule* s); /* replaces the entry for s->n */
+int mc_schedule_get(int n, mc_schedule* out); /* MC_E_ARG when none is set */
+void mc_schedule_clear(void);
+/* Codelet lengths Q the pair column stage accepts for side n; returns the
+ * count (at most max written to q_out). */
+int mc_schedule_candidates(int n, int* q_out, int max);
+
+typedef struct mc_batch mc_batch;
+
+typedef struct mc_batch_job {
+  const void* frames;    /* the run's frames (positions nStart..nEnd), back to back */
+  int on_device;         /* 1: frames is device memory of params.GPUNum, read in place */
+  int nx, ny, nz, mode;  /* stack geometry and MRC pixel mode */
+  mc_params params;      /* as mc_verify_params left them; no dark/gain references */
+  float* image;          /* out: nsam*nsam host floats, or NULL */
+  double* frame_shifts;  /* out: 2*nframe host doubles ("Shift of Frame"), or NULL */
+} mc_batch_job;
+
+typedef struct mc_batch_result {
+  int status;            /* MC_OK or the movie's error code */
+  int nsam, nframe, npairs;
+  int lane;              /* lane that ran the movie */
+  double start_ms;       /* host clock, from the start of mc_batch_run */
+  double end_ms;         /* results on the host */
+  float gpu_ms;          /* device time of the movie (CUDA events) */
+  char message[160];     /* mc_last_error() text of a failed movie */
+} mc_batch_result;
+
+/* A batch runner with `lanes` worker threads on one GPU, each with its own
+ * stream and its own plans (one per stack geometry, kept across runs and
+ * replayed as CUDA graphs per frame configuration). */
+int mc_batch_create(int device, int lanes, mc_batch** out);
+void mc_batch_destroy(mc_batch* b);
+/* Aligns every job; lanes take jobs in order from a shared queue.  Returns
+ * MC_OK when every movie succeeded, else the first failing movie's code
+ * (the others still run; see results[i].status). */
+int mc_batch_run(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results);
+/* Device memory held by the runner's plans. */
+size_t mc_batch_device_bytes(const mc_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,22 @@ class McTimings(C.Structure):
                 ("refine_ms", C.c_float)]
 
 
+class McSchedule(C.Structure):
+    _fields_ = [("n", C.c_int), ("pair_q", C.c_int), ("pairs_per_cta", C.c_int), ("pair_variant", C.c_int)]
+
+
+class McBatchJob(C.Structure):
+    _fields_ = [("frames", C.c_void_p), ("on_device", C.c_int),
+                ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("mode", C.c_int),
+                ("params", McParams), ("image", C.c_void_p), ("frame_shifts", C.c_void_p)]
+
+
+class McBatchResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("nsam", C.c_int), ("nframe", C.c_int), ("npairs", C.c_int),
+                ("lane", C.c_int), ("start_ms", C.c_double), ("end_ms", C.c_double), ("gpu_ms", C.c_float),
+                ("message", C.c_char * 160)]
+
+
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 
 # name -> (restype, argtypes)
@@ -88,6 +104,18 @@ SIGNATURES = {
     "mc_pair_window_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p,
                                         C.c_void_p]),
     "mc_fft1d": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mc_plan_reframe": (C.c_int, [C.c_void_p, C.POINTER(McParams), C.c_int]),
+    "mc_plan_create_capacity": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.POINTER(C.c_void_p)]),
+    "mc_plan_bind_frames_device": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mc_schedule_set": (C.c_int, [C.POINTER(McSchedule)]),
+    "mc_schedule_get": (C.c_int, [C.c_int, C.POINTER(McSchedule)]),
+    "mc_schedule_clear": (None, []),
+    "mc_schedule_candidates": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_int]),
+    "mc_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mc_batch_destroy": (None, [C.c_void_p]),
+    "mc_batch_run": (C.c_int, [C.c_void_p, C.POINTER(McBatchJob), C.c_int, C.POINTER(McBatchResult)]),
+    "mc_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
 }
 
 

@@ -74,19 +74,38 @@ class Plan:
     """One stack geometry on one GPU (mc_plan_create)."""
 
     def __init__(self, params: Params, nx: int, ny: int, nz: int, mode: int,
-                 log: Optional[Callable[[str], None]] = None):
+                 log: Optional[Callable[[str], None]] = None, cap_frames: int = 0, cap_pairs: int = 0):
         self._lib = L.lib()
         h = C.c_void_p()
         c = params.to_c()
-        L.check(self._lib.mc_plan_create(C.byref(c), nx, ny, nz, mode, C.byref(h)))
+        if cap_frames or cap_pairs:
+            L.check(self._lib.mc_plan_create_capacity(C.byref(c), nx, ny, nz, mode, cap_frames, cap_pairs,
+                                                      C.byref(h)))
+        else:
+            L.check(self._lib.mc_plan_create(C.byref(c), nx, ny, nz, mode, C.byref(h)))
         self._h = h
         self.params = params
         self._logcb = None
         if log is not None:
             self.set_log(log)
+        self._refresh_info()
+
+    def _refresh_info(self) -> None:
         info = L.McInfo()
         L.check(self._lib.mc_plan_info(self._h, C.byref(info)))
         self.info = {f: getattr(info, f) for f, _ in L.McInfo._fields_}
+
+    def reframe(self, params: Params, nz: int) -> None:
+        """New frame range / pair distance / threshold on the same geometry
+        (mc_plan_reframe); frames must be loaded or bound again."""
+        c = params.to_c()
+        L.check(self._lib.mc_plan_reframe(self._h, C.byref(c), nz))
+        self.params = params
+        self._refresh_info()
+
+    def bind_frames_device(self, dev_ptr: int) -> None:
+        """Read the run's frames in place from device memory (0 unbinds)."""
+        L.check(self._lib.mc_plan_bind_frames_device(self._h, C.c_void_p(dev_ptr) if dev_ptr else None))
 
     # -- lifecycle
     def close(self) -> None:
@@ -286,6 +305,106 @@ def solve_pairs(nframe: int, pairs: np.ndarray, shifts: np.ndarray, kithresh: fl
     L.check(L.lib().mc_solve_pairs(nframe, P, _ptr(ij), _ptr(sh), kithresh, _ptr(step), _ptr(ki1),
                                    C.byref(nk), _ptr(kept), _ptr(ki2)))
     return {"step": step, "ki1": ki1, "kept": kept[: nk.value].copy(), "ki2": ki2[: nk.value].copy()}
+
+
+def schedule_set(n: int, pair_q: int = 0, pairs_per_cta: int = 0, pair_variant: int = 0) -> None:
+    """Pair-stage schedule for binned side n, used by plans created afterwards."""
+    L.check(L.lib().mc_schedule_set(C.byref(L.McSchedule(n, pair_q, pairs_per_cta, pair_variant))))
+
+
+def schedule_get(n: int) -> Optional[dict]:
+    s = L.McSchedule()
+    if L.lib().mc_schedule_get(n, C.byref(s)) != L.MC_OK:
+        return None
+    return {f: getattr(s, f) for f, _ in L.McSchedule._fields_}
+
+
+def schedule_clear() -> None:
+    L.lib().mc_schedule_clear()
+
+
+def schedule_candidates(n: int) -> list[int]:
+    """Codelet lengths Q the pair column stage takes for side n."""
+    cnt = L.lib().mc_schedule_candidates(n, None, 0)
+    q = (C.c_int * max(cnt, 1))()
+    L.lib().mc_schedule_candidates(n, q, cnt)
+    return list(q[:cnt])
+
+
+class Batch:
+    """Many movies on one GPU (mc_batch_*): `lanes` worker threads, each with
+    its own stream and plans reused across movies of a geometry."""
+
+    def __init__(self, device: int = 0, lanes: int = 2):
+        self._lib = L.lib()
+        h = C.c_void_p()
+        L.check(self._lib.mc_batch_create(device, lanes, C.byref(h)))
+        self._h = h
+        self.device = device
+        self.lanes = lanes
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.mc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.mc_batch_device_bytes(self._h))
+
+    def run(self, movies: list[dict], check: bool = True) -> list[dict]:
+        """movies: dicts with `params` (verified Params), `nx`, `ny`, `nz`,
+        `mode` and either `frames` (host array of the run's positions) or
+        `device_ptr` (device address of them); optional `image` (float32
+        nsam x nsam) and `frame_shifts` (float64 nframe x 2) outputs.
+        Returns per movie: status, nsam, nframe, npairs, lane, start_ms,
+        end_ms, gpu_ms, message."""
+        n = len(movies)
+        jobs = (L.McBatchJob * max(n, 1))()
+        res = (L.McBatchResult * max(n, 1))()
+        keep = []
+        for i, m in enumerate(movies):
+            j = jobs[i]
+            if "device_ptr" in m:
+                j.frames = C.c_void_p(int(m["device_ptr"]))
+                j.on_device = 1
+            else:
+                a = np.ascontiguousarray(m["frames"])
+                keep.append(a)
+                j.frames = C.c_void_p(a.ctypes.data)
+                j.on_device = 0
+            j.nx, j.ny, j.nz, j.mode = m["nx"], m["ny"], m["nz"], m["mode"]
+            j.params = m["params"].to_c()
+            for key in ("image", "frame_shifts"):
+                arr = m.get(key)
+                if arr is not None:
+                    want = np.float32 if key == "image" else np.float64
+                    if arr.dtype != want or not arr.flags["C_CONTIGUOUS"]:
+                        raise ValueError(f"{key} must be a C-contiguous {np.dtype(want).name} array")
+                    setattr(j, key, C.c_void_p(arr.ctypes.data))
+        rc = self._lib.mc_batch_run(self._h, jobs, n, res)
+        out = []
+        for i in range(n):
+            r = res[i]
+            out.append({"status": r.status, "nsam": r.nsam, "nframe": r.nframe, "npairs": r.npairs,
+                        "lane": r.lane, "start_ms": r.start_ms, "end_ms": r.end_ms, "gpu_ms": r.gpu_ms,
+                        "message": r.message.decode(errors="replace")})
+        if check and rc != L.MC_OK:
+            bad = next(o for o in out if o["status"] != L.MC_OK)
+            raise L.McError(rc, bad["message"])
+        return out
 
 
 def fft1d(d_in: int, d_out: int, n: int, batch: int, inverse: bool, stream: int = 0) -> None:

@@ -152,6 +152,36 @@ struct ObjectiveArgs {
   double* out;           // [nframes][5] (with the -2) then J at out[5*nframes]
 };
 cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st);
+
+// ------------------------------------------------------------ device solve --
+// Single-CTA FP64 drift solve + sum-shift preparation (mc_solve.cu).
+struct SolveArgs {
+  const int2* pairs;     // (i, j), i < j
+  int npairs;
+  const float* pshift;   // [P][2] measured pair shifts
+  int nframe;
+  float kithresh;
+  int align_to_mid, mid_steps, sum_first, sum_last;
+  // scratch
+  double* M;             // [(nframe-1)^2]
+  double* rhs;           // [2 (nframe-1)]
+  double* work;          // [2 (nframe-1) + 2 nframe]
+  int* mask;             // [P]
+  int* order;            // [P]
+  int* uf;               // [nframe]
+  // outputs
+  double* ki1;           // [P]
+  int* kept;             // [P] kept rows, ascending (first *nkept valid)
+  int* nkept;
+  double* ki2;           // [P] residuals of the kept rows
+  double* shift;         // [nframe-1][2] per-step shifts
+  double* frame_shift;   // [nframe][2]
+  double2* sum_shift;    // [sum_last - sum_first + 1]
+  int* sum_frames;
+  int* sum_apply;
+  int* status;           // 0 ok, -6 singular system
+};
+cudaError_t launch_solve(const SolveArgs& a, cudaStream_t st);
 cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st);
 
 cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st);

@@ -13,7 +13,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -150,16 +152,31 @@ double radix_cost(int r) {
   }
 }
 
+// Pair-stage schedules by binned side n (mc_schedule_set): the autotuner's
+// choices, read when a plan is created.
+std::mutex g_sched_mu;
+std::map<int, mc_schedule> g_sched;
+
+bool find_schedule(int n, mc_schedule* out) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  auto it = g_sched.find(n);
+  if (it == g_sched.end()) return false;
+  *out = it->second;
+  return true;
+}
+
 // n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
 void choose_prune(int n, int box, int& P, int& Q) {
-  // MC_PRUNE_Q=<q> forces the split n = (n/q)*q when the codelet kernel takes it
-  if (const char* env = getenv("MC_PRUNE_Q")) {
-    const int q = atoi(env);
-    if (q > 1 && n % q == 0 && mc::pair_cols_reg_supported(n / q, q)) {
-      P = n / q;
-      Q = q;
-      return;
-    }
+  // MC_PRUNE_Q=<q> forces the split n = (n/q)*q when the codelet kernel takes
+  // it; next a schedule set for this n
+  int want = 0;
+  if (const char* env = getenv("MC_PRUNE_Q")) want = atoi(env);
+  mc_schedule sc;
+  if (want <= 0 && find_schedule(n, &sc)) want = sc.pair_q;
+  if (want > 1 && n % want == 0 && mc::pair_cols_reg_supported(n / want, want)) {
+    P = n / want;
+    Q = want;
+    return;
   }
   // first choice: a split the register-codelet kernel handles
   double best = 1e300;
@@ -237,6 +254,8 @@ struct mc_plan {
   mc_params p{};
   int nx = 0, ny = 0, nz = 0, mode = 0, wl = 0;
   int nstart = 0, nend = 0, nframe = 0;
+  int cap_frames = 0, cap_pairs = 0;  // buffer capacities (mc_plan_reframe stays within them)
+  int ppc = 32;                       // pairs per CTA of the pair column stage
   int nu = 0, n = 0, H = 0, ldn = 0, ldu = 0, ldt2 = 0;
   int box = 0, ystart = 0, P = 1, Q = 1;
   bool two_sets = false;
@@ -256,6 +275,7 @@ struct mc_plan {
 
   // device memory
   void* d_frames = nullptr;
+  const void* frames_src = nullptr;  // bound caller device frames (mc_plan_bind_frames_device) or null
   float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
   float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
   float2 *d_tw_nu = nullptr, *d_tw_n = nullptr, *d_twQ = nullptr, *d_twO = nullptr, *d_cs = nullptr;
@@ -273,6 +293,27 @@ struct mc_plan {
   double2* d_sumshift = nullptr;
   double* d_opart = nullptr;  // objective partials [H][nframe][5] + [H]
   double* d_oout = nullptr;   // objective totals [nframe][5] + J
+
+  // device-only movie pipeline (forward -> pairs -> device solve -> sum)
+  int2* d_pairs_main = nullptr;  // the plan's pair list, uploaded once
+  double *d_M = nullptr, *d_rhs = nullptr, *d_work = nullptr, *d_ki1 = nullptr, *d_ki2 = nullptr;
+  double *d_dshift = nullptr, *d_dfshift = nullptr;
+  int *d_mask = nullptr, *d_order = nullptr, *d_uf = nullptr, *d_kept = nullptr, *d_nkept = nullptr;
+  int* d_status = nullptr;
+  unsigned char* h_stage = nullptr;  // pinned copies of the per-movie results
+  size_t st_dc = 0, st_pshift = 0, st_pcc = 0, st_ppeak = 0, st_ki1 = 0, st_kept = 0, st_nkept = 0, st_ki2 = 0,
+         st_work = 0, st_status = 0, st_bytes = 0;
+  // captured movie graphs, one per frame configuration (frame range, sum
+  // range, pair distance, threshold, reference frame) the plan has run
+  struct GraphEntry {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+    double kbytes[MC_KERNEL_KINDS] = {};
+    long long kcount[MC_KERNEL_KINDS] = {};
+  };
+  std::vector<GraphEntry> graphs;
+  bool graph_failed = false;
+  bool capturing = false;
   int maxp = 0;
   std::vector<void*> allocs;
 
@@ -316,9 +357,11 @@ struct mc_plan {
     *e = kpool[kused++];
     return MC_OK;
   }
+  double graph_kbytes[MC_KERNEL_KINDS] = {};
+  long long graph_kcount[MC_KERNEL_KINDS] = {};
   int kstart(int kind, int* slot) {
     *slot = -1;
-    if (!profiling) return MC_OK;
+    if (!profiling || capturing) return MC_OK;
     cudaEvent_t e;
     CKR(kevent(&e));
     CK(cudaEventRecord(e, st));
@@ -327,6 +370,11 @@ struct mc_plan {
     return MC_OK;
   }
   int kstop(int kind, int slot, double bytes) {
+    if (capturing) {  // counted once per graph replay instead
+      graph_kcount[kind]++;
+      graph_kbytes[kind] += bytes;
+      return MC_OK;
+    }
     kcount[kind]++;
     kbytes[kind] += bytes;
     if (slot < 0) return MC_OK;
@@ -379,6 +427,9 @@ struct mc_plan {
     for (void* q : allocs) cudaFree(q);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (h_stage) cudaFreeHost(h_stage);
     for (auto& e : kpool) cudaEventDestroy(e);
     for (auto& e : chunk_ev) cudaEventDestroy(e);
     if (start_ev) cudaEventDestroy(start_ev);
@@ -411,17 +462,12 @@ float2* specA_at(mc_plan* pl, int f) { return pl->d_specA + (long long)f * pl->f
 float2* specB_at(mc_plan* pl, int f) { return pl->d_specB + (long long)f * pl->fstride; }
 
 // pair stage over an explicit list: (a-frame, b-frame) into a/b spectrum sets
-int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
-                  const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
-                  std::vector<int>& peak) {
+// Launches the pair kernels for `list`, whose device copy is d_list; results
+// land in d_pshift / d_pcc / d_ppeak.  No host synchronisation.
+int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
+                       const std::vector<mc::PairIJ>& list, const int2* d_list) {
   const int np = (int)list.size();
-  shift.assign(2 * (size_t)np, 0.f);
-  cc.assign(np, 0.f);
-  peak.assign(2 * (size_t)np, 0);
-  std::vector<int2> pr(np);
-  for (int i = 0; i < np; i++) pr[i] = make_int2(list[i].first, list[i].second);
   if (np > pl->maxp) return set_err(MC_E_STATE, "pair list larger than the plan's capacity");
-  CK(cudaMemcpyAsync(pl->d_pairs, pr.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, pl->st));
   const float mbf = (float)(-0.5 * (double)pl->p.bfactor / pl->n / pl->n);
   for (int p0 = 0; p0 < np; p0 += kPairBatch) {
     const int nb = std::min(kPairBatch, np - p0);
@@ -430,9 +476,9 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
     a.strideA = strideA;
     a.specB = specB;
     a.strideB = strideB;
-    a.pairs = pl->d_pairs + p0;
+    a.pairs = d_list + p0;
     a.npairs = nb;
-    a.pairs_per_cta = kPairsPerCta;
+    a.pairs_per_cta = pl->ppc;
     a.n = pl->n;
     a.ldn = pl->ldn;
     a.H = pl->H;
@@ -502,6 +548,22 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
   k.peak = pl->d_ppeak;
   LAUNCH(pl, MC_K_PEAK, (double)np * pl->box * pl->box * sizeof(float) + (double)np * 5 * sizeof(float),
          mc::launch_peak(k, pl->st));
+  return MC_OK;
+}
+
+// pair stage over an explicit list, synchronous, results to the host
+int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
+                  const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
+                  std::vector<int>& peak) {
+  const int np = (int)list.size();
+  shift.assign(2 * (size_t)np, 0.f);
+  cc.assign(np, 0.f);
+  peak.assign(2 * (size_t)np, 0);
+  std::vector<int2> pr(np);
+  for (int i = 0; i < np; i++) pr[i] = make_int2(list[i].first, list[i].second);
+  if (np > pl->maxp) return set_err(MC_E_STATE, "pair list larger than the plan's capacity");
+  CK(cudaMemcpyAsync(pl->d_pairs, pr.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, pl->st));
+  CKR(enqueue_pair_stage(pl, specA, strideA, specB, strideB, list, pl->d_pairs));
   CK(cudaMemcpyAsync(shift.data(), pl->d_pshift, sizeof(float) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
   CK(cudaMemcpyAsync(cc.data(), pl->d_pcc, sizeof(float) * np, cudaMemcpyDeviceToHost, pl->st));
   CK(cudaMemcpyAsync(peak.data(), pl->d_ppeak, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
@@ -616,7 +678,114 @@ void mc_plan_set_log(mc_plan* pl, mc_log_fn fn, void* user) {
 
 void mc_plan_destroy(mc_plan* pl) { delete pl; }
 
+}  // extern "C"
+
+// Frame range and pair list of the run (DFAlign.cu:528-530, mfunc.h:64-84);
+// the buffers were sized for cap_frames / cap_pairs.
+static int configure_frames(mc_plan* pl, const mc_params& q, int nz) {
+  mc_params& p = pl->p;
+  p.nStart = q.nStart;
+  p.nEnd = q.nEnd;
+  p.nStartSum = q.nStartSum;
+  p.nEndSum = q.nEndSum;
+  p.FrameDistOffset = q.FrameDistOffset;
+  p.kiThresh = q.kiThresh;
+  p.bAlignToMid = q.bAlignToMid;
+  pl->nz = nz;
+  pl->nstart = std::max(p.nStart, 0);
+  pl->nend = std::min(p.nEnd, nz - 1);
+  pl->nframe = pl->nend - pl->nstart + 1;
+  if (pl->nframe < 2) return set_err(MC_E_ARG, "need at least two frames (nStart %d, nEnd %d)", pl->nstart, pl->nend);
+  int dist = pl->nframe / 2 - p.FrameDistOffset;
+  if (dist <= 0) dist = 1;
+  if (dist > pl->nframe / 2) dist = pl->nframe / 2;
+  std::vector<mc::PairIJ> pairs;
+  for (int i = 0; i < pl->nframe; i++)
+    for (int j = i + dist; j < pl->nframe; j++) pairs.push_back({i, j});
+  if (pl->cap_frames && (pl->nframe > pl->cap_frames || (int)pairs.size() > pl->cap_pairs))
+    return set_err(MC_E_SIZE, "%d frames / %d pairs exceed the plan's capacity (%d / %d)", pl->nframe,
+                   (int)pairs.size(), pl->cap_frames, pl->cap_pairs);
+  const bool same = pairs == pl->pairs;
+  pl->pairs = pairs;
+  if (pl->d_pairs_main && !same) {
+    std::vector<int2> pr(pairs.size());
+    for (size_t i = 0; i < pairs.size(); i++) pr[i] = make_int2(pairs[i].first, pairs[i].second);
+    CK(cudaMemcpyAsync(pl->d_pairs_main, pr.data(), sizeof(int2) * pr.size(), cudaMemcpyHostToDevice, pl->st));
+    CK(cudaStreamSynchronize(pl->st));
+  }
+  pl->loaded.assign(pl->nframe, 0);
+  pl->frames_src = nullptr;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
+static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                       mc_plan** out);
+
+extern "C" {
+
 int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_plan** out) {
+  return create_plan(pin, nx, ny, nz, mode, 0, 0, out);
+}
+
+int mc_plan_create_capacity(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                            mc_plan** out) {
+  if (cap_frames < 0 || cap_pairs < 0) return set_err(MC_E_ARG, "negative capacity");
+  return create_plan(pin, nx, ny, nz, mode, cap_frames, cap_pairs, out);
+}
+
+int mc_schedule_set(const mc_schedule* s) {
+  if (!s) return set_err(MC_E_ARG, "null schedule");
+  if (s->n < 16 || s->pair_q < 0 || s->pairs_per_cta < 0 || s->pair_variant < 0 || s->pair_variant > 1)
+    return set_err(MC_E_ARG, "bad schedule for n=%d", s->n);
+  if (s->pair_q > 1 && (s->n % s->pair_q || !mc::pair_cols_reg_supported(s->n / s->pair_q, s->pair_q)))
+    return set_err(MC_E_ARG, "pair stage takes no split %d = %d * %d", s->n, s->n / std::max(s->pair_q, 1),
+                   s->pair_q);
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched[s->n] = *s;
+  return MC_OK;
+}
+
+int mc_schedule_get(int n, mc_schedule* out) {
+  if (!out) return set_err(MC_E_ARG, "null argument");
+  if (!find_schedule(n, out)) return set_err(MC_E_ARG, "no schedule set for n=%d", n);
+  return MC_OK;
+}
+
+void mc_schedule_clear(void) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched.clear();
+}
+
+int mc_schedule_candidates(int n, int* q_out, int max) {
+  int c = 0;
+  for (int q = 2; q <= n; q++) {
+    if (n % q || !mc::pair_cols_reg_supported(n / q, q)) continue;
+    if (q_out && c < max) q_out[c] = q;
+    c++;
+  }
+  return c;
+}
+
+int mc_plan_reframe(mc_plan* pl, const mc_params* p, int nz) {
+  if (!pl || !p) return set_err(MC_E_ARG, "null argument");
+  if (nz <= 1) return set_err(MC_E_ARG, "Not a stack or wrong file. Abort");
+  const mc_params& g = pl->p;
+  if (p->crop_offsetx != g.crop_offsetx || p->crop_offsety != g.crop_offsety || p->crop_nsam != g.crop_nsam ||
+      std::fabs(p->bin - pl->binf) > 1e-4f || p->CCPeakSearchDim != g.CCPeakSearchDim ||
+      p->bfactor != g.bfactor || p->NoisePeakSize != g.NoisePeakSize || p->GPUNum != g.GPUNum)
+    return set_err(MC_E_ARG, "reframe changes the plan geometry; create a new plan");
+  CK(cudaSetDevice(pl->device));
+  pl->p.iter = p->iter;
+  pl->p.iterthres = p->iterthres;
+  pl->p.refine = p->refine;
+  return configure_frames(pl, *p, nz);
+}
+
+}  // extern "C"
+
+static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                       mc_plan** out) {
   if (!pin || !out) return set_err(MC_E_ARG, "null argument");
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0) return set_err(MC_E_ARG, "bad stack size %d x %d x %d", nx, ny, nz);
@@ -645,10 +814,6 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
   if (pl->nu <= 0) return set_err(MC_E_ARG, "Error: Wrong image Size.");
   pl->n = (int)((float)pl->nu / p.bin) / 2 * 2;
   if (pl->n < 16) return set_err(MC_E_SIZE, "binned size %d below 16", pl->n);
-  pl->nstart = std::max(p.nStart, 0);
-  pl->nend = std::min(p.nEnd, nz - 1);
-  pl->nframe = pl->nend - pl->nstart + 1;
-  if (pl->nframe < 2) return set_err(MC_E_ARG, "need at least two frames (nStart %d, nEnd %d)", pl->nstart, pl->nend);
   pl->box = p.CCPeakSearchDim;
   if (pl->box < 16 || pl->box > 256 || pl->box > pl->n)
     return set_err(MC_E_SIZE, "-pbx %d outside [16, min(256, %d)]", pl->box, pl->n);
@@ -674,25 +839,27 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
     // measured slower than the ungrouped kernel at n = 3710 (1 CTA per SM:
     // shared-memory bound), so it runs only when asked for
     const char* env = getenv("MC_PAIR_KERNEL");
-    pl->grouped = reg && (pl->n % 2 == 0) && mc::pair_cols_grp_smem(pl->n, 128 / gteam) <= 227 * 1024 &&
-                  env && std::strcmp(env, "grp") == 0;
+    mc_schedule sc{};
+    const bool have_sc = find_schedule(pl->n, &sc);
+    const bool want_grp = env ? std::strcmp(env, "grp") == 0 : (have_sc && sc.pair_variant == 1);
+    pl->grouped = reg && (pl->n % 2 == 0) && mc::pair_cols_grp_smem(pl->n, 128 / gteam) <= 227 * 1024 && want_grp;
+    pl->ppc = (have_sc && sc.pairs_per_cta > 0) ? std::min(sc.pairs_per_cta, 512) : kPairsPerCta;
   }
 
   CK(cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking));
   for (auto& e : pl->ev) CK(cudaEventCreate(&e));
 
-  // pair list (mfunc.h:64-84)
-  int dist = pl->nframe / 2 - p.FrameDistOffset;
-  if (dist <= 0) dist = 1;
-  if (dist > pl->nframe / 2) dist = pl->nframe / 2;
-  for (int i = 0; i < pl->nframe; i++)
-    for (int j = i + dist; j < pl->nframe; j++) pl->pairs.push_back({i, j});
-  pl->maxp = std::max((int)pl->pairs.size(), pl->nframe);
+  // frame range and pair list; capacities default to this run's sizes
+  CKR(configure_frames(pl, p, nz));
+  pl->cap_frames = std::max(cap_frames, pl->nframe);
+  pl->cap_pairs = std::max(cap_pairs, (int)pl->pairs.size());
+  pl->maxp = std::max(pl->cap_pairs, pl->cap_frames);
+  const int capf = pl->cap_frames;
 
   // device buffers
   pl->frame_bytes = (size_t)nx * ny * pl->wl;
-  CKR(pl->alloc(&pl->d_frames, pl->frame_bytes * pl->nframe));
-  CKR(pl->alloc(&pl->d_specA, sizeof(float2) * pl->fstride * pl->nframe));
+  CKR(pl->alloc(&pl->d_frames, pl->frame_bytes * capf));
+  CKR(pl->alloc(&pl->d_specA, sizeof(float2) * pl->fstride * capf));
   pl->d_specB = pl->d_specA;
   if (pl->nu != pl->n) CKR(pl->alloc(&pl->d_T, sizeof(float2) * (size_t)pl->H * pl->ldu));
   CKR(pl->alloc(&pl->d_pairs, sizeof(int2) * pl->maxp));
@@ -704,13 +871,51 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
   CKR(pl->alloc(&pl->d_ppeak, sizeof(int) * 2 * pl->maxp));
   CKR(pl->alloc(&pl->d_sum, sizeof(float2) * pl->fstride));
   CKR(pl->alloc(&pl->d_T2, sizeof(float2) * (size_t)pl->n * pl->ldt2));
-  CKR(pl->alloc(&pl->d_ey, sizeof(float2) * (size_t)pl->nframe * pl->n));
+  CKR(pl->alloc(&pl->d_ey, sizeof(float2) * (size_t)capf * pl->n));
   CKR(pl->alloc(&pl->d_image, sizeof(float) * (size_t)pl->n * pl->n));
-  CKR(pl->alloc(&pl->d_sumframes, sizeof(int) * pl->nframe));
-  CKR(pl->alloc(&pl->d_apply, sizeof(int) * pl->nframe));
-  CKR(pl->alloc(&pl->d_sumshift, sizeof(double2) * pl->nframe));
-  CKR(pl->alloc(&pl->d_opart, sizeof(double) * ((size_t)pl->H * pl->nframe * 5 + pl->H)));
-  CKR(pl->alloc(&pl->d_oout, sizeof(double) * ((size_t)pl->nframe * 5 + 1)));
+  CKR(pl->alloc(&pl->d_sumframes, sizeof(int) * capf));
+  CKR(pl->alloc(&pl->d_apply, sizeof(int) * capf));
+  CKR(pl->alloc(&pl->d_sumshift, sizeof(double2) * capf));
+  CKR(pl->alloc(&pl->d_opart, sizeof(double) * ((size_t)pl->H * capf * 5 + pl->H)));
+  CKR(pl->alloc(&pl->d_oout, sizeof(double) * ((size_t)capf * 5 + 1)));
+  {
+    // device-only pipeline: pair list, solve scratch and pinned result staging
+    const int np = pl->cap_pairs, nf = capf, nc = nf - 1;
+    std::vector<int2> pr(pl->pairs.size());
+    for (size_t i = 0; i < pr.size(); i++) pr[i] = make_int2(pl->pairs[i].first, pl->pairs[i].second);
+    CKR(pl->alloc(&pl->d_pairs_main, sizeof(int2) * np));
+    CKR(upload(pl, pl->d_pairs_main, pr));
+    CKR(pl->alloc(&pl->d_M, sizeof(double) * (size_t)nc * nc));
+    CKR(pl->alloc(&pl->d_rhs, sizeof(double) * 2 * (size_t)nc));
+    CKR(pl->alloc(&pl->d_work, sizeof(double) * (2 * (size_t)nc + 2 * (size_t)nf)));
+    CKR(pl->alloc(&pl->d_ki1, sizeof(double) * np));
+    CKR(pl->alloc(&pl->d_ki2, sizeof(double) * np));
+    CKR(pl->alloc(&pl->d_dshift, sizeof(double) * 2 * (size_t)nc));
+    CKR(pl->alloc(&pl->d_dfshift, sizeof(double) * 2 * (size_t)nf));
+    CKR(pl->alloc(&pl->d_mask, sizeof(int) * np));
+    CKR(pl->alloc(&pl->d_order, sizeof(int) * np));
+    CKR(pl->alloc(&pl->d_uf, sizeof(int) * nf));
+    CKR(pl->alloc(&pl->d_kept, sizeof(int) * np));
+    CKR(pl->alloc(&pl->d_nkept, sizeof(int)));
+    CKR(pl->alloc(&pl->d_status, sizeof(int)));
+    size_t o = 0;
+    auto place = [&](size_t& off, size_t bytes) {
+      off = o;
+      o += (bytes + 15) / 16 * 16;
+    };
+    place(pl->st_dc, sizeof(float2) * nf);
+    place(pl->st_pshift, sizeof(float) * 2 * np);
+    place(pl->st_pcc, sizeof(float) * np);
+    place(pl->st_ppeak, sizeof(int) * 2 * np);
+    place(pl->st_ki1, sizeof(double) * np);
+    place(pl->st_kept, sizeof(int) * np);
+    place(pl->st_nkept, sizeof(int));
+    place(pl->st_ki2, sizeof(double) * np);
+    place(pl->st_work, sizeof(double) * 2 * (size_t)nc);
+    place(pl->st_status, sizeof(int));
+    pl->st_bytes = o;
+    CK(cudaMallocHost(&pl->h_stage, o));
+  }
 
   // tables
   CKR(pl->alloc(&pl->d_tw_nu, sizeof(float2) * pl->nu));
@@ -763,6 +968,8 @@ int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_pl
   *out = guard.release();
   return MC_OK;
 }
+
+extern "C" {
 
 int mc_plan_info(const mc_plan* pl, mc_info* i) {
   if (!pl || !i) return set_err(MC_E_ARG, "null argument");
@@ -822,6 +1029,11 @@ static int load_frames(mc_plan* pl, const void* src, int first, int count, cudaM
                      kind, pl->st));
   // the caller may reuse a host buffer as soon as this returns
   if (kind == cudaMemcpyHostToDevice) CK(cudaStreamSynchronize(pl->st));
+  if (pl->frames_src) {
+    // back to the plan's own frame buffer: nothing of it is loaded yet
+    pl->frames_src = nullptr;
+    pl->loaded.assign(pl->nframe, 0);
+  }
   for (int i = first; i < first + count; i++) pl->loaded[i] = 1;
   pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
   return MC_OK;
@@ -835,18 +1047,36 @@ int mc_plan_load_frames_device(mc_plan* pl, const void* d_frames, int first, int
   return load_frames(pl, d_frames, first, count, cudaMemcpyDeviceToDevice);
 }
 
+int mc_plan_bind_frames_device(mc_plan* pl, const void* d_frames) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (d_frames) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, d_frames) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+        at.device != pl->device) {
+      cudaGetLastError();
+      return set_err(MC_E_ARG, "bound frames are not device memory of GPU %d", pl->device);
+    }
+  }
+  pl->frames_src = d_frames;
+  pl->loaded.assign(pl->nframe, d_frames ? 1 : 0);
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  return MC_OK;
+}
+
 }  // extern "C"
+
+static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEvent_t>* waits, int chunk);
+static bool device_path(const mc_plan* pl);
 
 // Forward transforms of every position.  With `waits`, the plan stream waits
 // for (*waits)[f / chunk] before the first frame of each chunk (pipelined
 // upload); the per-frame means are read back and logged at the end.
-static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
-  CK(cudaEventRecord(pl->ev[0], pl->st));
+static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
   const bool binned = pl->nu != pl->n;
   for (int f = 0; f < pl->nframe; f++) {
     if (waits && f % chunk == 0) CK(cudaStreamWaitEvent(pl->st, (*waits)[f / chunk], 0));
     mc::FwdRowsArgs a{};
-    a.frame = (const char*)pl->d_frames + (size_t)f * pl->frame_bytes;
+    a.frame = (const char*)(pl->frames_src ? pl->frames_src : pl->d_frames) + (size_t)f * pl->frame_bytes;
     a.mode = pl->mode;
     a.nx = pl->nx;
     a.ny = pl->ny;
@@ -914,20 +1144,61 @@ static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int c
       LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, pl->st));
     }
   }
-  CK(cudaEventRecord(pl->ev[1], pl->st));
-  // per-frame mean: Re F(0,0) / n / n (DFAlign.cu:818)
-  std::vector<float2> dc(pl->nframe);
-  CK(cudaMemcpy2DAsync(dc.data(), sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
-                       pl->nframe, cudaMemcpyDeviceToHost, pl->st));
-  CK(cudaStreamSynchronize(pl->st));
-  CKR(pl->collect());
-  CK(cudaEventElapsedTime(&pl->tm.forward_ms, pl->ev[0], pl->ev[1]));
+  return MC_OK;
+}
+
+// pair lines (DFAlign.cu:903-904)
+static void log_pairs(mc_plan* pl) {
+  pl->log("\nCalculate relative drift between frames\n");
+  for (size_t j = 0; j < pl->pairs.size(); j++)
+    pl->log("......%03d Frame #%03d VS #%03d xy-shift: %8.4f %8.4f      CC:%f\n", (int)j,
+            pl->pairs[j].first + pl->nstart, pl->pairs[j].second + pl->nstart, pl->pshift[2 * j],
+            pl->pshift[2 * j + 1], pl->pcc[j]);
+}
+
+// ki lines of both rounds (DFAlign.cu:917-948)
+static void log_solve(mc_plan* pl) {
+  const int np = (int)pl->pairs.size();
+  pl->log("\n......ki: First round \n");
+  double acc = 0;
+  for (int j = 0; j < np; j++) {
+    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4lf \n", j + pl->nstart, pl->pairs[j].first + pl->nstart,
+            pl->pairs[j].second + pl->nstart, pl->ki1[j]);
+    acc += pl->ki1[j];
+  }
+  pl->log("................................Average ki: %8.4lf \n\n", acc / np);
+  pl->log("......ki: Second round \n");
+  acc = 0;
+  for (size_t j = 0; j < pl->good.size(); j++) {
+    const auto& pr = pl->pairs[pl->good[j]];
+    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4f \n", (int)j + pl->nstart, pr.first + pl->nstart,
+            pr.second + pl->nstart, pl->ki2[j]);
+    acc += pl->ki2[j];
+  }
+  pl->log("................................Average ki: %8.4lf \n\n", acc / (double)pl->good.size());
+}
+
+// per-frame mean: Re F(0,0) / n / n (DFAlign.cu:818), from the DC terms
+static void log_frame_means(mc_plan* pl, const float2* dc) {
   pl->frame_mean.resize(pl->nframe);
   pl->log("\nRead stack:\n");
   for (int f = 0; f < pl->nframe; f++) {
     pl->frame_mean[f] = dc[f].x / pl->n / pl->n;
     pl->log("......Read and sum frame #%03d   mean:%f\n", f + pl->nstart, pl->frame_mean[f]);
   }
+}
+
+static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
+  CK(cudaEventRecord(pl->ev[0], pl->st));
+  CKR(enqueue_forward(pl, waits, chunk));
+  CK(cudaEventRecord(pl->ev[1], pl->st));
+  std::vector<float2> dc(pl->nframe);
+  CK(cudaMemcpy2DAsync(dc.data(), sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
+                       pl->nframe, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CKR(pl->collect());
+  CK(cudaEventElapsedTime(&pl->tm.forward_ms, pl->ev[0], pl->ev[1]));
+  log_frame_means(pl, dc.data());
   pl->have_forward = true;
   pl->have_pairs = pl->have_solve = pl->have_iter = false;
   return MC_OK;
@@ -961,6 +1232,7 @@ int mc_plan_run_host(mc_plan* pl, const void* frames, float* image_host) {
   if (!pl->start_ev) CK(cudaEventCreateWithFlags(&pl->start_ev, cudaEventDisableTiming));
   CK(cudaEventRecord(pl->start_ev, pl->st));
   CK(cudaStreamWaitEvent(pl->st_copy, pl->start_ev, 0));
+  pl->frames_src = nullptr;
   for (int c = 0; c < nchunk; c++) {
     const int f0 = c * chunk, cnt = std::min(chunk, pl->nframe - f0);
     CK(cudaMemcpyAsync((char*)pl->d_frames + (size_t)f0 * pl->frame_bytes,
@@ -972,6 +1244,7 @@ int mc_plan_run_host(mc_plan* pl, const void* frames, float* image_host) {
   pl->log("Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", pl->nx, pl->ny, pl->nz, pl->mode);
   pl->log("Crop Image: Offset(%d %d) RawDim(%d) BinnedDim(%d)\n", pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu,
           pl->n);
+  if (device_path(pl)) return run_device(pl, image_host, &pl->chunk_ev, chunk);
   CKR(forward_all(pl, &pl->chunk_ev, chunk));
   CKR(mc_plan_pairs(pl));
   CKR(mc_plan_solve(pl));
@@ -993,11 +1266,7 @@ int mc_plan_pairs(mc_plan* pl) {
   CK(cudaEventRecord(pl->ev[3], pl->st));
   CK(cudaEventSynchronize(pl->ev[3]));
   CK(cudaEventElapsedTime(&pl->tm.pairs_ms, pl->ev[2], pl->ev[3]));
-  pl->log("\nCalculate relative drift between frames\n");
-  for (size_t j = 0; j < pl->pairs.size(); j++)
-    pl->log("......%03d Frame #%03d VS #%03d xy-shift: %8.4f %8.4f      CC:%f\n", (int)j,
-            pl->pairs[j].first + pl->nstart, pl->pairs[j].second + pl->nstart, pl->pshift[2 * j],
-            pl->pshift[2 * j + 1], pl->pcc[j]);
+  log_pairs(pl);
   pl->have_pairs = true;
   pl->have_solve = pl->have_iter = false;
   return MC_OK;
@@ -1015,26 +1284,10 @@ int mc_plan_solve(mc_plan* pl) {
   std::vector<cplx> s;
   if (!mc::lsq_intervals(pl->pairs, all, ncol, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
   pl->ki1 = mc::lsq_residuals(pl->pairs, all, b, s);
-  pl->log("\n......ki: First round \n");
-  double acc = 0;
-  for (int j = 0; j < np; j++) {
-    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4lf \n", j + pl->nstart, pl->pairs[j].first + pl->nstart,
-            pl->pairs[j].second + pl->nstart, pl->ki1[j]);
-    acc += pl->ki1[j];
-  }
-  pl->log("................................Average ki: %8.4lf \n\n", acc / np);
   pl->good = mc::od_threshold(pl->pairs, pl->ki1, pl->nframe, (double)pl->p.kiThresh);
   if (!mc::lsq_intervals(pl->pairs, pl->good, ncol, b, s)) return set_err(MC_E_NUMERIC, "singular pair system");
   pl->ki2 = mc::lsq_residuals(pl->pairs, pl->good, b, s);
-  pl->log("......ki: Second round \n");
-  acc = 0;
-  for (size_t j = 0; j < pl->good.size(); j++) {
-    const auto& pr = pl->pairs[pl->good[j]];
-    pl->log("......ki #%03d of Frame #%03d VS #%03d: %8.4f \n", (int)j + pl->nstart, pr.first + pl->nstart,
-            pr.second + pl->nstart, pl->ki2[j]);
-    acc += pl->ki2[j];
-  }
-  pl->log("................................Average ki: %8.4lf \n\n", acc / (double)pl->good.size());
+  log_solve(pl);
   pl->shift = s;
   pl->have_solve = true;
   pl->have_iter = false;
@@ -1126,41 +1379,66 @@ int mc_plan_iterate(mc_plan* pl) {
   return MC_OK;
 }
 
-int mc_plan_sum(mc_plan* pl, float* image_host) {
-  if (!pl) return set_err(MC_E_ARG, "null plan");
-  if (!pl->have_iter) return set_err(MC_E_STATE, "sum before the shifts are final");
-  CK(cudaSetDevice(pl->device));
+}  // extern "C"
+
+// Frame range of the sum and the steps entering the middle-frame offset
+// (DFAlign.cu:1115-1139); the reference reads past the shift vector when
+// RefFrame - nStart > nframe - 1, here the offset stops at the last step.
+static void sum_range(const mc_plan* pl, int* nss_out, int* nes_out, int* mid_steps) {
   const int nf = pl->nframe;
   const mc_params& p = pl->p;
   int nss = p.nStartSum - pl->nstart;
   int nes = p.nEndSum - pl->nstart;
   if (nss <= 0) nss = 0;
   if (nes <= nss || nes >= nf) nes = nf - 1;
-  pl->log("\nSum Frame #%03d - #%03d\n", nss + pl->nstart, nes + pl->nstart);
-  cplx mid(0, 0);
+  int lim = 0;
   if (p.bAlignToMid) {
     int ref = pl->nz / 2 + 1;
     if (ref < pl->nstart) ref = pl->nstart;
-    // the reference reads past the shift vector when ref-nStart > nframe-1
-    const int lim = std::min(ref - pl->nstart, nf - 1);
-    for (int j = 0; j < lim; j++) mid += pl->shift[j];
+    lim = std::max(0, std::min(ref - pl->nstart, nf - 1));
   }
+  *nss_out = nss;
+  *nes_out = nes;
+  *mid_steps = lim;
+}
+
+// Sum shifts s_k = -total_k + mid of the summed frames with the reference's
+// log lines (DFAlign.cu:1124-1181).
+static void sum_shifts(mc_plan* pl, std::vector<int>& frames, std::vector<cplx>& sh, std::vector<int>& apply) {
+  const int nf = pl->nframe;
+  int nss, nes, lim;
+  sum_range(pl, &nss, &nes, &lim);
+  pl->log("\nSum Frame #%03d - #%03d\n", nss + pl->nstart, nes + pl->nstart);
+  cplx mid(0, 0);
+  for (int j = 0; j < lim; j++) mid += pl->shift[j];
   cplx total(0, 0);
   for (int j = 1; j < nss + 1; j++) total += pl->shift[j - 1];
-  std::vector<int> frames, apply;
-  std::vector<cplx> sh;
+  frames.clear();
+  sh.clear();
+  apply.clear();
   pl->sum_shift.assign(nf, cplx(0, 0));
   for (int k = nss; k <= nes; k++) {
     if (k > nss) total += pl->shift[k - 1];
     const cplx s = -total + mid;
     frames.push_back(k);
     sh.push_back(s);
-    apply.push_back((k == nss && !p.bAlignToMid) ? 0 : 1);
+    apply.push_back((k == nss && !pl->p.bAlignToMid) ? 0 : 1);
     pl->sum_shift[k] = s;
     pl->log("......Add Frame #%03d with xy shift: %8.4lf %8.4lf\n", k + pl->nstart, s.real(), s.imag());
   }
   pl->sum_first = nss;
   pl->sum_last = nes;
+}
+
+extern "C" {
+
+int mc_plan_sum(mc_plan* pl, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_iter) return set_err(MC_E_STATE, "sum before the shifts are final");
+  CK(cudaSetDevice(pl->device));
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  sum_shifts(pl, frames, sh, apply);
   CK(cudaEventRecord(pl->ev[6], pl->st));
   CKR(run_shift_sum(pl, frames, sh, apply, 1));
   CK(cudaEventRecord(pl->ev[7], pl->st));
@@ -1271,11 +1549,209 @@ int mc_plan_refine(mc_plan* pl, int iterations) {
   return MC_OK;
 }
 
+}  // extern "C"
+
+// pairs -> device solve -> sum -> result copies into the pinned staging,
+// all on the plan stream without a host synchronisation.
+static int enqueue_tail(mc_plan* pl) {
+  const int np = (int)pl->pairs.size(), nf = pl->nframe, nc = nf - 1;
+  unsigned char* hs = pl->h_stage;
+  CK(cudaMemcpy2DAsync(hs + pl->st_dc, sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
+                       nf, cudaMemcpyDeviceToHost, pl->st));
+  CKR(enqueue_pair_stage(pl, pl->d_specA, pl->fstride, pl->d_specB, pl->fstride, pl->pairs, pl->d_pairs_main));
+  int nss, nes, lim;
+  sum_range(pl, &nss, &nes, &lim);
+  mc::SolveArgs s{};
+  s.pairs = pl->d_pairs_main;
+  s.npairs = np;
+  s.pshift = pl->d_pshift;
+  s.nframe = nf;
+  s.kithresh = pl->p.kiThresh;
+  s.align_to_mid = pl->p.bAlignToMid ? 1 : 0;
+  s.mid_steps = lim;
+  s.sum_first = nss;
+  s.sum_last = nes;
+  s.M = pl->d_M;
+  s.rhs = pl->d_rhs;
+  s.work = pl->d_work;
+  s.mask = pl->d_mask;
+  s.order = pl->d_order;
+  s.uf = pl->d_uf;
+  s.ki1 = pl->d_ki1;
+  s.kept = pl->d_kept;
+  s.nkept = pl->d_nkept;
+  s.ki2 = pl->d_ki2;
+  s.shift = pl->d_dshift;
+  s.frame_shift = pl->d_dfshift;
+  s.sum_shift = pl->d_sumshift;
+  s.sum_frames = pl->d_sumframes;
+  s.sum_apply = pl->d_apply;
+  s.status = pl->d_status;
+  CK(mc::launch_solve(s, pl->st));
+  mc::ShiftSumArgs a{};
+  a.spec = pl->d_specA;
+  a.stride = pl->fstride;
+  a.frames = pl->d_sumframes;
+  a.shifts = pl->d_sumshift;
+  a.apply = pl->d_apply;
+  a.nsum = nes - nss + 1;
+  a.n = pl->n;
+  a.ldn = pl->ldn;
+  a.H = pl->H;
+  a.mode = 1;
+  a.plan = pl->plan_n;
+  a.tw = pl->d_tw_n;
+  a.out = pl->d_T2;
+  a.ld_out = pl->ldt2;
+  const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);
+  LAUNCH(pl, MC_K_SHIFT_SUM, (double)a.nsum * spec_bytes + spec_bytes, mc::launch_shift_sum(a, pl->d_ey, pl->st));
+  mc::C2rRowsArgs c{};
+  c.t2 = pl->d_T2;
+  c.ld_t2 = pl->ldt2;
+  c.n = pl->n;
+  c.H = pl->H;
+  c.scale = (float)(1.0 / ((double)pl->n * pl->n));
+  c.image = pl->d_image;
+  c.plan = pl->plan_n;
+  c.tw = pl->d_tw_n;
+  LAUNCH(pl, MC_K_C2R_ROWS, spec_bytes + (double)pl->n * pl->n * sizeof(float), mc::launch_c2r_rows(c, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_pshift, pl->d_pshift, sizeof(float) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_pcc, pl->d_pcc, sizeof(float) * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_ppeak, pl->d_ppeak, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_ki1, pl->d_ki1, sizeof(double) * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_kept, pl->d_kept, sizeof(int) * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_nkept, pl->d_nkept, sizeof(int), cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_ki2, pl->d_ki2, sizeof(double) * np, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_work, pl->d_work, sizeof(double) * 2 * (size_t)nc, cudaMemcpyDeviceToHost,
+                     pl->st));
+  CK(cudaMemcpyAsync(hs + pl->st_status, pl->d_status, sizeof(int), cudaMemcpyDeviceToHost, pl->st));
+  return MC_OK;
+}
+
+// After the stream synchronised: results into the plan's host state, with the
+// same log lines as the staged path.
+static int finish_device_movie(mc_plan* pl) {
+  const int np = (int)pl->pairs.size(), nc = pl->nframe - 1;
+  const unsigned char* hs = pl->h_stage;
+  if (*(const int*)(hs + pl->st_status) != 0) return set_err(MC_E_NUMERIC, "singular pair system");
+  log_frame_means(pl, (const float2*)(hs + pl->st_dc));
+  pl->have_forward = true;
+  const float* ps = (const float*)(hs + pl->st_pshift);
+  pl->pshift.assign(ps, ps + 2 * (size_t)np);
+  const float* pc = (const float*)(hs + pl->st_pcc);
+  pl->pcc.assign(pc, pc + np);
+  const int* pk = (const int*)(hs + pl->st_ppeak);
+  pl->ppeak.assign(pk, pk + 2 * (size_t)np);
+  log_pairs(pl);
+  pl->have_pairs = true;
+  const double* k1 = (const double*)(hs + pl->st_ki1);
+  pl->ki1.assign(k1, k1 + np);
+  const int nk = *(const int*)(hs + pl->st_nkept);
+  const int* kp = (const int*)(hs + pl->st_kept);
+  pl->good.assign(kp, kp + nk);
+  const double* k2 = (const double*)(hs + pl->st_ki2);
+  pl->ki2.assign(k2, k2 + nk);
+  log_solve(pl);
+  const double* w = (const double*)(hs + pl->st_work);
+  pl->shift.resize(nc);
+  for (int k = 0; k < nc; k++) pl->shift[k] = cplx(w[k], w[nc + k]);
+  pl->have_solve = true;
+  CKR(mc_plan_iterate(pl));  // itr = 0: the reference's conversions and log lines only
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  sum_shifts(pl, frames, sh, apply);
+  return MC_OK;
+}
+
+// Whole movie on the device with one synchronisation; captured once into a
+// CUDA graph and replayed (unless profiling, MC_NO_GRAPH, or a capture failure).
+static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEvent_t>* waits, int chunk) {
+  const bool graph_ok = !waits && !pl->profiling && !pl->graph_failed && !getenv("MC_NO_GRAPH");
+  CK(cudaEventRecord(pl->ev[0], pl->st));
+  mc_plan::GraphEntry* ge = nullptr;
+  if (graph_ok) {
+    int nss, nes, lim;
+    sum_range(pl, &nss, &nes, &lim);
+    long long kt;
+    float kf = pl->p.kiThresh;
+    std::memcpy(&kt, &kf, sizeof(float));
+    const std::vector<long long> key = {pl->nstart, pl->nend, nss, nes, lim, pl->p.FrameDistOffset,
+                                        pl->p.bAlignToMid ? 1 : 0, kt & 0xffffffffLL,
+                                        (long long)(uintptr_t)pl->frames_src};
+    for (auto& g : pl->graphs)
+      if (g.key == key) ge = &g;
+    if (!ge) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(pl->st, cudaStreamCaptureModeThreadLocal));
+      pl->capturing = true;
+      for (int k = 0; k < MC_KERNEL_KINDS; k++) {
+        pl->graph_kcount[k] = 0;
+        pl->graph_kbytes[k] = 0;
+      }
+      int rc = enqueue_forward(pl, nullptr, 1);
+      if (rc == MC_OK) rc = enqueue_tail(pl);
+      pl->capturing = false;
+      const cudaError_t e = cudaStreamEndCapture(pl->st, &g);
+      cudaGetLastError();
+      cudaGraphExec_t x = nullptr;
+      if (rc == MC_OK && e == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (pl->graphs.size() >= 16) {  // keep the cache bounded: drop the oldest
+          cudaGraphExecDestroy(pl->graphs.front().exec);
+          pl->graphs.erase(pl->graphs.begin());
+        }
+        mc_plan::GraphEntry n;
+        n.key = key;
+        n.exec = x;
+        std::copy(pl->graph_kcount, pl->graph_kcount + MC_KERNEL_KINDS, n.kcount);
+        std::copy(pl->graph_kbytes, pl->graph_kbytes + MC_KERNEL_KINDS, n.kbytes);
+        pl->graphs.push_back(n);
+        ge = &pl->graphs.back();
+      } else {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        pl->graph_failed = true;
+      }
+    }
+  }
+  if (ge) {
+    CK(cudaGraphLaunch(ge->exec, pl->st));
+    for (int k = 0; k < MC_KERNEL_KINDS; k++) {
+      pl->kcount[k] += ge->kcount[k];
+      pl->kbytes[k] += ge->kbytes[k];
+    }
+  } else {
+    CKR(enqueue_forward(pl, waits, chunk));
+    CKR(enqueue_tail(pl));
+  }
+  CK(cudaEventRecord(pl->ev[1], pl->st));
+  if (image_host)
+    CK(cudaMemcpyAsync(image_host, pl->d_image, sizeof(float) * (size_t)pl->n * pl->n, cudaMemcpyDeviceToHost,
+                       pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CKR(pl->collect());
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, pl->ev[0], pl->ev[1]));
+  pl->tm = mc_timings{};
+  pl->tm.total_ms = ms;
+  return finish_device_movie(pl);
+}
+
+static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine && !pl->grouped; }
+
+extern "C" {
+
 int mc_plan_run(mc_plan* pl, float* image_host) {
   if (!pl) return set_err(MC_E_ARG, "null plan");
   pl->log("Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", pl->nx, pl->ny, pl->nz, pl->mode);
   pl->log("Crop Image: Offset(%d %d) RawDim(%d) BinnedDim(%d)\n", pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu,
           pl->n);
+  if (device_path(pl)) {
+    for (int f = 0; f < pl->nframe; f++)
+      if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
+    CK(cudaSetDevice(pl->device));
+    return run_device(pl, image_host, nullptr, 1);
+  }
   CKR(mc_plan_forward(pl));
   CKR(mc_plan_pairs(pl));
   CKR(mc_plan_solve(pl));

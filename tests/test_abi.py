@@ -87,3 +87,34 @@ def test_solve_pairs_matches_oracle(nframe, fod, seed):
 def test_solve_pairs_rejects_bad_pairs():
     with pytest.raises(_lib.McError):
         api.solve_pairs(4, np.array([[2, 1]]), np.zeros((1, 2)))
+
+
+def test_schedule_table_host_only():
+    api.schedule_clear()
+    assert api.schedule_get(3710) is None
+    qs = api.schedule_candidates(3710)
+    assert 70 in qs and 35 in qs and all(3710 % q == 0 for q in qs)
+    api.schedule_set(3710, pair_q=35, pairs_per_cta=16)
+    assert api.schedule_get(3710) == {"n": 3710, "pair_q": 35, "pairs_per_cta": 16, "pair_variant": 0}
+    api.schedule_set(3710, pair_q=70)
+    assert api.schedule_get(3710)["pair_q"] == 70
+    with pytest.raises(_lib.McError):
+        api.schedule_set(3710, pair_q=3)          # 3710 = 1236.67 * 3: no split
+    with pytest.raises(_lib.McError):
+        api.schedule_set(3710, pair_q=2)          # P = 1855 above the codelet team size
+    with pytest.raises(_lib.McError):
+        api.schedule_set(3710, pair_variant=2)
+    api.schedule_clear()
+    assert api.schedule_get(3710) is None
+
+
+def test_batch_requires_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("host-only check")
+    with pytest.raises(_lib.McError):
+        api.Batch(0, 2)
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.mc_batch_create(0, 0, C.byref(h)) == -1   # lanes outside [1, 16]
+    assert L.mc_batch_run(None, None, 0, None) == -1

@@ -67,7 +67,7 @@ def test_torch_autograd_function(gpu):
         J.backward()
         _, g, _ = pl.objective(s.detach().numpy())
         np.testing.assert_allclose(s.grad.numpy(), g, rtol=1e-12, atol=0)
-        assert float(J) == pytest.approx(pl.objective(s.detach().numpy())[0], rel=1e-12)
+        assert float(J.detach()) == pytest.approx(pl.objective(s.detach().numpy())[0], rel=1e-12)
 
 
 def _truth_rmse(shifts, truth):
