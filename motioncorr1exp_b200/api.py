@@ -8,6 +8,7 @@ call goes through the C ABI of libmc.so; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, fields
 from typing import Callable, Optional
 
@@ -70,12 +71,29 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
 
 
+_schedules_loaded = False
+
+
+def _load_schedules() -> None:
+    """Installs the autotuner's cached pair-stage schedules once per process
+    (MC_SCHEDULES=0 keeps the built-in choices)."""
+    global _schedules_loaded
+    if _schedules_loaded:
+        return
+    _schedules_loaded = True
+    if os.environ.get("MC_SCHEDULES", "1") == "0":
+        return
+    from . import autotune
+    autotune.load()
+
+
 class Plan:
     """One stack geometry on one GPU (mc_plan_create)."""
 
     def __init__(self, params: Params, nx: int, ny: int, nz: int, mode: int,
                  log: Optional[Callable[[str], None]] = None, cap_frames: int = 0, cap_pairs: int = 0):
         self._lib = L.lib()
+        _load_schedules()
         h = C.c_void_p()
         c = params.to_c()
         if cap_frames or cap_pairs:
@@ -337,6 +355,7 @@ class Batch:
 
     def __init__(self, device: int = 0, lanes: int = 2):
         self._lib = L.lib()
+        _load_schedules()
         h = C.c_void_p()
         L.check(self._lib.mc_batch_create(device, lanes, C.byref(h)))
         self._h = h

@@ -187,3 +187,25 @@ def make_workload(name: str, seed: int = 0, nframes: int | None = None,
         w["nx"] //= scale
         w["ny"] //= scale
     return make_movie(seed=seed, **w), flags
+
+
+# Batch workload: movies of three sizes, uneven depth and pair distance.
+C5_GEOMETRIES = [(2048, 2048), (3838, 3710), (4096, 4096)]
+
+
+def c5_jobs(seed: int = 0, n_movies: int = 32, max_frames: int = 80) -> tuple[list[dict], list[float]]:
+    """Job list of the batch workload: per movie a geometry from
+    C5_GEOMETRIES, F ~ U[20, max_frames] frames, fod in {2, 4, 7} and a
+    window [offset, offset + F) of that geometry's base movie (max_frames
+    frames, mean dose U[0.8, 1.5] e/px/frame, returned per geometry)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    means = [float(rng.uniform(0.8, 1.5)) for _ in C5_GEOMETRIES]
+    jobs = []
+    for _ in range(n_movies):
+        g = int(rng.integers(0, len(C5_GEOMETRIES)))
+        nf = int(rng.integers(20, max_frames + 1))
+        fod = int(rng.choice([2, 4, 7]))
+        off = int(rng.integers(0, max_frames - nf + 1))
+        nx, ny = C5_GEOMETRIES[g]
+        jobs.append(dict(geometry=g, nx=nx, ny=ny, nframes=nf, fod=fod, offset=off))
+    return jobs, means
