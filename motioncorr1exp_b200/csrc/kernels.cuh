@@ -196,6 +196,10 @@ cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 // Sets the calling thread's mc_last_error() text; returns `code`.
 int record_error(int code, const char* text);
 
+// Opt-in to `bytes` of dynamic shared memory for `func` on the current device;
+// never lowers an earlier, larger opt-in (safe with concurrent host threads).
+cudaError_t allow_smem(const void* func, size_t bytes);
+
 // true when the register-codelet column stage handles the split n = P*Q
 bool pair_cols_reg_supported(int P, int Q);
 size_t pair_cols_reg_smem(int n, int team);

@@ -10,10 +10,32 @@
 //   k_c2r_rows    final C2R rows x 1/n^2                                   (DFAlign.cu:1287-1292)
 #include <math.h>
 #include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "kernels.cuh"
 #include "codelets_gen.cuh"
 
 namespace mc {
+
+// Raise-only, thread-safe opt-in to large dynamic shared memory.  The
+// attribute is per function and per device; two host threads that launch
+// the same kernel with different sizes must never lower it under each other.
+cudaError_t allow_smem(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = done[{dev, func}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 namespace {
 
@@ -106,7 +128,7 @@ cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st) {
   int n1, n2;
   if (two_level_split(a.nu, n1, n2)) return launch_fwd_rows2l(a, st);
   const size_t smem = fwd_rows_smem(a.nu);
-  cudaError_t e = cudaFuncSetAttribute(k_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_fwd_rows, smem);
   if (e != cudaSuccess) return e;
   const int grid = a.two_outputs ? a.nu : a.nu / 2;
   k_fwd_rows<<<grid, kThreads, smem, st>>>(a);
@@ -152,11 +174,11 @@ cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta
   const int grid = (a.nrows + rows_per_cta - 1) / rows_per_cta;
   cudaError_t e;
   if (inverse) {
-    e = cudaFuncSetAttribute(k_rows_fft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void*)k_rows_fft<true>, smem);
     if (e != cudaSuccess) return e;
     k_rows_fft<true><<<grid, kThreads, smem, st>>>(a, rows_per_cta);
   } else {
-    e = cudaFuncSetAttribute(k_rows_fft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void*)k_rows_fft<false>, smem);
     if (e != cudaSuccess) return e;
     k_rows_fft<false><<<grid, kThreads, smem, st>>>(a, rows_per_cta);
   }
@@ -356,8 +378,7 @@ cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
 #define MC_TL_LAUNCH(A, B)                                                                           \
   if (n1 == (A) && n2 == (B)) {                                                                      \
     const size_t smem = (size_t)2 * (A) * (B) * sizeof(float2);                                      \
-    cudaError_t e = cudaFuncSetAttribute(k_fwd_rows2l<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)smem);                                                 \
+    cudaError_t e = allow_smem((const void*)k_fwd_rows2l<A, B>, smem);                               \
     if (e != cudaSuccess) return e;                                                                  \
     k_fwd_rows2l<A, B><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                                    \
     return cudaGetLastError();                                                                       \
@@ -609,7 +630,7 @@ __global__ void __launch_bounds__(kRegThreads) k_pair_cols_grp(PairColsArgs a, c
 template <int Q>
 cudaError_t launch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
   const size_t smem = pair_cols_grp_smem(a.n, kRegThreads / team);
-  cudaError_t e = cudaFuncSetAttribute(k_pair_cols_grp<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_pair_cols_grp<Q>, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(ngroups, a.H);
   k_pair_cols_grp<Q><<<grid, kRegThreads, smem, st>>>(a, groups, team);
@@ -642,7 +663,7 @@ bool pair_cols_reg_supported(int P, int Q) {
 
 template <int Q>
 cudaError_t launch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_pair_cols_reg<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_pair_cols_reg<Q>, smem);
   if (e != cudaSuccess) return e;
   k_pair_cols_reg<Q><<<grid, kRegThreads, smem, st>>>(a, team);
   return cudaGetLastError();
@@ -666,7 +687,7 @@ cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
     return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);
   }
   const size_t smem = pair_cols_smem(a.n, a.P, a.Q, a.box) + 16;
-  cudaError_t e = cudaFuncSetAttribute(k_pair_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_pair_cols, smem);
   if (e != cudaSuccess) return e;
   k_pair_cols<<<grid, kThreads, smem, st>>>(a);
   return cudaGetLastError();
@@ -928,7 +949,7 @@ __global__ void __launch_bounds__(kThreads) k_peak(PeakArgs a) {
 
 cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st) {
   const size_t smem = peak_smem();
-  cudaError_t e = cudaFuncSetAttribute(k_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_peak, smem);
   if (e != cudaSuccess) return e;
   k_peak<<<a.npairs, kThreads, smem, st>>>(a);
   return cudaGetLastError();
@@ -1065,7 +1086,7 @@ cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st)
     const size_t smem2 = (size_t)(2 * a.n + a.nsum) * sizeof(float2);
 #define MC_TL_SUM(A, B)                                                                                       \
   if (n1 == (A) && n2 == (B)) {                                                                               \
-    e = cudaFuncSetAttribute(k_shift_sum2l<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);   \
+    e = allow_smem((const void*)k_shift_sum2l<A, B>, smem2);                                                \
     if (e != cudaSuccess) return e;                                                                           \
     k_shift_sum2l<A, B><<<a.H, kThreads, smem2, st>>>(a, ey);                                                 \
     return cudaGetLastError();                                                                                \
@@ -1074,7 +1095,7 @@ cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st)
 #undef MC_TL_SUM
   }
   const size_t smem = shift_sum_smem(a.n, a.nsum);
-  e = cudaFuncSetAttribute(k_shift_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = allow_smem((const void*)k_shift_sum, smem);
   if (e != cudaSuccess) return e;
   k_shift_sum<<<a.H, kThreads, smem, st>>>(a, ey);
   return cudaGetLastError();
@@ -1238,15 +1259,15 @@ cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
   cudaError_t e;
   const int E = (a.n + kThreads - 1) / kThreads;
   if (E <= 8) {
-    e = cudaFuncSetAttribute(k_objective<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void*)k_objective<8>, smem);
     if (e != cudaSuccess) return e;
     k_objective<8><<<a.H, kThreads, smem, st>>>(a);
   } else if (E <= 16) {
-    e = cudaFuncSetAttribute(k_objective<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void*)k_objective<16>, smem);
     if (e != cudaSuccess) return e;
     k_objective<16><<<a.H, kThreads, smem, st>>>(a);
   } else if (E <= 36) {
-    e = cudaFuncSetAttribute(k_objective<36>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void*)k_objective<36>, smem);
     if (e != cudaSuccess) return e;
     k_objective<36><<<a.H, kThreads, smem, st>>>(a);
   } else {
@@ -1309,7 +1330,7 @@ cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st) {
 #undef MC_TL_C2R
   }
   const size_t smem = c2r_rows_smem(a.n);
-  cudaError_t e = cudaFuncSetAttribute(k_c2r_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_c2r_rows, smem);
   if (e != cudaSuccess) return e;
   k_c2r_rows<<<a.n / 2, kThreads, smem, st>>>(a);
   return cudaGetLastError();
