@@ -204,6 +204,28 @@ int mc_solve_pairs(int nframe, int npairs, const int* ij, const float* shifts_xy
 int mc_pair_window_static(const void* d_spec_a, const void* d_spec_b, int n, int ldn, int pbx, float bfactor,
                           float* d_window, void* stream);
 
+/* Extra outputs of the sum stage.  Images are nsam*nsam floats (host).
+ * mc_plan_raw_sum: the unaligned sum of frames nStartSum..nEndSum, the
+ *   "-srs" output (raw sums DFAlign.cu:807-813, transform and scale
+ *   :851-858); needs mc_plan_forward (or a whole run).
+ * mc_plan_sum_to: the aligned sum of frames nStartSum..last_frame with the
+ *   final shifts, the "-2es" second sum (DFAlign.cu:1117-1122, 1198-1208;
+ *   last_frame is an absolute frame number, clamped as the reference does);
+ *   needs mc_plan_sum or mc_plan_run.
+ * mc_plan_corrected_frame: one aligned frame of the "-ssc" corrected stack
+ *   (DFAlign.cu:1154-1163, 1185-1195; absolute frame number in
+ *   [nStartSum, nEndSum]); needs mc_plan_sum or mc_plan_run. */
+int mc_plan_raw_sum(mc_plan* plan, float* image_host);
+int mc_plan_sum_to(mc_plan* plan, int last_frame, float* image_host);
+int mc_plan_corrected_frame(mc_plan* plan, int frame, float* image_host);
+
+/* No counterpart in the reference (its raw sums are FP32 spectra): the
+ * exact integer sum of the raw pixels of frames nStartSum..nEndSum over the
+ * square crop, nsam_unbin*nsam_unbin int32 values (host), pixels decoded as
+ * read2DIm_32bit does (mode 0 signed char, 1 int16, 6 uint16; mode 2 is
+ * rejected).  Needs the frames loaded or bound. */
+int mc_plan_count_sum(mc_plan* plan, int32_t* host_counts);
+
 /* Batched 1-D complex FFT of the library's engine on device memory
  * (un-normalised; inverse = exp(+2 pi i)).  Stream may be NULL. */
 int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void* stream);

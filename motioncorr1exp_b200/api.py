@@ -227,6 +227,28 @@ class Plan:
         L.check(self._lib.mc_plan_run_host(self._h, _ptr(a), _ptr(img)))
         return img
 
+    # -- extra sum-stage outputs (-srs, -2es, -ssc) and the exact count sum
+    def raw_sum(self) -> np.ndarray:
+        img = np.empty((self.nsam, self.nsam), dtype=np.float32)
+        L.check(self._lib.mc_plan_raw_sum(self._h, _ptr(img)))
+        return img
+
+    def sum_to(self, last_frame: int) -> np.ndarray:
+        img = np.empty((self.nsam, self.nsam), dtype=np.float32)
+        L.check(self._lib.mc_plan_sum_to(self._h, last_frame, _ptr(img)))
+        return img
+
+    def corrected_frame(self, frame: int) -> np.ndarray:
+        img = np.empty((self.nsam, self.nsam), dtype=np.float32)
+        L.check(self._lib.mc_plan_corrected_frame(self._h, frame, _ptr(img)))
+        return img
+
+    def count_sum(self) -> np.ndarray:
+        nu = self.info["nsam_unbin"]
+        out = np.empty((nu, nu), dtype=np.int32)
+        L.check(self._lib.mc_plan_count_sum(self._h, _ptr(out)))
+        return out
+
     # -- results
     def frame_shifts(self) -> np.ndarray:
         xy = np.empty((self.nframe, 2), dtype=np.float64)

@@ -18,7 +18,7 @@ namespace {
 struct Options {
   mc_params p;
   float xscale = 1.f, yscale = 1.f;  // -scx -scy (accepted, not applied)
-  int nEndSum2 = 0;                  // -2es (accepted, not applied)
+  int nEndSum2 = 0;                  // -2es
   int bSaveSubAreaCorrSum = 0, bSaveRawSum = 0, bSaveStackCorr = 0, bSaveCCmap = 0;
   int bSaveLog = 1, bLogFSC = 0;
   bool bSaveDisp = true;
@@ -41,7 +41,17 @@ void text_output(const char* s) {
   }
 }
 
-void log_cb(const char* text, void*) { text_output(text); }
+// Library log lines; held back while a run is in flight so that the lines of
+// the extra outputs (-srs, -2es) can be placed where the reference prints them.
+bool g_hold = false;
+std::vector<std::string> g_held;
+
+void log_cb(const char* text, void*) {
+  if (g_hold) g_held.push_back(text);
+  else text_output(text);
+}
+
+bool starts_with(const std::string& s, const char* p) { return s.compare(0, std::strlen(p), p) == 0; }
 
 // Message (DFAlign.cu:51-54)
 void message(const char* s) { printf("%s\n", s); }
@@ -344,8 +354,7 @@ int run_align(Options& o) {
   }
   const MrcHeader h = stack.header();
   if (o.xscale > 1.0f || o.yscale > 1.0f) message("Warning: -scx/-scy stretching is not applied by this build.");
-  if (o.bSaveRawSum || o.bSaveStackCorr || o.bSaveCCmap || o.bLogFSC || o.nEndSum2 > 0 || o.bSaveSubAreaCorrSum)
-    message("Warning: -srs/-ssc/-scc/-fsc/-2es/-sub outputs are not produced by this build.");
+  if (o.bSaveCCmap || o.bLogFSC) message("Warning: -scc/-fsc outputs are not produced by this build.");
   mc_plan* plan = nullptr;
   int rc = mc_plan_create(&o.p, h.nx, h.ny, h.nz, h.mode, &plan);
   if (rc != MC_OK) {
@@ -394,23 +403,91 @@ int run_align(Options& o) {
     }
   }
   std::vector<float> image((size_t)info.nsam * info.nsam);
+  g_hold = true;
+  g_held.clear();
   rc = mc_plan_run(plan, image.data());
-  if (rc != MC_OK) {
-    snprintf(str, sizeof(str), "Error: %s (%s)", mc_strerror(rc), mc_last_error());
+  g_hold = false;
+  auto fail = [&](const char* what) {
+    for (const auto& l : g_held) text_output(l.c_str());
+    snprintf(str, sizeof(str), "Error: %s (%s)", what, mc_last_error());
     message(str);
     mc_plan_destroy(plan);
     return 1;
+  };
+  if (rc != MC_OK) return fail(mc_strerror(rc));
+  // the sum range and the frame after whose "Add Frame" line the second sum
+  // is saved (DFAlign.cu:1115-1122, 1198)
+  std::vector<double> sxy((size_t)info.nframe * 2);
+  int sfirst = 0, slast = 0;
+  mc_plan_get_sum_shifts(plan, sxy.data(), &sfirst, &slast);
+  const bool second = o.nEndSum2 > 0 && o.nEndSum2 < o.p.nEndSum;
+  int sum2_last = o.nEndSum2 - info.nstart;
+  if (sum2_last <= sfirst || sum2_last >= info.nframe) sum2_last = info.nframe - 1;
+  if (sum2_last > slast) sum2_last = slast;
+  auto sub_name = [&](const std::string& fn) {
+    char b2[1024];
+    snprintf(b2, sizeof(b2), "%s_ox%d_oy%d_dim%d.mrc", fn.substr(0, fn.size() >= 4 ? fn.size() - 4 : 0).c_str(),
+             o.p.crop_offsetx, o.p.crop_offsety, info.nsam_unbin);
+    return std::string(b2);
+  };
+  std::vector<float> extra((size_t)info.nsam * info.nsam);
+  std::vector<std::string> raw_lines, sum2_lines;
+  // -srs: unaligned sum (DFAlign.cu:851-872)
+  if (o.bSaveRawSum) {
+    if (mc_plan_raw_sum(plan, extra.data()) != MC_OK) return fail("raw sum");
+    MrcHeader rh;
+    if (!write_mrc_float(o.fnRawsum.c_str(), extra.data(), info.nsam, info.nsam, 1, &rh)) return fail("write");
+    snprintf(str, sizeof(str), "Mean=%f   Min=%f   Max=%f\n", rh.dmean, rh.dmin, rh.dmax);
+    raw_lines.push_back(str);
+    snprintf(str, sizeof(str), "Save Unaligned Sum to: %s\n", o.fnRawsum.c_str());
+    raw_lines.push_back(str);
   }
+  // -2es: aligned sum of nStartSum..nEndSum2 (DFAlign.cu:1198-1229)
+  if (second) {
+    if (mc_plan_sum_to(plan, sum2_last + info.nstart, extra.data()) != MC_OK) return fail("second sum");
+    const std::string fn = o.bSaveSubAreaCorrSum ? sub_name(o.fnAlignsum2) : o.fnAlignsum2;
+    MrcHeader sh;
+    if (!write_mrc_float(fn.c_str(), extra.data(), info.nsam, info.nsam, 1, &sh)) return fail("write");
+    snprintf(str, sizeof(str), "Mean=%f   Min=%f   Max=%f\n", sh.dmean, sh.dmin, sh.dmax);
+    sum2_lines.push_back(str);
+    snprintf(str, sizeof(str), "Save Sum to: %s\n", fn.c_str());
+    sum2_lines.push_back(str);
+  }
+  // -ssc: the aligned frames nStartSum..nEndSum (DFAlign.cu:1104-1113, 1154-1263)
+  if (o.bSaveStackCorr) {
+    MrcStackWriter w;
+    if (!w.open(o.fnStackCorr.c_str(), info.nsam, info.nsam, o.p.nEndSum - o.p.nStartSum + 1))
+      return fail("write");
+    for (int k = sfirst; k <= slast; k++) {
+      if (mc_plan_corrected_frame(plan, k + info.nstart, extra.data()) != MC_OK) return fail("corrected frame");
+      if (!w.write_frame(extra.data(), k - sfirst)) return fail("write");
+    }
+    if (!w.close()) return fail("write");
+  }
+  // the held log with the extra lines in the reference's places
+  char add2[64];
+  snprintf(add2, sizeof(add2), "......Add Frame #%03d ", sum2_last + info.nstart);
+  for (size_t i = 0; i < g_held.size(); i++) {
+    text_output(g_held[i].c_str());
+    const bool last_read = starts_with(g_held[i], "......Read and sum frame") &&
+                           (i + 1 == g_held.size() || !starts_with(g_held[i + 1], "......Read and sum frame"));
+    if (last_read)
+      for (const auto& l : raw_lines) text_output(l.c_str());
+    if (second && starts_with(g_held[i], add2))
+      for (const auto& l : sum2_lines) text_output(l.c_str());
+  }
+  g_held.clear();
+  const std::string fnsum = o.bSaveSubAreaCorrSum ? sub_name(o.fnAlignsum) : o.fnAlignsum;
   MrcHeader oh;
-  if (!write_mrc_float(o.fnAlignsum.c_str(), image.data(), info.nsam, info.nsam, 1, &oh)) {
-    snprintf(str, sizeof(str), "Error: Failed to write %s\n", o.fnAlignsum.c_str());
+  if (!write_mrc_float(fnsum.c_str(), image.data(), info.nsam, info.nsam, 1, &oh)) {
+    snprintf(str, sizeof(str), "Error: Failed to write %s\n", fnsum.c_str());
     text_output(str);
     mc_plan_destroy(plan);
     return 1;
   }
   snprintf(str, sizeof(str), "Mean=%f   Min=%f   Max=%f\n", oh.dmean, oh.dmin, oh.dmax);
   text_output(str);
-  snprintf(str, sizeof(str), "Save Sum to: %s\n", o.fnAlignsum.c_str());
+  snprintf(str, sizeof(str), "Save Sum to: %s\n", fnsum.c_str());
   text_output(str);
   text_output("Done.\n");
   mc_plan_destroy(plan);

@@ -127,3 +127,38 @@ bool write_mrc_float(const char* path, const float* data, int nx, int ny, int nz
   if (out_header) *out_header = h;
   return ok;
 }
+
+MrcStackWriter::~MrcStackWriter() { close(); }
+
+bool MrcStackWriter::open(const char* path, int nx, int ny, int nz) {
+  close();
+  fp_ = fopen(path, "wb");
+  if (!fp_) return false;
+  MrcHeader h;
+  std::memset(&h, 0, sizeof(h));
+  h.nx = nx;
+  h.ny = ny;
+  h.nz = nz;
+  h.mode = 2;
+  h.cellb[0] = h.cellb[1] = h.cellb[2] = 90;
+  h.mapc = 1;
+  h.mapr = 2;
+  h.maps = 3;
+  nx_ = nx;
+  ny_ = ny;
+  return fwrite(&h, 1, 1024, fp_) == 1024;
+}
+
+bool MrcStackWriter::write_frame(const float* data, int n) {
+  if (!fp_ || n < 0) return false;
+  const size_t bytes = (size_t)nx_ * ny_ * sizeof(float);
+  if (fseeko(fp_, (off_t)(1024 + (size_t)n * bytes), SEEK_SET) != 0) return false;
+  return fwrite(data, 1, bytes, fp_) == bytes;
+}
+
+bool MrcStackWriter::close() {
+  if (!fp_) return true;
+  const bool ok = fclose(fp_) == 0;
+  fp_ = nullptr;
+  return ok;
+}

@@ -61,3 +61,22 @@ bool starts_with_tiff(const char* path);
 
 // createMRC(float*) semantics; fills dmin/dmax/dmean; returns false on I/O error.
 bool write_mrc_float(const char* path, const float* data, int nx, int ny, int nz, MrcHeader* out_header);
+
+// Corrected-stack writer: the header a default MRC() object carries
+// (mrc.cpp:5-16: mode 2, cellb 90, mapc/mapr/maps 1/2/3, statistics 0) with
+// nx, ny, nz set and written by updateHeader (mrc.cpp:237-241); frame n at
+// 1024 + n * nx*ny*4 as write2DIm puts it (mrc.cpp:188-194).
+class MrcStackWriter {
+ public:
+  MrcStackWriter() = default;
+  ~MrcStackWriter();
+  MrcStackWriter(const MrcStackWriter&) = delete;
+  MrcStackWriter& operator=(const MrcStackWriter&) = delete;
+  bool open(const char* path, int nx, int ny, int nz);
+  bool write_frame(const float* data, int n);
+  bool close();
+
+ private:
+  FILE* fp_ = nullptr;
+  int nx_ = 0, ny_ = 0;
+};

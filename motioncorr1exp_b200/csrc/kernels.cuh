@@ -184,6 +184,18 @@ struct SolveArgs {
 cudaError_t launch_solve(const SolveArgs& a, cudaStream_t st);
 cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st);
 
+// Exact integer sum of raw frames over the square crop (A1 count sums):
+// out[y*nu + x] = sum_f frame_f[offy + y][offx + x] for f in [first, last],
+// pixels decoded as the reference does (mode 0 signed char, 1 int16, 6 uint16).
+struct CountSumArgs {
+  const void* frames;    // run positions back to back, nx*ny pixels each
+  long long frame_pixels;
+  int mode, nx, offx, offy, nu;
+  int first, last;       // run positions
+  int* out;              // nu*nu
+};
+cudaError_t launch_count_sum(const CountSumArgs& a, cudaStream_t st);
+
 cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st);
 cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st);
 cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st);

@@ -11,6 +11,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -198,6 +199,11 @@ __device__ __forceinline__ void fft_n1(float2* v) {
   else fft_reg<N1, INV>(v);
 }
 
+// Resident CTAs per SM the two-level transforms are compiled for (register cap).
+#ifndef MC_TL_MIN_BLOCKS
+#define MC_TL_MIN_BLOCKS 1
+#endif
+
 template <int N1, int N2>
 struct TwoLevel {
   static constexpr int N = N1 * N2;
@@ -246,7 +252,7 @@ struct TwoLevel {
 
 // Batched rows: out_row[i] = scale * X[i < keep_lo ? i : i + (n - n_out)].
 template <int N1, int N2, bool INV>
-__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_rows_fft2l(RowsFftArgs a) {
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_fft2l(RowsFftArgs a) {
   using TL = TwoLevel<N1, N2>;
   __shared__ float2 ysm[TL::N];
   const long long row = blockIdx.x;
@@ -299,7 +305,7 @@ __device__ __forceinline__ void stage_rows(float2* xin, const FwdRowsArgs& a, lo
 }
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_fwd_rows2l(FwdRowsArgs a) {
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows2l(FwdRowsArgs a) {
   using TL = TwoLevel<N1, N2>;
   constexpr int N = TL::N;
   extern __shared__ float2 dyn2l[];
@@ -997,6 +1003,45 @@ __global__ void __launch_bounds__(kThreads) k_shift_sum(ShiftSumArgs a, const fl
   }
   float2* X = fft_run<true, false>(acc, b1, a.plan, 1, n, tw, tid, nth);
   for (int y = tid; y < n; y += nth) a.out[(long long)y * a.ld_out + kx] = X[y];
+}
+
+// ============================================================ count sums ==
+// One thread per 4 consecutive crop pixels of a row; frames summed in int32
+// registers (exact: |pixel| <= 65535 and at most 2^15 frames).
+template <typename Px>
+__global__ void __launch_bounds__(kThreads) k_count_sum(CountSumArgs a) {
+  const int per_row = (a.nu + 3) / 4;
+  const long long total = (long long)per_row * a.nu;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(t / per_row);
+    const int x0 = (int)(t - (long long)y * per_row) * 4;
+    const int cnt = min(4, a.nu - x0);
+    int acc[4] = {0, 0, 0, 0};
+    const Px* base = reinterpret_cast<const Px*>(a.frames) + (long long)(a.offy + y) * a.nx + a.offx + x0;
+    for (int f = a.first; f <= a.last; f++) {
+      const Px* row = base + (long long)f * a.frame_pixels;
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (i < cnt) acc[i] += (int)row[i];
+    }
+    int* o = a.out + (long long)y * a.nu + x0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (i < cnt) o[i] = acc[i];
+  }
+}
+
+cudaError_t launch_count_sum(const CountSumArgs& a, cudaStream_t st) {
+  const long long items = (long long)((a.nu + 3) / 4) * a.nu;
+  const int grid = (int)std::min<long long>((items + kThreads - 1) / kThreads, 148LL * 16);
+  switch (a.mode) {
+    case 0: k_count_sum<int8_t><<<grid, kThreads, 0, st>>>(a); break;
+    case 1: k_count_sum<int16_t><<<grid, kThreads, 0, st>>>(a); break;
+    case 6: k_count_sum<uint16_t><<<grid, kThreads, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 __global__ void k_ramp(RampArgs a) {

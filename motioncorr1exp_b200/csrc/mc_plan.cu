@@ -275,6 +275,7 @@ struct mc_plan {
 
   // device memory
   void* d_frames = nullptr;
+  int* d_count = nullptr;  // exact count sum (allocated on first use)
   const void* frames_src = nullptr;  // bound caller device frames (mc_plan_bind_frames_device) or null
   float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
   float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
@@ -319,6 +320,7 @@ struct mc_plan {
 
   // state
   bool loaded_all = false, have_forward = false, have_pairs = false, have_solve = false, have_iter = false;
+  bool have_sum = false;  // sum_shift / sum_first / sum_last belong to the current shifts
   std::vector<char> loaded;
 
   // results
@@ -715,7 +717,7 @@ static int configure_frames(mc_plan* pl, const mc_params& q, int nz) {
   }
   pl->loaded.assign(pl->nframe, 0);
   pl->frames_src = nullptr;
-  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1016,7 +1018,7 @@ int mc_plan_set_refs(mc_plan* pl, const float* dark, const float* dark2, const f
     pl->two_sets = true;
   }
   CK(cudaStreamSynchronize(pl->st));
-  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1035,7 +1037,7 @@ static int load_frames(mc_plan* pl, const void* src, int first, int count, cudaM
     pl->loaded.assign(pl->nframe, 0);
   }
   for (int i = first; i < first + count; i++) pl->loaded[i] = 1;
-  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1059,7 +1061,7 @@ int mc_plan_bind_frames_device(mc_plan* pl, const void* d_frames) {
   }
   pl->frames_src = d_frames;
   pl->loaded.assign(pl->nframe, d_frames ? 1 : 0);
-  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1200,7 +1202,7 @@ static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int c
   CK(cudaEventElapsedTime(&pl->tm.forward_ms, pl->ev[0], pl->ev[1]));
   log_frame_means(pl, dc.data());
   pl->have_forward = true;
-  pl->have_pairs = pl->have_solve = pl->have_iter = false;
+  pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1268,7 +1270,7 @@ int mc_plan_pairs(mc_plan* pl) {
   CK(cudaEventElapsedTime(&pl->tm.pairs_ms, pl->ev[2], pl->ev[3]));
   log_pairs(pl);
   pl->have_pairs = true;
-  pl->have_solve = pl->have_iter = false;
+  pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1290,7 +1292,7 @@ int mc_plan_solve(mc_plan* pl) {
   log_solve(pl);
   pl->shift = s;
   pl->have_solve = true;
-  pl->have_iter = false;
+  pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
 
@@ -1428,6 +1430,7 @@ static void sum_shifts(mc_plan* pl, std::vector<int>& frames, std::vector<cplx>&
   }
   pl->sum_first = nss;
   pl->sum_last = nes;
+  pl->have_sum = true;
 }
 
 extern "C" {
@@ -1448,6 +1451,92 @@ int mc_plan_sum(mc_plan* pl, float* image_host) {
   CK(cudaStreamSynchronize(pl->st));
   CK(cudaEventElapsedTime(&pl->tm.sum_ms, pl->ev[6], pl->ev[7]));
   CKR(pl->collect());
+  return MC_OK;
+}
+
+// ------------------------------------------------- extra sum-stage outputs --
+static int image_out(mc_plan* pl, float* image_host) {
+  if (image_host)
+    CK(cudaMemcpyAsync(image_host, pl->d_image, sizeof(float) * (size_t)pl->n * pl->n, cudaMemcpyDeviceToHost,
+                       pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  return pl->collect();
+}
+
+int mc_plan_raw_sum(mc_plan* pl, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_forward) return set_err(MC_E_STATE, "raw sum before forward");
+  CK(cudaSetDevice(pl->device));
+  int nss, nes, lim;
+  sum_range(pl, &nss, &nes, &lim);
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  for (int k = nss; k <= nes; k++) {
+    frames.push_back(k);
+    sh.push_back(cplx(0, 0));
+    apply.push_back(0);
+  }
+  CKR(run_shift_sum(pl, frames, sh, apply, 1));
+  return image_out(pl, image_host);
+}
+
+int mc_plan_sum_to(mc_plan* pl, int last_frame, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_sum) return set_err(MC_E_STATE, "second sum before the corrected sum");
+  CK(cudaSetDevice(pl->device));
+  // nEndSum2 clamps of DFAlign.cu:1117-1122
+  int last = last_frame - pl->nstart;
+  if (last <= pl->sum_first || last >= pl->nframe) last = pl->nframe - 1;
+  if (last > pl->sum_last) last = pl->sum_last;
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  for (int k = pl->sum_first; k <= last; k++) {
+    frames.push_back(k);
+    sh.push_back(pl->sum_shift[k]);
+    apply.push_back((k == pl->sum_first && !pl->p.bAlignToMid) ? 0 : 1);
+  }
+  CKR(run_shift_sum(pl, frames, sh, apply, 1));
+  return image_out(pl, image_host);
+}
+
+int mc_plan_corrected_frame(mc_plan* pl, int frame, float* image_host) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_sum) return set_err(MC_E_STATE, "corrected frame before the corrected sum");
+  const int k = frame - pl->nstart;
+  if (k < pl->sum_first || k > pl->sum_last)
+    return set_err(MC_E_ARG, "frame %d outside the summed range [%d, %d]", frame, pl->sum_first + pl->nstart,
+                   pl->sum_last + pl->nstart);
+  CK(cudaSetDevice(pl->device));
+  const std::vector<int> frames{k};
+  const std::vector<cplx> sh{pl->sum_shift[k]};
+  const std::vector<int> apply{(k == pl->sum_first && !pl->p.bAlignToMid) ? 0 : 1};
+  CKR(run_shift_sum(pl, frames, sh, apply, 1));
+  return image_out(pl, image_host);
+}
+
+int mc_plan_count_sum(mc_plan* pl, int32_t* host) {
+  if (!pl || !host) return set_err(MC_E_ARG, "null argument");
+  if (pl->mode == 2) return set_err(MC_E_ARG, "count sums need integer pixels (MRC mode 0, 1 or 6)");
+  for (int f = 0; f < pl->nframe; f++)
+    if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
+  CK(cudaSetDevice(pl->device));
+  if (!pl->d_count) CKR(pl->alloc(&pl->d_count, sizeof(int) * (size_t)pl->nu * pl->nu));
+  int nss, nes, lim;
+  sum_range(pl, &nss, &nes, &lim);
+  mc::CountSumArgs a{};
+  a.frames = pl->frames_src ? pl->frames_src : pl->d_frames;
+  a.frame_pixels = (long long)pl->nx * pl->ny;
+  a.mode = pl->mode;
+  a.nx = pl->nx;
+  a.offx = pl->p.crop_offsetx;
+  a.offy = pl->p.crop_offsety;
+  a.nu = pl->nu;
+  a.first = nss;
+  a.last = nes;
+  a.out = pl->d_count;
+  CK(mc::launch_count_sum(a, pl->st));
+  CK(cudaMemcpyAsync(host, pl->d_count, sizeof(int) * (size_t)pl->nu * pl->nu, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
   return MC_OK;
 }
 
@@ -1542,6 +1631,7 @@ int mc_plan_refine(mc_plan* pl, int iterations) {
   CK(cudaEventElapsedTime(&pl->tm.refine_ms, pl->ev[4], pl->ev[5]));
   for (int k = 0; k < nf; k++) pl->frame_shift[k] = s[0] - s[k];
   for (int k = 0; k < nf - 1; k++) pl->shift[k] = pl->frame_shift[k + 1] - pl->frame_shift[k];
+  pl->have_sum = false;
   pl->log("\nGradient refinement: %d Newton step(s), last max update %.5f px, objective %.6e\n", it, maxd, J);
   for (int k = 0; k < nf; k++)
     pl->log("......Refined shift of Frame #%03d : %8.4f %8.4f\n", k + pl->nstart, pl->frame_shift[k].real(),

@@ -366,6 +366,28 @@ def spectrum_to_image(Fsum: np.ndarray) -> np.ndarray:
     return _irfft2(Fsum, s=(n, n))
 
 
+def raw_sum_image(F: list, first: int, last: int) -> np.ndarray:
+    """Unaligned sum of spectra first..last (run positions): the raw even/odd
+    sums of DFAlign.cu:807-813 added at :821-824, transformed and scaled as
+    the "-srs" output (:851-858)."""
+    S = np.zeros_like(F[first])
+    for k in range(first, last + 1):
+        S = S + F[k]
+    return spectrum_to_image(S)
+
+
+def count_sum(frames: np.ndarray, mode: int, offx: int, offy: int, nu: int, first: int,
+              last: int) -> np.ndarray:
+    """Exact integer sum of the decoded raw pixels (read2DIm_32bit,
+    mrc.cpp:325-382) of run positions first..last over the square crop (the
+    count sums of the precision method; no reference counterpart)."""
+    dt = _MODE_DTYPE[mode]
+    acc = np.zeros((nu, nu), dtype=np.int64)
+    for k in range(first, last + 1):
+        acc += np.asarray(frames[k]).view(dt)[offy:offy + nu, offx:offx + nu].astype(np.int64)
+    return acc
+
+
 # ---------------------------------------------------------------------------
 # frame-to-sum objective of the added gradient refinement (no reference
 # counterpart: north-star method 3), FP64

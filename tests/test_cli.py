@@ -95,3 +95,44 @@ def test_cli_full_run_matches_api(gpu, tmp_path):
     assert "Save Sum to: sum.mrc" in log and "Done." in log
     h = mrc.read_header(str(tmp_path / "sum.mrc"))
     assert int(h["mode"]) == 2 and bytes(h["map"]) == b""
+
+
+@pytest.mark.gpu
+def test_cli_extra_outputs(gpu, tmp_path):
+    """-srs (unaligned sum), -2es (second sum), -ssc (aligned stack) and -sub
+    names, with their log lines where the reference prints them."""
+    mv = synth.make_movie(200, 190, 10, mean=2.0, seed=5, dtype="u8", speed=0.8, rw_sigma=0.3)
+    p = tmp_path / "m.mrc"
+    mrc.write_stack(str(p), mv.frames, 0)
+    rc, out = run([str(p), "-pbx", "64", "-fod", "2", "-dsp", "0", "-srs", "1", "-ssc", "1", "-2es", "5",
+                   "-nss", "1", "-flg", "log.txt"], tmp_path)
+    assert rc == 0, out
+    prm = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2, nStartSum=1), 10)
+    with api.Plan(prm, 200, 190, 10, 0) as pl:
+        pl.load_frames(mv.frames)
+        img = pl.run()
+        raw, sum2 = pl.raw_sum(), pl.sum_to(5)
+        stack = np.stack([pl.corrected_frame(k) for k in range(1, 10)])
+    tol = 1e-5 * np.abs(img).max()
+    np.testing.assert_allclose(mrc.read_image(str(tmp_path / "m_SumCorr.mrc")), img, rtol=0, atol=tol)
+    np.testing.assert_allclose(mrc.read_image(str(tmp_path / "m_SumRaw.mrc")), raw, rtol=0, atol=tol)
+    np.testing.assert_allclose(mrc.read_image(str(tmp_path / "m_SumCorr2.mrc")), sum2, rtol=0, atol=tol)
+    h = mrc.read_header(str(tmp_path / "m_Corrected.mrc"))
+    assert (int(h["nx"]), int(h["ny"]), int(h["nz"]), int(h["mode"])) == (190, 190, 9, 2)
+    got = np.fromfile(str(tmp_path / "m_Corrected.mrc"), dtype=np.float32, offset=1024).reshape(9, 190, 190)
+    np.testing.assert_allclose(got, stack, rtol=0, atol=tol)
+    log = (tmp_path / "log.txt").read_text()
+    lines = log.splitlines()
+    i_raw = lines.index("Save Unaligned Sum to: m_SumRaw.mrc")
+    i_pair = lines.index("Calculate relative drift between frames")
+    i_read = max(i for i, l in enumerate(lines) if l.startswith("......Read and sum frame"))
+    assert i_read < i_raw < i_pair
+    i_add5 = next(i for i, l in enumerate(lines) if l.startswith("......Add Frame #005"))
+    assert lines[i_add5 + 2] == "Save Sum to: m_SumCorr2.mrc"
+    assert lines[i_add5 + 3].startswith("......Add Frame #006")
+    # -sub: crop-tagged names of both sums
+    rc, out = run([str(p), "-pbx", "64", "-fod", "2", "-dsp", "0", "-sub", "1", "-2es", "5", "-crx", "4"],
+                  tmp_path)
+    assert rc == 0, out
+    assert (tmp_path / "m_SumCorr_ox4_oy0_dim190.mrc").exists()
+    assert (tmp_path / "m_SumCorr2_ox4_oy0_dim190.mrc").exists()

@@ -1,0 +1,95 @@
+"""Extra sum-stage outputs (-srs raw sum, -2es second sum, -ssc corrected
+frames) and the exact count sums, through the C ABI against the FP64 oracle.
+
+Tolerances: images relative L2 <= 1e-5 (FP32 transforms vs FP64); count
+sums bit-exact."""
+import numpy as np
+import pytest
+
+from motioncorr1exp_b200 import api, synth
+from oracle import mc_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+IMAGE_RTOL = 1e-5
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _spectra(frames, mode, p, nu, n):
+    return [O.forward_spectrum(O.decode_frame(frames[f], mode), p.crop_offsetx, p.crop_offsety, nu, n)
+            for f in range(p.nStart, p.nEnd + 1)]
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(bAlignToMid=0, nStartSum=2, nEndSum=9), dict(bin=2.0, nStart=1)])
+def test_raw_second_and_corrected(gpu, kw):
+    nz = 12
+    mv = synth.make_movie(300, 292, nz, mean=2.0, seed=61, dtype="u8", speed=0.6, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, **kw), nz)
+    with api.Plan(p, 300, 292, nz, 0) as pl:
+        pl.load_frames(mv.frames[pl.info["nstart"]: pl.info["nend"] + 1])
+        img = pl.run()
+        nu, n = pl.info["nsam_unbin"], pl.nsam
+        F = _spectra(mv.frames, 0, p, nu, n)
+        sh, first, last = pl.sum_shifts()
+        # -srs: unaligned sum of nStartSum..nEndSum
+        raw = pl.raw_sum()
+        assert rel_l2(raw, O.raw_sum_image(F, first, last)) <= IMAGE_RTOL
+        # -2es: the aligned prefix sum; up to nEndSum it is the corrected sum itself
+        assert rel_l2(pl.sum_to(last + pl.info["nstart"]), img) <= 1e-6
+        mid = first + (last - first) // 2
+        part = pl.sum_to(mid + pl.info["nstart"])
+        S = np.zeros_like(F[0])
+        for k in range(first, mid + 1):
+            apply = not (k == first and not p.bAlignToMid)
+            S = S + (O.phase_shift(F[k], sh[k, 0], sh[k, 1]) if apply else F[k])
+        assert rel_l2(part, O.spectrum_to_image(S)) <= IMAGE_RTOL
+        # the reference's clamp: a last frame at or before the first summed one means "all frames"
+        assert rel_l2(pl.sum_to(first + pl.info["nstart"]), img) <= 1e-6
+        # -ssc: each aligned frame; together they add up to the corrected sum
+        acc = np.zeros((n, n))
+        for k in range(first, last + 1):
+            fr = pl.corrected_frame(k + pl.info["nstart"])
+            apply = not (k == first and not p.bAlignToMid)
+            want = O.spectrum_to_image(O.phase_shift(F[k], sh[k, 0], sh[k, 1]) if apply else F[k])
+            assert rel_l2(fr, want) <= IMAGE_RTOL
+            acc += fr
+        assert rel_l2(acc, img) <= IMAGE_RTOL
+        with pytest.raises(Exception):
+            pl.corrected_frame(last + pl.info["nstart"] + 1)
+
+
+@pytest.mark.parametrize("mode,dtype", [(0, np.int8), (1, np.int16), (6, np.uint16)])
+def test_count_sum_exact(gpu, mode, dtype):
+    rng = np.random.default_rng(62 + mode)
+    nz, ny, nx = 9, 203, 230
+    lo, hi = (-128, 128) if mode == 0 else ((-32768, 32768) if mode == 1 else (0, 65536))
+    frames = rng.integers(lo, hi, size=(nz, ny, nx)).astype(dtype)
+    p = api.verify_params(api.Params(CCPeakSearchDim=32, crop_offsetx=5, crop_offsety=3, nStartSum=1,
+                                     nEndSum=7, FrameDistOffset=1), nz)
+    with api.Plan(p, nx, ny, nz, mode) as pl:
+        pl.load_frames(frames)
+        got = pl.count_sum()
+        nu = pl.info["nsam_unbin"]
+        want = O.count_sum(frames, mode, 5, 3, nu, 1, 7)
+        np.testing.assert_array_equal(got.astype(np.int64), want)
+
+
+def test_count_sum_bound_frames_and_float_rejected(gpu):
+    import torch
+    mv = synth.make_movie(256, 256, 6, mean=1.5, seed=63, dtype="u8")
+    p = api.verify_params(api.Params(CCPeakSearchDim=32, FrameDistOffset=1), 6)
+    d = torch.from_numpy(mv.frames).cuda()
+    with api.Plan(p, 256, 256, 6, 0) as pl:
+        pl.bind_frames_device(d.data_ptr())
+        np.testing.assert_array_equal(pl.count_sum().astype(np.int64),
+                                      O.count_sum(mv.frames, 0, 0, 0, 256, 0, 5))
+    f32 = synth.make_movie(128, 128, 6, mean=1.5, seed=64, dtype="f32")
+    with api.Plan(p, 128, 128, 6, 2) as pl:
+        pl.load_frames(f32.frames)
+        with pytest.raises(Exception):
+            pl.count_sum()
