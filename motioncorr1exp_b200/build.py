@@ -59,7 +59,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     objdir = os.path.join(LIB, "obj")
     os.makedirs(objdir, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in LIB_HEADERS] + [os.path.join(INCLUDE, "mc.h")]
-    objs = []
+    objs, jobs = [], []
     for src in LIB_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
@@ -71,7 +71,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             if s.endswith(".cpp"):
                 cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
                        "-x", "c++", "-c", s, "-o", o]
-            _run(cmd, verbose or ptxas_info)
+            jobs.append(cmd)
+    # translation units compile in parallel (the kernel file dominates)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, c, verbose or ptxas_info) for c in jobs]:
+            f.result()
     so = os.path.join(LIB, "libmc.so")
     if force or _stale(so, objs):
         _run([nvcc()] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart"], verbose)

@@ -2112,7 +2112,7 @@ __constant__ float2 c_tw53[27][27] = {{{1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f},
   {{1.0f, 0.0f}, {-0.956400990486145f, 0.29205676913261414f}, {0.829405665397644f, -0.5586467385292053f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.3758275806903839f, -0.926689624786377f}, {-0.08879589289426804f, 0.9960498213768005f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.4827921986579895f, 0.8757349252700806f}, {-0.7175072431564331f, -0.6965510249137878f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.9842305779457092f, -0.1768902689218521f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.26358717679977417f, -0.9646356105804443f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.3202698528766632f, -0.9473263621330261f}, {0.5829795002937317f, 0.8124868869781494f}, {-0.794854462146759f, -0.6068001389503479f}, {0.9374196529388428f, 0.3482016324996948f}, {-0.9982437491416931f, -0.05924062803387642f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.674983024597168f, -0.7378332614898682f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.14764656126499176f, -0.989040195941925f}},
   {{1.0f, 0.0f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.14764656126499176f, -0.989040195941925f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.3758275806903839f, 0.926689624786377f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.674983024597168f, 0.7378332614898682f}, {-0.794854462146759f, -0.6068001389503479f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.829405665397644f, -0.5586467385292053f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.08879589289426804f, 0.9960498213768005f}},
   {{1.0f, 0.0f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.956400990486145f, 0.29205676913261414f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.8896570801734924f, -0.4566292464733124f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.829405665397644f, -0.5586467385292053f}, {-0.794854462146759f, 0.6068001389503479f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.674983024597168f, -0.7378332614898682f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.3758275806903839f, -0.926689624786377f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.2059786170721054f, 0.9785565137863159f}, {0.14764656126499176f, -0.989040195941925f}, {-0.08879589289426804f, 0.9960498213768005f}, {0.029633328318595886f, -0.9995608329772949f}}};
-template <bool INV, typename St>
+template <bool INV, bool PAIRED = false, typename St>
 __device__ __forceinline__ void dft_r53_compact(const float2* v, St&& st) {
   const float2 x0 = v[0];
   const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
@@ -2168,38 +2168,77 @@ __device__ __forceinline__ void dft_r53_compact(const float2* v, St&& st) {
   const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
   const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
   st(0, make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y)));
+  if constexpr (PAIRED) {
 #pragma unroll 1
-  for (int k = 1; k <= 26; k++) {
-    const float2* t = c_tw53[k];
-    float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
-    { const float2 c = t[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); }
-    { const float2 c = t[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); }
-    { const float2 c = t[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); }
-    { const float2 c = t[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); }
-    { const float2 c = t[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); }
-    { const float2 c = t[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); }
-    { const float2 c = t[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); }
-    { const float2 c = t[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); }
-    { const float2 c = t[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); }
-    { const float2 c = t[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); }
-    { const float2 c = t[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); }
-    { const float2 c = t[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); }
-    { const float2 c = t[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); }
-    { const float2 c = t[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); }
-    { const float2 c = t[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); }
-    { const float2 c = t[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); }
-    { const float2 c = t[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); }
-    { const float2 c = t[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); }
-    { const float2 c = t[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); }
-    { const float2 c = t[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); }
-    { const float2 c = t[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); }
-    { const float2 c = t[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); }
-    { const float2 c = t[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); }
-    { const float2 c = t[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); }
-    { const float2 c = t[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); }
-    { const float2 c = t[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); }
-    if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - k, make_float2(ar - bi, ai + br)); }
-    else { st(k, make_float2(ar - bi, ai + br)); st(53 - k, make_float2(ar + bi, ai - br)); }
+    for (int k = 1; k <= 13; k++) {
+      const float2* t = c_tw53[k];
+      const float2* u = c_tw53[k + 13];
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      float cr = x0.x, ci = x0.y, dr = 0.0f, di = 0.0f;
+      { const float2 c = t[1], e = u[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); cr = fmaf(s1.x, e.x, cr); ci = fmaf(s1.y, e.x, ci); dr = fmaf(d1.x, e.y, dr); di = fmaf(d1.y, e.y, di); }
+      { const float2 c = t[2], e = u[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); cr = fmaf(s2.x, e.x, cr); ci = fmaf(s2.y, e.x, ci); dr = fmaf(d2.x, e.y, dr); di = fmaf(d2.y, e.y, di); }
+      { const float2 c = t[3], e = u[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); cr = fmaf(s3.x, e.x, cr); ci = fmaf(s3.y, e.x, ci); dr = fmaf(d3.x, e.y, dr); di = fmaf(d3.y, e.y, di); }
+      { const float2 c = t[4], e = u[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); cr = fmaf(s4.x, e.x, cr); ci = fmaf(s4.y, e.x, ci); dr = fmaf(d4.x, e.y, dr); di = fmaf(d4.y, e.y, di); }
+      { const float2 c = t[5], e = u[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); cr = fmaf(s5.x, e.x, cr); ci = fmaf(s5.y, e.x, ci); dr = fmaf(d5.x, e.y, dr); di = fmaf(d5.y, e.y, di); }
+      { const float2 c = t[6], e = u[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); cr = fmaf(s6.x, e.x, cr); ci = fmaf(s6.y, e.x, ci); dr = fmaf(d6.x, e.y, dr); di = fmaf(d6.y, e.y, di); }
+      { const float2 c = t[7], e = u[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); cr = fmaf(s7.x, e.x, cr); ci = fmaf(s7.y, e.x, ci); dr = fmaf(d7.x, e.y, dr); di = fmaf(d7.y, e.y, di); }
+      { const float2 c = t[8], e = u[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); cr = fmaf(s8.x, e.x, cr); ci = fmaf(s8.y, e.x, ci); dr = fmaf(d8.x, e.y, dr); di = fmaf(d8.y, e.y, di); }
+      { const float2 c = t[9], e = u[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); cr = fmaf(s9.x, e.x, cr); ci = fmaf(s9.y, e.x, ci); dr = fmaf(d9.x, e.y, dr); di = fmaf(d9.y, e.y, di); }
+      { const float2 c = t[10], e = u[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); cr = fmaf(s10.x, e.x, cr); ci = fmaf(s10.y, e.x, ci); dr = fmaf(d10.x, e.y, dr); di = fmaf(d10.y, e.y, di); }
+      { const float2 c = t[11], e = u[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); cr = fmaf(s11.x, e.x, cr); ci = fmaf(s11.y, e.x, ci); dr = fmaf(d11.x, e.y, dr); di = fmaf(d11.y, e.y, di); }
+      { const float2 c = t[12], e = u[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); cr = fmaf(s12.x, e.x, cr); ci = fmaf(s12.y, e.x, ci); dr = fmaf(d12.x, e.y, dr); di = fmaf(d12.y, e.y, di); }
+      { const float2 c = t[13], e = u[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); cr = fmaf(s13.x, e.x, cr); ci = fmaf(s13.y, e.x, ci); dr = fmaf(d13.x, e.y, dr); di = fmaf(d13.y, e.y, di); }
+      { const float2 c = t[14], e = u[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); cr = fmaf(s14.x, e.x, cr); ci = fmaf(s14.y, e.x, ci); dr = fmaf(d14.x, e.y, dr); di = fmaf(d14.y, e.y, di); }
+      { const float2 c = t[15], e = u[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); cr = fmaf(s15.x, e.x, cr); ci = fmaf(s15.y, e.x, ci); dr = fmaf(d15.x, e.y, dr); di = fmaf(d15.y, e.y, di); }
+      { const float2 c = t[16], e = u[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); cr = fmaf(s16.x, e.x, cr); ci = fmaf(s16.y, e.x, ci); dr = fmaf(d16.x, e.y, dr); di = fmaf(d16.y, e.y, di); }
+      { const float2 c = t[17], e = u[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); cr = fmaf(s17.x, e.x, cr); ci = fmaf(s17.y, e.x, ci); dr = fmaf(d17.x, e.y, dr); di = fmaf(d17.y, e.y, di); }
+      { const float2 c = t[18], e = u[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); cr = fmaf(s18.x, e.x, cr); ci = fmaf(s18.y, e.x, ci); dr = fmaf(d18.x, e.y, dr); di = fmaf(d18.y, e.y, di); }
+      { const float2 c = t[19], e = u[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); cr = fmaf(s19.x, e.x, cr); ci = fmaf(s19.y, e.x, ci); dr = fmaf(d19.x, e.y, dr); di = fmaf(d19.y, e.y, di); }
+      { const float2 c = t[20], e = u[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); cr = fmaf(s20.x, e.x, cr); ci = fmaf(s20.y, e.x, ci); dr = fmaf(d20.x, e.y, dr); di = fmaf(d20.y, e.y, di); }
+      { const float2 c = t[21], e = u[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); cr = fmaf(s21.x, e.x, cr); ci = fmaf(s21.y, e.x, ci); dr = fmaf(d21.x, e.y, dr); di = fmaf(d21.y, e.y, di); }
+      { const float2 c = t[22], e = u[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); cr = fmaf(s22.x, e.x, cr); ci = fmaf(s22.y, e.x, ci); dr = fmaf(d22.x, e.y, dr); di = fmaf(d22.y, e.y, di); }
+      { const float2 c = t[23], e = u[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); cr = fmaf(s23.x, e.x, cr); ci = fmaf(s23.y, e.x, ci); dr = fmaf(d23.x, e.y, dr); di = fmaf(d23.y, e.y, di); }
+      { const float2 c = t[24], e = u[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); cr = fmaf(s24.x, e.x, cr); ci = fmaf(s24.y, e.x, ci); dr = fmaf(d24.x, e.y, dr); di = fmaf(d24.y, e.y, di); }
+      { const float2 c = t[25], e = u[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); cr = fmaf(s25.x, e.x, cr); ci = fmaf(s25.y, e.x, ci); dr = fmaf(d25.x, e.y, dr); di = fmaf(d25.y, e.y, di); }
+      { const float2 c = t[26], e = u[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); cr = fmaf(s26.x, e.x, cr); ci = fmaf(s26.y, e.x, ci); dr = fmaf(d26.x, e.y, dr); di = fmaf(d26.y, e.y, di); }
+      const int k2 = k + 13;
+      if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - k, make_float2(ar - bi, ai + br)); st(k2, make_float2(cr + di, ci - dr)); st(53 - k2, make_float2(cr - di, ci + dr)); }
+      else { st(k, make_float2(ar - bi, ai + br)); st(53 - k, make_float2(ar + bi, ai - br)); st(k2, make_float2(cr - di, ci + dr)); st(53 - k2, make_float2(cr + di, ci - dr)); }
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 1; k <= 26; k++) {
+      const float2* t = c_tw53[k];
+      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
+      { const float2 c = t[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); }
+      { const float2 c = t[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); }
+      { const float2 c = t[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); }
+      { const float2 c = t[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); }
+      { const float2 c = t[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); }
+      { const float2 c = t[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); }
+      { const float2 c = t[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); }
+      { const float2 c = t[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); }
+      { const float2 c = t[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); }
+      { const float2 c = t[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); }
+      { const float2 c = t[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); }
+      { const float2 c = t[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); }
+      { const float2 c = t[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); }
+      { const float2 c = t[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); }
+      { const float2 c = t[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); }
+      { const float2 c = t[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); }
+      { const float2 c = t[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); }
+      { const float2 c = t[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); }
+      { const float2 c = t[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); }
+      { const float2 c = t[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); }
+      { const float2 c = t[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); }
+      { const float2 c = t[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); }
+      { const float2 c = t[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); }
+      { const float2 c = t[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); }
+      { const float2 c = t[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); }
+      { const float2 c = t[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); }
+      if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - (k), make_float2(ar - bi, ai + br)); }
+      else { st(k, make_float2(ar - bi, ai + br)); st(53 - (k), make_float2(ar + bi, ai - br)); }
+    }
   }
 }
 }  // namespace mc

@@ -125,9 +125,15 @@ bool two_level_split(int n, int& n1, int& n2);
 cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st);
 cudaError_t launch_rows_fft2l(const RowsFftArgs& a, bool inverse, cudaStream_t st);
 
+cudaError_t launch_fwd_rows_dif(const FwdRowsArgs& a, cudaStream_t st);
+cudaError_t launch_rows_fft_dif(const RowsFftArgs& a, cudaStream_t st);
+bool dif_supported(int n);
+
 cudaError_t launch_fwd_rows(const FwdRowsArgs& a, cudaStream_t st) {
   int n1, n2;
   if (two_level_split(a.nu, n1, n2)) return launch_fwd_rows2l(a, st);
+  const bool raw = !a.two_outputs && !a.dark && !a.dark2 && !a.norm && !a.norm2;
+  if (raw && dif_supported(a.nu)) return launch_fwd_rows_dif(a, st);
   const size_t smem = fwd_rows_smem(a.nu);
   cudaError_t e = allow_smem((const void*)k_fwd_rows, smem);
   if (e != cudaSuccess) return e;
@@ -171,6 +177,7 @@ size_t rows_fft_smem(int n, int rows_per_cta) {
 cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta, cudaStream_t st) {
   int n1, n2;
   if (two_level_split(a.plan.n, n1, n2)) return launch_rows_fft2l(a, inverse, st);
+  if (!inverse && dif_supported(a.plan.n)) return launch_rows_fft_dif(a, st);
   const size_t smem = rows_fft_smem(a.plan.n, rows_per_cta);
   const int grid = (a.nrows + rows_per_cta - 1) / rows_per_cta;
   cudaError_t e;
@@ -200,8 +207,16 @@ __device__ __forceinline__ void fft_n1(float2* v) {
 }
 
 // Resident CTAs per SM the two-level transforms are compiled for (register cap).
+// MC_FWD_PAIRED / MC_COL_PAIRED: two radix-53 output pairs per loop iteration
+// in the forward row / column transforms.
+#ifndef MC_FWD_PAIRED
+#define MC_FWD_PAIRED false
+#endif
+#ifndef MC_COL_PAIRED
+#define MC_COL_PAIRED false
+#endif
 #ifndef MC_TL_MIN_BLOCKS
-#define MC_TL_MIN_BLOCKS 1
+#define MC_TL_MIN_BLOCKS 4
 #endif
 
 template <int N1, int N2>
@@ -210,10 +225,10 @@ struct TwoLevel {
   static constexpr int T = ((N1 > N2 ? N1 : N2) + 31) / 32 * 32;
 
   // step A + exchange + step B; load(i) gives x[i], store(k, X[k]) takes the
-  // result.  T >= N2, so each thread owns at most one k2 in step B; with
-  // SYNC_STORE the stores wait for every thread's step-B reads, which lets
-  // store() write back into ysm.
-  template <bool INV, bool SYNC_STORE, class Load, class Store>
+  // result; tw[TWS * j] = exp(-2 pi i j / N).  T >= N2, so each thread owns at most one k2 in step B; with
+  // SYNC_STORE a barrier follows every thread's step-B reads of ysm, which
+  // lets store() write back into ysm.
+  template <bool INV, bool SYNC_STORE, bool PAIRED = false, int TWS = 1, class Load, class Store>
   __device__ static void run(float2* ysm, const float2* __restrict__ tw, Load&& load, Store&& store) {
     static_assert(T >= N2, "one k2 per thread");
     const int lt = threadIdx.x;
@@ -224,7 +239,7 @@ struct TwoLevel {
       fft_reg<N2, INV>(x);
 #pragma unroll
       for (int k2 = 0; k2 < N2; k2++) {
-        float2 w = __ldg(tw + lt * k2);
+        float2 w = __ldg(tw + TWS * lt * k2);
         if (INV) w.y = -w.y;
         ysm[k2 * N1 + lt] = k2 ? cmul(x[k2], w) : x[k2];
       }
@@ -236,12 +251,12 @@ struct TwoLevel {
 #pragma unroll
       for (int n1 = 0; n1 < N1; n1++) v[n1] = ysm[lt * N1 + n1];
     }
-    if constexpr (N1 == 53 && !SYNC_STORE) {
+    if (SYNC_STORE) __syncthreads();
+    if constexpr (N1 == 53) {
       // compact radix-53 DFT: small code, outputs stored as they are formed
-      if (act) dft_r53_compact<INV>(v, [&](int k1, float2 x) { store(lt + N2 * k1, x); });
+      if (act) dft_r53_compact<INV, PAIRED>(v, [&](int k1, float2 x) { store(lt + N2 * k1, x); });
     } else {
       if (act) fft_n1<N1, INV>(v);
-      if (SYNC_STORE) __syncthreads();
       if (act) {
 #pragma unroll
         for (int k1 = 0; k1 < N1; k1++) store(lt + N2 * k1, v[k1]);
@@ -260,7 +275,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_
   float2* out = a.out + row * a.ld_out;
   const int shift = TL::N - a.n_out, keep = a.keep_lo;
   const float sc = a.scale;
-  TL::template run<INV, false>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
+  TL::template run<INV, false, MC_COL_PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
                         [&](int k, float2 v) {
                           int o;
                           if (k < keep) o = k;
@@ -301,6 +316,70 @@ __device__ __forceinline__ void stage_rows(float2* xin, const FwdRowsArgs& a, lo
   } else {
 #pragma unroll 8
     for (int x = threadIdx.x; x < n; x += nth) xin[x] = make_float2((float)f[r0 + x], (float)f[r1 + x]);
+  }
+}
+
+// Raw pixels of one crop row into shared memory with aligned 16-byte loads:
+// the bytes of [src, src + n) land at dst[d + i] with d = src mod 16, so
+// every interior 16-byte chunk keeps its alignment in shared memory; the
+// unaligned head and tail go pixel by pixel.  Every load stays inside the row.
+template <typename Px>
+__device__ __forceinline__ void stage_raw_row(unsigned char* dst, const Px* src, int n, int tid, int nth) {
+  const uintptr_t s = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t e = s + (uintptr_t)n * sizeof(Px);
+  const uintptr_t a0 = s & ~(uintptr_t)15;
+  uintptr_t as = (s + 15) & ~(uintptr_t)15;
+  uintptr_t ae = e & ~(uintptr_t)15;
+  if (as > ae) as = ae = e;  // row shorter than one aligned chunk: all pixel by pixel
+  const int head = (int)((as - s) / sizeof(Px)), tail0 = (int)((ae - s) / sizeof(Px));
+  Px* dpx = reinterpret_cast<Px*>(dst + (s - a0));
+  for (int i = tid; i < head; i += nth) dpx[i] = src[i];
+  for (int i = tail0 + tid; i < n; i += nth) dpx[i] = src[i];
+  const int chunks = (int)((ae - as) / 16);
+  const uint4* g = reinterpret_cast<const uint4*>(as);
+  uint4* d4 = reinterpret_cast<uint4*>(dst + (as - a0));
+  for (int c = tid; c < chunks; c += nth) d4[c] = __ldg(g + c);
+}
+
+// Shared bytes one staged row takes: n pixels + up to 15 bytes of alignment,
+// rounded to 16.
+template <typename Px>
+constexpr int raw_row_bytes(int n) {
+  return (n * (int)sizeof(Px) + 15 + 15) / 16 * 16;
+}
+
+// Forward rows without references: two rows staged as raw pixels (a quarter
+// of the float staging for 8-bit frames), decoded in the step-A loads; the
+// spectrum Z is written back into the exchange buffer after the barrier that
+// follows the step-B reads.
+template <int N1, int N2, typename Px>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows2l_raw(FwdRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  constexpr int RB = raw_row_bytes<Px>(N);
+  extern __shared__ float2 dynraw[];
+  float2* ysm = dynraw;
+  unsigned char* raw0 = reinterpret_cast<unsigned char*>(dynraw + N);
+  unsigned char* raw1 = raw0 + RB;
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const Px* row0 = f + (long long)(a.offy + y0) * a.nx + a.offx;
+  const Px* row1 = f + (long long)(a.offy + y1) * a.nx + a.offx;
+  stage_raw_row<Px>(raw0, row0, N, threadIdx.x, TL::T);
+  stage_raw_row<Px>(raw1, row1, N, threadIdx.x, TL::T);
+  __syncthreads();
+  const Px* p0 = reinterpret_cast<const Px*>(raw0 + (reinterpret_cast<uintptr_t>(row0) & 15));
+  const Px* p1 = reinterpret_cast<const Px*>(raw1 + (reinterpret_cast<uintptr_t>(row1) & 15));
+  TL::template run<false, true, MC_FWD_PAIRED>(
+      ysm, a.tw, [&](int x) { return make_float2((float)p0[x], (float)p1[x]); },
+      [&](int k, float2 v) { ysm[k] = v; });
+  __syncthreads();
+  for (int k = threadIdx.x; k < a.hk; k += TL::T) {
+    const float2 z = ysm[k];
+    const float2 zc = ysm[k == 0 ? 0 : N - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    *reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0) = make_float4(X.x, X.y, Y.x, Y.y);
   }
 }
 
@@ -348,6 +427,99 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
   }
 }
 
+// ---------------------------------------------------------------------------
+// Lengths L = 2N with a two-level N (7420 = 2 x 3710 at -bin 2): one radix-2
+// decimation-in-frequency step folded into the step-A loads,
+//   A[m] = FFT_N(z_n + z_{n+N})[m] = Z[2m],
+//   B[m] = FFT_N((z_n - z_{n+N}) W_L^n)[m] = Z[2m+1],
+// then the two N-point two-level transforms, whose outputs go straight to
+// the kept indices.  tw is the L-entry table exp(-2 pi i j / L).
+
+// Forward rows of length L without references: two rows staged as raw
+// pixels; only the Z indices the half-spectrum split needs are kept in
+// shared memory (Z[0, hk) and Z(L - hk, L)).
+template <int N1, int N2, typename Px>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows_dif(FwdRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N, L = 2 * N;
+  constexpr int RB = raw_row_bytes<Px>(L);
+  extern __shared__ float2 dyndif[];
+  const int hk = a.hk;
+  float2* ysm = dyndif;
+  float2* zlo = dyndif + N;   // Z[0 .. hk-1]
+  float2* zhi = zlo + hk;     // Z[L-hk+1 .. L-1]
+  unsigned char* raw0 = reinterpret_cast<unsigned char*>(zhi + hk);
+  unsigned char* raw1 = raw0 + RB;
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const Px* row0 = f + (long long)(a.offy + y0) * a.nx + a.offx;
+  const Px* row1 = f + (long long)(a.offy + y1) * a.nx + a.offx;
+  stage_raw_row<Px>(raw0, row0, L, threadIdx.x, TL::T);
+  stage_raw_row<Px>(raw1, row1, L, threadIdx.x, TL::T);
+  __syncthreads();
+  const Px* p0 = reinterpret_cast<const Px*>(raw0 + (reinterpret_cast<uintptr_t>(row0) & 15));
+  const Px* p1 = reinterpret_cast<const Px*>(raw1 + (reinterpret_cast<uintptr_t>(row1) & 15));
+  const float2* tw = a.tw;
+  auto keep = [&](int idx, float2 v) {
+    if (idx < hk) zlo[idx] = v;
+    else if (idx > L - hk) zhi[idx - (L - hk + 1)] = v;
+  };
+  TL::template run<false, false, MC_FWD_PAIRED, 2>(
+      ysm, tw,
+      [&](int n) {
+        return make_float2((float)p0[n] + (float)p0[n + N], (float)p1[n] + (float)p1[n + N]);
+      },
+      [&](int m, float2 v) { keep(2 * m, v); });
+  __syncthreads();
+  TL::template run<false, false, MC_FWD_PAIRED, 2>(
+      ysm, tw,
+      [&](int n) {
+        const float2 d = make_float2((float)p0[n] - (float)p0[n + N], (float)p1[n] - (float)p1[n + N]);
+        return cmul(d, __ldg(tw + n));
+      },
+      [&](int m, float2 v) { keep(2 * m + 1, v); });
+  __syncthreads();
+  for (int k = threadIdx.x; k < hk; k += TL::T) {
+    const float2 z = zlo[k];
+    const float2 zc = k == 0 ? zlo[0] : zhi[hk - 1 - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    *reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0) = make_float4(X.x, X.y, Y.x, Y.y);
+  }
+}
+
+// Forward columns of length L: out_row[i] = scale * X[i < keep_lo ? i : i + (L - n_out)].
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_fft_dif(RowsFftArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N, L = 2 * N;
+  __shared__ float2 ysm[N];
+  const long long row = blockIdx.x;
+  const float2* in = a.in + row * a.ld_in;
+  float2* out = a.out + row * a.ld_out;
+  const int shift = L - a.n_out, keep = a.keep_lo;
+  const float sc = a.scale;
+  const float2* tw = a.tw;
+  auto put = [&](int i, float2 v) {
+    int o;
+    if (i < keep) o = i;
+    else if (i >= keep + shift) o = i - shift;
+    else return;
+    out[o] = make_float2(v.x * sc, v.y * sc);
+  };
+  TL::template run<false, false, MC_COL_PAIRED, 2>(
+      ysm, tw, [&](int n) { return cadd(__ldg(in + n), __ldg(in + n + N)); },
+      [&](int m, float2 v) { put(2 * m, v); });
+  __syncthreads();
+  TL::template run<false, false, MC_COL_PAIRED, 2>(
+      ysm, tw,
+      [&](int n) {
+        const float2 x0 = __ldg(in + n), x1 = __ldg(in + n + N);
+        return cmul(make_float2(x0.x - x1.x, x0.y - x1.y), __ldg(tw + n));
+      },
+      [&](int m, float2 v) { put(2 * m + 1, v); });
+}
+
 // Two-level splits compiled in (N1, N2).
 #define MC_TWO_LEVEL_LIST(X) X(53, 70) X(64, 64) X(32, 64) X(32, 32) X(16, 16) X(16, 32)
 
@@ -381,8 +553,25 @@ cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
   int n1 = 0, n2 = 0;
   if (!two_level_split(a.nu, n1, n2)) return cudaErrorInvalidValue;
   const int grid = a.two_outputs ? a.nu : a.nu / 2;
+  const bool raw = !a.two_outputs && !a.dark && !a.dark2 && !a.norm && !a.norm2;
+#define MC_TL_RAW(A, B, PX)                                                                          \
+  {                                                                                                  \
+    const size_t smem = (size_t)(A) * (B) * sizeof(float2) + 2 * (size_t)raw_row_bytes<PX>((A) * (B)); \
+    cudaError_t e = allow_smem((const void*)k_fwd_rows2l_raw<A, B, PX>, smem);                       \
+    if (e != cudaSuccess) return e;                                                                  \
+    k_fwd_rows2l_raw<A, B, PX><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                            \
+    return cudaGetLastError();                                                                       \
+  }
 #define MC_TL_LAUNCH(A, B)                                                                           \
   if (n1 == (A) && n2 == (B)) {                                                                      \
+    if (raw) {                                                                                       \
+      switch (a.mode) {                                                                              \
+        case 0: MC_TL_RAW(A, B, int8_t)                                                              \
+        case 1: MC_TL_RAW(A, B, int16_t)                                                             \
+        case 6: MC_TL_RAW(A, B, uint16_t)                                                            \
+        default: MC_TL_RAW(A, B, float)                                                              \
+      }                                                                                              \
+    }                                                                                                \
     const size_t smem = (size_t)2 * (A) * (B) * sizeof(float2);                                      \
     cudaError_t e = allow_smem((const void*)k_fwd_rows2l<A, B>, smem);                               \
     if (e != cudaSuccess) return e;                                                                  \
@@ -391,6 +580,53 @@ cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
   }
   MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)
 #undef MC_TL_LAUNCH
+#undef MC_TL_RAW
+  return cudaErrorInvalidValue;
+}
+
+bool dif_supported(int n) {
+  int n1, n2;
+  return n % 2 == 0 && two_level_split(n / 2, n1, n2);
+}
+
+cudaError_t launch_fwd_rows_dif(const FwdRowsArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (a.nu % 2 || !two_level_split(a.nu / 2, n1, n2)) return cudaErrorInvalidValue;
+  const int grid = a.nu / 2;
+#define MC_DIF_RAW(A, B, PX)                                                                          \
+  {                                                                                                   \
+    const size_t smem = ((size_t)(A) * (B) + 2 * (size_t)a.hk) * sizeof(float2) +                     \
+                        2 * (size_t)raw_row_bytes<PX>(2 * (A) * (B));                                 \
+    cudaError_t e = allow_smem((const void*)k_fwd_rows_dif<A, B, PX>, smem);                          \
+    if (e != cudaSuccess) return e;                                                                   \
+    k_fwd_rows_dif<A, B, PX><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                               \
+    return cudaGetLastError();                                                                        \
+  }
+#define MC_DIF_LAUNCH(A, B)                                                                           \
+  if (n1 == (A) && n2 == (B)) {                                                                       \
+    switch (a.mode) {                                                                                 \
+      case 0: MC_DIF_RAW(A, B, int8_t)                                                                \
+      case 1: MC_DIF_RAW(A, B, int16_t)                                                               \
+      case 6: MC_DIF_RAW(A, B, uint16_t)                                                              \
+      default: MC_DIF_RAW(A, B, float)                                                                \
+    }                                                                                                 \
+  }
+  MC_TWO_LEVEL_LIST(MC_DIF_LAUNCH)
+#undef MC_DIF_LAUNCH
+#undef MC_DIF_RAW
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rows_fft_dif(const RowsFftArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (a.plan.n % 2 || !two_level_split(a.plan.n / 2, n1, n2)) return cudaErrorInvalidValue;
+#define MC_DIF_LAUNCH(A, B)                                                        \
+  if (n1 == (A) && n2 == (B)) {                                                    \
+    k_rows_fft_dif<A, B><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);                \
+    return cudaGetLastError();                                                     \
+  }
+  MC_TWO_LEVEL_LIST(MC_DIF_LAUNCH)
+#undef MC_DIF_LAUNCH
   return cudaErrorInvalidValue;
 }
 

@@ -115,6 +115,12 @@ def test_fft_engine(gpu, n):
     (424, 430, 6, 0, 0, 0, 2.0),
     (260, 250, 2, 3, 5, 200, 1.0),
     (300, 300, 2, 0, 0, 0, 1.5),
+    # -bin 2 from 2N with a two-level N: the radix-2 split kernels (raw staging
+    # of every pixel type, unaligned crop rows)
+    (520, 512, 0, 0, 0, 0, 2.0),
+    (512, 530, 1, 0, 0, 0, 2.0),
+    (515, 520, 6, 3, 0, 0, 2.0),
+    (2060, 2050, 2, 5, 1, 2048, 2.0),
 ])
 def test_forward_matches_oracle(gpu, nx, ny, mode, offx, offy, crd, bin_):
     rng = np.random.default_rng(nx + ny)
@@ -240,4 +246,14 @@ def test_pipeline_3710_crop(gpu):
     mv = synth.make_movie(3730, 3710, 6, mean=1.2, seed=2, dtype="u8", speed=0.3, rw_sigma=0.5)
     g, ref, p = run_both(mv.frames, 0, api.Params(FrameDistOffset=1))
     assert ref.nsam == 3710
+    compare_full(g, ref, 3710, 0)
+
+
+@pytest.mark.slow
+def test_pipeline_c3_geometry(gpu):
+    """The c3 geometry (7676x7420 class, -bin 2: forward at 7420 = 2*3710,
+    Fourier crop to 3710) on a short stack."""
+    mv = synth.make_movie(7440, 7420, 4, mean=0.3, seed=12, dtype="u8", speed=0.3, rw_sigma=0.5)
+    g, ref, p = run_both(mv.frames, 0, api.Params(bin=2.0, FrameDistOffset=1))
+    assert (ref.nsam_unbin, ref.nsam) == (7420, 3710)
     compare_full(g, ref, 3710, 0)
