@@ -2,12 +2,13 @@
 // Straight-line odd-radix DFT butterflies (symmetric direct form).
 #pragma once
 #include <cuda_runtime.h>
+#include "f2ops.cuh"
 namespace mc {
 constexpr int kGeneratedOddRadices[] = {3, 5, 7, 11, 13, 53};
 template <bool INV> __device__ __forceinline__ void dft_r3(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[2].x, v[1].y + v[2].y);
-  const float2 d1 = make_float2(v[1].x - v[2].x, v[1].y - v[2].y);
+  const float2 s1 = padd(v[1], v[2]);
+  const float2 d1 = psub(v[1], v[2]);
   v[0] = make_float2(x0.x + (s1.x), x0.y + (s1.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -21,10 +22,10 @@ template <bool INV> __device__ __forceinline__ void dft_r3(float2* v) {
 }
 template <bool INV> __device__ __forceinline__ void dft_r5(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[4].x, v[1].y + v[4].y);
-  const float2 d1 = make_float2(v[1].x - v[4].x, v[1].y - v[4].y);
-  const float2 s2 = make_float2(v[2].x + v[3].x, v[2].y + v[3].y);
-  const float2 d2 = make_float2(v[2].x - v[3].x, v[2].y - v[3].y);
+  const float2 s1 = padd(v[1], v[4]);
+  const float2 d1 = psub(v[1], v[4]);
+  const float2 s2 = padd(v[2], v[3]);
+  const float2 d2 = psub(v[2], v[3]);
   v[0] = make_float2(x0.x + (s1.x + s2.x), x0.y + (s1.y + s2.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -49,12 +50,12 @@ template <bool INV> __device__ __forceinline__ void dft_r5(float2* v) {
 }
 template <bool INV> __device__ __forceinline__ void dft_r7(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[6].x, v[1].y + v[6].y);
-  const float2 d1 = make_float2(v[1].x - v[6].x, v[1].y - v[6].y);
-  const float2 s2 = make_float2(v[2].x + v[5].x, v[2].y + v[5].y);
-  const float2 d2 = make_float2(v[2].x - v[5].x, v[2].y - v[5].y);
-  const float2 s3 = make_float2(v[3].x + v[4].x, v[3].y + v[4].y);
-  const float2 d3 = make_float2(v[3].x - v[4].x, v[3].y - v[4].y);
+  const float2 s1 = padd(v[1], v[6]);
+  const float2 d1 = psub(v[1], v[6]);
+  const float2 s2 = padd(v[2], v[5]);
+  const float2 d2 = psub(v[2], v[5]);
+  const float2 s3 = padd(v[3], v[4]);
+  const float2 d3 = psub(v[3], v[4]);
   v[0] = make_float2(x0.x + (s1.x + s2.x + s3.x), x0.y + (s1.y + s2.y + s3.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -92,16 +93,16 @@ template <bool INV> __device__ __forceinline__ void dft_r7(float2* v) {
 }
 template <bool INV> __device__ __forceinline__ void dft_r11(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[10].x, v[1].y + v[10].y);
-  const float2 d1 = make_float2(v[1].x - v[10].x, v[1].y - v[10].y);
-  const float2 s2 = make_float2(v[2].x + v[9].x, v[2].y + v[9].y);
-  const float2 d2 = make_float2(v[2].x - v[9].x, v[2].y - v[9].y);
-  const float2 s3 = make_float2(v[3].x + v[8].x, v[3].y + v[8].y);
-  const float2 d3 = make_float2(v[3].x - v[8].x, v[3].y - v[8].y);
-  const float2 s4 = make_float2(v[4].x + v[7].x, v[4].y + v[7].y);
-  const float2 d4 = make_float2(v[4].x - v[7].x, v[4].y - v[7].y);
-  const float2 s5 = make_float2(v[5].x + v[6].x, v[5].y + v[6].y);
-  const float2 d5 = make_float2(v[5].x - v[6].x, v[5].y - v[6].y);
+  const float2 s1 = padd(v[1], v[10]);
+  const float2 d1 = psub(v[1], v[10]);
+  const float2 s2 = padd(v[2], v[9]);
+  const float2 d2 = psub(v[2], v[9]);
+  const float2 s3 = padd(v[3], v[8]);
+  const float2 d3 = psub(v[3], v[8]);
+  const float2 s4 = padd(v[4], v[7]);
+  const float2 d4 = psub(v[4], v[7]);
+  const float2 s5 = padd(v[5], v[6]);
+  const float2 d5 = psub(v[5], v[6]);
   v[0] = make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -171,18 +172,18 @@ template <bool INV> __device__ __forceinline__ void dft_r11(float2* v) {
 }
 template <bool INV> __device__ __forceinline__ void dft_r13(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[12].x, v[1].y + v[12].y);
-  const float2 d1 = make_float2(v[1].x - v[12].x, v[1].y - v[12].y);
-  const float2 s2 = make_float2(v[2].x + v[11].x, v[2].y + v[11].y);
-  const float2 d2 = make_float2(v[2].x - v[11].x, v[2].y - v[11].y);
-  const float2 s3 = make_float2(v[3].x + v[10].x, v[3].y + v[10].y);
-  const float2 d3 = make_float2(v[3].x - v[10].x, v[3].y - v[10].y);
-  const float2 s4 = make_float2(v[4].x + v[9].x, v[4].y + v[9].y);
-  const float2 d4 = make_float2(v[4].x - v[9].x, v[4].y - v[9].y);
-  const float2 s5 = make_float2(v[5].x + v[8].x, v[5].y + v[8].y);
-  const float2 d5 = make_float2(v[5].x - v[8].x, v[5].y - v[8].y);
-  const float2 s6 = make_float2(v[6].x + v[7].x, v[6].y + v[7].y);
-  const float2 d6 = make_float2(v[6].x - v[7].x, v[6].y - v[7].y);
+  const float2 s1 = padd(v[1], v[12]);
+  const float2 d1 = psub(v[1], v[12]);
+  const float2 s2 = padd(v[2], v[11]);
+  const float2 d2 = psub(v[2], v[11]);
+  const float2 s3 = padd(v[3], v[10]);
+  const float2 d3 = psub(v[3], v[10]);
+  const float2 s4 = padd(v[4], v[9]);
+  const float2 d4 = psub(v[4], v[9]);
+  const float2 s5 = padd(v[5], v[8]);
+  const float2 d5 = psub(v[5], v[8]);
+  const float2 s6 = padd(v[6], v[7]);
+  const float2 d6 = psub(v[6], v[7]);
   v[0] = make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -271,58 +272,58 @@ template <bool INV> __device__ __forceinline__ void dft_r13(float2* v) {
 }
 template <bool INV> __device__ __forceinline__ void dft_r53(float2* v) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
-  const float2 d1 = make_float2(v[1].x - v[52].x, v[1].y - v[52].y);
-  const float2 s2 = make_float2(v[2].x + v[51].x, v[2].y + v[51].y);
-  const float2 d2 = make_float2(v[2].x - v[51].x, v[2].y - v[51].y);
-  const float2 s3 = make_float2(v[3].x + v[50].x, v[3].y + v[50].y);
-  const float2 d3 = make_float2(v[3].x - v[50].x, v[3].y - v[50].y);
-  const float2 s4 = make_float2(v[4].x + v[49].x, v[4].y + v[49].y);
-  const float2 d4 = make_float2(v[4].x - v[49].x, v[4].y - v[49].y);
-  const float2 s5 = make_float2(v[5].x + v[48].x, v[5].y + v[48].y);
-  const float2 d5 = make_float2(v[5].x - v[48].x, v[5].y - v[48].y);
-  const float2 s6 = make_float2(v[6].x + v[47].x, v[6].y + v[47].y);
-  const float2 d6 = make_float2(v[6].x - v[47].x, v[6].y - v[47].y);
-  const float2 s7 = make_float2(v[7].x + v[46].x, v[7].y + v[46].y);
-  const float2 d7 = make_float2(v[7].x - v[46].x, v[7].y - v[46].y);
-  const float2 s8 = make_float2(v[8].x + v[45].x, v[8].y + v[45].y);
-  const float2 d8 = make_float2(v[8].x - v[45].x, v[8].y - v[45].y);
-  const float2 s9 = make_float2(v[9].x + v[44].x, v[9].y + v[44].y);
-  const float2 d9 = make_float2(v[9].x - v[44].x, v[9].y - v[44].y);
-  const float2 s10 = make_float2(v[10].x + v[43].x, v[10].y + v[43].y);
-  const float2 d10 = make_float2(v[10].x - v[43].x, v[10].y - v[43].y);
-  const float2 s11 = make_float2(v[11].x + v[42].x, v[11].y + v[42].y);
-  const float2 d11 = make_float2(v[11].x - v[42].x, v[11].y - v[42].y);
-  const float2 s12 = make_float2(v[12].x + v[41].x, v[12].y + v[41].y);
-  const float2 d12 = make_float2(v[12].x - v[41].x, v[12].y - v[41].y);
-  const float2 s13 = make_float2(v[13].x + v[40].x, v[13].y + v[40].y);
-  const float2 d13 = make_float2(v[13].x - v[40].x, v[13].y - v[40].y);
-  const float2 s14 = make_float2(v[14].x + v[39].x, v[14].y + v[39].y);
-  const float2 d14 = make_float2(v[14].x - v[39].x, v[14].y - v[39].y);
-  const float2 s15 = make_float2(v[15].x + v[38].x, v[15].y + v[38].y);
-  const float2 d15 = make_float2(v[15].x - v[38].x, v[15].y - v[38].y);
-  const float2 s16 = make_float2(v[16].x + v[37].x, v[16].y + v[37].y);
-  const float2 d16 = make_float2(v[16].x - v[37].x, v[16].y - v[37].y);
-  const float2 s17 = make_float2(v[17].x + v[36].x, v[17].y + v[36].y);
-  const float2 d17 = make_float2(v[17].x - v[36].x, v[17].y - v[36].y);
-  const float2 s18 = make_float2(v[18].x + v[35].x, v[18].y + v[35].y);
-  const float2 d18 = make_float2(v[18].x - v[35].x, v[18].y - v[35].y);
-  const float2 s19 = make_float2(v[19].x + v[34].x, v[19].y + v[34].y);
-  const float2 d19 = make_float2(v[19].x - v[34].x, v[19].y - v[34].y);
-  const float2 s20 = make_float2(v[20].x + v[33].x, v[20].y + v[33].y);
-  const float2 d20 = make_float2(v[20].x - v[33].x, v[20].y - v[33].y);
-  const float2 s21 = make_float2(v[21].x + v[32].x, v[21].y + v[32].y);
-  const float2 d21 = make_float2(v[21].x - v[32].x, v[21].y - v[32].y);
-  const float2 s22 = make_float2(v[22].x + v[31].x, v[22].y + v[31].y);
-  const float2 d22 = make_float2(v[22].x - v[31].x, v[22].y - v[31].y);
-  const float2 s23 = make_float2(v[23].x + v[30].x, v[23].y + v[30].y);
-  const float2 d23 = make_float2(v[23].x - v[30].x, v[23].y - v[30].y);
-  const float2 s24 = make_float2(v[24].x + v[29].x, v[24].y + v[29].y);
-  const float2 d24 = make_float2(v[24].x - v[29].x, v[24].y - v[29].y);
-  const float2 s25 = make_float2(v[25].x + v[28].x, v[25].y + v[28].y);
-  const float2 d25 = make_float2(v[25].x - v[28].x, v[25].y - v[28].y);
-  const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
-  const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
+  const float2 s1 = padd(v[1], v[52]);
+  const float2 d1 = psub(v[1], v[52]);
+  const float2 s2 = padd(v[2], v[51]);
+  const float2 d2 = psub(v[2], v[51]);
+  const float2 s3 = padd(v[3], v[50]);
+  const float2 d3 = psub(v[3], v[50]);
+  const float2 s4 = padd(v[4], v[49]);
+  const float2 d4 = psub(v[4], v[49]);
+  const float2 s5 = padd(v[5], v[48]);
+  const float2 d5 = psub(v[5], v[48]);
+  const float2 s6 = padd(v[6], v[47]);
+  const float2 d6 = psub(v[6], v[47]);
+  const float2 s7 = padd(v[7], v[46]);
+  const float2 d7 = psub(v[7], v[46]);
+  const float2 s8 = padd(v[8], v[45]);
+  const float2 d8 = psub(v[8], v[45]);
+  const float2 s9 = padd(v[9], v[44]);
+  const float2 d9 = psub(v[9], v[44]);
+  const float2 s10 = padd(v[10], v[43]);
+  const float2 d10 = psub(v[10], v[43]);
+  const float2 s11 = padd(v[11], v[42]);
+  const float2 d11 = psub(v[11], v[42]);
+  const float2 s12 = padd(v[12], v[41]);
+  const float2 d12 = psub(v[12], v[41]);
+  const float2 s13 = padd(v[13], v[40]);
+  const float2 d13 = psub(v[13], v[40]);
+  const float2 s14 = padd(v[14], v[39]);
+  const float2 d14 = psub(v[14], v[39]);
+  const float2 s15 = padd(v[15], v[38]);
+  const float2 d15 = psub(v[15], v[38]);
+  const float2 s16 = padd(v[16], v[37]);
+  const float2 d16 = psub(v[16], v[37]);
+  const float2 s17 = padd(v[17], v[36]);
+  const float2 d17 = psub(v[17], v[36]);
+  const float2 s18 = padd(v[18], v[35]);
+  const float2 d18 = psub(v[18], v[35]);
+  const float2 s19 = padd(v[19], v[34]);
+  const float2 d19 = psub(v[19], v[34]);
+  const float2 s20 = padd(v[20], v[33]);
+  const float2 d20 = psub(v[20], v[33]);
+  const float2 s21 = padd(v[21], v[32]);
+  const float2 d21 = psub(v[21], v[32]);
+  const float2 s22 = padd(v[22], v[31]);
+  const float2 d22 = psub(v[22], v[31]);
+  const float2 s23 = padd(v[23], v[30]);
+  const float2 d23 = psub(v[23], v[30]);
+  const float2 s24 = padd(v[24], v[29]);
+  const float2 d24 = psub(v[24], v[29]);
+  const float2 s25 = padd(v[25], v[28]);
+  const float2 d25 = psub(v[25], v[28]);
+  const float2 s26 = padd(v[26], v[27]);
+  const float2 d26 = psub(v[26], v[27]);
   v[0] = make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y));
   {
     float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
@@ -1213,58 +1214,58 @@ constexpr int kSplit53 = 3;
 template <bool INV, typename St>
 __device__ __forceinline__ void dft_r53_part(const float2* v, int part, St&& st) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
-  const float2 d1 = make_float2(v[1].x - v[52].x, v[1].y - v[52].y);
-  const float2 s2 = make_float2(v[2].x + v[51].x, v[2].y + v[51].y);
-  const float2 d2 = make_float2(v[2].x - v[51].x, v[2].y - v[51].y);
-  const float2 s3 = make_float2(v[3].x + v[50].x, v[3].y + v[50].y);
-  const float2 d3 = make_float2(v[3].x - v[50].x, v[3].y - v[50].y);
-  const float2 s4 = make_float2(v[4].x + v[49].x, v[4].y + v[49].y);
-  const float2 d4 = make_float2(v[4].x - v[49].x, v[4].y - v[49].y);
-  const float2 s5 = make_float2(v[5].x + v[48].x, v[5].y + v[48].y);
-  const float2 d5 = make_float2(v[5].x - v[48].x, v[5].y - v[48].y);
-  const float2 s6 = make_float2(v[6].x + v[47].x, v[6].y + v[47].y);
-  const float2 d6 = make_float2(v[6].x - v[47].x, v[6].y - v[47].y);
-  const float2 s7 = make_float2(v[7].x + v[46].x, v[7].y + v[46].y);
-  const float2 d7 = make_float2(v[7].x - v[46].x, v[7].y - v[46].y);
-  const float2 s8 = make_float2(v[8].x + v[45].x, v[8].y + v[45].y);
-  const float2 d8 = make_float2(v[8].x - v[45].x, v[8].y - v[45].y);
-  const float2 s9 = make_float2(v[9].x + v[44].x, v[9].y + v[44].y);
-  const float2 d9 = make_float2(v[9].x - v[44].x, v[9].y - v[44].y);
-  const float2 s10 = make_float2(v[10].x + v[43].x, v[10].y + v[43].y);
-  const float2 d10 = make_float2(v[10].x - v[43].x, v[10].y - v[43].y);
-  const float2 s11 = make_float2(v[11].x + v[42].x, v[11].y + v[42].y);
-  const float2 d11 = make_float2(v[11].x - v[42].x, v[11].y - v[42].y);
-  const float2 s12 = make_float2(v[12].x + v[41].x, v[12].y + v[41].y);
-  const float2 d12 = make_float2(v[12].x - v[41].x, v[12].y - v[41].y);
-  const float2 s13 = make_float2(v[13].x + v[40].x, v[13].y + v[40].y);
-  const float2 d13 = make_float2(v[13].x - v[40].x, v[13].y - v[40].y);
-  const float2 s14 = make_float2(v[14].x + v[39].x, v[14].y + v[39].y);
-  const float2 d14 = make_float2(v[14].x - v[39].x, v[14].y - v[39].y);
-  const float2 s15 = make_float2(v[15].x + v[38].x, v[15].y + v[38].y);
-  const float2 d15 = make_float2(v[15].x - v[38].x, v[15].y - v[38].y);
-  const float2 s16 = make_float2(v[16].x + v[37].x, v[16].y + v[37].y);
-  const float2 d16 = make_float2(v[16].x - v[37].x, v[16].y - v[37].y);
-  const float2 s17 = make_float2(v[17].x + v[36].x, v[17].y + v[36].y);
-  const float2 d17 = make_float2(v[17].x - v[36].x, v[17].y - v[36].y);
-  const float2 s18 = make_float2(v[18].x + v[35].x, v[18].y + v[35].y);
-  const float2 d18 = make_float2(v[18].x - v[35].x, v[18].y - v[35].y);
-  const float2 s19 = make_float2(v[19].x + v[34].x, v[19].y + v[34].y);
-  const float2 d19 = make_float2(v[19].x - v[34].x, v[19].y - v[34].y);
-  const float2 s20 = make_float2(v[20].x + v[33].x, v[20].y + v[33].y);
-  const float2 d20 = make_float2(v[20].x - v[33].x, v[20].y - v[33].y);
-  const float2 s21 = make_float2(v[21].x + v[32].x, v[21].y + v[32].y);
-  const float2 d21 = make_float2(v[21].x - v[32].x, v[21].y - v[32].y);
-  const float2 s22 = make_float2(v[22].x + v[31].x, v[22].y + v[31].y);
-  const float2 d22 = make_float2(v[22].x - v[31].x, v[22].y - v[31].y);
-  const float2 s23 = make_float2(v[23].x + v[30].x, v[23].y + v[30].y);
-  const float2 d23 = make_float2(v[23].x - v[30].x, v[23].y - v[30].y);
-  const float2 s24 = make_float2(v[24].x + v[29].x, v[24].y + v[29].y);
-  const float2 d24 = make_float2(v[24].x - v[29].x, v[24].y - v[29].y);
-  const float2 s25 = make_float2(v[25].x + v[28].x, v[25].y + v[28].y);
-  const float2 d25 = make_float2(v[25].x - v[28].x, v[25].y - v[28].y);
-  const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
-  const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
+  const float2 s1 = padd(v[1], v[52]);
+  const float2 d1 = psub(v[1], v[52]);
+  const float2 s2 = padd(v[2], v[51]);
+  const float2 d2 = psub(v[2], v[51]);
+  const float2 s3 = padd(v[3], v[50]);
+  const float2 d3 = psub(v[3], v[50]);
+  const float2 s4 = padd(v[4], v[49]);
+  const float2 d4 = psub(v[4], v[49]);
+  const float2 s5 = padd(v[5], v[48]);
+  const float2 d5 = psub(v[5], v[48]);
+  const float2 s6 = padd(v[6], v[47]);
+  const float2 d6 = psub(v[6], v[47]);
+  const float2 s7 = padd(v[7], v[46]);
+  const float2 d7 = psub(v[7], v[46]);
+  const float2 s8 = padd(v[8], v[45]);
+  const float2 d8 = psub(v[8], v[45]);
+  const float2 s9 = padd(v[9], v[44]);
+  const float2 d9 = psub(v[9], v[44]);
+  const float2 s10 = padd(v[10], v[43]);
+  const float2 d10 = psub(v[10], v[43]);
+  const float2 s11 = padd(v[11], v[42]);
+  const float2 d11 = psub(v[11], v[42]);
+  const float2 s12 = padd(v[12], v[41]);
+  const float2 d12 = psub(v[12], v[41]);
+  const float2 s13 = padd(v[13], v[40]);
+  const float2 d13 = psub(v[13], v[40]);
+  const float2 s14 = padd(v[14], v[39]);
+  const float2 d14 = psub(v[14], v[39]);
+  const float2 s15 = padd(v[15], v[38]);
+  const float2 d15 = psub(v[15], v[38]);
+  const float2 s16 = padd(v[16], v[37]);
+  const float2 d16 = psub(v[16], v[37]);
+  const float2 s17 = padd(v[17], v[36]);
+  const float2 d17 = psub(v[17], v[36]);
+  const float2 s18 = padd(v[18], v[35]);
+  const float2 d18 = psub(v[18], v[35]);
+  const float2 s19 = padd(v[19], v[34]);
+  const float2 d19 = psub(v[19], v[34]);
+  const float2 s20 = padd(v[20], v[33]);
+  const float2 d20 = psub(v[20], v[33]);
+  const float2 s21 = padd(v[21], v[32]);
+  const float2 d21 = psub(v[21], v[32]);
+  const float2 s22 = padd(v[22], v[31]);
+  const float2 d22 = psub(v[22], v[31]);
+  const float2 s23 = padd(v[23], v[30]);
+  const float2 d23 = psub(v[23], v[30]);
+  const float2 s24 = padd(v[24], v[29]);
+  const float2 d24 = psub(v[24], v[29]);
+  const float2 s25 = padd(v[25], v[28]);
+  const float2 d25 = psub(v[25], v[28]);
+  const float2 s26 = padd(v[26], v[27]);
+  const float2 d26 = psub(v[26], v[27]);
   if (part == 0) st(0, make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y)));
   switch (part) {
   case 0: {
@@ -2113,131 +2114,163 @@ __constant__ float2 c_tw53[27][27] = {{{1.0f, 0.0f}, {1.0f, 0.0f}, {1.0f, 0.0f},
   {{1.0f, 0.0f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.14764656126499176f, -0.989040195941925f}, {0.029633328318595886f, 0.9995608329772949f}, {-0.2059786170721054f, -0.9785565137863159f}, {0.3758275806903839f, 0.926689624786377f}, {-0.5338233709335327f, -0.8455960154533386f}, {0.674983024597168f, 0.7378332614898682f}, {-0.794854462146759f, -0.6068001389503479f}, {0.8896570801734924f, 0.4566292464733124f}, {-0.956400990486145f, -0.29205676913261414f}, {0.9929810762405396f, 0.11827316880226135f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.829405665397644f, -0.5586467385292053f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.08879589289426804f, 0.9960498213768005f}},
   {{1.0f, 0.0f}, {-0.9982437491416931f, 0.05924062803387642f}, {0.9929810762405396f, -0.11827316880226135f}, {-0.9842305779457092f, 0.1768902689218521f}, {0.9720228910446167f, -0.2348860502243042f}, {-0.956400990486145f, 0.29205676913261414f}, {0.9374196529388428f, -0.3482016324996948f}, {-0.9151456356048584f, 0.4031234383583069f}, {0.8896570801734924f, -0.4566292464733124f}, {-0.8610436320304871f, 0.5085310935974121f}, {0.829405665397644f, -0.5586467385292053f}, {-0.794854462146759f, 0.6068001389503479f}, {0.7575112581253052f, -0.6528221368789673f}, {-0.7175072431564331f, 0.6965510249137878f}, {0.674983024597168f, -0.7378332614898682f}, {-0.6300878524780273f, 0.7765238881111145f}, {0.5829795002937317f, -0.8124868869781494f}, {-0.5338233709335327f, 0.8455960154533386f}, {0.4827921986579895f, -0.8757349252700806f}, {-0.43006521463394165f, 0.9027978181838989f}, {0.3758275806903839f, -0.926689624786377f}, {-0.3202698528766632f, 0.9473263621330261f}, {0.26358717679977417f, -0.9646356105804443f}, {-0.2059786170721054f, 0.9785565137863159f}, {0.14764656126499176f, -0.989040195941925f}, {-0.08879589289426804f, 0.9960498213768005f}, {0.029633328318595886f, -0.9995608329772949f}}};
 template <bool INV, bool PAIRED = false, typename St>
-__device__ __forceinline__ void dft_r53_compact(const float2* v, St&& st) {
+__device__ __forceinline__ void dft_r53_compact(const float2* v, St&& st, int kmax = 26) {
   const float2 x0 = v[0];
-  const float2 s1 = make_float2(v[1].x + v[52].x, v[1].y + v[52].y);
-  const float2 d1 = make_float2(v[1].x - v[52].x, v[1].y - v[52].y);
-  const float2 s2 = make_float2(v[2].x + v[51].x, v[2].y + v[51].y);
-  const float2 d2 = make_float2(v[2].x - v[51].x, v[2].y - v[51].y);
-  const float2 s3 = make_float2(v[3].x + v[50].x, v[3].y + v[50].y);
-  const float2 d3 = make_float2(v[3].x - v[50].x, v[3].y - v[50].y);
-  const float2 s4 = make_float2(v[4].x + v[49].x, v[4].y + v[49].y);
-  const float2 d4 = make_float2(v[4].x - v[49].x, v[4].y - v[49].y);
-  const float2 s5 = make_float2(v[5].x + v[48].x, v[5].y + v[48].y);
-  const float2 d5 = make_float2(v[5].x - v[48].x, v[5].y - v[48].y);
-  const float2 s6 = make_float2(v[6].x + v[47].x, v[6].y + v[47].y);
-  const float2 d6 = make_float2(v[6].x - v[47].x, v[6].y - v[47].y);
-  const float2 s7 = make_float2(v[7].x + v[46].x, v[7].y + v[46].y);
-  const float2 d7 = make_float2(v[7].x - v[46].x, v[7].y - v[46].y);
-  const float2 s8 = make_float2(v[8].x + v[45].x, v[8].y + v[45].y);
-  const float2 d8 = make_float2(v[8].x - v[45].x, v[8].y - v[45].y);
-  const float2 s9 = make_float2(v[9].x + v[44].x, v[9].y + v[44].y);
-  const float2 d9 = make_float2(v[9].x - v[44].x, v[9].y - v[44].y);
-  const float2 s10 = make_float2(v[10].x + v[43].x, v[10].y + v[43].y);
-  const float2 d10 = make_float2(v[10].x - v[43].x, v[10].y - v[43].y);
-  const float2 s11 = make_float2(v[11].x + v[42].x, v[11].y + v[42].y);
-  const float2 d11 = make_float2(v[11].x - v[42].x, v[11].y - v[42].y);
-  const float2 s12 = make_float2(v[12].x + v[41].x, v[12].y + v[41].y);
-  const float2 d12 = make_float2(v[12].x - v[41].x, v[12].y - v[41].y);
-  const float2 s13 = make_float2(v[13].x + v[40].x, v[13].y + v[40].y);
-  const float2 d13 = make_float2(v[13].x - v[40].x, v[13].y - v[40].y);
-  const float2 s14 = make_float2(v[14].x + v[39].x, v[14].y + v[39].y);
-  const float2 d14 = make_float2(v[14].x - v[39].x, v[14].y - v[39].y);
-  const float2 s15 = make_float2(v[15].x + v[38].x, v[15].y + v[38].y);
-  const float2 d15 = make_float2(v[15].x - v[38].x, v[15].y - v[38].y);
-  const float2 s16 = make_float2(v[16].x + v[37].x, v[16].y + v[37].y);
-  const float2 d16 = make_float2(v[16].x - v[37].x, v[16].y - v[37].y);
-  const float2 s17 = make_float2(v[17].x + v[36].x, v[17].y + v[36].y);
-  const float2 d17 = make_float2(v[17].x - v[36].x, v[17].y - v[36].y);
-  const float2 s18 = make_float2(v[18].x + v[35].x, v[18].y + v[35].y);
-  const float2 d18 = make_float2(v[18].x - v[35].x, v[18].y - v[35].y);
-  const float2 s19 = make_float2(v[19].x + v[34].x, v[19].y + v[34].y);
-  const float2 d19 = make_float2(v[19].x - v[34].x, v[19].y - v[34].y);
-  const float2 s20 = make_float2(v[20].x + v[33].x, v[20].y + v[33].y);
-  const float2 d20 = make_float2(v[20].x - v[33].x, v[20].y - v[33].y);
-  const float2 s21 = make_float2(v[21].x + v[32].x, v[21].y + v[32].y);
-  const float2 d21 = make_float2(v[21].x - v[32].x, v[21].y - v[32].y);
-  const float2 s22 = make_float2(v[22].x + v[31].x, v[22].y + v[31].y);
-  const float2 d22 = make_float2(v[22].x - v[31].x, v[22].y - v[31].y);
-  const float2 s23 = make_float2(v[23].x + v[30].x, v[23].y + v[30].y);
-  const float2 d23 = make_float2(v[23].x - v[30].x, v[23].y - v[30].y);
-  const float2 s24 = make_float2(v[24].x + v[29].x, v[24].y + v[29].y);
-  const float2 d24 = make_float2(v[24].x - v[29].x, v[24].y - v[29].y);
-  const float2 s25 = make_float2(v[25].x + v[28].x, v[25].y + v[28].y);
-  const float2 d25 = make_float2(v[25].x - v[28].x, v[25].y - v[28].y);
-  const float2 s26 = make_float2(v[26].x + v[27].x, v[26].y + v[27].y);
-  const float2 d26 = make_float2(v[26].x - v[27].x, v[26].y - v[27].y);
-  st(0, make_float2(x0.x + (s1.x + s2.x + s3.x + s4.x + s5.x + s6.x + s7.x + s8.x + s9.x + s10.x + s11.x + s12.x + s13.x + s14.x + s15.x + s16.x + s17.x + s18.x + s19.x + s20.x + s21.x + s22.x + s23.x + s24.x + s25.x + s26.x), x0.y + (s1.y + s2.y + s3.y + s4.y + s5.y + s6.y + s7.y + s8.y + s9.y + s10.y + s11.y + s12.y + s13.y + s14.y + s15.y + s16.y + s17.y + s18.y + s19.y + s20.y + s21.y + s22.y + s23.y + s24.y + s25.y + s26.y)));
+  const f2reg X0 = f2pk(x0);
+  const f2reg S1 = f2add(f2pk(v[1]), f2pk(v[52]));
+  const f2reg D1 = f2sub(f2pk(v[1]), f2pk(v[52]));
+  const f2reg S2 = f2add(f2pk(v[2]), f2pk(v[51]));
+  const f2reg D2 = f2sub(f2pk(v[2]), f2pk(v[51]));
+  const f2reg S3 = f2add(f2pk(v[3]), f2pk(v[50]));
+  const f2reg D3 = f2sub(f2pk(v[3]), f2pk(v[50]));
+  const f2reg S4 = f2add(f2pk(v[4]), f2pk(v[49]));
+  const f2reg D4 = f2sub(f2pk(v[4]), f2pk(v[49]));
+  const f2reg S5 = f2add(f2pk(v[5]), f2pk(v[48]));
+  const f2reg D5 = f2sub(f2pk(v[5]), f2pk(v[48]));
+  const f2reg S6 = f2add(f2pk(v[6]), f2pk(v[47]));
+  const f2reg D6 = f2sub(f2pk(v[6]), f2pk(v[47]));
+  const f2reg S7 = f2add(f2pk(v[7]), f2pk(v[46]));
+  const f2reg D7 = f2sub(f2pk(v[7]), f2pk(v[46]));
+  const f2reg S8 = f2add(f2pk(v[8]), f2pk(v[45]));
+  const f2reg D8 = f2sub(f2pk(v[8]), f2pk(v[45]));
+  const f2reg S9 = f2add(f2pk(v[9]), f2pk(v[44]));
+  const f2reg D9 = f2sub(f2pk(v[9]), f2pk(v[44]));
+  const f2reg S10 = f2add(f2pk(v[10]), f2pk(v[43]));
+  const f2reg D10 = f2sub(f2pk(v[10]), f2pk(v[43]));
+  const f2reg S11 = f2add(f2pk(v[11]), f2pk(v[42]));
+  const f2reg D11 = f2sub(f2pk(v[11]), f2pk(v[42]));
+  const f2reg S12 = f2add(f2pk(v[12]), f2pk(v[41]));
+  const f2reg D12 = f2sub(f2pk(v[12]), f2pk(v[41]));
+  const f2reg S13 = f2add(f2pk(v[13]), f2pk(v[40]));
+  const f2reg D13 = f2sub(f2pk(v[13]), f2pk(v[40]));
+  const f2reg S14 = f2add(f2pk(v[14]), f2pk(v[39]));
+  const f2reg D14 = f2sub(f2pk(v[14]), f2pk(v[39]));
+  const f2reg S15 = f2add(f2pk(v[15]), f2pk(v[38]));
+  const f2reg D15 = f2sub(f2pk(v[15]), f2pk(v[38]));
+  const f2reg S16 = f2add(f2pk(v[16]), f2pk(v[37]));
+  const f2reg D16 = f2sub(f2pk(v[16]), f2pk(v[37]));
+  const f2reg S17 = f2add(f2pk(v[17]), f2pk(v[36]));
+  const f2reg D17 = f2sub(f2pk(v[17]), f2pk(v[36]));
+  const f2reg S18 = f2add(f2pk(v[18]), f2pk(v[35]));
+  const f2reg D18 = f2sub(f2pk(v[18]), f2pk(v[35]));
+  const f2reg S19 = f2add(f2pk(v[19]), f2pk(v[34]));
+  const f2reg D19 = f2sub(f2pk(v[19]), f2pk(v[34]));
+  const f2reg S20 = f2add(f2pk(v[20]), f2pk(v[33]));
+  const f2reg D20 = f2sub(f2pk(v[20]), f2pk(v[33]));
+  const f2reg S21 = f2add(f2pk(v[21]), f2pk(v[32]));
+  const f2reg D21 = f2sub(f2pk(v[21]), f2pk(v[32]));
+  const f2reg S22 = f2add(f2pk(v[22]), f2pk(v[31]));
+  const f2reg D22 = f2sub(f2pk(v[22]), f2pk(v[31]));
+  const f2reg S23 = f2add(f2pk(v[23]), f2pk(v[30]));
+  const f2reg D23 = f2sub(f2pk(v[23]), f2pk(v[30]));
+  const f2reg S24 = f2add(f2pk(v[24]), f2pk(v[29]));
+  const f2reg D24 = f2sub(f2pk(v[24]), f2pk(v[29]));
+  const f2reg S25 = f2add(f2pk(v[25]), f2pk(v[28]));
+  const f2reg D25 = f2sub(f2pk(v[25]), f2pk(v[28]));
+  const f2reg S26 = f2add(f2pk(v[26]), f2pk(v[27]));
+  const f2reg D26 = f2sub(f2pk(v[26]), f2pk(v[27]));
+  {
+    f2reg t = S1;
+    t = f2add(t, S2);
+    t = f2add(t, S3);
+    t = f2add(t, S4);
+    t = f2add(t, S5);
+    t = f2add(t, S6);
+    t = f2add(t, S7);
+    t = f2add(t, S8);
+    t = f2add(t, S9);
+    t = f2add(t, S10);
+    t = f2add(t, S11);
+    t = f2add(t, S12);
+    t = f2add(t, S13);
+    t = f2add(t, S14);
+    t = f2add(t, S15);
+    t = f2add(t, S16);
+    t = f2add(t, S17);
+    t = f2add(t, S18);
+    t = f2add(t, S19);
+    t = f2add(t, S20);
+    t = f2add(t, S21);
+    t = f2add(t, S22);
+    t = f2add(t, S23);
+    t = f2add(t, S24);
+    t = f2add(t, S25);
+    t = f2add(t, S26);
+    st(0, f2up(f2add(X0, t)));
+  }
   if constexpr (PAIRED) {
 #pragma unroll 1
     for (int k = 1; k <= 13; k++) {
       const float2* t = c_tw53[k];
       const float2* u = c_tw53[k + 13];
-      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
-      float cr = x0.x, ci = x0.y, dr = 0.0f, di = 0.0f;
-      { const float2 c = t[1], e = u[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); cr = fmaf(s1.x, e.x, cr); ci = fmaf(s1.y, e.x, ci); dr = fmaf(d1.x, e.y, dr); di = fmaf(d1.y, e.y, di); }
-      { const float2 c = t[2], e = u[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); cr = fmaf(s2.x, e.x, cr); ci = fmaf(s2.y, e.x, ci); dr = fmaf(d2.x, e.y, dr); di = fmaf(d2.y, e.y, di); }
-      { const float2 c = t[3], e = u[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); cr = fmaf(s3.x, e.x, cr); ci = fmaf(s3.y, e.x, ci); dr = fmaf(d3.x, e.y, dr); di = fmaf(d3.y, e.y, di); }
-      { const float2 c = t[4], e = u[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); cr = fmaf(s4.x, e.x, cr); ci = fmaf(s4.y, e.x, ci); dr = fmaf(d4.x, e.y, dr); di = fmaf(d4.y, e.y, di); }
-      { const float2 c = t[5], e = u[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); cr = fmaf(s5.x, e.x, cr); ci = fmaf(s5.y, e.x, ci); dr = fmaf(d5.x, e.y, dr); di = fmaf(d5.y, e.y, di); }
-      { const float2 c = t[6], e = u[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); cr = fmaf(s6.x, e.x, cr); ci = fmaf(s6.y, e.x, ci); dr = fmaf(d6.x, e.y, dr); di = fmaf(d6.y, e.y, di); }
-      { const float2 c = t[7], e = u[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); cr = fmaf(s7.x, e.x, cr); ci = fmaf(s7.y, e.x, ci); dr = fmaf(d7.x, e.y, dr); di = fmaf(d7.y, e.y, di); }
-      { const float2 c = t[8], e = u[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); cr = fmaf(s8.x, e.x, cr); ci = fmaf(s8.y, e.x, ci); dr = fmaf(d8.x, e.y, dr); di = fmaf(d8.y, e.y, di); }
-      { const float2 c = t[9], e = u[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); cr = fmaf(s9.x, e.x, cr); ci = fmaf(s9.y, e.x, ci); dr = fmaf(d9.x, e.y, dr); di = fmaf(d9.y, e.y, di); }
-      { const float2 c = t[10], e = u[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); cr = fmaf(s10.x, e.x, cr); ci = fmaf(s10.y, e.x, ci); dr = fmaf(d10.x, e.y, dr); di = fmaf(d10.y, e.y, di); }
-      { const float2 c = t[11], e = u[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); cr = fmaf(s11.x, e.x, cr); ci = fmaf(s11.y, e.x, ci); dr = fmaf(d11.x, e.y, dr); di = fmaf(d11.y, e.y, di); }
-      { const float2 c = t[12], e = u[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); cr = fmaf(s12.x, e.x, cr); ci = fmaf(s12.y, e.x, ci); dr = fmaf(d12.x, e.y, dr); di = fmaf(d12.y, e.y, di); }
-      { const float2 c = t[13], e = u[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); cr = fmaf(s13.x, e.x, cr); ci = fmaf(s13.y, e.x, ci); dr = fmaf(d13.x, e.y, dr); di = fmaf(d13.y, e.y, di); }
-      { const float2 c = t[14], e = u[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); cr = fmaf(s14.x, e.x, cr); ci = fmaf(s14.y, e.x, ci); dr = fmaf(d14.x, e.y, dr); di = fmaf(d14.y, e.y, di); }
-      { const float2 c = t[15], e = u[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); cr = fmaf(s15.x, e.x, cr); ci = fmaf(s15.y, e.x, ci); dr = fmaf(d15.x, e.y, dr); di = fmaf(d15.y, e.y, di); }
-      { const float2 c = t[16], e = u[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); cr = fmaf(s16.x, e.x, cr); ci = fmaf(s16.y, e.x, ci); dr = fmaf(d16.x, e.y, dr); di = fmaf(d16.y, e.y, di); }
-      { const float2 c = t[17], e = u[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); cr = fmaf(s17.x, e.x, cr); ci = fmaf(s17.y, e.x, ci); dr = fmaf(d17.x, e.y, dr); di = fmaf(d17.y, e.y, di); }
-      { const float2 c = t[18], e = u[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); cr = fmaf(s18.x, e.x, cr); ci = fmaf(s18.y, e.x, ci); dr = fmaf(d18.x, e.y, dr); di = fmaf(d18.y, e.y, di); }
-      { const float2 c = t[19], e = u[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); cr = fmaf(s19.x, e.x, cr); ci = fmaf(s19.y, e.x, ci); dr = fmaf(d19.x, e.y, dr); di = fmaf(d19.y, e.y, di); }
-      { const float2 c = t[20], e = u[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); cr = fmaf(s20.x, e.x, cr); ci = fmaf(s20.y, e.x, ci); dr = fmaf(d20.x, e.y, dr); di = fmaf(d20.y, e.y, di); }
-      { const float2 c = t[21], e = u[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); cr = fmaf(s21.x, e.x, cr); ci = fmaf(s21.y, e.x, ci); dr = fmaf(d21.x, e.y, dr); di = fmaf(d21.y, e.y, di); }
-      { const float2 c = t[22], e = u[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); cr = fmaf(s22.x, e.x, cr); ci = fmaf(s22.y, e.x, ci); dr = fmaf(d22.x, e.y, dr); di = fmaf(d22.y, e.y, di); }
-      { const float2 c = t[23], e = u[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); cr = fmaf(s23.x, e.x, cr); ci = fmaf(s23.y, e.x, ci); dr = fmaf(d23.x, e.y, dr); di = fmaf(d23.y, e.y, di); }
-      { const float2 c = t[24], e = u[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); cr = fmaf(s24.x, e.x, cr); ci = fmaf(s24.y, e.x, ci); dr = fmaf(d24.x, e.y, dr); di = fmaf(d24.y, e.y, di); }
-      { const float2 c = t[25], e = u[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); cr = fmaf(s25.x, e.x, cr); ci = fmaf(s25.y, e.x, ci); dr = fmaf(d25.x, e.y, dr); di = fmaf(d25.y, e.y, di); }
-      { const float2 c = t[26], e = u[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); cr = fmaf(s26.x, e.x, cr); ci = fmaf(s26.y, e.x, ci); dr = fmaf(d26.x, e.y, dr); di = fmaf(d26.y, e.y, di); }
-      const int k2 = k + 13;
-      if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - k, make_float2(ar - bi, ai + br)); st(k2, make_float2(cr + di, ci - dr)); st(53 - k2, make_float2(cr - di, ci + dr)); }
-      else { st(k, make_float2(ar - bi, ai + br)); st(53 - k, make_float2(ar + bi, ai - br)); st(k2, make_float2(cr - di, ci + dr)); st(53 - k2, make_float2(cr + di, ci - dr)); }
+      f2reg A = X0, B = 0ull, C = X0, E = 0ull;
+      { const float2 c = t[1], e = u[1]; A = f2fma(S1, f2splat(c.x), A); B = f2fma(D1, f2splat(c.y), B); C = f2fma(S1, f2splat(e.x), C); E = f2fma(D1, f2splat(e.y), E); }
+      { const float2 c = t[2], e = u[2]; A = f2fma(S2, f2splat(c.x), A); B = f2fma(D2, f2splat(c.y), B); C = f2fma(S2, f2splat(e.x), C); E = f2fma(D2, f2splat(e.y), E); }
+      { const float2 c = t[3], e = u[3]; A = f2fma(S3, f2splat(c.x), A); B = f2fma(D3, f2splat(c.y), B); C = f2fma(S3, f2splat(e.x), C); E = f2fma(D3, f2splat(e.y), E); }
+      { const float2 c = t[4], e = u[4]; A = f2fma(S4, f2splat(c.x), A); B = f2fma(D4, f2splat(c.y), B); C = f2fma(S4, f2splat(e.x), C); E = f2fma(D4, f2splat(e.y), E); }
+      { const float2 c = t[5], e = u[5]; A = f2fma(S5, f2splat(c.x), A); B = f2fma(D5, f2splat(c.y), B); C = f2fma(S5, f2splat(e.x), C); E = f2fma(D5, f2splat(e.y), E); }
+      { const float2 c = t[6], e = u[6]; A = f2fma(S6, f2splat(c.x), A); B = f2fma(D6, f2splat(c.y), B); C = f2fma(S6, f2splat(e.x), C); E = f2fma(D6, f2splat(e.y), E); }
+      { const float2 c = t[7], e = u[7]; A = f2fma(S7, f2splat(c.x), A); B = f2fma(D7, f2splat(c.y), B); C = f2fma(S7, f2splat(e.x), C); E = f2fma(D7, f2splat(e.y), E); }
+      { const float2 c = t[8], e = u[8]; A = f2fma(S8, f2splat(c.x), A); B = f2fma(D8, f2splat(c.y), B); C = f2fma(S8, f2splat(e.x), C); E = f2fma(D8, f2splat(e.y), E); }
+      { const float2 c = t[9], e = u[9]; A = f2fma(S9, f2splat(c.x), A); B = f2fma(D9, f2splat(c.y), B); C = f2fma(S9, f2splat(e.x), C); E = f2fma(D9, f2splat(e.y), E); }
+      { const float2 c = t[10], e = u[10]; A = f2fma(S10, f2splat(c.x), A); B = f2fma(D10, f2splat(c.y), B); C = f2fma(S10, f2splat(e.x), C); E = f2fma(D10, f2splat(e.y), E); }
+      { const float2 c = t[11], e = u[11]; A = f2fma(S11, f2splat(c.x), A); B = f2fma(D11, f2splat(c.y), B); C = f2fma(S11, f2splat(e.x), C); E = f2fma(D11, f2splat(e.y), E); }
+      { const float2 c = t[12], e = u[12]; A = f2fma(S12, f2splat(c.x), A); B = f2fma(D12, f2splat(c.y), B); C = f2fma(S12, f2splat(e.x), C); E = f2fma(D12, f2splat(e.y), E); }
+      { const float2 c = t[13], e = u[13]; A = f2fma(S13, f2splat(c.x), A); B = f2fma(D13, f2splat(c.y), B); C = f2fma(S13, f2splat(e.x), C); E = f2fma(D13, f2splat(e.y), E); }
+      { const float2 c = t[14], e = u[14]; A = f2fma(S14, f2splat(c.x), A); B = f2fma(D14, f2splat(c.y), B); C = f2fma(S14, f2splat(e.x), C); E = f2fma(D14, f2splat(e.y), E); }
+      { const float2 c = t[15], e = u[15]; A = f2fma(S15, f2splat(c.x), A); B = f2fma(D15, f2splat(c.y), B); C = f2fma(S15, f2splat(e.x), C); E = f2fma(D15, f2splat(e.y), E); }
+      { const float2 c = t[16], e = u[16]; A = f2fma(S16, f2splat(c.x), A); B = f2fma(D16, f2splat(c.y), B); C = f2fma(S16, f2splat(e.x), C); E = f2fma(D16, f2splat(e.y), E); }
+      { const float2 c = t[17], e = u[17]; A = f2fma(S17, f2splat(c.x), A); B = f2fma(D17, f2splat(c.y), B); C = f2fma(S17, f2splat(e.x), C); E = f2fma(D17, f2splat(e.y), E); }
+      { const float2 c = t[18], e = u[18]; A = f2fma(S18, f2splat(c.x), A); B = f2fma(D18, f2splat(c.y), B); C = f2fma(S18, f2splat(e.x), C); E = f2fma(D18, f2splat(e.y), E); }
+      { const float2 c = t[19], e = u[19]; A = f2fma(S19, f2splat(c.x), A); B = f2fma(D19, f2splat(c.y), B); C = f2fma(S19, f2splat(e.x), C); E = f2fma(D19, f2splat(e.y), E); }
+      { const float2 c = t[20], e = u[20]; A = f2fma(S20, f2splat(c.x), A); B = f2fma(D20, f2splat(c.y), B); C = f2fma(S20, f2splat(e.x), C); E = f2fma(D20, f2splat(e.y), E); }
+      { const float2 c = t[21], e = u[21]; A = f2fma(S21, f2splat(c.x), A); B = f2fma(D21, f2splat(c.y), B); C = f2fma(S21, f2splat(e.x), C); E = f2fma(D21, f2splat(e.y), E); }
+      { const float2 c = t[22], e = u[22]; A = f2fma(S22, f2splat(c.x), A); B = f2fma(D22, f2splat(c.y), B); C = f2fma(S22, f2splat(e.x), C); E = f2fma(D22, f2splat(e.y), E); }
+      { const float2 c = t[23], e = u[23]; A = f2fma(S23, f2splat(c.x), A); B = f2fma(D23, f2splat(c.y), B); C = f2fma(S23, f2splat(e.x), C); E = f2fma(D23, f2splat(e.y), E); }
+      { const float2 c = t[24], e = u[24]; A = f2fma(S24, f2splat(c.x), A); B = f2fma(D24, f2splat(c.y), B); C = f2fma(S24, f2splat(e.x), C); E = f2fma(D24, f2splat(e.y), E); }
+      { const float2 c = t[25], e = u[25]; A = f2fma(S25, f2splat(c.x), A); B = f2fma(D25, f2splat(c.y), B); C = f2fma(S25, f2splat(e.x), C); E = f2fma(D25, f2splat(e.y), E); }
+      { const float2 c = t[26], e = u[26]; A = f2fma(S26, f2splat(c.x), A); B = f2fma(D26, f2splat(c.y), B); C = f2fma(S26, f2splat(e.x), C); E = f2fma(D26, f2splat(e.y), E); }
+      { const float2 a = f2up(A), b = f2up(B);
+        if (!INV) { st(k, make_float2(a.x + b.y, a.y - b.x)); st(53 - (k), make_float2(a.x - b.y, a.y + b.x)); }
+        else { st(k, make_float2(a.x - b.y, a.y + b.x)); st(53 - (k), make_float2(a.x + b.y, a.y - b.x)); } }
+      { const float2 a = f2up(C), b = f2up(E);
+        if (!INV) { st(k + 13, make_float2(a.x + b.y, a.y - b.x)); st(53 - (k + 13), make_float2(a.x - b.y, a.y + b.x)); }
+        else { st(k + 13, make_float2(a.x - b.y, a.y + b.x)); st(53 - (k + 13), make_float2(a.x + b.y, a.y - b.x)); } }
     }
   } else {
 #pragma unroll 1
-    for (int k = 1; k <= 26; k++) {
+    for (int k = 1; k <= kmax; k++) {
       const float2* t = c_tw53[k];
-      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;
-      { const float2 c = t[1]; ar = fmaf(s1.x, c.x, ar); ai = fmaf(s1.y, c.x, ai); br = fmaf(d1.x, c.y, br); bi = fmaf(d1.y, c.y, bi); }
-      { const float2 c = t[2]; ar = fmaf(s2.x, c.x, ar); ai = fmaf(s2.y, c.x, ai); br = fmaf(d2.x, c.y, br); bi = fmaf(d2.y, c.y, bi); }
-      { const float2 c = t[3]; ar = fmaf(s3.x, c.x, ar); ai = fmaf(s3.y, c.x, ai); br = fmaf(d3.x, c.y, br); bi = fmaf(d3.y, c.y, bi); }
-      { const float2 c = t[4]; ar = fmaf(s4.x, c.x, ar); ai = fmaf(s4.y, c.x, ai); br = fmaf(d4.x, c.y, br); bi = fmaf(d4.y, c.y, bi); }
-      { const float2 c = t[5]; ar = fmaf(s5.x, c.x, ar); ai = fmaf(s5.y, c.x, ai); br = fmaf(d5.x, c.y, br); bi = fmaf(d5.y, c.y, bi); }
-      { const float2 c = t[6]; ar = fmaf(s6.x, c.x, ar); ai = fmaf(s6.y, c.x, ai); br = fmaf(d6.x, c.y, br); bi = fmaf(d6.y, c.y, bi); }
-      { const float2 c = t[7]; ar = fmaf(s7.x, c.x, ar); ai = fmaf(s7.y, c.x, ai); br = fmaf(d7.x, c.y, br); bi = fmaf(d7.y, c.y, bi); }
-      { const float2 c = t[8]; ar = fmaf(s8.x, c.x, ar); ai = fmaf(s8.y, c.x, ai); br = fmaf(d8.x, c.y, br); bi = fmaf(d8.y, c.y, bi); }
-      { const float2 c = t[9]; ar = fmaf(s9.x, c.x, ar); ai = fmaf(s9.y, c.x, ai); br = fmaf(d9.x, c.y, br); bi = fmaf(d9.y, c.y, bi); }
-      { const float2 c = t[10]; ar = fmaf(s10.x, c.x, ar); ai = fmaf(s10.y, c.x, ai); br = fmaf(d10.x, c.y, br); bi = fmaf(d10.y, c.y, bi); }
-      { const float2 c = t[11]; ar = fmaf(s11.x, c.x, ar); ai = fmaf(s11.y, c.x, ai); br = fmaf(d11.x, c.y, br); bi = fmaf(d11.y, c.y, bi); }
-      { const float2 c = t[12]; ar = fmaf(s12.x, c.x, ar); ai = fmaf(s12.y, c.x, ai); br = fmaf(d12.x, c.y, br); bi = fmaf(d12.y, c.y, bi); }
-      { const float2 c = t[13]; ar = fmaf(s13.x, c.x, ar); ai = fmaf(s13.y, c.x, ai); br = fmaf(d13.x, c.y, br); bi = fmaf(d13.y, c.y, bi); }
-      { const float2 c = t[14]; ar = fmaf(s14.x, c.x, ar); ai = fmaf(s14.y, c.x, ai); br = fmaf(d14.x, c.y, br); bi = fmaf(d14.y, c.y, bi); }
-      { const float2 c = t[15]; ar = fmaf(s15.x, c.x, ar); ai = fmaf(s15.y, c.x, ai); br = fmaf(d15.x, c.y, br); bi = fmaf(d15.y, c.y, bi); }
-      { const float2 c = t[16]; ar = fmaf(s16.x, c.x, ar); ai = fmaf(s16.y, c.x, ai); br = fmaf(d16.x, c.y, br); bi = fmaf(d16.y, c.y, bi); }
-      { const float2 c = t[17]; ar = fmaf(s17.x, c.x, ar); ai = fmaf(s17.y, c.x, ai); br = fmaf(d17.x, c.y, br); bi = fmaf(d17.y, c.y, bi); }
-      { const float2 c = t[18]; ar = fmaf(s18.x, c.x, ar); ai = fmaf(s18.y, c.x, ai); br = fmaf(d18.x, c.y, br); bi = fmaf(d18.y, c.y, bi); }
-      { const float2 c = t[19]; ar = fmaf(s19.x, c.x, ar); ai = fmaf(s19.y, c.x, ai); br = fmaf(d19.x, c.y, br); bi = fmaf(d19.y, c.y, bi); }
-      { const float2 c = t[20]; ar = fmaf(s20.x, c.x, ar); ai = fmaf(s20.y, c.x, ai); br = fmaf(d20.x, c.y, br); bi = fmaf(d20.y, c.y, bi); }
-      { const float2 c = t[21]; ar = fmaf(s21.x, c.x, ar); ai = fmaf(s21.y, c.x, ai); br = fmaf(d21.x, c.y, br); bi = fmaf(d21.y, c.y, bi); }
-      { const float2 c = t[22]; ar = fmaf(s22.x, c.x, ar); ai = fmaf(s22.y, c.x, ai); br = fmaf(d22.x, c.y, br); bi = fmaf(d22.y, c.y, bi); }
-      { const float2 c = t[23]; ar = fmaf(s23.x, c.x, ar); ai = fmaf(s23.y, c.x, ai); br = fmaf(d23.x, c.y, br); bi = fmaf(d23.y, c.y, bi); }
-      { const float2 c = t[24]; ar = fmaf(s24.x, c.x, ar); ai = fmaf(s24.y, c.x, ai); br = fmaf(d24.x, c.y, br); bi = fmaf(d24.y, c.y, bi); }
-      { const float2 c = t[25]; ar = fmaf(s25.x, c.x, ar); ai = fmaf(s25.y, c.x, ai); br = fmaf(d25.x, c.y, br); bi = fmaf(d25.y, c.y, bi); }
-      { const float2 c = t[26]; ar = fmaf(s26.x, c.x, ar); ai = fmaf(s26.y, c.x, ai); br = fmaf(d26.x, c.y, br); bi = fmaf(d26.y, c.y, bi); }
-      if (!INV) { st(k, make_float2(ar + bi, ai - br)); st(53 - (k), make_float2(ar - bi, ai + br)); }
-      else { st(k, make_float2(ar - bi, ai + br)); st(53 - (k), make_float2(ar + bi, ai - br)); }
+      f2reg A = X0, B = 0ull;
+      { const float2 c = t[1]; A = f2fma(S1, f2splat(c.x), A); B = f2fma(D1, f2splat(c.y), B); }
+      { const float2 c = t[2]; A = f2fma(S2, f2splat(c.x), A); B = f2fma(D2, f2splat(c.y), B); }
+      { const float2 c = t[3]; A = f2fma(S3, f2splat(c.x), A); B = f2fma(D3, f2splat(c.y), B); }
+      { const float2 c = t[4]; A = f2fma(S4, f2splat(c.x), A); B = f2fma(D4, f2splat(c.y), B); }
+      { const float2 c = t[5]; A = f2fma(S5, f2splat(c.x), A); B = f2fma(D5, f2splat(c.y), B); }
+      { const float2 c = t[6]; A = f2fma(S6, f2splat(c.x), A); B = f2fma(D6, f2splat(c.y), B); }
+      { const float2 c = t[7]; A = f2fma(S7, f2splat(c.x), A); B = f2fma(D7, f2splat(c.y), B); }
+      { const float2 c = t[8]; A = f2fma(S8, f2splat(c.x), A); B = f2fma(D8, f2splat(c.y), B); }
+      { const float2 c = t[9]; A = f2fma(S9, f2splat(c.x), A); B = f2fma(D9, f2splat(c.y), B); }
+      { const float2 c = t[10]; A = f2fma(S10, f2splat(c.x), A); B = f2fma(D10, f2splat(c.y), B); }
+      { const float2 c = t[11]; A = f2fma(S11, f2splat(c.x), A); B = f2fma(D11, f2splat(c.y), B); }
+      { const float2 c = t[12]; A = f2fma(S12, f2splat(c.x), A); B = f2fma(D12, f2splat(c.y), B); }
+      { const float2 c = t[13]; A = f2fma(S13, f2splat(c.x), A); B = f2fma(D13, f2splat(c.y), B); }
+      { const float2 c = t[14]; A = f2fma(S14, f2splat(c.x), A); B = f2fma(D14, f2splat(c.y), B); }
+      { const float2 c = t[15]; A = f2fma(S15, f2splat(c.x), A); B = f2fma(D15, f2splat(c.y), B); }
+      { const float2 c = t[16]; A = f2fma(S16, f2splat(c.x), A); B = f2fma(D16, f2splat(c.y), B); }
+      { const float2 c = t[17]; A = f2fma(S17, f2splat(c.x), A); B = f2fma(D17, f2splat(c.y), B); }
+      { const float2 c = t[18]; A = f2fma(S18, f2splat(c.x), A); B = f2fma(D18, f2splat(c.y), B); }
+      { const float2 c = t[19]; A = f2fma(S19, f2splat(c.x), A); B = f2fma(D19, f2splat(c.y), B); }
+      { const float2 c = t[20]; A = f2fma(S20, f2splat(c.x), A); B = f2fma(D20, f2splat(c.y), B); }
+      { const float2 c = t[21]; A = f2fma(S21, f2splat(c.x), A); B = f2fma(D21, f2splat(c.y), B); }
+      { const float2 c = t[22]; A = f2fma(S22, f2splat(c.x), A); B = f2fma(D22, f2splat(c.y), B); }
+      { const float2 c = t[23]; A = f2fma(S23, f2splat(c.x), A); B = f2fma(D23, f2splat(c.y), B); }
+      { const float2 c = t[24]; A = f2fma(S24, f2splat(c.x), A); B = f2fma(D24, f2splat(c.y), B); }
+      { const float2 c = t[25]; A = f2fma(S25, f2splat(c.x), A); B = f2fma(D25, f2splat(c.y), B); }
+      { const float2 c = t[26]; A = f2fma(S26, f2splat(c.x), A); B = f2fma(D26, f2splat(c.y), B); }
+      { const float2 a = f2up(A), b = f2up(B);
+        if (!INV) { st(k, make_float2(a.x + b.y, a.y - b.x)); st(53 - (k), make_float2(a.x - b.y, a.y + b.x)); }
+        else { st(k, make_float2(a.x - b.y, a.y + b.x)); st(53 - (k), make_float2(a.x + b.y, a.y - b.x)); } }
     }
   }
 }

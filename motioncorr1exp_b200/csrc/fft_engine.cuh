@@ -17,6 +17,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "f2ops.cuh"
 #include "dft_gen.cuh"
 
 namespace mc {
@@ -83,18 +84,18 @@ __device__ __forceinline__ float2 rot90(float2 z) {
 template <bool INV>
 __device__ __forceinline__ void dft_r2(float2* v) {
   float2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
+  v[0] = padd(a, b);
+  v[1] = psub(a, b);
 }
 
 template <bool INV>
 __device__ __forceinline__ void dft_r4(float2* v) {
-  float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-  float2 t2 = cadd(v[1], v[3]), t3 = rot90<INV>(csub(v[1], v[3]));
-  v[0] = cadd(t0, t2);
-  v[2] = csub(t0, t2);
-  v[1] = cadd(t1, t3);
-  v[3] = csub(t1, t3);
+  float2 t0 = padd(v[0], v[2]), t1 = psub(v[0], v[2]);
+  float2 t2 = padd(v[1], v[3]), t3 = rot90<INV>(psub(v[1], v[3]));
+  v[0] = padd(t0, t2);
+  v[2] = psub(t0, t2);
+  v[1] = padd(t1, t3);
+  v[3] = psub(t1, t3);
 }
 
 template <bool INV>
@@ -112,8 +113,8 @@ __device__ __forceinline__ void dft_r8(float2* v) {
              : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    v[k] = cadd(e[k], o[k]);
-    v[k + 4] = csub(e[k], o[k]);
+    v[k] = padd(e[k], o[k]);
+    v[k + 4] = psub(e[k], o[k]);
   }
 }
 

@@ -31,8 +31,8 @@ def emit_odd(R: int) -> str:
     L.append(f"template <bool INV> __device__ __forceinline__ void dft_r{R}(float2* v) {{")
     L.append("  const float2 x0 = v[0];")
     for n in range(1, h + 1):
-        L.append(f"  const float2 s{n} = make_float2(v[{n}].x + v[{R-n}].x, v[{n}].y + v[{R-n}].y);")
-        L.append(f"  const float2 d{n} = make_float2(v[{n}].x - v[{R-n}].x, v[{n}].y - v[{R-n}].y);")
+        L.append(f"  const float2 s{n} = padd(v[{n}], v[{R-n}]);")
+        L.append(f"  const float2 d{n} = psub(v[{n}], v[{R-n}]);")
     sx = " + ".join([f"s{n}.x" for n in range(1, h + 1)])
     sy = " + ".join([f"s{n}.y" for n in range(1, h + 1)])
     L.append(f"  v[0] = make_float2(x0.x + ({sx}), x0.y + ({sy}));")
@@ -66,8 +66,8 @@ def emit_odd_split(R: int, S: int) -> str:
          f"__device__ __forceinline__ void dft_r{R}_part(const float2* v, int part, St&& st) {{",
          "  const float2 x0 = v[0];"]
     for n in range(1, h + 1):
-        L.append(f"  const float2 s{n} = make_float2(v[{n}].x + v[{R-n}].x, v[{n}].y + v[{R-n}].y);")
-        L.append(f"  const float2 d{n} = make_float2(v[{n}].x - v[{R-n}].x, v[{n}].y - v[{R-n}].y);")
+        L.append(f"  const float2 s{n} = padd(v[{n}], v[{R-n}]);")
+        L.append(f"  const float2 d{n} = psub(v[{n}], v[{R-n}]);")
     sx = " + ".join([f"s{n}.x" for n in range(1, h + 1)])
     sy = " + ".join([f"s{n}.y" for n in range(1, h + 1)])
     L.append(f"  if (part == 0) st(0, make_float2(x0.x + ({sx}), x0.y + ({sy})));")
@@ -98,9 +98,12 @@ def emit_odd_compact(R: int) -> str:
     """Radix-R DFT with a runtime loop over the (R-1)/2 output pairs: the
     pairs' twiddles come from a __constant__ table (uniform index, broadcast),
     so the code is ~h times smaller than the straight-line form; each output
-    goes to st(index, value) as soon as it is formed.  PAIRED = true forms two
-    output pairs (k, k + h/2) per iteration (eight independent FMA chains
-    instead of four, four more registers)."""
+    goes to st(index, value) as soon as it is formed.  The sums run on packed
+    FP32 pairs (one fma.f32x2 per term for the real and imaginary halves,
+    each rounded as the scalar FMA).  PAIRED = true forms two output pairs
+    (k, k + h/2) per iteration (twice the independent chains).  Without
+    PAIRED only the output pairs (k, R - k) with k <= kmax are formed (X_0
+    always): a pruned transform whose other outputs are not wanted."""
     h = (R - 1) // 2
     rows = []
     for k in range(h + 1):
@@ -111,25 +114,33 @@ def emit_odd_compact(R: int) -> str:
         rows.append("{" + ", ".join(row) + "}")
     L = [f"__constant__ float2 c_tw{R}[{h + 1}][{h + 1}] = {{" + ",\n  ".join(rows) + "};",
          f"template <bool INV, bool PAIRED = false, typename St>",
-         f"__device__ __forceinline__ void dft_r{R}_compact(const float2* v, St&& st) {{",
-         "  const float2 x0 = v[0];"]
+         f"__device__ __forceinline__ void dft_r{R}_compact(const float2* v, St&& st, int kmax = {h}) {{",
+         "  const float2 x0 = v[0];",
+         "  const f2reg X0 = f2pk(x0);"]
     for n in range(1, h + 1):
-        L.append(f"  const float2 s{n} = make_float2(v[{n}].x + v[{R-n}].x, v[{n}].y + v[{R-n}].y);")
-        L.append(f"  const float2 d{n} = make_float2(v[{n}].x - v[{R-n}].x, v[{n}].y - v[{R-n}].y);")
-    sx = " + ".join([f"s{n}.x" for n in range(1, h + 1)])
-    sy = " + ".join([f"s{n}.y" for n in range(1, h + 1)])
-    L.append(f"  st(0, make_float2(x0.x + ({sx}), x0.y + ({sy})));")
+        L.append(f"  const f2reg S{n} = f2add(f2pk(v[{n}]), f2pk(v[{R-n}]));")
+        L.append(f"  const f2reg D{n} = f2sub(f2pk(v[{n}]), f2pk(v[{R-n}]));")
+    L.append("  {")
+    L.append("    f2reg t = S1;")
+    for n in range(2, h + 1):
+        L.append(f"    t = f2add(t, S{n});")
+    L.append("    st(0, f2up(f2add(X0, t)));")
+    L.append("  }")
+
+    def emit_out(kexpr, A, B, indent):
+        return [f"{indent}{{ const float2 a = f2up({A}), b = f2up({B});",
+                f"{indent}  if (!INV) {{ st({kexpr}, make_float2(a.x + b.y, a.y - b.x));"
+                f" st({R} - ({kexpr}), make_float2(a.x - b.y, a.y + b.x)); }}",
+                f"{indent}  else {{ st({kexpr}, make_float2(a.x - b.y, a.y + b.x));"
+                f" st({R} - ({kexpr}), make_float2(a.x + b.y, a.y - b.x)); }} }}"]
 
     def single(kexpr, indent):
         out = [f"{indent}const float2* t = c_tw{R}[{kexpr}];",
-               f"{indent}float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;"]
+               f"{indent}f2reg A = X0, B = 0ull;"]
         for n in range(1, h + 1):
-            out.append(f"{indent}{{ const float2 c = t[{n}]; ar = fmaf(s{n}.x, c.x, ar); ai = fmaf(s{n}.y, c.x, ai);"
-                       f" br = fmaf(d{n}.x, c.y, br); bi = fmaf(d{n}.y, c.y, bi); }}")
-        out.append(f"{indent}if (!INV) {{ st({kexpr}, make_float2(ar + bi, ai - br));"
-                   f" st({R} - ({kexpr}), make_float2(ar - bi, ai + br)); }}")
-        out.append(f"{indent}else {{ st({kexpr}, make_float2(ar - bi, ai + br));"
-                   f" st({R} - ({kexpr}), make_float2(ar + bi, ai - br)); }}")
+            out.append(f"{indent}{{ const float2 c = t[{n}]; A = f2fma(S{n}, f2splat(c.x), A);"
+                       f" B = f2fma(D{n}, f2splat(c.y), B); }}")
+        out += emit_out(kexpr, "A", "B", indent)
         return out
 
     half = h // 2
@@ -138,19 +149,13 @@ def emit_odd_compact(R: int) -> str:
     L.append(f"    for (int k = 1; k <= {half}; k++) {{")
     L.append(f"      const float2* t = c_tw{R}[k];")
     L.append(f"      const float2* u = c_tw{R}[k + {half}];")
-    L.append("      float ar = x0.x, ai = x0.y, br = 0.0f, bi = 0.0f;")
-    L.append("      float cr = x0.x, ci = x0.y, dr = 0.0f, di = 0.0f;")
+    L.append("      f2reg A = X0, B = 0ull, C = X0, E = 0ull;")
     for n in range(1, h + 1):
         L.append(f"      {{ const float2 c = t[{n}], e = u[{n}];"
-                 f" ar = fmaf(s{n}.x, c.x, ar); ai = fmaf(s{n}.y, c.x, ai);"
-                 f" br = fmaf(d{n}.x, c.y, br); bi = fmaf(d{n}.y, c.y, bi);"
-                 f" cr = fmaf(s{n}.x, e.x, cr); ci = fmaf(s{n}.y, e.x, ci);"
-                 f" dr = fmaf(d{n}.x, e.y, dr); di = fmaf(d{n}.y, e.y, di); }}")
-    L.append(f"      const int k2 = k + {half};")
-    L.append(f"      if (!INV) {{ st(k, make_float2(ar + bi, ai - br)); st({R} - k, make_float2(ar - bi, ai + br));"
-             f" st(k2, make_float2(cr + di, ci - dr)); st({R} - k2, make_float2(cr - di, ci + dr)); }}")
-    L.append(f"      else {{ st(k, make_float2(ar - bi, ai + br)); st({R} - k, make_float2(ar + bi, ai - br));"
-             f" st(k2, make_float2(cr - di, ci + dr)); st({R} - k2, make_float2(cr + di, ci - dr)); }}")
+                 f" A = f2fma(S{n}, f2splat(c.x), A); B = f2fma(D{n}, f2splat(c.y), B);"
+                 f" C = f2fma(S{n}, f2splat(e.x), C); E = f2fma(D{n}, f2splat(e.y), E); }}")
+    L += emit_out("k", "A", "B", "      ")
+    L += emit_out(f"k + {half}", "C", "E", "      ")
     L.append("    }")
     if h % 2:
         L.append("    {")
@@ -158,7 +163,7 @@ def emit_odd_compact(R: int) -> str:
         L.append("    }")
     L.append("  } else {")
     L.append("#pragma unroll 1")
-    L.append(f"    for (int k = 1; k <= {h}; k++) {{")
+    L.append(f"    for (int k = 1; k <= kmax; k++) {{")
     L += single("k", "      ")
     L.append("    }")
     L.append("  }")
@@ -251,6 +256,7 @@ def main() -> None:
         out.append("// Straight-line odd-radix DFT butterflies (symmetric direct form).")
         out.append("#pragma once")
         out.append("#include <cuda_runtime.h>")
+        out.append('#include "f2ops.cuh"')
         out.append("namespace mc {")
         out.append(f"constexpr int kGeneratedOddRadices[] = {{{', '.join(map(str, ODD_RADICES))}}};")
         for R in ODD_RADICES:

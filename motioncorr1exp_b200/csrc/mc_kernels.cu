@@ -225,11 +225,13 @@ struct TwoLevel {
   static constexpr int T = ((N1 > N2 ? N1 : N2) + 31) / 32 * 32;
 
   // step A + exchange + step B; load(i) gives x[i], store(k, X[k]) takes the
-  // result; tw[TWS * j] = exp(-2 pi i j / N).  T >= N2, so each thread owns at most one k2 in step B; with
+  // result; tw[TWS * j] = exp(-2 pi i j / N).  For N1 = 53 only the outputs
+  // with k1 or N1 - k1 <= kmax are formed (pruned transforms).  T >= N2, so each thread owns at most one k2 in step B; with
   // SYNC_STORE a barrier follows every thread's step-B reads of ysm, which
   // lets store() write back into ysm.
   template <bool INV, bool SYNC_STORE, bool PAIRED = false, int TWS = 1, class Load, class Store>
-  __device__ static void run(float2* ysm, const float2* __restrict__ tw, Load&& load, Store&& store) {
+  __device__ static void run(float2* ysm, const float2* __restrict__ tw, Load&& load, Store&& store,
+                             int kmax = (N1 - 1) / 2) {
     static_assert(T >= N2, "one k2 per thread");
     const int lt = threadIdx.x;
     if (lt < N1) {
@@ -254,7 +256,7 @@ struct TwoLevel {
     if (SYNC_STORE) __syncthreads();
     if constexpr (N1 == 53) {
       // compact radix-53 DFT: small code, outputs stored as they are formed
-      if (act) dft_r53_compact<INV, PAIRED>(v, [&](int k1, float2 x) { store(lt + N2 * k1, x); });
+      if (act) dft_r53_compact<INV, PAIRED>(v, [&](int k1, float2 x) { store(lt + N2 * k1, x); }, kmax);
     } else {
       if (act) fft_n1<N1, INV>(v);
       if (act) {
@@ -435,6 +437,16 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
 // then the two N-point two-level transforms, whose outputs go straight to
 // the kept indices.  tw is the L-entry table exp(-2 pi i j / L).
 
+// Output pairs (k1, N1 - k1) of the N1-point step a radix-2 split transform
+// needs when only its outputs below `lo` (2m < lo) and their mirror images
+// (2m > L - lo) are kept: m = k2 + N2*k1 < lo/2 needs k1 <= (lo/2 - 1)/N2,
+// one more pair for the boundary row; all pairs when that reaches (N1-1)/2.
+template <int N1, int N2>
+__device__ __forceinline__ int dif_kmax(int lo) {
+  const int k = (lo / 2) / N2 + 1;
+  return k < (N1 - 1) / 2 ? k : (N1 - 1) / 2;
+}
+
 // Forward rows of length L without references: two rows staged as raw
 // pixels; only the Z indices the half-spectrum split needs are kept in
 // shared memory (Z[0, hk) and Z(L - hk, L)).
@@ -464,20 +476,23 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
     if (idx < hk) zlo[idx] = v;
     else if (idx > L - hk) zhi[idx - (L - hk + 1)] = v;
   };
-  TL::template run<false, false, MC_FWD_PAIRED, 2>(
+  // wanted A/B outputs: m < hk/2 or m > N - hk/2, i.e. m = k2 + N2*k1 with
+  // k1 or N1 - 1 - k1 at most (hk/2)/N2
+  const int kmax = dif_kmax<N1, N2>(hk);
+  TL::template run<false, false, false, 2>(
       ysm, tw,
       [&](int n) {
         return make_float2((float)p0[n] + (float)p0[n + N], (float)p1[n] + (float)p1[n + N]);
       },
-      [&](int m, float2 v) { keep(2 * m, v); });
+      [&](int m, float2 v) { keep(2 * m, v); }, kmax);
   __syncthreads();
-  TL::template run<false, false, MC_FWD_PAIRED, 2>(
+  TL::template run<false, false, false, 2>(
       ysm, tw,
       [&](int n) {
         const float2 d = make_float2((float)p0[n] - (float)p0[n + N], (float)p1[n] - (float)p1[n + N]);
         return cmul(d, __ldg(tw + n));
       },
-      [&](int m, float2 v) { keep(2 * m + 1, v); });
+      [&](int m, float2 v) { keep(2 * m + 1, v); }, kmax);
   __syncthreads();
   for (int k = threadIdx.x; k < hk; k += TL::T) {
     const float2 z = zlo[k];
@@ -507,17 +522,19 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_
     else return;
     out[o] = make_float2(v.x * sc, v.y * sc);
   };
-  TL::template run<false, false, MC_COL_PAIRED, 2>(
+  // wanted outputs i < keep or i >= keep + shift: with no crop all of them
+  const int kmax = shift == 0 ? (N1 - 1) / 2 : dif_kmax<N1, N2>(keep + 1);
+  TL::template run<false, false, false, 2>(
       ysm, tw, [&](int n) { return cadd(__ldg(in + n), __ldg(in + n + N)); },
-      [&](int m, float2 v) { put(2 * m, v); });
+      [&](int m, float2 v) { put(2 * m, v); }, kmax);
   __syncthreads();
-  TL::template run<false, false, MC_COL_PAIRED, 2>(
+  TL::template run<false, false, false, 2>(
       ysm, tw,
       [&](int n) {
         const float2 x0 = __ldg(in + n), x1 = __ldg(in + n + N);
         return cmul(make_float2(x0.x - x1.x, x0.y - x1.y), __ldg(tw + n));
       },
-      [&](int m, float2 v) { put(2 * m + 1, v); });
+      [&](int m, float2 v) { put(2 * m + 1, v); }, kmax);
 }
 
 // Two-level splits compiled in (N1, N2).
