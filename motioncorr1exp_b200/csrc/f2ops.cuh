@@ -33,8 +33,25 @@ __device__ __forceinline__ f2reg f2fma(f2reg a, f2reg b, f2reg c) {  // a*b + c 
   return d;
 }
 __device__ __forceinline__ f2reg f2splat(float c) { return f2pk(make_float2(c, c)); }
-// complex add / subtract as one packed instruction
-__device__ __forceinline__ float2 padd(float2 a, float2 b) { return f2up(f2add(f2pk(a), f2pk(b))); }
-__device__ __forceinline__ float2 psub(float2 a, float2 b) { return f2up(f2sub(f2pk(a), f2pk(b))); }
+// Complex add / subtract of the butterflies.  MC_PACKED_ADD=1 makes each one
+// packed instruction; measured slower inside the codelets (the register
+// pairs raise the register count), so they stay scalar by default.
+#ifndef MC_PACKED_ADD
+#define MC_PACKED_ADD 0
+#endif
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+#if MC_PACKED_ADD
+  return f2up(f2add(f2pk(a), f2pk(b)));
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+#if MC_PACKED_ADD
+  return f2up(f2sub(f2pk(a), f2pk(b)));
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 
 }  // namespace mc

@@ -730,8 +730,13 @@ size_t pair_cols_reg_smem(int n, int team) {
   return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)teams * n * sizeof(float2);
 }
 
+// Resident 128-thread CTAs per SM the one-thread-per-subsequence kernel is
+// compiled for: four (128 registers) up to Q = 40, three (168) up to 56, two
+// (255) above.
+constexpr int pair_reg_min_blocks(int Q) { return Q <= 40 ? 4 : (Q <= 56 ? 3 : 2); }
+
 template <int Q>
-__global__ void __launch_bounds__(kRegThreads) k_pair_cols_reg(PairColsArgs a, int team) {
+__global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_cols_reg(PairColsArgs a, int team) {
   extern __shared__ float2 sm[];
   const int n = a.n, P = a.P, box = a.box;
   float* wcol = reinterpret_cast<float*>(sm);
