@@ -17,6 +17,11 @@ namespace mc {
 // written transposed: T[kx * ldt + y].
 struct FwdRowsArgs {
   const void* frame;   // ny rows of nx pixels (MRC pixel type `mode`)
+  // when set, the frame is *frames_slot + frame_offset bytes instead: the base
+  // of the run's frames is read on the device, so a captured graph serves any
+  // frame buffer written to the slot before its launch
+  const void* const* frames_slot;
+  long long frame_offset;
   int mode;            // 0 int8, 1 int16, 2 float32, 6 uint16
   int nx, ny;
   int offx, offy, nu;  // square crop

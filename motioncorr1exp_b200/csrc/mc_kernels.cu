@@ -58,8 +58,16 @@ __device__ __forceinline__ void copy_table(float2* dst, const float2* __restrict
 
 }  // namespace
 
+// Frame read by a forward launch (direct pointer, or the run's base from the
+// device-side slot plus this frame's offset).
+__device__ __forceinline__ const void* fwd_frame(const FwdRowsArgs& a) {
+  return a.frames_slot ? static_cast<const void*>(static_cast<const char*>(*a.frames_slot) + a.frame_offset)
+                       : a.frame;
+}
+
 // =========================================================== forward rows ==
 __global__ void __launch_bounds__(kThreads) k_fwd_rows(FwdRowsArgs a) {
+  const void* frame = fwd_frame(a);
   extern __shared__ float2 sm[];
   const int nu = a.nu;
   float2* b0 = sm;
@@ -83,7 +91,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_rows(FwdRowsArgs a) {
     float re, im;
     if (a.two_outputs) {
       const long long i0 = r0 + x;
-      const float raw = load_pixel(a.frame, a.mode, i0);
+      const float raw = load_pixel(frame, a.mode, i0);
       const float d1 = hasd ? a.dark[i0] : 0.f;
       const float d2 = hasd ? (a.dark2 ? a.dark2[i0] : 0.f) : 0.f;
       const float g1 = hasn ? a.norm[i0] : 1.f;
@@ -91,8 +99,8 @@ __global__ void __launch_bounds__(kThreads) k_fwd_rows(FwdRowsArgs a) {
       re = (raw - d1) * g1;  // hbuf   (DFAlign.cu:725)
       im = (raw - d2) * g2;  // hbuf2  (DFAlign.cu:724)
     } else {
-      re = load_pixel(a.frame, a.mode, r0 + x);
-      im = load_pixel(a.frame, a.mode, r1 + x);
+      re = load_pixel(frame, a.mode, r0 + x);
+      im = load_pixel(frame, a.mode, r1 + x);
       if (hasd || hasn) {  // identical references: one spectrum per frame
         const long long i0 = r0 + x, i1 = r1 + x;
         re = (re - (hasd ? a.dark[i0] : 0.f)) * (hasn ? a.norm[i0] : 1.f);
@@ -294,7 +302,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_
 template <typename Px>
 __device__ __forceinline__ void stage_rows(float2* xin, const FwdRowsArgs& a, long long r0, long long r1, int n,
                                            int nth) {
-  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const Px* f = reinterpret_cast<const Px*>(fwd_frame(a));
   const bool hasd = a.dark != nullptr, hasn = a.norm != nullptr;
   if (a.two_outputs) {
 #pragma unroll 4
@@ -364,7 +372,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
   unsigned char* raw0 = reinterpret_cast<unsigned char*>(dynraw + N);
   unsigned char* raw1 = raw0 + RB;
   const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
-  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const Px* f = reinterpret_cast<const Px*>(fwd_frame(a));
   const Px* row0 = f + (long long)(a.offy + y0) * a.nx + a.offx;
   const Px* row1 = f + (long long)(a.offy + y1) * a.nx + a.offx;
   stage_raw_row<Px>(raw0, row0, N, threadIdx.x, TL::T);
@@ -463,7 +471,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
   unsigned char* raw0 = reinterpret_cast<unsigned char*>(zhi + hk);
   unsigned char* raw1 = raw0 + RB;
   const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
-  const Px* f = reinterpret_cast<const Px*>(a.frame);
+  const Px* f = reinterpret_cast<const Px*>(fwd_frame(a));
   const Px* row0 = f + (long long)(a.offy + y0) * a.nx + a.offx;
   const Px* row1 = f + (long long)(a.offy + y1) * a.nx + a.offx;
   stage_raw_row<Px>(raw0, row0, L, threadIdx.x, TL::T);

@@ -302,8 +302,9 @@ struct mc_plan {
   int *d_mask = nullptr, *d_order = nullptr, *d_uf = nullptr, *d_kept = nullptr, *d_nkept = nullptr;
   int* d_status = nullptr;
   unsigned char* h_stage = nullptr;  // pinned copies of the per-movie results
+  const void** d_src_slot = nullptr;  // device word: base of the run's frames (read by the forward kernels)
   size_t st_dc = 0, st_pshift = 0, st_pcc = 0, st_ppeak = 0, st_ki1 = 0, st_kept = 0, st_nkept = 0, st_ki2 = 0,
-         st_work = 0, st_status = 0, st_bytes = 0;
+         st_work = 0, st_status = 0, st_slot = 0, st_bytes = 0;
   // captured movie graphs, one per frame configuration (frame range, sum
   // range, pair distance, threshold, reference frame) the plan has run
   struct GraphEntry {
@@ -915,8 +916,10 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
     place(pl->st_ki2, sizeof(double) * np);
     place(pl->st_work, sizeof(double) * 2 * (size_t)nc);
     place(pl->st_status, sizeof(int));
+    place(pl->st_slot, sizeof(void*));
     pl->st_bytes = o;
     CK(cudaMallocHost(&pl->h_stage, o));
+    CKR(pl->alloc(&pl->d_src_slot, sizeof(void*)));
   }
 
   // tables
@@ -1079,6 +1082,8 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     if (waits && f % chunk == 0) CK(cudaStreamWaitEvent(pl->st, (*waits)[f / chunk], 0));
     mc::FwdRowsArgs a{};
     a.frame = (const char*)(pl->frames_src ? pl->frames_src : pl->d_frames) + (size_t)f * pl->frame_bytes;
+    a.frames_slot = pl->d_src_slot;
+    a.frame_offset = (long long)f * (long long)pl->frame_bytes;
     a.mode = pl->mode;
     a.nx = pl->nx;
     a.ny = pl->ny;
@@ -1190,7 +1195,20 @@ static void log_frame_means(mc_plan* pl, const float2* dc) {
   }
 }
 
+// Base of the run's frames (the plan's buffer or bound caller frames) into
+// the device word the forward kernels read, ordered on the plan stream
+// before them; outside any capture, so a captured movie serves every frame
+// buffer.  The pinned source word is rewritten only after the previous
+// movie synchronised.
+static int upload_frame_base(mc_plan* pl) {
+  const void** h = reinterpret_cast<const void**>(pl->h_stage + pl->st_slot);
+  *h = pl->frames_src ? pl->frames_src : pl->d_frames;
+  CK(cudaMemcpyAsync(pl->d_src_slot, h, sizeof(void*), cudaMemcpyHostToDevice, pl->st));
+  return MC_OK;
+}
+
 static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
+  CKR(upload_frame_base(pl));
   CK(cudaEventRecord(pl->ev[0], pl->st));
   CKR(enqueue_forward(pl, waits, chunk));
   CK(cudaEventRecord(pl->ev[1], pl->st));
@@ -1757,6 +1775,7 @@ static int finish_device_movie(mc_plan* pl) {
 // CUDA graph and replayed (unless profiling, MC_NO_GRAPH, or a capture failure).
 static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEvent_t>* waits, int chunk) {
   const bool graph_ok = !waits && !pl->profiling && !pl->graph_failed && !getenv("MC_NO_GRAPH");
+  CKR(upload_frame_base(pl));
   CK(cudaEventRecord(pl->ev[0], pl->st));
   mc_plan::GraphEntry* ge = nullptr;
   if (graph_ok) {
@@ -1767,7 +1786,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
     std::memcpy(&kt, &kf, sizeof(float));
     const std::vector<long long> key = {pl->nstart, pl->nend, nss, nes, lim, pl->p.FrameDistOffset,
                                         pl->p.bAlignToMid ? 1 : 0, kt & 0xffffffffLL,
-                                        (long long)(uintptr_t)pl->frames_src};
+                                        };
     for (auto& g : pl->graphs)
       if (g.key == key) ge = &g;
     if (!ge) {

@@ -141,3 +141,21 @@ def test_batch_reports_failing_movie(gpu):
         np.testing.assert_array_equal(img, _one(mv, p)[0])
         with pytest.raises(_lib.McError):
             b.run(movies)
+
+
+def test_graph_serves_every_bound_buffer(gpu):
+    """One captured movie graph, frame buffers swapped between replays: the
+    frame base is read on the device, so each replay aligns the bound movie."""
+    a, b = _movie(256, 256, 10, 47), _movie(256, 256, 10, 48)
+    p = api.verify_params(api.Params(CCPeakSearchDim=64), 10)
+    ref_a, ref_b = _one(a, p), _one(b, p)
+    da, db = torch.from_numpy(a.frames).cuda(), torch.from_numpy(b.frames).cuda()
+    with api.Plan(p, 256, 256, 10, 0) as pl:
+        for d, ref in ((da, ref_a), (db, ref_b), (da, ref_a), (db, ref_b)):
+            pl.bind_frames_device(d.data_ptr())
+            img = pl.run()
+            np.testing.assert_array_equal(img, ref[0])
+            np.testing.assert_array_equal(pl.frame_shifts(), ref[1])
+        # the plan's own buffer after bound ones
+        pl.load_frames(a.frames)
+        np.testing.assert_array_equal(pl.run(), ref_a[0])
