@@ -234,7 +234,276 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(SolveArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory form of the same solve (used when its working set fits):
+// the pair list, the measured shifts, the normal matrix and the residuals
+// live in shared memory; the normal equations are built one frame step per
+// thread in a single pass over the pairs (a histogram of the pair ends per
+// step, then suffix sums), and the per-row residual and compaction loops run
+// in parallel.  Sums run in the same order as the global-memory form.
+namespace {
+
+struct SolveSmem {
+  int2* pr;        // [P]
+  float2* ps;      // [P]
+  int* mask;       // [P]
+  double* ki;      // [P]
+  int* hist;       // [nc][nf]
+  double* M;       // [nc][nc]
+  double* rx;      // [nc]
+  double* ry;      // [nc]
+};
+
+__device__ bool solve_masked_smem(const SolveSmem& m, int P, int nf, double* sx, double* sy) {
+  const int nc = nf - 1, tid = threadIdx.x;
+  __shared__ int s_bad;
+  if (tid == 0) s_bad = 0;
+  // step k: rows with i <= k < j; histogram of their ends j and rhs sums
+  for (int k = tid; k < nc; k += kSolveThreads) {
+    int* h = m.hist + (size_t)k * nf;
+    for (int j = 0; j < nf; j++) h[j] = 0;
+    double x = 0.0, y = 0.0;
+    for (int r = 0; r < P; r++) {
+      const int2 q = m.pr[r];
+      if (m.mask[r] && q.x <= k && k < q.y) {
+        h[q.y]++;
+        x += (double)m.ps[r].x;
+        y += (double)m.ps[r].y;
+      }
+    }
+    m.rx[k] = x;
+    m.ry[k] = y;
+    // M[k][l] (l >= k) = rows with i <= k and j > l: suffix sums of the ends
+    int c = 0;
+    for (int l = nc - 1; l >= k; l--) {
+      c += h[l + 1];
+      m.M[(size_t)k * nc + l] = (double)c;
+      m.M[(size_t)l * nc + k] = (double)c;
+    }
+  }
+  __syncthreads();
+  double dmax = 1.0;
+  for (int k = 0; k < nc; k++) dmax = fmax(dmax, m.M[(size_t)k * nc + k]);
+  const double tiny = 1e-12 * dmax;
+  double* M = m.M;
+  for (int k = 0; k < nc; k++) {
+    if (tid == 0) {
+      const double d = M[(size_t)k * nc + k];
+      if (!(d > tiny)) s_bad = 1;
+      M[(size_t)k * nc + k] = sqrt(fmax(d, tiny));
+    }
+    __syncthreads();
+    const double lkk = M[(size_t)k * nc + k];
+    for (int i = k + 1 + tid; i < nc; i += kSolveThreads) M[(size_t)i * nc + k] /= lkk;
+    __syncthreads();
+    const int w = nc - k - 1;
+    for (int idx = tid; idx < w * w; idx += kSolveThreads) {
+      const int i = k + 1 + idx / w, j = k + 1 + idx % w;
+      if (j <= i) M[(size_t)i * nc + j] -= M[(size_t)i * nc + k] * M[(size_t)j * nc + k];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < nc; i++) {
+      double vx = m.rx[i], vy = m.ry[i];
+      for (int q = 0; q < i; q++) {
+        vx -= M[(size_t)i * nc + q] * m.rx[q];
+        vy -= M[(size_t)i * nc + q] * m.ry[q];
+      }
+      m.rx[i] = vx / M[(size_t)i * nc + i];
+      m.ry[i] = vy / M[(size_t)i * nc + i];
+    }
+    for (int i = nc - 1; i >= 0; i--) {
+      double vx = m.rx[i], vy = m.ry[i];
+      for (int q = i + 1; q < nc; q++) {
+        vx -= M[(size_t)q * nc + i] * sx[q];
+        vy -= M[(size_t)q * nc + i] * sy[q];
+      }
+      sx[i] = vx / M[(size_t)i * nc + i];
+      sy[i] = vy / M[(size_t)i * nc + i];
+    }
+  }
+  __syncthreads();
+  return s_bad == 0;
+}
+
+// residual |sum of steps i..j-1 - measured| of row r (steps summed k ascending)
+__device__ double row_residual(const SolveSmem& m, const double* wx, const double* wy, int r) {
+  const int2 q = m.pr[r];
+  double ax = 0.0, ay = 0.0;
+  for (int k = q.x; k < q.y; k++) {
+    ax += wx[k];
+    ay += wy[k];
+  }
+  const double dx = ax - (double)m.ps[r].x, dy = ay - (double)m.ps[r].y;
+  return sqrt(dx * dx + dy * dy);
+}
+
+size_t solve_smem_bytes(int P, int nf) {
+  const size_t nc = nf - 1;
+  return (size_t)P * (sizeof(int2) + sizeof(float2) + sizeof(int) + sizeof(double)) + nc * nf * sizeof(int) +
+         nc * nc * sizeof(double) + 6 * (size_t)nf * sizeof(double) + 64;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
+  extern __shared__ double sdyn[];
+  const int P = a.npairs, nf = a.nframe, nc = nf - 1, tid = threadIdx.x;
+  SolveSmem m;
+  m.M = sdyn;
+  m.rx = m.M + (size_t)nc * nc;
+  m.ry = m.rx + nc;
+  double* wx = m.ry + nc;
+  double* wy = wx + nc;
+  m.ki = wy + nc;
+  m.ps = reinterpret_cast<float2*>(m.ki + P);
+  m.pr = reinterpret_cast<int2*>(m.ps + P);
+  m.mask = reinterpret_cast<int*>(m.pr + P);
+  m.hist = m.mask + P;
+  for (int r = tid; r < P; r += kSolveThreads) {
+    m.pr[r] = a.pairs[r];
+    m.ps[r] = make_float2(a.pshift[2 * r], a.pshift[2 * r + 1]);
+    m.mask[r] = 1;
+  }
+  __syncthreads();
+  if (!solve_masked_smem(m, P, nf, wx, wy)) {
+    if (tid == 0) *a.status = -6;
+    return;
+  }
+  for (int r = tid; r < P; r += kSolveThreads) {
+    const double v = row_residual(m, wx, wy, r);
+    m.ki[r] = v;
+    a.ki1[r] = v;
+  }
+  __syncthreads();
+  // stable ascending rank of ki1 (OD_Threshold's repeated first-minimum pick)
+  int* order = a.order;
+  for (int r = tid; r < P; r += kSolveThreads) {
+    const double v = m.ki[r];
+    int pos = 0;
+    for (int q = 0; q < P; q++) {
+      const double u = m.ki[q];
+      pos += (u < v || (u == v && q < r)) ? 1 : 0;
+    }
+    order[pos] = r;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int i;
+    for (i = P - 1; i >= nc; i--)
+      if (m.ki[order[i]] < (double)a.kithresh) break;
+    int len = i + 1;
+    int* par = a.uf;
+    for (int f = 0; f < nf; f++) par[f] = f;
+    int comps = nf;
+    for (int q = 0; q < P; q++) m.mask[q] = 0;
+    auto add = [&](int row) {
+      m.mask[row] = 1;
+      const int x = uf_find(par, m.pr[row].x), y = uf_find(par, m.pr[row].y);
+      if (x != y) {
+        par[x] = y;
+        comps--;
+      }
+    };
+    for (int q = 0; q < len && q < P; q++) add(order[q]);
+    while (comps > 1 && len < P) add(order[len++]);
+    *a.nkept = min(len, P);
+  }
+  __syncthreads();
+  if (!solve_masked_smem(m, P, nf, wx, wy)) {
+    if (tid == 0) *a.status = -6;
+    return;
+  }
+  // kept rows ascending with their second-round residuals: an exclusive scan
+  // of the mask gives each kept row its slot
+  __shared__ int s_base;
+  __shared__ int s_warp[kSolveThreads / 32];
+  if (tid == 0) s_base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < P; c0 += kSolveThreads) {
+    const int r = c0 + tid;
+    const int f = (r < P && m.mask[r]) ? 1 : 0;
+    const int lane = tid & 31, wid = tid >> 5;
+    int incl = f;
+    for (int d = 1; d < 32; d <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    int before = s_base;
+    for (int w = 0; w < wid; w++) before += s_warp[w];
+    if (f) {
+      const int slot = before + incl - 1;
+      a.kept[slot] = r;
+      a.ki2[slot] = row_residual(m, wx, wy, r);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < kSolveThreads / 32; w++) t += s_warp[w];
+      s_base += t;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double* sx = a.shift;
+    double ox = 0.0, oy = 0.0, px = 0.0, py = 0.0, tx = 0.0, ty = 0.0;
+    a.frame_shift[0] = 0.0;
+    a.frame_shift[1] = 0.0;
+    for (int k = 0; k < nc; k++) {
+      const double nx = ox + wx[k], ny = oy + wy[k];
+      ox = nx;
+      oy = ny;
+      const double stx = nx - px, sty = ny - py;
+      px = nx;
+      py = ny;
+      sx[2 * k] = stx;
+      sx[2 * k + 1] = sty;
+      tx += stx;
+      ty += sty;
+      a.frame_shift[2 * (k + 1)] = tx;
+      a.frame_shift[2 * (k + 1) + 1] = ty;
+    }
+    double mx = 0.0, my = 0.0;
+    if (a.align_to_mid)
+      for (int k = 0; k < a.mid_steps; k++) {
+        mx += sx[2 * k];
+        my += sx[2 * k + 1];
+      }
+    double Tx = 0.0, Ty = 0.0;
+    for (int k = 1; k < a.sum_first + 1; k++) {
+      Tx += sx[2 * (k - 1)];
+      Ty += sx[2 * (k - 1) + 1];
+    }
+    for (int k = a.sum_first; k <= a.sum_last; k++) {
+      if (k > a.sum_first) {
+        Tx += sx[2 * (k - 1)];
+        Ty += sx[2 * (k - 1) + 1];
+      }
+      const int q2 = k - a.sum_first;
+      a.sum_shift[q2] = make_double2(-Tx + mx, -Ty + my);
+      a.sum_frames[q2] = k;
+      a.sum_apply[q2] = (k == a.sum_first && !a.align_to_mid) ? 0 : 1;
+    }
+    // the final solve's per-step shifts into work[], where the host reads them
+    for (int k = 0; k < nc; k++) {
+      a.work[k] = wx[k];
+      a.work[nc + k] = wy[k];
+    }
+    *a.status = 0;
+  }
+}
+
 cudaError_t launch_solve(const SolveArgs& a, cudaStream_t st) {
+  const size_t smem = solve_smem_bytes(a.npairs, a.nframe);
+  if (smem <= 200 * 1024) {
+    cudaError_t e = allow_smem((const void*)k_solve_smem, smem);
+    if (e != cudaSuccess) return e;
+    k_solve_smem<<<1, kSolveThreads, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   k_solve<<<1, kSolveThreads, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -257,3 +257,27 @@ def test_pipeline_c3_geometry(gpu):
     g, ref, p = run_both(mv.frames, 0, api.Params(bin=2.0, FrameDistOffset=1))
     assert (ref.nsam_unbin, ref.nsam) == (7420, 3710)
     compare_full(g, ref, 3710, 0)
+
+
+@pytest.mark.parametrize("n,q,ppc", [(256, 8, 4), (240, 16, 3), (256, 64, 64), (256, 32, 7)])
+def test_pair_boxes_scheduled(gpu, n, q, ppc):
+    """Schedules other than the built-in choice (split n = P*Q, pairs per CTA,
+    a last CTA with fewer pairs) against the oracle's CC windows."""
+    mv = synth.make_movie(n + 6, n, 8, mean=1.5, seed=n + q, dtype="f32", speed=0.7, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2), 8)
+    api.schedule_set(n, pair_q=q, pairs_per_cta=ppc)
+    try:
+        with api.Plan(p, n + 6, n, 8, 2) as pl:
+            assert (pl.info["prune_p"], pl.info["prune_q"]) == (n // q, q)
+            pl.load_frames(mv.frames)
+            pl.forward()
+            pl.pairs()
+            gb = pl.boxes()
+            gres = pl.pair_results()
+    finally:
+        api.schedule_clear()
+    ob, _, _ = oracle_boxes(mv.frames, 2, p)
+    for r in range(len(ob)):
+        assert rel_l2(gb[r], ob[r]) < 1e-5
+    ref = O.align_movie(mv.frames, 2, to_oparams(p))
+    check_pairs(gres, ref, n, 0, ob)
