@@ -23,8 +23,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills"]
 
-LIB_SOURCES = ["mc_kernels.cu", "mc_plan.cu", "mc_solve.cu", "mc_noalloc.cu", "lsq.cpp", "mc_batch.cpp"]
-LIB_HEADERS = ["kernels.cuh", "fft_engine.cuh", "f2ops.cuh", "dft_gen.cuh", "codelets_gen.cuh", "lsq.h"]
+LIB_SOURCES = ["mc_kernels.cu", "mc_fwd.cu", "mc_fwd_raw.cu", "mc_fwd_dif.cu", "mc_pair.cu", "mc_sum.cu", "mc_plan.cu",
+               "mc_solve.cu", "mc_noalloc.cu", "lsq.cpp", "mc_batch.cpp"]
+LIB_HEADERS = ["kernels.cuh", "kcommon.cuh", "fft_engine.cuh", "f2ops.cuh", "dft_gen.cuh", "codelets_gen.cuh", "lsq.h"]
 CLI_SOURCES = ["cli/dosefgpu_driftcorr.cpp", "cli/mrc_file.cpp"]
 CLI_HEADERS = ["cli/mrc_file.h"]
 

@@ -1,0 +1,126 @@
+// Forward row pass of libmc for two-level lengths (sm_100a): two rows packed
+// as one complex FFT, raw-pixel staging when no dark/gain references apply
+// (DFAlign.cu:710-806).
+#include <algorithm>
+
+#include "kcommon.cuh"
+
+namespace mc {
+
+// Forward rows without references: two rows staged as raw pixels (a quarter
+// of the float staging for 8-bit frames), decoded in the step-A loads; the
+// spectrum Z is written back into the exchange buffer after the barrier that
+// follows the step-B reads.
+template <int N1, int N2, typename Px>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows2l_raw(FwdRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  constexpr int RB = raw_row_bytes<Px>(N);
+  extern __shared__ float2 dynraw[];
+  float2* ysm = dynraw;
+  unsigned char* raw0 = reinterpret_cast<unsigned char*>(dynraw + N);
+  unsigned char* raw1 = raw0 + RB;
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const Px* f = reinterpret_cast<const Px*>(fwd_frame(a));
+  const Px* row0 = f + (long long)(a.offy + y0) * a.nx + a.offx;
+  const Px* row1 = f + (long long)(a.offy + y1) * a.nx + a.offx;
+  stage_raw_row<Px>(raw0, row0, N, threadIdx.x, TL::T);
+  stage_raw_row<Px>(raw1, row1, N, threadIdx.x, TL::T);
+  __syncthreads();
+  const Px* p0 = reinterpret_cast<const Px*>(raw0 + (reinterpret_cast<uintptr_t>(row0) & 15));
+  const Px* p1 = reinterpret_cast<const Px*>(raw1 + (reinterpret_cast<uintptr_t>(row1) & 15));
+  TL::template run<false, true, MC_FWD_PAIRED>(
+      ysm, a.tw, [&](int x) { return make_float2((float)p0[x], (float)p1[x]); },
+      [&](int k, float2 v) { ysm[k] = v; });
+  __syncthreads();
+  for (int k = threadIdx.x; k < a.hk; k += TL::T) {
+    const float2 z = ysm[k];
+    const float2 zc = ysm[k == 0 ? 0 : N - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    *reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0) = make_float4(X.x, X.y, Y.x, Y.y);
+  }
+}
+
+// Forward rows: two image rows (or the two reference sets of one row) packed
+// as one complex transform, then split into the two real half spectra.
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows2l(FwdRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  extern __shared__ float2 dyn2l[];
+  float2* xin = dyn2l;      // packed input rows, later the spectrum Z
+  float2* ysm = dyn2l + N;  // exchange buffer
+  int y0, y1;
+  if (a.two_outputs) {
+    y0 = blockIdx.x;
+    y1 = y0;
+  } else {
+    y0 = 2 * blockIdx.x;
+    y1 = y0 + 1;
+  }
+  const long long r0 = (long long)(a.offy + y0) * a.nx + a.offx;
+  const long long r1 = (long long)(a.offy + y1) * a.nx + a.offx;
+  switch (a.mode) {
+    case 0: stage_rows<int8_t>(xin, a, r0, r1, N, TL::T); break;
+    case 1: stage_rows<int16_t>(xin, a, r0, r1, N, TL::T); break;
+    case 6: stage_rows<uint16_t>(xin, a, r0, r1, N, TL::T); break;
+    default: stage_rows<float>(xin, a, r0, r1, N, TL::T); break;
+  }
+  __syncthreads();
+  // step B writes Z into xin: every step-A read of xin precedes the barrier
+  // between the steps, and step B reads only ysm
+  float2* zsm = xin;
+  TL::template run<false, false>(
+      ysm, a.tw, [&](int x) { return xin[x]; }, [&](int k, float2 v) { zsm[k] = v; });
+  __syncthreads();
+  for (int k = threadIdx.x; k < a.hk; k += TL::T) {
+    const float2 z = zsm[k];
+    const float2 zc = zsm[k == 0 ? 0 : N - k];
+    const float2 X = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 Y = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    if (a.two_outputs) {
+      a.outA[(long long)k * a.ldt + y0] = X;
+      a.outB[(long long)k * a.ldt + y0] = Y;
+    } else {
+      *reinterpret_cast<float4*>(a.outA + (long long)k * a.ldt + y0) = make_float4(X.x, X.y, Y.x, Y.y);
+    }
+  }
+}
+
+cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (!two_level_split(a.nu, n1, n2)) return cudaErrorInvalidValue;
+  const int grid = a.two_outputs ? a.nu : a.nu / 2;
+  const bool raw = !a.two_outputs && !a.dark && !a.dark2 && !a.norm && !a.norm2;
+#define MC_TL_RAW(A, B, PX)                                                                          \
+  {                                                                                                  \
+    const size_t smem = (size_t)(A) * (B) * sizeof(float2) + 2 * (size_t)raw_row_bytes<PX>((A) * (B)); \
+    cudaError_t e = allow_smem((const void*)k_fwd_rows2l_raw<A, B, PX>, smem);                       \
+    if (e != cudaSuccess) return e;                                                                  \
+    k_fwd_rows2l_raw<A, B, PX><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                            \
+    return cudaGetLastError();                                                                       \
+  }
+#define MC_TL_LAUNCH(A, B)                                                                           \
+  if (n1 == (A) && n2 == (B)) {                                                                      \
+    if (raw) {                                                                                       \
+      switch (a.mode) {                                                                              \
+        case 0: MC_TL_RAW(A, B, int8_t)                                                              \
+        case 1: MC_TL_RAW(A, B, int16_t)                                                             \
+        case 6: MC_TL_RAW(A, B, uint16_t)                                                            \
+        default: MC_TL_RAW(A, B, float)                                                              \
+      }                                                                                              \
+    }                                                                                                \
+    const size_t smem = (size_t)2 * (A) * (B) * sizeof(float2);                                      \
+    cudaError_t e = allow_smem((const void*)k_fwd_rows2l<A, B>, smem);                               \
+    if (e != cudaSuccess) return e;                                                                  \
+    k_fwd_rows2l<A, B><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                                    \
+    return cudaGetLastError();                                                                       \
+  }
+  MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)
+#undef MC_TL_LAUNCH
+#undef MC_TL_RAW
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace mc

@@ -1,0 +1,382 @@
+// Pair stage of libmc (sm_100a): cross power x B-factor with the inverse
+// along ky pruned to the pbx rows (cufunc.cu:343-370), and the pruned C2R
+// along kx onto the pbx window (cufunc.cu:229-233, 404-407).
+#include <algorithm>
+
+#include "kcommon.cuh"
+
+namespace mc {
+
+// ============================================================ pair columns ==
+size_t pair_cols_smem(int n, int P, int Q, int box) {
+  return (size_t)2 * n * sizeof(float2)       // ping-pong
+         + (size_t)n * sizeof(float)          // B-factor column
+         + (size_t)Q * sizeof(float2)         // inner twiddles
+         + (size_t)P * box * sizeof(float2);  // outer twiddles
+}
+
+__global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, P = a.P, Q = a.Q, box = a.box;
+  float2* x0 = sm;
+  float2* x1 = sm + n;
+  float* wcol = reinterpret_cast<float*>(sm + 2 * n);
+  float2* twQ = reinterpret_cast<float2*>(wcol + n + (n & 1));  // keep 8-byte alignment
+  float2* twO = twQ + Q;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int kx = blockIdx.y;
+  copy_table(twQ, a.twQ, Q);
+  copy_table(twO, a.twO, P * box);
+  const int half = n / 2;
+  for (int ky = tid; ky < n; ky += nth) {
+    const int y = ky < half ? ky : ky - n;
+    const float r2 = (float)(kx * kx + y * y);
+    wcol[ky] = expf(a.mbf * r2) * a.inv_size;
+  }
+  __syncthreads();
+  const int p0 = blockIdx.x * a.pairs_per_cta;
+  const int p1 = min(p0 + a.pairs_per_cta, a.npairs);
+  const int nout = box * 2;  // two threads per output (k1 halves)
+  const int khalf = (P + 1) / 2;
+  for (int p = p0; p < p1; p++) {
+    const int2 pr = a.pairs[p];
+    const float2* ca = a.specA + (long long)pr.x * a.strideA + (long long)kx * a.ldn;
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    for (int ky = tid; ky < n; ky += nth) {
+      const float2 u = ca[ky], v = cb[ky];
+      x0[ky] = cscale(cmulc(u, v), wcol[ky]);
+    }
+    __syncthreads();
+    const float2* Y = fft_run<true, true>(x0, x1, a.qplan, P, 0, twQ, tid, nth);
+    for (int base = 0; base < nout; base += nth) {
+      const int o = base + tid;
+      const bool ok = o < nout;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = Y + (long long)P * r;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = twO[k * box + m];
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Register-codelet variant of the column stage (P <= 128, Q a codelet length).
+// A CTA of 128 threads owns one column kx; it is split into teams of `team`
+// threads (team = P rounded up to a warp multiple) and each team takes whole
+// pairs.  Thread k1 < P of a team gathers its stride-P subsequence
+// c(k1 + P*k2), k2 < Q, straight from the two spectra (coalesced over k1),
+// runs the Q-point inverse FFT in registers, and parks the result in shared
+// memory; the team then forms the pbx output rows as P-term sums.
+constexpr int kRegThreads = 128;
+
+__device__ __forceinline__ void team_barrier(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+size_t pair_cols_reg_smem(int n, int team) {
+  const int teams = kRegThreads / team;
+  return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)teams * n * sizeof(float2);
+}
+
+// Resident 128-thread CTAs per SM the one-thread-per-subsequence kernel is
+// compiled for: four (128 registers) up to Q = 40, three (168) up to 56, two
+// (255) above.
+constexpr int pair_reg_min_blocks(int Q) { return Q <= 40 ? 4 : (Q <= 56 ? 3 : 2); }
+
+template <int Q>
+__global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_cols_reg(PairColsArgs a, int team) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, P = a.P, box = a.box;
+  float* wcol = reinterpret_cast<float*>(sm);
+  const int teams = kRegThreads / team;
+  const int tid = threadIdx.x;
+  const int tm = tid / team, lt = tid - tm * team;
+  float2* Y = sm + (n + 1) / 2 + (size_t)tm * n;
+  const int kx = blockIdx.y;
+  const int half = n / 2;
+  for (int ky = tid; ky < n; ky += kRegThreads) {
+    const int y = ky < half ? ky : ky - n;
+    wcol[ky] = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+  }
+  __syncthreads();
+  const int p0 = blockIdx.x * a.pairs_per_cta;
+  const int p1 = min(p0 + a.pairs_per_cta, a.npairs);
+  const int khalf = (P + 1) / 2;
+  for (int p = p0 + tm; p < p1; p += teams) {
+    const int2 pr = a.pairs[p];
+    const float2* ca = a.specA + (long long)pr.x * a.strideA + (long long)kx * a.ldn;
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    if (lt < P) {
+      float2 x[Q];
+#pragma unroll
+      for (int k2 = 0; k2 < Q; k2++) {
+        const int ky = lt + P * k2;
+        x[k2] = cscale(cmulc(__ldg(ca + ky), __ldg(cb + ky)), wcol[ky]);
+      }
+      fft_reg<Q, true>(x);
+#pragma unroll
+      for (int r = 0; r < Q; r++) Y[lt + P * r] = x[r];
+    }
+    team_barrier(1 + tm, team);
+    for (int base = 0; base < 2 * box; base += team) {
+      const int o = base + lt;
+      const bool ok = o < 2 * box;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = Y + P * r;
+        const float2* tw = a.twO + m;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = __ldg(tw + k * box);
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    team_barrier(1 + tm, team);
+  }
+}
+
+// ---- grouped variant: one CTA per (A frame group, column kx) -------------
+// The pairs of a batch come in groups that share their A spectrum (the
+// reference's i-major order).  The CTA stages A(kx,:) x B-factor once in
+// shared memory; each team double-buffers the B columns of its pairs with
+// 16-byte cp.async copies, so the copy of pair p+1 overlaps the transform of
+// pair p.  Thread k1 reads only positions k1 + P*k2 of the B buffer and
+// writes Y back to the same positions, so Y lives in the consumed buffer.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+size_t pair_cols_grp_smem(int n, int teams) { return (size_t)(1 + 2 * teams) * n * sizeof(float2); }
+
+template <int Q>
+__global__ void __launch_bounds__(kRegThreads) k_pair_cols_grp(PairColsArgs a, const int2* __restrict__ groups,
+                                                               int team) {
+  extern __shared__ float2 smg[];
+  const int n = a.n, P = a.P, box = a.box;
+  const int teams = kRegThreads / team;
+  const int tid = threadIdx.x;
+  const int tm = tid / team, lt = tid - tm * team;
+  float2* aw = smg;
+  float2* buf0 = smg + n + (size_t)2 * tm * n;
+  const int kx = blockIdx.y;
+  const int2 g = groups[blockIdx.x];  // (first pair, count)
+  const int half = n / 2;
+  const int2 pr0 = a.pairs[g.x];
+  const float2* ca = a.specA + (long long)pr0.x * a.strideA + (long long)kx * a.ldn;
+  for (int ky = tid; ky < n; ky += kRegThreads) {
+    const int y = ky < half ? ky : ky - n;
+    const float w = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+    aw[ky] = cscale(__ldg(ca + ky), w);
+  }
+  const int nchunk = n / 2;  // 16-byte chunks of a column (n is even)
+  auto fetch = [&](int q, float2* dst) {
+    const int2 pr = a.pairs[g.x + q];
+    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
+    for (int c = lt; c < nchunk; c += team) cp_async16(dst + 2 * c, cb + 2 * c);
+  };
+  int cur = 0;
+  if (tm < g.y) fetch(tm, buf0);
+  cp_async_commit();
+  __syncthreads();  // aw visible to every team
+  const int khalf = (P + 1) / 2;
+  for (int q = tm; q < g.y; q += teams) {
+    float2* bc = buf0 + (size_t)cur * n;
+    if (q + teams < g.y) fetch(q + teams, buf0 + (size_t)(cur ^ 1) * n);
+    cp_async_commit();
+    cp_async_wait<1>();
+    team_barrier(1 + tm, team);
+    if (lt < P) {
+      float2 x[Q];
+#pragma unroll
+      for (int k2 = 0; k2 < Q; k2++) {
+        const int ky = lt + P * k2;
+        x[k2] = cmulc(aw[ky], bc[ky]);
+      }
+      fft_reg<Q, true>(x);
+#pragma unroll
+      for (int r = 0; r < Q; r++) bc[lt + P * r] = x[r];
+    }
+    team_barrier(1 + tm, team);
+    const int p = g.x + q;
+    for (int base = 0; base < 2 * box; base += team) {
+      const int o = base + lt;
+      const bool ok = o < 2 * box;
+      const int m = o >> 1, h = o & 1;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int r = (a.ystart + m) % Q;
+        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
+        const float2* yr = bc + P * r;
+        const float2* tw = a.twO + m;
+        for (int k = k0; k < k1; k++) {
+          const float2 t = __ldg(tw + k * box);
+          const float2 yv = yr[k];
+          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
+    }
+    team_barrier(1 + tm, team);  // buffer `cur` may now be refilled
+    cur ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+template <int Q>
+cudaError_t launch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
+  const size_t smem = pair_cols_grp_smem(a.n, kRegThreads / team);
+  cudaError_t e = allow_smem((const void*)k_pair_cols_grp<Q>, smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(ngroups, a.H);
+  k_pair_cols_grp<Q><<<grid, kRegThreads, smem, st>>>(a, groups, team);
+  return cudaGetLastError();
+}
+
+template <int I = 0>
+cudaError_t dispatch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
+  if constexpr (I < kNumCodelets) {
+    constexpr int Q = kCodelets[I];
+    if (a.Q == Q) return launch_grp<Q>(a, groups, ngroups, team, st);
+    return dispatch_grp<I + 1>(a, groups, ngroups, team, st);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,
+                                     cudaStream_t st) {
+  if (!pair_cols_reg_supported(a.P, a.Q) || (a.n & 1)) return cudaErrorInvalidValue;
+  return dispatch_grp(a, groups, ngroups, team, st);
+}
+
+bool pair_cols_reg_supported(int P, int Q) {
+  if (P < 1 || P > kRegThreads) return false;
+  for (int q : kCodelets)
+    if (q == Q) return true;
+  return false;
+}
+
+template <int Q>
+cudaError_t launch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid, cudaStream_t st) {
+  cudaError_t e = allow_smem((const void*)k_pair_cols_reg<Q>, smem);
+  if (e != cudaSuccess) return e;
+  k_pair_cols_reg<Q><<<grid, kRegThreads, smem, st>>>(a, team);
+  return cudaGetLastError();
+}
+
+template <int I = 0>
+cudaError_t dispatch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid, cudaStream_t st) {
+  if constexpr (I < kNumCodelets) {
+    constexpr int Q = kCodelets[I];
+    if (a.Q == Q) return launch_reg<Q>(a, team, smem, grid, st);
+    return dispatch_reg<I + 1>(a, team, smem, grid, st);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
+  dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
+  if (pair_cols_reg_supported(a.P, a.Q)) {
+    const int team = a.P <= 32 ? 32 : (a.P <= 64 ? 64 : 128);
+    return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);
+  }
+  const size_t smem = pair_cols_smem(a.n, a.P, a.Q, a.box) + 16;
+  cudaError_t e = allow_smem((const void*)k_pair_cols, smem);
+  if (e != cudaSuccess) return e;
+  k_pair_cols<<<grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// =============================================================== pair rows ==
+// 16x16 threads, each a 6x6 register tile of the 96x96 output block; kx in
+// chunks of 32 staged through shared memory.
+constexpr int kRowTile = 96;
+constexpr int kRowK = 16;
+
+__global__ void __launch_bounds__(kThreads) k_pair_rows(PairRowsArgs a) {
+  __shared__ float2 gs[kRowK][kRowTile];
+  __shared__ float2 cs[kRowK][kRowTile];
+  const int p = blockIdx.x;
+  const int box = a.box;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const float2* G = a.G + (long long)p * a.H * box;
+  for (int yb0 = 0; yb0 < box; yb0 += kRowTile) {
+    for (int xb0 = 0; xb0 < box; xb0 += kRowTile) {
+      float acc[6][6];
+#pragma unroll
+      for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) acc[i][j] = 0.f;
+      for (int k0 = 0; k0 < a.H; k0 += kRowK) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kRowK * kRowTile; t += blockDim.x) {
+          const int kk = t / kRowTile, c = t - kk * kRowTile;
+          const int kx = k0 + kk;
+          const bool okk = kx < a.H;
+          gs[kk][c] = (okk && yb0 + c < box) ? G[(long long)kx * box + yb0 + c] : make_float2(0.f, 0.f);
+          cs[kk][c] = (okk && xb0 + c < box) ? a.cs[(long long)kx * box + xb0 + c] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < kRowK; kk++) {
+          float2 g[6], c[6];
+#pragma unroll
+          for (int i = 0; i < 6; i++) g[i] = gs[kk][ty + 16 * i];
+#pragma unroll
+          for (int j = 0; j < 6; j++) c[j] = cs[kk][tx + 16 * j];
+#pragma unroll
+          for (int i = 0; i < 6; i++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) acc[i][j] = fmaf(g[i].x, c[j].x, fmaf(-g[i].y, c[j].y, acc[i][j]));
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        const int yb = yb0 + ty + 16 * i;
+        if (yb >= box) continue;
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          const int xb = xb0 + tx + 16 * j;
+          if (xb < box) a.boxes[((long long)p * box + yb) * box + xb] = acc[i][j];
+        }
+      }
+    }
+  }
+}
+
+cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st) {
+  k_pair_rows<<<a.npairs, kThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace mc

@@ -1,0 +1,632 @@
+// Peak search, sum and adjoint kernels of libmc (sm_100a): integer peak and
+// x32 Fourier-upsampled sub-pixel peak (cufunc.cu:396-497), phase-shift-and-
+// accumulate with the inverse column FFT (cufunc.cu:372-393), final C2R rows
+// (DFAlign.cu:1287-1292), exact count sums and the objective of the gradient
+// refinement.
+#include <algorithm>
+
+#include "kcommon.cuh"
+
+namespace mc {
+
+// ==================================================================== peak ==
+constexpr int kSub = 16;
+constexpr int kPad = 512;
+constexpr int kUp = 32;
+
+struct PeakSmem {
+  double2 g1[kPad][8];     // column-inverse of the masked sub-box spectrum
+  double2 tw[kPad];        // exp(+2 pi i m / 512)
+  double2 s[kSub][9];      // masked 16x16 half spectrum
+  double2 rx[kSub][9];     // row transforms of the sub-box
+  double sub[kSub][kSub];
+  double rv[kThreads / 32];
+  int ri[kThreads / 32];
+  float fv[kThreads / 32];
+  int fi[kThreads / 32];
+  double f00;
+};
+
+size_t peak_smem() { return sizeof(PeakSmem); }
+
+// (v, i) beats (bv, bi): larger value, or equal value and earlier scan index.
+template <typename T>
+__device__ __forceinline__ bool better(T v, int i, T bv, int bi) {
+  return v > bv || (v == bv && i < bi);
+}
+
+__global__ void __launch_bounds__(kThreads) k_peak(PeakArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  PeakSmem& S = *reinterpret_cast<PeakSmem*>(smraw);
+  const int p = blockIdx.x;
+  const int box = a.box;
+  const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5;
+  const float* bm = a.boxes + (long long)p * box * box;
+  const int wnoise = a.nps - 1;
+  const int hb = box / 2;
+
+  // ---- integer peak (cufunc.cu:409-424): strict '>' from -1e9, y outer, x inner
+  float bv = -1e9f;
+  int bi = 0x7fffffff;
+  for (int idx = tid; idx < box * box; idx += nth) {
+    const int yy = idx / box, xx = idx - yy * box;
+    if (abs(xx - hb) <= wnoise && abs(yy - hb) <= wnoise) continue;
+    const float v = bm[idx];
+    if (v > -1e9f && better(v, idx, bv, bi)) {
+      bv = v;
+      bi = idx;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (better(ov, oi, bv, bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  if (lane == 0) {
+    S.fv[wid] = bv;
+    S.fi[wid] = bi;
+  }
+  __syncthreads();
+  bv = S.fv[0];
+  bi = S.fi[0];
+  for (int w = 1; w < nth / 32; w++)
+    if (better(S.fv[w], S.fi[w], bv, bi)) {
+      bv = S.fv[w];
+      bi = S.fi[w];
+    }
+  int ix = 0, iy = 0;
+  if (bi != 0x7fffffff) {
+    iy = bi / box;
+    ix = bi - iy * box;
+  }
+  int offx = ix - kSub / 2, offy = iy - kSub / 2;
+  if (offx + kSub > box) offx = box - kSub;
+  else if (offx < 0) offx = 0;
+  if (offy + kSub > box) offy = box - kSub;
+  else if (offy < 0) offy = 0;
+
+  // ---- sub-box, tables
+  for (int t = tid; t < kSub * kSub; t += nth) {
+    const int yy = t / kSub, xx = t - yy * kSub;
+    S.sub[yy][xx] = (double)bm[(offy + yy) * box + offx + xx];
+  }
+  for (int m = tid; m < kPad; m += nth) {
+    double sn, cn;
+    sincospi((double)m / (kPad / 2), &sn, &cn);
+    S.tw[m] = make_double2(cn, sn);
+  }
+  __syncthreads();
+  // R2C along x: rx[y][kx] = sum_x sub[y][x] exp(-2 pi i kx x / 16)
+  for (int t = tid; t < kSub * 9; t += nth) {
+    const int yy = t / 9, k = t - yy * 9;
+    double re = 0.0, im = 0.0;
+    for (int xx = 0; xx < kSub; xx++) {
+      const double2 w = S.tw[((k * xx) & (kSub - 1)) * (kPad / kSub)];
+      re += S.sub[yy][xx] * w.x;
+      im -= S.sub[yy][xx] * w.y;
+    }
+    S.rx[yy][k] = make_double2(re, im);
+  }
+  __syncthreads();
+  // along y, then the cosine mask (func.cpp:348-370)
+  for (int t = tid; t < kSub * 9; t += nth) {
+    const int j = t / 9, k = t - j * 9;
+    double re = 0.0, im = 0.0;
+    for (int yy = 0; yy < kSub; yy++) {
+      const double2 w = S.tw[((j * yy) & (kSub - 1)) * (kPad / kSub)];  // exp(+i..)
+      const double2 v = S.rx[yy][k];
+      re += v.x * w.x + v.y * w.y;  // v * conj(w)
+      im += v.y * w.x - v.x * w.y;
+    }
+    const double wt = a.w16[j * 9 + k];
+    S.s[j][k] = make_double2(re * wt, im * wt);
+  }
+  __syncthreads();
+  // zero-padded inverse along y: g1[Y][kx] = sum_j s[j][kx] exp(+2 pi i ky_j Y / 512)
+  for (int t = tid; t < kPad * 8; t += nth) {
+    const int Y = t >> 3, k = t & 7;
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < kSub; j++) {
+      const int ky = j < kSub / 2 ? j : j - kSub;
+      const double2 w = S.tw[(ky * Y) & (kPad - 1)];
+      const double2 v = S.s[j][k];
+      re += v.x * w.x - v.y * w.y;
+      im += v.x * w.y + v.y * w.x;
+    }
+    S.g1[Y][k] = make_double2(re, im);
+  }
+  __syncthreads();
+  // C2R along x on the 512 grid and the argmax (cufunc.cu:457-476)
+  const int ox = (hb - offx) * kUp, oy = (hb - offy) * kUp, wns = kUp * wnoise;
+  double best = -INFINITY;
+  int bidx = 0x7fffffff;
+  for (int X = tid; X < kPad; X += nth) {
+    double2 c[8];
+#pragma unroll
+    for (int k = 1; k < 8; k++) c[k] = S.tw[(k * X) & (kPad - 1)];
+    const bool xex = abs(X - ox) <= wns;
+    for (int Y = 0; Y < kPad; Y++) {
+      double f = S.g1[Y][0].x;
+#pragma unroll
+      for (int k = 1; k < 8; k++) {
+        const double2 g = S.g1[Y][k];
+        f += 2.0 * (g.x * c[k].x - g.y * c[k].y);
+      }
+      if (X == 0 && Y == 0) S.f00 = f;
+      if (xex && abs(Y - oy) <= wns) continue;
+      const int idx = Y * kPad + X;
+      if (better(f, idx, best, bidx)) {
+        best = f;
+        bidx = idx;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    if (better(ov, oi, best, bidx)) {
+      best = ov;
+      bidx = oi;
+    }
+  }
+  __syncthreads();
+  if (lane == 0) {
+    S.rv[wid] = best;
+    S.ri[wid] = bidx;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < nth / 32; w++)
+      if (better(S.rv[w], S.ri[w], best, bidx)) {
+        best = S.rv[w];
+        bidx = S.ri[w];
+      }
+    int sxp = 0, syp = 0;
+    double bestcc = S.f00;
+    if (bidx != 0x7fffffff && best > S.f00) {
+      sxp = bidx % kPad;
+      syp = bidx / kPad;
+      bestcc = best;
+    }
+    const float sx = (float)(offx + sxp / (double)kUp) - (float)hb;
+    const float sy = (float)(offy + syp / (double)kUp) - (float)hb;
+    a.shift[2 * p] = sx;
+    a.shift[2 * p + 1] = sy;
+    a.cc[p] = (float)(bestcc / a.n / a.n / kSub / kSub);
+    a.peak[2 * p] = ix;
+    a.peak[2 * p + 1] = iy;
+  }
+}
+
+cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st) {
+  const size_t smem = peak_smem();
+  cudaError_t e = allow_smem((const void*)k_peak, smem);
+  if (e != cudaSuccess) return e;
+  k_peak<<<a.npairs, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ============================================================== shift-sum ==
+size_t shift_sum_smem(int n, int nsum) {
+  return (size_t)3 * n * sizeof(float2) + (size_t)nsum * sizeof(float2);
+}
+
+__global__ void __launch_bounds__(kThreads) k_shift_sum(ShiftSumArgs a, const float2* __restrict__ ey) {
+  extern __shared__ float2 sm[];
+  const int n = a.n;
+  float2* acc = sm;
+  float2* b1 = sm + n;
+  float2* tw = sm + 2 * n;
+  float2* ex = sm + 3 * n;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int kx = blockIdx.x;
+  if (a.mode == 1) copy_table(tw, a.tw, n);
+  for (int f = tid; f < a.nsum; f += nth) {
+    double sn, cn;
+    // exp(+2 pi i sx kx / n), argument reduced in double
+    const double t = a.shifts[f].x * (double)kx / (double)n;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  for (int ky = tid; ky < n; ky += nth) acc[ky] = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int f = 0; f < a.nsum; f++) {
+    const float2* col = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
+    const float2 e = ex[f];
+    const float2* eyf = ey + (long long)f * n;
+    const bool ap = a.apply[f] != 0;
+    for (int ky = tid; ky < n; ky += nth) {
+      float2 v = col[ky];
+      if (ap) v = cmul(v, cmul(e, eyf[ky]));
+      acc[ky] = cadd(acc[ky], v);
+    }
+  }
+  __syncthreads();
+  if (a.mode == 0) {
+    for (int ky = tid; ky < n; ky += nth) a.out[(long long)kx * a.ld_out + ky] = acc[ky];
+    return;
+  }
+  float2* X = fft_run<true, false>(acc, b1, a.plan, 1, n, tw, tid, nth);
+  for (int y = tid; y < n; y += nth) a.out[(long long)y * a.ld_out + kx] = X[y];
+}
+
+// ============================================================ count sums ==
+// One thread per 4 consecutive crop pixels of a row; frames summed in int32
+// registers (exact: |pixel| <= 65535 and at most 2^15 frames).
+template <typename Px>
+__global__ void __launch_bounds__(kThreads) k_count_sum(CountSumArgs a) {
+  const int per_row = (a.nu + 3) / 4;
+  const long long total = (long long)per_row * a.nu;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(t / per_row);
+    const int x0 = (int)(t - (long long)y * per_row) * 4;
+    const int cnt = min(4, a.nu - x0);
+    int acc[4] = {0, 0, 0, 0};
+    const Px* base = reinterpret_cast<const Px*>(a.frames) + (long long)(a.offy + y) * a.nx + a.offx + x0;
+    for (int f = a.first; f <= a.last; f++) {
+      const Px* row = base + (long long)f * a.frame_pixels;
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (i < cnt) acc[i] += (int)row[i];
+    }
+    int* o = a.out + (long long)y * a.nu + x0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (i < cnt) o[i] = acc[i];
+  }
+}
+
+cudaError_t launch_count_sum(const CountSumArgs& a, cudaStream_t st) {
+  const long long items = (long long)((a.nu + 3) / 4) * a.nu;
+  const int grid = (int)std::min<long long>((items + kThreads - 1) / kThreads, 148LL * 16);
+  switch (a.mode) {
+    case 0: k_count_sum<int8_t><<<grid, kThreads, 0, st>>>(a); break;
+    case 1: k_count_sum<int16_t><<<grid, kThreads, 0, st>>>(a); break;
+    case 6: k_count_sum<uint16_t><<<grid, kThreads, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+__global__ void k_ramp(RampArgs a) {
+  const int f = blockIdx.y;
+  const double sy = a.shifts[f].y;
+  for (int ky = blockIdx.x * blockDim.x + threadIdx.x; ky < a.n; ky += gridDim.x * blockDim.x) {
+    const int y = ky < a.n / 2 ? ky : ky - a.n;
+    const double t = sy * (double)y / (double)a.n;
+    double sn, cn;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    a.ey[(long long)f * a.n + ky] = make_float2((float)cn, (float)sn);
+  }
+}
+
+// Two-level variant for columns of length N1*N2: each thread keeps the
+// running sums of its E = ceil(n/256) column elements in registers, so a
+// frame's column is requested with E independent loads per thread; the final
+// inverse along ky is the two-level transform.
+template <int N1, int N2>
+__global__ void __launch_bounds__(kThreads) k_shift_sum2l(ShiftSumArgs a, const float2* __restrict__ ey) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  constexpr int E = (N + kThreads - 1) / kThreads;
+  extern __shared__ float2 sm2l[];
+  float2* col = sm2l;         // accumulated column, then the step-A input
+  float2* ysm = sm2l + N;     // exchange buffer
+  float2* ex = sm2l + 2 * N;  // per-frame exp(+2 pi i sx kx / n)
+  const int tid = threadIdx.x;
+  const int kx = blockIdx.x;
+  for (int f = tid; f < a.nsum; f += kThreads) {
+    double sn, cn;
+    const double t = a.shifts[f].x * (double)kx / (double)N;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  __syncthreads();
+  float2 acc[E];
+#pragma unroll
+  for (int j = 0; j < E; j++) acc[j] = make_float2(0.f, 0.f);
+  for (int f = 0; f < a.nsum; f++) {
+    const float2* c = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
+    const float2* eyf = ey + (long long)f * N;
+    const float2 e = ex[f];
+    const bool ap = a.apply[f] != 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < N) {
+        float2 v = __ldg(c + ky);
+        if (ap) v = cmul(v, cmul(e, __ldg(eyf + ky)));
+        acc[j] = cadd(acc[j], v);
+      }
+    }
+  }
+  if (a.mode == 0) {
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < N) a.out[(long long)kx * a.ld_out + ky] = acc[j];
+    }
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int ky = tid + kThreads * j;
+    if (ky < N) col[ky] = acc[j];
+  }
+  __syncthreads();
+  float2* out = a.out;
+  const long long ld = a.ld_out;
+  TL::template run<true, false>(ysm, a.tw, [&](int i) { return col[i]; },
+                                [&](int k, float2 v) { out[(long long)k * ld + kx] = v; });
+}
+
+cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st) {
+  RampArgs r;
+  r.shifts = a.shifts;
+  r.nsum = a.nsum;
+  r.n = a.n;
+  r.ey = ey;
+  dim3 g((a.n + 255) / 256, a.nsum);
+  k_ramp<<<g, 256, 0, st>>>(r);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int n1 = 0, n2 = 0;
+  if (two_level_split(a.n, n1, n2)) {
+    const size_t smem2 = (size_t)(2 * a.n + a.nsum) * sizeof(float2);
+#define MC_TL_SUM(A, B)                                                                                       \
+  if (n1 == (A) && n2 == (B)) {                                                                               \
+    e = allow_smem((const void*)k_shift_sum2l<A, B>, smem2);                                                \
+    if (e != cudaSuccess) return e;                                                                           \
+    k_shift_sum2l<A, B><<<a.H, kThreads, smem2, st>>>(a, ey);                                                 \
+    return cudaGetLastError();                                                                                \
+  }
+    MC_TWO_LEVEL_LIST(MC_TL_SUM)
+#undef MC_TL_SUM
+  }
+  const size_t smem = shift_sum_smem(a.n, a.nsum);
+  e = allow_smem((const void*)k_shift_sum, smem);
+  if (e != cudaSuccess) return e;
+  k_shift_sum<<<a.H, kThreads, smem, st>>>(a, ey);
+  return cudaGetLastError();
+}
+
+// ================================================================ C2R rows ==
+size_t c2r_rows_smem(int n) { return (size_t)3 * n * sizeof(float2); }
+
+__global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.n, H = a.H, half = n / 2;
+  float2* b0 = sm;
+  float2* b1 = sm + n;
+  float2* tw = sm + 2 * n;
+  copy_table(tw, a.tw, n);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const float2* g0 = a.t2 + (long long)y0 * a.ld_t2;
+  const float2* g1 = a.t2 + (long long)y1 * a.ld_t2;
+  for (int k = tid; k < n; k += nth) {
+    float2 u, v;
+    if (k <= half) {
+      u = g0[k];
+      v = g1[k];
+      if (k == 0 || k == half) {  // C2R uses only the real part of DC and Nyquist
+        u.y = 0.f;
+        v.y = 0.f;
+      }
+    } else {
+      u = g0[n - k];
+      v = g1[n - k];
+      u.y = -u.y;
+      v.y = -v.y;
+    }
+    b0[k] = make_float2(u.x - v.y, u.y + v.x);  // u + i v
+  }
+  (void)H;
+  __syncthreads();
+  float2* X = fft_run<true, false>(b0, b1, a.plan, 1, n, tw, tid, nth);
+  for (int x = tid; x < n; x += nth) {
+    const float2 z = X[x];
+    a.image[(long long)y0 * n + x] = z.x * a.scale;
+    a.image[(long long)y1 * n + x] = z.y * a.scale;
+  }
+}
+
+// =============================================================== adjoint ==
+template <int E>
+__global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
+  extern __shared__ double smo[];
+  double* red = smo;                                                   // [warps][5]
+  float2* ex = reinterpret_cast<float2*>(smo + (kThreads / 32) * 5);  // [nframes]
+  const int n = a.n, half = n / 2;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int kx = blockIdx.x;
+  const float h = (kx == 0 || kx == half) ? 1.f : 2.f;
+  const float ox = 6.283185307179586f * (float)kx / (float)n;
+  for (int f = tid; f < a.nframes; f += kThreads) {
+    double sn, cn;
+    const double t = a.shifts[f].x * (double)kx / (double)n;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    ex[f] = make_float2((float)cn, (float)sn);
+  }
+  float2 s[E];
+  float hw[E], oy[E];
+  double jsum = 0.0;
+  const float2* Scol = a.S + (long long)kx * a.ldn;
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int ky = tid + kThreads * j;
+    if (ky < n) {
+      const int y = ky < half ? ky : ky - n;
+      s[j] = __ldg(Scol + ky);
+      hw[j] = h * expf(a.mbf * (float)(kx * kx + y * y));
+      oy[j] = 6.283185307179586f * (float)y / (float)n;
+      jsum += (double)(hw[j] * (s[j].x * s[j].x + s[j].y * s[j].y));
+    } else {
+      s[j] = make_float2(0.f, 0.f);
+      hw[j] = 0.f;
+      oy[j] = 0.f;
+    }
+  }
+  __syncthreads();
+  // J partial
+  for (int o = 16; o > 0; o >>= 1) jsum += __shfl_xor_sync(0xffffffffu, jsum, o);
+  if (lane == 0) red[wid * 5] = jsum;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; w++) t += red[w * 5];
+    a.partialJ[kx] = t;
+  }
+  __syncthreads();
+  for (int f = 0; f < a.nframes; f++) {
+    const float2* c = a.spec + (long long)f * a.stride + (long long)kx * a.ldn;
+    const float2* eyf = a.ey + (long long)f * n;
+    const float2 e = ex[f];
+    double gx = 0, gy = 0, hxx = 0, hxy = 0, hyy = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int ky = tid + kThreads * j;
+      if (ky < n) {
+        const float2 P = cmul(__ldg(c + ky), cmul(e, __ldg(eyf + ky)));
+        const float2 d = csub(s[j], P);
+        const float2 u = cmulc(P, d);  // conj(d) * P
+        const double wi = (double)(hw[j] * u.y), wr = (double)(hw[j] * u.x);
+        const double y = (double)oy[j];
+        gx += wi;
+        gy += wi * y;
+        hxx += wr;
+        hxy += wr * y;
+        hyy += wr * y * y;
+      }
+    }
+    // omega_x is constant over the column: apply it after the sums
+    double v[5] = {gx * ox, gy, hxx * ox * ox, hxy * ox, hyy};
+#pragma unroll
+    for (int q = 0; q < 5; q++)
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 5; q++) red[wid * 5 + q] = v[q];
+    __syncthreads();
+    if (tid < 5) {
+      double t = 0.0;
+      for (int w = 0; w < kThreads / 32; w++) t += red[w * 5 + tid];
+      a.partial[((long long)kx * a.nframes + f) * 5 + tid] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Column partials -> per-frame totals in a fixed order (deterministic).
+__global__ void k_objective_reduce(ObjectiveArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nv = a.nframes * 5;
+  if (t < nv) {
+    double acc = 0.0;
+    for (int kx = 0; kx < a.H; kx++) acc += a.partial[(long long)kx * nv + t];
+    a.out[t] = -2.0 * acc;
+  } else if (t == nv) {
+    double acc = 0.0;
+    for (int kx = 0; kx < a.H; kx++) acc += a.partialJ[kx];
+    a.out[nv] = acc;
+  }
+}
+
+cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st) {
+  RampArgs r;
+  r.shifts = shifts;
+  r.nsum = nsum;
+  r.n = n;
+  r.ey = ey;
+  dim3 g((n + 255) / 256, nsum);
+  k_ramp<<<g, 256, 0, st>>>(r);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (kThreads / 32) * 5 + sizeof(float2) * (size_t)a.nframes;
+  cudaError_t e;
+  const int E = (a.n + kThreads - 1) / kThreads;
+  if (E <= 8) {
+    e = allow_smem((const void*)k_objective<8>, smem);
+    if (e != cudaSuccess) return e;
+    k_objective<8><<<a.H, kThreads, smem, st>>>(a);
+  } else if (E <= 16) {
+    e = allow_smem((const void*)k_objective<16>, smem);
+    if (e != cudaSuccess) return e;
+    k_objective<16><<<a.H, kThreads, smem, st>>>(a);
+  } else if (E <= 36) {
+    e = allow_smem((const void*)k_objective<36>, smem);
+    if (e != cudaSuccess) return e;
+    k_objective<36><<<a.H, kThreads, smem, st>>>(a);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nv = a.nframes * 5 + 1;
+  k_objective_reduce<<<(nv + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Two-level variant: rows y, y+1 packed as Z = G_y + i G_{y+1} with the
+// Hermitian extension formed in the load (real DC and Nyquist).
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T) k_c2r_rows2l(C2rRowsArgs a) {
+  using TL = TwoLevel<N1, N2>;
+  constexpr int N = TL::N;
+  __shared__ float2 ysm[N];
+  const int y0 = 2 * blockIdx.x, y1 = y0 + 1;
+  const float2* g0 = a.t2 + (long long)y0 * a.ld_t2;
+  const float2* g1 = a.t2 + (long long)y1 * a.ld_t2;
+  float* i0 = a.image + (long long)y0 * N;
+  float* i1 = a.image + (long long)y1 * N;
+  const float sc = a.scale;
+  TL::template run<true, false>(
+      ysm, a.tw,
+      [&](int k) {
+        float2 u, v;
+        if (k <= N / 2) {
+          u = __ldg(g0 + k);
+          v = __ldg(g1 + k);
+          if (k == 0 || k == N / 2) {
+            u.y = 0.f;
+            v.y = 0.f;
+          }
+        } else {
+          u = __ldg(g0 + N - k);
+          v = __ldg(g1 + N - k);
+          u.y = -u.y;
+          v.y = -v.y;
+        }
+        return make_float2(u.x - v.y, u.y + v.x);
+      },
+      [&](int x, float2 z) {
+        i0[x] = z.x * sc;
+        i1[x] = z.y * sc;
+      });
+}
+
+cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st) {
+  int n1 = 0, n2 = 0;
+  if (two_level_split(a.n, n1, n2)) {
+#define MC_TL_C2R(A, B)                                              \
+  if (n1 == (A) && n2 == (B)) {                                      \
+    k_c2r_rows2l<A, B><<<a.n / 2, TwoLevel<A, B>::T, 0, st>>>(a);    \
+    return cudaGetLastError();                                       \
+  }
+    MC_TWO_LEVEL_LIST(MC_TL_C2R)
+#undef MC_TL_C2R
+  }
+  const size_t smem = c2r_rows_smem(a.n);
+  cudaError_t e = allow_smem((const void*)k_c2r_rows, smem);
+  if (e != cudaSuccess) return e;
+  k_c2r_rows<<<a.n / 2, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace mc
