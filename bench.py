@@ -31,6 +31,14 @@ UNIT = "frames/s"
 WORKLOAD = ("c2: 40 frames 3838x3710 uint8 (MRC mode 0), mean 1.2 e/px/frame, RW 0.5 + 0.3 px/frame drift; "
             "-bin 1 -fod 7 -bft 150 -pbx 96 -atm 1 -itr 0; crop 3710^2, 378 pairs")
 FALLBACK_HBM_GBS = 6650.0
+WORKLOADS_TEXT = {
+    "c1": "c1: 16 frames 1024x1024 float32 (MRC mode 2), mean 1.5 e/px/frame, 0.4 px/frame linear + RW 0.3; "
+          "-bin 1 -fod 2 -bft 150 -pbx 96 -nps 0; 55 pairs",
+    "c3": "c3: 50 frames 7676x7420 uint8, mean 0.3 e/px/frame, RW 0.5 + 0.3 px/frame; -bin 2 (crop 7420, "
+          "Fourier crop to 3710), -fod 2; 378 pairs",
+    "c4": "c4: 60 frames 4096x4096 float32, mean 1.0 e/px/frame, RW 0.8 + sinusoid 1.5 px period 20; -fod 2, "
+          "-itr 3 -ith 0.01, gradient refinement (-ref 1); 528 pairs",
+}
 
 
 def c2_params(api):
@@ -60,40 +68,63 @@ def committed_traffic(kernel):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region.
+
+    The sampler starts before the region and waits for its first sample (the
+    tool takes a moment to start); samples are stamped on arrival and only
+    those inside the region count (the first one after its start when the
+    region is shorter than the sampling period)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=20):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
+        self.samples = []       # (host time, line)
+        self.t0 = self.t1 = None
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.perf_counter(), line))
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._reader, daemon=True)
+            self.thread.start()
+            deadline = time.perf_counter() + 10.0
+            while not self.samples and time.perf_counter() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        self.t1 = time.perf_counter()
         if self.proc:
+            time.sleep(2.0 * self.period_ms / 1000.0)   # one more sample after the region
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.thread.join(timeout=5)
 
     def summary(self):
+        inside = [l for t, l in self.samples if self.t0 <= t <= self.t1]
+        if not inside:
+            inside = [l for t, l in self.samples if t >= self.t0][:1]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in inside:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue
@@ -180,15 +211,23 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    nx, ny, nz = 3838, 3710, args.frames
-    frames, truth = synth.make_movie_torch(nx, ny, nz, mean=1.2, seed=args.seed + rank, dtype="u8",
-                                           kind="linear", speed=0.3, rw_sigma=0.5, device=f"cuda:{local}")
-    host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
+    w = dict(synth.WORKLOADS[args.workload])
+    flags = dict(w.pop("flags"))
+    if args.workload == "c4":
+        flags["refine"] = 1            # the gradient refinement after the iterations
+    nx, ny = w["nx"], w["ny"]
+    nz = args.frames or w["nframes"]
+    mode = 0 if w["dtype"] == "u8" else 2
+    frames, truth = synth.make_movie_torch(nx, ny, nz, mean=w["mean"], seed=args.seed + rank, dtype=w["dtype"],
+                                           kind=w["kind"], speed=w.get("speed", 0.4),
+                                           rw_sigma=w.get("rw_sigma", 0.3), amp=w.get("amp", 1.5),
+                                           period=w.get("period", 20.0), device=f"cuda:{local}")
+    host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)
     host.copy_(frames)
-    p = c2_params(api)
+    p = c2_params(api) if args.workload == "c2" else api.Params(**flags)
     p.GPUNum = local
     p = api.verify_params(p, nz)
-    plan = api.Plan(p, nx, ny, nz, 0)
+    plan = api.Plan(p, nx, ny, nz, mode)
     stream = torch.cuda.ExternalStream(plan.stream, device=f"cuda:{local}")
     image = torch.empty((plan.nsam, plan.nsam), dtype=torch.float32, pin_memory=True)
     image_np = image.numpy()
@@ -229,7 +268,7 @@ def run_ours(args):
     # one movie's serial tail (peak search, solve, sum) with the next one's
     # transforms
     batch = api.Batch(local, 2)
-    dev = [{"params": p, "nx": nx, "ny": ny, "nz": nz, "mode": 0, "device_ptr": frames.data_ptr()}
+    dev = [{"params": p, "nx": nx, "ny": ny, "nz": nz, "mode": mode, "device_ptr": frames.data_ptr()}
            for _ in range(args.steps)]
     for _ in range(max(1, args.warmup // 2)):
         batch.run(dev[:2])
@@ -253,7 +292,7 @@ def run_ours(args):
     # every step uploads its movie and reads its image back
     images = [torch.empty((plan.nsam, plan.nsam), dtype=torch.float32, pin_memory=True).numpy()
               for _ in range(args.steps)]
-    mv = [{"params": p, "nx": nx, "ny": ny, "nz": nz, "mode": 0, "frames": host_np, "image": im}
+    mv = [{"params": p, "nx": nx, "ny": ny, "nz": nz, "mode": mode, "frames": host_np, "image": im}
           for im in images]
     batch.run(mv[:2])
     e2e_ms, res = timed(lambda: batch.run(mv))
@@ -276,12 +315,21 @@ def run_ours(args):
         peak, peak_kind = measured_peak()
         achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": committed_traffic(dom), "peak_source": peak_kind,
-                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "frac": achieved / peak, "traffic": committed_traffic(dom) if args.workload == "c2" else None,
+                "peak_source": peak_kind, "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms}
+        # compulsory bytes of a whole movie: every frame read once and its
+        # spectrum written once, every spectrum read by the pair stage and by
+        # the sum (twice more per realignment iteration), the image written
+        S = plan.nsam * (plan.nsam // 2 + 1) * 8
+        raw = host[0].numel() * host.element_size()
+        b_movie = nz * (raw + 3 * S) + 2 * p.iter * nz * S + 4 * plan.nsam ** 2
+        movie_gbs = b_movie / (ms_max / args.steps / 1000.0) / 1e9
+        metric = METRIC if args.workload == "c2" else f"aligned frames/s at {nx}x{ny}x{nz}"
+        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD if nz == 40 else f"profiling case: {nz} frames, else as c2",
+                "config": {"workload": (WORKLOAD if nz == 40 else f"profiling case: {nz} frames, else as c2")
+                           if args.workload == "c2" else WORKLOADS_TEXT[args.workload],
                            "nsam": plan.nsam, "pairs": plan.npairs,
                            "l2": "inputs larger than L2 (570 MB frames, 2.2 GB spectra per movie), no flush",
                            "parallelism": f"replicas x{world}"},
@@ -294,12 +342,14 @@ def run_ours(args):
                 "latency_p50_ms": _pct(dev_lat, 50), "latency_p99_ms": _pct(dev_lat, 99),
                 "single_plan_value": nz * args.steps * world / (single_ms / 1000.0),
                 "gpu_launches": launches, "roofline": roof,
+                "movie_roofline": {"bytes_per_movie": b_movie, "achieved": movie_gbs, "peak": peak, "unit": "GB/s",
+                                   "frac": movie_gbs / peak},
                 "kernels": {k: {"ms_per_step": v["ms"] / prof_steps, "launches": v["launches"] // prof_steps,
                                 "GBps": (v["bytes"] / (v["ms"] / 1000.0) / 1e9) if v["ms"] > 0 else None}
                             for k, v in stats.items()},
                 "shift_rmse_vs_truth_px": truth_rmse,
                 "clocks": clk.summary()}
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.workload == "c2":
             v, parts = oracle_sample(seed=args.seed)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                                     "sample": "FP64 oracle, one frame forward + one pair + one frame sum at "
@@ -418,11 +468,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--frames", type=int, default=40,
-                    help="movie length; 40 is the benchmark workload, fewer only for profiling captures")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="movie length (0: the workload's; fewer only for profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
-                    help="c2: the 40-frame 3838x3710 movie (headline); c5: the 32-movie batch")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2: the 40-frame 3838x3710 movie (headline); c1 1024^2x16 f32; c3 7676x7420x50 "
+                         "uint8 -bin 2; c4 4096^2x60 f32 with 3 realignment iterations and the gradient "
+                         "refinement; c5: the 32-movie batch")
     ap.add_argument("--lanes", type=int, default=2, help="batch lanes (c5 workload)")
     args = ap.parse_args()
     if args.impl == "reference":
