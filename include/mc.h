@@ -219,6 +219,19 @@ int mc_plan_raw_sum(mc_plan* plan, float* image_host);
 int mc_plan_sum_to(mc_plan* plan, int last_frame, float* image_host);
 int mc_plan_corrected_frame(mc_plan* plan, int frame, float* image_host);
 
+/* Quick-look displays of -dsp 1 (DFAlign.cu:73-178, 841-849, 1270-1286;
+ * func.cpp:372-556): MC_QUICKLOOK_DIM^2 int16 pixels with values 0..255 (the
+ * reference writes them as mode-1 MRC files in dosef_quick/).
+ *   which 0: "RawFFT"  log(1 + 1e-4 |unaligned sum spectrum|) as the centred
+ *            modulus image, Fourier-binned to 400 x 400;
+ *   which 1: "CorrSum" the corrected sum, Fourier-binned to 400 x 400;
+ *   which 2: "CorrFFT" as 0 for the corrected sum.
+ * Contrast: 0.5 % histogram tails clipped, then linear to 0..255.  Needs a
+ * binned side of at least 400; 0 needs mc_plan_forward, 1 and 2 a finished
+ * sum (mc_plan_sum or mc_plan_run). */
+#define MC_QUICKLOOK_DIM 400
+int mc_plan_quicklook(mc_plan* plan, int which, int16_t* out);
+
 /* No counterpart in the reference (its raw sums are FP32 spectra): the
  * exact integer sum of the raw pixels of frames nStartSum..nEndSum over the
  * square crop, nsam_unbin*nsam_unbin int32 values (host), pixels decoded as

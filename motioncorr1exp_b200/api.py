@@ -243,6 +243,14 @@ class Plan:
         L.check(self._lib.mc_plan_corrected_frame(self._h, frame, _ptr(img)))
         return img
 
+    QUICKLOOK = {"raw_fft": 0, "corr_sum": 1, "corr_fft": 2}
+
+    def quicklook(self, which: str) -> np.ndarray:
+        """-dsp 1 display (400 x 400 int16, 0..255): "raw_fft", "corr_sum" or "corr_fft"."""
+        out = np.empty((400, 400), dtype=np.int16)
+        L.check(self._lib.mc_plan_quicklook(self._h, self.QUICKLOOK[which], _ptr(out)))
+        return out
+
     def count_sum(self) -> np.ndarray:
         nu = self.info["nsam_unbin"]
         out = np.empty((nu, nu), dtype=np.int32)

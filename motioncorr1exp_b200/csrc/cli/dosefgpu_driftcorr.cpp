@@ -477,6 +477,22 @@ int run_align(Options& o) {
       for (const auto& l : sum2_lines) text_output(l.c_str());
   }
   g_held.clear();
+  // -dsp 1: the three 400 x 400 displays in ./dosef_quick
+  // (dosefgpu_driftcorr.cpp:484-512; DFAlign.cu:73-178, 841-849, 1270-1286)
+  if (o.bSaveDisp) {
+    struct stat st;
+    if (stat("dosef_quick", &st) != 0) mkdir("dosef_quick", 0755);
+    std::vector<int16_t> disp((size_t)MC_QUICKLOOK_DIM * MC_QUICKLOOK_DIM);
+    const std::string* names[3] = {&o.dispRawFFT, &o.dispCorrSum, &o.dispCorrFFT};
+    for (int which = 0; which < 3; which++) {
+      rc = mc_plan_quicklook(plan, which, disp.data());
+      if (rc == MC_OK && write_mrc_short(names[which]->c_str(), disp.data(), MC_QUICKLOOK_DIM, MC_QUICKLOOK_DIM, 1))
+        continue;
+      snprintf(str, sizeof(str), "Warning: display %s not written (%s)\n", names[which]->c_str(),
+               rc == MC_OK ? "write" : mc_last_error());
+      text_output(str);
+    }
+  }
   const std::string fnsum = o.bSaveSubAreaCorrSum ? sub_name(o.fnAlignsum) : o.fnAlignsum;
   MrcHeader oh;
   if (!write_mrc_float(fnsum.c_str(), image.data(), info.nsam, info.nsam, 1, &oh)) {

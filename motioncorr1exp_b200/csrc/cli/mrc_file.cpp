@@ -128,6 +128,36 @@ bool write_mrc_float(const char* path, const float* data, int nx, int ny, int nz
   return ok;
 }
 
+bool write_mrc_short(const char* path, const int16_t* data, int nx, int ny, int nz) {
+  MrcHeader h;
+  std::memset(&h, 0, sizeof(h));
+  h.nx = nx;
+  h.ny = ny;
+  h.nz = nz;
+  h.mode = 1;
+  h.cellb[0] = h.cellb[1] = h.cellb[2] = 90;
+  h.mapc = 1;
+  h.mapr = 2;
+  h.maps = 3;
+  const size_t size = (size_t)nx * ny * nz;
+  int16_t mn = size ? data[0] : 0, mx = mn;
+  double mean = 0;
+  for (size_t i = 0; i < size; i++) {
+    if (mn > data[i]) mn = data[i];
+    if (mx < data[i]) mx = data[i];
+    mean += data[i];
+  }
+  if (size) mean /= (double)size;
+  h.dmin = mn;
+  h.dmax = mx;
+  h.dmean = (float)mean;
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return false;
+  bool ok = fwrite(&h, 1, 1024, fp) == 1024;
+  ok = ok && fwrite(data, sizeof(int16_t), size, fp) == size;
+  return (fclose(fp) == 0) && ok;
+}
+
 MrcStackWriter::~MrcStackWriter() { close(); }
 
 bool MrcStackWriter::open(const char* path, int nx, int ny, int nz) {

@@ -62,6 +62,10 @@ bool starts_with_tiff(const char* path);
 // createMRC(float*) semantics; fills dmin/dmax/dmean; returns false on I/O error.
 bool write_mrc_float(const char* path, const float* data, int nx, int ny, int nz, MrcHeader* out_header);
 
+// createMRC(short*) semantics (mrc.cpp:276-307): mode 1, the same geometry
+// fields, dmin/dmax/dmean of the shorts; returns false on I/O error.
+bool write_mrc_short(const char* path, const int16_t* data, int nx, int ny, int nz);
+
 // Corrected-stack writer: the header a default MRC() object carries
 // (mrc.cpp:5-16: mode 2, cellb 90, mapc/mapr/maps 1/2/3, statistics 0) with
 // nx, ny, nz set and written by updateHeader (mrc.cpp:237-241); frame n at

@@ -210,6 +210,21 @@ cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 
+// ------------------------------------------------------------ quick-look --
+// Displays of -dsp 1 (DFAlign.cu:73-178, 841-849, 1270-1286; func.cpp:459-556).
+// Log modulus of a half spectrum spec[kx*ldn + ky] laid out as the centred
+// n x n display image of FFTModulusToDispBuf: column c >= n/2 holds kx = c - n/2,
+// row r holds ky = r + n/2 (r < n/2) or r - n/2; the left half mirrors the
+// right through the centre, row 0's left half repeats row 1's.
+cudaError_t launch_ql_logmod(const float2* spec, int ldn, int n, float scale, float* img, cudaStream_t st);
+// Fourier crop of a half spectrum [kx][ky] (ld ldn, side n) to side d:
+// out[kx*d + k] for kx <= d/2, k < d/2 from ky = k, else from ky = n - d + k.
+cudaError_t launch_ql_crop(const float2* spec, int ldn, int n, int d, float2* out, cudaStream_t st);
+// Unnormalised C2R of a side-d half spectrum in[kx*d + ky] (kx <= d/2):
+// img[y*d + x] = scale * sum_kx h(kx) Re(exp(+2 pi i kx x/d) sum_ky in exp(+2 pi i ky y/d)),
+// h = 1 at kx = 0, d/2, else 2; tmp holds (d/2+1) x d complex.
+cudaError_t launch_ql_c2r(const float2* in, int d, float scale, float2* tmp, float* img, cudaStream_t st);
+
 // Sets the calling thread's mc_last_error() text; returns `code`.
 int record_error(int code, const char* text);
 

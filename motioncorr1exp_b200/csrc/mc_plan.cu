@@ -276,6 +276,8 @@ struct mc_plan {
   // device memory
   void* d_frames = nullptr;
   int* d_count = nullptr;  // exact count sum (allocated on first use)
+  float2* d_ql = nullptr;  // quick-look: side-400 spectrum + C2R scratch (first use)
+  float* d_qlimg = nullptr;
   const void* frames_src = nullptr;  // bound caller device frames (mc_plan_bind_frames_device) or null
   float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
   float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
@@ -1530,6 +1532,132 @@ int mc_plan_corrected_frame(mc_plan* pl, int frame, float* image_host) {
   const std::vector<int> apply{(k == pl->sum_first && !pl->p.bAlignToMid) ? 0 : 1};
   CKR(run_shift_sum(pl, frames, sh, apply, 1));
   return image_out(pl, image_host);
+}
+
+// Contrast mapping of the displays (histMinMax with a 0.5 % tail on each
+// side over 400 bins, then buf2DispShort's linear map to 0..255;
+// func.cpp:372-455), in the reference's float arithmetic.
+static void display_short(const float* buf, int size, int16_t* disp) {
+  float mn = 1e20f, mx = -1e20f;
+  for (int i = 0; i < size; i++) {
+    if (buf[i] < mn) mn = buf[i];
+    if (buf[i] > mx) mx = buf[i];
+  }
+  std::fill(disp, disp + size, (int16_t)0);
+  if (mn >= mx) return;
+  const int nbin = 400;
+  std::vector<int> hist(nbin, 0);
+  const float step = (mx - mn) / nbin;
+  for (int i = 0; i < size; i++) {
+    int id = (int)((buf[i] - mn) / step);
+    if (id >= nbin) id = nbin - 1;
+    hist[id]++;
+  }
+  const int percent = (int)(size * 0.005f);
+  int count = 0;
+  for (int i = 0; i < nbin; i++) {
+    count += hist[i];
+    if (count > percent) {
+      mn += i * step;
+      break;
+    }
+  }
+  count = 0;
+  for (int i = nbin - 1; i > 0; i--) {
+    count += hist[i];
+    if (count > percent) {
+      mx -= (nbin - 1 - i) * step;
+      break;
+    }
+  }
+  if (mn >= mx) return;
+  const float scale = 255.0f / (mx - mn);
+  for (int i = 0; i < size; i++) {
+    if (buf[i] <= mn) disp[i] = 0;
+    else if (buf[i] >= mx) disp[i] = 255;
+    else disp[i] = (int16_t)((buf[i] - mn) * scale);
+  }
+}
+
+int mc_plan_quicklook(mc_plan* pl, int which, int16_t* out) {
+  constexpr int D = MC_QUICKLOOK_DIM;
+  if (!pl || !out) return set_err(MC_E_ARG, "null argument");
+  if (which < 0 || which > 2) return set_err(MC_E_ARG, "quick-look kind %d outside [0, 2]", which);
+  const int n = pl->n;
+  if (n < D) return set_err(MC_E_SIZE, "quick-look displays need a binned side of at least %d (got %d)", D, n);
+  CK(cudaSetDevice(pl->device));
+  // the sum spectrum into d_sum: unaligned (raw FFT) or corrected
+  std::vector<int> frames, apply;
+  std::vector<cplx> sh;
+  if (which == 0) {
+    if (!pl->have_forward) return set_err(MC_E_STATE, "quick-look before forward");
+    int nss, nes, lim;
+    sum_range(pl, &nss, &nes, &lim);
+    for (int k = nss; k <= nes; k++) {
+      frames.push_back(k);
+      sh.push_back(cplx(0, 0));
+      apply.push_back(0);
+    }
+  } else {
+    if (!pl->have_sum) return set_err(MC_E_STATE, "quick-look of the corrected sum before the sum");
+    for (int k = pl->sum_first; k <= pl->sum_last; k++) {
+      frames.push_back(k);
+      sh.push_back(pl->sum_shift[k]);
+      apply.push_back((k == pl->sum_first && !pl->p.bAlignToMid) ? 0 : 1);
+    }
+  }
+  CKR(run_shift_sum(pl, frames, sh, apply, 0));
+  if (!pl->d_ql) {
+    CKR(pl->alloc(&pl->d_ql, sizeof(float2) * 2 * (size_t)(D / 2 + 1) * D));
+    CKR(pl->alloc(&pl->d_qlimg, sizeof(float) * (size_t)D * D));
+  }
+  float2* spec = pl->d_ql;
+  float2* tmp = pl->d_ql + (size_t)(D / 2 + 1) * D;
+  float scale = 1.0f;
+  if (which == 1) {
+    // GPUMemBinD2H + ifft2d of the sum (DFAlign.cu:1278-1282, 73-88)
+    CK(mc::launch_ql_crop(pl->d_sum, pl->ldn, n, D, spec, pl->st));
+  } else {
+    // log modulus as the centred display image (cufunc.cu:178-188,
+    // func.cpp:459-489), its R2C, Fourier crop to D, C2R / D^2
+    // (BinFFTDispBufToChar, func.cpp:524-556)
+    float* img = pl->d_image;
+    CK(mc::launch_ql_logmod(pl->d_sum, pl->ldn, n, 1.0e-4f, img, pl->st));
+    const int hk = D / 2 + 1;
+    const int ldt = (int)round_up(n, 2);
+    mc::FwdRowsArgs a{};
+    a.frame = img;
+    a.mode = 2;
+    a.nx = n;
+    a.ny = n;
+    a.nu = n;
+    a.hk = hk;
+    a.outA = pl->d_T2;
+    a.ldt = ldt;
+    a.plan = pl->plan_n;
+    a.tw = pl->d_tw_n;
+    CK(mc::launch_fwd_rows(a, pl->st));
+    mc::RowsFftArgs c{};
+    c.in = pl->d_T2;
+    c.ld_in = ldt;
+    c.out = spec;
+    c.ld_out = D;
+    c.nrows = hk;
+    c.n_out = D;
+    c.keep_lo = D / 2;
+    c.scale = 1.f;
+    c.plan = pl->plan_n;
+    c.tw = pl->d_tw_n;
+    CK(mc::launch_rows_fft(c, false, 1, pl->st));
+    scale = 1.0f / ((float)D * D);
+  }
+  CK(mc::launch_ql_c2r(spec, D, scale, tmp, pl->d_qlimg, pl->st));
+  std::vector<float> h((size_t)D * D);
+  CK(cudaMemcpyAsync(h.data(), pl->d_qlimg, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  CKR(pl->collect());
+  display_short(h.data(), D * D, out);
+  return MC_OK;
 }
 
 int mc_plan_count_sum(mc_plan* pl, int32_t* host) {

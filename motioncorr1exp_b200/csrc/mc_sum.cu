@@ -438,9 +438,11 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
 // =============================================================== adjoint ==
 template <int E>
 __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
+  constexpr int W = kThreads / 32;
   extern __shared__ double smo[];
-  double* red = smo;                                                   // [warps][5]
-  float2* ex = reinterpret_cast<float2*>(smo + (kThreads / 32) * 5);  // [nframes]
+  double* red = smo;                                                          // [warps][5] (J)
+  double* fred = smo + W * 5;                                                 // [nframes][warps][5]
+  float2* ex = reinterpret_cast<float2*>(fred + (size_t)a.nframes * W * 5);  // [nframes]
   const int n = a.n, half = n / 2;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int kx = blockIdx.x;
@@ -482,6 +484,7 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
     a.partialJ[kx] = t;
   }
   __syncthreads();
+  // per frame: warp sums into shared memory, one barrier for all frames
   for (int f = 0; f < a.nframes; f++) {
     const float2* c = a.spec + (long long)f * a.stride + (long long)kx * a.ldn;
     const float2* eyf = a.ey + (long long)f * n;
@@ -510,14 +513,14 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
       for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
     if (lane == 0)
 #pragma unroll
-      for (int q = 0; q < 5; q++) red[wid * 5 + q] = v[q];
-    __syncthreads();
-    if (tid < 5) {
-      double t = 0.0;
-      for (int w = 0; w < kThreads / 32; w++) t += red[w * 5 + tid];
-      a.partial[((long long)kx * a.nframes + f) * 5 + tid] = t;
-    }
-    __syncthreads();
+      for (int q = 0; q < 5; q++) fred[((size_t)f * W + wid) * 5 + q] = v[q];
+  }
+  __syncthreads();
+  for (int i = tid; i < a.nframes * 5; i += kThreads) {
+    const int f = i / 5, q = i - f * 5;
+    double t = 0.0;
+    for (int w = 0; w < W; w++) t += fred[((size_t)f * W + w) * 5 + q];
+    a.partial[((long long)kx * a.nframes + f) * 5 + q] = t;
   }
 }
 
@@ -548,7 +551,9 @@ cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cuda
 }
 
 cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
-  const size_t smem = sizeof(double) * (kThreads / 32) * 5 + sizeof(float2) * (size_t)a.nframes;
+  const size_t smem = sizeof(double) * (kThreads / 32) * 5 * (1 + (size_t)a.nframes) +
+                      sizeof(float2) * (size_t)a.nframes;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;  // more than ~600 frames
   cudaError_t e;
   const int E = (a.n + kThreads - 1) / kThreads;
   if (E <= 8) {
@@ -626,6 +631,106 @@ cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st) {
   cudaError_t e = allow_smem((const void*)k_c2r_rows, smem);
   if (e != cudaSuccess) return e;
   k_c2r_rows<<<a.n / 2, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ============================================================= quick-look ==
+__global__ void k_ql_logmod(const float2* __restrict__ spec, int ldn, int n, float scale, float* __restrict__ img) {
+  const int h = n / 2;
+  const long long total = (long long)n * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int r = (int)(t / n), c = (int)(t - (long long)r * n);
+    if (c < h) {  // mirrored half (FFTModulusToDispBuf), row 0 repeats row 1
+      if (r == 0) r = 1;
+      r = n - r;
+      c = n - c;
+    }
+    const int kx = c - h;
+    const int ky = r >= h ? r - h : r + h;
+    const float2 v = spec[(long long)kx * ldn + ky];
+    img[t] = logf(1.f + sqrtf(v.x * v.x + v.y * v.y) * scale);
+  }
+}
+
+__global__ void k_ql_crop(const float2* __restrict__ spec, int ldn, int n, int d, float2* __restrict__ out) {
+  const int hd = d / 2;
+  const int total = (hd + 1) * d;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int kx = t / d, k = t - kx * d;
+    const int ky = k < hd ? k : n - d + k;
+    out[t] = spec[(long long)kx * ldn + ky];
+  }
+}
+
+// exp(+2 pi i m / d), m < d, into shared memory (one table per block)
+__device__ __forceinline__ void ql_table(float2* tw, int d) {
+  for (int m = threadIdx.x; m < d; m += blockDim.x) {
+    double sn, cn;
+    sincospi(2.0 * (double)m / (double)d, &sn, &cn);
+    tw[m] = make_float2((float)cn, (float)sn);
+  }
+  __syncthreads();
+}
+
+// pass 1: tmp[kx][y] = sum_ky in[kx][ky] exp(+2 pi i ky y / d)
+__global__ void k_ql_c2r_cols(const float2* __restrict__ in, int d, float2* __restrict__ tmp) {
+  extern __shared__ float2 qtw[];
+  ql_table(qtw, d);
+  const int kx = blockIdx.x;
+  const float2* row = in + (long long)kx * d;
+  for (int y = threadIdx.x; y < d; y += blockDim.x) {
+    float re = 0.f, im = 0.f;
+    int e = 0;
+    for (int ky = 0; ky < d; ky++) {
+      const float2 w = qtw[e];
+      const float2 v = row[ky];
+      re += v.x * w.x - v.y * w.y;
+      im += v.x * w.y + v.y * w.x;
+      e += y;
+      if (e >= d) e -= d;
+    }
+    tmp[(long long)kx * d + y] = make_float2(re, im);
+  }
+}
+
+// pass 2: img[y][x] = scale * sum_kx h(kx) Re(tmp[kx][y] exp(+2 pi i kx x / d))
+__global__ void k_ql_c2r_rows(const float2* __restrict__ tmp, int d, float scale, float* __restrict__ img) {
+  extern __shared__ float2 qtw[];
+  ql_table(qtw, d);
+  const int y = blockIdx.x, hd = d / 2;
+  for (int x = threadIdx.x; x < d; x += blockDim.x) {
+    float acc = 0.f;
+    int e = 0;
+    for (int kx = 0; kx <= hd; kx++) {
+      const float2 w = qtw[e];
+      const float2 v = tmp[(long long)kx * d + y];
+      const float h = (kx == 0 || kx == hd) ? 1.f : 2.f;
+      acc += h * (v.x * w.x - v.y * w.y);
+      e += x;
+      if (e >= d) e -= d;
+    }
+    img[(long long)y * d + x] = acc * scale;
+  }
+}
+
+cudaError_t launch_ql_logmod(const float2* spec, int ldn, int n, float scale, float* img, cudaStream_t st) {
+  k_ql_logmod<<<148 * 8, 256, 0, st>>>(spec, ldn, n, scale, img);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ql_crop(const float2* spec, int ldn, int n, int d, float2* out, cudaStream_t st) {
+  k_ql_crop<<<(((d / 2 + 1) * d) + 255) / 256, 256, 0, st>>>(spec, ldn, n, d, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ql_c2r(const float2* in, int d, float scale, float2* tmp, float* img, cudaStream_t st) {
+  if (d > 4096) return cudaErrorInvalidValue;
+  const size_t sm = sizeof(float2) * (size_t)d;
+  k_ql_c2r_cols<<<d / 2 + 1, 256, sm, st>>>(in, d, tmp);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_ql_c2r_rows<<<d, 256, sm, st>>>(tmp, d, scale, img);
   return cudaGetLastError();
 }
 

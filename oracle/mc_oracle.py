@@ -376,6 +376,85 @@ def raw_sum_image(F: list, first: int, last: int) -> np.ndarray:
     return spectrum_to_image(S)
 
 
+# ---------------------------------------------------------------------------
+# quick-look displays of -dsp 1 (DFAlign.cu:73-178, 841-849, 1270-1286)
+# ---------------------------------------------------------------------------
+DISPDIM = 400  # DFAlign.h:13
+
+
+def hist_min_max(buf: np.ndarray, threshold: float = 0.005):
+    """histMinMax (func.cpp:372-420): 400-bin histogram, the lowest and the
+    highest `threshold` fraction cut off; float arithmetic."""
+    b = np.asarray(buf, np.float32).ravel()
+    mn, mx = np.float32(b.min()), np.float32(b.max())
+    if mn >= mx:
+        return mn, mx
+    nbin = 400
+    step = np.float32((mx - mn) / np.float32(nbin))
+    ids = ((b - mn) / step).astype(np.int64)
+    ids[ids >= nbin] = nbin - 1
+    hist = np.bincount(ids, minlength=nbin)
+    percent = int(b.size * threshold)
+    c = np.cumsum(hist)
+    i = int(np.argmax(c > percent))
+    lo = np.float32(mn + np.float32(i) * step)
+    c2 = np.cumsum(hist[::-1][:-1])              # bins nbin-1 down to 1
+    hi = mx
+    if np.any(c2 > percent):
+        k = int(np.argmax(c2 > percent))         # bin nbin-1-k
+        hi = np.float32(mx - np.float32(k) * step)
+    return lo, hi
+
+
+def display_short(buf: np.ndarray) -> np.ndarray:
+    """buf2DispShort (func.cpp:440-455): linear map of [min, max] to 0..255."""
+    b = np.asarray(buf, np.float32)
+    mn, mx = hist_min_max(b)
+    out = np.zeros(b.shape, np.int16)
+    if mn >= mx:
+        return out
+    scale = np.float32(255.0) / np.float32(mx - mn)
+    v = ((b - mn) * scale).astype(np.int16)
+    out = np.where(b <= mn, 0, np.where(b >= mx, 255, v)).astype(np.int16)
+    return out
+
+
+def modulus_display(F: np.ndarray, scale: float = 1e-4) -> np.ndarray:
+    """cuFFTLogModulus (cufunc.cu:178-188) + FFTModulusToDispBuf
+    (func.cpp:459-489): log(1 + |F| scale) as the centred n x n image."""
+    n = F.shape[0]
+    h = n // 2
+    L = np.log1p(np.abs(F) * scale)              # (n, n/2+1), rows ky
+    out = np.zeros((n, n + 2))
+    out[h:, h:n + 1] = L[:h, :]
+    out[:h, h:n + 1] = L[h:, :]
+    for j in range(1, n):
+        out[j, :h] = out[n - j, n - np.arange(h)]
+    out[0, :h] = out[1, :h]
+    return out[:, :n]
+
+
+def bin_spectrum(F: np.ndarray, d: int = DISPDIM) -> np.ndarray:
+    """GPUMemBinD2H (cufunc.cu:147-161): rows ky < d/2 and the last d/2 rows,
+    kx <= d/2 of a half spectrum (rows ky)."""
+    h = d // 2
+    return np.concatenate([F[:h, :h + 1], F[F.shape[0] - h:, :h + 1]], axis=0)
+
+
+def quicklook(F: np.ndarray, which: int) -> np.ndarray:
+    """The three displays: 0 raw FFT and 2 corrected FFT from a sum spectrum
+    (BinFFTDispBufToChar, func.cpp:524-556: R2C of the modulus image, Fourier
+    bin to 400, C2R / 400^2), 1 the sum itself binned (ImageOutputThread,
+    DFAlign.cu:73-93: C2R unnormalised)."""
+    d = DISPDIM
+    if which == 1:
+        img = np.fft.irfft2(bin_spectrum(F, d), s=(d, d)) * (d * d)
+    else:
+        M = modulus_display(F)
+        img = np.fft.irfft2(bin_spectrum(np.fft.rfft2(M), d), s=(d, d))
+    return display_short(img)
+
+
 def count_sum(frames: np.ndarray, mode: int, offx: int, offy: int, nu: int, first: int,
               last: int) -> np.ndarray:
     """Exact integer sum of the decoded raw pixels (read2DIm_32bit,

@@ -136,3 +136,33 @@ def test_cli_extra_outputs(gpu, tmp_path):
     assert rc == 0, out
     assert (tmp_path / "m_SumCorr_ox4_oy0_dim190.mrc").exists()
     assert (tmp_path / "m_SumCorr2_ox4_oy0_dim190.mrc").exists()
+
+
+@pytest.mark.gpu
+def test_cli_quicklook_displays(gpu, tmp_path):
+    """-dsp 1 (the default): three 400 x 400 mode-1 displays in ./dosef_quick,
+    equal to the C ABI's; below 400 pixels the run warns and still saves."""
+    mv = synth.make_movie(520, 512, 6, mean=2.0, seed=6, dtype="u8", speed=0.6, rw_sigma=0.3)
+    p = tmp_path / "m.mrc"
+    mrc.write_stack(str(p), mv.frames, 0)
+    rc, out = run([str(p), "-pbx", "64", "-fod", "1"], tmp_path)
+    assert rc == 0, out
+    prm = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=1), 6)
+    with api.Plan(prm, 520, 512, 6, 0) as pl:
+        pl.load_frames(mv.frames)
+        pl.run()
+        want = {k: pl.quicklook(v) for k, v in (("RawFFT", "raw_fft"), ("CorrSum", "corr_sum"),
+                                                  ("CorrFFT", "corr_fft"))}
+    for k, w in want.items():
+        f = tmp_path / "dosef_quick" / f"m_{k}.mrc"
+        h = mrc.read_header(str(f))
+        assert (int(h["nx"]), int(h["ny"]), int(h["nz"]), int(h["mode"])) == (400, 400, 1, 1)
+        got = np.fromfile(str(f), dtype=np.int16, offset=1024).reshape(400, 400)
+        np.testing.assert_array_equal(got, w)
+        assert float(h["dmin"]) == w.min() and float(h["dmax"]) == w.max()
+    small = tmp_path / "s.mrc"
+    mrc.write_stack(str(small), mv.frames[:, :200, :200].copy(), 0)
+    rc, out = run([str(small), "-pbx", "64", "-fod", "1", "-flg", "s.txt"], tmp_path)
+    assert rc == 0, out
+    assert "Warning: display ./dosef_quick/s_RawFFT.mrc not written" in (tmp_path / "s.txt").read_text()
+    assert (tmp_path / "s_SumCorr.mrc").exists()
