@@ -28,6 +28,13 @@ extern "C" {
 
 #define MC_VERSION 10000 /* 1.0.0 */
 
+/* Pixel modes a plan decodes on the GPU: the MRC modes 0 (signed 8-bit, as
+ * read2DIm_32bit converts char, mrc.cpp:338-348), 1 (int16), 2 (float32),
+ * 6 (uint16), and MC_MODE_U8: unsigned 8-bit pixels, as 8-bit TIFF strips
+ * hold them (MRCT::read2DIm converts unsigned char, mrct.cpp:137-150).
+ * 16-bit TIFF strips are mode 6. */
+#define MC_MODE_U8 100
+
 enum {
   MC_OK = 0,
   MC_E_ARG = -1,      /* invalid argument / parameter combination */
@@ -35,7 +42,8 @@ enum {
   MC_E_NOMEM = -3,    /* device or host allocation failed */
   MC_E_SIZE = -4,     /* geometry the kernels do not support */
   MC_E_STATE = -5,    /* call out of order (e.g. pairs before forward) */
-  MC_E_NUMERIC = -6   /* singular least-squares system */
+  MC_E_NUMERIC = -6,  /* singular least-squares system */
+  MC_E_IO = -7        /* stack file missing, unreadable, malformed or of an unsupported kind */
 };
 
 /* Alignment parameters: the fields of APARA (DFAlign.h:16-63) that act on the
@@ -65,7 +73,7 @@ typedef struct mc_params {
 typedef struct mc_plan mc_plan;
 
 typedef struct mc_info {
-  int nx, ny, nz, mode;  /* stack geometry and MRC pixel mode (0, 1, 2, 6) */
+  int nx, ny, nz, mode;  /* stack geometry and pixel mode (0, 1, 2, 6, MC_MODE_U8) */
   int nsam_unbin;        /* square crop side (verifyCropSize, func.cpp:80-103) */
   int nsam;              /* binned side (DFAlign.cu:515) */
   int nstart, nend, nframe;
@@ -316,6 +324,43 @@ void mc_batch_destroy(mc_batch* b);
 int mc_batch_run(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results);
 /* Device memory held by the runner's plans. */
 size_t mc_batch_device_bytes(const mc_batch* b);
+
+/* ---- Stack files (host only; no GPU needed) -------------------------------
+ * One handle over the three stack formats: replaces the readers MRC, MRCZ
+ * and MRCT (mrc.cpp:29-157, 325-382; mrcz.cpp:23-110; mrct.cpp:29-152) and
+ * the detection order of the alignment thread (DFAlign.cu:470-479): TIFF by
+ * its byte-order mark (isTIFF, func.cpp:608-627), MRC-gz by the gzip magic
+ * plus the 'MAP ' stamp of the inflated header (isMRCZ, func.cpp:580-606),
+ * MRC by the stamp or a file name containing "mrc" (isMRC, func.cpp:557-578).
+ * TIFF: one image per directory, 8- or 16-bit, one sample, strips (no
+ * tiles), compression none, LZW, Deflate or PackBits, predictor 1 or 2,
+ * classic or BigTIFF, either byte order; no libtiff is linked. */
+typedef struct mc_stack mc_stack;
+enum { MC_STACK_MRC = 0, MC_STACK_MRCZ = 1, MC_STACK_TIFF = 2 };
+typedef struct mc_stack_info {
+  int nx, ny, nz;
+  int mode;         /* pixel mode of the raw frames below: the MRC mode, or
+                       MC_MODE_U8 / 6 for 8- / 16-bit TIFF (mc_plan_create's mode) */
+  int file_mode;    /* the mode the reference reports: the MRC header's, 7199 for
+                       TIFF (fakeReadHeader, mrct.cpp:104-123) */
+  int format;       /* MC_STACK_* */
+  int bits;         /* bits per pixel */
+  int compression;  /* TIFF Compression tag (1, 5, 8, 32773, 32946); 0 for MRC */
+} mc_stack_info;
+/* MC_E_IO (message in mc_last_error) when the file is none of the three or
+ * holds a variant this reader does not decode. */
+int mc_stack_open(const char* path, mc_stack** out);
+int mc_stack_get_info(const mc_stack* s, mc_stack_info* info);
+/* Raw pixels of frames [first, first+count) back to back into dst
+ * (nx*ny*word length bytes each; TIFF directory k is frame k).  TIFF frames
+ * decode in parallel on host threads.  *got (may be NULL) = the leading
+ * frames read; MC_E_IO when fewer than count.  Replaces read2DIm
+ * (mrc.cpp:151-157, mrcz.cpp:103-109, mrct.cpp:113-152). */
+int mc_stack_read_frames(mc_stack* s, void* dst, int first, int count, int* got);
+/* Frame n converted to float as read2DIm_32bit does (mrc.cpp:325-382; TIFF
+ * bytes and words unsigned, mrct.cpp:137-150). */
+int mc_stack_read_frame_float(mc_stack* s, float* dst, int n);
+void mc_stack_close(mc_stack* s);
 
 #ifdef __cplusplus
 }

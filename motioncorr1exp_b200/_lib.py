@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libmc.so")
 
 MC_OK = 0
 ERRORS = {-1: "MC_E_ARG", -2: "MC_E_CUDA", -3: "MC_E_NOMEM", -4: "MC_E_SIZE", -5: "MC_E_STATE",
-          -6: "MC_E_NUMERIC"}
+          -6: "MC_E_NUMERIC", -7: "MC_E_IO"}
 
 
 class McParams(C.Structure):
@@ -58,6 +58,11 @@ class McBatchResult(C.Structure):
     _fields_ = [("status", C.c_int), ("nsam", C.c_int), ("nframe", C.c_int), ("npairs", C.c_int),
                 ("lane", C.c_int), ("start_ms", C.c_double), ("end_ms", C.c_double), ("gpu_ms", C.c_float),
                 ("message", C.c_char * 160)]
+
+
+class McStackInfo(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("mode", C.c_int), ("file_mode", C.c_int),
+                ("format", C.c_int), ("bits", C.c_int), ("compression", C.c_int)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
@@ -121,6 +126,11 @@ SIGNATURES = {
     "mc_batch_destroy": (None, [C.c_void_p]),
     "mc_batch_run": (C.c_int, [C.c_void_p, C.POINTER(McBatchJob), C.c_int, C.POINTER(McBatchResult)]),
     "mc_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "mc_stack_open": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mc_stack_get_info": (C.c_int, [C.c_void_p, C.POINTER(McStackInfo)]),
+    "mc_stack_read_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "mc_stack_read_frame_float": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "mc_stack_close": (None, [C.c_void_p]),
 }
 
 

@@ -63,7 +63,8 @@ def verify_params(p: Params, nz: int) -> Params:
     return Params.from_c(c)
 
 
-_WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2}
+MODE_U8 = 100  # unsigned 8-bit pixels (8-bit TIFF)
+_WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2, MODE_U8: 1}
 KERNEL_KINDS = 8
 
 
@@ -453,6 +454,57 @@ class Batch:
         if check and rc != L.MC_OK:
             bad = next(o for o in out if o["status"] != L.MC_OK)
             raise L.McError(rc, bad["message"])
+        return out
+
+
+_PIXEL_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, MODE_U8: np.uint8}
+STACK_FORMATS = {0: "mrc", 1: "mrc-gz", 2: "tiff"}
+
+
+class Stack:
+    """A movie stack file (MRC, MRC-gz or strip TIFF) through mc_stack_*:
+    the host-side readers MRC/MRCZ/MRCT and their detection order
+    (DFAlign.cu:470-479).  Needs no GPU."""
+
+    def __init__(self, path: str):
+        self._lib = L.lib()
+        h = C.c_void_p()
+        L.check(self._lib.mc_stack_open(os.fsencode(path), C.byref(h)))
+        self._h = h
+        i = L.McStackInfo()
+        L.check(self._lib.mc_stack_get_info(self._h, C.byref(i)))
+        self.info = {k: getattr(i, k) for k, _ in L.McStackInfo._fields_}
+        self.info["format_name"] = STACK_FORMATS[i.format]
+        self.nx, self.ny, self.nz, self.mode = i.nx, i.ny, i.nz, i.mode
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.mc_stack_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def read_frames(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        """Raw pixels (count, ny, nx) in the plan's pixel type for `mode`."""
+        count = self.nz - first if count is None else count
+        out = np.empty((count, self.ny, self.nx), dtype=_PIXEL_DTYPE[self.mode])
+        got = C.c_int()
+        L.check(self._lib.mc_stack_read_frames(self._h, _ptr(out), first, count, C.byref(got)))
+        return out
+
+    def read_frame_float(self, n: int) -> np.ndarray:
+        out = np.empty((self.ny, self.nx), dtype=np.float32)
+        L.check(self._lib.mc_stack_read_frame_float(self._h, _ptr(out), n))
         return out
 
 

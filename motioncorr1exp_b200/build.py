@@ -24,8 +24,9 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
               "-Xptxas", "-warn-spills"]
 
 LIB_SOURCES = ["mc_kernels.cu", "mc_fwd.cu", "mc_fwd_raw.cu", "mc_fwd_dif.cu", "mc_pair.cu", "mc_sum.cu", "mc_plan.cu",
-               "mc_solve.cu", "mc_noalloc.cu", "lsq.cpp", "mc_batch.cpp"]
-LIB_HEADERS = ["kernels.cuh", "kcommon.cuh", "fft_engine.cuh", "f2ops.cuh", "dft_gen.cuh", "codelets_gen.cuh", "lsq.h"]
+               "mc_solve.cu", "mc_noalloc.cu", "lsq.cpp", "mc_batch.cpp", "stack_io.cpp", "tiff_read.cpp"]
+LIB_HEADERS = ["kernels.cuh", "kcommon.cuh", "fft_engine.cuh", "f2ops.cuh", "dft_gen.cuh", "codelets_gen.cuh", "lsq.h",
+               "tiff_read.h"]
 CLI_SOURCES = ["cli/dosefgpu_driftcorr.cpp", "cli/mrc_file.cpp"]
 CLI_HEADERS = ["cli/mrc_file.h"]
 
@@ -80,7 +81,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             f.result()
     so = os.path.join(LIB, "libmc.so")
     if force or _stale(so, objs):
-        _run([nvcc()] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart"], verbose)
+        _run([nvcc()] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart", "-lz", "-lpthread"], verbose)
     cli = os.path.join(LIB, "dosefgpu_driftcorr")
     cli_src = [os.path.join(CSRC, c) for c in CLI_SOURCES]
     if all(os.path.exists(c) for c in cli_src):

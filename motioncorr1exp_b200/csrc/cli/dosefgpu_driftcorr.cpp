@@ -46,9 +46,21 @@ void text_output(const char* s) {
 bool g_hold = false;
 std::vector<std::string> g_held;
 
+// The mode the "Input Stack" line names: the reference prints the stack
+// object's header mode, 7199 for TIFF (mrct.cpp:106), while the plan decodes
+// TIFF words as MC_MODE_U8 or 6.
+int g_file_mode = -1;
+
 void log_cb(const char* text, void*) {
-  if (g_hold) g_held.push_back(text);
-  else text_output(text);
+  std::string line = text;
+  int nx, ny, nz, mode;
+  if (g_file_mode >= 0 && std::sscanf(text, "Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)", &nx, &ny, &nz, &mode) == 4) {
+    char b[160];
+    std::snprintf(b, sizeof(b), "Input Stack: Nx(%d) Ny(%d) Nz(%d) Mode(%d)\n\n", nx, ny, nz, g_file_mode);
+    line = b;
+  }
+  if (g_hold) g_held.push_back(line);
+  else text_output(line.c_str());
 }
 
 bool starts_with(const std::string& s, const char* p) { return s.compare(0, std::strlen(p), p) == 0; }
@@ -101,11 +113,19 @@ void usage() {
   printf("           -ref       0                 1: gradient refinement of the sub-pixel shifts. 0: Not.\n");
 }
 
+// getNFrame (DFAlign.cu:344-368).  The reference tries MRC first, so a
+// gzip file whose name contains "mrc" is read as a raw MRC header there;
+// here the stack is opened in the alignment thread's order (TIFF, MRC-gz,
+// MRC) so the frame count is the file's.
 int stack_nframe(const std::string& fn) {
-  if (!is_mrc(fn.c_str())) return 0;
-  MrcStack s;
-  if (s.open(fn.c_str()) <= 0) return 0;
-  return s.header().nz;
+  const char* f = fn.c_str();
+  if (!starts_with_tiff(f) && !starts_with_gzip(f)) is_mrc(f, false);  // its MRC2000 line
+  mc_stack* s = nullptr;
+  if (mc_stack_open(f, &s) != MC_OK) return 0;
+  mc_stack_info si;
+  mc_stack_get_info(s, &si);
+  mc_stack_close(s);
+  return si.nz;
 }
 
 // VerifyPara (dosefgpu_driftcorr.cpp:60-118)
@@ -338,21 +358,30 @@ bool read_ref(const std::string& fn, const char* what, const char* plural, int n
 int run_align(Options& o) {
   char str[2048];
   const char* fn = o.fnStack.c_str();
-  if (starts_with_tiff(fn) || starts_with_gzip(fn)) {
-    message("Error: TIFF and MRC-gz stacks are not supported by this build; convert to MRC.");
+  // format detection of RunAlign (DFAlign.cu:470-479)
+  mc_stack* stack = nullptr;
+  const int orc = mc_stack_open(fn, &stack);
+  mc_stack_info h{};
+  if (orc == MC_OK) mc_stack_get_info(stack, &h);
+  if (orc == MC_OK && h.format == MC_STACK_TIFF) {
+    printf("Auto-detected file format: TIFF\n");
+  } else if (orc == MC_OK && h.format == MC_STACK_MRCZ) {
+    printf("Auto-detected file format: MRC-gz\n");
+  } else if (!is_mrc(fn, true)) {
+    message(orc == MC_OK ? "Only MRC, MRC-gz, TIFF file formats are supported." : mc_last_error());
+    if (stack) mc_stack_close(stack);
     return 1;
   }
-  if (!is_mrc(fn)) {
-    message("Only MRC, MRC-gz, TIFF file formats are supported.");
-    return 1;
-  }
-  MrcStack stack;
-  if (stack.open(fn) <= 0) {
-    snprintf(str, sizeof(str), "Error: Failed to open stack %s .", fn);
+  if (orc != MC_OK) {
+    snprintf(str, sizeof(str), "Error: Failed to open stack %s . (%s)", fn, mc_last_error());
     message(str);
     return 1;
   }
-  const MrcHeader h = stack.header();
+  struct StackCloser {
+    mc_stack* s;
+    ~StackCloser() { mc_stack_close(s); }
+  } closer{stack};
+  g_file_mode = h.file_mode;
   if (o.xscale > 1.0f || o.yscale > 1.0f) message("Warning: -scx/-scy stretching is not applied by this build.");
   if (o.bSaveCCmap || o.bLogFSC) message("Warning: -scc/-fsc outputs are not produced by this build.");
   mc_plan* plan = nullptr;
@@ -384,13 +413,17 @@ int run_align(Options& o) {
     }
   }
   // frames nStart..nEnd, read in chunks and handed to the library
-  const size_t fb = stack.frame_bytes();
-  const int chunk = 8;
+  // frames nStart..nEnd in chunks (TIFF chunks decode on host threads)
+  const size_t fb = (size_t)h.nx * h.ny * (h.bits / 8);
+  const int chunk = 16;
   std::vector<unsigned char> buf(fb * chunk);
   for (int f = 0; f < info.nframe; f += chunk) {
     const int cnt = std::min(chunk, info.nframe - f);
-    const int got = stack.read_frames(buf.data(), info.nstart + f, cnt);
+    int got = 0;
+    mc_stack_read_frames(stack, buf.data(), info.nstart + f, cnt, &got);
     for (int k = got; k < cnt; k++) {
+      if (mc_stack_read_frames(stack, buf.data() + (size_t)k * fb, info.nstart + f + k, 1, nullptr) == MC_OK)
+        continue;
       snprintf(str, sizeof(str), "Error when reading #%03d\n", info.nstart + f + k);
       text_output(str);
       std::memset(buf.data() + (size_t)k * fb, 0, fb);

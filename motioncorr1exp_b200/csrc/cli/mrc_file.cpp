@@ -64,7 +64,7 @@ bool MrcStack::read_frame_float(float* dst, int n) {
   return true;
 }
 
-bool is_mrc(const char* path) {
+bool is_mrc(const char* path, bool verb) {
   MrcStack s;
   if (s.open(path) > 0) {
     const MrcHeader& h = s.header();
@@ -72,7 +72,10 @@ bool is_mrc(const char* path) {
       printf("Auto-detected file format: MRC2000\n");
       return true;
     }
-    return std::strstr(path, "mrc") != nullptr;
+    if (std::strstr(path, "mrc") != nullptr) {
+      if (verb) printf("Auto-detected file format: old MRC with mrc extension.\n");
+      return true;
+    }
   }
   return false;
 }

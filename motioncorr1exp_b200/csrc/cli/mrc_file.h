@@ -55,7 +55,8 @@ class MrcStack {
 
 // Format detection of isMRC (func.cpp:557-578): 'MAP ' stamp, or a file
 // name containing "mrc".
-bool is_mrc(const char* path);
+// verb also prints the old-MRC line (isMRC's verb argument).
+bool is_mrc(const char* path, bool verb);
 bool starts_with_gzip(const char* path);
 bool starts_with_tiff(const char* path);
 

@@ -17,6 +17,7 @@ constexpr int kThreads = 256;
 __device__ __forceinline__ float load_pixel(const void* frame, int mode, long long idx) {
   switch (mode) {
     case 0: return (float)((const int8_t*)frame)[idx];
+    case MC_MODE_U8: return (float)((const uint8_t*)frame)[idx];
     case 1: return (float)((const int16_t*)frame)[idx];
     case 6: return (float)((const uint16_t*)frame)[idx];
     default: return ((const float*)frame)[idx];

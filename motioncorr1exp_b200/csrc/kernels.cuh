@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "fft_engine.cuh"
+#include "mc.h"
 
 namespace mc {
 

@@ -136,6 +136,7 @@ cudaError_t launch_fwd_rows_dif(const FwdRowsArgs& a, cudaStream_t st) {
   if (n1 == (A) && n2 == (B)) {                                                                       \
     switch (a.mode) {                                                                                 \
       case 0: MC_DIF_RAW(A, B, int8_t)                                                                \
+      case MC_MODE_U8: MC_DIF_RAW(A, B, uint8_t)                                                      \
       case 1: MC_DIF_RAW(A, B, int16_t)                                                               \
       case 6: MC_DIF_RAW(A, B, uint16_t)                                                              \
       default: MC_DIF_RAW(A, B, float)                                                                \

@@ -243,6 +243,7 @@ int word_length(int mode) {
     case 1: return 2;
     case 2: return 4;
     case 6: return 2;
+    case MC_MODE_U8: return 1;
     default: return 0;
   }
 }
@@ -638,6 +639,7 @@ const char* mc_strerror(int code) {
     case MC_E_SIZE: return "unsupported size";
     case MC_E_STATE: return "call out of order";
     case MC_E_NUMERIC: return "singular least-squares system";
+    case MC_E_IO: return "stack file error";
     default: return "unknown error";
   }
 }
@@ -1662,7 +1664,7 @@ int mc_plan_quicklook(mc_plan* pl, int which, int16_t* out) {
 
 int mc_plan_count_sum(mc_plan* pl, int32_t* host) {
   if (!pl || !host) return set_err(MC_E_ARG, "null argument");
-  if (pl->mode == 2) return set_err(MC_E_ARG, "count sums need integer pixels (MRC mode 0, 1 or 6)");
+  if (pl->mode == 2) return set_err(MC_E_ARG, "count sums need integer pixels (mode 0, 1, 6 or MC_MODE_U8)");
   for (int f = 0; f < pl->nframe; f++)
     if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
   CK(cudaSetDevice(pl->device));

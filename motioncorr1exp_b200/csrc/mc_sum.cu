@@ -285,6 +285,7 @@ cudaError_t launch_count_sum(const CountSumArgs& a, cudaStream_t st) {
   const int grid = (int)std::min<long long>((items + kThreads - 1) / kThreads, 148LL * 16);
   switch (a.mode) {
     case 0: k_count_sum<int8_t><<<grid, kThreads, 0, st>>>(a); break;
+    case MC_MODE_U8: k_count_sum<uint8_t><<<grid, kThreads, 0, st>>>(a); break;
     case 1: k_count_sum<int16_t><<<grid, kThreads, 0, st>>>(a); break;
     case 6: k_count_sum<uint16_t><<<grid, kThreads, 0, st>>>(a); break;
     default: return cudaErrorInvalidValue;

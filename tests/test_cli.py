@@ -166,3 +166,54 @@ def test_cli_quicklook_displays(gpu, tmp_path):
     assert rc == 0, out
     assert "Warning: display ./dosef_quick/s_RawFFT.mrc not written" in (tmp_path / "s.txt").read_text()
     assert (tmp_path / "s_SumCorr.mrc").exists()
+
+
+def _tiff(path, frames, **kw):
+    from PIL import Image
+    ims = [Image.fromarray(f) for f in frames]
+    ims[0].save(str(path), save_all=True, append_images=ims[1:], **kw)
+
+
+def test_tiff_and_mrcgz_stacks_pass_verify(tmp_path):
+    """TIFF and MRC-gz stacks are detected and counted (getNFrame,
+    DFAlign.cu:344-368): a bad -fod then aborts as for MRC."""
+    pytest.importorskip("PIL")
+    import gzip
+    frames = np.random.default_rng(1).integers(0, 5, (6, 40, 48)).astype(np.uint8)
+    _tiff(tmp_path / "m.tif", frames, compression="tiff_lzw")
+    mrc.write_stack(str(tmp_path / "m.mrc"), frames, 0)
+    (tmp_path / "m.mrc.gz").write_bytes(gzip.compress((tmp_path / "m.mrc").read_bytes()))
+    for name in ("m.tif", "m.mrc.gz"):
+        rc, out = run([str(tmp_path / name), "-fod", "9"], tmp_path)
+        assert rc == 1 and "Frame distance offset is too big" in out and "Not a stack" not in out
+    (tmp_path / "x.txt").write_text("hello" * 300)
+    rc, out = run([str(tmp_path / "x.txt")], tmp_path)
+    assert rc == 1 and "Not a stack or wrong file. Abort" in out
+
+
+@pytest.mark.gpu
+def test_cli_tiff_and_mrcgz_runs(gpu, tmp_path):
+    """One movie as MRC, 8-bit LZW TIFF, 16-bit Deflate TIFF and MRC-gz: the
+    same aligned sum; the TIFF log names mode 7199 as the reference does."""
+    pytest.importorskip("PIL")
+    import gzip
+    mv = synth.make_movie(200, 190, 8, mean=2.0, seed=7, dtype="u8", speed=0.8, rw_sigma=0.3)
+    mrc.write_stack(str(tmp_path / "a.mrc"), mv.frames, 0)
+    _tiff(tmp_path / "b.tif", mv.frames, compression="tiff_lzw")
+    _tiff(tmp_path / "c.tif", mv.frames.astype(np.uint16), compression="tiff_adobe_deflate")
+    (tmp_path / "d.mrc.gz").write_bytes(gzip.compress((tmp_path / "a.mrc").read_bytes()))
+    sums = {}
+    for name in ("a.mrc", "b.tif", "c.tif", "d.mrc.gz"):
+        stem = name[0]
+        rc, out = run([str(tmp_path / name), "-pbx", "64", "-fod", "2", "-dsp", "0", "-flg", stem + ".txt"],
+                      tmp_path)
+        assert rc == 0, out
+        # default names drop only the last extension (dosefgpu_driftcorr.cpp:433-481)
+        sums[stem] = mrc.read_image(str(tmp_path / f"{name[:name.rfind('.')]}_SumCorr.mrc"))
+        log = (tmp_path / f"{stem}.txt").read_text()
+        mode = 7199 if name.endswith(".tif") else 0
+        assert f"Input Stack: Nx(200) Ny(190) Nz(8) Mode({mode})" in log
+        fmt = {"a": "MRC2000", "b": "TIFF", "c": "TIFF", "d": "MRC-gz"}[stem]
+        assert f"Auto-detected file format: {fmt}" in out
+    for k in ("b", "c", "d"):
+        np.testing.assert_array_equal(sums[k], sums["a"])

@@ -63,11 +63,11 @@ def test_raw_second_and_corrected(gpu, kw):
             pl.corrected_frame(last + pl.info["nstart"] + 1)
 
 
-@pytest.mark.parametrize("mode,dtype", [(0, np.int8), (1, np.int16), (6, np.uint16)])
+@pytest.mark.parametrize("mode,dtype", [(0, np.int8), (1, np.int16), (6, np.uint16), (api.MODE_U8, np.uint8)])
 def test_count_sum_exact(gpu, mode, dtype):
     rng = np.random.default_rng(62 + mode)
     nz, ny, nx = 9, 203, 230
-    lo, hi = (-128, 128) if mode == 0 else ((-32768, 32768) if mode == 1 else (0, 65536))
+    lo, hi = {0: (-128, 128), 1: (-32768, 32768), 6: (0, 65536), api.MODE_U8: (0, 256)}[mode]
     frames = rng.integers(lo, hi, size=(nz, ny, nx)).astype(dtype)
     p = api.verify_params(api.Params(CCPeakSearchDim=32, crop_offsetx=5, crop_offsety=3, nStartSum=1,
                                      nEndSum=7, FrameDistOffset=1), nz)
@@ -93,3 +93,21 @@ def test_count_sum_bound_frames_and_float_rejected(gpu):
         pl.load_frames(f32.frames)
         with pytest.raises(Exception):
             pl.count_sum()
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(bin=2.0)])
+def test_unsigned_bytes_equal_uint16(gpu, kw):
+    """MC_MODE_U8 (8-bit TIFF words) decodes bytes above 127 as unsigned: the
+    same movie as uint16 (mode 6) gives bit-identical results; mode 0 reads
+    the same bytes as signed char and differs."""
+    rng = np.random.default_rng(65)
+    base = synth.make_movie(300, 292, 8, mean=2.0, seed=66, dtype="u8", speed=0.6, rw_sigma=0.4).frames
+    frames = (base.astype(np.int32) + rng.integers(100, 140, base.shape)).clip(0, 255).astype(np.uint8)
+    assert frames.max() > 127
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2, **kw), 8)
+    r8 = api.align(frames, api.MODE_U8, p)
+    r16 = api.align(frames.astype(np.uint16), 6, p)
+    np.testing.assert_array_equal(r8["image"], r16["image"])
+    np.testing.assert_array_equal(r8["frame_shifts"], r16["frame_shifts"])
+    rs = api.align(frames.view(np.int8), 0, p)
+    assert not np.array_equal(rs["image"], r8["image"])
