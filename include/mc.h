@@ -120,6 +120,15 @@ void mc_plan_set_log(mc_plan* plan, mc_log_fn fn, void* user);
 int mc_plan_set_refs(mc_plan* plan, const float* dark, const float* dark2, const float* norm,
                      const float* norm2);
 
+/* Anisotropic magnification correction of -scx/-scy (DFAlign.cu:503-504,
+ * 751-765), for the forward transforms of later runs: with r = 1/yscale and
+ * c = 1/xscale in float, each dark/gain-corrected pixel (y, x) with y, x >= 1
+ * takes the value at (int(y*r + 0.5), int(x*c + 0.5)) (float product, double
+ * sum, nearest neighbour); row 0 and column 0 keep theirs.  Factors >= 1
+ * (MC_E_ARG otherwise, with the reference's message); 1, 1 switches it off.
+ * The exact count sums stay on the unstretched pixels. */
+int mc_plan_set_stretch(mc_plan* plan, float xscale, float yscale);
+
 /* Copy raw frames (MRC pixel type of the plan's mode, nx*ny each) for
  * positions [first, first+count) from host memory (pinned or pageable) or
  * from device memory.  Replaces MRC::read2DIm_32bit + GPUMemH2D per frame
@@ -238,6 +247,17 @@ int mc_plan_corrected_frame(mc_plan* plan, int frame, float* image_host);
  * binned side of at least 400; 0 needs mc_plan_forward, 1 and 2 a finished
  * sum (mc_plan_sum or mc_plan_run). */
 #define MC_QUICKLOOK_DIM 400
+
+/* FSC of -fsc (CDFAlign::PlotFSC, DFAlign.cu:212-326) from the resident
+ * spectra and the current sum shifts: the summed frames split into even and
+ * odd positions, unaligned (Raw) and aligned (Corr), correlated per Fourier
+ * shell of width nsam/400 (nsam >= 400, else MC_E_SIZE), separately along
+ * the drift of the last summed frame (D, |cos| > cos 45 deg) and across it
+ * (U).  Fills min(cap, *nbox) rows of 5 doubles: Nq%, D_Raw, U_Raw, D_Corr,
+ * U_Corr; *nbox = (nsam/2+1)/(nsam/400) + 1 (rows NULL: only this size,
+ * nothing computed).  Shell sums in FP64 (the reference accumulates in
+ * float). */
+int mc_plan_fsc(mc_plan* plan, double* rows, int cap, int* nbox);
 int mc_plan_quicklook(mc_plan* plan, int which, int16_t* out);
 
 /* No counterpart in the reference (its raw sums are FP32 spectra): the

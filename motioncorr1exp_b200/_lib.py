@@ -114,6 +114,8 @@ SIGNATURES = {
     "mc_plan_corrected_frame": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "mc_plan_count_sum": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mc_plan_quicklook": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mc_plan_fsc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "mc_plan_set_stretch": (C.c_int, [C.c_void_p, C.c_float, C.c_float]),
     "mc_plan_reframe": (C.c_int, [C.c_void_p, C.POINTER(McParams), C.c_int]),
     "mc_plan_create_capacity": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.POINTER(C.c_void_p)]),

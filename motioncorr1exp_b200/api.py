@@ -183,6 +183,10 @@ class Plan:
         L.check(self._lib.mc_plan_set_refs(self._h, p(dark), p(dark2), p(norm), p(norm2)))
         self.info["two_sets"] = int(dark is not None or norm is not None)
 
+    def set_stretch(self, xscale: float = 1.0, yscale: float = 1.0) -> None:
+        """-scx/-scy: nearest-neighbour magnification correction (factors >= 1)."""
+        L.check(self._lib.mc_plan_set_stretch(self._h, xscale, yscale))
+
     def load_frames(self, frames: np.ndarray, first: int = 0) -> None:
         """Raw frames (count, ny, nx) in the plan's MRC pixel type, host memory."""
         a = np.ascontiguousarray(frames)
@@ -251,6 +255,15 @@ class Plan:
         out = np.empty((400, 400), dtype=np.int16)
         L.check(self._lib.mc_plan_quicklook(self._h, self.QUICKLOOK[which], _ptr(out)))
         return out
+
+    def fsc(self) -> np.ndarray:
+        """-fsc table (nbox, 5): Nq%, D_Raw, U_Raw, D_Corr, U_Corr."""
+        n = self.nsam
+        nbox = (n // 2 + 1) // max(1, n // 400) + 1
+        out = np.empty((nbox, 5), dtype=np.float64)
+        nb = C.c_int()
+        L.check(self._lib.mc_plan_fsc(self._h, _ptr(out), nbox, C.byref(nb)))
+        return out[:nb.value]
 
     def count_sum(self) -> np.ndarray:
         nu = self.info["nsam_unbin"]
@@ -515,12 +528,14 @@ def fft1d(d_in: int, d_out: int, n: int, batch: int, inverse: bool, stream: int 
 
 
 def align(frames: np.ndarray, mode: int, params: Params, nz: Optional[int] = None,
-          refs: Optional[dict] = None, log=None) -> dict:
+          refs: Optional[dict] = None, log=None, stretch: Optional[tuple] = None) -> dict:
     """Whole path on a stack already in host memory: frames (nz, ny, nx) in
     the file's pixel type.  Returns shifts, pair results and the sum."""
     nf, ny, nx = frames.shape
     nz = nz if nz is not None else nf
     with Plan(params, nx, ny, nz, mode, log=log) as pl:
+        if stretch:
+            pl.set_stretch(*stretch)
         if refs:
             pl.set_refs(**refs)
         pl.load_frames(frames[pl.info["nstart"]: pl.info["nend"] + 1])

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills"]
 
-LIB_SOURCES = ["mc_kernels.cu", "mc_fwd.cu", "mc_fwd_raw.cu", "mc_fwd_dif.cu", "mc_pair.cu", "mc_sum.cu", "mc_plan.cu",
+LIB_SOURCES = ["mc_kernels.cu", "mc_fwd.cu", "mc_fwd_raw.cu", "mc_fwd_dif.cu", "mc_pair.cu", "mc_sum.cu", "mc_fsc.cu", "mc_stretch.cu", "mc_plan.cu",
                "mc_solve.cu", "mc_noalloc.cu", "lsq.cpp", "mc_batch.cpp", "stack_io.cpp", "tiff_read.cpp"]
 LIB_HEADERS = ["kernels.cuh", "kcommon.cuh", "fft_engine.cuh", "f2ops.cuh", "dft_gen.cuh", "codelets_gen.cuh", "lsq.h",
                "tiff_read.h"]

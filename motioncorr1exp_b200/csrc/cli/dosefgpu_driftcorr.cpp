@@ -17,7 +17,7 @@ namespace {
 
 struct Options {
   mc_params p;
-  float xscale = 1.f, yscale = 1.f;  // -scx -scy (accepted, not applied)
+  float xscale = 1.f, yscale = 1.f;  // -scx -scy
   int nEndSum2 = 0;                  // -2es
   int bSaveSubAreaCorrSum = 0, bSaveRawSum = 0, bSaveStackCorr = 0, bSaveCCmap = 0;
   int bSaveLog = 1, bLogFSC = 0;
@@ -382,8 +382,6 @@ int run_align(Options& o) {
     ~StackCloser() { mc_stack_close(s); }
   } closer{stack};
   g_file_mode = h.file_mode;
-  if (o.xscale > 1.0f || o.yscale > 1.0f) message("Warning: -scx/-scy stretching is not applied by this build.");
-  if (o.bSaveCCmap || o.bLogFSC) message("Warning: -scc/-fsc outputs are not produced by this build.");
   mc_plan* plan = nullptr;
   int rc = mc_plan_create(&o.p, h.nx, h.ny, h.nz, h.mode, &plan);
   if (rc != MC_OK) {
@@ -392,6 +390,11 @@ int run_align(Options& o) {
     return 1;
   }
   mc_plan_set_log(plan, log_cb, nullptr);
+  if (mc_plan_set_stretch(plan, o.xscale, o.yscale) != MC_OK) {
+    message(mc_last_error());
+    mc_plan_destroy(plan);
+    return 1;
+  }
   mc_info info;
   mc_plan_info(plan, &info);
   std::vector<float> dark, dark2, norm, norm2;
@@ -497,6 +500,16 @@ int run_align(Options& o) {
     }
     if (!w.close()) return fail("write");
   }
+  // -scc: the pair CC windows, box x box x npairs (DFAlign.cu:882-900, 1094-1099)
+  std::vector<std::string> cc_lines;
+  if (o.bSaveCCmap) {
+    const int box = o.p.CCPeakSearchDim;
+    std::vector<float> boxes((size_t)box * box * info.npairs);
+    if (mc_plan_get_boxes(plan, boxes.data()) != MC_OK) return fail("CC map");
+    if (!write_mrc_float(o.fnCCmap.c_str(), boxes.data(), box, box, info.npairs, nullptr)) return fail("write");
+    snprintf(str, sizeof(str), "Save CC map to: %s\n", o.fnCCmap.c_str());
+    cc_lines.push_back(str);
+  }
   // the held log with the extra lines in the reference's places
   char add2[64];
   snprintf(add2, sizeof(add2), "......Add Frame #%03d ", sum2_last + info.nstart);
@@ -508,6 +521,10 @@ int run_align(Options& o) {
       for (const auto& l : raw_lines) text_output(l.c_str());
     if (second && starts_with(g_held[i], add2))
       for (const auto& l : sum2_lines) text_output(l.c_str());
+    const bool last_shift = starts_with(g_held[i], "......Shift of Frame") &&
+                            (i + 1 == g_held.size() || !starts_with(g_held[i + 1], "......Shift of Frame"));
+    if (last_shift)
+      for (const auto& l : cc_lines) text_output(l.c_str());
   }
   g_held.clear();
   // -dsp 1: the three 400 x 400 displays in ./dosef_quick
@@ -538,6 +555,29 @@ int run_align(Options& o) {
   text_output(str);
   snprintf(str, sizeof(str), "Save Sum to: %s\n", fnsum.c_str());
   text_output(str);
+  // -fsc (PlotFSC's table, DFAlign.cu:309-319)
+  if (o.bLogFSC) {
+    std::vector<double> rows;
+    int nbox = 0;
+    rc = mc_plan_fsc(plan, nullptr, 0, &nbox);
+    if (rc == MC_OK) {
+      rows.resize((size_t)nbox * 5);
+      rc = mc_plan_fsc(plan, rows.data(), nbox, &nbox);
+    }
+    if (rc == MC_OK) {
+      text_output("\nFSC parallel(D) and perpendicular(U) to drift direction:\n");
+      text_output("   Nq%       D_Raw       U_Raw       D_Corr       U_Corr\n");
+      for (int i = 0; i < nbox; i++) {
+        const double* r = rows.data() + (size_t)i * 5;
+        snprintf(str, sizeof(str), "%7.2f %12.4f %12.4f %12.4f %12.4f\n", r[0], r[1], r[2], r[3], r[4]);
+        text_output(str);
+      }
+      text_output("\n");
+    } else {
+      snprintf(str, sizeof(str), "Warning: FSC not computed (%s)\n", mc_last_error());
+      text_output(str);
+    }
+  }
   text_output("Done.\n");
   mc_plan_destroy(plan);
   return 0;

@@ -75,6 +75,8 @@ struct PairColsArgs {
   FftPlan1D qplan;     // length Q
   const float2* twQ;   // Q twiddles exp(-2 pi i m / Q)
   const float2* twO;   // [P][box] exp(+2 pi i k1 y_m / n)
+  const float2* twN;   // exp(+2 pi i e / n), n entries: when set (P*box > n), the generic
+                       // kernel reads twO[k1][m] as twN[(k1 * y_m) mod n] (the same floats)
   int box;
   int ystart;
   float2* G;           // [npairs][H][box]
@@ -117,6 +119,22 @@ struct ShiftSumArgs {
   long long ld_out;
   FftPlan1D plan;        // length n (mode 1)
   const float2* tw;
+};
+
+// FSC shell sums of -fsc over the listed frames (even / odd list positions).
+struct FscArgs {
+  const float2* spec;
+  long long stride;
+  const int* frames;
+  const double2* shifts;  // sum shifts of the listed frames
+  const int* apply;
+  int nsum;
+  int n, ldn, H;
+  int step, nbox;          // shell width n/400 and shell count (n/2+1)/step + 1
+  double dirx, diry;       // unit drift direction
+  float edge;              // cos(pi/4) in float
+  double* part;            // H x [2][nbox][6] per-column tables
+  double* out;             // [2][nbox][6]: along / across drift; raw (x, aa, bb), corrected (x, aa, bb)
 };
 
 // C2R of rows y, y+1 packed as one complex inverse FFT: image[y][x] * scale.
@@ -210,6 +228,17 @@ cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 // ey: scratch of nsum*n float2 for the per-frame ky phase ramps
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
+// -scx/-scy stretch: the crop region of one raw frame (word length wl, read
+// through `slot` + offset when slot is set, else from `frame`) gathered into
+// the same region of the full-size frame dst; and a whole float reference.
+cudaError_t launch_stretch_crop(const void* const* slot, long long offset, const void* frame, int wl, void* dst,
+                                const int* rmap, const int* cmap, int nx, int offx, int offy, int nu,
+                                cudaStream_t st);
+cudaError_t launch_stretch_full(const float* src, float* dst, const int* rmap, const int* cmap, int nx, int ny,
+                                cudaStream_t st);
+// ey: scratch of nsum*n float2 (the ky phase ramps of the listed frames)
+cudaError_t launch_fsc(const FscArgs& a, float2* ey, cudaStream_t st);
+size_t fsc_smem(int nbox, int nsum);
 
 // ------------------------------------------------------------ quick-look --
 // Displays of -dsp 1 (DFAlign.cu:73-178, 841-849, 1270-1286; func.cpp:459-556).
@@ -244,6 +273,8 @@ cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, 
 size_t fwd_rows_smem(int nu);
 size_t rows_fft_smem(int n, int rows_per_cta);
 size_t pair_cols_smem(int n, int P, int Q, int box);
+// the generic column kernel keeps a length-n twiddle table instead of P x box
+inline bool pair_cols_tabn(int n, int P, int box) { return (long long)P * box > n; }
 size_t shift_sum_smem(int n, int nsum);
 size_t c2r_rows_smem(int n);
 size_t peak_smem();

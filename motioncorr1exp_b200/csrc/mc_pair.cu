@@ -9,10 +9,11 @@ namespace mc {
 
 // ============================================================ pair columns ==
 size_t pair_cols_smem(int n, int P, int Q, int box) {
-  return (size_t)2 * n * sizeof(float2)       // ping-pong
-         + (size_t)n * sizeof(float)          // B-factor column
-         + (size_t)Q * sizeof(float2)         // inner twiddles
-         + (size_t)P * box * sizeof(float2);  // outer twiddles
+  const size_t outer = pair_cols_tabn(n, P, box) ? (size_t)n : (size_t)P * box;
+  return (size_t)2 * n * sizeof(float2)     // ping-pong
+         + (size_t)n * sizeof(float)        // B-factor column
+         + (size_t)Q * sizeof(float2)       // inner twiddles
+         + outer * sizeof(float2);          // outer twiddles
 }
 
 __global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
@@ -25,8 +26,10 @@ __global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
   float2* twO = twQ + Q;
   const int tid = threadIdx.x, nth = blockDim.x;
   const int kx = blockIdx.y;
+  const bool tabn = a.twN != nullptr;
   copy_table(twQ, a.twQ, Q);
-  copy_table(twO, a.twO, P * box);
+  if (tabn) copy_table(twO, a.twN, n);
+  else copy_table(twO, a.twO, P * box);
   const int half = n / 2;
   for (int ky = tid; ky < n; ky += nth) {
     const int y = ky < half ? ky : ky - n;
@@ -57,11 +60,24 @@ __global__ void __launch_bounds__(kThreads) k_pair_cols(PairColsArgs a) {
         const int r = (a.ystart + m) % Q;
         const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
         const float2* yr = Y + (long long)P * r;
-        for (int k = k0; k < k1; k++) {
-          const float2 t = twO[k * box + m];
-          const float2 yv = yr[k];
-          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
-          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+        if (tabn) {
+          const int y = (a.ystart + m) % n;
+          int e = (int)(((long long)k0 * y) % n);
+          for (int k = k0; k < k1; k++) {
+            const float2 t = twO[e];
+            const float2 yv = yr[k];
+            acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+            acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+            e += y;
+            if (e >= n) e -= n;
+          }
+        } else {
+          for (int k = k0; k < k1; k++) {
+            const float2 t = twO[k * box + m];
+            const float2 yv = yr[k];
+            acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+            acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
+          }
         }
       }
       acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
@@ -310,6 +326,8 @@ cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
     const int team = a.P <= 32 ? 32 : (a.P <= 64 ? 64 : 128);
     return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);
   }
+  // the shared-memory size assumes the outer table the kernel will copy
+  if ((a.twN != nullptr) != pair_cols_tabn(a.n, a.P, a.box)) return cudaErrorInvalidValue;
   const size_t smem = pair_cols_smem(a.n, a.P, a.Q, a.box) + 16;
   cudaError_t e = allow_smem((const void*)k_pair_cols, smem);
   if (e != cudaSuccess) return e;

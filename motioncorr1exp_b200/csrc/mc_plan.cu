@@ -201,7 +201,7 @@ void choose_prune(int n, int box, int& P, int& Q) {
   for (int q = 1; q <= n; q++) {
     if (n % q) continue;
     const int p = n / q;
-    if ((long long)p * box > 8192) continue;  // outer table must fit in shared memory
+    if (mc::pair_cols_smem(n, p, q, box) + 16 > 227 * 1024) continue;  // must fit shared memory
     if (q > 1 && max_prime(q) > 13) continue;
     double c = 0.0;
     if (q > 1) {
@@ -279,10 +279,18 @@ struct mc_plan {
   int* d_count = nullptr;  // exact count sum (allocated on first use)
   float2* d_ql = nullptr;  // quick-look: side-400 spectrum + C2R scratch (first use)
   float* d_qlimg = nullptr;
+  double* d_fsc = nullptr;  // FSC: per-column shell tables + the reduced table (first use)
+  // -scx/-scy stretch (mc_plan_set_stretch): row/column source maps, one
+  // stretched raw frame, and the references gathered through the same maps
+  bool stretch = false;
+  int *d_rmap = nullptr, *d_cmap = nullptr;
+  void* d_sframe = nullptr;
+  float *d_dark_s = nullptr, *d_dark2_s = nullptr, *d_norm_s = nullptr, *d_norm2_s = nullptr;
   const void* frames_src = nullptr;  // bound caller device frames (mc_plan_bind_frames_device) or null
   float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
   float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
   float2 *d_tw_nu = nullptr, *d_tw_n = nullptr, *d_twQ = nullptr, *d_twO = nullptr, *d_cs = nullptr;
+  float2* d_twN = nullptr;  // length-n outer table of the generic pair kernel (large P x box)
   double* d_w16 = nullptr;
   int2* d_pairs = nullptr;
   int2* d_groups = nullptr;
@@ -495,6 +503,7 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     a.qplan = pl->plan_q;
     a.twQ = pl->d_twQ;
     a.twO = pl->d_twO;
+    a.twN = pl->d_twN;
     a.box = pl->box;
     a.ystart = pl->ystart;
     a.G = pl->d_G;
@@ -937,6 +946,16 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   }
   CKR(pl->alloc(&pl->d_twQ, sizeof(float2) * pl->Q));
   CKR(upload(pl, pl->d_twQ, twiddles(pl->Q, -1)));
+  if (!mc::pair_cols_reg_supported(pl->P, pl->Q) && mc::pair_cols_tabn(pl->n, pl->P, pl->box)) {
+    // generic column kernel with a length-n outer table: exp(+2 pi i e / n)
+    std::vector<float2> tn(pl->n);
+    for (int e = 0; e < pl->n; e++) {
+      const double ang = 2.0 * kPi * (double)e / pl->n;
+      tn[e] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    CKR(pl->alloc(&pl->d_twN, sizeof(float2) * tn.size()));
+    CKR(upload(pl, pl->d_twN, tn));
+  }
   {
     std::vector<float2> two((size_t)pl->P * pl->box);
     for (int k = 0; k < pl->P; k++)
@@ -975,6 +994,33 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   CK(cudaStreamSynchronize(pl->st));
   pl->loaded.assign(pl->nframe, 0);
   *out = guard.release();
+  return MC_OK;
+}
+
+// Forget the captured movie graphs (their kernels hold the reference and
+// frame-source pointers of the configuration they were captured with).
+static void drop_graphs(mc_plan* pl) {
+  if (pl->st) cudaStreamSynchronize(pl->st);
+  for (auto& g : pl->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  pl->graphs.clear();
+}
+
+// The references gathered through the stretch maps (first use allocates).
+static int stretch_refs(mc_plan* pl) {
+  if (!pl->stretch) return MC_OK;
+  const size_t bytes = sizeof(float) * (size_t)pl->nx * pl->ny;
+  auto one = [&](const float* src, float** dst) -> int {
+    if (!src) return MC_OK;
+    if (!*dst) CKR(pl->alloc(dst, bytes));
+    CK(mc::launch_stretch_full(src, *dst, pl->d_rmap, pl->d_cmap, pl->nx, pl->ny, pl->st));
+    return MC_OK;
+  };
+  CKR(one(pl->d_dark, &pl->d_dark_s));
+  CKR(one(pl->d_dark2, &pl->d_dark2_s));
+  CKR(one(pl->d_norm, &pl->d_norm_s));
+  CKR(one(pl->d_norm2, &pl->d_norm2_s));
+  CK(cudaStreamSynchronize(pl->st));
   return MC_OK;
 }
 
@@ -1025,6 +1071,39 @@ int mc_plan_set_refs(mc_plan* pl, const float* dark, const float* dark2, const f
     pl->two_sets = true;
   }
   CK(cudaStreamSynchronize(pl->st));
+  CKR(stretch_refs(pl));
+  drop_graphs(pl);  // captured movies hold the previous reference pointers
+  pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
+  return MC_OK;
+}
+
+// -scx/-scy (DFAlign.cu:503-504, 751-765).
+int mc_plan_set_stretch(mc_plan* pl, float xscale, float yscale) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!(xscale >= 1.0f)) return set_err(MC_E_ARG, "Stretching factor along X-axis needs to be >=1.0.");
+  if (!(yscale >= 1.0f)) return set_err(MC_E_ARG, "Stretching factor along Y-axis needs to be >=1.0.");
+  CK(cudaSetDevice(pl->device));
+  const float xs = (float)(1.0 / xscale), ys = (float)(1.0 / yscale);
+  const bool on = xs < 1.0f || ys < 1.0f;
+  if (on) {
+    // addr_orig = int(ky*yscale+0.5)*nx + int(kx*xscale+0.5): float product, double sum
+    auto map = [](int len, float s) {
+      std::vector<int> m(len);
+      for (int k = 0; k < len; k++) m[k] = std::min(len - 1, std::max(0, (int)((double)((float)k * s) + 0.5)));
+      return m;
+    };
+    const std::vector<int> rm = map(pl->ny, ys), cm = map(pl->nx, xs);
+    if (!pl->d_rmap) {
+      CKR(pl->alloc(&pl->d_rmap, sizeof(int) * (size_t)pl->ny));
+      CKR(pl->alloc(&pl->d_cmap, sizeof(int) * (size_t)pl->nx));
+      CKR(pl->alloc(&pl->d_sframe, pl->frame_bytes));
+    }
+    CK(cudaMemcpyAsync(pl->d_rmap, rm.data(), sizeof(int) * rm.size(), cudaMemcpyHostToDevice, pl->st));
+    CK(cudaMemcpyAsync(pl->d_cmap, cm.data(), sizeof(int) * cm.size(), cudaMemcpyHostToDevice, pl->st));
+  }
+  pl->stretch = on;
+  CKR(stretch_refs(pl));
+  drop_graphs(pl);
   pl->have_forward = pl->have_pairs = pl->have_solve = pl->have_iter = pl->have_sum = false;
   return MC_OK;
 }
@@ -1088,6 +1167,15 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     a.frame = (const char*)(pl->frames_src ? pl->frames_src : pl->d_frames) + (size_t)f * pl->frame_bytes;
     a.frames_slot = pl->d_src_slot;
     a.frame_offset = (long long)f * (long long)pl->frame_bytes;
+    if (pl->stretch) {
+      // the crop of this frame through the stretch maps, then transformed from there
+      LAUNCH(pl, MC_K_FWD_ROWS, 2.0 * pl->nu * pl->nu * pl->wl,
+             mc::launch_stretch_crop(pl->d_src_slot, a.frame_offset, a.frame, pl->wl, pl->d_sframe, pl->d_rmap,
+                                     pl->d_cmap, pl->nx, pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu, pl->st));
+      a.frame = pl->d_sframe;
+      a.frames_slot = nullptr;
+      a.frame_offset = 0;
+    }
     a.mode = pl->mode;
     a.nx = pl->nx;
     a.ny = pl->ny;
@@ -1095,10 +1183,11 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     a.offy = pl->p.crop_offsety;
     a.nu = pl->nu;
     a.hk = pl->H;
-    a.dark = pl->d_dark;
-    a.dark2 = pl->d_dark2;
-    a.norm = pl->d_norm;
-    a.norm2 = pl->d_norm2;
+    const bool stretched = pl->stretch;
+    a.dark = stretched ? pl->d_dark_s : pl->d_dark;
+    a.dark2 = stretched ? pl->d_dark2_s : pl->d_dark2;
+    a.norm = stretched ? pl->d_norm_s : pl->d_norm;
+    a.norm2 = stretched ? pl->d_norm2_s : pl->d_norm2;
     a.two_outputs = pl->two_sets ? 1 : 0;
     float2* TA = binned ? pl->d_T : specA_at(pl, f);
     a.outA = TA;
@@ -1117,8 +1206,8 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
       for (int set = 0; set < 2; set++) {
         mc::FwdRowsArgs b = a;
         b.two_outputs = 0;
-        b.dark = set == 0 ? pl->d_dark : pl->d_dark2;
-        b.norm = set == 0 ? pl->d_norm : pl->d_norm2;
+        b.dark = set == 0 ? a.dark : a.dark2;
+        b.norm = set == 0 ? a.norm : a.norm2;
         b.dark2 = nullptr;
         b.norm2 = nullptr;
         b.outA = pl->d_T;
@@ -1579,6 +1668,75 @@ static void display_short(const float* buf, int size, int16_t* disp) {
     else if (buf[i] >= mx) disp[i] = 255;
     else disp[i] = (int16_t)((buf[i] - mn) * scale);
   }
+}
+
+// FSC of -fsc (PlotFSC, DFAlign.cu:212-326) over the corrected sum's frames.
+int mc_plan_fsc(mc_plan* pl, double* rows, int cap, int* nbox_out) {
+  if (!pl) return set_err(MC_E_ARG, "null plan");
+  if (!pl->have_sum) return set_err(MC_E_STATE, "FSC before the corrected sum");
+  const int n = pl->n;
+  if (n < 400) return set_err(MC_E_SIZE, "FSC needs nsam >= 400 (shell width nsam/400), nsam is %d", n);
+  const int step = n / 400, nsamc = n / 2 + 1, nbox = nsamc / step + 1;
+  if (nbox_out) *nbox_out = nbox;
+  if (!rows) return MC_OK;  // size query
+  CK(cudaSetDevice(pl->device));
+  const int ns = pl->sum_last - pl->sum_first + 1;
+  std::vector<int> frames(ns), apply(ns);
+  std::vector<double2> sh(ns);
+  for (int i = 0; i < ns; i++) {
+    const int k = pl->sum_first + i;
+    frames[i] = k;
+    apply[i] = (k == pl->sum_first && !pl->p.bAlignToMid) ? 0 : 1;
+    sh[i] = make_double2(pl->sum_shift[k].real(), pl->sum_shift[k].imag());
+  }
+  CK(cudaMemcpyAsync(pl->d_sumframes, frames.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_apply, apply.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_sumshift, sh.data(), sizeof(double2) * ns, cudaMemcpyHostToDevice, pl->st));
+  const size_t nh = 12 * (size_t)nbox;
+  if (!pl->d_fsc) {
+    CKR(pl->alloc(&pl->d_fsc, sizeof(double) * nh * ((size_t)pl->H + 1)));
+  }
+  // direction: the drift of the last summed frame (totalshift, DFAlign.cu:1232-1234), unit length
+  // when longer than 0.1 px, else the x axis (DFAlign.cu:235-236)
+  cplx dir = pl->frame_shift.empty() ? cplx(0, 0) : pl->frame_shift[pl->sum_last];
+  if (std::abs(dir) > 0.1) dir /= std::abs(dir);
+  else dir = cplx(1.0, 0.0);
+  mc::FscArgs a{};
+  a.spec = pl->d_specA;
+  a.stride = pl->fstride;
+  a.frames = pl->d_sumframes;
+  a.shifts = pl->d_sumshift;
+  a.apply = pl->d_apply;
+  a.nsum = ns;
+  a.n = n;
+  a.ldn = pl->ldn;
+  a.H = pl->H;
+  a.step = step;
+  a.nbox = nbox;
+  a.dirx = dir.real();
+  a.diry = dir.imag();
+  a.edge = (float)std::cos(M_PI / 4);
+  a.part = pl->d_fsc + nh;
+  a.out = pl->d_fsc;
+  CK(mc::launch_fsc(a, pl->d_ey, pl->st));
+  std::vector<double> t(nh);
+  CK(cudaMemcpyAsync(t.data(), pl->d_fsc, sizeof(double) * nh, cudaMemcpyDeviceToHost, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  auto fsc = [](const double* v) {
+    const double p = v[1] * v[2];
+    return p > 0.00001 ? v[0] / std::sqrt(p) : 0.0;
+  };
+  for (int i = 0; i < nbox && i < cap; i++) {
+    const double* d = t.data() + (size_t)i * 6;           // along the drift
+    const double* u = t.data() + (size_t)(nbox + i) * 6;  // across it
+    double* r = rows + (size_t)i * 5;
+    r[0] = i * 100.0 / nbox;
+    r[1] = fsc(d);
+    r[2] = fsc(u);
+    r[3] = fsc(d + 3);
+    r[4] = fsc(u + 3);
+  }
+  return MC_OK;
 }
 
 int mc_plan_quicklook(mc_plan* pl, int which, int16_t* out) {

@@ -157,6 +157,25 @@ def decode_frame(raw: np.ndarray, mode: int) -> np.ndarray:
     return np.asarray(raw).view(dt).astype(np.float64)
 
 
+def stretch_image(img: np.ndarray, xscale: float = 1.0, yscale: float = 1.0) -> np.ndarray:
+    """Image stretch of -scx/-scy (DFAlign.cu:503-504, 751-765): with
+    r = float(1/yscale), c = float(1/xscale), pixel (y, x), y, x >= 1, takes
+    the value at (int(float(y*r) + 0.5), int(float(x*c) + 0.5)); row 0 and
+    column 0 are kept.  In place from the last pixel backwards in the
+    reference, which reads only pixels not yet overwritten, so it equals a
+    gather from the unstretched image."""
+    xs = np.float32(1.0 / np.float64(np.float32(xscale)))
+    ys = np.float32(1.0 / np.float64(np.float32(yscale)))
+    if not (xs < 1.0 or ys < 1.0):
+        return img
+    ny, nx = img.shape
+    rm = ((np.arange(ny, dtype=np.float32) * ys).astype(np.float64) + 0.5).astype(np.int64)
+    cm = ((np.arange(nx, dtype=np.float32) * xs).astype(np.float64) + 0.5).astype(np.int64)
+    out = np.array(img, copy=True)
+    out[1:, 1:] = img[np.ix_(rm[1:], cm[1:])]
+    return out
+
+
 def apply_refs(raw: np.ndarray, dark=None, dark2=None, norm=None, norm2=None):
     """Two-reference dark/gain correction of DFAlign.cu:614-750.
 
@@ -457,6 +476,51 @@ def quicklook(F: np.ndarray, which: int) -> np.ndarray:
     return display_short(img)
 
 
+def fsc_table(F: list, first: int, last: int, sum_shift, align_to_mid: bool, drift) -> np.ndarray:
+    """PlotFSC (DFAlign.cu:212-326) in FP64 over spectra (n, n//2+1).
+
+    Even/odd halves: run positions first, first+2, ... and first+1, ...
+    (raw: DFAlign.cu:806-812; aligned: DFAlign.cu:1142-1179, 1237-1244, the
+    first frame shifted only with -atm 1).  Shells: r = sqrtf(x^2+y^2) in
+    float over the MkPosList coordinates (cufunc.cu:309-339), skipped when
+    int(r) <= 0 or r >= n/2+1, shell int(r/step) with step = n/400; along the
+    drift when float(|x dx + y dy| / r) > float(cos 45 deg) for the unit drift
+    (x axis below 0.1 px).  Returns (nbox, 5): Nq%, D_Raw, U_Raw, D_Corr,
+    U_Corr, each x/sqrt(aa*bb) or 0 when aa*bb <= 1e-5."""
+    n = F[first].shape[0]
+    step = n // 400
+    nsamc = n // 2 + 1
+    nbox = nsamc // step + 1
+    raw = [np.zeros_like(F[first]), np.zeros_like(F[first])]
+    cor = [np.zeros_like(F[first]), np.zeros_like(F[first])]
+    for k in range(first, last + 1):
+        h = (k - first) & 1
+        raw[h] = raw[h] + F[k]
+        apply = not (k == first and not align_to_mid)
+        cor[h] = cor[h] + (phase_shift(F[k], sum_shift[k][0], sum_shift[k][1]) if apply else F[k])
+    d = complex(drift[0], drift[1])
+    d = d / abs(d) if abs(d) > 0.1 else complex(1.0, 0.0)
+    ky = np.arange(n)
+    y = np.where(ky < n // 2, ky, ky - n)[:, None].astype(np.int64)
+    x = np.arange(nsamc)[None, :].astype(np.int64)
+    r = np.sqrt((x * x + y * y).astype(np.float32))
+    keep = (r.astype(np.int64) > 0) & (r < np.float32(nsamc))
+    sid = (r / np.float32(step)).astype(np.int64)
+    with np.errstate(divide="ignore", invalid="ignore"):  # r = 0 is outside `keep`
+        ang = (np.abs(x * d.real + y * d.imag) / r.astype(np.float64)).astype(np.float32)
+    along = ang > np.float32(math.cos(math.pi / 4))
+    out = np.zeros((nbox, 5))
+    out[:, 0] = np.arange(nbox) * 100.0 / nbox
+    for col, (a, b) in ((1, raw), (3, cor)):
+        prods = [(a * b.conj()).real, np.abs(a) ** 2, np.abs(b) ** 2]
+        for j, cls in ((0, along), (1, ~along)):
+            m = keep & cls
+            s = [np.bincount(sid[m], weights=p[m], minlength=nbox) for p in prods]
+            t = s[1] * s[2]
+            out[:, col + j] = np.where(t > 1e-5, s[0] / np.sqrt(np.where(t > 0, t, 1.0)), 0.0)
+    return out
+
+
 def count_sum(frames: np.ndarray, mode: int, offx: int, offy: int, nu: int, first: int,
               last: int) -> np.ndarray:
     """Exact integer sum of the decoded raw pixels (read2DIm_32bit,
@@ -528,7 +592,7 @@ class Result:
 
 
 def align_movie(frames: np.ndarray, mode: int, p: Params, nz_file: Optional[int] = None,
-                refs: Optional[dict] = None, want_image: bool = True) -> Result:
+                refs: Optional[dict] = None, want_image: bool = True, stretch=(1.0, 1.0)) -> Result:
     """ThreadFunc_cuAlign (DFAlign.cu:456-1355) on decoded frames.
 
     ``frames``: raw stack (nz, ny, nx) in the file's pixel type.  ``p`` must
@@ -554,6 +618,10 @@ def align_movie(frames: np.ndarray, mode: int, p: Params, nz_file: Optional[int]
     for f in range(nstart, nend + 1):
         raw = decode_frame(frames[f], mode)
         a, b = apply_refs(raw, refs.get("dark"), refs.get("dark2"), refs.get("norm"), refs.get("norm2"))
+        if b is a:
+            a = b = stretch_image(a, *stretch)
+        else:
+            a, b = stretch_image(a, *stretch), stretch_image(b, *stretch)
         sa = forward_spectrum(a, p.crop_offsetx, p.crop_offsety, nu, n)
         sb = sa if b is a else forward_spectrum(b, p.crop_offsetx, p.crop_offsety, nu, n)
         Fa.append(sa)

@@ -217,3 +217,53 @@ def test_cli_tiff_and_mrcgz_runs(gpu, tmp_path):
         assert f"Auto-detected file format: {fmt}" in out
     for k in ("b", "c", "d"):
         np.testing.assert_array_equal(sums[k], sums["a"])
+
+
+@pytest.mark.gpu
+def test_cli_fsc_and_ccmap(gpu, tmp_path):
+    """-fsc 1: PlotFSC's table after the sum (DFAlign.cu:309-319); -scc 1: the
+    pair CC windows as a box x box x npairs float stack, logged after the
+    final shifts (DFAlign.cu:1094-1099)."""
+    mv = synth.make_movie(520, 512, 8, mean=2.0, seed=8, dtype="u8", speed=0.8, rw_sigma=0.3)
+    p = tmp_path / "m.mrc"
+    mrc.write_stack(str(p), mv.frames, 0)
+    rc, out = run([str(p), "-pbx", "64", "-fod", "2", "-dsp", "0", "-fsc", "1", "-scc", "1", "-flg", "log.txt"],
+                  tmp_path)
+    assert rc == 0, out
+    prm = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2), 8)
+    with api.Plan(prm, 520, 512, 8, 0) as pl:
+        pl.load_frames(mv.frames)
+        pl.run()
+        fsc = pl.fsc()
+        boxes = pl.boxes()
+        npairs = pl.npairs
+    lines = (tmp_path / "log.txt").read_text().splitlines()
+    i = lines.index("FSC parallel(D) and perpendicular(U) to drift direction:")
+    assert lines[i - 2].startswith("Save Sum to: m_SumCorr.mrc") and lines[i - 1] == ""
+    assert lines[i + 1] == "   Nq%       D_Raw       U_Raw       D_Corr       U_Corr"
+    rows = lines[i + 2:i + 2 + len(fsc)]
+    want = ["%7.2f %12.4f %12.4f %12.4f %12.4f" % tuple(r) for r in fsc]
+    assert rows == want
+    assert lines[i + 2 + len(fsc)] == "" and lines[-1] == "Done."
+    h = mrc.read_header(str(tmp_path / "m_CCMap.mrc"))
+    assert (int(h["nx"]), int(h["ny"]), int(h["nz"]), int(h["mode"])) == (64, 64, npairs, 2)
+    got = np.fromfile(str(tmp_path / "m_CCMap.mrc"), dtype=np.float32, offset=1024).reshape(boxes.shape)
+    np.testing.assert_array_equal(got, boxes)
+    j = lines.index("Save CC map to: m_CCMap.mrc")
+    assert lines[j - 1].startswith("......Shift of Frame #007")
+
+
+@pytest.mark.gpu
+def test_cli_stretch(gpu, tmp_path):
+    """-scx/-scy reach the plan: the CLI's sum equals the API's with the same
+    stretch and differs from the unstretched one."""
+    mv = synth.make_movie(200, 190, 8, mean=2.0, seed=9, dtype="u8", speed=0.8, rw_sigma=0.3)
+    p = tmp_path / "m.mrc"
+    mrc.write_stack(str(p), mv.frames, 0)
+    rc, out = run([str(p), "-pbx", "64", "-fod", "2", "-dsp", "0", "-scx", "1.04", "-scy", "1.02"], tmp_path)
+    assert rc == 0, out
+    img = mrc.read_image(str(tmp_path / "m_SumCorr.mrc"))
+    prm = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2), 8)
+    want = api.align(mv.frames, 0, prm, stretch=(1.04, 1.02))["image"]
+    np.testing.assert_array_equal(img, want)
+    assert not np.array_equal(img, api.align(mv.frames, 0, prm)["image"])

@@ -32,11 +32,11 @@ def to_oparams(p: api.Params) -> O.Params:
     return O.Params(**{k: getattr(p, k) for k in O.Params.__dataclass_fields__})
 
 
-def run_both(frames, mode, params, refs=None, nz=None):
+def run_both(frames, mode, params, refs=None, nz=None, stretch=None):
     nz = nz if nz is not None else frames.shape[0]
     p = api.verify_params(params, nz)
-    g = api.align(frames, mode, p, nz=nz, refs=refs)
-    ref = O.align_movie(frames, mode, to_oparams(p), nz_file=nz, refs=refs)
+    g = api.align(frames, mode, p, nz=nz, refs=refs, stretch=stretch)
+    ref = O.align_movie(frames, mode, to_oparams(p), nz_file=nz, refs=refs, stretch=stretch or (1.0, 1.0))
     return g, ref, p
 
 
@@ -176,7 +176,9 @@ def test_refs_two_spectrum_sets(gpu, two_frame_refs, bin_):
 
 # ------------------------------------------------------------------ pairs --
 @pytest.mark.parametrize("n,box,nps,fod", [(256, 96, 0, 2), (240, 64, 0, 3), (212, 95, 0, 2), (256, 48, 3, 2),
-                                           (256, 16, 0, 2)])
+                                           (256, 16, 0, 2),
+                                           # a large prime factor: generic column kernel, length-n outer table
+                                           (514, 64, 0, 2), (502, 128, 0, 3)])
 def test_pair_boxes_and_peaks(gpu, n, box, nps, fod):
     mv = synth.make_movie(n + 6, n + 2, 8, mean=1.5, seed=n + box, dtype="f32", speed=0.7, rw_sigma=0.4)
     params = api.Params(CCPeakSearchDim=box, NoisePeakSize=nps, FrameDistOffset=fod)
@@ -238,6 +240,49 @@ def test_pipeline_refs(gpu):
             "norm": rng.normal(1.0, 0.02, (256, 256)).astype(np.float32)}
     g, ref, p = run_both(mv.frames, 0, api.Params(), refs=refs)
     compare_full(g, ref, 256, 0)
+
+
+@pytest.mark.parametrize("stretch,refs,kw", [
+    ((1.03, 1.0), None, dict()),
+    ((1.0, 1.05), "one", dict(crop_offsetx=3, crop_offsety=2)),
+    ((1.02, 1.04), "two", dict(bin=2.0, CCPeakSearchDim=64)),
+])
+def test_pipeline_stretch(gpu, stretch, refs, kw):
+    """-scx/-scy: the nearest-neighbour stretch after dark/gain
+    (DFAlign.cu:751-765), with one- and two-frame references."""
+    mv = synth.make_movie(300, 290, 8, mean=2.0, seed=21, dtype="u8", speed=0.6, rw_sigma=0.4)
+    rng = np.random.default_rng(22)
+    r = None
+    if refs:
+        r = {"dark": rng.normal(0.2, 0.05, (290, 300)).astype(np.float32),
+             "norm": rng.normal(1.0, 0.05, (290, 300)).astype(np.float32)}
+        if refs == "two":
+            r["dark2"] = rng.normal(0.3, 0.05, (290, 300)).astype(np.float32)
+            r["norm2"] = rng.normal(1.0, 0.05, (290, 300)).astype(np.float32)
+    g, ref, p = run_both(mv.frames, 0, api.Params(**kw), refs=r, stretch=stretch)
+    compare_full(g, ref, ref.nsam, p.NoisePeakSize)
+    plain = O.align_movie(mv.frames, 0, to_oparams(p), refs=r)
+    assert rel_l2(plain.image, ref.image) > 1e-3  # the stretch changed the input
+
+
+def test_stretch_switch_and_limits(gpu):
+    """Stretch on, off again and refs set after it: every run matches the
+    oracle (no captured movie keeps stale pointers); factors < 1 refused."""
+    mv = synth.make_movie(256, 256, 6, mean=2.0, seed=23, dtype="u8", speed=0.6, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=1), 6)
+    rng = np.random.default_rng(24)
+    refs = {"dark": rng.normal(0.2, 0.05, (256, 256)).astype(np.float32)}
+    with api.Plan(p, 256, 256, 6, 0) as pl:
+        pl.load_frames(mv.frames)
+        for st, rf in [((1.0, 1.0), None), ((1.04, 1.0), None), ((1.04, 1.0), refs), ((1.0, 1.0), refs)]:
+            pl.set_stretch(*st)
+            if rf is not None:
+                pl.set_refs(**rf)
+            img = pl.run()
+            want = O.align_movie(mv.frames, 0, to_oparams(p), refs=rf, stretch=st).image
+            assert rel_l2(img, want) <= IMAGE_RTOL
+        with pytest.raises(Exception, match="X-axis"):
+            pl.set_stretch(0.9, 1.0)
 
 
 @pytest.mark.slow

@@ -277,3 +277,20 @@ def test_decode_modes():
     u16 = np.array([0, 40000], dtype=np.uint16)
     np.testing.assert_array_equal(O.decode_frame(u16, 6), [0, 40000])
     np.testing.assert_array_equal(O.decode_frame(u16.view(np.int16), 1), [0, 40000 - 65536])
+
+
+def test_stretch_gather_equals_inplace_loop():
+    """The stretch restated as a gather equals the reference's in-place loop
+    from the last pixel backwards (DFAlign.cu:751-765)."""
+    img = np.arange(23 * 31, dtype=np.float64).reshape(23, 31) * 1.5
+    for xs, ys in [(1.03, 1.07), (3.0, 1.0), (1.0, 2.5), (1.0, 1.0)]:
+        b = img.copy().ravel()
+        ny, nx = img.shape
+        fx = np.float32(1.0 / np.float32(xs))
+        fy = np.float32(1.0 / np.float32(ys))
+        if fx < 1.0 or fy < 1.0:
+            for ky in range(ny - 1, 0, -1):
+                for kx in range(nx - 1, 0, -1):
+                    o = int(float(np.float32(ky) * fy) + 0.5) * nx + int(float(np.float32(kx) * fx) + 0.5)
+                    b[ky * nx + kx] = b[o]
+        np.testing.assert_array_equal(O.stretch_image(img, xs, ys), b.reshape(ny, nx))
