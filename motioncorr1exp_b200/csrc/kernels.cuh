@@ -80,6 +80,8 @@ struct PairColsArgs {
   int box;
   int ystart;
   float2* G;           // [npairs][H][box]
+  int variant;         // 0: compiled (Q, P) split when there is one (recurrence twiddles);
+                       // 1: runtime-P register kernel; 2: compiled split, table twiddles
 };
 
 // Row stage: box[p][yb][xb] = sum_kx Re(G[p][kx][yb] * h(kx) exp(+2 pi i kx x_xb / n))
@@ -265,6 +267,8 @@ cudaError_t allow_smem(const void* func, size_t bytes);
 // true when the register-codelet column stage handles the split n = P*Q
 bool pair_cols_reg_supported(int P, int Q);
 size_t pair_cols_reg_smem(int n, int team);
+// dynamic shared memory launch_pair_cols asks for with this split
+size_t pair_cols_launch_smem(int n, int P, int Q, int box);
 // grouped column stage: groups[g] = (first pair, count) of pairs sharing A
 size_t pair_cols_grp_smem(int n, int teams);
 cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,

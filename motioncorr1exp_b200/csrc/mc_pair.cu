@@ -171,6 +171,141 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
   }
 }
 
+// ---- split n = P x Q fixed at compile time ----------------------------------
+// The gather reads the stride-P subsequence at immediate offsets.  The outer
+// sum is blocked by residue: the output rows m with (ystart + m) mod Q = r all
+// read row r of Y, so a thread takes one residue r and one chunk of k1 and
+// keeps the up to JB rows m0(r) + j Q in registers (one shared-memory load of
+// Y feeds 4 JB FMAs; the twiddle loads of a warp stay on consecutive m).  The
+// chunk partials go to shared memory and are added in chunk order.
+template <int Q, int P>
+struct RpShape {
+  static constexpr int T = P <= 32 ? 32 : (P <= 64 ? 64 : 128);     // team threads
+  static constexpr int C = (2 * T) / Q > 1 ? (2 * T) / Q : 1;        // k1 chunks
+  static constexpr int L = (P + C - 1) / C;                          // chunk length
+  static constexpr int JB = Q >= 96 ? 1 : (Q >= 48 ? 2 : 3);         // rows per residue block
+  // Y row stride: odd in float2 units, so the rows read by 16 consecutive
+  // residues fall on 16 different bank pairs
+  static constexpr int PS = P | 1;
+  static constexpr int YN = Q * PS;
+};
+
+size_t pair_cols_rp_smem(int n, int yn, int team, int chunks, int box) {
+  const int teams = kRegThreads / team;
+  return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)teams * ((size_t)yn + (size_t)chunks * box) * sizeof(float2);
+}
+
+// REC: the twiddles of a chunk by recurrence in registers, t(k+1) = t(k) W^y
+// from t(kb) = twO[kb][m] and W^y = twO[1][m] (a chunk is at most 16 steps,
+// so the product drifts by ~1e-6); else each twiddle is loaded from twO.
+template <int Q, int P, bool REC>
+__global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_cols_rp(PairColsArgs a) {
+  using S = RpShape<Q, P>;
+  constexpr int T = S::T, C = S::C, L = S::L, JB = S::JB, N = P * Q, PS = S::PS, YN = S::YN;
+  extern __shared__ float2 sm[];
+  const int box = a.box;
+  float* wcol = reinterpret_cast<float*>(sm);
+  constexpr int teams = kRegThreads / T;
+  const int tid = threadIdx.x;
+  const int tm = tid / T, lt = tid - tm * T;
+  float2* Y = sm + (N + 1) / 2 + (size_t)tm * (YN + C * box);
+  float2* part = Y + YN;
+  const int kx = blockIdx.y;
+  for (int ky = tid; ky < N; ky += kRegThreads) {
+    const int y = ky < N / 2 ? ky : ky - N;
+    wcol[ky] = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+  }
+  __syncthreads();
+  const int ys = a.ystart % Q;
+  const int p0 = blockIdx.x * a.pairs_per_cta;
+  const int p1 = min(p0 + a.pairs_per_cta, a.npairs);
+  for (int p = p0 + tm; p < p1; p += teams) {
+    const int2 pr = a.pairs[p];
+    if (lt < P) {
+      const float2* ca = a.specA + (long long)pr.x * a.strideA + (long long)kx * a.ldn + lt;
+      const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn + lt;
+      const float* wc = wcol + lt;
+      float2 x[Q];
+#pragma unroll
+      for (int k2 = 0; k2 < Q; k2++) x[k2] = cscale(cmulc(__ldg(ca + P * k2), __ldg(cb + P * k2)), wc[P * k2]);
+      fft_reg<Q, true>(x);
+#pragma unroll
+      for (int r = 0; r < Q; r++) Y[lt + PS * r] = x[r];
+    }
+    team_barrier(1 + tm, T);
+    for (int it = lt; it < Q * C; it += T) {
+      const int r = it % Q, c = it / Q;
+      const int m0 = (r - ys + Q) % Q;  // first row with (ystart + m) mod Q = r
+      const int kb = c * L;
+      const float2* yr = Y + PS * r + kb;
+      for (int j0 = 0; m0 + j0 * Q < box; j0 += JB) {
+        float2 acc[JB];
+#pragma unroll
+        for (int j = 0; j < JB; j++) acc[j] = make_float2(0.f, 0.f);
+        bool on[JB];
+#pragma unroll
+        for (int j = 0; j < JB; j++) on[j] = m0 + (j0 + j) * Q < box;
+        const float2* tw = a.twO + (long long)kb * box + m0 + j0 * Q;
+        float2 tr[JB], wr[JB];
+        if (REC) {
+#pragma unroll
+          for (int j = 0; j < JB; j++) {
+            tr[j] = on[j] ? __ldg(tw + j * Q) : make_float2(0.f, 0.f);
+            wr[j] = on[j] ? __ldg(a.twO + box + m0 + (j0 + j) * Q) : make_float2(0.f, 0.f);
+          }
+        }
+#pragma unroll
+        for (int kk = 0; kk < L; kk++) {
+          if (L * C == P || kb + kk < P) {
+            const float2 yv = yr[kk];
+#pragma unroll
+            for (int j = 0; j < JB; j++) {
+              if (on[j]) {
+                const float2 t = REC ? tr[j] : __ldg(tw + (long long)kk * box + j * Q);
+                acc[j].x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc[j].x));
+                acc[j].y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc[j].y));
+                if (REC) tr[j] = cmul(t, wr[j]);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < JB; j++)
+          if (on[j]) part[c * box + m0 + (j0 + j) * Q] = acc[j];
+      }
+    }
+    team_barrier(1 + tm, T);
+    for (int m = lt; m < box; m += T) {
+      float2 s = part[m];
+#pragma unroll
+      for (int c = 1; c < C; c++) s = cadd(s, part[c * box + m]);
+      a.G[((long long)p * a.H + kx) * box + m] = s;
+    }
+    // the next pair writes Y before its first barrier and part after it:
+    // every read of this pair's Y precedes the second barrier above, and every
+    // read of part precedes the next pair's first barrier
+  }
+}
+
+// the compiled (Q, P) splits of the tuned lengths: 3710, 4096, 2048, 1024
+#define MC_RP_LIST(X) X(35, 106) X(70, 53) X(64, 64) X(64, 32) X(32, 64) X(32, 32)
+
+bool pair_cols_rp_supported(int P, int Q) {
+#define MC_RP_HAS(A, B) if (Q == (A) && P == (B)) return true;
+  MC_RP_LIST(MC_RP_HAS)
+#undef MC_RP_HAS
+  return false;
+}
+
+size_t pair_cols_launch_smem(int n, int P, int Q, int box) {
+#define MC_RP_SMEM(A, B) \
+  if (Q == (A) && P == (B)) return pair_cols_rp_smem(n, RpShape<A, B>::YN, RpShape<A, B>::T, RpShape<A, B>::C, box);
+  MC_RP_LIST(MC_RP_SMEM)
+#undef MC_RP_SMEM
+  if (pair_cols_reg_supported(P, Q)) return pair_cols_reg_smem(n, P <= 32 ? 32 : (P <= 64 ? 64 : 128));
+  return pair_cols_smem(n, P, Q, box) + 16;
+}
+
 // ---- grouped variant: one CTA per (A frame group, column kx) -------------
 // The pairs of a batch come in groups that share their A spectrum (the
 // reference's i-major order).  The CTA stages A(kx,:) x B-factor once in
@@ -322,6 +457,20 @@ cudaError_t dispatch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid
 
 cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
   dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
+  if (a.variant != 1) {
+#define MC_RP_LAUNCH(A, B)                                                                    \
+  if (a.Q == (A) && a.P == (B) && a.n == (A) * (B)) {                                        \
+    const size_t smem = pair_cols_rp_smem(a.n, RpShape<A, B>::YN, RpShape<A, B>::T, RpShape<A, B>::C, a.box); \
+    const void* fn = a.variant == 2 ? (const void*)k_pair_cols_rp<A, B, false> : (const void*)k_pair_cols_rp<A, B, true>; \
+    cudaError_t e = allow_smem(fn, smem);                                                    \
+    if (e != cudaSuccess) return e;                                                          \
+    if (a.variant == 2) k_pair_cols_rp<A, B, false><<<grid, kRegThreads, smem, st>>>(a);     \
+    else k_pair_cols_rp<A, B, true><<<grid, kRegThreads, smem, st>>>(a);                     \
+    return cudaGetLastError();                                                               \
+  }
+    MC_RP_LIST(MC_RP_LAUNCH)
+#undef MC_RP_LAUNCH
+  }
   if (pair_cols_reg_supported(a.P, a.Q)) {
     const int team = a.P <= 32 ? 32 : (a.P <= 64 ? 64 : 128);
     return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);

@@ -506,6 +506,10 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     a.twN = pl->d_twN;
     a.box = pl->box;
     a.ystart = pl->ystart;
+    // MC_PAIR_RP=0 selects the runtime-P register kernel over the compiled split,
+    // MC_PAIR_RP=2 the compiled split with table twiddles
+    a.variant = getenv("MC_PAIR_RP") ? std::min(2, std::max(0, atoi(getenv("MC_PAIR_RP")))) : 0;
+    if (a.variant == 0 && getenv("MC_PAIR_RP")) a.variant = 1;
     a.G = pl->d_G;
     // algorithmic bytes: every distinct spectrum the batch touches read once,
     // the column-stage output written once
@@ -848,7 +852,8 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   {
     const bool reg = mc::pair_cols_reg_supported(pl->P, pl->Q);
     const int team = pl->P <= 32 ? 32 : (pl->P <= 64 ? 64 : 128);
-    const size_t need = reg ? mc::pair_cols_reg_smem(pl->n, team) : mc::pair_cols_smem(pl->n, pl->P, pl->Q, pl->box) + 16;
+    const size_t need = std::max(mc::pair_cols_launch_smem(pl->n, pl->P, pl->Q, pl->box),
+                                 reg ? mc::pair_cols_reg_smem(pl->n, team) : (size_t)0);
     if (need > 227 * 1024) return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
     // grouped variant: A column + two B buffers per team (teams = 128 / team)
     const int gteam = pl->P <= 64 ? 64 : 128;
