@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
 }
 
 // the compiled (Q, P) splits of the tuned lengths: 3710, 4096, 2048, 1024
-#define MC_RP_LIST(X) X(35, 106) X(70, 53) X(64, 64) X(64, 32) X(32, 64) X(32, 32)
+#define MC_RP_LIST(X) X(35, 106) X(70, 53) X(64, 64) X(32, 128) X(64, 32) X(32, 64) X(16, 128) X(32, 32) X(16, 64)
 
 bool pair_cols_rp_supported(int P, int Q) {
 #define MC_RP_HAS(A, B) if (Q == (A) && P == (B)) return true;
