@@ -3,10 +3,31 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "f2ops.cuh"
+// MC_PACKED_FMA=1: the odd butterflies' sums on packed FP32 pairs (bitwise
+// the same results: each half is the scalar FMA chain)
+#ifndef MC_PACKED_FMA
+#define MC_PACKED_FMA 0
+#endif
 namespace mc {
 constexpr int kGeneratedOddRadices[] = {3, 5, 7, 11, 13, 53};
 template <bool INV> __device__ __forceinline__ void dft_r3(float2* v) {
   const float2 x0 = v[0];
+#if MC_PACKED_FMA
+  const f2reg S1 = f2pk(padd(v[1], v[2]));
+  const f2reg D1 = f2pk(psub(v[1], v[2]));
+  { float2 t = f2up(S1);
+    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.5f), A); B = f2fma(D1, f2splat(0.8660253882408142f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[1] = make_float2(a.x + b.y, a.y - b.x); v[2] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[1] = make_float2(a.x - b.y, a.y + b.x); v[2] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+#else
   const float2 s1 = padd(v[1], v[2]);
   const float2 d1 = psub(v[1], v[2]);
   v[0] = make_float2(x0.x + (s1.x), x0.y + (s1.y));
@@ -19,9 +40,41 @@ template <bool INV> __device__ __forceinline__ void dft_r3(float2* v) {
       v[1] = make_float2(ar - bi, ai + br); v[2] = make_float2(ar + bi, ai - br);
     }
   }
+#endif
 }
 template <bool INV> __device__ __forceinline__ void dft_r5(float2* v) {
   const float2 x0 = v[0];
+#if MC_PACKED_FMA
+  const f2reg S1 = f2pk(padd(v[1], v[4]));
+  const f2reg D1 = f2pk(psub(v[1], v[4]));
+  const f2reg S2 = f2pk(padd(v[2], v[3]));
+  const f2reg D2 = f2pk(psub(v[2], v[3]));
+  { float2 t = f2up(S1);
+    { const float2 u = f2up(S2); t.x += u.x; t.y += u.y; }
+    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.30901700258255005f), A); B = f2fma(D1, f2splat(0.9510565400123596f), B);
+    A = f2fma(S2, f2splat(-0.80901700258255f), A); B = f2fma(D2, f2splat(0.5877852439880371f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[1] = make_float2(a.x + b.y, a.y - b.x); v[4] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[1] = make_float2(a.x - b.y, a.y + b.x); v[4] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.80901700258255f), A); B = f2fma(D1, f2splat(0.5877852439880371f), B);
+    A = f2fma(S2, f2splat(0.30901700258255005f), A); B = f2fma(D2, f2splat(-0.9510565400123596f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[2] = make_float2(a.x + b.y, a.y - b.x); v[3] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[2] = make_float2(a.x - b.y, a.y + b.x); v[3] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+#else
   const float2 s1 = padd(v[1], v[4]);
   const float2 d1 = psub(v[1], v[4]);
   const float2 s2 = padd(v[2], v[3]);
@@ -47,9 +100,58 @@ template <bool INV> __device__ __forceinline__ void dft_r5(float2* v) {
       v[2] = make_float2(ar - bi, ai + br); v[3] = make_float2(ar + bi, ai - br);
     }
   }
+#endif
 }
 template <bool INV> __device__ __forceinline__ void dft_r7(float2* v) {
   const float2 x0 = v[0];
+#if MC_PACKED_FMA
+  const f2reg S1 = f2pk(padd(v[1], v[6]));
+  const f2reg D1 = f2pk(psub(v[1], v[6]));
+  const f2reg S2 = f2pk(padd(v[2], v[5]));
+  const f2reg D2 = f2pk(psub(v[2], v[5]));
+  const f2reg S3 = f2pk(padd(v[3], v[4]));
+  const f2reg D3 = f2pk(psub(v[3], v[4]));
+  { float2 t = f2up(S1);
+    { const float2 u = f2up(S2); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S3); t.x += u.x; t.y += u.y; }
+    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.6234897971153259f), A); B = f2fma(D1, f2splat(0.7818315029144287f), B);
+    A = f2fma(S2, f2splat(-0.22252093255519867f), A); B = f2fma(D2, f2splat(0.9749279022216797f), B);
+    A = f2fma(S3, f2splat(-0.9009688496589661f), A); B = f2fma(D3, f2splat(0.4338837265968323f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[1] = make_float2(a.x + b.y, a.y - b.x); v[6] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[1] = make_float2(a.x - b.y, a.y + b.x); v[6] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.22252093255519867f), A); B = f2fma(D1, f2splat(0.9749279022216797f), B);
+    A = f2fma(S2, f2splat(-0.9009688496589661f), A); B = f2fma(D2, f2splat(-0.4338837265968323f), B);
+    A = f2fma(S3, f2splat(0.6234897971153259f), A); B = f2fma(D3, f2splat(-0.7818315029144287f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[2] = make_float2(a.x + b.y, a.y - b.x); v[5] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[2] = make_float2(a.x - b.y, a.y + b.x); v[5] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.9009688496589661f), A); B = f2fma(D1, f2splat(0.4338837265968323f), B);
+    A = f2fma(S2, f2splat(0.6234897971153259f), A); B = f2fma(D2, f2splat(-0.7818315029144287f), B);
+    A = f2fma(S3, f2splat(-0.22252093255519867f), A); B = f2fma(D3, f2splat(0.9749279022216797f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[3] = make_float2(a.x + b.y, a.y - b.x); v[4] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[3] = make_float2(a.x - b.y, a.y + b.x); v[4] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+#else
   const float2 s1 = padd(v[1], v[6]);
   const float2 d1 = psub(v[1], v[6]);
   const float2 s2 = padd(v[2], v[5]);
@@ -90,9 +192,98 @@ template <bool INV> __device__ __forceinline__ void dft_r7(float2* v) {
       v[3] = make_float2(ar - bi, ai + br); v[4] = make_float2(ar + bi, ai - br);
     }
   }
+#endif
 }
 template <bool INV> __device__ __forceinline__ void dft_r11(float2* v) {
   const float2 x0 = v[0];
+#if MC_PACKED_FMA
+  const f2reg S1 = f2pk(padd(v[1], v[10]));
+  const f2reg D1 = f2pk(psub(v[1], v[10]));
+  const f2reg S2 = f2pk(padd(v[2], v[9]));
+  const f2reg D2 = f2pk(psub(v[2], v[9]));
+  const f2reg S3 = f2pk(padd(v[3], v[8]));
+  const f2reg D3 = f2pk(psub(v[3], v[8]));
+  const f2reg S4 = f2pk(padd(v[4], v[7]));
+  const f2reg D4 = f2pk(psub(v[4], v[7]));
+  const f2reg S5 = f2pk(padd(v[5], v[6]));
+  const f2reg D5 = f2pk(psub(v[5], v[6]));
+  { float2 t = f2up(S1);
+    { const float2 u = f2up(S2); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S3); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S4); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S5); t.x += u.x; t.y += u.y; }
+    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.8412535190582275f), A); B = f2fma(D1, f2splat(0.5406408309936523f), B);
+    A = f2fma(S2, f2splat(0.4154150187969208f), A); B = f2fma(D2, f2splat(0.9096319675445557f), B);
+    A = f2fma(S3, f2splat(-0.1423148363828659f), A); B = f2fma(D3, f2splat(0.9898214340209961f), B);
+    A = f2fma(S4, f2splat(-0.6548607349395752f), A); B = f2fma(D4, f2splat(0.7557495832443237f), B);
+    A = f2fma(S5, f2splat(-0.9594929814338684f), A); B = f2fma(D5, f2splat(0.28173255920410156f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[1] = make_float2(a.x + b.y, a.y - b.x); v[10] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[1] = make_float2(a.x - b.y, a.y + b.x); v[10] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.4154150187969208f), A); B = f2fma(D1, f2splat(0.9096319675445557f), B);
+    A = f2fma(S2, f2splat(-0.6548607349395752f), A); B = f2fma(D2, f2splat(0.7557495832443237f), B);
+    A = f2fma(S3, f2splat(-0.9594929814338684f), A); B = f2fma(D3, f2splat(-0.28173255920410156f), B);
+    A = f2fma(S4, f2splat(-0.1423148363828659f), A); B = f2fma(D4, f2splat(-0.9898214340209961f), B);
+    A = f2fma(S5, f2splat(0.8412535190582275f), A); B = f2fma(D5, f2splat(-0.5406408309936523f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[2] = make_float2(a.x + b.y, a.y - b.x); v[9] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[2] = make_float2(a.x - b.y, a.y + b.x); v[9] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.1423148363828659f), A); B = f2fma(D1, f2splat(0.9898214340209961f), B);
+    A = f2fma(S2, f2splat(-0.9594929814338684f), A); B = f2fma(D2, f2splat(-0.28173255920410156f), B);
+    A = f2fma(S3, f2splat(0.4154150187969208f), A); B = f2fma(D3, f2splat(-0.9096319675445557f), B);
+    A = f2fma(S4, f2splat(0.8412535190582275f), A); B = f2fma(D4, f2splat(0.5406408309936523f), B);
+    A = f2fma(S5, f2splat(-0.6548607349395752f), A); B = f2fma(D5, f2splat(0.7557495832443237f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[3] = make_float2(a.x + b.y, a.y - b.x); v[8] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[3] = make_float2(a.x - b.y, a.y + b.x); v[8] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.6548607349395752f), A); B = f2fma(D1, f2splat(0.7557495832443237f), B);
+    A = f2fma(S2, f2splat(-0.1423148363828659f), A); B = f2fma(D2, f2splat(-0.9898214340209961f), B);
+    A = f2fma(S3, f2splat(0.8412535190582275f), A); B = f2fma(D3, f2splat(0.5406408309936523f), B);
+    A = f2fma(S4, f2splat(-0.9594929814338684f), A); B = f2fma(D4, f2splat(0.28173255920410156f), B);
+    A = f2fma(S5, f2splat(0.4154150187969208f), A); B = f2fma(D5, f2splat(-0.9096319675445557f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[4] = make_float2(a.x + b.y, a.y - b.x); v[7] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[4] = make_float2(a.x - b.y, a.y + b.x); v[7] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.9594929814338684f), A); B = f2fma(D1, f2splat(0.28173255920410156f), B);
+    A = f2fma(S2, f2splat(0.8412535190582275f), A); B = f2fma(D2, f2splat(-0.5406408309936523f), B);
+    A = f2fma(S3, f2splat(-0.6548607349395752f), A); B = f2fma(D3, f2splat(0.7557495832443237f), B);
+    A = f2fma(S4, f2splat(0.4154150187969208f), A); B = f2fma(D4, f2splat(-0.9096319675445557f), B);
+    A = f2fma(S5, f2splat(-0.1423148363828659f), A); B = f2fma(D5, f2splat(0.9898214340209961f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[5] = make_float2(a.x + b.y, a.y - b.x); v[6] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[5] = make_float2(a.x - b.y, a.y + b.x); v[6] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+#else
   const float2 s1 = padd(v[1], v[10]);
   const float2 d1 = psub(v[1], v[10]);
   const float2 s2 = padd(v[2], v[9]);
@@ -169,9 +360,121 @@ template <bool INV> __device__ __forceinline__ void dft_r11(float2* v) {
       v[5] = make_float2(ar - bi, ai + br); v[6] = make_float2(ar + bi, ai - br);
     }
   }
+#endif
 }
 template <bool INV> __device__ __forceinline__ void dft_r13(float2* v) {
   const float2 x0 = v[0];
+#if MC_PACKED_FMA
+  const f2reg S1 = f2pk(padd(v[1], v[12]));
+  const f2reg D1 = f2pk(psub(v[1], v[12]));
+  const f2reg S2 = f2pk(padd(v[2], v[11]));
+  const f2reg D2 = f2pk(psub(v[2], v[11]));
+  const f2reg S3 = f2pk(padd(v[3], v[10]));
+  const f2reg D3 = f2pk(psub(v[3], v[10]));
+  const f2reg S4 = f2pk(padd(v[4], v[9]));
+  const f2reg D4 = f2pk(psub(v[4], v[9]));
+  const f2reg S5 = f2pk(padd(v[5], v[8]));
+  const f2reg D5 = f2pk(psub(v[5], v[8]));
+  const f2reg S6 = f2pk(padd(v[6], v[7]));
+  const f2reg D6 = f2pk(psub(v[6], v[7]));
+  { float2 t = f2up(S1);
+    { const float2 u = f2up(S2); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S3); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S4); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S5); t.x += u.x; t.y += u.y; }
+    { const float2 u = f2up(S6); t.x += u.x; t.y += u.y; }
+    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.8854560256004333f), A); B = f2fma(D1, f2splat(0.4647231698036194f), B);
+    A = f2fma(S2, f2splat(0.5680647492408752f), A); B = f2fma(D2, f2splat(0.8229838609695435f), B);
+    A = f2fma(S3, f2splat(0.1205366775393486f), A); B = f2fma(D3, f2splat(0.9927088618278503f), B);
+    A = f2fma(S4, f2splat(-0.35460489988327026f), A); B = f2fma(D4, f2splat(0.9350162148475647f), B);
+    A = f2fma(S5, f2splat(-0.7485107779502869f), A); B = f2fma(D5, f2splat(0.6631226539611816f), B);
+    A = f2fma(S6, f2splat(-0.9709418416023254f), A); B = f2fma(D6, f2splat(0.23931565880775452f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[1] = make_float2(a.x + b.y, a.y - b.x); v[12] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[1] = make_float2(a.x - b.y, a.y + b.x); v[12] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.5680647492408752f), A); B = f2fma(D1, f2splat(0.8229838609695435f), B);
+    A = f2fma(S2, f2splat(-0.35460489988327026f), A); B = f2fma(D2, f2splat(0.9350162148475647f), B);
+    A = f2fma(S3, f2splat(-0.9709418416023254f), A); B = f2fma(D3, f2splat(0.23931565880775452f), B);
+    A = f2fma(S4, f2splat(-0.7485107779502869f), A); B = f2fma(D4, f2splat(-0.6631226539611816f), B);
+    A = f2fma(S5, f2splat(0.1205366775393486f), A); B = f2fma(D5, f2splat(-0.9927088618278503f), B);
+    A = f2fma(S6, f2splat(0.8854560256004333f), A); B = f2fma(D6, f2splat(-0.4647231698036194f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[2] = make_float2(a.x + b.y, a.y - b.x); v[11] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[2] = make_float2(a.x - b.y, a.y + b.x); v[11] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(0.1205366775393486f), A); B = f2fma(D1, f2splat(0.9927088618278503f), B);
+    A = f2fma(S2, f2splat(-0.9709418416023254f), A); B = f2fma(D2, f2splat(0.23931565880775452f), B);
+    A = f2fma(S3, f2splat(-0.35460489988327026f), A); B = f2fma(D3, f2splat(-0.9350162148475647f), B);
+    A = f2fma(S4, f2splat(0.8854560256004333f), A); B = f2fma(D4, f2splat(-0.4647231698036194f), B);
+    A = f2fma(S5, f2splat(0.5680647492408752f), A); B = f2fma(D5, f2splat(0.8229838609695435f), B);
+    A = f2fma(S6, f2splat(-0.7485107779502869f), A); B = f2fma(D6, f2splat(0.6631226539611816f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[3] = make_float2(a.x + b.y, a.y - b.x); v[10] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[3] = make_float2(a.x - b.y, a.y + b.x); v[10] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.35460489988327026f), A); B = f2fma(D1, f2splat(0.9350162148475647f), B);
+    A = f2fma(S2, f2splat(-0.7485107779502869f), A); B = f2fma(D2, f2splat(-0.6631226539611816f), B);
+    A = f2fma(S3, f2splat(0.8854560256004333f), A); B = f2fma(D3, f2splat(-0.4647231698036194f), B);
+    A = f2fma(S4, f2splat(0.1205366775393486f), A); B = f2fma(D4, f2splat(0.9927088618278503f), B);
+    A = f2fma(S5, f2splat(-0.9709418416023254f), A); B = f2fma(D5, f2splat(-0.23931565880775452f), B);
+    A = f2fma(S6, f2splat(0.5680647492408752f), A); B = f2fma(D6, f2splat(-0.8229838609695435f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[4] = make_float2(a.x + b.y, a.y - b.x); v[9] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[4] = make_float2(a.x - b.y, a.y + b.x); v[9] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.7485107779502869f), A); B = f2fma(D1, f2splat(0.6631226539611816f), B);
+    A = f2fma(S2, f2splat(0.1205366775393486f), A); B = f2fma(D2, f2splat(-0.9927088618278503f), B);
+    A = f2fma(S3, f2splat(0.5680647492408752f), A); B = f2fma(D3, f2splat(0.8229838609695435f), B);
+    A = f2fma(S4, f2splat(-0.9709418416023254f), A); B = f2fma(D4, f2splat(-0.23931565880775452f), B);
+    A = f2fma(S5, f2splat(0.8854560256004333f), A); B = f2fma(D5, f2splat(-0.4647231698036194f), B);
+    A = f2fma(S6, f2splat(-0.35460489988327026f), A); B = f2fma(D6, f2splat(0.9350162148475647f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[5] = make_float2(a.x + b.y, a.y - b.x); v[8] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[5] = make_float2(a.x - b.y, a.y + b.x); v[8] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+  {
+    f2reg A = f2pk(x0), B = 0ull;
+    A = f2fma(S1, f2splat(-0.9709418416023254f), A); B = f2fma(D1, f2splat(0.23931565880775452f), B);
+    A = f2fma(S2, f2splat(0.8854560256004333f), A); B = f2fma(D2, f2splat(-0.4647231698036194f), B);
+    A = f2fma(S3, f2splat(-0.7485107779502869f), A); B = f2fma(D3, f2splat(0.6631226539611816f), B);
+    A = f2fma(S4, f2splat(0.5680647492408752f), A); B = f2fma(D4, f2splat(-0.8229838609695435f), B);
+    A = f2fma(S5, f2splat(-0.35460489988327026f), A); B = f2fma(D5, f2splat(0.9350162148475647f), B);
+    A = f2fma(S6, f2splat(0.1205366775393486f), A); B = f2fma(D6, f2splat(-0.9927088618278503f), B);
+    const float2 a = f2up(A), b = f2up(B);
+    if (!INV) {
+      v[6] = make_float2(a.x + b.y, a.y - b.x); v[7] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      v[6] = make_float2(a.x - b.y, a.y + b.x); v[7] = make_float2(a.x + b.y, a.y - b.x);
+    }
+  }
+#else
   const float2 s1 = padd(v[1], v[12]);
   const float2 d1 = psub(v[1], v[12]);
   const float2 s2 = padd(v[2], v[11]);
@@ -269,6 +572,7 @@ template <bool INV> __device__ __forceinline__ void dft_r13(float2* v) {
       v[6] = make_float2(ar - bi, ai + br); v[7] = make_float2(ar + bi, ai - br);
     }
   }
+#endif
 }
 template <bool INV> __device__ __forceinline__ void dft_r53(float2* v) {
   const float2 x0 = v[0];

@@ -30,6 +30,35 @@ def emit_odd(R: int) -> str:
     L = []
     L.append(f"template <bool INV> __device__ __forceinline__ void dft_r{R}(float2* v) {{")
     L.append("  const float2 x0 = v[0];")
+    if R < 53:
+        # MC_PACKED_FMA=1: the cosine and sine sums on packed FP32 pairs, one
+        # fma.f32x2 per term for the real and imaginary halves
+        L.append("#if MC_PACKED_FMA")
+        for n in range(1, h + 1):
+            L.append(f"  const f2reg S{n} = f2pk(padd(v[{n}], v[{R-n}]));")
+            L.append(f"  const f2reg D{n} = f2pk(psub(v[{n}], v[{R-n}]));")
+        sx = " + ".join([f"v[{n}].x + v[{R-n}].x" for n in range(1, h + 1)])
+        sy = " + ".join([f"v[{n}].y + v[{R-n}].y" for n in range(1, h + 1)])
+        L.append(f"  {{ float2 t = f2up(S1);")
+        for n in range(2, h + 1):
+            L.append(f"    {{ const float2 u = f2up(S{n}); t.x += u.x; t.y += u.y; }}")
+        L.append("    v[0] = make_float2(x0.x + t.x, x0.y + t.y); }")
+        for k in range(1, h + 1):
+            L.append("  {")
+            L.append("    f2reg A = f2pk(x0), B = 0ull;")
+            for n in range(1, h + 1):
+                m = (n * k) % R
+                c = flit(math.cos(2.0 * math.pi * m / R))
+                s = flit(math.sin(2.0 * math.pi * m / R))
+                L.append(f"    A = f2fma(S{n}, f2splat({c}), A); B = f2fma(D{n}, f2splat({s}), B);")
+            L.append("    const float2 a = f2up(A), b = f2up(B);")
+            L.append("    if (!INV) {")
+            L.append(f"      v[{k}] = make_float2(a.x + b.y, a.y - b.x); v[{R-k}] = make_float2(a.x - b.y, a.y + b.x);")
+            L.append("    } else {")
+            L.append(f"      v[{k}] = make_float2(a.x - b.y, a.y + b.x); v[{R-k}] = make_float2(a.x + b.y, a.y - b.x);")
+            L.append("    }")
+            L.append("  }")
+        L.append("#else")
     for n in range(1, h + 1):
         L.append(f"  const float2 s{n} = padd(v[{n}], v[{R-n}]);")
         L.append(f"  const float2 d{n} = psub(v[{n}], v[{R-n}]);")
@@ -52,6 +81,8 @@ def emit_odd(R: int) -> str:
         L.append(f"      v[{k}] = make_float2(ar - bi, ai + br); v[{R-k}] = make_float2(ar + bi, ai - br);")
         L.append("    }")
         L.append("  }")
+    if R < 53:
+        L.append("#endif")
     L.append("}")
     return "\n".join(L)
 
@@ -257,6 +288,11 @@ def main() -> None:
         out.append("#pragma once")
         out.append("#include <cuda_runtime.h>")
         out.append('#include "f2ops.cuh"')
+        out.append("// MC_PACKED_FMA=1: the odd butterflies' sums on packed FP32 pairs (bitwise")
+        out.append("// the same results: each half is the scalar FMA chain)")
+        out.append("#ifndef MC_PACKED_FMA")
+        out.append("#define MC_PACKED_FMA 0")
+        out.append("#endif")
         out.append("namespace mc {")
         out.append(f"constexpr int kGeneratedOddRadices[] = {{{', '.join(map(str, ODD_RADICES))}}};")
         for R in ODD_RADICES:

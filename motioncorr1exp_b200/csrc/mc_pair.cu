@@ -3,6 +3,10 @@
 // along kx onto the pbx window (cufunc.cu:229-233, 404-407).
 #include <algorithm>
 
+// The column stage's Q-point codelets use packed FP32 FMAs in their odd-radix
+// butterflies (bitwise the scalar results; 3 % faster here, while the
+// forward kernels' 70-point codelets spill more with them).
+#define MC_PACKED_FMA 1
 #include "kcommon.cuh"
 
 namespace mc {
@@ -173,47 +177,56 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
 
 // ---- split n = P x Q fixed at compile time ----------------------------------
 // The gather reads the stride-P subsequence at immediate offsets.  The outer
-// sum is blocked by residue: the output rows m with (ystart + m) mod Q = r all
-// read row r of Y, so a thread takes one residue r and one chunk of k1 and
-// keeps the up to JB rows m0(r) + j Q in registers (one shared-memory load of
-// Y feeds 4 JB FMAs; the twiddle loads of a warp stay on consecutive m).  The
-// chunk partials go to shared memory and are added in chunk order.
+// sum out[m] = sum_k1 Y[r(m)][k1] W^(k1 y_m), r(m) = (ystart + m) mod Q, runs
+// as items (output row m, chunk of at most 16 k1): Horner's rule from the
+// chunk's last term down, acc = acc w + Y with w = W^(y_m) (4 FMAs per term,
+// no twiddle loads; the powers of the rounded w drift by ~1e-6 over a chunk),
+// then one multiply by W^(kb y_m).  Consecutive threads take consecutive rows
+// m, so their Y rows (odd stride in float2) fall on different bank pairs and
+// their twiddle loads are contiguous.  The chunk partials meet in shared
+// memory and are added in chunk order.
 template <int Q, int P>
 struct RpShape {
-  static constexpr int T = P <= 32 ? 32 : (P <= 64 ? 64 : 128);     // team threads
-  static constexpr int C = (2 * T) / Q > 1 ? (2 * T) / Q : 1;        // k1 chunks
-  static constexpr int L = (P + C - 1) / C;                          // chunk length
-  static constexpr int JB = Q >= 96 ? 1 : (Q >= 48 ? 2 : 3);         // rows per residue block
-  // Y row stride: odd in float2 units, so the rows read by 16 consecutive
-  // residues fall on 16 different bank pairs
-  static constexpr int PS = P | 1;
+  static constexpr int T = P <= 32 ? 32 : (P <= 64 ? 64 : 128);  // team threads
+  static constexpr int W = T / 32;                                // chunk count granule
+  static constexpr int C = ((P + 15) / 16 + W - 1) / W * W;       // k1 chunks (96 C / T whole)
+  static constexpr int L = (P + C - 1) / C;                       // chunk length <= 16
+  static constexpr int PS = P | 1;                                // odd Y row stride (float2)
   static constexpr int YN = Q * PS;
 };
 
 size_t pair_cols_rp_smem(int n, int yn, int team, int chunks, int box) {
   const int teams = kRegThreads / team;
-  return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)teams * ((size_t)yn + (size_t)chunks * box) * sizeof(float2);
+  return (size_t)((n + 1) / 2) * sizeof(float2) + (size_t)(chunks + 1) * box * sizeof(float2) +
+         (size_t)teams * ((size_t)yn + (size_t)chunks * box) * sizeof(float2);
 }
 
-// REC: the twiddles of a chunk by recurrence in registers, t(k+1) = t(k) W^y
-// from t(kb) = twO[kb][m] and W^y = twO[1][m] (a chunk is at most 16 steps,
-// so the product drifts by ~1e-6); else each twiddle is loaded from twO.
-template <int Q, int P, bool REC>
+// HORNER = false: each twiddle W^(k1 y_m) loaded from twO (the measured
+// slower form, kept for comparison).
+template <int Q, int P, bool HORNER>
 __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_cols_rp(PairColsArgs a) {
   using S = RpShape<Q, P>;
-  constexpr int T = S::T, C = S::C, L = S::L, JB = S::JB, N = P * Q, PS = S::PS, YN = S::YN;
+  constexpr int T = S::T, C = S::C, L = S::L, N = P * Q, PS = S::PS, YN = S::YN;
   extern __shared__ float2 sm[];
   const int box = a.box;
   float* wcol = reinterpret_cast<float*>(sm);
+  // twiddle rows the sums need: tws[0][m] = W^(y_m) (twO row 1), tws[1 + c][m]
+  // = W^(kb(c) y_m) (twO row c L)
+  float2* tws = sm + (N + 1) / 2;
   constexpr int teams = kRegThreads / T;
   const int tid = threadIdx.x;
   const int tm = tid / T, lt = tid - tm * T;
-  float2* Y = sm + (N + 1) / 2 + (size_t)tm * (YN + C * box);
+  float2* Y = tws + (C + 1) * box + (size_t)tm * (YN + C * box);
   float2* part = Y + YN;
   const int kx = blockIdx.y;
   for (int ky = tid; ky < N; ky += kRegThreads) {
     const int y = ky < N / 2 ? ky : ky - N;
     wcol[ky] = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
+  }
+  for (int i = tid; i < (C + 1) * box; i += kRegThreads) {
+    const int row = i / box, m = i - row * box;
+    const int k = row == 0 ? 1 : min((row - 1) * L, P - 1);
+    tws[i] = __ldg(a.twO + (long long)k * box + m);
   }
   __syncthreads();
   const int ys = a.ystart % Q;
@@ -233,45 +246,49 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
       for (int r = 0; r < Q; r++) Y[lt + PS * r] = x[r];
     }
     team_barrier(1 + tm, T);
-    for (int it = lt; it < Q * C; it += T) {
-      const int r = it % Q, c = it / Q;
-      const int m0 = (r - ys + Q) % Q;  // first row with (ystart + m) mod Q = r
+    int c = lt / box, m = lt - (lt / box) * box;
+    for (int it = lt; it < box * C; it += T) {
+      int r = ys + m % Q;
+      if (r >= Q) r -= Q;
       const int kb = c * L;
       const float2* yr = Y + PS * r + kb;
-      for (int j0 = 0; m0 + j0 * Q < box; j0 += JB) {
-        float2 acc[JB];
+      float2 acc = make_float2(0.f, 0.f);
+      if (HORNER) {
+        // two independent chains over the even and odd terms in w^2, then
+        // S = S_even + w S_odd: twice the instruction-level parallelism of
+        // one chain of dependent FMAs
+        const float2 w = tws[m];
+        const float2 w2 = cmul(w, w);
+        float2 ae = make_float2(0.f, 0.f), ao = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < JB; j++) acc[j] = make_float2(0.f, 0.f);
-        bool on[JB];
-#pragma unroll
-        for (int j = 0; j < JB; j++) on[j] = m0 + (j0 + j) * Q < box;
-        const float2* tw = a.twO + (long long)kb * box + m0 + j0 * Q;
-        float2 tr[JB], wr[JB];
-        if (REC) {
-#pragma unroll
-          for (int j = 0; j < JB; j++) {
-            tr[j] = on[j] ? __ldg(tw + j * Q) : make_float2(0.f, 0.f);
-            wr[j] = on[j] ? __ldg(a.twO + box + m0 + (j0 + j) * Q) : make_float2(0.f, 0.f);
+        for (int kk = L - 1; kk >= 0; kk--) {
+          if (L * C == P || kb + kk < P) {
+            const float2 yv = yr[kk];
+            float2& h = (kk & 1) ? ao : ae;
+            const float2 s = h;
+            h.x = fmaf(s.x, w2.x, fmaf(-s.y, w2.y, yv.x));
+            h.y = fmaf(s.x, w2.y, fmaf(s.y, w2.x, yv.y));
           }
         }
+        acc.x = fmaf(ao.x, w.x, fmaf(-ao.y, w.y, ae.x));
+        acc.y = fmaf(ao.x, w.y, fmaf(ao.y, w.x, ae.y));
+        if (kb < P) acc = cmul(acc, tws[(1 + c) * box + m]);
+      } else {
 #pragma unroll
         for (int kk = 0; kk < L; kk++) {
           if (L * C == P || kb + kk < P) {
+            const float2 t = __ldg(a.twO + (long long)(kb + kk) * box + m);
             const float2 yv = yr[kk];
-#pragma unroll
-            for (int j = 0; j < JB; j++) {
-              if (on[j]) {
-                const float2 t = REC ? tr[j] : __ldg(tw + (long long)kk * box + j * Q);
-                acc[j].x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc[j].x));
-                acc[j].y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc[j].y));
-                if (REC) tr[j] = cmul(t, wr[j]);
-              }
-            }
+            acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
+            acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
           }
         }
-#pragma unroll
-        for (int j = 0; j < JB; j++)
-          if (on[j]) part[c * box + m0 + (j0 + j) * Q] = acc[j];
+      }
+      part[c * box + m] = acc;
+      m += T;
+      while (m >= box) {
+        m -= box;
+        c++;
       }
     }
     team_barrier(1 + tm, T);

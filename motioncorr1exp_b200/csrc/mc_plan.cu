@@ -327,6 +327,12 @@ struct mc_plan {
   std::vector<GraphEntry> graphs;
   bool graph_failed = false;
   bool capturing = false;
+  // forward transforms of independent frames on kForwardStreams forked
+  // streams (parallel branches in a captured movie), so one frame's last
+  // partial wave of CTAs overlaps the next frames' work
+  static constexpr int kForwardStreams = 4;
+  cudaStream_t fst[kForwardStreams] = {};
+  cudaEvent_t fev[kForwardStreams + 1] = {};
   int maxp = 0;
   std::vector<void*> allocs;
 
@@ -443,6 +449,10 @@ struct mc_plan {
       if (e) cudaEventDestroy(e);
     for (auto& g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& s : fst)
+      if (s) cudaStreamDestroy(s);
+    for (auto& e : fev)
+      if (e) cudaEventDestroy(e);
     if (h_stage) cudaFreeHost(h_stage);
     for (auto& e : kpool) cudaEventDestroy(e);
     for (auto& e : chunk_ev) cudaEventDestroy(e);
@@ -1166,8 +1176,24 @@ static bool device_path(const mc_plan* pl);
 // upload); the per-frame means are read back and logged at the end.
 static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
   const bool binned = pl->nu != pl->n;
+  // frames write only their own spectrum slots unless a shared scratch is in
+  // play (binning's row buffer, the stretched frame); per-launch timing
+  // events need the one stream
+  const bool multi = !binned && !pl->stretch && pl->nframe > 1 && !(pl->profiling && !pl->capturing) &&
+                     !getenv("MC_FORWARD_ONE_STREAM");
+  constexpr int NS = mc_plan::kForwardStreams;
+  if (multi) {
+    for (int i = 0; i < NS; i++) {
+      if (!pl->fst[i]) CK(cudaStreamCreateWithFlags(&pl->fst[i], cudaStreamNonBlocking));
+      if (!pl->fev[i]) CK(cudaEventCreateWithFlags(&pl->fev[i], cudaEventDisableTiming));
+    }
+    if (!pl->fev[NS]) CK(cudaEventCreateWithFlags(&pl->fev[NS], cudaEventDisableTiming));
+    CK(cudaEventRecord(pl->fev[NS], pl->st));
+    for (int i = 0; i < NS; i++) CK(cudaStreamWaitEvent(pl->fst[i], pl->fev[NS], 0));
+  }
   for (int f = 0; f < pl->nframe; f++) {
-    if (waits && f % chunk == 0) CK(cudaStreamWaitEvent(pl->st, (*waits)[f / chunk], 0));
+    cudaStream_t fs = multi ? pl->fst[f % NS] : pl->st;
+    if (waits && (multi || f % chunk == 0)) CK(cudaStreamWaitEvent(fs, (*waits)[f / chunk], 0));
     mc::FwdRowsArgs a{};
     a.frame = (const char*)(pl->frames_src ? pl->frames_src : pl->d_frames) + (size_t)f * pl->frame_bytes;
     a.frames_slot = pl->d_src_slot;
@@ -1176,7 +1202,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
       // the crop of this frame through the stretch maps, then transformed from there
       LAUNCH(pl, MC_K_FWD_ROWS, 2.0 * pl->nu * pl->nu * pl->wl,
              mc::launch_stretch_crop(pl->d_src_slot, a.frame_offset, a.frame, pl->wl, pl->d_sframe, pl->d_rmap,
-                                     pl->d_cmap, pl->nx, pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu, pl->st));
+                                     pl->d_cmap, pl->nx, pl->p.crop_offsetx, pl->p.crop_offsety, pl->nu, fs));
       a.frame = pl->d_sframe;
       a.frames_slot = nullptr;
       a.frame_offset = 0;
@@ -1216,7 +1242,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
         b.dark2 = nullptr;
         b.norm2 = nullptr;
         b.outA = pl->d_T;
-        LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes, mc::launch_fwd_rows(b, pl->st));
+        LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes, mc::launch_fwd_rows(b, fs));
         mc::RowsFftArgs c{};
         c.in = pl->d_T;
         c.ld_in = pl->ldu;
@@ -1228,12 +1254,12 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
         c.scale = 1.f;
         c.plan = pl->plan_nu;
         c.tw = pl->d_tw_nu;
-        LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, pl->st));
+        LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, fs));
       }
       continue;
     }
     a.outB = TB;
-    LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes * (pl->two_sets ? 2 : 1), mc::launch_fwd_rows(a, pl->st));
+    LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes * (pl->two_sets ? 2 : 1), mc::launch_fwd_rows(a, fs));
     for (int set = 0; set < (pl->two_sets ? 2 : 1); set++) {
       mc::RowsFftArgs c{};
       c.in = set == 0 ? TA : TB;
@@ -1246,9 +1272,14 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
       c.scale = 1.f;
       c.plan = pl->plan_nu;
       c.tw = pl->d_tw_nu;
-      LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, pl->st));
+      LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, fs));
     }
   }
+  if (multi)
+    for (int i = 0; i < NS; i++) {
+      CK(cudaEventRecord(pl->fev[i], pl->fst[i]));
+      CK(cudaStreamWaitEvent(pl->st, pl->fev[i], 0));
+    }
   return MC_OK;
 }
 
