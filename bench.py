@@ -317,6 +317,20 @@ def run_ours(args):
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": committed_traffic(dom) if args.workload == "c2" else None,
                 "peak_source": peak_kind, "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms}
+        if dom == "k_pair_cols":
+            # the kernel is FP32-issue bound: its compute roofline beside the
+            # HBM one.  Algorithmic FLOPs per (pair, column): the cross power
+            # x B-factor (8 n), P inverse FFTs of length Q (5 Q log2 Q each,
+            # the usual FFT count) and the 96-row P-term sums (8 P box)
+            info = plan.info
+            n, P, Q = plan.nsam, info["prune_p"], info["prune_q"]
+            per_pc = 8.0 * n + P * 5.0 * Q * np.log2(Q) + 8.0 * P * p.CCPeakSearchDim
+            flops = per_pc * plan.npairs * (n // 2 + 1)
+            fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+            roof["fp32"] = {"achieved": flops / (per_launch_ms / 1000.0) / 1e12, "peak": fp32_peak,
+                            "unit": "TFLOP/s", "frac": flops / (per_launch_ms / 1000.0) / 1e12 / fp32_peak,
+                            "flops_per_launch": flops,
+                            "peak_source": "nominal FP32 (non-tensor): 148 SMs x 128 lanes x 2 x 1.965 GHz"}
         # compulsory bytes of a whole movie: every frame read once and its
         # spectrum written once, every spectrum read by the pair stage and by
         # the sum (twice more per realignment iteration), the image written

@@ -91,6 +91,10 @@ struct PairRowsArgs {
   int npairs, H, box;
   const float2* cs;    // [H][box]
   float* boxes;        // [npairs][box][box]
+  // when set with a compiled split n = P*Q: the pruned-transform row kernel
+  // (twO and ystart as in PairColsArgs); variant 1 keeps the product kernel
+  const float2* twO;
+  int P, Q, ystart, variant;
 };
 
 // Peak: integer argmax over the box, 16x16 sub-box, x32 Fourier upsampling,

@@ -304,6 +304,127 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
   }
 }
 
+// ---- row stage with the same compiled split --------------------------------
+// box[p][yb][xb] = sum_kx h(kx) Re(G[p][kx][yb] exp(+2 pi i kx x_xb / n)) is
+// the length-n inverse DFT of the Hermitian extension of row yb (real parts
+// at kx = 0 and n/2, conj(G[n - kx]) above n/2), evaluated at the box's
+// columns.  Two rows ride in one complex sequence z = Ga + i Gb, so the real
+// and imaginary parts of the result are the two output rows.  A CTA stages
+// G[p][:, 2 teams rows] (coalesced, odd row stride), each team gathers its
+// row pair, runs the inverse Q-point codelet on the stride-P subsequences and
+// forms the box columns by the column stage's Horner sums.
+template <int Q, int P>
+__host__ __device__ __forceinline__ size_t pair_rows_rp_region(int H) {
+  using S = RpShape<Q, P>;
+  constexpr int teams = kRegThreads / S::T;
+  const size_t g = (size_t)H * (2 * teams + 1);
+  const size_t y = (size_t)teams * S::YN;
+  return g > y ? g : y;
+}
+
+template <int Q, int P>
+size_t pair_rows_rp_smem(int H, int box) {
+  using S = RpShape<Q, P>;
+  constexpr int teams = kRegThreads / S::T;
+  return (pair_rows_rp_region<Q, P>(H) + (size_t)(S::C + 1) * box + (size_t)teams * S::C * box) * sizeof(float2);
+}
+
+template <int Q, int P>
+__global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_rows_rp(PairRowsArgs a, const float2* __restrict__ twO,
+                                                                                        int ystart) {
+  using S = RpShape<Q, P>;
+  constexpr int T = S::T, C = S::C, L = S::L, N = P * Q, PS = S::PS;
+  constexpr int teams = kRegThreads / T, R = 2 * teams, RS = R + 1;
+  extern __shared__ float2 sm[];
+  const int box = a.box, H = a.H;
+  float2* reg = sm;                                    // staged G rows, then the teams' Y
+  float2* tws = sm + pair_rows_rp_region<Q, P>(H);
+  float2* part0 = tws + (C + 1) * box;
+  const int tid = threadIdx.x, tm = tid / T, lt = tid - tm * T;
+  const int p = blockIdx.x, yb0 = blockIdx.y * R;
+  const float2* G = a.G + (long long)p * H * box;
+  for (int i = tid; i < H * R; i += kRegThreads) {
+    const int kx = i / R, r = i - kx * R;
+    reg[kx * RS + r] = yb0 + r < box ? G[(long long)kx * box + yb0 + r] : make_float2(0.f, 0.f);
+  }
+  for (int i = tid; i < (C + 1) * box; i += kRegThreads) {
+    const int row = i / box, m = i - row * box;
+    const int k = row == 0 ? 1 : min((row - 1) * L, P - 1);
+    tws[i] = __ldg(twO + (long long)k * box + m);
+  }
+  __syncthreads();
+  float2 x[Q];
+  if (lt < P) {
+    const int ra = 2 * tm, rb = ra + 1;
+#pragma unroll
+    for (int k2 = 0; k2 < Q; k2++) {
+      const int kx = lt + P * k2;
+      float2 z;
+      if (kx == 0 || 2 * kx == N) {
+        z = make_float2(reg[kx * RS + ra].x, reg[kx * RS + rb].x);
+      } else if (2 * kx < N) {
+        const float2 ga = reg[kx * RS + ra], gb = reg[kx * RS + rb];
+        z = make_float2(ga.x - gb.y, ga.y + gb.x);
+      } else {
+        const int kr = N - kx;
+        const float2 ga = reg[kr * RS + ra], gb = reg[kr * RS + rb];
+        z = make_float2(ga.x + gb.y, gb.x - ga.y);
+      }
+      x[k2] = z;
+    }
+    fft_reg<Q, true>(x);
+  }
+  __syncthreads();  // every team has gathered: the staged rows give way to Y
+  float2* Y = reg + (size_t)tm * S::YN;
+  float2* part = part0 + (size_t)tm * C * box;
+  if (lt < P) {
+#pragma unroll
+    for (int r = 0; r < Q; r++) Y[lt + PS * r] = x[r];
+  }
+  team_barrier(1 + tm, T);
+  const int ys = ystart % Q;
+  int c = lt / box, m = lt - (lt / box) * box;
+  for (int it = lt; it < box * C; it += T) {
+    int r = ys + m % Q;
+    if (r >= Q) r -= Q;
+    const int kb = c * L;
+    const float2* yr = Y + PS * r + kb;
+    const float2 w = tws[m];
+    const float2 w2 = cmul(w, w);
+    float2 ae = make_float2(0.f, 0.f), ao = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int kk = L - 1; kk >= 0; kk--) {
+      if (L * C == P || kb + kk < P) {
+        const float2 yv = yr[kk];
+        float2& h = (kk & 1) ? ao : ae;
+        const float2 s = h;
+        h.x = fmaf(s.x, w2.x, fmaf(-s.y, w2.y, yv.x));
+        h.y = fmaf(s.x, w2.y, fmaf(s.y, w2.x, yv.y));
+      }
+    }
+    float2 acc;
+    acc.x = fmaf(ao.x, w.x, fmaf(-ao.y, w.y, ae.x));
+    acc.y = fmaf(ao.x, w.y, fmaf(ao.y, w.x, ae.y));
+    if (kb < P) acc = cmul(acc, tws[(1 + c) * box + m]);
+    else acc = make_float2(0.f, 0.f);
+    part[c * box + m] = acc;
+    m += T;
+    while (m >= box) {
+      m -= box;
+      c++;
+    }
+  }
+  team_barrier(1 + tm, T);
+  const int ya = yb0 + 2 * tm, yb = ya + 1;
+  for (int mm = lt; mm < box; mm += T) {
+    float2 s = part[mm];
+#pragma unroll
+    for (int cc = 1; cc < C; cc++) s = cadd(s, part[cc * box + mm]);
+    if (ya < box) a.boxes[((long long)p * box + ya) * box + mm] = s.x;
+    if (yb < box) a.boxes[((long long)p * box + yb) * box + mm] = s.y;
+  }
+}
+
 // the compiled (Q, P) splits of the tuned lengths: 3710, 4096, 2048, 1024
 #define MC_RP_LIST(X) X(35, 106) X(70, 53) X(64, 64) X(32, 128) X(64, 32) X(32, 64) X(16, 128) X(32, 32) X(16, 64)
 
@@ -559,6 +680,20 @@ __global__ void __launch_bounds__(kThreads) k_pair_rows(PairRowsArgs a) {
 }
 
 cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st) {
+  if (a.twO && a.variant == 0) {
+#define MC_RP_ROWS(A, B)                                                                            \
+  if (a.Q == (A) && a.P == (B) && 2 * (a.H - 1) == (A) * (B)) {                                    \
+    constexpr int rows = 2 * (kRegThreads / RpShape<A, B>::T);                                     \
+    const size_t smem = pair_rows_rp_smem<A, B>(a.H, a.box);                                       \
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;                                            \
+    cudaError_t e = allow_smem((const void*)k_pair_rows_rp<A, B>, smem);                           \
+    if (e != cudaSuccess) return e;                                                                 \
+    k_pair_rows_rp<A, B><<<dim3(a.npairs, (a.box + rows - 1) / rows), kRegThreads, smem, st>>>(a, a.twO, a.ystart); \
+    return cudaGetLastError();                                                                      \
+  }
+    MC_RP_LIST(MC_RP_ROWS)
+#undef MC_RP_ROWS
+  }
   k_pair_rows<<<a.npairs, kThreads, 0, st>>>(a);
   return cudaGetLastError();
 }

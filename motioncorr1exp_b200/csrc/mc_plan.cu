@@ -561,6 +561,12 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     r.box = pl->box;
     r.cs = pl->d_cs;
     r.boxes = pl->d_boxes + (long long)p0 * pl->box * pl->box;
+    r.twO = pl->d_twO;
+    r.P = pl->P;
+    r.Q = pl->Q;
+    r.ystart = pl->ystart;
+    // MC_PAIR_ROWS=0 keeps the dense product kernel
+    r.variant = (getenv("MC_PAIR_ROWS") && atoi(getenv("MC_PAIR_ROWS")) == 0) ? 1 : 0;
     LAUNCH(pl, MC_K_PAIR_ROWS,
            gbytes + (double)pl->H * pl->box * sizeof(float2) + (double)nb * pl->box * pl->box * sizeof(float),
            mc::launch_pair_rows(r, pl->st));
