@@ -303,7 +303,9 @@ def run_ours(args):
         step_e2e()
     single_e2e_ms, _ = timed(lambda: [step_e2e() for _ in range(args.steps)])
 
-    truth_rmse = float(np.sqrt(np.mean(np.sum((shifts + (truth - truth[0])) ** 2, axis=1))))
+    # shifts come in binned pixels (nsam / nsam_unbin of a raw pixel)
+    to_binned = plan.nsam / plan.info["nsam_unbin"]
+    truth_rmse = float(np.sqrt(np.mean(np.sum((shifts + to_binned * (truth - truth[0])) ** 2, axis=1))))
 
     if rank == 0:
         value = nz * args.steps * world / (ms_max / 1000.0)
