@@ -204,6 +204,28 @@ def compare_full(g, ref, n, nps, boxes=None):
     assert rel_l2(g["image"], ref.image) <= IMAGE_RTOL
 
 
+@pytest.mark.parametrize("n,box,nz", [(1024, 16, 8), (1024, 95, 8), (1024, 256, 6), (2048, 128, 6), (4096, 96, 5)])
+def test_pair_boxes_compiled_splits(gpu, n, box, nz):
+    """The pair kernels with the split n = P*Q compiled in (1024 = 32*32,
+    2048 = 32*64, 4096 = 64*64 under the tuned schedules): column-stage Horner
+    sums and the pruned-transform row stage at box sizes other than 96, odd
+    included, against the oracle's windows and peaks."""
+    mv = synth.make_movie(n + 4, n, nz, mean=1.0, seed=n + box, dtype="u8", speed=0.7, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=box, FrameDistOffset=1), nz)
+    with api.Plan(p, n + 4, n, nz, 0) as pl:
+        assert pl.info["prune_p"] * pl.info["prune_q"] == n and pl.info["prune_p"] <= 128
+        pl.load_frames(mv.frames)
+        pl.forward()
+        pl.pairs()
+        gb = pl.boxes()
+        gres = pl.pair_results()
+    ob, _, _ = oracle_boxes(mv.frames, 0, p)
+    for r in range(len(ob)):
+        assert rel_l2(gb[r], ob[r]) < 1e-5, r
+    ref = O.align_movie(mv.frames, 0, to_oparams(p))
+    check_pairs(gres, ref, n, p.NoisePeakSize, ob)
+
+
 def test_pipeline_c1_shape(gpu):
     """c1 geometry: 16 x 1024^2 float32, -fod 2 -bft 150 -pbx 96."""
     mv = synth.make_movie(1024, 1024, 16, mean=1.5, seed=11, dtype="f32", speed=0.4, rw_sigma=0.3)
