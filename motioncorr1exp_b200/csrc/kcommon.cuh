@@ -53,9 +53,10 @@ __device__ __forceinline__ void fft_n1(float2* v) {
 
 // Resident CTAs per SM the two-level transforms are compiled for (register cap).
 // MC_FWD_PAIRED / MC_COL_PAIRED: two radix-53 output pairs per loop iteration
-// in the forward row / column transforms.
+// in the forward row / column transforms (measured on c2: the row pass 9 %
+// faster with it, the column pass 27 % slower).
 #ifndef MC_FWD_PAIRED
-#define MC_FWD_PAIRED false
+#define MC_FWD_PAIRED true
 #endif
 #ifndef MC_COL_PAIRED
 #define MC_COL_PAIRED false
