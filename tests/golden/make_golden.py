@@ -1,11 +1,14 @@
-"""Regenerate the MRC golden fixtures with the reference's own MRC class.
+"""Regenerate the MRC golden fixtures with the reference's own MRC classes.
 
-Needs oracle/_ref/ref_mrc (oracle/build_ref.sh, reference tree present).
-Writes into tests/golden/:
-  ref_createMRC_17x13x2.mrc   bytes of MRC::createMRC(float*) for a known array
-  stack_mode{0,1,2,6}.mrc     small stacks (written by motioncorr1exp_b200.mrc)
-  ref_decode_mode{m}_f{k}.f32 MRC::read2DIm_32bit of frame k of each stack
+Needs oracle/_ref/ref_mrc and oracle/_ref/ref_mrcz (oracle/build_ref.sh,
+reference tree present).  Writes into tests/golden/:
+  ref_createMRC_17x13x2.mrc      bytes of MRC::createMRC(float*) for a known array
+  stack_mode{0,1,2,6}.mrc        small stacks (written by motioncorr1exp_b200.mrc)
+  ref_decode_mode{m}_f{k}.f32    MRC::read2DIm_32bit of frame k of each stack
+  stack_mode{0,1,2,6}.mrc.gz     the same stacks gzip-compressed (mtime 0)
+  ref_gz_decode_mode{m}_f{k}.f32 MRCZ's read2DIm_32bit of frame k (mrcz.cpp)
 """
+import gzip
 import os
 import subprocess
 import sys
@@ -19,6 +22,7 @@ sys.path.insert(0, ROOT)
 from motioncorr1exp_b200 import mrc  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "ref_mrc")
+REFZ = os.path.join(ROOT, "oracle", "_ref", "ref_mrcz")
 
 
 def image_array():
@@ -38,8 +42,8 @@ def stack_array(mode):
 
 
 def main():
-    if not os.path.exists(REF):
-        sys.exit("oracle/_ref/ref_mrc missing: run oracle/build_ref.sh")
+    if not os.path.exists(REF) or not os.path.exists(REFZ):
+        sys.exit("oracle/_ref/ref_mrc or ref_mrcz missing: run oracle/build_ref.sh")
     img = image_array()
     tmp = os.path.join(HERE, "_in.f32")
     img.tofile(tmp)
@@ -50,6 +54,12 @@ def main():
         mrc.write_stack(path, stack_array(mode), mode)
         for k in range(3):
             subprocess.run([REF, "read", path, str(k), os.path.join(HERE, f"ref_decode_mode{mode}_f{k}.f32")],
+                           check=True)
+        gz = path + ".gz"
+        with open(path, "rb") as f, open(gz, "wb") as g:
+            g.write(gzip.compress(f.read(), mtime=0))
+        for k in (2, 0, 1):  # a backward seek after the first read
+            subprocess.run([REFZ, "read", gz, str(k), os.path.join(HERE, f"ref_gz_decode_mode{mode}_f{k}.f32")],
                            check=True)
 
 
