@@ -1,8 +1,10 @@
 #!/usr/bin/env bash
 # Builds the parts of the reference that compile from their own sources into
-# oracle/_ref/ (git-ignored): the MRC class (mrc.cpp) and the MRC-gz reader
-# on top of it (mrcz.cpp, with zlib).  The alignment code needs FFTW3, SP++
-# 3.0 and libtiff, which are not installed, so it is not built here.
+# oracle/_ref/ (git-ignored): the MRC class (mrc.cpp), the MRC-gz reader on
+# top of it (mrcz.cpp, with zlib), and func.cpp against the stand-in FFTW and
+# libtiff headers of oracle/stubs/ (only its FFT-free functions are called).
+# The alignment code needs FFTW3, SP++ 3.0 and libtiff, which are not
+# installed, so it is not built here.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 SRC=/root/reference/src-1125
@@ -17,5 +19,9 @@ if [ ! -x "$OUT/ref_mrc" ] || [ "$HERE/ref_mrc_harness.cpp" -nt "$OUT/ref_mrc" ]
 fi
 if [ ! -x "$OUT/ref_mrcz" ] || [ "$HERE/ref_mrcz_harness.cpp" -nt "$OUT/ref_mrcz" ]; then
   g++ -O2 -w -I "$SRC" "$HERE/ref_mrcz_harness.cpp" "$SRC/mrc.cpp" "$SRC/mrcz.cpp" -lz -o "$OUT/ref_mrcz"
+fi
+if [ ! -x "$OUT/ref_func" ] || [ "$HERE/ref_func_harness.cpp" -nt "$OUT/ref_func" ]; then
+  g++ -O2 -w -I "$HERE/stubs" -I "$SRC" "$HERE/ref_func_harness.cpp" "$SRC/func.cpp" "$SRC/mrc.cpp" \
+      "$SRC/mrcz.cpp" -lz -lpthread -o "$OUT/ref_func"
 fi
 echo "$OUT/ref_mrc"

@@ -13,11 +13,14 @@ arithmetic is widened to FP64.
 
 Parity status: the reference publishes no tests, fixtures or golden vectors
 and its alignment code cannot be built here (it needs FFTW3, SP++ 3.0 and
-libtiff, none of which are installed).  The MRC decode/encode restatement is
-pinned against the reference's own ``mrc.cpp`` compiled by
-``oracle/build_ref.sh``; the alignment math is pinned only by project-written
-known-answer tests (brute-force DFTs, analytic peaks, exactly consistent
-shifts).  For the alignment math this oracle is therefore "parity unpinned".
+libtiff, none of which are installed).  Pinned against the reference's own
+code compiled by ``oracle/build_ref.sh`` (golden fixtures in tests/golden/):
+the MRC and MRC-gz decode/encode (``mrc.cpp``, ``mrcz.cpp``) and, through
+``func.cpp`` built against stand-in FFTW/libtiff headers, the crop size and
+crop, the sub-pixel cosine mask and the display contrast and layout.  The
+transforms, cross-correlation, peak search and least-squares solve are pinned
+only by project-written known-answer tests (brute-force DFTs, analytic peaks,
+exactly consistent shifts): for those this oracle is "parity unpinned".
 """
 from __future__ import annotations
 
@@ -440,19 +443,26 @@ def display_short(buf: np.ndarray) -> np.ndarray:
     return out
 
 
-def modulus_display(F: np.ndarray, scale: float = 1e-4) -> np.ndarray:
-    """cuFFTLogModulus (cufunc.cu:178-188) + FFTModulusToDispBuf
-    (func.cpp:459-489): log(1 + |F| scale) as the centred n x n image."""
-    n = F.shape[0]
+def modulus_layout(L: np.ndarray) -> np.ndarray:
+    """FFTModulusToDispBuf (func.cpp:459-489): a half-spectrum image L
+    (n, n/2+1), rows ky, placed as the centred display buffer (n, n+2): the
+    right half from L, the left half mirrored through the centre, row 0's
+    left half repeating row 1's."""
+    n = L.shape[0]
     h = n // 2
-    L = np.log1p(np.abs(F) * scale)              # (n, n/2+1), rows ky
-    out = np.zeros((n, n + 2))
+    out = np.zeros((n, n + 2), dtype=np.asarray(L).dtype)
     out[h:, h:n + 1] = L[:h, :]
     out[:h, h:n + 1] = L[h:, :]
     for j in range(1, n):
         out[j, :h] = out[n - j, n - np.arange(h)]
     out[0, :h] = out[1, :h]
-    return out[:, :n]
+    return out
+
+
+def modulus_display(F: np.ndarray, scale: float = 1e-4) -> np.ndarray:
+    """cuFFTLogModulus (cufunc.cu:178-188) + FFTModulusToDispBuf
+    (func.cpp:459-489): log(1 + |F| scale) as the centred n x n image."""
+    return modulus_layout(np.log1p(np.abs(F) * scale))[:, :F.shape[0]]
 
 
 def bin_spectrum(F: np.ndarray, d: int = DISPDIM) -> np.ndarray:

@@ -294,3 +294,49 @@ def test_stretch_gather_equals_inplace_loop():
                     o = int(float(np.float32(ky) * fy) + 0.5) * nx + int(float(np.float32(kx) * fx) + 0.5)
                     b[ky * nx + kx] = b[o]
         np.testing.assert_array_equal(O.stretch_image(img, xs, ys), b.reshape(ny, nx))
+
+
+# -- pins against the reference's own func.cpp (golden fixtures written by
+# tests/golden/make_golden.py with oracle/_ref/ref_func)
+import json
+import os
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _golden(name, dtype, shape=None):
+    a = np.fromfile(os.path.join(GOLDEN, name), dtype=dtype)
+    return a.reshape(shape) if shape else a
+
+
+def test_verify_crop_size_matches_reference():
+    for nx, ny, ox, oy, ns, b, want in json.load(open(os.path.join(GOLDEN, "ref_func.json")))["cropsize"]:
+        assert O.verify_crop_size(nx, ny, ox, oy, ns, b) == want, (nx, ny, ox, oy, ns, b)
+
+
+def test_crop_matches_reference_crop2fft():
+    img = _golden("func_in_37x29.f32", np.float32, (29, 37))
+    nu = O.verify_crop_size(37, 29, 3, 2, 0, 1.0)
+    ref = _golden("ref_crop2fft_37x29.f32", np.float32, (nu, nu + 2))
+    np.testing.assert_array_equal(ref[:, :nu], img[2:2 + nu, 3:3 + nu])
+
+
+def test_cosmask_matches_reference():
+    ref = _golden("ref_cosmask16.c64", np.complex64, (16, 9))
+    w = O.cosmask16_weights()
+    # the reference scales complex<float> ones by the weight: float rounding of w
+    assert np.abs(ref.real - w).max() < 6e-8 and np.abs(ref.imag - w).max() < 6e-8
+    np.testing.assert_array_equal(ref.real == 0, w == 0)
+
+
+def test_display_contrast_matches_reference():
+    buf = _golden("func_in_400.f32", np.float32)
+    for th, lo, hi in json.load(open(os.path.join(GOLDEN, "ref_func.json")))["hist"]:
+        mn, mx = O.hist_min_max(buf, th)
+        assert (float(mn), float(mx)) == (np.float32(lo), np.float32(hi)), th
+    np.testing.assert_array_equal(O.display_short(buf), _golden("ref_dispshort_400.i16", np.int16))
+
+
+def test_modulus_layout_matches_reference():
+    L = _golden("func_in_16x9.f32", np.float32, (16, 9))
+    np.testing.assert_array_equal(O.modulus_layout(L), _golden("ref_moddisp_16.f32", np.float32, (16, 18)))
