@@ -17,10 +17,12 @@ libtiff, none of which are installed).  Pinned against the reference's own
 code compiled by ``oracle/build_ref.sh`` (golden fixtures in tests/golden/):
 the MRC and MRC-gz decode/encode (``mrc.cpp``, ``mrcz.cpp``) and, through
 ``func.cpp`` built against stand-in FFTW/libtiff headers, the crop size and
-crop, the sub-pixel cosine mask and the display contrast and layout.  The
-transforms, cross-correlation, peak search and least-squares solve are pinned
-only by project-written known-answer tests (brute-force DFTs, analytic peaks,
-exactly consistent shifts): for those this oracle is "parity unpinned".
+crop, the sub-pixel cosine mask and the display contrast and layout; the
+pair stage (CC windows, FindShift's shifts and CC) against the reference's
+own cufunc.cu run on the GPU (tests/test_gpu_reference_pair.py).  The
+least-squares solve and the sum are pinned only by project-written
+known-answer tests (brute-force DFTs, analytic peaks, exactly consistent
+shifts): for those this oracle is "parity unpinned".
 """
 from __future__ import annotations
 

@@ -1,0 +1,76 @@
+// Test-infrastructure driver of the reference's own pair stage (cufunc.cu
+// and func.cpp compiled from the reference tree by oracle/build_ref.sh, FFTW
+// replaced by the direct DFTs of oracle/ref_fftw_dft.cpp; never shipped).
+// For frames already cropped to nsam x nsam it runs what ThreadFunc_cuAlign
+// does per pair (DFAlign.cu:768-770, 882-900): cuFFT R2C of every frame in
+// place on padded rows, MkPosList with the B-factor, then per pair
+// GPUShiftCC(frame j, frame i), cuFFT C2R and FindShift.
+//
+//   ref_pair <frames.f32> <nz> <nsam> <bfactor> <box> <nps> <pairs.i32> <npairs> <out.txt> <boxes.f32>
+//   out.txt: one line per pair "i j sx sy cc"
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "cufunc.h"
+#include "func.h"
+
+int main(int argc, char** argv) {
+  if (argc != 11) return 2;
+  const int nz = atoi(argv[2]), nsam = atoi(argv[3]), box = atoi(argv[5]), nps = atoi(argv[6]);
+  const float bfactor = (float)atof(argv[4]);
+  const int npairs = atoi(argv[8]);
+  if (!initGPU(0)) return 3;
+  const int sizeb = (nsam + 2) * nsam, sizec = (nsam / 2 + 1) * nsam;
+  std::vector<float> frames((size_t)nz * nsam * nsam);
+  FILE* f = fopen(argv[1], "rb");
+  if (!f || fread(frames.data(), sizeof(float), frames.size(), f) != frames.size()) return 4;
+  fclose(f);
+  std::vector<int> pairs(2 * (size_t)npairs);
+  f = fopen(argv[7], "rb");
+  if (!f || fread(pairs.data(), sizeof(int), pairs.size(), f) != pairs.size()) return 5;
+  fclose(f);
+  float *dfft = 0, *dsum = 0;
+  MASK* dPosList = 0;
+  if (!GPUMemAlloc((void**)&dfft, sizeof(float) * sizeb) || !GPUMemAlloc((void**)&dsum, sizeof(float) * sizeb) ||
+      !GPUMemAlloc((void**)&dPosList, sizeof(MASK) * sizec))
+    return 6;
+  cufftHandle fplan = GPUFFTPlan(nsam), iplan = GPUIFFTPlan(nsam);
+  // forward transforms (crop2fft lays the rows out padded to nsam + 2)
+  std::vector<float> hbuf((size_t)nz * sizeb), pad(sizeb);
+  for (int k = 0; k < nz; k++) {
+    crop2fft(frames.data() + (size_t)k * nsam * nsam, nsam, pad.data(), 0, 0, nsam, 1.0f);
+    GPUMemH2D(dfft, pad.data(), sizeof(float) * sizeb);
+    GPUFFT2d(dfft, fplan);
+    GPUSync();
+    GPUMemD2H(hbuf.data() + (size_t)k * sizeb, dfft, sizeof(float) * sizeb);
+  }
+  std::vector<MASK> pos(sizec);
+  MkPosList(pos.data(), nsam, bfactor);
+  GPUMemH2D(dPosList, pos.data(), sizeof(MASK) * sizec);
+  FILE* out = fopen(argv[9], "w");
+  FILE* boxes = fopen(argv[10], "wb");
+  if (!out || !boxes) return 7;
+  std::vector<float> hbox((size_t)box * box);
+  for (int p = 0; p < npairs; p++) {
+    const int i = pairs[2 * p], j = pairs[2 * p + 1];
+    GPUMemH2D(dsum, hbuf.data() + (size_t)i * sizeb, sizeof(float) * sizeb);
+    GPUMemH2D(dfft, hbuf.data() + (size_t)j * sizeb, sizeof(float) * sizeb);
+    GPUShiftCC(dfft, dsum, dPosList, 0, 0, nsam);
+    GPUSync();
+    GPUIFFT2d(dfft, iplan);
+    GPUSync();
+    float sx = 0, sy = 0;
+    const float cc = FindShift(dfft, nsam, hbox.data(), box, sx, sy, nps - 1);
+    fprintf(out, "%d %d %.9g %.9g %.9g\n", i, j, sx, sy, cc);
+    fwrite(hbox.data(), sizeof(float), hbox.size(), boxes);
+  }
+  fclose(out);
+  fclose(boxes);
+  GPUFFTDestroy(fplan);
+  GPUFFTDestroy(iplan);
+  GPUMemFree((void**)&dfft);
+  GPUMemFree((void**)&dsum);
+  GPUMemFree((void**)&dPosList);
+  return 0;
+}

@@ -1,0 +1,82 @@
+"""The reference's own pair stage on the GPU against the oracle and the
+CUDA path: oracle/_ref/ref_pair runs cufunc.cu's cuFFT R2C, MkPosList,
+GPUShiftCC, cuFFT C2R and FindShift (DFAlign.cu:768-770, 882-900), compiled
+from the reference tree by oracle/build_ref.sh, with FFTW's host transforms
+answered by direct DFTs (oracle/ref_fftw_dft.cpp).  The binary is built
+where the reference tree is present and travels with the repository; the
+test is skipped where it is absent.
+
+Tolerances: CC windows relative L2 <= 1e-5 (the reference and this path in
+FP32, the oracle in FP64); pair shifts equal on the 1/32 grid apart from the
+documented near-ties; the peak CC within 1e-4 (relative)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from motioncorr1exp_b200 import api, synth
+from oracle import mc_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "ref_pair")
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def near_tie(box_map, sx_a, sy_a, sx_b, sy_b, nps):
+    """Shifts one 1/32 step apart where the oracle's upsampled map is flat to 1e-5."""
+    if max(abs(sx_a - sx_b), abs(sy_a - sy_b)) > 1.5 / 32:
+        return False
+    box = box_map.shape[0]
+    ix, iy = O.integer_peak(box_map, nps)
+    offx = min(max(ix - 8, 0), box - 16)
+    offy = min(max(iy - 8, 0), box - 16)
+    f = O.upsampled_subbox(box_map, offx, offy)
+
+    def val(sx, sy):
+        return f[int(round((sy + box // 2 - offy) * 32)) % 512, int(round((sx + box // 2 - offx) * 32)) % 512]
+    a, b = val(sx_a, sy_a), val(sx_b, sy_b)
+    return abs(a - b) <= 1e-5 * abs(a)
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference pair harness not built (reference tree absent)")
+@pytest.mark.parametrize("n,box,nz,fod", [(1024, 96, 6, 2), (1024, 64, 5, 1)])
+def test_reference_pair_stage(gpu, tmp_path, n, box, nz, fod):
+    mv = synth.make_movie(n, n, nz, mean=1.5, seed=200 + box, dtype="f32", speed=0.7, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=box, FrameDistOffset=fod), nz)
+    with api.Plan(p, n, n, nz, 2) as pl:
+        pl.load_frames(mv.frames)
+        pl.forward()
+        pl.pairs()
+        ours = pl.pair_results()
+        ours_boxes = pl.boxes()
+    pairs = np.asarray(ours["pairs"], np.int32)
+    mv.frames.astype(np.float32).tofile(tmp_path / "frames.f32")
+    pairs.tofile(tmp_path / "pairs.i32")
+    subprocess.run([REF, str(tmp_path / "frames.f32"), str(nz), str(n), str(p.bfactor), str(box),
+                    str(p.NoisePeakSize), str(tmp_path / "pairs.i32"), str(len(pairs)), str(tmp_path / "out.txt"),
+                    str(tmp_path / "boxes.f32")], check=True, timeout=600, capture_output=True)
+    ref = np.loadtxt(tmp_path / "out.txt", ndmin=2)
+    ref_boxes = np.fromfile(tmp_path / "boxes.f32", dtype=np.float32).reshape(len(pairs), box, box)
+    assert np.array_equal(ref[:, :2].astype(np.int32), pairs)
+    F = [O.forward_spectrum(O.decode_frame(mv.frames[f], 2), 0, 0, n, n) for f in range(nz)]
+    mask = O.bfactor_mask(n, p.bfactor)
+    ties = 0
+    for r, (i, j) in enumerate(pairs):
+        ob = O.cc_box(O.cc_map(F[i], F[j], mask, n), n, box)
+        assert rel_l2(ref_boxes[r], ob) <= 1e-5, r          # reference vs oracle
+        assert rel_l2(ours_boxes[r], ref_boxes[r]) <= 1e-5, r  # this path vs reference
+        sx_o, sy_o = O.find_shift(ob, n, p.NoisePeakSize)[:2]
+        for sx, sy in [(ref[r, 2], ref[r, 3]), tuple(ours["shift"][r])]:
+            if (sx, sy) != (np.float32(sx_o), np.float32(sy_o)):
+                assert near_tie(ob, sx, sy, sx_o, sy_o, p.NoisePeakSize), (r, sx, sy, sx_o, sy_o)
+                ties += 1
+        np.testing.assert_allclose(ours["cc"][r], ref[r, 4], rtol=1e-4)
+    assert ties <= max(1, len(pairs) // 25)
