@@ -18,9 +18,10 @@ code compiled by ``oracle/build_ref.sh`` (golden fixtures in tests/golden/):
 the MRC and MRC-gz decode/encode (``mrc.cpp``, ``mrcz.cpp``) and, through
 ``func.cpp`` built against stand-in FFTW/libtiff headers, the crop size and
 crop, the sub-pixel cosine mask and the display contrast and layout; the
-pair stage (CC windows, FindShift's shifts and CC) against the reference's
-own cufunc.cu run on the GPU (tests/test_gpu_reference_pair.py).  The
-least-squares solve and the sum are pinned only by project-written
+forward spectra, the pair stage (CC windows, FindShift's shifts and CC) and
+the shift-and-sum against the reference's own cufunc.cu run on the GPU
+(tests/test_gpu_reference_pair.py).  The least-squares solve, the binning
+and the realignment iterations are pinned only by project-written
 known-answer tests (brute-force DFTs, analytic peaks, exactly consistent
 shifts): for those this oracle is "parity unpinned".
 """

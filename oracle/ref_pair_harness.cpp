@@ -7,7 +7,12 @@
 // GPUShiftCC(frame j, frame i), cuFFT C2R and FindShift.
 //
 //   ref_pair <frames.f32> <nz> <nsam> <bfactor> <box> <nps> <pairs.i32> <npairs> <out.txt> <boxes.f32>
+//            [<spectra.f32> [<sum.f64> <nsum> <image.f32>]]
 //   out.txt: one line per pair "i j sx sy cc"
+//   spectra.f32: every frame's cuFFT R2C, (nsam/2+1) x nsam complex rows ky
+//   sum.f64: nsum records (frame, sx, sy, apply) summed as DFAlign.cu:1142-1292
+//   does (first frame shifted only when apply; even positions into one sum,
+//   odd into the other, added; C2R, times 1/nsam^2); image.f32 nsam x nsam
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -16,7 +21,7 @@
 #include "func.h"
 
 int main(int argc, char** argv) {
-  if (argc != 11) return 2;
+  if (argc != 11 && argc != 12 && argc != 15) return 2;
   const int nz = atoi(argv[2]), nsam = atoi(argv[3]), box = atoi(argv[5]), nps = atoi(argv[6]);
   const float bfactor = (float)atof(argv[4]);
   const int npairs = atoi(argv[8]);
@@ -67,6 +72,42 @@ int main(int argc, char** argv) {
   }
   fclose(out);
   fclose(boxes);
+  if (argc >= 12) {
+    FILE* sp = fopen(argv[11], "wb");
+    if (!sp) return 8;
+    for (int k = 0; k < nz; k++) fwrite(hbuf.data() + (size_t)k * sizeb, sizeof(float), sizeb, sp);
+    fclose(sp);
+  }
+  if (argc == 15) {
+    const int nsum = atoi(argv[13]);
+    std::vector<double> rec(4 * (size_t)nsum);
+    FILE* sf = fopen(argv[12], "rb");
+    if (!sf || fread(rec.data(), sizeof(double), rec.size(), sf) != rec.size()) return 9;
+    fclose(sf);
+    float* dsum2 = 0;
+    if (!GPUMemAlloc((void**)&dsum2, sizeof(float) * sizeb)) return 10;
+    GPUMemZero((void**)&dsum, sizeof(float) * sizeb);
+    GPUMemZero((void**)&dsum2, sizeof(float) * sizeb);
+    for (int q = 0; q < nsum; q++) {
+      const int k = (int)rec[4 * q];
+      GPUMemH2D(dfft, hbuf.data() + (size_t)k * sizeb, sizeof(float) * sizeb);
+      if (rec[4 * q + 3] != 0.0) GPUShift(dfft, dPosList, (float)rec[4 * q + 1], (float)rec[4 * q + 2], nsam);
+      GPUAdd((q & 1) ? dsum2 : dsum, dfft, sizeb);
+      GPUSync();
+    }
+    GPUAdd(dsum, dsum2, sizeb);
+    GPUIFFT2d(dsum, iplan);
+    GPUMultiplyNum(dsum, (float)(1.0 / ((double)nsam * nsam)), sizeb);  // 1.0/size, size = nsam*nsam
+    GPUSync();
+    std::vector<float> img(sizeb), flat((size_t)nsam * nsam);
+    GPUMemD2H(img.data(), dsum, sizeof(float) * sizeb);
+    fft2buf(flat.data(), img.data(), nsam);
+    FILE* im = fopen(argv[14], "wb");
+    if (!im) return 11;
+    fwrite(flat.data(), sizeof(float), flat.size(), im);
+    fclose(im);
+    GPUMemFree((void**)&dsum2);
+  }
   GPUFFTDestroy(fplan);
   GPUFFTDestroy(iplan);
   GPUMemFree((void**)&dfft);

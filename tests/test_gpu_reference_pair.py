@@ -1,14 +1,17 @@
-"""The reference's own pair stage on the GPU against the oracle and the
-CUDA path: oracle/_ref/ref_pair runs cufunc.cu's cuFFT R2C, MkPosList,
-GPUShiftCC, cuFFT C2R and FindShift (DFAlign.cu:768-770, 882-900), compiled
+"""The reference's own forward transform, pair stage and shift-and-sum on
+the GPU against the oracle and the CUDA path: oracle/_ref/ref_pair runs
+cufunc.cu's cuFFT R2C, MkPosList, GPUShiftCC, cuFFT C2R and FindShift
+(DFAlign.cu:768-770, 882-900) and GPUShift + GPUAdd + C2R for the sum
+(DFAlign.cu:1142-1292), compiled
 from the reference tree by oracle/build_ref.sh, with FFTW's host transforms
 answered by direct DFTs (oracle/ref_fftw_dft.cpp).  The binary is built
 where the reference tree is present and travels with the repository; the
 test is skipped where it is absent.
 
-Tolerances: CC windows relative L2 <= 1e-5 (the reference and this path in
-FP32, the oracle in FP64); pair shifts equal on the 1/32 grid apart from the
-documented near-ties; the peak CC within 1e-4 (relative)."""
+Tolerances: spectra, CC windows and the summed image relative L2 <= 1e-5
+(the reference and this path in FP32, the oracle in FP64); pair shifts equal
+on the 1/32 grid apart from the documented near-ties; the peak CC within
+1e-4 (relative)."""
 import os
 import subprocess
 
@@ -25,8 +28,9 @@ REF = os.path.join(ROOT, "oracle", "_ref", "ref_pair")
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    dt = np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64
+    a = np.asarray(a, dt)
+    b = np.asarray(b, dt)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
@@ -54,19 +58,39 @@ def test_reference_pair_stage(gpu, tmp_path, n, box, nz, fod):
     with api.Plan(p, n, n, nz, 2) as pl:
         pl.load_frames(mv.frames)
         pl.forward()
+        ours_spec = [pl.spectrum(f, 0) for f in range(nz)]
         pl.pairs()
         ours = pl.pair_results()
         ours_boxes = pl.boxes()
+        pl.solve()
+        pl.iterate()
+        image = pl.sum()
+        sh, first, last = pl.sum_shifts()
     pairs = np.asarray(ours["pairs"], np.int32)
     mv.frames.astype(np.float32).tofile(tmp_path / "frames.f32")
     pairs.tofile(tmp_path / "pairs.i32")
+    rec = np.array([[k, sh[k, 0], sh[k, 1], 0.0 if (k == first and not p.bAlignToMid) else 1.0]
+                    for k in range(first, last + 1)], np.float64)
+    rec.tofile(tmp_path / "sum.f64")
     subprocess.run([REF, str(tmp_path / "frames.f32"), str(nz), str(n), str(p.bfactor), str(box),
                     str(p.NoisePeakSize), str(tmp_path / "pairs.i32"), str(len(pairs)), str(tmp_path / "out.txt"),
-                    str(tmp_path / "boxes.f32")], check=True, timeout=600, capture_output=True)
+                    str(tmp_path / "boxes.f32"), str(tmp_path / "spec.f32"), str(tmp_path / "sum.f64"), str(len(rec)),
+                    str(tmp_path / "image.f32")], check=True, timeout=600, capture_output=True)
+    ref_spec = np.fromfile(tmp_path / "spec.f32", np.float32).view(np.complex64).reshape(nz, n, n // 2 + 1)
+    ref_image = np.fromfile(tmp_path / "image.f32", np.float32).reshape(n, n)
     ref = np.loadtxt(tmp_path / "out.txt", ndmin=2)
     ref_boxes = np.fromfile(tmp_path / "boxes.f32", dtype=np.float32).reshape(len(pairs), box, box)
     assert np.array_equal(ref[:, :2].astype(np.int32), pairs)
     F = [O.forward_spectrum(O.decode_frame(mv.frames[f], 2), 0, 0, n, n) for f in range(nz)]
+    for f in range(nz):
+        assert rel_l2(ref_spec[f], F[f]) <= 1e-5, f                  # reference vs oracle
+        assert rel_l2(ours_spec[f], ref_spec[f]) <= 1e-5, f          # this path vs reference
+    S = np.zeros_like(F[0])
+    for k, _, _, apply in rec.tolist():
+        k = int(k)
+        S = S + (O.phase_shift(F[k], sh[k, 0], sh[k, 1]) if apply else F[k])
+    assert rel_l2(ref_image, O.spectrum_to_image(S)) <= 1e-5
+    assert rel_l2(image, ref_image) <= 1e-5
     mask = O.bfactor_mask(n, p.bfactor)
     ties = 0
     for r, (i, j) in enumerate(pairs):
