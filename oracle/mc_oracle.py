@@ -20,8 +20,8 @@ the MRC and MRC-gz decode/encode (``mrc.cpp``, ``mrcz.cpp``) and, through
 crop, the sub-pixel cosine mask and the display contrast and layout; the
 forward spectra, the pair stage (CC windows, FindShift's shifts and CC) and
 the shift-and-sum against the reference's own cufunc.cu run on the GPU
-(tests/test_gpu_reference_pair.py).  The least-squares solve, the binning
-and the realignment iterations are pinned only by project-written
+(tests/test_gpu_reference_pair.py), binning included.  The least-squares
+solve and the realignment iterations are pinned only by project-written
 known-answer tests (brute-force DFTs, analytic peaks, exactly consistent
 shifts): for those this oracle is "parity unpinned".
 """

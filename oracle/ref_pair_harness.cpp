@@ -6,15 +6,18 @@
 // place on padded rows, MkPosList with the B-factor, then per pair
 // GPUShiftCC(frame j, frame i), cuFFT C2R and FindShift.
 //
-//   ref_pair <frames.f32> <nz> <nsam> <bfactor> <box> <nps> <pairs.i32> <npairs> <out.txt> <boxes.f32>
+//   ref_pair <frames.f32> <nz> <nsam|nu/nsam> <bfactor> <box> <nps> <pairs.i32> <npairs> <out.txt> <boxes.f32>
 //            [<spectra.f32> [<sum.f64> <nsum> <image.f32>]]
 //   out.txt: one line per pair "i j sx sy cc"
+//   nu/nsam: frames of nu x nu transformed at nu and Fourier-cropped to nsam
+//   by GPUMemBinD2D (DFAlign.cu:773-779)
 //   spectra.f32: every frame's cuFFT R2C, (nsam/2+1) x nsam complex rows ky
 //   sum.f64: nsum records (frame, sx, sy, apply) summed as DFAlign.cu:1142-1292
 //   does (first frame shifted only when apply; even positions into one sum,
 //   odd into the other, added; C2R, times 1/nsam^2); image.f32 nsam x nsam
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "cufunc.h"
@@ -22,12 +25,14 @@
 
 int main(int argc, char** argv) {
   if (argc != 11 && argc != 12 && argc != 15) return 2;
-  const int nz = atoi(argv[2]), nsam = atoi(argv[3]), box = atoi(argv[5]), nps = atoi(argv[6]);
+  const int nz = atoi(argv[2]), box = atoi(argv[5]), nps = atoi(argv[6]);
+  int nu = atoi(argv[3]), nsam = nu;
+  if (const char* sl = strchr(argv[3], '/')) nsam = atoi(sl + 1);
   const float bfactor = (float)atof(argv[4]);
   const int npairs = atoi(argv[8]);
   if (!initGPU(0)) return 3;
-  const int sizeb = (nsam + 2) * nsam, sizec = (nsam / 2 + 1) * nsam;
-  std::vector<float> frames((size_t)nz * nsam * nsam);
+  const int sizeb = (nsam + 2) * nsam, sizec = (nsam / 2 + 1) * nsam, sizebu = (nu + 2) * nu;
+  std::vector<float> frames((size_t)nz * nu * nu);
   FILE* f = fopen(argv[1], "rb");
   if (!f || fread(frames.data(), sizeof(float), frames.size(), f) != frames.size()) return 4;
   fclose(f);
@@ -35,18 +40,22 @@ int main(int argc, char** argv) {
   f = fopen(argv[7], "rb");
   if (!f || fread(pairs.data(), sizeof(int), pairs.size(), f) != pairs.size()) return 5;
   fclose(f);
-  float *dfft = 0, *dsum = 0;
+  float *dfft = 0, *dsum = 0, *dunb = 0;
   MASK* dPosList = 0;
   if (!GPUMemAlloc((void**)&dfft, sizeof(float) * sizeb) || !GPUMemAlloc((void**)&dsum, sizeof(float) * sizeb) ||
-      !GPUMemAlloc((void**)&dPosList, sizeof(MASK) * sizec))
+      !GPUMemAlloc((void**)&dunb, sizeof(float) * sizebu) || !GPUMemAlloc((void**)&dPosList, sizeof(MASK) * sizec))
     return 6;
-  cufftHandle fplan = GPUFFTPlan(nsam), iplan = GPUIFFTPlan(nsam);
-  // forward transforms (crop2fft lays the rows out padded to nsam + 2)
-  std::vector<float> hbuf((size_t)nz * sizeb), pad(sizeb);
+  cufftHandle uplan = GPUFFTPlan(nu), iplan = GPUIFFTPlan(nsam);
+  // forward transforms (crop2fft lays the rows out padded to nu + 2), then
+  // the Fourier crop to nsam when binning
+  std::vector<float> hbuf((size_t)nz * sizeb), pad(sizebu);
   for (int k = 0; k < nz; k++) {
-    crop2fft(frames.data() + (size_t)k * nsam * nsam, nsam, pad.data(), 0, 0, nsam, 1.0f);
-    GPUMemH2D(dfft, pad.data(), sizeof(float) * sizeb);
-    GPUFFT2d(dfft, fplan);
+    crop2fft(frames.data() + (size_t)k * nu * nu, nu, pad.data(), 0, 0, nu, 1.0f);
+    GPUMemH2D(dunb, pad.data(), sizeof(float) * sizebu);
+    GPUFFT2d(dunb, uplan);
+    GPUSync();
+    if (nu != nsam) GPUMemBinD2D(dfft, dunb, nsam, nu);
+    else GPUMemD2D(dfft, dunb, sizeof(float) * sizeb);
     GPUSync();
     GPUMemD2H(hbuf.data() + (size_t)k * sizeb, dfft, sizeof(float) * sizeb);
   }
@@ -108,10 +117,11 @@ int main(int argc, char** argv) {
     fclose(im);
     GPUMemFree((void**)&dsum2);
   }
-  GPUFFTDestroy(fplan);
+  GPUFFTDestroy(uplan);
   GPUFFTDestroy(iplan);
   GPUMemFree((void**)&dfft);
   GPUMemFree((void**)&dsum);
+  GPUMemFree((void**)&dunb);
   GPUMemFree((void**)&dPosList);
   return 0;
 }

@@ -51,11 +51,14 @@ def near_tie(box_map, sx_a, sy_a, sx_b, sy_b, nps):
 
 
 @pytest.mark.skipif(not os.path.exists(REF), reason="reference pair harness not built (reference tree absent)")
-@pytest.mark.parametrize("n,box,nz,fod", [(1024, 96, 6, 2), (1024, 64, 5, 1)])
-def test_reference_pair_stage(gpu, tmp_path, n, box, nz, fod):
-    mv = synth.make_movie(n, n, nz, mean=1.5, seed=200 + box, dtype="f32", speed=0.7, rw_sigma=0.4)
-    p = api.verify_params(api.Params(CCPeakSearchDim=box, FrameDistOffset=fod), nz)
-    with api.Plan(p, n, n, nz, 2) as pl:
+@pytest.mark.parametrize("nu,n,box,nz,fod", [(1024, 1024, 96, 6, 2), (1024, 1024, 64, 5, 1), (1024, 512, 64, 5, 1)])
+def test_reference_pair_stage(gpu, tmp_path, nu, n, box, nz, fod):
+    """nu != n: the frames transformed at nu and Fourier-cropped to n (-bin 2,
+    GPUMemBinD2D)."""
+    mv = synth.make_movie(nu, nu, nz, mean=1.5, seed=200 + box + n, dtype="f32", speed=0.7, rw_sigma=0.4)
+    p = api.verify_params(api.Params(CCPeakSearchDim=box, FrameDistOffset=fod, bin=nu / n), nz)
+    with api.Plan(p, nu, nu, nz, 2) as pl:
+        assert pl.nsam == n
         pl.load_frames(mv.frames)
         pl.forward()
         ours_spec = [pl.spectrum(f, 0) for f in range(nz)]
@@ -72,7 +75,7 @@ def test_reference_pair_stage(gpu, tmp_path, n, box, nz, fod):
     rec = np.array([[k, sh[k, 0], sh[k, 1], 0.0 if (k == first and not p.bAlignToMid) else 1.0]
                     for k in range(first, last + 1)], np.float64)
     rec.tofile(tmp_path / "sum.f64")
-    subprocess.run([REF, str(tmp_path / "frames.f32"), str(nz), str(n), str(p.bfactor), str(box),
+    subprocess.run([REF, str(tmp_path / "frames.f32"), str(nz), f"{nu}/{n}", str(p.bfactor), str(box),
                     str(p.NoisePeakSize), str(tmp_path / "pairs.i32"), str(len(pairs)), str(tmp_path / "out.txt"),
                     str(tmp_path / "boxes.f32"), str(tmp_path / "spec.f32"), str(tmp_path / "sum.f64"), str(len(rec)),
                     str(tmp_path / "image.f32")], check=True, timeout=600, capture_output=True)
@@ -81,7 +84,7 @@ def test_reference_pair_stage(gpu, tmp_path, n, box, nz, fod):
     ref = np.loadtxt(tmp_path / "out.txt", ndmin=2)
     ref_boxes = np.fromfile(tmp_path / "boxes.f32", dtype=np.float32).reshape(len(pairs), box, box)
     assert np.array_equal(ref[:, :2].astype(np.int32), pairs)
-    F = [O.forward_spectrum(O.decode_frame(mv.frames[f], 2), 0, 0, n, n) for f in range(nz)]
+    F = [O.forward_spectrum(O.decode_frame(mv.frames[f], 2), 0, 0, nu, n) for f in range(nz)]
     for f in range(nz):
         assert rel_l2(ref_spec[f], F[f]) <= 1e-5, f                  # reference vs oracle
         assert rel_l2(ours_spec[f], ref_spec[f]) <= 1e-5, f          # this path vs reference
