@@ -125,6 +125,8 @@ struct ShiftSumArgs {
   long long ld_out;
   FftPlan1D plan;        // length n (mode 1)
   const float2* tw;
+  float2* acc;           // mode 1: H x ldn scratch for the sum spectrum (split
+                         // accumulate / transform); null = fused kernel
 };
 
 // FSC shell sums of -fsc over the listed frames (even / odd list positions).
@@ -233,6 +235,8 @@ cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st);
 cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 // ey: scratch of nsum*n float2 for the per-frame ky phase ramps
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
+// n = N1 * N2 for one of the compiled two-level splits
+bool two_level_split(int n, int& n1, int& n2);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);
 // -scx/-scy stretch: the crop region of one raw frame (word length wl, read
 // through `slot` + offset when slot is set, else from `frame`) gathered into

@@ -300,6 +300,7 @@ struct mc_plan {
   float *d_pshift = nullptr, *d_pcc = nullptr;
   int* d_ppeak = nullptr;
   float2 *d_sum = nullptr, *d_T2 = nullptr, *d_ey = nullptr;
+  float2* d_sumacc = nullptr;  // sum spectrum of the split image sum (two-level n)
   float* d_image = nullptr;
   int *d_sumframes = nullptr, *d_apply = nullptr;
   double2* d_sumshift = nullptr;
@@ -628,6 +629,7 @@ int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector
   a.mode = mode;
   a.plan = pl->plan_n;
   a.tw = pl->d_tw_n;
+  a.acc = pl->d_sumacc;
   if (mode == 0) {
     a.out = pl->d_sum;
     a.ld_out = pl->ldn;
@@ -908,6 +910,13 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   CKR(pl->alloc(&pl->d_ppeak, sizeof(int) * 2 * pl->maxp));
   CKR(pl->alloc(&pl->d_sum, sizeof(float2) * pl->fstride));
   CKR(pl->alloc(&pl->d_T2, sizeof(float2) * (size_t)pl->n * pl->ldt2));
+  {
+    // image sums of two-level sizes accumulate into d_sumacc, then transform
+    // (MC_SUM_FUSED=1 keeps the single fused kernel)
+    int n1, n2;
+    if (mc::two_level_split(pl->n, n1, n2) && !getenv("MC_SUM_FUSED"))
+      CKR(pl->alloc(&pl->d_sumacc, sizeof(float2) * pl->fstride));
+  }
   CKR(pl->alloc(&pl->d_ey, sizeof(float2) * (size_t)capf * pl->n));
   CKR(pl->alloc(&pl->d_image, sizeof(float) * (size_t)pl->n * pl->n));
   CKR(pl->alloc(&pl->d_sumframes, sizeof(int) * capf));
@@ -2039,6 +2048,7 @@ static int enqueue_tail(mc_plan* pl) {
   a.mode = 1;
   a.plan = pl->plan_n;
   a.tw = pl->d_tw_n;
+  a.acc = pl->d_sumacc;
   a.out = pl->d_T2;
   a.ld_out = pl->ldt2;
   const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);

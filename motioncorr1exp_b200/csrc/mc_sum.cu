@@ -365,6 +365,77 @@ __global__ void __launch_bounds__(kThreads) k_shift_sum2l(ShiftSumArgs a, const 
                                 [&](int k, float2 v) { out[(long long)k * ld + kx] = v; });
 }
 
+// Accumulation alone (no transform): each CTA covers kSumChunk consecutive ky
+// of one kx column, kSumE per thread, with the operations and frame order of
+// the fused kernels, so the sum spectrum is bitwise the same.  Few registers
+// let eight CTAs share an SM and keep 2 * kSumE loads per thread in flight,
+// where the fused two-level kernel (its transform needs most of the register
+// file) runs one.
+constexpr int kSumE = 4;
+constexpr int kSumChunk = kThreads * kSumE;
+
+__global__ void __launch_bounds__(kThreads) k_shift_acc(ShiftSumArgs a, const float2* __restrict__ ey,
+                                                        float2* out, long long ld_out) {
+  extern __shared__ float2 exs[];  // per-frame exp(+2 pi i sx kx / n)
+  const int tid = threadIdx.x, kx = blockIdx.y, n = a.n;
+  for (int f = tid; f < a.nsum; f += kThreads) {
+    double sn, cn;
+    const double t = a.shifts[f].x * (double)kx / (double)n;
+    sincospi(2.0 * (t - rint(t)), &sn, &cn);
+    exs[f] = make_float2((float)cn, (float)sn);
+  }
+  __syncthreads();
+  const int k0 = blockIdx.x * kSumChunk + tid;
+  float2 acc[kSumE];
+#pragma unroll
+  for (int j = 0; j < kSumE; j++) acc[j] = make_float2(0.f, 0.f);
+  for (int f = 0; f < a.nsum; f++) {
+    const float2* c = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
+    const float2* eyf = ey + (long long)f * n;
+    const float2 e = exs[f];
+    const bool ap = a.apply[f] != 0;
+#pragma unroll
+    for (int j = 0; j < kSumE; j++) {
+      const int ky = k0 + kThreads * j;
+      if (ky < n) {
+        float2 v = __ldg(c + ky);
+        if (ap) v = cmul(v, cmul(e, __ldg(eyf + ky)));
+        acc[j] = cadd(acc[j], v);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kSumE; j++) {
+    const int ky = k0 + kThreads * j;
+    if (ky < n) out[(long long)kx * ld_out + ky] = acc[j];
+  }
+}
+
+// The inverse along ky of each accumulated column, written transposed
+// (out[y * ld_out + kx]) for the C2R row pass: the transform of the fused
+// two-level kernel, here at TwoLevel's own CTA size.
+template <int N1, int N2>
+__global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS)
+    k_sum_cols2l(const float2* __restrict__ in, long long ld_in, const float2* __restrict__ tw, float2* out,
+                 long long ld_out) {
+  using TL = TwoLevel<N1, N2>;
+  __shared__ float2 ysm[TL::N];
+  const int kx = blockIdx.x;
+  const float2* col = in + (long long)kx * ld_in;
+  TL::template run<true, false>(ysm, tw, [&](int i) { return __ldg(col + i); },
+                                [&](int k, float2 v) { out[(long long)k * ld_out + kx] = v; });
+}
+
+cudaError_t launch_shift_acc(const ShiftSumArgs& a, const float2* ey, float2* out, long long ld_out,
+                             cudaStream_t st) {
+  const size_t smem = (size_t)a.nsum * sizeof(float2);
+  cudaError_t e = allow_smem((const void*)k_shift_acc, smem);
+  if (e != cudaSuccess) return e;
+  dim3 g((a.n + kSumChunk - 1) / kSumChunk, a.H);
+  k_shift_acc<<<g, kThreads, smem, st>>>(a, ey, out, ld_out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st) {
   RampArgs r;
   r.shifts = a.shifts;
@@ -375,7 +446,19 @@ cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st)
   k_ramp<<<g, 256, 0, st>>>(r);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (a.mode == 0) return launch_shift_acc(a, ey, a.out, a.ld_out, st);
   int n1 = 0, n2 = 0;
+  if (a.acc && two_level_split(a.n, n1, n2)) {
+    e = launch_shift_acc(a, ey, a.acc, a.ldn, st);
+    if (e != cudaSuccess) return e;
+#define MC_TL_COLS(A, B)                                                                     \
+  if (n1 == (A) && n2 == (B)) {                                                              \
+    k_sum_cols2l<A, B><<<a.H, TwoLevel<A, B>::T, 0, st>>>(a.acc, a.ldn, a.tw, a.out, a.ld_out); \
+    return cudaGetLastError();                                                               \
+  }
+    MC_TWO_LEVEL_LIST(MC_TL_COLS)
+#undef MC_TL_COLS
+  }
   if (two_level_split(a.n, n1, n2)) {
     const size_t smem2 = (size_t)(2 * a.n + a.nsum) * sizeof(float2);
 #define MC_TL_SUM(A, B)                                                                                       \
