@@ -235,6 +235,7 @@ cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st);
 cudaError_t launch_peak(const PeakArgs& a, cudaStream_t st);
 // ey: scratch of nsum*n float2 for the per-frame ky phase ramps
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st);
+int shift_sum_kernels(const ShiftSumArgs& a);  // kernels launch_shift_sum launches
 // n = N1 * N2 for one of the compiled two-level splits
 bool two_level_split(int n, int& n1, int& n2);
 cudaError_t launch_c2r_rows(const C2rRowsArgs& a, cudaStream_t st);

@@ -390,13 +390,13 @@ struct mc_plan {
     *slot = (int)krec.size() - 1;
     return MC_OK;
   }
-  int kstop(int kind, int slot, double bytes) {
+  int kstop(int kind, int slot, double bytes, int nk = 1) {
     if (capturing) {  // counted once per graph replay instead
-      graph_kcount[kind]++;
+      graph_kcount[kind] += nk;
       graph_kbytes[kind] += bytes;
       return MC_OK;
     }
-    kcount[kind]++;
+    kcount[kind] += nk;
     kbytes[kind] += bytes;
     if (slot < 0) return MC_OK;
     cudaEvent_t e;
@@ -469,13 +469,15 @@ struct mc_plan {
 namespace {
 
 // launch `call` as kernel kind `kind` moving `bytes` algorithmic bytes
-#define LAUNCH(pl, kind, bytes, call)        \
-  do {                                       \
-    int slot_;                               \
-    CKR((pl)->kstart((kind), &slot_));       \
-    CK(call);                                \
-    CKR((pl)->kstop((kind), slot_, (bytes))); \
+// one stage of nk kernel launches, timed and counted under one kind
+#define LAUNCH_N(pl, kind, bytes, nk, call)         \
+  do {                                              \
+    int slot_;                                      \
+    CKR((pl)->kstart((kind), &slot_));              \
+    CK(call);                                       \
+    CKR((pl)->kstop((kind), slot_, (bytes), (nk))); \
   } while (0)
+#define LAUNCH(pl, kind, bytes, call) LAUNCH_N(pl, kind, bytes, 1, call)
 
 template <typename T>
 int upload(mc_plan* pl, T* dst, const std::vector<T>& src) {
@@ -638,7 +640,8 @@ int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector
     a.ld_out = pl->ldt2;
   }
   const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);
-  LAUNCH(pl, MC_K_SHIFT_SUM, (double)ns * spec_bytes + spec_bytes, mc::launch_shift_sum(a, pl->d_ey, pl->st));
+  LAUNCH_N(pl, MC_K_SHIFT_SUM, (double)ns * spec_bytes + spec_bytes, mc::shift_sum_kernels(a),
+           mc::launch_shift_sum(a, pl->d_ey, pl->st));
   if (mode == 1) {
     mc::C2rRowsArgs c{};
     c.t2 = pl->d_T2;
@@ -1919,7 +1922,7 @@ static int objective(mc_plan* pl, const std::vector<cplx>& s, double* J, double*
   a.partial = pl->d_opart;
   a.partialJ = pl->d_opart + (size_t)pl->H * nf * 5;
   a.out = pl->d_oout;
-  LAUNCH(pl, MC_K_OBJECTIVE, (double)(nf + 1) * pl->H * pl->n * sizeof(float2), mc::launch_objective(a, pl->st));
+  LAUNCH_N(pl, MC_K_OBJECTIVE, (double)(nf + 1) * pl->H * pl->n * sizeof(float2), 2, mc::launch_objective(a, pl->st));
   std::vector<double> out((size_t)nf * 5 + 1);
   CK(cudaMemcpyAsync(out.data(), pl->d_oout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, pl->st));
   CK(cudaStreamSynchronize(pl->st));
@@ -2052,7 +2055,8 @@ static int enqueue_tail(mc_plan* pl) {
   a.out = pl->d_T2;
   a.ld_out = pl->ldt2;
   const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);
-  LAUNCH(pl, MC_K_SHIFT_SUM, (double)a.nsum * spec_bytes + spec_bytes, mc::launch_shift_sum(a, pl->d_ey, pl->st));
+  LAUNCH_N(pl, MC_K_SHIFT_SUM, (double)a.nsum * spec_bytes + spec_bytes, mc::shift_sum_kernels(a),
+           mc::launch_shift_sum(a, pl->d_ey, pl->st));
   mc::C2rRowsArgs c{};
   c.t2 = pl->d_T2;
   c.ld_t2 = pl->ldt2;

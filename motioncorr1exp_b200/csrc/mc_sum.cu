@@ -367,11 +367,14 @@ __global__ void __launch_bounds__(kThreads) k_shift_sum2l(ShiftSumArgs a, const 
 
 // Accumulation alone (no transform): each CTA covers kSumChunk consecutive ky
 // of one kx column, kSumE per thread, with the operations and frame order of
-// the fused kernels, so the sum spectrum is bitwise the same.  Few registers
-// let eight CTAs share an SM and keep 2 * kSumE loads per thread in flight,
-// where the fused two-level kernel (its transform needs most of the register
-// file) runs one.
+// the fused kernels, so the sum spectrum is bitwise the same.  The loads of
+// kSumG frames are issued before their products are added: 64 registers,
+// four CTAs per SM and 2 * kSumE * kSumG loads per thread in flight, where
+// the fused two-level kernel (its transform needs most of the register file)
+// runs one CTA per SM.  Measured on 3710^2 x 40 frames: 0.38 ms against a
+// 0.34 ms HBM floor (kSumG = 1: 0.56 ms; kSumE = 2 or 8: slower).
 constexpr int kSumE = 4;
+constexpr int kSumG = 2;
 constexpr int kSumChunk = kThreads * kSumE;
 
 __global__ void __launch_bounds__(kThreads) k_shift_acc(ShiftSumArgs a, const float2* __restrict__ ey,
@@ -389,18 +392,38 @@ __global__ void __launch_bounds__(kThreads) k_shift_acc(ShiftSumArgs a, const fl
   float2 acc[kSumE];
 #pragma unroll
   for (int j = 0; j < kSumE; j++) acc[j] = make_float2(0.f, 0.f);
-  for (int f = 0; f < a.nsum; f++) {
-    const float2* c = a.spec + (long long)a.frames[f] * a.stride + (long long)kx * a.ldn;
-    const float2* eyf = ey + (long long)f * n;
-    const float2 e = exs[f];
-    const bool ap = a.apply[f] != 0;
+  const float2* colx = a.spec + (long long)kx * a.ldn;
+  for (int f0 = 0; f0 < a.nsum; f0 += kSumG) {
+    float2 v[kSumG][kSumE], y[kSumG][kSumE];
+    bool ap[kSumG];
 #pragma unroll
-    for (int j = 0; j < kSumE; j++) {
-      const int ky = k0 + kThreads * j;
-      if (ky < n) {
-        float2 v = __ldg(c + ky);
-        if (ap) v = cmul(v, cmul(e, __ldg(eyf + ky)));
-        acc[j] = cadd(acc[j], v);
+    for (int g = 0; g < kSumG; g++) {
+      const int f = f0 + g;
+      ap[g] = f < a.nsum && a.apply[f] != 0;
+      if (f < a.nsum) {
+        const float2* c = colx + (long long)a.frames[f] * a.stride;
+        const float2* eyf = ey + (long long)f * n;
+#pragma unroll
+        for (int j = 0; j < kSumE; j++) {
+          const int ky = k0 + kThreads * j;
+          if (ky < n) {
+            v[g][j] = __ldg(c + ky);
+            if (ap[g]) y[g][j] = __ldg(eyf + ky);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kSumG; g++) {
+      const int f = f0 + g;
+      if (f < a.nsum) {
+        const float2 e = exs[f];
+#pragma unroll
+        for (int j = 0; j < kSumE; j++) {
+          float2 w = v[g][j];
+          if (ap[g]) w = cmul(w, cmul(e, y[g][j]));
+          acc[j] = cadd(acc[j], w);
+        }
       }
     }
   }
@@ -434,6 +457,11 @@ cudaError_t launch_shift_acc(const ShiftSumArgs& a, const float2* ey, float2* ou
   dim3 g((a.n + kSumChunk - 1) / kSumChunk, a.H);
   k_shift_acc<<<g, kThreads, smem, st>>>(a, ey, out, ld_out);
   return cudaGetLastError();
+}
+
+int shift_sum_kernels(const ShiftSumArgs& a) {
+  int n1, n2;
+  return (a.mode == 1 && a.acc && two_level_split(a.n, n1, n2)) ? 3 : 2;  // k_ramp first
 }
 
 cudaError_t launch_shift_sum(const ShiftSumArgs& a, float2* ey, cudaStream_t st) {
