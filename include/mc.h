@@ -188,7 +188,8 @@ enum {
   MC_K_SHIFT_SUM = 5, /* phase-shift-and-accumulate (+ inverse columns) */
   MC_K_C2R_ROWS = 6,  /* final C2R rows x 1/n^2 */
   MC_K_OBJECTIVE = 7, /* adjoint of the shift-and-sum: objective, gradient, Hessian blocks */
-  MC_KERNEL_KINDS = 8
+  MC_K_SOLVE = 8,     /* FP64 drift solve of a device-only movie (k_solve_smem / k_solve) */
+  MC_KERNEL_KINDS = 9
 };
 void mc_plan_set_profiling(mc_plan* plan, int on);
 int mc_plan_reset_stats(mc_plan* plan);

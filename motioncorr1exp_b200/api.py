@@ -65,7 +65,7 @@ def verify_params(p: Params, nz: int) -> Params:
 
 MODE_U8 = 100  # unsigned 8-bit pixels (8-bit TIFF)
 _WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2, MODE_U8: 1}
-KERNEL_KINDS = 8
+KERNEL_KINDS = 9
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:

@@ -2037,7 +2037,8 @@ static int enqueue_tail(mc_plan* pl) {
   s.sum_frames = pl->d_sumframes;
   s.sum_apply = pl->d_apply;
   s.status = pl->d_status;
-  CK(mc::launch_solve(s, pl->st));
+  LAUNCH(pl, MC_K_SOLVE, (double)np * (2 * sizeof(float) + 2 * sizeof(double) + sizeof(int)) + (double)nf * 4 * sizeof(double),
+         mc::launch_solve(s, pl->st));
   mc::ShiftSumArgs a{};
   a.spec = pl->d_specA;
   a.stride = pl->fstride;
@@ -2329,7 +2330,8 @@ int mc_plan_kernel_stats(const mc_plan* pl, int kind, double* ms, long long* lau
 
 const char* mc_kernel_name(int kind) {
   static const char* names[MC_KERNEL_KINDS] = {"k_fwd_rows", "k_rows_fft", "k_pair_cols", "k_pair_rows",
-                                               "k_peak", "k_shift_sum", "k_c2r_rows", "k_objective"};
+                                               "k_peak", "k_shift_sum", "k_c2r_rows", "k_objective",
+                                               "k_solve"};
   return (kind >= 0 && kind < MC_KERNEL_KINDS) ? names[kind] : "";
 }
 
