@@ -548,6 +548,12 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
 }
 
 // =============================================================== adjoint ==
+// Each thread's per-frame partials over its E <= 36 column elements add in
+// FP32 (the terms themselves are FP32 products): five conversions per frame
+// instead of three per element; warps and columns add in FP64.  The column
+// loads go out in batches of eight spectrum and eight ramp values before any
+// is used (issued one by one, each waited for its own latency: 3.3 ms per
+// call at 4096^2 x 60 frames, batched 2.2 ms).
 template <int E>
 __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
   constexpr int W = kThreads / 32;
@@ -601,23 +607,38 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
     const float2* c = a.spec + (long long)f * a.stride + (long long)kx * a.ldn;
     const float2* eyf = a.ey + (long long)f * n;
     const float2 e = ex[f];
-    double gx = 0, gy = 0, hxx = 0, hxy = 0, hyy = 0;
+    // loads in batches of KB spectrum + KB ramp values, all issued before use
+    constexpr int KB = E < 8 ? E : 8;
+    float fx = 0.f, fy = 0.f, fxx = 0.f, fxy = 0.f, fyy = 0.f;
 #pragma unroll
-    for (int j = 0; j < E; j++) {
-      const int ky = tid + kThreads * j;
-      if (ky < n) {
-        const float2 P = cmul(__ldg(c + ky), cmul(e, __ldg(eyf + ky)));
-        const float2 d = csub(s[j], P);
-        const float2 u = cmulc(P, d);  // conj(d) * P
-        const double wi = (double)(hw[j] * u.y), wr = (double)(hw[j] * u.x);
-        const double y = (double)oy[j];
-        gx += wi;
-        gy += wi * y;
-        hxx += wr;
-        hxy += wr * y;
-        hyy += wr * y * y;
+    for (int j0 = 0; j0 < E; j0 += KB) {
+      float2 pv[KB], qv[KB];
+#pragma unroll
+      for (int b = 0; b < KB; b++) {
+        const int ky = tid + kThreads * (j0 + b);
+        if (j0 + b < E && ky < n) {
+          pv[b] = __ldg(c + ky);
+          qv[b] = __ldg(eyf + ky);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < KB; b++) {
+        const int j = j0 + b;
+        const int ky = tid + kThreads * j;
+        if (j < E && ky < n) {
+          const float2 P = cmul(pv[b], cmul(e, qv[b]));
+          const float2 d = csub(s[j], P);
+          const float2 u = cmulc(P, d);  // conj(d) * P
+          const float wi = hw[j] * u.y, wr = hw[j] * u.x, y = oy[j];
+          fx += wi;
+          fy = fmaf(wi, y, fy);
+          fxx += wr;
+          fxy = fmaf(wr, y, fxy);
+          fyy = fmaf(wr * y, y, fyy);
+        }
       }
     }
+    const double gx = fx, gy = fy, hxx = fxx, hxy = fxy, hyy = fyy;
     // omega_x is constant over the column: apply it after the sums
     double v[5] = {gx * ox, gy, hxx * ox * ox, hxy * ox, hyy};
 #pragma unroll
@@ -636,19 +657,25 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
   }
 }
 
-// Column partials -> per-frame totals in a fixed order (deterministic).
-__global__ void k_objective_reduce(ObjectiveArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nv = a.nframes * 5;
+// Column partials -> per-frame totals in a fixed order (deterministic): one
+// CTA per total, each thread a strided run of columns, then a fixed tree.
+constexpr int kReduceThreads = 256;
+__global__ void __launch_bounds__(kReduceThreads) k_objective_reduce(ObjectiveArgs a) {
+  __shared__ double part[kReduceThreads];
+  const int t = blockIdx.x, nv = a.nframes * 5;
+  double acc = 0.0;
   if (t < nv) {
-    double acc = 0.0;
-    for (int kx = 0; kx < a.H; kx++) acc += a.partial[(long long)kx * nv + t];
-    a.out[t] = -2.0 * acc;
-  } else if (t == nv) {
-    double acc = 0.0;
-    for (int kx = 0; kx < a.H; kx++) acc += a.partialJ[kx];
-    a.out[nv] = acc;
+    for (int kx = threadIdx.x; kx < a.H; kx += kReduceThreads) acc += a.partial[(long long)kx * nv + t];
+  } else {
+    for (int kx = threadIdx.x; kx < a.H; kx += kReduceThreads) acc += a.partialJ[kx];
   }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.out[t] = t < nv ? -2.0 * part[0] : part[0];
 }
 
 cudaError_t launch_ramp(const double2* shifts, int nsum, int n, float2* ey, cudaStream_t st) {
@@ -666,27 +693,22 @@ cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
   const size_t smem = sizeof(double) * (kThreads / 32) * 5 * (1 + (size_t)a.nframes) +
                       sizeof(float2) * (size_t)a.nframes;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;  // more than ~600 frames
-  cudaError_t e;
+  cudaError_t e = cudaSuccess;
   const int E = (a.n + kThreads - 1) / kThreads;
-  if (E <= 8) {
-    e = allow_smem((const void*)k_objective<8>, smem);
-    if (e != cudaSuccess) return e;
-    k_objective<8><<<a.H, kThreads, smem, st>>>(a);
-  } else if (E <= 16) {
-    e = allow_smem((const void*)k_objective<16>, smem);
-    if (e != cudaSuccess) return e;
-    k_objective<16><<<a.H, kThreads, smem, st>>>(a);
-  } else if (E <= 36) {
-    e = allow_smem((const void*)k_objective<36>, smem);
-    if (e != cudaSuccess) return e;
-    k_objective<36><<<a.H, kThreads, smem, st>>>(a);
-  } else {
-    return cudaErrorInvalidValue;
+#define MC_OBJ(EE)                                                          \
+  {                                                                         \
+    e = allow_smem((const void*)k_objective<EE>, smem);                     \
+    if (e != cudaSuccess) return e;                                         \
+    k_objective<EE><<<a.H, kThreads, smem, st>>>(a);                        \
   }
+  if (E <= 8) MC_OBJ(8)
+  else if (E <= 16) MC_OBJ(16)
+  else if (E <= 36) MC_OBJ(36)
+  else return cudaErrorInvalidValue;
+#undef MC_OBJ
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int nv = a.nframes * 5 + 1;
-  k_objective_reduce<<<(nv + 127) / 128, 128, 0, st>>>(a);
+  k_objective_reduce<<<a.nframes * 5 + 1, kReduceThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
