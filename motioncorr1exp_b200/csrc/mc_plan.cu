@@ -468,8 +468,8 @@ struct mc_plan {
 
 namespace {
 
-// launch `call` as kernel kind `kind` moving `bytes` algorithmic bytes
-// one stage of nk kernel launches, timed and counted under one kind
+// launch `call` (a stage of nk kernels) as kernel kind `kind`, moving `bytes`
+// algorithmic bytes; the stage is timed once and its nk launches counted
 #define LAUNCH_N(pl, kind, bytes, nk, call)         \
   do {                                              \
     int slot_;                                      \
