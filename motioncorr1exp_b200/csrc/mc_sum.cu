@@ -554,13 +554,23 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(C2rRowsArgs a) {
 // loads go out in batches of eight spectrum and eight ramp values before any
 // is used (issued one by one, each waited for its own latency: 3.3 ms per
 // call at 4096^2 x 60 frames, batched 2.2 ms).
-template <int E>
+//
+// STAGE (E <= 16): the column's S, weight and frequency terms live in shared
+// memory ([j][thread], each thread reading only its own entries) instead of
+// registers, which leaves room for all E spectrum and ramp loads of a frame
+// in flight at two CTAs per SM.
+template <int E, bool STAGE = false>
 __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
   constexpr int W = kThreads / 32;
+  constexpr int KB = STAGE ? E : (E < 8 ? E : 8);
+  constexpr int R = STAGE ? 1 : E;  // register copies of the column terms
   extern __shared__ double smo[];
   double* red = smo;                                                          // [warps][5] (J)
   double* fred = smo + W * 5;                                                 // [nframes][warps][5]
   float2* ex = reinterpret_cast<float2*>(fred + (size_t)a.nframes * W * 5);  // [nframes]
+  float2* ss = ex + a.nframes;                                                // [E][kThreads] (STAGE)
+  float* shw = reinterpret_cast<float*>(ss + (STAGE ? E * kThreads : 0));     // [E][kThreads]
+  float* soy = shw + (STAGE ? E * kThreads : 0);                              // [E][kThreads]
   const int n = a.n, half = n / 2;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int kx = blockIdx.x;
@@ -572,23 +582,30 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
     sincospi(2.0 * (t - rint(t)), &sn, &cn);
     ex[f] = make_float2((float)cn, (float)sn);
   }
-  float2 s[E];
-  float hw[E], oy[E];
+  float2 s[R];
+  float hw[R], oy[R];
   double jsum = 0.0;
   const float2* Scol = a.S + (long long)kx * a.ldn;
 #pragma unroll
   for (int j = 0; j < E; j++) {
     const int ky = tid + kThreads * j;
+    float2 sv = make_float2(0.f, 0.f);
+    float hv = 0.f, ov = 0.f;
     if (ky < n) {
       const int y = ky < half ? ky : ky - n;
-      s[j] = __ldg(Scol + ky);
-      hw[j] = h * expf(a.mbf * (float)(kx * kx + y * y));
-      oy[j] = 6.283185307179586f * (float)y / (float)n;
-      jsum += (double)(hw[j] * (s[j].x * s[j].x + s[j].y * s[j].y));
+      sv = __ldg(Scol + ky);
+      hv = h * expf(a.mbf * (float)(kx * kx + y * y));
+      ov = 6.283185307179586f * (float)y / (float)n;
+      jsum += (double)(hv * (sv.x * sv.x + sv.y * sv.y));
+    }
+    if constexpr (STAGE) {
+      ss[j * kThreads + tid] = sv;
+      shw[j * kThreads + tid] = hv;
+      soy[j * kThreads + tid] = ov;
     } else {
-      s[j] = make_float2(0.f, 0.f);
-      hw[j] = 0.f;
-      oy[j] = 0.f;
+      s[j] = sv;
+      hw[j] = hv;
+      oy[j] = ov;
     }
   }
   __syncthreads();
@@ -608,7 +625,6 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
     const float2* eyf = a.ey + (long long)f * n;
     const float2 e = ex[f];
     // loads in batches of KB spectrum + KB ramp values, all issued before use
-    constexpr int KB = E < 8 ? E : 8;
     float fx = 0.f, fy = 0.f, fxx = 0.f, fxy = 0.f, fyy = 0.f;
 #pragma unroll
     for (int j0 = 0; j0 < E; j0 += KB) {
@@ -626,10 +642,21 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
         const int j = j0 + b;
         const int ky = tid + kThreads * j;
         if (j < E && ky < n) {
+          float2 sj;
+          float hj, y;
+          if constexpr (STAGE) {
+            sj = ss[j * kThreads + tid];
+            hj = shw[j * kThreads + tid];
+            y = soy[j * kThreads + tid];
+          } else {
+            sj = s[j];
+            hj = hw[j];
+            y = oy[j];
+          }
           const float2 P = cmul(pv[b], cmul(e, qv[b]));
-          const float2 d = csub(s[j], P);
+          const float2 d = csub(sj, P);
           const float2 u = cmulc(P, d);  // conj(d) * P
-          const float wi = hw[j] * u.y, wr = hw[j] * u.x, y = oy[j];
+          const float wi = hj * u.y, wr = hj * u.x;
           fx += wi;
           fy = fmaf(wi, y, fy);
           fxx += wr;
@@ -695,6 +722,18 @@ cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
   if (smem > 200 * 1024) return cudaErrorInvalidValue;  // more than ~600 frames
   cudaError_t e = cudaSuccess;
   const int E = (a.n + kThreads - 1) / kThreads;
+  // staged column terms: 16 bytes per element; used while two CTAs fit an SM
+  // (MC_OBJ_REGS=1 keeps them in registers)
+  const size_t smem_st = smem + (size_t)16 * kThreads * 16;
+  if (E > 8 && E <= 16 && smem_st <= 110 * 1024 && !getenv("MC_OBJ_REGS")) {
+    e = allow_smem((const void*)k_objective<16, true>, smem_st);
+    if (e != cudaSuccess) return e;
+    k_objective<16, true><<<a.H, kThreads, smem_st, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_objective_reduce<<<a.nframes * 5 + 1, kReduceThreads, 0, st>>>(a);
+    return cudaGetLastError();
+  }
 #define MC_OBJ(EE)                                                          \
   {                                                                         \
     e = allow_smem((const void*)k_objective<EE>, smem);                     \
