@@ -557,6 +557,8 @@ def sum_objective(F: list, shifts: np.ndarray, bfactor: float):
     hess (F, 3) = (xx, xy, yy) diagonal 2x2 blocks) where, with
     P_k = F_k exp(i w.s_k) and u_k = conj(S - P_k) P_k,
         grad_k = -2 sum h w  w_vec Im(u_k),  hess_k = -2 sum h w w_vec w_vec^T Re(u_k).
+    Each P_k is formed twice (once for S, once for its terms) so that only
+    S and one P_k are held at a time.
     """
     n = F[0].shape[0]
     ky = np.arange(n)
@@ -567,12 +569,17 @@ def sum_objective(F: list, shifts: np.ndarray, bfactor: float):
     hw = h * wgt
     ox = 2.0 * math.pi * x / n
     oy = 2.0 * math.pi * y / n
-    P = [Fk * np.exp(1j * (ox * s[0] + oy * s[1])) for Fk, s in zip(F, shifts)]
-    S = np.sum(P, axis=0)
+
+    def term(k):
+        return F[k] * np.exp(1j * (ox * shifts[k][0] + oy * shifts[k][1]))
+    S = np.zeros_like(F[0], dtype=np.complex128)
+    for k in range(len(F)):
+        S += term(k)
     J = float(np.sum(hw * np.abs(S) ** 2))
     grad = np.zeros((len(F), 2))
     hess = np.zeros((len(F), 3))
-    for k, Pk in enumerate(P):
+    for k in range(len(F)):
+        Pk = term(k)
         u = np.conj(S - Pk) * Pk
         grad[k, 0] = -2.0 * np.sum(hw * ox * u.imag)
         grad[k, 1] = -2.0 * np.sum(hw * oy * u.imag)
@@ -582,9 +589,66 @@ def sum_objective(F: list, shifts: np.ndarray, bfactor: float):
     return J, grad, hess
 
 
+def newton_steps(F: list, shifts: np.ndarray, bfactor: float) -> np.ndarray:
+    """Per-frame block-Newton step -H_k^{-1} g_k of sum_objective at sum
+    shifts ``shifts`` (F, 2): the update the gradient refinement would take
+    from there in FP64 (zero for a frame whose block is not negative
+    definite).  Its length bounds how far a refined solution is from a fixed
+    point of the FP64 iteration."""
+    _, g, hs = sum_objective(F, shifts, bfactor)
+    out = np.zeros((len(F), 2))
+    for k in range(len(F)):
+        a, b, c = hs[k]
+        det = a * c - b * b
+        if a < 0.0 and det > 0.0:
+            out[k, 0] = -(c * g[k, 0] - b * g[k, 1]) / det
+            out[k, 1] = -(-b * g[k, 0] + a * g[k, 1]) / det
+    return out
+
+
 # ---------------------------------------------------------------------------
 # whole movie
 # ---------------------------------------------------------------------------
+def corrected_sum(Fa: list, shift: np.ndarray, p: Params, nstart: int, nz_file: int,
+                  want_image: bool = True):
+    """The corrected sum of DFAlign.cu:1114-1292 from per-step shifts
+    ``shift`` (nframe-1, complex): frames nStartSum..nEndSum, each shifted
+    by -cumulative + mid (mid = the steps up to nz/2+1 with -atm 1,
+    DFAlign.cu:1132-1139); the first summed frame is left unshifted unless
+    -atm 1 (DFAlign.cu:1148).  Returns (sum_shift per frame, image or None)."""
+    nframe = len(Fa)
+    nss = p.nStartSum - nstart
+    nes = p.nEndSum - nstart
+    if nss <= 0:
+        nss = 0
+    if nes <= nss or nes >= nframe:
+        nes = nframe - 1
+    mid = 0.0 + 0.0j
+    if p.bAlignToMid:
+        ref = nz_file // 2 + 1
+        if ref < nstart:
+            ref = nstart
+        # the reference reads past shift[] when ref-nstart > nframe-1; clamp
+        for jj in range(min(ref - nstart, nframe - 1)):
+            mid += shift[jj]
+    total = 0.0 + 0.0j
+    for jj in range(1, nss + 1):          # DFAlign.cu:1142-1146
+        total += shift[jj - 1]
+    sum_shift = np.zeros(nframe, dtype=np.complex128)
+    S = None
+    for k in range(nss, nes + 1):
+        if k > nss:
+            total += shift[k - 1]
+        s = -total + mid
+        sum_shift[k] = s
+        if k == nss and not p.bAlignToMid:
+            term = Fa[k]
+        else:
+            term = phase_shift(Fa[k], s.real, s.imag)
+        S = term if S is None else S + term
+    return sum_shift, (spectrum_to_image(S) if want_image else None)
+
+
 @dataclass
 class Result:
     nsam: int
@@ -602,14 +666,19 @@ class Result:
     image: Optional[np.ndarray]
     frame_mean: np.ndarray
     iter_log: list = field(default_factory=list)
+    boxes: Optional[np.ndarray] = None  # (P, box, box) CC windows when asked for
+    spectra: Optional[list] = None      # set-A spectra of the aligned frames when asked for
 
 
 def align_movie(frames: np.ndarray, mode: int, p: Params, nz_file: Optional[int] = None,
-                refs: Optional[dict] = None, want_image: bool = True, stretch=(1.0, 1.0)) -> Result:
+                refs: Optional[dict] = None, want_image: bool = True, stretch=(1.0, 1.0),
+                keep_boxes: bool = False, keep_spectra: bool = False) -> Result:
     """ThreadFunc_cuAlign (DFAlign.cu:456-1355) on decoded frames.
 
     ``frames``: raw stack (nz, ny, nx) in the file's pixel type.  ``p`` must
     already be repaired by verify_para (the CLI does it before RunAlign).
+    ``keep_boxes`` keeps every pair's CC window (hboxmap, DFAlign.cu:880) for
+    near-tie checks; ``keep_spectra`` the frames' spectra (hbuf).
     """
     nz, ny, nx = frames.shape
     if nz_file is None:
@@ -647,8 +716,11 @@ def align_movie(frames: np.ndarray, mode: int, p: Params, nz_file: Optional[int]
     bvec = np.zeros(len(pairs), dtype=np.complex128)
     cc = np.zeros(len(pairs))
     peaks = np.zeros((len(pairs), 2), dtype=np.int64)
+    boxes = np.zeros((len(pairs), box, box)) if keep_boxes else None
     for r, (i, j) in enumerate(pairs):
         bm = cc_box(cc_map(Fa[i], Fb[j], mask, n), n, box)
+        if keep_boxes:
+            boxes[r] = bm
         sx, sy, c, ix, iy = find_shift(bm, n, p.NoisePeakSize)
         bvec[r] = sx + 1j * sy
         cc[r] = c
@@ -697,39 +769,9 @@ def align_movie(frames: np.ndarray, mode: int, p: Params, nz_file: Optional[int]
     frame_shift = np.concatenate([[0.0 + 0.0j], np.cumsum(shift)])
 
     # (E) final sum: DFAlign.cu:1114-1292
-    nss = p.nStartSum - nstart
-    nes = p.nEndSum - nstart
-    if nss <= 0:
-        nss = 0
-    if nes <= nss or nes >= nframe:
-        nes = nframe - 1
-    mid = 0.0 + 0.0j
-    if p.bAlignToMid:
-        ref = nz_file // 2 + 1
-        if ref < nstart:
-            ref = nstart
-        # the reference reads past shift[] when ref-nstart > nframe-1; clamp
-        for jj in range(min(ref - nstart, nframe - 1)):
-            mid += shift[jj]
-    total = 0.0 + 0.0j
-    for jj in range(1, nss + 1):          # DFAlign.cu:1142-1146
-        total += shift[jj - 1]
-    sum_shift = np.zeros(nframe, dtype=np.complex128)
-    S = None
-    image = None
-    for k in range(nss, nes + 1):
-        if k > nss:
-            total += shift[k - 1]
-        s = -total + mid
-        sum_shift[k] = s
-        if k == nss and not p.bAlignToMid:
-            term = Fa[k]
-        else:
-            term = phase_shift(Fa[k], s.real, s.imag)
-        S = term if S is None else S + term
-    if want_image:
-        image = spectrum_to_image(S)
+    sum_shift, image = corrected_sum(Fa, shift, p, nstart, nz_file, want_image)
     return Result(nsam=n, nsam_unbin=nu, pairs=pairs, pair_shift=bvec, pair_cc=cc,
                   pair_peak=peaks, ki1=ki1, goodlist=good, ki2=ki2, shift=shift,
                   frame_shift=frame_shift, sum_shift=sum_shift, image=image,
-                  frame_mean=np.array(fmean), iter_log=iter_log)
+                  frame_mean=np.array(fmean), iter_log=iter_log, boxes=boxes,
+                  spectra=Fa if keep_spectra else None)

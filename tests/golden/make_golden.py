@@ -13,6 +13,10 @@ and, from oracle/_ref/ref_func (func.cpp's FFT-free functions):
   ref_cosmask16.c64              cosmask2d of a 16 x 16 half spectrum of ones
   func_in_400.f32, ref_dispshort_400.i16      buf2DispShort of known values
   func_in_16x9.f32, ref_moddisp_16.f32        FFTModulusToDispBuf layout
+and, from oracle/_ref/ref_solve (mfunc.h + the steps of DFAlign.cu:875-948
+against the project's SP++ stand-in):
+  ref_solve_cases.json           pair shifts in, pair list, ki1, kept rows, ki2
+                                 and per-step shifts out, for SOLVE_CASES
 """
 import json
 import gzip
@@ -31,6 +35,64 @@ from motioncorr1exp_b200 import mrc  # noqa: E402
 REF = os.path.join(ROOT, "oracle", "_ref", "ref_mrc")
 REFZ = os.path.join(ROOT, "oracle", "_ref", "ref_mrcz")
 REFF = os.path.join(ROOT, "oracle", "_ref", "ref_func")
+REFS = os.path.join(ROOT, "oracle", "_ref", "ref_solve")
+
+# (nframe, fod, kithresh, noise px, outliers, seed): exact systems, noisy ones,
+# planted outliers, thresholds that keep only a rank-deficient prefix (the
+# rank loop must add rows), the benchmark shapes (16/2, 40/7, 50/2, 60/2)
+SOLVE_CASES = [(6, 0, 1.0, 0.0, 0, 1), (12, 2, 1.0, 0.05, 2, 2), (12, 2, 0.01, 0.3, 0, 3),
+               (16, 2, 1.0, 0.1, 1, 4), (16, 2, 0.001, 0.5, 3, 5), (40, 7, 1.0, 0.2, 4, 6),
+               (40, 7, 0.05, 0.2, 0, 7), (50, 2, 1.0, 0.3, 5, 8), (60, 2, 0.2, 0.4, 6, 9),
+               (9, 4, 0.5, 1.0, 2, 10), (20, 9, 0.0, 0.1, 0, 11)]
+
+
+def run_ref_solve(nframe, fod, kithresh, b):
+    """Runs oracle/_ref/ref_solve; returns its outputs as a dict."""
+    inp = f"{nframe} {fod} {kithresh!r}\n" + "".join(f"{float(x.real)!r} {float(x.imag)!r}\n" for x in b)
+    out = subprocess.run([REFS], input=inp, check=True, capture_output=True, text=True).stdout.split("\n")
+    k = 0
+    res = {}
+    np_ = int(out[k].split()[1])
+    res["pairs"] = [[int(v) for v in out[k + 1 + i].split()] for i in range(np_)]
+    k += 1 + np_
+    assert out[k] == "ki1"
+    res["ki1"] = [float(v) for v in out[k + 1:k + 1 + np_]]
+    k += 1 + np_
+    ng = int(out[k].split()[1])
+    res["good"] = [int(v) for v in out[k + 1:k + 1 + ng]]
+    k += 1 + ng
+    assert out[k] == "ki2"
+    res["ki2"] = [float(v) for v in out[k + 1:k + 1 + ng]]
+    k += 1 + ng
+    assert out[k] == "shift"
+    res["shift"] = [[float(v) for v in out[k + 1 + i].split()] for i in range(nframe - 1)]
+    return res
+
+
+def solve_case_input(nframe, fod, noise, outliers, seed):
+    """Pair shifts of a random drift: float32-rounded like the pair stage's."""
+    rng = np.random.default_rng(seed)
+    dist = max(1, min(nframe // 2 - fod, nframe // 2))
+    pairs = [(i, j) for i in range(nframe) for j in range(i + dist, nframe)]
+    steps = rng.normal(0, 1, nframe - 1) + 1j * rng.normal(0, 1, nframe - 1)
+    b = np.array([steps[i:j].sum() for i, j in pairs])
+    b += noise * (rng.normal(size=len(pairs)) + 1j * rng.normal(size=len(pairs)))
+    for r in rng.choice(len(pairs), size=outliers, replace=False):
+        b[r] += rng.choice([-1, 1]) * rng.uniform(3, 8) + 1j * rng.uniform(-5, 5)
+    return (b.real.astype(np.float32) + 1j * b.imag.astype(np.float32)).astype(np.complex128)
+
+
+def solve_fixtures():
+    cases = []
+    for nf, fod, kit, noise, nout, seed in SOLVE_CASES:
+        b = solve_case_input(nf, fod, noise, nout, seed)
+        r = run_ref_solve(nf, fod, kit, b)
+        r.update({"nframe": nf, "fod": fod, "kithresh": kit,
+                  "b": [[float(x.real), float(x.imag)] for x in b]})
+        cases.append(r)
+    with open(os.path.join(HERE, "ref_solve_cases.json"), "w") as f:
+        json.dump(cases, f)
+        f.write("\n")
 
 CROP_CASES = [(3838, 3710, 0, 0, 0, 1.0), (7676, 7420, 0, 0, 0, 2.0), (4096, 4096, 0, 0, 0, 1.0),
               (3838, 3710, 64, 10, 0, 1.0), (3838, 3710, 0, 0, 2048, 1.0), (3838, 3710, 3000, 0, 1000, 1.0),
@@ -83,9 +145,13 @@ def stack_array(mode):
 
 
 def main():
-    if not all(os.path.exists(p) for p in (REF, REFZ, REFF)):
-        sys.exit("oracle/_ref/ref_mrc, ref_mrcz or ref_func missing: run oracle/build_ref.sh")
+    if not all(os.path.exists(p) for p in (REF, REFZ, REFF, REFS)):
+        sys.exit("oracle/_ref/ref_mrc, ref_mrcz, ref_func or ref_solve missing: run oracle/build_ref.sh")
+    if sys.argv[1:] == ["solve"]:
+        solve_fixtures()
+        return
     func_fixtures()
+    solve_fixtures()
     img = image_array()
     tmp = os.path.join(HERE, "_in.f32")
     img.tofile(tmp)

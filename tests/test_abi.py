@@ -84,6 +84,23 @@ def test_solve_pairs_matches_oracle(nframe, fod, seed):
     np.testing.assert_allclose(got["ki2"], np.abs(A[good] @ s2 - bo[good]), atol=1e-9)
 
 
+@pytest.mark.parametrize("case", range(11))
+def test_solve_pairs_matches_reference_build(case):
+    """The product's host FP64 solve against the reference's own OD_Threshold
+    and least-squares steps (mfunc.h, DFAlign.cu:875-948 built with the
+    project's SP++ stand-in; fixtures from tests/golden/make_golden.py)."""
+    import json
+    c = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_solve_cases.json")))[case]
+    nf = c["nframe"]
+    pairs = np.array(c["pairs"], dtype=np.int32)
+    b = np.array(c["b"], dtype=np.float32)
+    r = api.solve_pairs(nf, pairs, b, c["kithresh"])
+    np.testing.assert_allclose(r["ki1"], c["ki1"], rtol=0, atol=1e-9)
+    assert r["kept"].tolist() == c["good"]
+    np.testing.assert_allclose(r["ki2"], c["ki2"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(r["step"], np.array(c["shift"]), rtol=0, atol=1e-9)
+
+
 def test_solve_pairs_rejects_bad_pairs():
     with pytest.raises(_lib.McError):
         api.solve_pairs(4, np.array([[2, 1]]), np.zeros((1, 2)))

@@ -159,3 +159,28 @@ def test_graph_serves_every_bound_buffer(gpu):
         # the plan's own buffer after bound ones
         pl.load_frames(a.frames)
         np.testing.assert_array_equal(pl.run(), ref_a[0])
+
+
+def _build_stress(tmp_path, libdir, extra=()):
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "batch_stress")
+    subprocess.run(["g++", "-O1", "-g", "-std=c++17", *extra, "-I", os.path.join(root, "include"),
+                    "-I", "/usr/local/cuda/include", os.path.join(root, "tests", "native", "batch_stress.cpp"),
+                    "-L", libdir, "-lmc", "-L", "/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{libdir}",
+                    "-o", exe], check=True, capture_output=True)
+    return exe
+
+
+def test_batch_stress_native(gpu, tmp_path):
+    """Three lanes, 30 movies of three geometries and two pixel types, frames
+    in device, pinned and pageable host memory, three rounds (plans
+    re-targeted, graphs replayed, the queue reversed): every image and shift
+    list bit-identical to a fresh one-at-a-time plan."""
+    import os
+    import subprocess
+    exe = _build_stress(tmp_path, os.path.dirname(_lib.LIB_PATH))
+    r = subprocess.run([exe, "3", "30", "3"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "0 mismatches" in r.stdout
