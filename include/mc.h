@@ -208,8 +208,8 @@ int mc_solve_pairs(int nframe, int npairs, const int* ij, const float* shifts_xy
  * device memory -- code inside a detector's acquisition/streaming loop that
  * owns a fixed, pre-reserved memory budget, or a host framework that forbids
  * allocation once its own pool is set up: the pbx x pbx cross-correlation
- * window of one frame pair (what GPUShiftCC + GPUIFFT2d + the FindShift box
- * copy produce, cufunc.cu:343-407), computed with no cudaMalloc/cudaFree and
+ * window of one frame pair, the same window a plan's pair stage stores for
+ * that pair (mc_plan_get_boxes), computed with no cudaMalloc/cudaFree and
  * no allocating library call.  Inputs: two half spectra already on the
  * device in this library's layout (spec[kx*ldn + ky], kx <= n/2, ky < n);
  * output: d_window, pbx*pbx floats on the device.  Intermediate data lives in
@@ -304,7 +304,7 @@ typedef struct mc_schedule {
   int n;             /* binned side the entry applies to */
   int pair_q;        /* codelet length Q of the split n = P*Q (0 = built-in cost model) */
   int pairs_per_cta; /* pairs per CTA of the pair column stage (0 = 32) */
-  int pair_variant;  /* 0 register codelets, 1 grouped cp.async (even n) */
+  int pair_variant;  /* reserved: 0 (the register-codelet column kernel) */
 } mc_schedule;
 int mc_schedule_set(const mc_schedule* s); /* replaces the entry for s->n */
 int mc_schedule_get(int n, mc_schedule* out); /* MC_E_ARG when none is set */

@@ -2,6 +2,11 @@
 
     python -m motioncorr1exp_b200.build            # build what is stale
     python -m motioncorr1exp_b200.build --force    # rebuild everything
+    python -m motioncorr1exp_b200.build --sanitize address
+        # host code instrumented by AddressSanitizer, into lib_asan/ (for
+        # hunting host memory errors; load it from an instrumented program,
+        # e.g. tests/native/batch_stress.cpp, with
+        # ASAN_OPTIONS=protect_shadow_gap=0 so CUDA can map its memory)
 
 Outputs go to motioncorr1exp_b200/lib/ (git-ignored, shipped with the tree).
 """
@@ -56,9 +61,11 @@ def _run(cmd: list[str], verbose: bool) -> None:
         sys.stderr.write(r.stdout + r.stderr)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(LIB, exist_ok=True)
-    objdir = os.path.join(LIB, "obj")
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, sanitize: str = "") -> str:
+    lib = os.path.join(HERE, "lib_asan") if sanitize else LIB
+    san = ["-Xcompiler", f"-fsanitize={sanitize}", "-Xcompiler", "-fno-omit-frame-pointer"] if sanitize else []
+    os.makedirs(lib, exist_ok=True)
+    objdir = os.path.join(lib, "obj")
     os.makedirs(objdir, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in LIB_HEADERS] + [os.path.join(INCLUDE, "mc.h")]
     objs, jobs = [], []
@@ -67,21 +74,23 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         o = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
+            cmd = [nvcc()] + ARCH + NVCC_FLAGS + san + ["-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
             if ptxas_info and s.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             if s.endswith(".cpp"):
-                cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
-                       "-x", "c++", "-c", s, "-o", o]
+                cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC"] + san + ["-I", INCLUDE, "-I", CSRC,
+                                                                                    "-x", "c++", "-c", s, "-o", o]
             jobs.append(cmd)
     # translation units compile in parallel (the kernel file dominates)
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         for f in [ex.submit(_run, c, verbose or ptxas_info) for c in jobs]:
             f.result()
-    so = os.path.join(LIB, "libmc.so")
+    so = os.path.join(lib, "libmc.so")
     if force or _stale(so, objs):
-        _run([nvcc()] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart", "-lz", "-lpthread"], verbose)
+        _run([nvcc()] + ARCH + san + ["-shared", "-o", so] + objs + ["-lcudart", "-lz", "-lpthread"], verbose)
+    if sanitize:
+        return so
     cli = os.path.join(LIB, "dosefgpu_driftcorr")
     cli_src = [os.path.join(CSRC, c) for c in CLI_SOURCES]
     if all(os.path.exists(c) for c in cli_src):
@@ -98,8 +107,9 @@ def main() -> None:
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true", help="print registers / spills per kernel")
+    ap.add_argument("--sanitize", default="", help="e.g. address: instrumented host code into lib_asan/")
     a = ap.parse_args()
-    print(build(a.force, a.verbose, a.ptxas_info))
+    print(build(a.force, a.verbose, a.ptxas_info, a.sanitize))
 
 
 if __name__ == "__main__":

@@ -80,8 +80,6 @@ struct PairColsArgs {
   int box;
   int ystart;
   float2* G;           // [npairs][H][box]
-  int variant;         // 0: compiled (Q, P) split when there is one (recurrence twiddles);
-                       // 1: runtime-P register kernel; 2: compiled split, table twiddles
 };
 
 // Row stage: box[p][yb][xb] = sum_kx Re(G[p][kx][yb] * h(kx) exp(+2 pi i kx x_xb / n))
@@ -92,9 +90,9 @@ struct PairRowsArgs {
   const float2* cs;    // [H][box]
   float* boxes;        // [npairs][box][box]
   // when set with a compiled split n = P*Q: the pruned-transform row kernel
-  // (twO and ystart as in PairColsArgs); variant 1 keeps the product kernel
+  // (twO and ystart as in PairColsArgs); otherwise the product kernel
   const float2* twO;
-  int P, Q, ystart, variant;
+  int P, Q, ystart;
 };
 
 // Peak: integer argmax over the box, 16x16 sub-box, x32 Fourier upsampling,
@@ -275,13 +273,12 @@ cudaError_t allow_smem(const void* func, size_t bytes);
 
 // true when the register-codelet column stage handles the split n = P*Q
 bool pair_cols_reg_supported(int P, int Q);
+// the split n = P*Q a plan's register-codelet column stage uses for (n, box)
+// (schedule or cost model); false when n has none (mc_plan.cu)
+bool reg_pair_split(int n, int box, int* P, int* Q);
 size_t pair_cols_reg_smem(int n, int team);
 // dynamic shared memory launch_pair_cols asks for with this split
 size_t pair_cols_launch_smem(int n, int P, int Q, int box);
-// grouped column stage: groups[g] = (first pair, count) of pairs sharing A
-size_t pair_cols_grp_smem(int n, int teams);
-cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,
-                                     cudaStream_t st);
 
 size_t fwd_rows_smem(int nu);
 size_t rows_fft_smem(int n, int rows_per_cta);

@@ -5,9 +5,11 @@
 // budget (an allocation there can block the loop or fail under memory
 // pressure), and host frameworks that forbid allocation once their own
 // memory pool is set up.  For them mc_pair_window_static() computes the
-// reference's pbx x pbx CC window (GPUShiftCC + GPUIFFT2d + the FindShift box
-// copy, cufunc.cu:343-407) for two spectra the caller already holds, using
-// only the file-scope scratch array below for its intermediate data.
+// pbx x pbx CC window of one frame pair that a plan's pair stage computes
+// (the reference's GPUShiftCC + GPUIFFT2d + the FindShift box copy,
+// cufunc.cu:343-407) for two spectra the caller already holds, with the same
+// column kernel and split as the plan, using only the file-scope scratch
+// array below for its intermediate data.
 //
 // Limits: n even, 16 <= n <= 4096, 16 <= pbx <= min(128, n), and n must split
 // as n = P*Q with P <= 128 and Q one of the register-codelet lengths.  The
@@ -84,46 +86,6 @@ __global__ void k_noalloc_tables(float2* two, float2* cs, int2* pair, int n, int
   if (blockIdx.x == 0 && threadIdx.x == 0) *pair = make_int2(0, 0);
 }
 
-// Per-point cost of a codelet of length q (odd radices, then 8/4/2): the
-// same model the plan uses to split n = P*Q.
-double codelet_cost(int q) {
-  double c = 0.0;
-  int stages = 0, m = q;
-  const int odd[] = {7, 5, 3};
-  const double odd_cost[] = {5.0, 4.0, 3.0};
-  for (int i = 0; i < 3; i++)
-    while (m % odd[i] == 0) {
-      c += odd_cost[i] + (stages++ ? 2.0 : 0.0);
-      m /= odd[i];
-    }
-  int twos = 0;
-  while (m % 2 == 0) {
-    twos++;
-    m /= 2;
-  }
-  while (twos > 0) {
-    const int r = (twos == 4 || twos == 2) ? 2 : (twos >= 3 ? 3 : 1);  // log2 of 4, 8, 2
-    c += (r == 3 ? 3.0 : r == 2 ? 2.5 : 2.0) + (stages++ ? 2.0 : 0.0);
-    twos -= r;
-  }
-  return c;
-}
-
-bool pick_split(int n, int box, int* P, int* Q) {
-  double best = 1e300;
-  *P = 0;
-  for (int q = 2; q <= n; q++) {
-    if (n % q || !mc::pair_cols_reg_supported(n / q, q)) continue;
-    const double cost = (double)n * codelet_cost(q) + 4.0 * box * (n / q);
-    if (cost < best) {
-      best = cost;
-      *P = n / q;
-      *Q = q;
-    }
-  }
-  return *P > 0;
-}
-
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
@@ -137,7 +99,7 @@ int mc_pair_window_static(const void* d_spec_a, const void* d_spec_b, int n, int
   if (ldn < n) return fail(MC_E_ARG, "ldn < n");
   if (pbx < 16 || pbx > kNoAllocMaxBox || pbx > n) return fail(MC_E_SIZE, "pbx must be in [16, min(128, n)]");
   int P = 0, Q = 0;
-  if (!pick_split(n, pbx, &P, &Q)) return fail(MC_E_SIZE, "n has no register-codelet split");
+  if (!mc::reg_pair_split(n, pbx, &P, &Q)) return fail(MC_E_SIZE, "n has no register-codelet split");
   const int H = n / 2 + 1;
   const size_t off_two = 256;  // the int2 pair record sits at the start
   const size_t off_cs = off_two + align256(sizeof(float2) * (size_t)P * pbx);
@@ -155,6 +117,9 @@ int mc_pair_window_static(const void* d_spec_a, const void* d_spec_b, int n, int
   cudaStream_t st = (cudaStream_t)stream;
   const int ori = (n - pbx) / 2;
   const int ystart = (ori + n / 2) % n;
+  // an error left by an earlier, unrelated launch must not be reported as
+  // this call's failure
+  (void)cudaGetLastError();
   k_noalloc_tables<<<64, 256, 0, st>>>(two, cs, pair, n, pbx, P, H, ystart);
   if (cudaGetLastError() != cudaSuccess) return fail(MC_E_CUDA, "table kernel launch failed");
   mc::PairColsArgs a{};

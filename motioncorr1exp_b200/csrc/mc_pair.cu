@@ -201,9 +201,7 @@ size_t pair_cols_rp_smem(int n, int yn, int team, int chunks, int box) {
          (size_t)teams * ((size_t)yn + (size_t)chunks * box) * sizeof(float2);
 }
 
-// HORNER = false: each twiddle W^(k1 y_m) loaded from twO (the measured
-// slower form, kept for comparison).
-template <int Q, int P, bool HORNER>
+template <int Q, int P>
 __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_cols_rp(PairColsArgs a) {
   using S = RpShape<Q, P>;
   constexpr int T = S::T, C = S::C, L = S::L, N = P * Q, PS = S::PS, YN = S::YN;
@@ -252,38 +250,26 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
       if (r >= Q) r -= Q;
       const int kb = c * L;
       const float2* yr = Y + PS * r + kb;
-      float2 acc = make_float2(0.f, 0.f);
-      if (HORNER) {
-        // two independent chains over the even and odd terms in w^2, then
-        // S = S_even + w S_odd: twice the instruction-level parallelism of
-        // one chain of dependent FMAs
-        const float2 w = tws[m];
-        const float2 w2 = cmul(w, w);
-        float2 ae = make_float2(0.f, 0.f), ao = make_float2(0.f, 0.f);
+      // two independent chains over the even and odd terms in w^2, then
+      // S = S_even + w S_odd: twice the instruction-level parallelism of one
+      // chain of dependent FMAs
+      const float2 w = tws[m];
+      const float2 w2 = cmul(w, w);
+      float2 ae = make_float2(0.f, 0.f), ao = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int kk = L - 1; kk >= 0; kk--) {
-          if (L * C == P || kb + kk < P) {
-            const float2 yv = yr[kk];
-            float2& h = (kk & 1) ? ao : ae;
-            const float2 s = h;
-            h.x = fmaf(s.x, w2.x, fmaf(-s.y, w2.y, yv.x));
-            h.y = fmaf(s.x, w2.y, fmaf(s.y, w2.x, yv.y));
-          }
-        }
-        acc.x = fmaf(ao.x, w.x, fmaf(-ao.y, w.y, ae.x));
-        acc.y = fmaf(ao.x, w.y, fmaf(ao.y, w.x, ae.y));
-        if (kb < P) acc = cmul(acc, tws[(1 + c) * box + m]);
-      } else {
-#pragma unroll
-        for (int kk = 0; kk < L; kk++) {
-          if (L * C == P || kb + kk < P) {
-            const float2 t = __ldg(a.twO + (long long)(kb + kk) * box + m);
-            const float2 yv = yr[kk];
-            acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
-            acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
-          }
+      for (int kk = L - 1; kk >= 0; kk--) {
+        if (L * C == P || kb + kk < P) {
+          const float2 yv = yr[kk];
+          float2& h = (kk & 1) ? ao : ae;
+          const float2 s = h;
+          h.x = fmaf(s.x, w2.x, fmaf(-s.y, w2.y, yv.x));
+          h.y = fmaf(s.x, w2.y, fmaf(s.y, w2.x, yv.y));
         }
       }
+      float2 acc;
+      acc.x = fmaf(ao.x, w.x, fmaf(-ao.y, w.y, ae.x));
+      acc.y = fmaf(ao.x, w.y, fmaf(ao.y, w.x, ae.y));
+      if (kb < P) acc = cmul(acc, tws[(1 + c) * box + m]);
       part[c * box + m] = acc;
       m += T;
       while (m >= box) {
@@ -444,129 +430,6 @@ size_t pair_cols_launch_smem(int n, int P, int Q, int box) {
   return pair_cols_smem(n, P, Q, box) + 16;
 }
 
-// ---- grouped variant: one CTA per (A frame group, column kx) -------------
-// The pairs of a batch come in groups that share their A spectrum (the
-// reference's i-major order).  The CTA stages A(kx,:) x B-factor once in
-// shared memory; each team double-buffers the B columns of its pairs with
-// 16-byte cp.async copies, so the copy of pair p+1 overlaps the transform of
-// pair p.  Thread k1 reads only positions k1 + P*k2 of the B buffer and
-// writes Y back to the same positions, so Y lives in the consumed buffer.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-size_t pair_cols_grp_smem(int n, int teams) { return (size_t)(1 + 2 * teams) * n * sizeof(float2); }
-
-template <int Q>
-__global__ void __launch_bounds__(kRegThreads) k_pair_cols_grp(PairColsArgs a, const int2* __restrict__ groups,
-                                                               int team) {
-  extern __shared__ float2 smg[];
-  const int n = a.n, P = a.P, box = a.box;
-  const int teams = kRegThreads / team;
-  const int tid = threadIdx.x;
-  const int tm = tid / team, lt = tid - tm * team;
-  float2* aw = smg;
-  float2* buf0 = smg + n + (size_t)2 * tm * n;
-  const int kx = blockIdx.y;
-  const int2 g = groups[blockIdx.x];  // (first pair, count)
-  const int half = n / 2;
-  const int2 pr0 = a.pairs[g.x];
-  const float2* ca = a.specA + (long long)pr0.x * a.strideA + (long long)kx * a.ldn;
-  for (int ky = tid; ky < n; ky += kRegThreads) {
-    const int y = ky < half ? ky : ky - n;
-    const float w = expf(a.mbf * (float)(kx * kx + y * y)) * a.inv_size;
-    aw[ky] = cscale(__ldg(ca + ky), w);
-  }
-  const int nchunk = n / 2;  // 16-byte chunks of a column (n is even)
-  auto fetch = [&](int q, float2* dst) {
-    const int2 pr = a.pairs[g.x + q];
-    const float2* cb = a.specB + (long long)pr.y * a.strideB + (long long)kx * a.ldn;
-    for (int c = lt; c < nchunk; c += team) cp_async16(dst + 2 * c, cb + 2 * c);
-  };
-  int cur = 0;
-  if (tm < g.y) fetch(tm, buf0);
-  cp_async_commit();
-  __syncthreads();  // aw visible to every team
-  const int khalf = (P + 1) / 2;
-  for (int q = tm; q < g.y; q += teams) {
-    float2* bc = buf0 + (size_t)cur * n;
-    if (q + teams < g.y) fetch(q + teams, buf0 + (size_t)(cur ^ 1) * n);
-    cp_async_commit();
-    cp_async_wait<1>();
-    team_barrier(1 + tm, team);
-    if (lt < P) {
-      float2 x[Q];
-#pragma unroll
-      for (int k2 = 0; k2 < Q; k2++) {
-        const int ky = lt + P * k2;
-        x[k2] = cmulc(aw[ky], bc[ky]);
-      }
-      fft_reg<Q, true>(x);
-#pragma unroll
-      for (int r = 0; r < Q; r++) bc[lt + P * r] = x[r];
-    }
-    team_barrier(1 + tm, team);
-    const int p = g.x + q;
-    for (int base = 0; base < 2 * box; base += team) {
-      const int o = base + lt;
-      const bool ok = o < 2 * box;
-      const int m = o >> 1, h = o & 1;
-      float2 acc = make_float2(0.f, 0.f);
-      if (ok) {
-        const int r = (a.ystart + m) % Q;
-        const int k0 = h ? khalf : 0, k1 = h ? P : khalf;
-        const float2* yr = bc + P * r;
-        const float2* tw = a.twO + m;
-        for (int k = k0; k < k1; k++) {
-          const float2 t = __ldg(tw + k * box);
-          const float2 yv = yr[k];
-          acc.x = fmaf(t.x, yv.x, fmaf(-t.y, yv.y, acc.x));
-          acc.y = fmaf(t.x, yv.y, fmaf(t.y, yv.x, acc.y));
-        }
-      }
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-      if (ok && h == 0) a.G[((long long)p * a.H + kx) * box + m] = acc;
-    }
-    team_barrier(1 + tm, team);  // buffer `cur` may now be refilled
-    cur ^= 1;
-  }
-  cp_async_wait<0>();
-}
-
-template <int Q>
-cudaError_t launch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
-  const size_t smem = pair_cols_grp_smem(a.n, kRegThreads / team);
-  cudaError_t e = allow_smem((const void*)k_pair_cols_grp<Q>, smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid(ngroups, a.H);
-  k_pair_cols_grp<Q><<<grid, kRegThreads, smem, st>>>(a, groups, team);
-  return cudaGetLastError();
-}
-
-template <int I = 0>
-cudaError_t dispatch_grp(const PairColsArgs& a, const int2* groups, int ngroups, int team, cudaStream_t st) {
-  if constexpr (I < kNumCodelets) {
-    constexpr int Q = kCodelets[I];
-    if (a.Q == Q) return launch_grp<Q>(a, groups, ngroups, team, st);
-    return dispatch_grp<I + 1>(a, groups, ngroups, team, st);
-  } else {
-    return cudaErrorInvalidValue;
-  }
-}
-
-cudaError_t launch_pair_cols_grouped(const PairColsArgs& a, const int2* groups, int ngroups, int team,
-                                     cudaStream_t st) {
-  if (!pair_cols_reg_supported(a.P, a.Q) || (a.n & 1)) return cudaErrorInvalidValue;
-  return dispatch_grp(a, groups, ngroups, team, st);
-}
-
 bool pair_cols_reg_supported(int P, int Q) {
   if (P < 1 || P > kRegThreads) return false;
   for (int q : kCodelets)
@@ -595,20 +458,16 @@ cudaError_t dispatch_reg(const PairColsArgs& a, int team, size_t smem, dim3 grid
 
 cudaError_t launch_pair_cols(const PairColsArgs& a, cudaStream_t st) {
   dim3 grid((a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta, a.H);
-  if (a.variant != 1) {
-#define MC_RP_LAUNCH(A, B)                                                                    \
-  if (a.Q == (A) && a.P == (B) && a.n == (A) * (B)) {                                        \
+#define MC_RP_LAUNCH(A, B)                                                                                  \
+  if (a.Q == (A) && a.P == (B) && a.n == (A) * (B)) {                                                      \
     const size_t smem = pair_cols_rp_smem(a.n, RpShape<A, B>::YN, RpShape<A, B>::T, RpShape<A, B>::C, a.box); \
-    const void* fn = a.variant == 2 ? (const void*)k_pair_cols_rp<A, B, false> : (const void*)k_pair_cols_rp<A, B, true>; \
-    cudaError_t e = allow_smem(fn, smem);                                                    \
-    if (e != cudaSuccess) return e;                                                          \
-    if (a.variant == 2) k_pair_cols_rp<A, B, false><<<grid, kRegThreads, smem, st>>>(a);     \
-    else k_pair_cols_rp<A, B, true><<<grid, kRegThreads, smem, st>>>(a);                     \
-    return cudaGetLastError();                                                               \
+    cudaError_t e = allow_smem((const void*)k_pair_cols_rp<A, B>, smem);                                   \
+    if (e != cudaSuccess) return e;                                                                        \
+    k_pair_cols_rp<A, B><<<grid, kRegThreads, smem, st>>>(a);                                              \
+    return cudaGetLastError();                                                                             \
   }
-    MC_RP_LIST(MC_RP_LAUNCH)
+  MC_RP_LIST(MC_RP_LAUNCH)
 #undef MC_RP_LAUNCH
-  }
   if (pair_cols_reg_supported(a.P, a.Q)) {
     const int team = a.P <= 32 ? 32 : (a.P <= 64 ? 64 : 128);
     return dispatch_reg(a, team, pair_cols_reg_smem(a.n, team), grid, st);
@@ -680,7 +539,7 @@ __global__ void __launch_bounds__(kThreads) k_pair_rows(PairRowsArgs a) {
 }
 
 cudaError_t launch_pair_rows(const PairRowsArgs& a, cudaStream_t st) {
-  if (a.twO && a.variant == 0) {
+  if (a.twO) {
 #define MC_RP_ROWS(A, B)                                                                            \
   if (a.Q == (A) && a.P == (B) && 2 * (a.H - 1) == (A) * (B)) {                                    \
     constexpr int rows = 2 * (kRegThreads / RpShape<A, B>::T);                                     \

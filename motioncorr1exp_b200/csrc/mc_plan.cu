@@ -165,23 +165,23 @@ bool find_schedule(int n, mc_schedule* out) {
   return true;
 }
 
-// n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
-void choose_prune(int n, int box, int& P, int& Q) {
-  // MC_PRUNE_Q=<q> forces the split n = (n/q)*q when the codelet kernel takes
-  // it; next a schedule set for this n
+}  // namespace
+
+// n = P*Q split of the register-codelet column kernel: the split a schedule
+// set for n names (mc_schedule_set), else the cheapest by the codelet cost
+// model (Q-point FFTs of the P subsequences + 4*box*P outer-sum terms).
+// Shared by the plans and mc_pair_window_static, so both run the same kernel.
+bool mc::reg_pair_split(int n, int box, int* Pout, int* Qout) {
   int want = 0;
-  if (const char* env = getenv("MC_PRUNE_Q")) want = atoi(env);
   mc_schedule sc;
-  if (want <= 0 && find_schedule(n, &sc)) want = sc.pair_q;
+  if (find_schedule(n, &sc)) want = sc.pair_q;
   if (want > 1 && n % want == 0 && mc::pair_cols_reg_supported(n / want, want)) {
-    P = n / want;
-    Q = want;
-    return;
+    *Pout = n / want;
+    *Qout = want;
+    return true;
   }
-  // first choice: a split the register-codelet kernel handles
   double best = 1e300;
-  P = 0;
-  Q = 0;
+  int P = 0, Q = 0;
   for (int q = 2; q <= n; q++) {
     if (n % q || !mc::pair_cols_reg_supported(n / q, q)) continue;
     std::vector<int> rad = factor_radices(q);
@@ -194,7 +194,18 @@ void choose_prune(int n, int box, int& P, int& Q) {
       Q = q;
     }
   }
-  if (P) return;
+  if (!P) return false;
+  *Pout = P;
+  *Qout = Q;
+  return true;
+}
+
+namespace {
+
+// n = P*Q for the pruned inverse: Q-point FFTs + P-term output sums.
+void choose_prune(int n, int box, int& P, int& Q) {
+  double best = 1e300;
+  if (mc::reg_pair_split(n, box, &P, &Q)) return;
   // otherwise the shared-memory kernel
   P = n;
   Q = 1;
@@ -293,8 +304,6 @@ struct mc_plan {
   float2* d_twN = nullptr;  // length-n outer table of the generic pair kernel (large P x box)
   double* d_w16 = nullptr;
   int2* d_pairs = nullptr;
-  int2* d_groups = nullptr;
-  bool grouped = false;  // grouped (cp.async, A staged once) column stage
   float2* d_G = nullptr;
   float* d_boxes = nullptr;
   float *d_pshift = nullptr, *d_pcc = nullptr;
@@ -519,10 +528,6 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     a.twN = pl->d_twN;
     a.box = pl->box;
     a.ystart = pl->ystart;
-    // MC_PAIR_RP=0 selects the runtime-P register kernel over the compiled split,
-    // MC_PAIR_RP=2 the compiled split with table twiddles
-    a.variant = getenv("MC_PAIR_RP") ? std::min(2, std::max(0, atoi(getenv("MC_PAIR_RP")))) : 0;
-    if (a.variant == 0 && getenv("MC_PAIR_RP")) a.variant = 1;
     a.G = pl->d_G;
     // algorithmic bytes: every distinct spectrum the batch touches read once,
     // the column-stage output written once
@@ -544,19 +549,7 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     }
     const double gbytes = (double)nb * pl->H * pl->box * sizeof(float2);
     const double cbytes = (double)nspec * pl->H * pl->n * sizeof(float2) + gbytes;
-    if (pl->grouped) {
-      // runs of consecutive pairs that share their A spectrum
-      std::vector<int2> groups;
-      for (int i = 0; i < nb; i++) {
-        if (i == 0 || list[p0 + i].first != list[p0 + i - 1].first) groups.push_back(make_int2(i, 0));
-        groups.back().y++;
-      }
-      CK(cudaMemcpyAsync(pl->d_groups, groups.data(), sizeof(int2) * groups.size(), cudaMemcpyHostToDevice, pl->st));
-      LAUNCH(pl, MC_K_PAIR_COLS, cbytes,
-             mc::launch_pair_cols_grouped(a, pl->d_groups, (int)groups.size(), pl->P <= 64 ? 64 : 128, pl->st));
-    } else {
-      LAUNCH(pl, MC_K_PAIR_COLS, cbytes, mc::launch_pair_cols(a, pl->st));
-    }
+    LAUNCH(pl, MC_K_PAIR_COLS, cbytes, mc::launch_pair_cols(a, pl->st));
     mc::PairRowsArgs r{};
     r.G = pl->d_G;
     r.npairs = nb;
@@ -568,8 +561,6 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
     r.P = pl->P;
     r.Q = pl->Q;
     r.ystart = pl->ystart;
-    // MC_PAIR_ROWS=0 keeps the dense product kernel
-    r.variant = (getenv("MC_PAIR_ROWS") && atoi(getenv("MC_PAIR_ROWS")) == 0) ? 1 : 0;
     LAUNCH(pl, MC_K_PAIR_ROWS,
            gbytes + (double)pl->H * pl->box * sizeof(float2) + (double)nb * pl->box * pl->box * sizeof(float),
            mc::launch_pair_rows(r, pl->st));
@@ -777,7 +768,7 @@ int mc_plan_create_capacity(const mc_params* pin, int nx, int ny, int nz, int mo
 
 int mc_schedule_set(const mc_schedule* s) {
   if (!s) return set_err(MC_E_ARG, "null schedule");
-  if (s->n < 16 || s->pair_q < 0 || s->pairs_per_cta < 0 || s->pair_variant < 0 || s->pair_variant > 1)
+  if (s->n < 16 || s->pair_q < 0 || s->pairs_per_cta < 0 || s->pair_variant != 0)
     return set_err(MC_E_ARG, "bad schedule for n=%d", s->n);
   if (s->pair_q > 1 && (s->n % s->pair_q || !mc::pair_cols_reg_supported(s->n / s->pair_q, s->pair_q)))
     return set_err(MC_E_ARG, "pair stage takes no split %d = %d * %d", s->n, s->n / std::max(s->pair_q, 1),
@@ -876,15 +867,8 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
     const size_t need = std::max(mc::pair_cols_launch_smem(pl->n, pl->P, pl->Q, pl->box),
                                  reg ? mc::pair_cols_reg_smem(pl->n, team) : (size_t)0);
     if (need > 227 * 1024) return set_err(MC_E_SIZE, "pair stage does not fit shared memory for n=%d", pl->n);
-    // grouped variant: A column + two B buffers per team (teams = 128 / team)
-    const int gteam = pl->P <= 64 ? 64 : 128;
-    // measured slower than the ungrouped kernel at n = 3710 (1 CTA per SM:
-    // shared-memory bound), so it runs only when asked for
-    const char* env = getenv("MC_PAIR_KERNEL");
     mc_schedule sc{};
     const bool have_sc = find_schedule(pl->n, &sc);
-    const bool want_grp = env ? std::strcmp(env, "grp") == 0 : (have_sc && sc.pair_variant == 1);
-    pl->grouped = reg && (pl->n % 2 == 0) && mc::pair_cols_grp_smem(pl->n, 128 / gteam) <= 227 * 1024 && want_grp;
     pl->ppc = (have_sc && sc.pairs_per_cta > 0) ? std::min(sc.pairs_per_cta, 512) : kPairsPerCta;
   }
 
@@ -905,7 +889,6 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   pl->d_specB = pl->d_specA;
   if (pl->nu != pl->n) CKR(pl->alloc(&pl->d_T, sizeof(float2) * (size_t)pl->H * pl->ldu));
   CKR(pl->alloc(&pl->d_pairs, sizeof(int2) * pl->maxp));
-  CKR(pl->alloc(&pl->d_groups, sizeof(int2) * pl->maxp));
   CKR(pl->alloc(&pl->d_G, sizeof(float2) * (size_t)std::min(pl->maxp, kPairBatch) * pl->H * pl->box));
   CKR(pl->alloc(&pl->d_boxes, sizeof(float) * (size_t)pl->maxp * pl->box * pl->box));
   CKR(pl->alloc(&pl->d_pshift, sizeof(float) * 2 * pl->maxp));
@@ -915,9 +898,9 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   CKR(pl->alloc(&pl->d_T2, sizeof(float2) * (size_t)pl->n * pl->ldt2));
   {
     // image sums of two-level sizes accumulate into d_sumacc, then transform
-    // (MC_SUM_FUSED=1 keeps the single fused kernel)
+    // (other sizes run the single fused kernel)
     int n1, n2;
-    if (mc::two_level_split(pl->n, n1, n2) && !getenv("MC_SUM_FUSED"))
+    if (mc::two_level_split(pl->n, n1, n2))
       CKR(pl->alloc(&pl->d_sumacc, sizeof(float2) * pl->fstride));
   }
   CKR(pl->alloc(&pl->d_ey, sizeof(float2) * (size_t)capf * pl->n));
@@ -1197,8 +1180,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
   // frames write only their own spectrum slots unless a shared scratch is in
   // play (binning's row buffer, the stretched frame); per-launch timing
   // events need the one stream
-  const bool multi = !binned && !pl->stretch && pl->nframe > 1 && !(pl->profiling && !pl->capturing) &&
-                     !getenv("MC_FORWARD_ONE_STREAM");
+  const bool multi = !binned && !pl->stretch && pl->nframe > 1 && !(pl->profiling && !pl->capturing);
   constexpr int NS = mc_plan::kForwardStreams;
   if (multi) {
     for (int i = 0; i < NS; i++) {
@@ -2117,9 +2099,9 @@ static int finish_device_movie(mc_plan* pl) {
 }
 
 // Whole movie on the device with one synchronisation; captured once into a
-// CUDA graph and replayed (unless profiling, MC_NO_GRAPH, or a capture failure).
+// CUDA graph and replayed (unless profiling or a capture failure).
 static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEvent_t>* waits, int chunk) {
-  const bool graph_ok = !waits && !pl->profiling && !pl->graph_failed && !getenv("MC_NO_GRAPH");
+  const bool graph_ok = !waits && !pl->profiling && !pl->graph_failed;
   CKR(upload_frame_base(pl));
   CK(cudaEventRecord(pl->ev[0], pl->st));
   mc_plan::GraphEntry* ge = nullptr;
@@ -2191,7 +2173,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
   return finish_device_movie(pl);
 }
 
-static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine && !pl->grouped; }
+static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine; }
 
 extern "C" {
 

@@ -723,9 +723,8 @@ cudaError_t launch_objective(const ObjectiveArgs& a, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   const int E = (a.n + kThreads - 1) / kThreads;
   // staged column terms: 16 bytes per element; used while two CTAs fit an SM
-  // (MC_OBJ_REGS=1 keeps them in registers)
   const size_t smem_st = smem + (size_t)16 * kThreads * 16;
-  if (E > 8 && E <= 16 && smem_st <= 110 * 1024 && !getenv("MC_OBJ_REGS")) {
+  if (E > 8 && E <= 16 && smem_st <= 110 * 1024) {
     e = allow_smem((const void*)k_objective<16, true>, smem_st);
     if (e != cudaSuccess) return e;
     k_objective<16, true><<<a.H, kThreads, smem_st, st>>>(a);
