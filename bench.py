@@ -277,6 +277,14 @@ def run_ours(args):
                                            kind=w["kind"], speed=w.get("speed", 0.4),
                                            rw_sigma=w.get("rw_sigma", 0.3), amp=w.get("amp", 1.5),
                                            period=w.get("period", 20.0), device=f"cuda:{local}")
+    if args.storage == "f16":
+        # integer counts held as IEEE half (MRC2014 mode 12): exact below 2048
+        if mode != 2:
+            raise SystemExit("--storage f16 applies to float32 workloads (c1, c4)")
+        if bool((frames != frames.round()).any()) or float(frames.abs().max()) > 2048:
+            raise SystemExit("--storage f16 needs integer counts below 2048")
+        frames = frames.half()
+        mode = api.MODE_F16
     host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)
     host.copy_(frames)
     p = c2_params(api) if args.workload == "c2" else api.Params(**flags)
@@ -426,6 +434,8 @@ def run_ours(args):
                 "config": {"workload": (WORKLOAD if nz == 40 else f"profiling case: {nz} frames, else as c2")
                            if args.workload == "c2" else WORKLOADS_TEXT[args.workload],
                            "nsam": plan.nsam, "pairs": plan.npairs,
+                           "frame_storage": ("IEEE half (MRC mode 12), exact for these counts"
+                                             if args.storage == "f16" else "file pixel type"),
                            "l2": "inputs larger than L2 (570 MB frames, 2.2 GB spectra per movie), no flush",
                            "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.numel()),
@@ -587,6 +597,8 @@ def main():
                          "uint8 -bin 2; c4 4096^2x60 f32 with 3 realignment iterations and the gradient "
                          "refinement; c5: the 32-movie batch")
     ap.add_argument("--lanes", type=int, default=2, help="batch lanes (each a host thread, stream and plans)")
+    ap.add_argument("--storage", default="native", choices=["native", "f16"],
+                    help="f16: float32 count frames held as IEEE half (MRC mode 12) on the device and the host")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

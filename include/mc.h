@@ -32,8 +32,12 @@ extern "C" {
  * read2DIm_32bit converts char, mrc.cpp:338-348), 1 (int16), 2 (float32),
  * 6 (uint16), and MC_MODE_U8: unsigned 8-bit pixels, as 8-bit TIFF strips
  * hold them (MRCT::read2DIm converts unsigned char, mrct.cpp:137-150).
- * 16-bit TIFF strips are mode 6. */
+ * 16-bit TIFF strips are mode 6.  Added (no reference counterpart):
+ * MC_MODE_F16, the MRC2014 mode 12 of IEEE-754 half floats -- frames stored
+ * in half the bytes of mode 2 and widened to FP32 in the forward kernels'
+ * loads; integer counts up to 2048 convert to it exactly. */
 #define MC_MODE_U8 100
+#define MC_MODE_F16 12
 
 enum {
   MC_OK = 0,

@@ -64,7 +64,8 @@ def verify_params(p: Params, nz: int) -> Params:
 
 
 MODE_U8 = 100  # unsigned 8-bit pixels (8-bit TIFF)
-_WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2, MODE_U8: 1}
+MODE_F16 = 12  # IEEE half floats (MRC2014 mode 12): frames held in half the bytes of mode 2
+_WORD_LENGTH = {0: 1, 1: 2, 2: 4, 6: 2, MODE_U8: 1, MODE_F16: 2}
 KERNEL_KINDS = 9
 
 
@@ -470,7 +471,7 @@ class Batch:
         return out
 
 
-_PIXEL_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, MODE_U8: np.uint8}
+_PIXEL_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, MODE_U8: np.uint8, MODE_F16: np.float16}
 STACK_FORMATS = {0: "mrc", 1: "mrc-gz", 2: "tiff"}
 
 

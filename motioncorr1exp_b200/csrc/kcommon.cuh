@@ -2,6 +2,7 @@
 // mc_pair.cu, mc_sum.cu): constants, pixel decode, the two-level register FFT
 // and the raw-row staging helpers.
 #pragma once
+#include <cuda_fp16.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -20,6 +21,7 @@ __device__ __forceinline__ float load_pixel(const void* frame, int mode, long lo
     case MC_MODE_U8: return (float)((const uint8_t*)frame)[idx];
     case 1: return (float)((const int16_t*)frame)[idx];
     case 6: return (float)((const uint16_t*)frame)[idx];
+    case MC_MODE_F16: return __half2float(((const __half*)frame)[idx]);
     default: return ((const float*)frame)[idx];
   }
 }

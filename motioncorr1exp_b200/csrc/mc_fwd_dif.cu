@@ -139,6 +139,7 @@ cudaError_t launch_fwd_rows_dif(const FwdRowsArgs& a, cudaStream_t st) {
       case MC_MODE_U8: MC_DIF_RAW(A, B, uint8_t)                                                      \
       case 1: MC_DIF_RAW(A, B, int16_t)                                                               \
       case 6: MC_DIF_RAW(A, B, uint16_t)                                                              \
+      case MC_MODE_F16: MC_DIF_RAW(A, B, __half)                                                      \
       default: MC_DIF_RAW(A, B, float)                                                                \
     }                                                                                                 \
   }

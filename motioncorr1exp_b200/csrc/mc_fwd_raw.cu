@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
     case MC_MODE_U8: stage_rows<uint8_t>(xin, a, r0, r1, N, TL::T); break;
     case 1: stage_rows<int16_t>(xin, a, r0, r1, N, TL::T); break;
     case 6: stage_rows<uint16_t>(xin, a, r0, r1, N, TL::T); break;
+    case MC_MODE_F16: stage_rows<__half>(xin, a, r0, r1, N, TL::T); break;
     default: stage_rows<float>(xin, a, r0, r1, N, TL::T); break;
   }
   __syncthreads();
@@ -110,6 +111,7 @@ cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
         case MC_MODE_U8: MC_TL_RAW(A, B, uint8_t)                                                    \
         case 1: MC_TL_RAW(A, B, int16_t)                                                             \
         case 6: MC_TL_RAW(A, B, uint16_t)                                                            \
+        case MC_MODE_F16: MC_TL_RAW(A, B, __half)                                                    \
         default: MC_TL_RAW(A, B, float)                                                              \
       }                                                                                              \
     }                                                                                                \

@@ -255,6 +255,7 @@ int word_length(int mode) {
     case 2: return 4;
     case 6: return 2;
     case MC_MODE_U8: return 1;
+    case MC_MODE_F16: return 2;
     default: return 0;
   }
 }
@@ -1858,7 +1859,8 @@ int mc_plan_quicklook(mc_plan* pl, int which, int16_t* out) {
 
 int mc_plan_count_sum(mc_plan* pl, int32_t* host) {
   if (!pl || !host) return set_err(MC_E_ARG, "null argument");
-  if (pl->mode == 2) return set_err(MC_E_ARG, "count sums need integer pixels (mode 0, 1, 6 or MC_MODE_U8)");
+  if (pl->mode == 2 || pl->mode == MC_MODE_F16)
+    return set_err(MC_E_ARG, "count sums need integer pixels (mode 0, 1, 6 or MC_MODE_U8)");
   for (int f = 0; f < pl->nframe; f++)
     if (!pl->loaded[f]) return set_err(MC_E_STATE, "frame position %d not loaded", f);
   CK(cudaSetDevice(pl->device));

@@ -7,8 +7,11 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -36,6 +39,17 @@ int32_t hdr_i32(const unsigned char* h, int off) {
 
 bool has_map_stamp(const unsigned char* h) { return std::memcmp(h + 208, "MAP ", 4) == 0; }
 
+// IEEE-754 binary16 -> binary32 (exact: every half is a float): sign,
+// 5-bit exponent (bias 15), 10-bit fraction; subnormals scaled by 2^-24.
+float half_bits_to_float(uint16_t h) {
+  const int sign = h >> 15, e = (h >> 10) & 31, f = h & 1023;
+  float v;
+  if (e == 0) v = std::ldexp((float)f, -24);
+  else if (e == 31) v = f ? std::numeric_limits<float>::quiet_NaN() : std::numeric_limits<float>::infinity();
+  else v = std::ldexp((float)(f | 1024), e - 25);
+  return sign ? -v : v;
+}
+
 // MRC::getWordLength (mrc.cpp:99-118) for the modes a plan decodes.
 int word_length(int mode) {
   switch (mode) {
@@ -44,6 +58,7 @@ int word_length(int mode) {
     case 2: return 4;
     case 6: return 2;
     case MC_MODE_U8: return 1;
+    case MC_MODE_F16: return 2;  // MRC2014 mode 12 (IEEE half); the reference reads no such files
     default: return 0;
   }
 }
@@ -212,6 +227,9 @@ int mc_stack_read_frame_float(mc_stack* s, float* dst, int n) {
       break;
     case 6:
       for (size_t i = 0; i < npx; i++) dst[i] = (float)((const uint16_t*)raw.data())[i];
+      break;
+    case MC_MODE_F16:
+      for (size_t i = 0; i < npx; i++) dst[i] = half_bits_to_float(((const uint16_t*)raw.data())[i]);
       break;
     default:
       std::memcpy(dst, raw.data(), npx * sizeof(float));

@@ -29,8 +29,8 @@ HEADER_DTYPE = np.dtype([
 assert HEADER_DTYPE.itemsize == 1024
 
 # MRC::getWordLength (mrc.cpp:99-118)
-WORD_LENGTH = {0: 1, 1: 2, 2: 4, 3: 4, 4: 8, 6: 2}
-PIXEL_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16}
+WORD_LENGTH = {0: 1, 1: 2, 2: 4, 3: 4, 4: 8, 6: 2, 12: 2}
+PIXEL_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, 12: np.float16}  # 12: MRC2014 half
 
 
 def default_header() -> np.ndarray:

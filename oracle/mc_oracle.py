@@ -152,13 +152,14 @@ def design_matrix(pairs, nframe: int) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # frames
 # ---------------------------------------------------------------------------
-_MODE_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, 100: np.uint8}
+_MODE_DTYPE = {0: np.int8, 1: np.int16, 2: np.float32, 6: np.uint16, 100: np.uint8, 12: np.float16}
 
 
 def decode_frame(raw: np.ndarray, mode: int) -> np.ndarray:
     """MRC::read2DIm_32bit (mrc.cpp:325-382): mode 0 is *signed* char; mode
     100 is the unsigned byte of an 8-bit TIFF strip (MRCT::read2DIm,
-    mrct.cpp:137-150)."""
+    mrct.cpp:137-150); mode 12 (MRC2014 IEEE half, no reference counterpart)
+    widens exactly."""
     dt = _MODE_DTYPE.get(mode, np.float32)
     return np.asarray(raw).view(dt).astype(np.float64)
 

@@ -111,3 +111,26 @@ def test_unsigned_bytes_equal_uint16(gpu, kw):
     np.testing.assert_array_equal(r8["frame_shifts"], r16["frame_shifts"])
     rs = api.align(frames.view(np.int8), 0, p)
     assert not np.array_equal(rs["image"], r8["image"])
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(crop_offsetx=6, crop_nsam=256, bin=2.0)])
+def test_half_frames(gpu, kw):
+    """MC_MODE_F16 (MRC2014 mode 12): integer counts stored as IEEE half give
+    results bit-identical to the same counts as float32 (the widening is
+    exact), on every forward path (two-level raw rows, -bin 2 split, the
+    generic engine); non-integer frames stored as half match the FP64
+    oracle run on the same half values."""
+    mv = synth.make_movie(300, 292, 8, mean=2.0, seed=67, dtype="f32", speed=0.6, rw_sigma=0.4)
+    assert mv.frames.max() < 2048
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=2, **kw), 8)
+    r32 = api.align(mv.frames, 2, p)
+    r16 = api.align(mv.frames.astype(np.float16), api.MODE_F16, p)
+    np.testing.assert_array_equal(r16["image"], r32["image"])
+    np.testing.assert_array_equal(r16["frame_shifts"], r32["frame_shifts"])
+    # non-integer pixels: the half values are what the oracle decodes
+    fr = (mv.frames * np.float32(1.37) + np.float32(0.25)).astype(np.float16)
+    g = api.align(fr, api.MODE_F16, p)
+    ref = O.align_movie(fr, api.MODE_F16, O.Params(**{k: getattr(p, k) for k in O.Params.__dataclass_fields__}))
+    fo = np.stack([ref.frame_shift.real, ref.frame_shift.imag], 1)
+    assert np.max(np.abs(g["frame_shifts"] - fo)) <= 0.01
+    assert np.linalg.norm(g["image"] - ref.image) / np.linalg.norm(ref.image) <= 1e-5

@@ -199,10 +199,13 @@ def _mrc_with_symdata(path, frames, mode, nsymbt):
     open(path, "wb").write(bytes(b[:1024]) + b"\x5a" * nsymbt + bytes(b[1024:]))
 
 
-@pytest.mark.parametrize("mode,dtype", [(0, np.int8), (1, np.int16), (2, np.float32), (6, np.uint16)])
+@pytest.mark.parametrize("mode,dtype", [(0, np.int8), (1, np.int16), (2, np.float32), (6, np.uint16),
+                                        (12, np.float16)])
 def test_mrc_and_mrcgz(tmp_path, mode, dtype):
+    """Every pixel mode a plan decodes; 12 is MRC2014's IEEE half (including
+    subnormals, infinities and a NaN), widened exactly on the host."""
     rng = np.random.default_rng(9 + mode)
-    frames = (rng.normal(0, 50, (5, 33, 47)) if mode == 2 else
+    frames = (rng.normal(0, 50, (5, 33, 47)) if mode in (2, 12) else
               rng.integers(np.iinfo(dtype).min, np.iinfo(dtype).max, (5, 33, 47))).astype(dtype)
     p = tmp_path / "s.mrc"
     _mrc_with_symdata(p, frames, mode, 80)
@@ -215,6 +218,18 @@ def test_mrc_and_mrcgz(tmp_path, mode, dtype):
             np.testing.assert_array_equal(s.read_frames(3, 2), frames[3:5])
             np.testing.assert_array_equal(s.read_frames(1, 1), frames[1:2])  # backward seek
             np.testing.assert_array_equal(s.read_frame_float(4), frames[4].astype(np.float32))
+
+
+def test_half_decode_special_values(tmp_path):
+    h = np.arange(65536, dtype=np.uint32).astype(np.uint16).view(np.float16).reshape(1, 256, 256)
+    p = tmp_path / "h.mrc"
+    _mrc_with_symdata(p, h, 12, 0)
+    with api.Stack(str(p)) as s:
+        got = s.read_frame_float(0)
+    want = h[0].astype(np.float32)
+    nan = np.isnan(want)
+    assert np.array_equal(np.isnan(got), nan)
+    np.testing.assert_array_equal(got[~nan], want[~nan])
 
 
 def test_detection_order_and_rejects(tmp_path):
