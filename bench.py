@@ -436,9 +436,10 @@ def run_ours(args):
                            "nsam": plan.nsam, "pairs": plan.npairs,
                            "frame_storage": ("IEEE half (MRC mode 12), exact for these counts"
                                              if args.storage == "f16" else "file pixel type"),
-                           "l2": "inputs larger than L2 (570 MB frames, 2.2 GB spectra per movie), no flush",
+                           "l2": (f"inputs larger than L2 ({nz * raw / 1e6:.0f} MB frames, "
+                                  f"{nz * S / 1e9:.1f} GB spectra per movie), no flush"),
                            "parallelism": f"replicas x{world}"},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.numel()),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.numel() * host.element_size()),
                         "d2h_bytes_per_step": int(image.numel() * 4),
                         "api": f"mc_batch_run, {args.lanes} lanes, frames and image in pinned host memory",
                         "latency_p50_ms": _pct(e2e_lat, 50), "latency_p99_ms": _pct(e2e_lat, 99),

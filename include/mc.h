@@ -97,6 +97,12 @@ int mc_version(void);
 const char* mc_strerror(int code);
 /* Text of the last error of the calling thread ("" if none). */
 const char* mc_last_error(void);
+/* Fault injection for tests (no reference counterpart): the nth device or
+ * pinned-host allocation a plan makes from now on, in any thread, fails with
+ * MC_E_NOMEM as if memory were exhausted; the countdown then disarms.
+ * 0 disarms it.  The failure is simulated on the host, nothing is asked of
+ * the GPU. */
+void mc_debug_fail_alloc(int nth);
 
 /* getDefaultPara (dosefgpu_driftcorr.cpp:8-58) plus itr=0, ith=0 (DFAlign.cu:15-16). */
 void mc_default_params(mc_params* p);

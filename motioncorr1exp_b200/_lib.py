@@ -72,6 +72,7 @@ SIGNATURES = {
     "mc_version": (C.c_int, []),
     "mc_strerror": (C.c_char_p, [C.c_int]),
     "mc_last_error": (C.c_char_p, []),
+    "mc_debug_fail_alloc": (None, [C.c_int]),
     "mc_default_params": (None, [C.POINTER(McParams)]),
     "mc_verify_params": (C.c_int, [C.POINTER(McParams), C.c_int]),
     "mc_plan_create": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdarg>
@@ -29,6 +30,18 @@ using mc::FftPlan1D;
 namespace {
 
 thread_local std::string g_err;
+
+// Host-side fault injection (mc_debug_fail_alloc): the device or pinned
+// allocation that takes this countdown from 1 to 0 fails as if the device
+// were out of memory.  0 = off.
+std::atomic<int> g_fail_alloc{0};
+
+bool injected_alloc_failure() {
+  int v = g_fail_alloc.load();
+  while (v > 0)
+    if (g_fail_alloc.compare_exchange_weak(v, v - 1)) return v == 1;
+  return false;
+}
 
 int set_err(int code, const char* fmt, ...) {
   char buf[1024];
@@ -440,6 +453,8 @@ struct mc_plan {
   template <typename T>
   int alloc(T** ptr, size_t bytes) {
     if (bytes == 0) bytes = 16;
+    if (injected_alloc_failure())
+      return set_err(MC_E_NOMEM, "cudaMalloc(%zu bytes) failed: injected failure (mc_debug_fail_alloc)", bytes);
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) {
@@ -671,6 +686,8 @@ const char* mc_strerror(int code) {
 }
 
 const char* mc_last_error(void) { return g_err.c_str(); }
+
+void mc_debug_fail_alloc(int nth) { g_fail_alloc.store(nth > 0 ? nth : 0); }
 
 void mc_default_params(mc_params* p) {
   if (!p) return;
@@ -948,6 +965,8 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
     place(pl->st_status, sizeof(int));
     place(pl->st_slot, sizeof(void*));
     pl->st_bytes = o;
+    if (injected_alloc_failure())
+      return set_err(MC_E_NOMEM, "cudaMallocHost(%zu bytes) failed: injected failure (mc_debug_fail_alloc)", o);
     CK(cudaMallocHost(&pl->h_stage, o));
     CKR(pl->alloc(&pl->d_src_slot, sizeof(void*)));
   }

@@ -72,7 +72,7 @@ def test_static_scratch_allocates_nothing(gpu):
     the device's free memory by nothing."""
     import torch
     n, box = 2048, 96
-    p, boxes, pairs, spectra, _ = _plan_windows(n, box, nz=4)
+    p, boxes, pairs, spectra, _ = _plan_windows(n, box, nz=6)
     L = _lib.lib()
     i, j = (int(v) for v in pairs[0])
     da = torch.from_numpy(np.ascontiguousarray(spectra[i].T).view(np.float32)).cuda()
