@@ -11,19 +11,18 @@ follows.  Index conventions, argmax tie-breaks, clamping rules and the
 1/32-pixel quantisation of the sub-pixel search are kept exactly; only the
 arithmetic is widened to FP64.
 
-Parity status: the reference publishes no tests, fixtures or golden vectors
-and its alignment code cannot be built here (it needs FFTW3, SP++ 3.0 and
-libtiff, none of which are installed).  Pinned against the reference's own
-code compiled by ``oracle/build_ref.sh`` (golden fixtures in tests/golden/):
-the MRC and MRC-gz decode/encode (``mrc.cpp``, ``mrcz.cpp``) and, through
-``func.cpp`` built against stand-in FFTW/libtiff headers, the crop size and
-crop, the sub-pixel cosine mask and the display contrast and layout; the
-forward spectra, the pair stage (CC windows, FindShift's shifts and CC) and
-the shift-and-sum against the reference's own cufunc.cu run on the GPU
-(tests/test_gpu_reference_pair.py), binning included.  The least-squares
-solve and the realignment iterations are pinned only by project-written
-known-answer tests (brute-force DFTs, analytic peaks, exactly consistent
-shifts): for those this oracle is "parity unpinned".
+Parity status: the reference publishes no tests, fixtures or golden
+vectors, and its build needs FFTW3, SP++ 3.0 and libtiff, none of which is
+installed.  ``oracle/build_ref.sh`` compiles the reference's own sources
+with project stand-ins for those (``oracle/stubs/``), and this oracle is
+pinned against what they produce: the MRC and MRC-gz decode/encode
+(``mrc.cpp``, ``mrcz.cpp``), ``func.cpp``'s crop size, crop, sub-pixel cosine
+mask and display contrast/layout, the drift solve (``mfunc.h`` and the
+least-squares steps of ``DFAlign.cu:875-948``; golden fixtures in
+tests/golden/), and on the GPU the reference's forward spectra, pair stage
+and shift-and-sum (``cufunc.cu`` with cuFFT, tests/test_gpu_reference_pair.py)
+and its whole program, realignment iterations included
+(tests/test_gpu_reference_full.py).
 """
 from __future__ import annotations
 

@@ -66,7 +66,12 @@ def test_truncated_stack_is_rejected(tmp_path):
         mrc.read_header(str(p))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src-1125"), reason="reference tree absent")
+def _reference_tree_present():
+    r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh"), "--where"], capture_output=True)
+    return r.returncode == 0
+
+
+@pytest.mark.skipif(not _reference_tree_present(), reason="reference tree absent")
 def test_live_reference_roundtrip(tmp_path):
     subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], check=True, capture_output=True)
     img = np.random.default_rng(0).normal(3, 2, (1, 31, 29)).astype(np.float32)
