@@ -230,6 +230,80 @@ def factor_codelet(q: int) -> list:
     return rad + pw
 
 
+# Radices the prime-factor codelets combine (dft_any handles each).
+PFA_RADICES = (2, 3, 4, 5, 7, 8)
+
+
+def pfa_plan(q: int):
+    """Good-Thomas prime-factor plan of length q: its prime-power groups when
+    there are at least two and each is a radix dft_any handles, else None.
+    Returns (groups, input multipliers M_i = q / g_i, CRT factors t_i =
+    M_i^-1 mod g_i).  With n = sum n_i M_i and k = sum k_i M_i t_i (mod q),
+    W_q^(n k) = prod W_(g_i)^(n_i k_i): the transform is a product of
+    independent g_i-point DFTs with no twiddle factors between them."""
+    groups, m, p = [], q, 2
+    while m > 1:
+        if m % p == 0:
+            g = 1
+            while m % p == 0:
+                g *= p
+                m //= p
+            groups.append(g)
+        p += 1
+    if len(groups) < 2 or any(g not in PFA_RADICES for g in groups):
+        return None
+    M = [q // g for g in groups]
+    t = [pow(M[i] % groups[i], -1, groups[i]) for i in range(len(groups))]
+    return groups, M, t
+
+
+def pfa_indices(q: int):
+    """(input index, output index) of every multi-index of the PFA plan, in
+    the working array's order (multi-index (n_0, n_1, ...) at
+    n_0 + g_0 (n_1 + g_1 (...)))."""
+    groups, M, t = pfa_plan(q)
+    import itertools
+    ins, outs = [], []
+    for idx in itertools.product(*[range(g) for g in reversed(groups)]):
+        nidx = list(reversed(idx))
+        ins.append(sum(n * Mi for n, Mi in zip(nidx, M)) % q)
+        outs.append(sum(k * Mi * ti for k, Mi, ti in zip(nidx, M, t)) % q)
+    return groups, ins, outs
+
+
+def emit_codelet_pfa(q: int) -> str:
+    """In-register prime-factor (Good-Thomas) FFT of length q: the input
+    gathered by the Ruritanian map, small DFTs along each group's axis with
+    no twiddles, the output scattered by the CRT map."""
+    groups, ins, outs = pfa_indices(q)
+    G = len(groups)
+    strides = [1] * G
+    for d in range(1, G):
+        strides[d] = strides[d - 1] * groups[d - 1]
+    L = [f"template <bool INV> __device__ __forceinline__ void fft_pfa_{q}(float2* a) {{",
+         f"  // prime-factor plan {' x '.join(map(str, groups))}: no twiddle factors",
+         f"  float2 b[{q}];"]
+    for w in range(q):
+        L.append(f"  b[{w}] = a[{ins[w]}];")
+    for d in range(G):
+        g, st = groups[d], strides[d]
+        for base in range(q):
+            if (base // st) % g:
+                continue
+            L.append("  {")
+            L.append(f"    float2 x[{g}];")
+            for r in range(g):
+                L.append(f"    x[{r}] = b[{base + r * st}];")
+            L.append(f"    dft_any<{g}, INV>(x);")
+            for r in range(g):
+                L.append(f"    b[{base + r * st}] = x[{r}];")
+            L.append("  }")
+    for w in range(q):
+        L.append(f"  a[{outs[w]}] = b[{w}];")
+    L.append("}")
+    return "\n".join(L)
+
+
 def emit_codelet(q: int) -> str:
     """In-register Stockham FFT of length q with every index and twiddle
     resolved at generation time: fft_reg_q<INV>(float2 a[q]), result in a."""
@@ -314,6 +388,20 @@ def main() -> None:
         for i, q in enumerate(CODELETS):
             kw = "if" if i == 0 else "else if"
             out.append(f"  {kw} constexpr (Q == {q}) fft_reg_{q}<INV>(a);")
+        out.append("}")
+        # prime-factor (Good-Thomas) forms of the lengths with coprime factors:
+        # the pair kernels use them (measured faster there; the forward
+        # transforms keep the Stockham forms, which measured faster in them)
+        for q in CODELETS:
+            if pfa_plan(q):
+                out.append(emit_codelet_pfa(q))
+        out.append("template <int Q, bool INV> __device__ __forceinline__ void fft_reg_pf(float2* a) {")
+        first = True
+        for q in CODELETS:
+            if pfa_plan(q):
+                out.append(f"  {'if' if first else 'else if'} constexpr (Q == {q}) fft_pfa_{q}<INV>(a);")
+                first = False
+        out.append("  else fft_reg<Q, INV>(a);")
         out.append("}")
         out.append("}  // namespace mc")
     sys.stdout.write("\n".join(out) + "\n")

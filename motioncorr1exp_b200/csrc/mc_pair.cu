@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
         const int ky = lt + P * k2;
         x[k2] = cscale(cmulc(__ldg(ca + ky), __ldg(cb + ky)), wcol[ky]);
       }
-      fft_reg<Q, true>(x);
+      fft_reg_pf<Q, true>(x);
 #pragma unroll
       for (int r = 0; r < Q; r++) Y[lt + P * r] = x[r];
     }
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
       float2 x[Q];
 #pragma unroll
       for (int k2 = 0; k2 < Q; k2++) x[k2] = cscale(cmulc(__ldg(ca + P * k2), __ldg(cb + P * k2)), wc[P * k2]);
-      fft_reg<Q, true>(x);
+      fft_reg_pf<Q, true>(x);
 #pragma unroll
       for (int r = 0; r < Q; r++) Y[lt + PS * r] = x[r];
     }
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_ro
       }
       x[k2] = z;
     }
-    fft_reg<Q, true>(x);
+    fft_reg_pf<Q, true>(x);
   }
   __syncthreads();  // every team has gathered: the staged rows give way to Y
   float2* Y = reg + (size_t)tm * S::YN;

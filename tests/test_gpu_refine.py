@@ -102,3 +102,36 @@ def test_refine_keeps_reference_frame_and_logs(gpu):
     assert after[0].tolist() == [0.0, 0.0]
     assert np.max(np.abs(after - before)) < 0.5
     assert any("Gradient refinement" in l for l in lines)
+
+
+@pytest.mark.slow
+def test_adjoint_at_4096(gpu):
+    """c4's frame size (4096^2 float32, counts of mean 1.0, the c4 drift
+    model) with 6 frames: the adjoint gradient against central finite
+    differences of the CUDA objective (h = 1e-3 px) and against the FP64
+    oracle's gradient and Hessian blocks."""
+    import torch
+    n, nf = 4096, 6
+    frames, _ = synth.make_movie_torch(n, n, nf, mean=1.0, seed=21, dtype="f32", kind="jitter", rw_sigma=0.8,
+                                       amp=1.5, period=20.0, device="cuda")
+    host = frames.cpu().numpy()
+    p = api.verify_params(api.Params(CCPeakSearchDim=96), nf)
+    with api.Plan(p, n, n, nf, 2) as pl:
+        pl.load_frames_device(frames.data_ptr(), 0, nf)
+        pl.forward()
+        torch.cuda.synchronize()
+        s = np.random.default_rng(4).uniform(-1.5, 1.5, (nf, 2))
+        J, g, h = pl.objective(s)
+        scale = np.abs(g).max()
+        for k in (0, nf // 2, nf - 1):
+            for c in (0, 1):
+                sp, sm = s.copy(), s.copy()
+                sp[k, c] += 1e-3
+                sm[k, c] -= 1e-3
+                fd = (pl.objective(sp)[0] - pl.objective(sm)[0]) / 2e-3
+                assert abs(fd - g[k, c]) <= 2e-3 * scale, (k, c, fd, g[k, c])
+    F = [O.forward_spectrum(O.decode_frame(host[k], 2), 0, 0, n, n) for k in range(nf)]
+    Jo, go, ho = O.sum_objective(F, s, p.bfactor)
+    assert abs(J - Jo) <= 1e-5 * abs(Jo)
+    np.testing.assert_allclose(g, go, atol=1e-4 * np.abs(go).max())
+    np.testing.assert_allclose(h, ho, atol=1e-4 * np.abs(ho).max())
