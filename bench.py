@@ -340,6 +340,17 @@ def run_ours(args):
     dev_lat = [r["end_ms"] - r["start_ms"] for r in res_dev]
     launches = int(round(launches_per_movie * args.steps))
 
+    # ---- the same K movies as one CUDA graph per batch (mc_batch_set_graph:
+    # lanes as graph branches, one launch, one synchronisation); the graph is
+    # captured in the warm-up and relaunched in the timed call
+    graph_ms = None
+    if p.iter == 0 and not p.refine:
+        gb = api.Batch(local, args.lanes, graph=True)
+        for _ in range(max(1, args.warmup // 2)):
+            gb.run(dev)
+        graph_ms, _ = timed(lambda: gb.run(dev))
+        gb.close()
+
     # ---- per-kernel CUDA-event durations: a profiled pass of the single plan
     # (events around every launch, so no graph), for the roofline
     plan.reset_stats()
@@ -361,6 +372,21 @@ def run_ours(args):
     e2e_ms, res = timed(lambda: batch.run(mv))
     e2e_lat = [r["end_ms"] - r["start_ms"] for r in res]
     batch.close()
+
+    # host->device copy bandwidth from pinned memory (the bound of the e2e
+    # figure: every step uploads its frames): 1 GiB copied 5 times, best
+    h2d_src = torch.empty(1 << 30, dtype=torch.uint8, pin_memory=True)
+    h2d_dst = torch.empty(1 << 30, dtype=torch.uint8, device=f"cuda:{local}")
+    h2d_s = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h2d_dst.copy_(h2d_src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        h2d_s.append(e0.elapsed_time(e1) / 1000.0)
+    h2d_gbs = (1 << 30) / min(h2d_s) / 1e9
+    del h2d_src, h2d_dst
     # the single-plan form of the same call, one movie at a time
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
@@ -397,6 +423,8 @@ def run_ours(args):
     if rank == 0:
         value = nz * args.steps * world / (ms_max / 1000.0)
         e2e_value = nz * args.steps * world / (e2e_ms / 1000.0)
+        # frames/s if every movie's upload ran back to back at the pinned copy bandwidth
+        h2d_bound = world * nz / (host.numel() * host.element_size() / (h2d_gbs * 1e9))
         dom = max(stats, key=lambda k: stats[k]["ms"])
         d = stats[dom]
         per_launch_ms = d["ms"] / max(d["launches"], 1)
@@ -440,6 +468,10 @@ def run_ours(args):
                                   f"{nz * S / 1e9:.1f} GB spectra per movie), no flush"),
                            "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.numel() * host.element_size()),
+                        "h2d_roofline": {"pinned_h2d_gbs": h2d_gbs,
+                                         "bound_frames_per_s": h2d_bound,
+                                         "frac": e2e_value / h2d_bound,
+                                         "note": "upload of each movie's frames at the measured pinned copy bandwidth"},
                         "d2h_bytes_per_step": int(image.numel() * 4),
                         "api": f"mc_batch_run, {args.lanes} lanes, frames and image in pinned host memory",
                         "latency_p50_ms": _pct(e2e_lat, 50), "latency_p99_ms": _pct(e2e_lat, 99),
@@ -447,6 +479,7 @@ def run_ours(args):
                 "api": f"mc_batch_run, {args.lanes} lanes, frames resident in HBM (bound in place)",
                 "latency_p50_ms": _pct(dev_lat, 50), "latency_p99_ms": _pct(dev_lat, 99),
                 "single_plan_value": nz * args.steps * world / (single_ms / 1000.0),
+                "single_graph_value": (nz * args.steps * world / (graph_ms / 1000.0)) if graph_ms else None,
                 "gpu_launches": launches, "roofline": roof,
                 "movie_roofline": {"bytes_per_movie": b_movie, "achieved": movie_gbs, "peak": peak, "unit": "GB/s",
                                    "frac": movie_gbs / peak},
@@ -470,6 +503,13 @@ def run_ours(args):
                                               "1/20 of this movie each (2 frame forwards, 18.9 pair "
                                               "correlations + FindShift, 2 frames of the sum; one warm-up "
                                               f"step); median step {statistics.median(ts):.2f} s"}
+        if world == 1 and args.workload == "c2" and not args.no_batch_c5:
+            # the batch workload beside the headline: 32 mixed movies, one lane
+            # (one movie at a time) against --lanes lanes
+            r5 = c5_measure(local, args.seed, (1, args.lanes), 2, 1)
+            line["batch_c5"] = {"workload": C5_WORKLOAD, "frames_per_batch": r5["frames_per_batch"],
+                                "lanes": {str(k): {kk: vv for kk, vv in v.items() if kk != "clocks"}
+                                          for k, v in r5["lanes"].items()}}
         if world == 1 and not args.no_oracle_check and args.workload in ("c1", "c2", "c3"):
             line["vs_oracle"] = oracle_check(host_np_all, mode, p, g_res, p.NoisePeakSize)
             line["shift_rmse_vs_oracle_px"] = line["vs_oracle"]["shift_rmse_vs_oracle_px"]
@@ -486,22 +526,18 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if xs else None
 
 
-def run_c5(args):
-    """Batch workload: 32 movies of mixed size and depth through the
-    multi-lane batch runner (mc_batch_run) against the same runner with one
-    lane (one movie at a time)."""
+def c5_measure(local, seed, lanes_list, steps, warmup):
+    """The batch workload (32 movies of mixed size and depth, frames windows
+    of one 80-frame base movie per geometry) through the batch runner with
+    each lane count of ``lanes_list``: frames/s with the frames in HBM and
+    from pinned host memory, per-movie latency and completion percentiles."""
     import numpy as np
     import torch
     from motioncorr1exp_b200 import api, synth
-    from motioncorr1exp_b200 import dist as D
-    rank, world, local = D.world()
-    if world > 1:
-        raise SystemExit("the batch workload runs on one GPU per process; use --gpus 1")
-    torch.cuda.set_device(local)
-    jobs, means = synth.c5_jobs(seed=args.seed, n_movies=32, max_frames=80)
+    jobs, means = synth.c5_jobs(seed=seed, n_movies=32, max_frames=80)
     base, base_host = [], []
     for g, (nx, ny) in enumerate(synth.C5_GEOMETRIES):
-        fr, _ = synth.make_movie_torch(nx, ny, 80, mean=means[g], seed=args.seed + 10 + g, dtype="u8",
+        fr, _ = synth.make_movie_torch(nx, ny, 80, mean=means[g], seed=seed + 10 + g, dtype="u8",
                                        kind="linear", speed=0.3, rw_sigma=0.5, device=f"cuda:{local}")
         base.append(fr)
         h = torch.empty(fr.shape, dtype=torch.uint8, pin_memory=True)
@@ -546,16 +582,16 @@ def run_c5(args):
         return lat, comp
 
     out = {}
-    for lanes in (1, args.lanes):
+    for lanes in lanes_list:
         with api.Batch(local, lanes) as b:
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 b.run(movies(True))
             ms = []
             with ClockSampler(local) as clk:
-                lat, comp = timed(b, ms, True, args.steps)
+                lat, comp = timed(b, ms, True, steps)
             e2e_ms = []
             b.run(movies(False))
-            lat_h, comp_h = timed(b, e2e_ms, False, args.steps)
+            lat_h, comp_h = timed(b, e2e_ms, False, steps)
             out[lanes] = {"value": nframes * len(ms) / (sum(ms) / 1000.0),
                           "e2e": nframes * len(e2e_ms) / (sum(e2e_ms) / 1000.0),
                           "ms_per_batch": sum(ms) / len(ms),
@@ -563,15 +599,34 @@ def run_c5(args):
                           "completion_p50_ms": _pct(comp, 50), "completion_p99_ms": _pct(comp, 99),
                           "e2e_latency_p50_ms": _pct(lat_h, 50), "e2e_latency_p99_ms": _pct(lat_h, 99),
                           "device_gb": b.device_bytes / 1e9, "clocks": clk.summary()}
+    del base, base_host
+    torch.cuda.empty_cache()
+    return {"frames_per_batch": nframes, "jobs": jobs, "lanes": out}
+
+
+C5_WORKLOAD = ("c5: 32 movies, geometry from {2048^2, 3838x3710, 4096^2}, F ~ U[20,80], fod in {2,4,7}, uint8, "
+               "-bft 150 -pbx 96 -atm 1; frames are windows of one 80-frame base movie per geometry "
+               "(mean U[0.8,1.5])")
+
+
+def run_c5(args):
+    """Batch workload: 32 movies of mixed size and depth through the
+    multi-lane batch runner (mc_batch_run) against the same runner with one
+    lane (one movie at a time)."""
+    import torch
+    from motioncorr1exp_b200 import dist as D
+    rank, world, local = D.world()
+    if world > 1:
+        raise SystemExit("the batch workload runs on one GPU per process; use --gpus 1")
+    torch.cuda.set_device(local)
+    r = c5_measure(local, args.seed, (1, args.lanes), args.steps, args.warmup)
+    jobs, nframes, out = r["jobs"], r["frames_per_batch"], r["lanes"]
     best = out[args.lanes]
     line = {"metric": "aligned frames/s, batch of 32 movies (2048^2 / 3838x3710 / 4096^2, F~U[20,80])",
             "value": best["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": best["ms_per_batch"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "c5: 32 movies, geometry from {2048^2, 3838x3710, 4096^2}, F ~ U[20,80], "
-                                   "fod in {2,4,7}, uint8, -bft 150 -pbx 96 -atm 1; frames are windows of one "
-                                   "80-frame base movie per geometry (mean U[0.8,1.5])",
-                       "frames_per_batch": nframes, "lanes": args.lanes,
+            "config": {"workload": C5_WORKLOAD, "frames_per_batch": nframes, "lanes": args.lanes,
                        "l2": "inputs larger than L2, no flush", "parallelism": "lanes on one GPU"},
             "e2e": {"value": best["e2e"], "unit": UNIT,
                     "h2d_bytes_per_step": int(sum(j["nframes"] * j["nx"] * j["ny"] for j in jobs)),
@@ -591,6 +646,8 @@ def main():
     ap.add_argument("--frames", type=int, default=0,
                     help="movie length (0: the workload's; fewer only for profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch-c5", action="store_true",
+                    help="skip the 32-movie batch workload reported beside the c2 line")
     ap.add_argument("--no-oracle-check", action="store_true",
                     help="skip the whole-movie FP64 oracle run that checks the result (and the step model)")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],

@@ -355,6 +355,17 @@ void mc_batch_destroy(mc_batch* b);
 int mc_batch_run(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results);
 /* Device memory held by the runner's plans. */
 size_t mc_batch_device_bytes(const mc_batch* b);
+/* Single-graph mode (on = 1): mc_batch_run captures the whole batch -- every
+ * movie's forward transforms, pair stage, FP64 solve, sum and C2R, lane l
+ * taking jobs l, l + lanes, ... as its own branch -- into one CUDA graph,
+ * launches it once and reads every movie's results after one
+ * synchronisation; the graph is kept and relaunched while the job list is
+ * the same.  Every job must hold device frames (on_device = 1), run
+ * device-only (-itr 0, no refinement) and give its image in pinned host or
+ * device memory (or NULL); otherwise mc_batch_run returns MC_E_ARG.  The
+ * per-movie gpu_ms is 0 and start/end times are the batch's.  No reference
+ * counterpart (the reference aligns one movie per process). */
+int mc_batch_set_graph(mc_batch* b, int on);
 
 /* ---- Stack files (host only; no GPU needed) -------------------------------
  * One handle over the three stack formats: replaces the readers MRC, MRCZ

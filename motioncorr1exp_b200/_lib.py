@@ -129,6 +129,7 @@ SIGNATURES = {
     "mc_batch_destroy": (None, [C.c_void_p]),
     "mc_batch_run": (C.c_int, [C.c_void_p, C.POINTER(McBatchJob), C.c_int, C.POINTER(McBatchResult)]),
     "mc_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "mc_batch_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "mc_stack_open": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "mc_stack_get_info": (C.c_int, [C.c_void_p, C.POINTER(McStackInfo)]),
     "mc_stack_read_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),

@@ -398,7 +398,10 @@ class Batch:
     """Many movies on one GPU (mc_batch_*): `lanes` worker threads, each with
     its own stream and plans reused across movies of a geometry."""
 
-    def __init__(self, device: int = 0, lanes: int = 2):
+    def __init__(self, device: int = 0, lanes: int = 2, graph: bool = False):
+        """graph=True: each run is captured into one CUDA graph and launched
+        once (mc_batch_set_graph; device frames, -itr 0, pinned or device
+        images)."""
         self._lib = L.lib()
         _load_schedules()
         h = C.c_void_p()
@@ -406,6 +409,8 @@ class Batch:
         self._h = h
         self.device = device
         self.lanes = lanes
+        if graph:
+            L.check(self._lib.mc_batch_set_graph(h, 1))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

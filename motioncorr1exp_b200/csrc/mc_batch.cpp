@@ -26,10 +26,7 @@
 #include <vector>
 
 #include "../../include/mc.h"
-
-namespace mc {
-int record_error(int code, const char* text);  // mc_plan.cu: sets mc_last_error()
-}
+#include "mc_internal.h"
 
 namespace {
 
@@ -79,6 +76,21 @@ double now_ms(std::chrono::steady_clock::time_point t0) {
 struct mc_batch {
   int device = 0;
   std::vector<std::unique_ptr<Lane>> lanes;
+  // single-graph mode (mc_batch_set_graph): the whole batch captured as one
+  // CUDA graph on `gst` and launched once; pinned per-movie blocks in `pin`
+  bool graph = false;
+  cudaStream_t gst = nullptr;
+  std::vector<cudaEvent_t> gev;
+  unsigned char* pin = nullptr;
+  size_t pin_bytes = 0;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<unsigned char> gkey;  // the job list the cached graph was captured for
+  ~mc_batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    for (auto e : gev) cudaEventDestroy(e);
+    if (gst) cudaStreamDestroy(gst);
+    if (pin) cudaFreeHost(pin);
+  }
 };
 
 extern "C" {
@@ -115,6 +127,226 @@ size_t mc_batch_device_bytes(const mc_batch* b) {
   return t;
 }
 
+int mc_batch_set_graph(mc_batch* b, int on) {
+  if (!b) return mc::record_error(MC_E_ARG, "null batch");
+  b->graph = on != 0;
+  return MC_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+#define BCK(call)                                                                               \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      char m_[256];                                                                             \
+      std::snprintf(m_, sizeof(m_), "%s failed: %s", #call, cudaGetErrorString(e_));           \
+      return mc::record_error(MC_E_CUDA, m_);                                                   \
+    }                                                                                           \
+  } while (0)
+
+size_t align64(size_t x) { return (x + 63) / 64 * 64; }
+
+// The whole batch as one CUDA graph: every movie's device-only pipeline
+// (forward transforms, pair stage, FP64 solve, sum, C2R, result copies)
+// captured in job order, lane l taking jobs l, l + lanes, ... on its own
+// plans and running as its own branch of the graph; the graph is launched
+// once and the host reads every movie's results after one synchronisation.
+// The captured graph is kept and relaunched while the job list is the same.
+int run_graph_impl(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results,
+                   const std::map<GeoKey, std::pair<int, int>>& need);
+
+// A failure of the batch as a whole (a job the mode cannot take, a capture
+// error) is every movie's status, with mc_last_error()'s text.
+int run_graph(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results,
+              const std::map<GeoKey, std::pair<int, int>>& need) {
+  const int rc = run_graph_impl(b, jobs, njobs, results, need);
+  if (rc != MC_OK) {
+    const std::string text = mc_last_error();
+    for (int i = 0; i < njobs; i++)
+      if (results[i].status == MC_E_STATE && results[i].lane < 0) {
+        results[i].status = rc;
+        std::snprintf(results[i].message, sizeof(results[i].message), "%s", text.c_str());
+      }
+    mc::record_error(rc, text.c_str());
+  }
+  return rc;
+}
+
+int run_graph_impl(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results,
+                   const std::map<GeoKey, std::pair<int, int>>& need) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const int nl = (int)b->lanes.size();
+  if (cudaSetDevice(b->device) != cudaSuccess) {
+    cudaGetLastError();
+    return mc::record_error(MC_E_CUDA, "cudaSetDevice failed");
+  }
+  for (int i = 0; i < njobs; i++) {
+    const mc_batch_job& j = jobs[i];
+    if (!j.on_device) return mc::record_error(MC_E_ARG, "graph mode needs the frames in device memory");
+    if (j.params.iter != 0 || j.params.refine != 0)
+      return mc::record_error(MC_E_ARG, "graph mode runs device-only movies (-itr 0, no refinement)");
+    if (j.params.GPUNum != b->device) return mc::record_error(MC_E_ARG, "job GPUNum differs from the runner's GPU");
+    if (j.image) {
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, j.image) != cudaSuccess ||
+          (at.type != cudaMemoryTypeHost && at.type != cudaMemoryTypeDevice)) {
+        cudaGetLastError();
+        return mc::record_error(MC_E_ARG, "graph mode needs images in pinned host or device memory");
+      }
+    }
+  }
+  // plans: lane l, geometry g, capacity of the deepest movie of g
+  std::vector<mc_plan*> plan_of(njobs, nullptr);
+  for (int i = 0; i < njobs; i++) {
+    const mc_batch_job& j = jobs[i];
+    Lane& lane = *b->lanes[i % nl];
+    const GeoKey key = geo_key(j);
+    const auto cap = need.at(key);
+    Lane::Entry& e = lane.plans[key];
+    if (e.plan && (e.cap_frames < cap.first || e.cap_pairs < cap.second)) {
+      mc_plan_destroy(e.plan);
+      e.plan = nullptr;
+    }
+    if (!e.plan) {
+      const int rc = mc_plan_create_capacity(&j.params, j.nx, j.ny, j.nz, j.mode, cap.first, cap.second, &e.plan);
+      if (rc != MC_OK) {
+        e.plan = nullptr;
+        return rc;
+      }
+      e.cap_frames = cap.first;
+      e.cap_pairs = cap.second;
+    }
+    plan_of[i] = e.plan;
+  }
+  // pinned per-movie blocks: frame word, pair words, result block
+  std::vector<size_t> off_word(njobs), off_pairs(njobs), off_stage(njobs);
+  size_t total = 0;
+  for (int i = 0; i < njobs; i++) {
+    int nf, np;
+    job_counts(jobs[i], &nf, &np);
+    off_word[i] = total;
+    total += 64;
+    off_pairs[i] = total;
+    total += align64(sizeof(int) * 2 * (size_t)std::max(np, 1));
+    off_stage[i] = total;
+    total += align64(mc::plan_stage_bytes(plan_of[i]));
+  }
+  // the job list (and the plans it maps to) the graph is captured for
+  std::vector<unsigned char> key(sizeof(mc_batch_job) * njobs + sizeof(mc_plan*) * njobs);
+  for (int i = 0; i < njobs; i++) {
+    mc_batch_job k = jobs[i];
+    k.frame_shifts = nullptr;  // filled on the host after the launch
+    std::memcpy(key.data() + sizeof(mc_batch_job) * i, &k, sizeof(k));
+  }
+  std::memcpy(key.data() + sizeof(mc_batch_job) * njobs, plan_of.data(), sizeof(mc_plan*) * njobs);
+  if (b->gexec && (key != b->gkey || total > b->pin_bytes)) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  if (total > b->pin_bytes) {
+    if (b->pin) cudaFreeHost(b->pin);
+    b->pin = nullptr;
+    b->pin_bytes = 0;
+    BCK(cudaMallocHost(&b->pin, total));
+    b->pin_bytes = total;
+  }
+  if (!b->gst) BCK(cudaStreamCreateWithFlags(&b->gst, cudaStreamNonBlocking));
+  while ((int)b->gev.size() < njobs + 1) {
+    cudaEvent_t e;
+    BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->gev.push_back(e);
+  }
+  if (!b->gexec) {
+    // the words the graph's copies read when it runs
+    for (int i = 0; i < njobs; i++) {
+      int rc = mc::plan_reframe_host(plan_of[i], &jobs[i].params, jobs[i].nz);
+      int nf, np;
+      job_counts(jobs[i], &nf, &np);
+      if (rc == MC_OK) rc = mc::plan_pair_words(plan_of[i], (int*)(b->pin + off_pairs[i]), std::max(np, 1));
+      if (rc != MC_OK) return rc;
+      *(const void**)(b->pin + off_word[i]) = jobs[i].frames;
+    }
+    BCK(cudaStreamBeginCapture(b->gst, cudaStreamCaptureModeThreadLocal));
+    int rc = MC_OK;
+    cudaError_t ce = cudaEventRecord(b->gev[njobs], b->gst);
+    std::vector<cudaEvent_t> last(nl, b->gev[njobs]);
+    for (int i = 0; i < njobs && rc == MC_OK && ce == cudaSuccess; i++) {
+      mc_plan* pl = plan_of[i];
+      rc = mc::plan_reframe_host(pl, &jobs[i].params, jobs[i].nz);
+      if (rc != MC_OK) break;
+      const cudaStream_t ps = mc::plan_stream(pl);
+      ce = cudaStreamWaitEvent(ps, last[i % nl], 0);
+      if (ce != cudaSuccess) break;
+      rc = mc::plan_enqueue_movie(pl, (const void* const*)(b->pin + off_word[i]), (const int*)(b->pin + off_pairs[i]),
+                                  b->pin + off_stage[i], jobs[i].image);
+      if (rc != MC_OK) break;
+      ce = cudaEventRecord(b->gev[i], ps);
+      last[i % nl] = b->gev[i];
+    }
+    for (int l = 0; l < nl && rc == MC_OK && ce == cudaSuccess; l++) ce = cudaStreamWaitEvent(b->gst, last[l], 0);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->gst, &g);
+    if (rc == MC_OK && (ce != cudaSuccess || ee != cudaSuccess || !g)) {
+      char m[256];
+      std::snprintf(m, sizeof(m), "batch graph capture failed: %s",
+                    cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+      rc = mc::record_error(MC_E_CUDA, m);
+    }
+    if (rc == MC_OK) {
+      const cudaError_t ie = cudaGraphInstantiate(&b->gexec, g, 0);
+      if (ie != cudaSuccess) {
+        b->gexec = nullptr;
+        char m[256];
+        std::snprintf(m, sizeof(m), "batch graph instantiation failed: %s", cudaGetErrorString(ie));
+        rc = mc::record_error(MC_E_CUDA, m);
+      }
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (rc != MC_OK) return rc;
+    b->gkey = key;
+  }
+  BCK(cudaGraphLaunch(b->gexec, b->gst));
+  BCK(cudaStreamSynchronize(b->gst));
+  const double t_done = now_ms(t0);
+  int first_bad = MC_OK;
+  for (int i = 0; i < njobs; i++) {
+    mc_batch_result& r = results[i];
+    r.lane = i % nl;
+    r.start_ms = 0.0;
+    mc_plan* pl = plan_of[i];
+    int rc = mc::plan_reframe_host(pl, &jobs[i].params, jobs[i].nz);
+    if (rc == MC_OK) rc = mc::plan_finish_movie(pl, b->pin + off_stage[i], jobs[i].frames);
+    if (rc == MC_OK && jobs[i].frame_shifts) rc = mc_plan_get_frame_shifts(pl, jobs[i].frame_shifts);
+    if (rc == MC_OK) {
+      mc_info in{};
+      mc_plan_info(pl, &in);
+      r.nsam = in.nsam;
+      r.nframe = in.nframe;
+      r.npairs = in.npairs;
+    }
+    r.gpu_ms = 0.f;
+    r.status = rc;
+    if (rc != MC_OK) {
+      std::snprintf(r.message, sizeof(r.message), "%s", mc_last_error());
+      if (first_bad == MC_OK) first_bad = rc;
+    }
+    r.end_ms = t_done;
+  }
+  if (first_bad != MC_OK) {
+    for (int i = 0; i < njobs; i++)
+      if (results[i].status != MC_OK) return mc::record_error(results[i].status, results[i].message);
+  }
+  return MC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mc_batch_run(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_result* results) {
   if (!b || (njobs > 0 && (!jobs || !results)) || njobs < 0) return mc::record_error(MC_E_ARG, "null argument");
   // capacity per geometry: the deepest movie of the batch
@@ -129,6 +361,7 @@ int mc_batch_run(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_resu
     results[i].status = MC_E_STATE;
     results[i].lane = -1;
   }
+  if (b->graph && njobs > 0) return run_graph(b, jobs, njobs, results, need);
   const auto t0 = std::chrono::steady_clock::now();
   std::atomic<int> next(0);
   auto work = [&](int li) {

@@ -23,6 +23,7 @@
 #include "../../include/mc.h"
 #include "kernels.cuh"
 #include "lsq.h"
+#include "mc_internal.h"
 
 using mc::cplx;
 using mc::FftPlan1D;
@@ -732,7 +733,7 @@ void mc_plan_destroy(mc_plan* pl) { delete pl; }
 
 // Frame range and pair list of the run (DFAlign.cu:528-530, mfunc.h:64-84);
 // the buffers were sized for cap_frames / cap_pairs.
-static int configure_frames(mc_plan* pl, const mc_params& q, int nz) {
+static int configure_frames(mc_plan* pl, const mc_params& q, int nz, bool upload_pairs = true) {
   mc_params& p = pl->p;
   p.nStart = q.nStart;
   p.nEnd = q.nEnd;
@@ -757,7 +758,7 @@ static int configure_frames(mc_plan* pl, const mc_params& q, int nz) {
                    (int)pairs.size(), pl->cap_frames, pl->cap_pairs);
   const bool same = pairs == pl->pairs;
   pl->pairs = pairs;
-  if (pl->d_pairs_main && !same) {
+  if (pl->d_pairs_main && !same && upload_pairs) {
     std::vector<int2> pr(pairs.size());
     for (size_t i = 0; i < pairs.size(); i++) pr[i] = make_int2(pairs[i].first, pairs[i].second);
     CK(cudaMemcpyAsync(pl->d_pairs_main, pr.data(), sizeof(int2) * pr.size(), cudaMemcpyHostToDevice, pl->st));
@@ -2006,9 +2007,8 @@ int mc_plan_refine(mc_plan* pl, int iterations) {
 
 // pairs -> device solve -> sum -> result copies into the pinned staging,
 // all on the plan stream without a host synchronisation.
-static int enqueue_tail(mc_plan* pl) {
+static int enqueue_tail(mc_plan* pl, unsigned char* hs) {
   const int np = (int)pl->pairs.size(), nf = pl->nframe, nc = nf - 1;
-  unsigned char* hs = pl->h_stage;
   CK(cudaMemcpy2DAsync(hs + pl->st_dc, sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
                        nf, cudaMemcpyDeviceToHost, pl->st));
   CKR(enqueue_pair_stage(pl, pl->d_specA, pl->fstride, pl->d_specB, pl->fstride, pl->pairs, pl->d_pairs_main));
@@ -2086,9 +2086,8 @@ static int enqueue_tail(mc_plan* pl) {
 
 // After the stream synchronised: results into the plan's host state, with the
 // same log lines as the staged path.
-static int finish_device_movie(mc_plan* pl) {
+static int finish_device_movie(mc_plan* pl, const unsigned char* hs) {
   const int np = (int)pl->pairs.size(), nc = pl->nframe - 1;
-  const unsigned char* hs = pl->h_stage;
   if (*(const int*)(hs + pl->st_status) != 0) return set_err(MC_E_NUMERIC, "singular pair system");
   log_frame_means(pl, (const float2*)(hs + pl->st_dc));
   pl->have_forward = true;
@@ -2146,7 +2145,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
         pl->graph_kbytes[k] = 0;
       }
       int rc = enqueue_forward(pl, nullptr, 1);
-      if (rc == MC_OK) rc = enqueue_tail(pl);
+      if (rc == MC_OK) rc = enqueue_tail(pl, pl->h_stage);
       pl->capturing = false;
       const cudaError_t e = cudaStreamEndCapture(pl->st, &g);
       cudaGetLastError();
@@ -2179,7 +2178,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
     }
   } else {
     CKR(enqueue_forward(pl, waits, chunk));
-    CKR(enqueue_tail(pl));
+    CKR(enqueue_tail(pl, pl->h_stage));
   }
   CK(cudaEventRecord(pl->ev[1], pl->st));
   if (image_host)
@@ -2191,7 +2190,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
   CK(cudaEventElapsedTime(&ms, pl->ev[0], pl->ev[1]));
   pl->tm = mc_timings{};
   pl->tm.total_ms = ms;
-  return finish_device_movie(pl);
+  return finish_device_movie(pl, pl->h_stage);
 }
 
 static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine; }
@@ -2400,3 +2399,52 @@ int mc_fft1d(int n, int batch, int inverse, const void* d_in, void* d_out, void*
 }
 
 }  // extern "C"
+
+// ------------------------------------------- batch captured as one graph --
+// (mc_internal.h; used by mc_batch.cpp)
+size_t mc::plan_stage_bytes(const mc_plan* pl) { return pl->st_bytes; }
+
+bool mc::plan_device_only(const mc_plan* pl) { return device_path(pl) && !pl->two_sets && !pl->stretch; }
+
+cudaStream_t mc::plan_stream(const mc_plan* pl) { return pl->st; }
+
+int mc::plan_reframe_host(mc_plan* pl, const mc_params* p, int nz) {
+  if (!pl || !p) return set_err(MC_E_ARG, "null argument");
+  if (nz <= 1) return set_err(MC_E_ARG, "Not a stack or wrong file. Abort");
+  pl->p.iter = p->iter;
+  pl->p.iterthres = p->iterthres;
+  pl->p.refine = p->refine;
+  return configure_frames(pl, *p, nz, false);
+}
+
+int mc::plan_pair_words(const mc_plan* pl, int* ij, int cap) {
+  const int np = (int)pl->pairs.size();
+  if (np > cap) return set_err(MC_E_STATE, "pair list larger than its block");
+  for (int j = 0; j < np; j++) {
+    ij[2 * j] = pl->pairs[j].first;
+    ij[2 * j + 1] = pl->pairs[j].second;
+  }
+  return MC_OK;
+}
+
+int mc::plan_enqueue_movie(mc_plan* pl, const void* const* frame_word, const int* pairs, unsigned char* stage,
+                           float* image) {
+  if (!device_path(pl)) return set_err(MC_E_STATE, "movie is not device-only (-itr 0, no refinement)");
+  CK(cudaMemcpyAsync(pl->d_pairs_main, pairs, sizeof(int2) * pl->pairs.size(), cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_src_slot, frame_word, sizeof(void*), cudaMemcpyHostToDevice, pl->st));
+  pl->capturing = true;
+  int rc = enqueue_forward(pl, nullptr, 1);
+  if (rc == MC_OK) rc = enqueue_tail(pl, stage);
+  pl->capturing = false;
+  CKR(rc);
+  if (image)
+    CK(cudaMemcpyAsync(image, pl->d_image, sizeof(float) * (size_t)pl->n * pl->n, cudaMemcpyDefault, pl->st));
+  return MC_OK;
+}
+
+int mc::plan_finish_movie(mc_plan* pl, const unsigned char* stage, const void* d_frames) {
+  pl->frames_src = d_frames;
+  pl->loaded.assign(pl->nframe, 1);
+  pl->tm = mc_timings{};
+  return finish_device_movie(pl, stage);
+}

@@ -184,3 +184,70 @@ def test_batch_stress_native(gpu, tmp_path):
     r = subprocess.run([exe, "3", "30", "3"], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "0 mismatches" in r.stdout
+
+
+def _graph_movies(seed, count, geos=((256, 256), (300, 290), (320, 320))):
+    rng = np.random.default_rng(seed)
+    movies, refs, keep = [], [], []
+    for i in range(count):
+        nx, ny = geos[i % len(geos)]
+        nz = int(rng.integers(6, 15))
+        fod = int(rng.choice([1, 2]))
+        if nz // 2 - fod < 1:
+            fod = 0
+        mv = _movie(nx, ny, nz, seed + i)
+        p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=fod), nz)
+        refs.append(_one(mv, p))
+        d = torch.from_numpy(np.ascontiguousarray(mv.frames)).cuda()
+        keep.append(d)
+        n = refs[-1][0].shape[0]
+        img = torch.zeros((n, n), dtype=torch.float32, pin_memory=True)
+        keep.append(img)
+        movies.append({"params": p, "nx": nx, "ny": ny, "nz": nz, "mode": 0, "device_ptr": d.data_ptr(),
+                       "image": img.numpy(), "frame_shifts": np.zeros((nz, 2))})
+    return movies, refs, keep
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 3])
+def test_batch_single_graph_matches_one_at_a_time(gpu, lanes):
+    """Single-graph mode: the whole batch captured as one CUDA graph (lanes as
+    branches), launched once per run and relaunched while the job list stays
+    the same; another job list is captured anew.  Every image and shift list
+    bit-identical to a fresh one-at-a-time plan."""
+    movies, refs, keep = _graph_movies(200, 8)
+    with api.Batch(0, lanes, graph=True) as b:
+        for sub in (movies, movies, movies[2:7], movies):
+            for m in sub:
+                m["image"][:] = -1.0
+                m["frame_shifts"][:] = -1.0
+            out = b.run(sub)
+            for m, r in zip(sub, out):
+                ref = refs[next(k for k, x in enumerate(movies) if x is m)]
+                assert r["status"] == 0 and r["nframe"] == m["frame_shifts"].shape[0]
+                np.testing.assert_array_equal(m["image"], ref[0])
+                np.testing.assert_array_equal(m["frame_shifts"], ref[1])
+        # the same plans then serve the threaded mode
+        b2 = api.Batch(0, lanes)
+        out = b2.run(movies)
+        b2.close()
+        for m, ref in zip(movies, refs):
+            np.testing.assert_array_equal(m["image"], ref[0])
+
+
+def test_batch_single_graph_rejects(gpu):
+    movies, refs, keep = _graph_movies(300, 2)
+    with api.Batch(0, 2, graph=True) as b:
+        host = dict(movies[0])
+        del host["device_ptr"]
+        host["frames"] = np.zeros((host["nz"], host["ny"], host["nx"]), np.uint8)
+        with pytest.raises(_lib.McError, match="device memory"):
+            b.run([host])
+        itr = dict(movies[0], params=api.Params(**{**movies[0]["params"].__dict__, "iter": 2}))
+        with pytest.raises(_lib.McError, match="device-only"):
+            b.run([itr])
+        pageable = dict(movies[1], image=np.zeros_like(movies[1]["image"]))
+        with pytest.raises(_lib.McError, match="pinned"):
+            b.run([pageable])
+        out = b.run(movies)              # and it still runs the valid list
+        for m, ref in zip(movies, refs):
+            np.testing.assert_array_equal(m["image"], ref[0])
