@@ -234,7 +234,7 @@ def factor_codelet(q: int) -> list:
 PFA_RADICES = (2, 3, 4, 5, 7, 8)
 
 
-def pfa_plan(q: int, radices=PFA_RADICES):
+def pfa_plan(q: int):
     """Good-Thomas prime-factor plan of length q: its prime-power groups when
     there are at least two and each is a radix dft_any handles, else None.
     Returns (groups, input multipliers M_i = q / g_i, CRT factors t_i =
@@ -250,18 +250,18 @@ def pfa_plan(q: int, radices=PFA_RADICES):
                 m //= p
             groups.append(g)
         p += 1
-    if len(groups) < 2 or any(g not in radices for g in groups):
+    if len(groups) < 2 or any(g not in PFA_RADICES for g in groups):
         return None
     M = [q // g for g in groups]
     t = [pow(M[i] % groups[i], -1, groups[i]) for i in range(len(groups))]
     return groups, M, t
 
 
-def pfa_indices(q: int, radices=PFA_RADICES):
+def pfa_indices(q: int):
     """(input index, output index) of every multi-index of the PFA plan, in
     the working array's order (multi-index (n_0, n_1, ...) at
     n_0 + g_0 (n_1 + g_1 (...)))."""
-    groups, M, t = pfa_plan(q, radices)
+    groups, M, t = pfa_plan(q)
     import itertools
     ins, outs = [], []
     for idx in itertools.product(*[range(g) for g in reversed(groups)]):
@@ -349,88 +349,6 @@ def emit_codelet(q: int) -> str:
     return "\n".join(L)
 
 
-def rader_plan(R: int = 53, g: int = 2):
-    """Rader's algorithm (C. M. Rader, "Discrete Fourier transforms when the
-    number of data samples is prime", Proc. IEEE 56, 1968) for a prime R with
-    primitive root g: with a[q] = x[g^q] and b[m] = W^(g^-m) (W = e^(-2 pi i
-    / R)), X[g^-p] = x[0] + (a conv b)[p] for p = 0..R-2, a cyclic
-    convolution of length R-1 done by two (R-1)-point DFTs and a pointwise
-    product with the precomputed DFT of b (times 1/(R-1)).  Returns the input
-    and output permutations and the product factors of the forward and the
-    inverse transform."""
-    import cmath
-    N = R - 1
-    assert sorted(pow(g, q, R) for q in range(N)) == list(range(1, R)), "g is not a primitive root"
-    ginv = pow(g, -1, R)
-    perm_in = [pow(g, q, R) for q in range(N)]
-    perm_out = [pow(ginv, p, R) for p in range(N)]
-    fac = {}
-    for inv in (False, True):
-        sgn = 1.0 if inv else -1.0
-        b = [cmath.exp(sgn * 2j * math.pi * pow(ginv, m, R) / R) for m in range(N)]
-        B = [sum(b[m] * cmath.exp(-2j * math.pi * k * m / N) for m in range(N)) / N for k in range(N)]
-        fac[inv] = B
-    return perm_in, perm_out, fac
-
-
-def emit_rader53() -> str:
-    """dft_r53_rader<INV>(v, st): the 53-point DFT by Rader's algorithm, the
-    52-point convolution transforms as 4 x 13 prime-factor DFTs (dft_any<4>,
-    dft_any<13>, no twiddles); every output handed to st(index, value)."""
-    R = 53
-    N = R - 1
-    perm_in, perm_out, fac = rader_plan(R)
-    groups, ins, outs = pfa_indices(N, (4, 13))
-    strides = [1, groups[0]]
-    L = ["template <bool INV, typename St>",
-         "__device__ __forceinline__ void dft_r53_rader(const float2* v, St&& st) {",
-         "  const float2 x0 = v[0];",
-         f"  float2 w[{N}];"]
-    # the permuted input straight into the PFA working order of the forward DFT52
-    inv_ins = {ins[wi]: wi for wi in range(N)}
-    for q in range(N):
-        L.append(f"  w[{inv_ins[q]}] = v[{perm_in[q]}];")
-    L.append("  float2 t = w[0];")
-    L.append(f"#pragma unroll\n  for (int i = 1; i < {N}; i++) t = cadd(t, w[i]);")
-    L.append("  st(0, cadd(x0, t));")
-
-    def pfa_pass(inv):
-        out = []
-        for d, g in enumerate(groups):
-            st_ = strides[d]
-            for base in range(N):
-                if (base // st_) % g:
-                    continue
-                out.append("  {")
-                out.append(f"    float2 x[{g}];")
-                for r in range(g):
-                    out.append(f"    x[{r}] = w[{base + r * st_}];")
-                out.append(f"    dft_any<{g}, {'true' if inv else 'false'}>(x);")
-                for r in range(g):
-                    out.append(f"    w[{base + r * st_}] = x[{r}];")
-                out.append("  }")
-        return out
-    L += pfa_pass(False)
-    # w[wi] holds A[outs[wi]]; product with the factor of that frequency; the
-    # inverse DFT52 then reads its input in the same PFA order (index ins[wi])
-    # -> move A[k] to the position whose input index is k
-    L.append(f"  float2 c[{N}];")
-    inv_ins2 = {ins[wi]: wi for wi in range(N)}
-    for wi in range(N):
-        k = outs[wi]
-        F, Fi = fac[False][k], fac[True][k]
-        L.append(f"  c[{inv_ins2[k]}] = cmul(w[{wi}], INV ? make_float2({flit(Fi.real)}, {flit(Fi.imag)})"
-                 f" : make_float2({flit(F.real)}, {flit(F.imag)}));")
-    L.append(f"#pragma unroll\n  for (int i = 0; i < {N}; i++) w[i] = c[i];")
-    L += pfa_pass(True)
-    # w[wi] = conv[outs[wi]] -> X[perm_out[p]] = x0 + conv[p]
-    for wi in range(N):
-        p_ = outs[wi]
-        L.append(f"  st({perm_out[p_]}, cadd(x0, w[{wi}]));")
-    L.append("}")
-    return "\n".join(L)
-
-
 CODELETS = [4, 8, 10, 12, 14, 16, 20, 24, 28, 30, 32, 35, 40, 48, 56, 60, 64, 70]
 SPLIT53 = 3
 
@@ -477,8 +395,6 @@ def main() -> None:
         for q in CODELETS:
             if pfa_plan(q):
                 out.append(emit_codelet_pfa(q))
-        # radix 53 by Rader's algorithm (the forward transforms' second step)
-        out.append(emit_rader53())
         out.append("template <int Q, bool INV> __device__ __forceinline__ void fft_reg_pf(float2* a) {")
         first = True
         for q in CODELETS:
