@@ -315,6 +315,9 @@ typedef struct mc_schedule {
   int pair_q;        /* codelet length Q of the split n = P*Q (0 = built-in cost model) */
   int pairs_per_cta; /* pairs per CTA of the pair column stage (0 = 32) */
   int pair_variant;  /* reserved: 0 (the register-codelet column kernel) */
+  int fwd_streams;   /* forked streams of the forward transforms, 1..8 (0 = 4) */
+  int fwd_rows_pairing; /* radix-53 step of the forward row pass: 0 built-in, 1 one output pair */
+  int fwd_cols_pairing; /* per loop pass, 2 two; likewise the column pass */
 } mc_schedule;
 int mc_schedule_set(const mc_schedule* s); /* replaces the entry for s->n */
 int mc_schedule_get(int n, mc_schedule* out); /* MC_E_ARG when none is set */

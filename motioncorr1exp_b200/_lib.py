@@ -45,7 +45,8 @@ class McTimings(C.Structure):
 
 
 class McSchedule(C.Structure):
-    _fields_ = [("n", C.c_int), ("pair_q", C.c_int), ("pairs_per_cta", C.c_int), ("pair_variant", C.c_int)]
+    _fields_ = [("n", C.c_int), ("pair_q", C.c_int), ("pairs_per_cta", C.c_int), ("pair_variant", C.c_int),
+                ("fwd_streams", C.c_int), ("fwd_rows_pairing", C.c_int), ("fwd_cols_pairing", C.c_int)]
 
 
 class McBatchJob(C.Structure):

@@ -370,9 +370,13 @@ def solve_pairs(nframe: int, pairs: np.ndarray, shifts: np.ndarray, kithresh: fl
     return {"step": step, "ki1": ki1, "kept": kept[: nk.value].copy(), "ki2": ki2[: nk.value].copy()}
 
 
-def schedule_set(n: int, pair_q: int = 0, pairs_per_cta: int = 0, pair_variant: int = 0) -> None:
-    """Pair-stage schedule for binned side n, used by plans created afterwards."""
-    L.check(L.lib().mc_schedule_set(C.byref(L.McSchedule(n, pair_q, pairs_per_cta, pair_variant))))
+def schedule_set(n: int, pair_q: int = 0, pairs_per_cta: int = 0, pair_variant: int = 0, fwd_streams: int = 0,
+                 fwd_rows_pairing: int = 0, fwd_cols_pairing: int = 0) -> None:
+    """Schedule for binned side n, used by plans created afterwards: the pair
+    stage's split and pairs per CTA, the forward transforms' forked streams
+    and radix-53 pairing of the row / column passes (0 = built-in)."""
+    L.check(L.lib().mc_schedule_set(C.byref(L.McSchedule(n, pair_q, pairs_per_cta, pair_variant, fwd_streams,
+                                                         fwd_rows_pairing, fwd_cols_pairing))))
 
 
 def schedule_get(n: int) -> Optional[dict]:

@@ -1,8 +1,11 @@
-"""Autotuner of the pair-stage schedule (mc_schedule_set).
+"""Autotuner of the pair-stage and forward-transform schedules (mc_schedule_set).
 
 For a binned side n it times the pair stage (column stage + row stage) of a
 synthetic movie under every split n = P*Q the register-codelet kernel takes
-and several pair-per-CTA counts, and keeps the fastest.  Results are cached
+and several pair-per-CTA counts, and keeps the fastest; then, with that pair
+schedule, the forward transforms of the movie under every forked-stream
+count (1, 2, 4, 8) and radix-53 pairing of the row and column passes (one or
+two output pairs per loop pass), and keeps the fastest.  Results are cached
 as JSON keyed by GPU name and n:
 
     {"NVIDIA B200": {"3710": {"pair_q": 35, "pairs_per_cta": 32, "pair_variant": 0,
@@ -49,6 +52,21 @@ def _time_pairs(n: int, frames, params: api.Params, reps: int) -> tuple[float, i
         return ms, pl.info["prune_q"]
 
 
+def _time_forward(n: int, frames, params: api.Params, reps: int) -> float:
+    nz = frames.shape[0]
+    with api.Plan(params, n, n, nz, 0) as pl:
+        pl.load_frames_device(frames.data_ptr(), 0, nz)
+        pl.forward()                    # warm-up
+        ts = []
+        for _ in range(reps):
+            pl.forward()
+            ts.append(pl.timings()["forward_ms"])
+        return float(sorted(ts)[len(ts) // 2])
+
+
+FWD_STREAMS = (1, 2, 4, 8)
+
+
 def tune(n: int, box: int = 96, nframes: int = 16, fod: int = 2, reps: int = 3, device: int = 0,
          seed: int = 0) -> dict:
     """Times every candidate schedule for side n; returns the best entry with
@@ -70,11 +88,24 @@ def tune(n: int, box: int = 96, nframes: int = 16, fod: int = 2, reps: int = 3, 
     if not trials:
         raise RuntimeError(f"no register-codelet split for n={n}")
     best = min(trials, key=lambda t: t["ms"])
+    # forward transforms under the chosen pair schedule (pairing only matters
+    # where the length has a radix-53 step; the others time the same)
+    fwd = []
+    for fs in FWD_STREAMS:
+        for rp in (1, 2):
+            for cp in (1, 2):
+                api.schedule_set(n, pair_q=best["pair_q"], pairs_per_cta=best["pairs_per_cta"], fwd_streams=fs,
+                                 fwd_rows_pairing=rp, fwd_cols_pairing=cp)
+                fwd.append({"fwd_streams": fs, "fwd_rows_pairing": rp, "fwd_cols_pairing": cp,
+                            "ms": _time_forward(n, frames, params, reps)})
+    bf = min(fwd, key=lambda t: t["ms"])
     api.schedule_set(n, pair_q=best["pair_q"], pairs_per_cta=best["pairs_per_cta"],
-                     pair_variant=best["pair_variant"])
-    return {**best, "box": box, "pairs": sum(max(0, nframes - (i + max(1, nframes // 2 - fod)))
-                                             for i in range(nframes)),
-            "trials": trials}
+                     pair_variant=best["pair_variant"], fwd_streams=bf["fwd_streams"],
+                     fwd_rows_pairing=bf["fwd_rows_pairing"], fwd_cols_pairing=bf["fwd_cols_pairing"])
+    return {**best, "fwd_streams": bf["fwd_streams"], "fwd_rows_pairing": bf["fwd_rows_pairing"],
+            "fwd_cols_pairing": bf["fwd_cols_pairing"], "fwd_ms": bf["ms"],
+            "box": box, "pairs": sum(max(0, nframes - (i + max(1, nframes // 2 - fod))) for i in range(nframes)),
+            "trials": trials, "fwd_trials": fwd}
 
 
 def save(results: dict, gpu: str, path: str = DEFAULT_PATH) -> None:
@@ -105,7 +136,9 @@ def load(path: Optional[str] = None, gpu: Optional[str] = None) -> int:
     for n, r in data.get(gpu, {}).items():
         try:
             api.schedule_set(int(n), pair_q=int(r["pair_q"]), pairs_per_cta=int(r["pairs_per_cta"]),
-                             pair_variant=int(r.get("pair_variant", 0)))
+                             pair_variant=int(r.get("pair_variant", 0)), fwd_streams=int(r.get("fwd_streams", 0)),
+                             fwd_rows_pairing=int(r.get("fwd_rows_pairing", 0)),
+                             fwd_cols_pairing=int(r.get("fwd_cols_pairing", 0)))
             count += 1
         except Exception:
             continue   # an entry this build's kernels no longer take
@@ -130,7 +163,10 @@ def main() -> None:
         res[n] = tune(n, a.box, a.frames, fod=a.fod, reps=a.reps, device=a.device)
         t = res[n]
         print(json.dumps({"n": n, "pair_q": t["pair_q"], "pairs_per_cta": t["pairs_per_cta"], "ms": t["ms"],
-                          "trials": [(x["pair_q"], x["pairs_per_cta"], round(x["ms"], 4)) for x in t["trials"]]}),
+                          "trials": [(x["pair_q"], x["pairs_per_cta"], round(x["ms"], 4)) for x in t["trials"]],
+                          "fwd": [t["fwd_streams"], t["fwd_rows_pairing"], t["fwd_cols_pairing"], t["fwd_ms"]],
+                          "fwd_trials": [(x["fwd_streams"], x["fwd_rows_pairing"], x["fwd_cols_pairing"],
+                                          round(x["ms"], 4)) for x in t["fwd_trials"]]}),
               flush=True)
     save(res, gpu_name(a.device), a.out)
 

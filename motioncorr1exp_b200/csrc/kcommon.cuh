@@ -53,16 +53,13 @@ __device__ __forceinline__ void fft_n1(float2* v) {
   else fft_reg<N1, INV>(v);
 }
 
+// Built-in radix-53 schedules of the forward row / column transforms: two
+// output pairs per loop pass in the row pass, one in the column pass
+// (measured on c2: the row pass 9 % faster paired, the column pass 27 %
+// slower); a schedule (mc_schedule_set, the autotuner) can pick either.
+constexpr bool kFwdRowsPaired = true;
+constexpr bool kFwdColsPaired = false;
 // Resident CTAs per SM the two-level transforms are compiled for (register cap).
-// MC_FWD_PAIRED / MC_COL_PAIRED: two radix-53 output pairs per loop iteration
-// in the forward row / column transforms (measured on c2: the row pass 9 %
-// faster with it, the column pass 27 % slower).
-#ifndef MC_FWD_PAIRED
-#define MC_FWD_PAIRED true
-#endif
-#ifndef MC_COL_PAIRED
-#define MC_COL_PAIRED false
-#endif
 #ifndef MC_TL_MIN_BLOCKS
 #define MC_TL_MIN_BLOCKS 4
 #endif

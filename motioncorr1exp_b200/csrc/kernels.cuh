@@ -37,6 +37,7 @@ struct FwdRowsArgs {
   int ldt;
   FftPlan1D plan;      // length nu, forward
   const float2* tw;    // nu twiddles exp(-2 pi i m / nu)
+  int paired;          // radix-53 step: 0 built-in, 1 one output pair per loop pass, 2 two
 };
 
 // Pass B and every other batched transform over contiguous rows:
@@ -52,6 +53,7 @@ struct RowsFftArgs {
   float scale;
   FftPlan1D plan;
   const float2* tw;
+  int paired;          // radix-53 step: 0 built-in, 1 one output pair per loop pass, 2 two
 };
 
 // ------------------------------------------------------------------ pairs --

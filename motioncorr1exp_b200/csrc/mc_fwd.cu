@@ -146,7 +146,7 @@ cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta
 }
 
 // Batched rows: out_row[i] = scale * X[i < keep_lo ? i : i + (n - n_out)].
-template <int N1, int N2, bool INV>
+template <int N1, int N2, bool INV, bool PAIRED>
 __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_fft2l(RowsFftArgs a) {
   using TL = TwoLevel<N1, N2>;
   __shared__ float2 ysm[TL::N];
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_
   float2* out = a.out + row * a.ld_out;
   const int shift = TL::N - a.n_out, keep = a.keep_lo;
   const float sc = a.scale;
-  TL::template run<INV, false, MC_COL_PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
+  TL::template run<INV, false, PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
                         [&](int k, float2 v) {
                           int o;
                           if (k < keep) o = k;
@@ -178,13 +178,27 @@ bool two_level_split(int n, int& n1, int& n2) {
   return false;
 }
 
+// Forward column launch with the radix-53 pairing the schedule asks for
+template <int A, int B>
+void launch_cols_fwd(const RowsFftArgs& a, bool paired, cudaStream_t st) {
+  if constexpr (A == 53) {
+    if (paired != kFwdColsPaired) {
+      k_rows_fft2l<A, B, false, !kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+      return;
+    }
+  }
+  k_rows_fft2l<A, B, false, kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+}
+
 cudaError_t launch_rows_fft2l(const RowsFftArgs& a, bool inverse, cudaStream_t st) {
   int n1 = 0, n2 = 0;
   if (!two_level_split(a.plan.n, n1, n2)) return cudaErrorInvalidValue;
+  // the pairing of the radix-53 step (only N1 = 53 has one): schedule or built-in
+  const bool paired = a.paired == 0 ? kFwdColsPaired : a.paired == 2;
 #define MC_TL_LAUNCH(A, B)                                                                   \
   if (n1 == (A) && n2 == (B)) {                                                              \
-    if (inverse) k_rows_fft2l<A, B, true><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);         \
-    else k_rows_fft2l<A, B, false><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);                \
+    if (inverse) k_rows_fft2l<A, B, true, kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a); \
+    else launch_cols_fwd<A, B>(a, paired, st);                                               \
     return cudaGetLastError();                                                               \
   }
   MC_TWO_LEVEL_LIST(MC_TL_LAUNCH)

@@ -11,7 +11,7 @@ namespace mc {
 // of the float staging for 8-bit frames), decoded in the step-A loads; the
 // spectrum Z is written back into the exchange buffer after the barrier that
 // follows the step-B reads.
-template <int N1, int N2, typename Px>
+template <int N1, int N2, typename Px, bool PAIRED>
 __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_rows2l_raw(FwdRowsArgs a) {
   using TL = TwoLevel<N1, N2>;
   constexpr int N = TL::N;
@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
   __syncthreads();
   const Px* p0 = reinterpret_cast<const Px*>(raw0 + (reinterpret_cast<uintptr_t>(row0) & 15));
   const Px* p1 = reinterpret_cast<const Px*>(raw1 + (reinterpret_cast<uintptr_t>(row1) & 15));
-  TL::template run<false, true, MC_FWD_PAIRED>(
+  TL::template run<false, true, PAIRED>(
       ysm, a.tw, [&](int x) { return make_float2((float)p0[x], (float)p1[x]); },
       [&](int k, float2 v) { ysm[k] = v; });
   __syncthreads();
@@ -90,19 +90,33 @@ __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_fwd_r
   }
 }
 
+template <int A, int B, typename PX, bool PR>
+cudaError_t launch_raw_rows_p(const FwdRowsArgs& a, int grid, cudaStream_t st) {
+  const size_t smem = (size_t)A * B * sizeof(float2) + 2 * (size_t)raw_row_bytes<PX>(A * B);
+  cudaError_t e = allow_smem((const void*)k_fwd_rows2l_raw<A, B, PX, PR>, smem);
+  if (e != cudaSuccess) return e;
+  k_fwd_rows2l_raw<A, B, PX, PR><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Raw-row launch with the radix-53 pairing the schedule asks for (other
+// lengths have no radix-53 step: one instantiation)
+template <int A, int B, typename PX>
+cudaError_t launch_raw_rows(const FwdRowsArgs& a, bool paired, int grid, cudaStream_t st) {
+  if constexpr (A == 53) {
+    if (paired != kFwdRowsPaired) return launch_raw_rows_p<A, B, PX, !kFwdRowsPaired>(a, grid, st);
+  }
+  return launch_raw_rows_p<A, B, PX, kFwdRowsPaired>(a, grid, st);
+}
+
 cudaError_t launch_fwd_rows2l(const FwdRowsArgs& a, cudaStream_t st) {
   int n1 = 0, n2 = 0;
   if (!two_level_split(a.nu, n1, n2)) return cudaErrorInvalidValue;
   const int grid = a.two_outputs ? a.nu : a.nu / 2;
   const bool raw = !a.two_outputs && !a.dark && !a.dark2 && !a.norm && !a.norm2;
-#define MC_TL_RAW(A, B, PX)                                                                          \
-  {                                                                                                  \
-    const size_t smem = (size_t)(A) * (B) * sizeof(float2) + 2 * (size_t)raw_row_bytes<PX>((A) * (B)); \
-    cudaError_t e = allow_smem((const void*)k_fwd_rows2l_raw<A, B, PX>, smem);                       \
-    if (e != cudaSuccess) return e;                                                                  \
-    k_fwd_rows2l_raw<A, B, PX><<<grid, TwoLevel<A, B>::T, smem, st>>>(a);                            \
-    return cudaGetLastError();                                                                       \
-  }
+  // the pairing of the radix-53 step (only N1 = 53 has one): schedule or built-in
+  const bool paired = a.paired == 0 ? kFwdRowsPaired : a.paired == 2;
+#define MC_TL_RAW(A, B, PX) return launch_raw_rows<A, B, PX>(a, paired, grid, st);
 #define MC_TL_LAUNCH(A, B)                                                                           \
   if (n1 == (A) && n2 == (B)) {                                                                      \
     if (raw) {                                                                                       \

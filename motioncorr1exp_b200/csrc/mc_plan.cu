@@ -352,12 +352,15 @@ struct mc_plan {
   std::vector<GraphEntry> graphs;
   bool graph_failed = false;
   bool capturing = false;
-  // forward transforms of independent frames on kForwardStreams forked
-  // streams (parallel branches in a captured movie), so one frame's last
-  // partial wave of CTAs overlaps the next frames' work
-  static constexpr int kForwardStreams = 4;
-  cudaStream_t fst[kForwardStreams] = {};
-  cudaEvent_t fev[kForwardStreams + 1] = {};
+  // forward transforms of independent frames on `nfs` forked streams
+  // (parallel branches in a captured movie; 4 unless a schedule sets it), so
+  // one frame's last partial wave of CTAs overlaps the next frames' work;
+  // the radix-53 pairing of the forward row / column passes (0 built-in)
+  static constexpr int kMaxForwardStreams = 8;
+  int nfs = 4;
+  int fwd_rows_pairing = 0, fwd_cols_pairing = 0;
+  cudaStream_t fst[kMaxForwardStreams] = {};
+  cudaEvent_t fev[kMaxForwardStreams + 1] = {};
   int maxp = 0;
   std::vector<void*> allocs;
 
@@ -787,7 +790,9 @@ int mc_plan_create_capacity(const mc_params* pin, int nx, int ny, int nz, int mo
 
 int mc_schedule_set(const mc_schedule* s) {
   if (!s) return set_err(MC_E_ARG, "null schedule");
-  if (s->n < 16 || s->pair_q < 0 || s->pairs_per_cta < 0 || s->pair_variant != 0)
+  if (s->n < 16 || s->pair_q < 0 || s->pairs_per_cta < 0 || s->pair_variant != 0 || s->fwd_streams < 0 ||
+      s->fwd_streams > 8 || s->fwd_rows_pairing < 0 || s->fwd_rows_pairing > 2 || s->fwd_cols_pairing < 0 ||
+      s->fwd_cols_pairing > 2)
     return set_err(MC_E_ARG, "bad schedule for n=%d", s->n);
   if (s->pair_q > 1 && (s->n % s->pair_q || !mc::pair_cols_reg_supported(s->n / s->pair_q, s->pair_q)))
     return set_err(MC_E_ARG, "pair stage takes no split %d = %d * %d", s->n, s->n / std::max(s->pair_q, 1),
@@ -889,6 +894,11 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
     mc_schedule sc{};
     const bool have_sc = find_schedule(pl->n, &sc);
     pl->ppc = (have_sc && sc.pairs_per_cta > 0) ? std::min(sc.pairs_per_cta, 512) : kPairsPerCta;
+    if (have_sc) {
+      if (sc.fwd_streams > 0) pl->nfs = std::min(sc.fwd_streams, (int)mc_plan::kMaxForwardStreams);
+      pl->fwd_rows_pairing = sc.fwd_rows_pairing;
+      pl->fwd_cols_pairing = sc.fwd_cols_pairing;
+    }
   }
 
   CK(cudaStreamCreateWithFlags(&pl->st, cudaStreamNonBlocking));
@@ -1202,15 +1212,16 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
   // play (binning's row buffer, the stretched frame); per-launch timing
   // events need the one stream
   const bool multi = !binned && !pl->stretch && pl->nframe > 1 && !(pl->profiling && !pl->capturing);
-  constexpr int NS = mc_plan::kForwardStreams;
+  const int NS = pl->nfs;
   if (multi) {
     for (int i = 0; i < NS; i++) {
       if (!pl->fst[i]) CK(cudaStreamCreateWithFlags(&pl->fst[i], cudaStreamNonBlocking));
       if (!pl->fev[i]) CK(cudaEventCreateWithFlags(&pl->fev[i], cudaEventDisableTiming));
     }
-    if (!pl->fev[NS]) CK(cudaEventCreateWithFlags(&pl->fev[NS], cudaEventDisableTiming));
-    CK(cudaEventRecord(pl->fev[NS], pl->st));
-    for (int i = 0; i < NS; i++) CK(cudaStreamWaitEvent(pl->fst[i], pl->fev[NS], 0));
+    cudaEvent_t& fork = pl->fev[mc_plan::kMaxForwardStreams];
+    if (!fork) CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaEventRecord(fork, pl->st));
+    for (int i = 0; i < NS; i++) CK(cudaStreamWaitEvent(pl->fst[i], fork, 0));
   }
   for (int f = 0; f < pl->nframe; f++) {
     cudaStream_t fs = multi ? pl->fst[f % NS] : pl->st;
@@ -1263,6 +1274,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
         b.dark2 = nullptr;
         b.norm2 = nullptr;
         b.outA = pl->d_T;
+        b.paired = pl->fwd_rows_pairing;
         LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes, mc::launch_fwd_rows(b, fs));
         mc::RowsFftArgs c{};
         c.in = pl->d_T;
@@ -1275,11 +1287,13 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
         c.scale = 1.f;
         c.plan = pl->plan_nu;
         c.tw = pl->d_tw_nu;
+        c.paired = pl->fwd_cols_pairing;
         LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, fs));
       }
       continue;
     }
     a.outB = TB;
+    a.paired = pl->fwd_rows_pairing;
     LAUNCH(pl, MC_K_FWD_ROWS, crop_bytes + t_bytes * (pl->two_sets ? 2 : 1), mc::launch_fwd_rows(a, fs));
     for (int set = 0; set < (pl->two_sets ? 2 : 1); set++) {
       mc::RowsFftArgs c{};
@@ -1293,6 +1307,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
       c.scale = 1.f;
       c.plan = pl->plan_nu;
       c.tw = pl->d_tw_nu;
+      c.paired = pl->fwd_cols_pairing;
       LAUNCH(pl, MC_K_FWD_COLS, t_bytes + s_bytes, mc::launch_rows_fft(c, false, 1, fs));
     }
   }

@@ -112,7 +112,10 @@ def test_schedule_table_host_only():
     qs = api.schedule_candidates(3710)
     assert 70 in qs and 35 in qs and all(3710 % q == 0 for q in qs)
     api.schedule_set(3710, pair_q=35, pairs_per_cta=16)
-    assert api.schedule_get(3710) == {"n": 3710, "pair_q": 35, "pairs_per_cta": 16, "pair_variant": 0}
+    assert api.schedule_get(3710) == {"n": 3710, "pair_q": 35, "pairs_per_cta": 16, "pair_variant": 0,
+                                      "fwd_streams": 0, "fwd_rows_pairing": 0, "fwd_cols_pairing": 0}
+    api.schedule_set(3710, pair_q=35, fwd_streams=2, fwd_rows_pairing=1, fwd_cols_pairing=2)
+    assert api.schedule_get(3710)["fwd_streams"] == 2 and api.schedule_get(3710)["fwd_cols_pairing"] == 2
     api.schedule_set(3710, pair_q=70)
     assert api.schedule_get(3710)["pair_q"] == 70
     with pytest.raises(_lib.McError):
@@ -121,6 +124,10 @@ def test_schedule_table_host_only():
         api.schedule_set(3710, pair_q=2)          # P = 1855 above the codelet team size
     with pytest.raises(_lib.McError):
         api.schedule_set(3710, pair_variant=2)
+    with pytest.raises(_lib.McError):
+        api.schedule_set(3710, fwd_streams=9)
+    with pytest.raises(_lib.McError):
+        api.schedule_set(3710, fwd_rows_pairing=3)
     api.schedule_clear()
     assert api.schedule_get(3710) is None
 

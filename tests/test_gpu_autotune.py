@@ -30,3 +30,32 @@ def test_tune_save_load(gpu, tmp_path):
         assert autotune.load(path, gpu="other-gpu") == 0
     finally:
         api.schedule_clear()
+
+
+def test_forward_schedule_trials_and_pairings(gpu):
+    """The forward half of the tuner (forked streams x radix-53 pairing of the
+    row and column passes), and every pairing of the 3710 = 53 x 70
+    transforms giving the oracle's spectra."""
+    import numpy as np
+    from motioncorr1exp_b200 import synth
+    from oracle import mc_oracle as O
+    api.schedule_clear()
+    try:
+        r = autotune.tune(512, box=64, nframes=8, fod=1, reps=1)
+        assert len(r["fwd_trials"]) == len(autotune.FWD_STREAMS) * 4
+        assert r["fwd_ms"] == min(t["ms"] for t in r["fwd_trials"]) > 0
+        assert api.schedule_get(512)["fwd_streams"] == r["fwd_streams"]
+        mv = synth.make_movie(3838, 3710, 3, mean=1.2, seed=71, dtype="u8")
+        o = O.forward_spectrum(O.decode_frame(mv.frames[2], 0), 0, 0, 3710, 3710)
+        p = api.verify_params(api.Params(FrameDistOffset=0), 3)
+        for rp in (1, 2):
+            for cp in (1, 2):
+                api.schedule_set(3710, pair_q=70, pairs_per_cta=32, fwd_streams=2, fwd_rows_pairing=rp,
+                                 fwd_cols_pairing=cp)
+                with api.Plan(p, 3838, 3710, 3, 0) as pl:
+                    pl.load_frames(mv.frames)
+                    pl.forward()
+                    g = pl.spectrum(2)
+                assert np.linalg.norm(g - o) / np.linalg.norm(o) <= 1e-5, (rp, cp)
+    finally:
+        api.schedule_clear()
