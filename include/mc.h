@@ -85,6 +85,10 @@ typedef struct mc_info {
   int two_sets;          /* 1 when dark/gain references make hbuf != hbuf2 */
   int prune_p, prune_q;  /* n = P*Q split of the pruned inverse transform */
   size_t device_bytes;   /* device memory held by the plan */
+  int spectrum_slots;    /* 0: every frame's spectrum stays in HBM; else the
+                            number of spectra held (mc_plan_create_slots) */
+  long long forward_recomputes; /* forward transforms run again because their
+                            spectrum had been given up (slot mode), since creation */
 } mc_info;
 
 typedef struct mc_timings { /* device time of the last run, CUDA events */
@@ -103,6 +107,10 @@ const char* mc_last_error(void);
  * 0 disarms it.  The failure is simulated on the host, nothing is asked of
  * the GPU. */
 void mc_debug_fail_alloc(int nth);
+/* Test hook (no reference counterpart): plans created from now on see at
+ * most `bytes` of free device memory when they size their spectrum store
+ * (mc_plan_create_slots with slots = 0).  0 restores the real figure. */
+void mc_debug_device_budget(size_t bytes);
 
 /* getDefaultPara (dosefgpu_driftcorr.cpp:8-58) plus itr=0, ith=0 (DFAlign.cu:15-16). */
 void mc_default_params(mc_params* p);
@@ -298,6 +306,26 @@ int mc_plan_reframe(mc_plan* plan, const mc_params* p, int nz);
  * frames and cap_pairs frame pairs (0 = this run's counts). */
 int mc_plan_create_capacity(const mc_params* p, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
                             mc_plan** out);
+
+/* mc_plan_create_capacity with a bound on the spectra held in HBM.  The
+ * reference keeps every frame's spectrum in host memory and streams pairs
+ * through the GPU (hbuf / hbuf2, DFAlign.cu:545-546); a plan keeps them in
+ * HBM, and when a movie's spectra do not fit it holds `slots` of them and
+ * recomputes a frame's forward transform from the raw frames (which stay in
+ * HBM) whenever a stage needs a spectrum it gave up: the pair stage runs in
+ * blocks of slots/2 frames against each other, the sums, iterations and the
+ * refinement objective (its adjoint pass included) in chunks of `slots`
+ * frames.  Results are those of the resident plan (the same kernels on the
+ * same spectra, sums accumulated in the same frame order).
+ *   slots = 0        : automatic -- every spectrum when the free device
+ *                      memory allows it (keeping 256 MiB free), else as many
+ *                      as fit; mc_plan_create and _capacity behave this way
+ *   slots >= frames  : every spectrum resident
+ *   4 <= slots       : at most `slots` spectra
+ * Slot mode runs the host-driven pipeline (no captured movie graph) and has
+ * no FSC (mc_plan_fsc returns MC_E_STATE). */
+int mc_plan_create_slots(const mc_params* p, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                         int slots, mc_plan** out);
 
 /* Reads the run's frames (positions nStart..nEnd, nx*ny pixels each in the
  * plan's MRC mode, back to back) in place from caller device memory on the

@@ -34,7 +34,7 @@ class McInfo(C.Structure):
         ("nsam_unbin", C.c_int), ("nsam", C.c_int),
         ("nstart", C.c_int), ("nend", C.c_int), ("nframe", C.c_int),
         ("npairs", C.c_int), ("two_sets", C.c_int), ("prune_p", C.c_int), ("prune_q", C.c_int),
-        ("device_bytes", C.c_size_t),
+        ("device_bytes", C.c_size_t), ("spectrum_slots", C.c_int), ("forward_recomputes", C.c_longlong),
     ]
 
 
@@ -74,6 +74,7 @@ SIGNATURES = {
     "mc_strerror": (C.c_char_p, [C.c_int]),
     "mc_last_error": (C.c_char_p, []),
     "mc_debug_fail_alloc": (None, [C.c_int]),
+    "mc_debug_device_budget": (None, [C.c_size_t]),
     "mc_default_params": (None, [C.POINTER(McParams)]),
     "mc_verify_params": (C.c_int, [C.POINTER(McParams), C.c_int]),
     "mc_plan_create": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -121,6 +122,8 @@ SIGNATURES = {
     "mc_plan_reframe": (C.c_int, [C.c_void_p, C.POINTER(McParams), C.c_int]),
     "mc_plan_create_capacity": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.POINTER(C.c_void_p)]),
+    "mc_plan_create_slots": (C.c_int, [C.POINTER(McParams), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "mc_plan_bind_frames_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mc_schedule_set": (C.c_int, [C.POINTER(McSchedule)]),
     "mc_schedule_get": (C.c_int, [C.c_int, C.POINTER(McSchedule)]),

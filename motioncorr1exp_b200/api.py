@@ -93,12 +93,20 @@ class Plan:
     """One stack geometry on one GPU (mc_plan_create)."""
 
     def __init__(self, params: Params, nx: int, ny: int, nz: int, mode: int,
-                 log: Optional[Callable[[str], None]] = None, cap_frames: int = 0, cap_pairs: int = 0):
+                 log: Optional[Callable[[str], None]] = None, cap_frames: int = 0, cap_pairs: int = 0,
+                 spectrum_slots: Optional[int] = None):
+        """spectrum_slots: None or 0 keeps every frame's spectrum in HBM when
+        it fits (else as many as fit); n >= 4 holds at most n spectra and
+        recomputes the others' forward transforms when a stage needs them
+        (mc_plan_create_slots)."""
         self._lib = L.lib()
         _load_schedules()
         h = C.c_void_p()
         c = params.to_c()
-        if cap_frames or cap_pairs:
+        if spectrum_slots:
+            L.check(self._lib.mc_plan_create_slots(C.byref(c), nx, ny, nz, mode, cap_frames, cap_pairs,
+                                                   spectrum_slots, C.byref(h)))
+        elif cap_frames or cap_pairs:
             L.check(self._lib.mc_plan_create_capacity(C.byref(c), nx, ny, nz, mode, cap_frames, cap_pairs,
                                                       C.byref(h)))
         else:
@@ -164,6 +172,17 @@ class Plan:
     @property
     def npairs(self) -> int:
         return self.info["npairs"]
+
+    @property
+    def spectrum_slots(self) -> int:
+        """0 when every frame's spectrum stays in HBM, else the spectra held."""
+        return self.info["spectrum_slots"]
+
+    @property
+    def forward_recomputes(self) -> int:
+        """Forward transforms run again for spectra the plan had given up."""
+        self._refresh_info()
+        return self.info["forward_recomputes"]
 
     def set_log(self, fn: Callable[[str], None]) -> None:
         def _cb(text, _user):
@@ -538,12 +557,13 @@ def fft1d(d_in: int, d_out: int, n: int, batch: int, inverse: bool, stream: int 
 
 
 def align(frames: np.ndarray, mode: int, params: Params, nz: Optional[int] = None,
-          refs: Optional[dict] = None, log=None, stretch: Optional[tuple] = None) -> dict:
+          refs: Optional[dict] = None, log=None, stretch: Optional[tuple] = None,
+          spectrum_slots: Optional[int] = None) -> dict:
     """Whole path on a stack already in host memory: frames (nz, ny, nx) in
     the file's pixel type.  Returns shifts, pair results and the sum."""
     nf, ny, nx = frames.shape
     nz = nz if nz is not None else nf
-    with Plan(params, nx, ny, nz, mode, log=log) as pl:
+    with Plan(params, nx, ny, nz, mode, log=log, spectrum_slots=spectrum_slots) as pl:
         if stretch:
             pl.set_stretch(*stretch)
         if refs:

@@ -127,6 +127,8 @@ struct ShiftSumArgs {
   const float2* tw;
   float2* acc;           // mode 1: H x ldn scratch for the sum spectrum (split
                          // accumulate / transform); null = fused kernel
+  int accumulate;        // mode 0: 1 = add the listed frames onto out's contents
+                         // (a sum over several launches), 0 = overwrite
 };
 
 // FSC shell sums of -fsc over the listed frames (even / odd list positions).
@@ -173,6 +175,7 @@ struct RampArgs {
 struct ObjectiveArgs {
   const float2* spec;
   long long stride;
+  const int* frames;     // spectrum index of each listed frame (null: 0, 1, ...)
   int nframes;
   const float2* S;       // [kx][ky], pitch ldn
   const double2* shifts; // per frame (sx, sy)

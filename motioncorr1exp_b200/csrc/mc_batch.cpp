@@ -219,6 +219,12 @@ int run_graph_impl(mc_batch* b, const mc_batch_job* jobs, int njobs, mc_batch_re
       e.cap_frames = cap.first;
       e.cap_pairs = cap.second;
     }
+    mc_info in{};
+    mc_plan_info(e.plan, &in);
+    if (in.spectrum_slots)
+      return mc::record_error(MC_E_STATE,
+                              "graph mode needs every spectrum of a movie in HBM; a plan of this batch holds "
+                              "fewer (spectrum slots): run the batch with lanes");
     plan_of[i] = e.plan;
   }
   // pinned per-movie blocks: frame word, pair words, result block

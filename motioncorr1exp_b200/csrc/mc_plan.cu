@@ -37,6 +37,10 @@ thread_local std::string g_err;
 // were out of memory.  0 = off.
 std::atomic<int> g_fail_alloc{0};
 
+// Test hook (mc_debug_device_budget): the free device memory plans see when
+// they size their spectrum store; 0 = the real figure.
+std::atomic<size_t> g_device_budget{0};
+
 bool injected_alloc_failure() {
   int v = g_fail_alloc.load();
   while (v > 0)
@@ -77,6 +81,11 @@ namespace {
 constexpr double kPi = 3.14159265358979323846;
 constexpr int kPairBatch = 512;
 constexpr int kPairsPerCta = 32;
+// spectrum slots: the fewest a plan works with (two blocks of two frames in
+// the pair stage), and the device memory the automatic choice leaves free
+// (kernel modules, captured graphs, first-use buffers, the caller's own)
+constexpr int kMinSlots = 4;
+constexpr size_t kKeepFree = (size_t)256 << 20;
 
 inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
@@ -315,6 +324,16 @@ struct mc_plan {
   const void* frames_src = nullptr;  // bound caller device frames (mc_plan_bind_frames_device) or null
   float *d_dark = nullptr, *d_dark2 = nullptr, *d_norm = nullptr, *d_norm2 = nullptr;
   float2 *d_specA = nullptr, *d_specB = nullptr, *d_T = nullptr;
+  // spectrum slots: 0 = every frame position keeps its spectrum in HBM;
+  // otherwise the store holds `slots` spectra and a stage that needs one it
+  // gave up runs that frame's forward transform again (least recently used
+  // slot first)
+  int slots = 0;
+  std::vector<int> slot_frame;     // frame position held by each slot, -1 none
+  std::vector<int> frame_slot;     // slot holding each frame position, -1 none
+  std::vector<long long> slot_use;  // last use of each slot (0 = empty)
+  long long slot_clock = 0, recomputes = 0;
+  float* d_boxes_all = nullptr;    // slot mode: pair windows gathered in list order
   float2 *d_tw_nu = nullptr, *d_tw_n = nullptr, *d_twQ = nullptr, *d_twO = nullptr, *d_cs = nullptr;
   float2* d_twN = nullptr;  // length-n outer table of the generic pair kernel (large P x box)
   double* d_w16 = nullptr;
@@ -495,6 +514,11 @@ struct mc_plan {
   }
 };
 
+// Forward transforms of every frame position into its own spectrum, or of the
+// listed (frame, slot) jobs (defined with the forward stage below).
+static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk,
+                           const std::vector<std::pair<int, int>>* only = nullptr);
+
 namespace {
 
 // launch `call` (a stage of nk kernels) as kernel kind `kind`, moving `bytes`
@@ -516,6 +540,51 @@ int upload(mc_plan* pl, T* dst, const std::vector<T>& src) {
 
 float2* specA_at(mc_plan* pl, int f) { return pl->d_specA + (long long)f * pl->fstride; }
 float2* specB_at(mc_plan* pl, int f) { return pl->d_specB + (long long)f * pl->fstride; }
+
+// Slot mode: forget every held spectrum (new frames, references or range).
+void clear_slots(mc_plan* pl) {
+  if (!pl->slots) return;
+  pl->slot_frame.assign(pl->slots, -1);
+  pl->slot_use.assign(pl->slots, 0);
+  pl->frame_slot.assign(pl->cap_frames, -1);
+}
+
+// The spectra of `frames` (frame positions, at most `slots` distinct ones)
+// in the store: `where` receives the spectrum index of each listed frame.
+// With every spectrum resident that is the frame position itself; in slot
+// mode frames not held are transformed again into the least recently used
+// slots that no listed frame occupies, on the plan stream, after the work
+// already queued there (which may still read the slots given up).  The
+// forward stage's own pass (`first_pass`) is not counted as recomputation.
+int hold_spectra(mc_plan* pl, const std::vector<int>& frames, std::vector<int>& where, bool first_pass = false) {
+  where = frames;
+  if (!pl->slots) return MC_OK;
+  std::vector<char> keep(pl->slots, 0);
+  for (int f : frames)
+    if (pl->frame_slot[f] >= 0) keep[pl->frame_slot[f]] = 1;
+  std::vector<std::pair<int, int>> jobs;
+  for (int f : frames) {
+    int& fs = pl->frame_slot[f];
+    if (fs < 0) {
+      int best = -1;
+      for (int s = 0; s < pl->slots; s++)
+        if (!keep[s] && (best < 0 || pl->slot_use[s] < pl->slot_use[best])) best = s;
+      if (best < 0) return set_err(MC_E_STATE, "more spectra asked at once than the plan's %d slots", pl->slots);
+      if (pl->slot_frame[best] >= 0) pl->frame_slot[pl->slot_frame[best]] = -1;
+      pl->slot_frame[best] = f;
+      fs = best;
+      keep[best] = 1;
+      jobs.push_back({f, best});
+    }
+    pl->slot_use[fs] = ++pl->slot_clock;
+  }
+  if (!jobs.empty()) {
+    CKR(enqueue_forward(pl, nullptr, 1, &jobs));
+    if (!first_pass) pl->recomputes += (long long)jobs.size();
+  }
+  for (size_t i = 0; i < frames.size(); i++) where[i] = pl->frame_slot[frames[i]];
+  return MC_OK;
+}
 
 // pair stage over an explicit list: (a-frame, b-frame) into a/b spectrum sets
 // Launches the pair kernels for `list`, whose device copy is d_list; results
@@ -600,10 +669,11 @@ int enqueue_pair_stage(mc_plan* pl, const float2* specA, long long strideA, cons
   return MC_OK;
 }
 
-// pair stage over an explicit list, synchronous, results to the host
-int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
-                  const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
-                  std::vector<int>& peak) {
+// pair stage over an explicit list of spectrum indices, synchronous,
+// results to the host
+int run_pair_list_held(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
+                       const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
+                       std::vector<int>& peak) {
   const int np = (int)list.size();
   shift.assign(2 * (size_t)np, 0.f);
   cc.assign(np, 0.f);
@@ -620,9 +690,73 @@ int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const flo
   return pl->collect();
 }
 
+// Pair stage over a list of frame positions (first = a frame of set A, or
+// any index when set A is the sum spectrum, strideA = 0), synchronous,
+// results to the host and the windows to d_boxes in list order.  In slot
+// mode the list runs in groups whose frames the slots hold at once: against
+// the sum, `slots` frames per group; frame against frame, the frames are cut
+// into blocks of slots/2 and each group is the pairs between two blocks (or
+// within one), so a block is transformed once per block it meets.  Every
+// pair is computed by the same kernels as in the resident plan.
+int run_pair_list(mc_plan* pl, const float2* specA, long long strideA, const float2* specB, long long strideB,
+                  const std::vector<mc::PairIJ>& list, std::vector<float>& shift, std::vector<float>& cc,
+                  std::vector<int>& peak) {
+  if (!pl->slots) return run_pair_list_held(pl, specA, strideA, specB, strideB, list, shift, cc, peak);
+  const int np = (int)list.size();
+  const bool vs_sum = strideA == 0;
+  shift.assign(2 * (size_t)np, 0.f);
+  cc.assign(np, 0.f);
+  peak.assign(2 * (size_t)np, 0);
+  const size_t box2 = (size_t)pl->box * pl->box;
+  if (!pl->d_boxes_all) CKR(pl->alloc(&pl->d_boxes_all, sizeof(float) * box2 * pl->maxp));
+  // groups of list positions, keyed by the frame blocks they touch
+  std::map<std::pair<int, int>, std::vector<int>> groups;
+  const int blk = vs_sum ? pl->slots : pl->slots / 2;
+  for (int i = 0; i < np; i++) {
+    const int bj = list[i].second / blk;
+    const int bi = vs_sum ? bj : list[i].first / blk;
+    groups[{std::min(bi, bj), std::max(bi, bj)}].push_back(i);
+  }
+  // against the sum, the last frames first: they are the ones the sum left held
+  std::vector<const std::vector<int>*> order;
+  for (auto& g : groups) order.push_back(&g.second);
+  if (vs_sum) std::reverse(order.begin(), order.end());
+  for (const std::vector<int>* g : order) {
+    std::vector<int> fr;
+    for (int i : *g) {
+      if (!vs_sum) fr.push_back(list[i].first);
+      fr.push_back(list[i].second);
+    }
+    std::sort(fr.begin(), fr.end());
+    fr.erase(std::unique(fr.begin(), fr.end()), fr.end());
+    std::vector<int> where;
+    CKR(hold_spectra(pl, fr, where));
+    std::vector<int> slot_of(pl->nframe, -1);
+    for (size_t k = 0; k < fr.size(); k++) slot_of[fr[k]] = where[k];
+    std::vector<mc::PairIJ> sub;
+    for (int i : *g) sub.push_back({vs_sum ? list[i].first : slot_of[list[i].first], slot_of[list[i].second]});
+    std::vector<float> s, c;
+    std::vector<int> p;
+    CKR(run_pair_list_held(pl, specA, strideA, specB, strideB, sub, s, c, p));
+    for (size_t r = 0; r < g->size(); r++) {
+      const int i = (*g)[r];
+      shift[2 * i] = s[2 * r];
+      shift[2 * i + 1] = s[2 * r + 1];
+      cc[i] = c[r];
+      peak[2 * i] = p[2 * r];
+      peak[2 * i + 1] = p[2 * r + 1];
+      CK(cudaMemcpyAsync(pl->d_boxes_all + (size_t)i * box2, pl->d_boxes + r * box2, sizeof(float) * box2,
+                         cudaMemcpyDeviceToDevice, pl->st));
+    }
+  }
+  CK(cudaMemcpyAsync(pl->d_boxes, pl->d_boxes_all, sizeof(float) * box2 * np, cudaMemcpyDeviceToDevice, pl->st));
+  CK(cudaStreamSynchronize(pl->st));
+  return MC_OK;
+}
+
 // sum of phase-shifted frames of set A; mode 0 -> d_sum spectrum, mode 1 -> image
-int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector<cplx>& shifts,
-                  const std::vector<int>& apply, int mode) {
+int run_shift_sum_held(mc_plan* pl, const std::vector<int>& frames, const std::vector<cplx>& shifts,
+                       const std::vector<int>& apply, int mode, int accumulate = 0) {
   const int ns = (int)frames.size();
   std::vector<double2> sh(ns);
   for (int i = 0; i < ns; i++) sh[i] = make_double2(shifts[i].real(), shifts[i].imag());
@@ -643,6 +777,7 @@ int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector
   a.plan = pl->plan_n;
   a.tw = pl->d_tw_n;
   a.acc = pl->d_sumacc;
+  a.accumulate = accumulate;
   if (mode == 0) {
     a.out = pl->d_sum;
     a.ld_out = pl->ldn;
@@ -668,6 +803,61 @@ int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector
   return MC_OK;
 }
 
+
+// The sum of phase-shifted frames (frame positions) as run_shift_sum_held.
+// In slot mode the frames are summed `slots` at a time into d_sum, each
+// chunk adding onto the last in frame order, so the sum spectrum is the
+// resident plan's bit for bit; mode 1 then transforms d_sum as the one
+// unshifted term of a sum (0 + S is S exactly).  Leaves the ramps of the
+// last chunk in d_ey.
+int run_shift_sum(mc_plan* pl, const std::vector<int>& frames, const std::vector<cplx>& shifts,
+                  const std::vector<int>& apply, int mode) {
+  if (!pl->slots) return run_shift_sum_held(pl, frames, shifts, apply, mode);
+  const int ns = (int)frames.size();
+  for (int c0 = 0; c0 < ns; c0 += pl->slots) {
+    const int cnt = std::min(pl->slots, ns - c0);
+    const std::vector<int> fr(frames.begin() + c0, frames.begin() + c0 + cnt);
+    std::vector<int> where;
+    CKR(hold_spectra(pl, fr, where));
+    CKR(run_shift_sum_held(pl, where, std::vector<cplx>(shifts.begin() + c0, shifts.begin() + c0 + cnt),
+                           std::vector<int>(apply.begin() + c0, apply.begin() + c0 + cnt), 0, c0 > 0 ? 1 : 0));
+  }
+  if (mode == 0) return MC_OK;
+  mc::ShiftSumArgs a{};
+  const std::vector<int> zero{0};
+  const std::vector<double2> none{make_double2(0.0, 0.0)};
+  CK(cudaMemcpyAsync(pl->d_sumframes, zero.data(), sizeof(int), cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_apply, zero.data(), sizeof(int), cudaMemcpyHostToDevice, pl->st));
+  CK(cudaMemcpyAsync(pl->d_sumshift, none.data(), sizeof(double2), cudaMemcpyHostToDevice, pl->st));
+  a.spec = pl->d_sum;
+  a.stride = 0;
+  a.frames = pl->d_sumframes;
+  a.shifts = pl->d_sumshift;
+  a.apply = pl->d_apply;
+  a.nsum = 1;
+  a.n = pl->n;
+  a.ldn = pl->ldn;
+  a.H = pl->H;
+  a.mode = 1;
+  a.plan = pl->plan_n;
+  a.tw = pl->d_tw_n;
+  a.acc = pl->d_sumacc;
+  a.out = pl->d_T2;
+  a.ld_out = pl->ldt2;
+  const double spec_bytes = (double)pl->H * pl->n * sizeof(float2);
+  LAUNCH_N(pl, MC_K_SHIFT_SUM, 2 * spec_bytes, mc::shift_sum_kernels(a), mc::launch_shift_sum(a, pl->d_ey, pl->st));
+  mc::C2rRowsArgs c{};
+  c.t2 = pl->d_T2;
+  c.ld_t2 = pl->ldt2;
+  c.n = pl->n;
+  c.H = pl->H;
+  c.scale = (float)(1.0 / ((double)pl->n * pl->n));
+  c.image = pl->d_image;
+  c.plan = pl->plan_n;
+  c.tw = pl->d_tw_n;
+  LAUNCH(pl, MC_K_C2R_ROWS, spec_bytes + (double)pl->n * pl->n * sizeof(float), mc::launch_c2r_rows(c, pl->st));
+  return MC_OK;
+}
 }  // namespace
 
 // ================================================================== C ABI ==
@@ -692,6 +882,8 @@ const char* mc_strerror(int code) {
 const char* mc_last_error(void) { return g_err.c_str(); }
 
 void mc_debug_fail_alloc(int nth) { g_fail_alloc.store(nth > 0 ? nth : 0); }
+
+void mc_debug_device_budget(size_t bytes) { g_device_budget.store(bytes); }
 
 void mc_default_params(mc_params* p) {
   if (!p) return;
@@ -774,18 +966,26 @@ static int configure_frames(mc_plan* pl, const mc_params& q, int nz, bool upload
 }
 
 static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
-                       mc_plan** out);
+                       int slots, mc_plan** out);
 
 extern "C" {
 
 int mc_plan_create(const mc_params* pin, int nx, int ny, int nz, int mode, mc_plan** out) {
-  return create_plan(pin, nx, ny, nz, mode, 0, 0, out);
+  return create_plan(pin, nx, ny, nz, mode, 0, 0, 0, out);
 }
 
 int mc_plan_create_capacity(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
                             mc_plan** out) {
   if (cap_frames < 0 || cap_pairs < 0) return set_err(MC_E_ARG, "negative capacity");
-  return create_plan(pin, nx, ny, nz, mode, cap_frames, cap_pairs, out);
+  return create_plan(pin, nx, ny, nz, mode, cap_frames, cap_pairs, 0, out);
+}
+
+int mc_plan_create_slots(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
+                         int slots, mc_plan** out) {
+  if (cap_frames < 0 || cap_pairs < 0) return set_err(MC_E_ARG, "negative capacity");
+  if (slots < 0 || (slots > 0 && slots < kMinSlots))
+    return set_err(MC_E_ARG, "spectrum slots %d: 0 (automatic) or at least %d", slots, kMinSlots);
+  return create_plan(pin, nx, ny, nz, mode, cap_frames, cap_pairs, slots, out);
 }
 
 int mc_schedule_set(const mc_schedule* s) {
@@ -841,7 +1041,7 @@ int mc_plan_reframe(mc_plan* pl, const mc_params* p, int nz) {
 }  // extern "C"
 
 static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, int cap_frames, int cap_pairs,
-                       mc_plan** out) {
+                       int slots, mc_plan** out) {
   if (!pin || !out) return set_err(MC_E_ARG, "null argument");
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0) return set_err(MC_E_ARG, "bad stack size %d x %d x %d", nx, ny, nz);
@@ -914,8 +1114,6 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
   // device buffers
   pl->frame_bytes = (size_t)nx * ny * pl->wl;
   CKR(pl->alloc(&pl->d_frames, pl->frame_bytes * capf));
-  CKR(pl->alloc(&pl->d_specA, sizeof(float2) * pl->fstride * capf));
-  pl->d_specB = pl->d_specA;
   if (pl->nu != pl->n) CKR(pl->alloc(&pl->d_T, sizeof(float2) * (size_t)pl->H * pl->ldu));
   CKR(pl->alloc(&pl->d_pairs, sizeof(int2) * pl->maxp));
   CKR(pl->alloc(&pl->d_G, sizeof(float2) * (size_t)std::min(pl->maxp, kPairBatch) * pl->H * pl->box));
@@ -1038,6 +1236,34 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
     CKR(pl->alloc(&pl->d_w16, sizeof(double) * w.size()));
     CKR(upload(pl, pl->d_w16, w));
   }
+  {
+    // the spectrum store, last: every frame position's spectrum, or `slots`
+    // of them when asked or when the free device memory holds fewer
+    const size_t spec = sizeof(float2) * (size_t)pl->fstride;
+    int ns = capf;
+    if (slots > 0) {
+      ns = std::min(slots, capf);
+    } else {
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      const size_t budget = g_device_budget.load();
+      if (budget) fr = std::min(fr, budget);
+      const size_t room = fr > kKeepFree ? fr - kKeepFree : 0;
+      if ((size_t)capf * spec > room) ns = (int)std::min<size_t>(room / spec, (size_t)capf);
+      if (ns < kMinSlots)
+        return set_err(MC_E_NOMEM,
+                       "%d spectra of %zu bytes do not fit the free device memory (%zu bytes), nor do %d of them",
+                       capf, spec, fr, kMinSlots);
+    }
+    CKR(pl->alloc(&pl->d_specA, spec * ns));
+    pl->d_specB = pl->d_specA;
+    if (ns < capf) {
+      pl->slots = ns;
+      pl->slot_frame.assign(ns, -1);
+      pl->slot_use.assign(ns, 0);
+      pl->frame_slot.assign(capf, -1);
+    }
+  }
   CK(cudaStreamSynchronize(pl->st));
   pl->loaded.assign(pl->nframe, 0);
   *out = guard.release();
@@ -1089,6 +1315,8 @@ int mc_plan_info(const mc_plan* pl, mc_info* i) {
   i->prune_p = pl->P;
   i->prune_q = pl->Q;
   i->device_bytes = pl->dev_bytes;
+  i->spectrum_slots = pl->slots;
+  i->forward_recomputes = pl->recomputes;
   return MC_OK;
 }
 
@@ -1114,7 +1342,8 @@ int mc_plan_set_refs(mc_plan* pl, const float* dark, const float* dark2, const f
   CKR(put(&pl->d_norm2, norm2));
   const bool two = dark || norm;
   if (two && !pl->two_sets) {
-    CKR(pl->alloc(&pl->d_specB, sizeof(float2) * pl->fstride * pl->nframe));
+    // as many spectra as set A holds (a reframe may grow nframe up to cap_frames)
+    CKR(pl->alloc(&pl->d_specB, sizeof(float2) * pl->fstride * (pl->slots ? pl->slots : pl->cap_frames)));
     pl->two_sets = true;
   }
   CK(cudaStreamSynchronize(pl->st));
@@ -1206,12 +1435,16 @@ static bool device_path(const mc_plan* pl);
 // Forward transforms of every position.  With `waits`, the plan stream waits
 // for (*waits)[f / chunk] before the first frame of each chunk (pipelined
 // upload); the per-frame means are read back and logged at the end.
-static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
+static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk,
+                           const std::vector<std::pair<int, int>>* only) {
+  // `only`: (frame, spectrum slot) pairs to transform (the spectra-slot mode);
+  // default every frame into its own slot
   const bool binned = pl->nu != pl->n;
   // frames write only their own spectrum slots unless a shared scratch is in
   // play (binning's row buffer, the stretched frame); per-launch timing
   // events need the one stream
-  const bool multi = !binned && !pl->stretch && pl->nframe > 1 && !(pl->profiling && !pl->capturing);
+  const int njob = only ? (int)only->size() : pl->nframe;
+  const bool multi = !binned && !pl->stretch && njob > 1 && !(pl->profiling && !pl->capturing);
   const int NS = pl->nfs;
   if (multi) {
     for (int i = 0; i < NS; i++) {
@@ -1223,8 +1456,10 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     CK(cudaEventRecord(fork, pl->st));
     for (int i = 0; i < NS; i++) CK(cudaStreamWaitEvent(pl->fst[i], fork, 0));
   }
-  for (int f = 0; f < pl->nframe; f++) {
-    cudaStream_t fs = multi ? pl->fst[f % NS] : pl->st;
+  for (int job = 0; job < njob; job++) {
+    const int f = only ? (*only)[job].first : job;
+    const int slot = only ? (*only)[job].second : job;
+    cudaStream_t fs = multi ? pl->fst[job % NS] : pl->st;
     if (waits && (multi || f % chunk == 0)) CK(cudaStreamWaitEvent(fs, (*waits)[f / chunk], 0));
     mc::FwdRowsArgs a{};
     a.frame = (const char*)(pl->frames_src ? pl->frames_src : pl->d_frames) + (size_t)f * pl->frame_bytes;
@@ -1252,7 +1487,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     a.norm = stretched ? pl->d_norm_s : pl->d_norm;
     a.norm2 = stretched ? pl->d_norm2_s : pl->d_norm2;
     a.two_outputs = pl->two_sets ? 1 : 0;
-    float2* TA = binned ? pl->d_T : specA_at(pl, f);
+    float2* TA = binned ? pl->d_T : specA_at(pl, slot);
     a.outA = TA;
     a.ldt = binned ? pl->ldu : pl->ldn;
     a.plan = pl->plan_nu;
@@ -1262,7 +1497,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
     const double t_bytes = (double)pl->H * pl->nu * sizeof(float2);
     const double s_bytes = (double)pl->H * pl->n * sizeof(float2);
     float2* TB = nullptr;
-    if (pl->two_sets) TB = binned ? nullptr : specB_at(pl, f);
+    if (pl->two_sets) TB = binned ? nullptr : specB_at(pl, slot);
     if (pl->two_sets && binned) {
       // binned two-set case: set A, then set B, each through the scratch d_T
       // with its references folded into the one-output row transform
@@ -1279,7 +1514,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
         mc::RowsFftArgs c{};
         c.in = pl->d_T;
         c.ld_in = pl->ldu;
-        c.out = set == 0 ? specA_at(pl, f) : specB_at(pl, f);
+        c.out = set == 0 ? specA_at(pl, slot) : specB_at(pl, slot);
         c.ld_out = pl->ldn;
         c.nrows = pl->H;
         c.n_out = pl->n;
@@ -1299,7 +1534,7 @@ static int enqueue_forward(mc_plan* pl, const std::vector<cudaEvent_t>* waits, i
       mc::RowsFftArgs c{};
       c.in = set == 0 ? TA : TB;
       c.ld_in = a.ldt;
-      c.out = set == 0 ? specA_at(pl, f) : specB_at(pl, f);
+      c.out = set == 0 ? specA_at(pl, slot) : specB_at(pl, slot);
       c.ld_out = pl->ldn;
       c.nrows = pl->H;
       c.n_out = pl->n;
@@ -1375,12 +1610,31 @@ static int upload_frame_base(mc_plan* pl) {
 static int forward_all(mc_plan* pl, const std::vector<cudaEvent_t>* waits, int chunk) {
   CKR(upload_frame_base(pl));
   CK(cudaEventRecord(pl->ev[0], pl->st));
-  CKR(enqueue_forward(pl, waits, chunk));
-  CK(cudaEventRecord(pl->ev[1], pl->st));
   std::vector<float2> dc(pl->nframe);
-  CK(cudaMemcpy2DAsync(dc.data(), sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
-                       pl->nframe, cudaMemcpyDeviceToHost, pl->st));
-  CK(cudaStreamSynchronize(pl->st));
+  if (pl->slots) {
+    // slot mode: every frame once, `slots` at a time, for its DC term; the
+    // last chunk stays held for the stage that follows
+    clear_slots(pl);
+    if (waits)
+      for (size_t c = 0; c * chunk < (size_t)pl->nframe; c++) CK(cudaStreamWaitEvent(pl->st, (*waits)[c], 0));
+    float2* hdc = reinterpret_cast<float2*>(pl->h_stage + pl->st_dc);
+    for (int f0 = 0; f0 < pl->nframe; f0 += pl->slots) {
+      std::vector<int> fr, where;
+      for (int f = f0; f < std::min(pl->nframe, f0 + pl->slots); f++) fr.push_back(f);
+      CKR(hold_spectra(pl, fr, where, true));
+      for (size_t i = 0; i < fr.size(); i++)
+        CK(cudaMemcpyAsync(hdc + fr[i], specA_at(pl, where[i]), sizeof(float2), cudaMemcpyDeviceToHost, pl->st));
+    }
+    CK(cudaEventRecord(pl->ev[1], pl->st));
+    CK(cudaStreamSynchronize(pl->st));
+    std::copy(hdc, hdc + pl->nframe, dc.begin());
+  } else {
+    CKR(enqueue_forward(pl, waits, chunk));
+    CK(cudaEventRecord(pl->ev[1], pl->st));
+    CK(cudaMemcpy2DAsync(dc.data(), sizeof(float2), pl->d_specA, sizeof(float2) * pl->fstride, sizeof(float2),
+                         pl->nframe, cudaMemcpyDeviceToHost, pl->st));
+    CK(cudaStreamSynchronize(pl->st));
+  }
   CKR(pl->collect());
   CK(cudaEventElapsedTime(&pl->tm.forward_ms, pl->ev[0], pl->ev[1]));
   log_frame_means(pl, dc.data());
@@ -1746,6 +2000,9 @@ static void display_short(const float* buf, int size, int16_t* disp) {
 int mc_plan_fsc(mc_plan* pl, double* rows, int cap, int* nbox_out) {
   if (!pl) return set_err(MC_E_ARG, "null plan");
   if (!pl->have_sum) return set_err(MC_E_STATE, "FSC before the corrected sum");
+  if (pl->slots)
+    return set_err(MC_E_STATE, "FSC reads every summed spectrum at once; this plan holds %d (spectrum slots)",
+                   pl->slots);
   const int n = pl->n;
   if (n < 400) return set_err(MC_E_SIZE, "FSC needs nsam >= 400 (shell width nsam/400), nsam is %d", n);
   const int step = n / 400, nsamc = n / 2 + 1, nbox = nsamc / step + 1;
@@ -1941,7 +2198,34 @@ static int objective(mc_plan* pl, const std::vector<cplx>& s, double* J, double*
   a.partial = pl->d_opart;
   a.partialJ = pl->d_opart + (size_t)pl->H * nf * 5;
   a.out = pl->d_oout;
-  LAUNCH_N(pl, MC_K_OBJECTIVE, (double)(nf + 1) * pl->H * pl->n * sizeof(float2), 2, mc::launch_objective(a, pl->st));
+  if (pl->slots) {
+    // slot mode: the adjoint pass over chunks of `slots` frames (their
+    // spectra held again, their shifts and ramps re-laid), each chunk's
+    // per-frame totals at its frames' places; every chunk also writes J at
+    // the entry after its last frame, which the next chunk overwrites, so the
+    // last chunk's J (the same sum over S each time) is the one left
+    for (int c0 = 0; c0 < nf; c0 += pl->slots) {
+      const int cnt = std::min(pl->slots, nf - c0);
+      const std::vector<int> fr(frames.begin() + c0, frames.begin() + c0 + cnt);
+      std::vector<int> where;
+      CKR(hold_spectra(pl, fr, where));
+      std::vector<double2> sh(cnt);
+      for (int i = 0; i < cnt; i++) sh[i] = make_double2(s[c0 + i].real(), s[c0 + i].imag());
+      CK(cudaMemcpyAsync(pl->d_sumframes, where.data(), sizeof(int) * cnt, cudaMemcpyHostToDevice, pl->st));
+      CK(cudaMemcpyAsync(pl->d_sumshift, sh.data(), sizeof(double2) * cnt, cudaMemcpyHostToDevice, pl->st));
+      CK(mc::launch_ramp(pl->d_sumshift, cnt, pl->n, pl->d_ey, pl->st));
+      mc::ObjectiveArgs b = a;
+      b.frames = pl->d_sumframes;
+      b.nframes = cnt;
+      b.partialJ = pl->d_opart + (size_t)pl->H * cnt * 5;
+      b.out = pl->d_oout + (size_t)c0 * 5;
+      LAUNCH_N(pl, MC_K_OBJECTIVE, (double)(cnt + 1) * pl->H * pl->n * sizeof(float2), 2,
+               mc::launch_objective(b, pl->st));
+    }
+  } else {
+    LAUNCH_N(pl, MC_K_OBJECTIVE, (double)(nf + 1) * pl->H * pl->n * sizeof(float2), 2,
+             mc::launch_objective(a, pl->st));
+  }
   std::vector<double> out((size_t)nf * 5 + 1);
   CK(cudaMemcpyAsync(out.data(), pl->d_oout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, pl->st));
   CK(cudaStreamSynchronize(pl->st));
@@ -2208,7 +2492,7 @@ static int run_device(mc_plan* pl, float* image_host, const std::vector<cudaEven
   return finish_device_movie(pl, pl->h_stage);
 }
 
-static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine; }
+static bool device_path(const mc_plan* pl) { return pl->p.iter == 0 && !pl->p.refine && !pl->slots; }
 
 extern "C" {
 
@@ -2288,7 +2572,9 @@ int mc_plan_get_spectrum(mc_plan* pl, int set, int pos, void* host) {
   if (!pl->have_forward) return set_err(MC_E_STATE, "no forward yet");
   if (pos < 0 || pos >= pl->nframe || set < 0 || set > 1) return set_err(MC_E_ARG, "bad set/pos");
   CK(cudaSetDevice(pl->device));
-  const float2* src = (set == 0 ? pl->d_specA : pl->d_specB) + (long long)pos * pl->fstride;
+  std::vector<int> where;
+  CKR(hold_spectra(pl, {pos}, where));
+  const float2* src = (set == 0 ? pl->d_specA : pl->d_specB) + (long long)where[0] * pl->fstride;
   CK(cudaMemcpy2DAsync(host, sizeof(float2) * pl->n, src, sizeof(float2) * pl->ldn, sizeof(float2) * pl->n, pl->H,
                        cudaMemcpyDeviceToHost, pl->st));
   CK(cudaStreamSynchronize(pl->st));
@@ -2444,7 +2730,8 @@ int mc::plan_pair_words(const mc_plan* pl, int* ij, int cap) {
 
 int mc::plan_enqueue_movie(mc_plan* pl, const void* const* frame_word, const int* pairs, unsigned char* stage,
                            float* image) {
-  if (!device_path(pl)) return set_err(MC_E_STATE, "movie is not device-only (-itr 0, no refinement)");
+  if (!device_path(pl))
+    return set_err(MC_E_STATE, "movie is not device-only (-itr 0, no refinement, every spectrum resident)");
   CK(cudaMemcpyAsync(pl->d_pairs_main, pairs, sizeof(int2) * pl->pairs.size(), cudaMemcpyHostToDevice, pl->st));
   CK(cudaMemcpyAsync(pl->d_src_slot, frame_word, sizeof(void*), cudaMemcpyHostToDevice, pl->st));
   pl->capturing = true;

@@ -391,7 +391,10 @@ __global__ void __launch_bounds__(kThreads) k_shift_acc(ShiftSumArgs a, const fl
   const int k0 = blockIdx.x * kSumChunk + tid;
   float2 acc[kSumE];
 #pragma unroll
-  for (int j = 0; j < kSumE; j++) acc[j] = make_float2(0.f, 0.f);
+  for (int j = 0; j < kSumE; j++) {
+    const int ky = k0 + kThreads * j;
+    acc[j] = (a.accumulate && ky < n) ? out[(long long)kx * ld_out + ky] : make_float2(0.f, 0.f);
+  }
   const float2* colx = a.spec + (long long)kx * a.ldn;
   for (int f0 = 0; f0 < a.nsum; f0 += kSumG) {
     float2 v[kSumG][kSumE], y[kSumG][kSumE];
@@ -621,7 +624,7 @@ __global__ void __launch_bounds__(kThreads) k_objective(ObjectiveArgs a) {
   __syncthreads();
   // per frame: warp sums into shared memory, one barrier for all frames
   for (int f = 0; f < a.nframes; f++) {
-    const float2* c = a.spec + (long long)f * a.stride + (long long)kx * a.ldn;
+    const float2* c = a.spec + (long long)(a.frames ? a.frames[f] : f) * a.stride + (long long)kx * a.ldn;
     const float2* eyf = a.ey + (long long)f * n;
     const float2 e = ex[f];
     // loads in batches of KB spectrum + KB ramp values, all issued before use
