@@ -181,7 +181,9 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
 // as items (output row m, chunk of at most 16 k1): Horner's rule from the
 // chunk's last term down, acc = acc w + Y with w = W^(y_m) (4 FMAs per term,
 // no twiddle loads; the powers of the rounded w drift by ~1e-6 over a chunk),
-// then one multiply by W^(kb y_m).  Consecutive threads take consecutive rows
+// then one multiply by W^(kb y_m).  A thread runs two items at a time with
+// their chains interleaved (5.85 -> 5.71 ms per c2 movie: with two warps
+// per scheduler the dependent FMAs of one item left issue slots empty).  Consecutive threads take consecutive rows
 // m, so their Y rows (odd stride in float2) fall on different bank pairs and
 // their twiddle loads are contiguous.  The chunk partials meet in shared
 // memory and are added in chunk order.
@@ -245,33 +247,56 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
     }
     team_barrier(1 + tm, T);
     int c = lt / box, m = lt - (lt / box) * box;
-    for (int it = lt; it < box * C; it += T) {
-      int r = ys + m % Q;
-      if (r >= Q) r -= Q;
-      const int kb = c * L;
-      const float2* yr = Y + PS * r + kb;
-      // two independent chains over the even and odd terms in w^2, then
-      // S = S_even + w S_odd: twice the instruction-level parallelism of one
-      // chain of dependent FMAs
-      const float2 w = tws[m];
-      const float2 w2 = cmul(w, w);
-      float2 ae = make_float2(0.f, 0.f), ao = make_float2(0.f, 0.f);
+    // two items per pass, their chains interleaved (twice the independent work)
+    for (int it = lt; it < box * C; it += 2 * T) {
+      int c1 = c, m1 = m + T;
+      while (m1 >= box) {
+        m1 -= box;
+        c1++;
+      }
+      const bool two = it + T < box * C;
+      if (!two) {
+        c1 = c;
+        m1 = m;
+      }
+      int r0 = ys + m % Q, r1 = ys + m1 % Q;
+      if (r0 >= Q) r0 -= Q;
+      if (r1 >= Q) r1 -= Q;
+      const int kb0 = c * L, kb1 = c1 * L;
+      const float2* yr0 = Y + PS * r0 + kb0;
+      const float2* yr1 = Y + PS * r1 + kb1;
+      const float2 w0 = tws[m], w1 = tws[m1];
+      const float2 v0 = cmul(w0, w0), v1 = cmul(w1, w1);
+      float2 ae0 = make_float2(0.f, 0.f), ao0 = make_float2(0.f, 0.f);
+      float2 ae1 = make_float2(0.f, 0.f), ao1 = make_float2(0.f, 0.f);
 #pragma unroll
       for (int kk = L - 1; kk >= 0; kk--) {
-        if (L * C == P || kb + kk < P) {
-          const float2 yv = yr[kk];
-          float2& h = (kk & 1) ? ao : ae;
+        if (L * C == P || kb0 + kk < P) {
+          const float2 yv = yr0[kk];
+          float2& h = (kk & 1) ? ao0 : ae0;
           const float2 s = h;
-          h.x = fmaf(s.x, w2.x, fmaf(-s.y, w2.y, yv.x));
-          h.y = fmaf(s.x, w2.y, fmaf(s.y, w2.x, yv.y));
+          h.x = fmaf(s.x, v0.x, fmaf(-s.y, v0.y, yv.x));
+          h.y = fmaf(s.x, v0.y, fmaf(s.y, v0.x, yv.y));
+        }
+        if (L * C == P || kb1 + kk < P) {
+          const float2 yv = yr1[kk];
+          float2& h = (kk & 1) ? ao1 : ae1;
+          const float2 s = h;
+          h.x = fmaf(s.x, v1.x, fmaf(-s.y, v1.y, yv.x));
+          h.y = fmaf(s.x, v1.y, fmaf(s.y, v1.x, yv.y));
         }
       }
-      float2 acc;
-      acc.x = fmaf(ao.x, w.x, fmaf(-ao.y, w.y, ae.x));
-      acc.y = fmaf(ao.x, w.y, fmaf(ao.y, w.x, ae.y));
-      if (kb < P) acc = cmul(acc, tws[(1 + c) * box + m]);
-      part[c * box + m] = acc;
-      m += T;
+      float2 acc0, acc1;
+      acc0.x = fmaf(ao0.x, w0.x, fmaf(-ao0.y, w0.y, ae0.x));
+      acc0.y = fmaf(ao0.x, w0.y, fmaf(ao0.y, w0.x, ae0.y));
+      acc1.x = fmaf(ao1.x, w1.x, fmaf(-ao1.y, w1.y, ae1.x));
+      acc1.y = fmaf(ao1.x, w1.y, fmaf(ao1.y, w1.x, ae1.y));
+      if (kb0 < P) acc0 = cmul(acc0, tws[(1 + c) * box + m]);
+      if (kb1 < P) acc1 = cmul(acc1, tws[(1 + c1) * box + m1]);
+      part[c * box + m] = acc0;
+      if (two) part[c1 * box + m1] = acc1;
+      m = m1 + T;
+      c = c1;
       while (m >= box) {
         m -= box;
         c++;

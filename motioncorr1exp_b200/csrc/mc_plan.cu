@@ -1249,11 +1249,13 @@ static int create_plan(const mc_params* pin, int nx, int ny, int nz, int mode, i
       const size_t budget = g_device_budget.load();
       if (budget) fr = std::min(fr, budget);
       const size_t room = fr > kKeepFree ? fr - kKeepFree : 0;
-      if ((size_t)capf * spec > room) ns = (int)std::min<size_t>(room / spec, (size_t)capf);
-      if (ns < kMinSlots)
-        return set_err(MC_E_NOMEM,
-                       "%d spectra of %zu bytes do not fit the free device memory (%zu bytes), nor do %d of them",
-                       capf, spec, fr, kMinSlots);
+      if ((size_t)capf * spec > room) {
+        ns = (int)std::min<size_t>(room / spec, (size_t)capf);
+        if (ns < kMinSlots)
+          return set_err(MC_E_NOMEM,
+                         "%d spectra of %zu bytes do not fit the free device memory (%zu bytes), nor do %d of them",
+                         capf, spec, fr, kMinSlots);
+      }
     }
     CKR(pl->alloc(&pl->d_specA, spec * ns));
     pl->d_specB = pl->d_specA;

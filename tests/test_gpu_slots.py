@@ -200,3 +200,13 @@ def test_c4_with_sixteen_slots_equals_resident(gpu):
     np.testing.assert_array_equal(s0, s1)
     np.testing.assert_array_equal(i0, i1)
     assert b1 < b0
+
+
+def test_short_movies_stay_resident(gpu):
+    """Fewer frames than the smallest slot count: every spectrum resident."""
+    mv = synth.make_movie(300, 290, 3, mean=2.0, seed=231, dtype="u8")
+    p = api.verify_params(api.Params(CCPeakSearchDim=64, FrameDistOffset=0), 3)
+    with api.Plan(p, 300, 290, 3, 0) as pl:
+        assert pl.spectrum_slots == 0
+        pl.load_frames(mv.frames)
+        pl.run()
