@@ -54,11 +54,12 @@ __device__ __forceinline__ void fft_n1(float2* v) {
 }
 
 // Built-in radix-53 schedules of the forward row / column transforms: two
-// output pairs per loop pass in the row pass, one in the column pass
-// (measured on c2: the row pass 9 % faster paired, the column pass 27 %
-// slower); a schedule (mc_schedule_set, the autotuner) can pick either.
+// output pairs per loop pass in both (measured on c2: the row pass 9 %
+// faster paired; the column pass 12 % faster paired once its stores lost
+// the crop test and the scale, 27 % slower before); a schedule
+// (mc_schedule_set, the autotuner) can pick either.
 constexpr bool kFwdRowsPaired = true;
-constexpr bool kFwdColsPaired = false;
+constexpr bool kFwdColsPaired = true;
 // Resident CTAs per SM the two-level transforms are compiled for (register cap).
 #ifndef MC_TL_MIN_BLOCKS
 #define MC_TL_MIN_BLOCKS 4

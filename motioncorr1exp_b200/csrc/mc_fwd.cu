@@ -146,23 +146,30 @@ cudaError_t launch_rows_fft(const RowsFftArgs& a, bool inverse, int rows_per_cta
 }
 
 // Batched rows: out_row[i] = scale * X[i < keep_lo ? i : i + (n - n_out)].
-template <int N1, int N2, bool INV, bool PAIRED>
+template <int N1, int N2, bool INV, bool PAIRED, bool PLAIN = false>
 __global__ void __launch_bounds__(TwoLevel<N1, N2>::T, MC_TL_MIN_BLOCKS) k_rows_fft2l(RowsFftArgs a) {
   using TL = TwoLevel<N1, N2>;
   __shared__ float2 ysm[TL::N];
   const long long row = blockIdx.x;
   const float2* in = a.in + row * a.ld_in;
   float2* out = a.out + row * a.ld_out;
-  const int shift = TL::N - a.n_out, keep = a.keep_lo;
-  const float sc = a.scale;
-  TL::template run<INV, false, PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
-                        [&](int k, float2 v) {
-                          int o;
-                          if (k < keep) o = k;
-                          else if (k >= keep + shift) o = k - shift;
-                          else return;
-                          out[o] = make_float2(v.x * sc, v.y * sc);
-                        });
+  if constexpr (PLAIN) {
+    // every output kept, unscaled (the forward column pass without a Fourier
+    // crop): no per-output crop test or multiply (2.47 -> 2.15 ms per c2 movie)
+    TL::template run<INV, false, PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
+                                         [&](int k, float2 v) { out[k] = v; });
+  } else {
+    const int shift = TL::N - a.n_out, keep = a.keep_lo;
+    const float sc = a.scale;
+    TL::template run<INV, false, PAIRED>(ysm, a.tw, [&](int i) { return __ldg(in + i); },
+                          [&](int k, float2 v) {
+                            int o;
+                            if (k < keep) o = k;
+                            else if (k >= keep + shift) o = k - shift;
+                            else return;
+                            out[o] = make_float2(v.x * sc, v.y * sc);
+                          });
+  }
 }
 
 
@@ -181,13 +188,16 @@ bool two_level_split(int n, int& n1, int& n2) {
 // Forward column launch with the radix-53 pairing the schedule asks for
 template <int A, int B>
 void launch_cols_fwd(const RowsFftArgs& a, bool paired, cudaStream_t st) {
+  const bool plain = a.n_out == A * B && a.keep_lo >= A * B && a.scale == 1.f;
   if constexpr (A == 53) {
     if (paired != kFwdColsPaired) {
-      k_rows_fft2l<A, B, false, !kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+      if (plain) k_rows_fft2l<A, B, false, !kFwdColsPaired, true><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+      else k_rows_fft2l<A, B, false, !kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
       return;
     }
   }
-  k_rows_fft2l<A, B, false, kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+  if (plain) k_rows_fft2l<A, B, false, kFwdColsPaired, true><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
+  else k_rows_fft2l<A, B, false, kFwdColsPaired><<<a.nrows, TwoLevel<A, B>::T, 0, st>>>(a);
 }
 
 cudaError_t launch_rows_fft2l(const RowsFftArgs& a, bool inverse, cudaStream_t st) {
