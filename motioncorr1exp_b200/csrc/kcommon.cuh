@@ -77,9 +77,11 @@ struct TwoLevel {
   // lets store() write back into ysm.
   template <bool INV, bool SYNC_STORE, bool PAIRED = false, int TWS = 1, class Load, class Store>
   __device__ static void run(float2* ysm, const float2* __restrict__ tw, Load&& load, Store&& store,
-                             int kmax = (N1 - 1) / 2) {
+                             int kmax = (N1 - 1) / 2, int lt_team = -1) {
     static_assert(T >= N2, "one k2 per thread");
-    const int lt = threadIdx.x;
+    // lt_team: the thread's index in its team of T when a CTA runs several
+    // transforms side by side (every team takes the same barriers)
+    const int lt = lt_team >= 0 ? lt_team : (int)threadIdx.x;
     if (lt < N1) {
       float2 x[N2];
 #pragma unroll

@@ -43,7 +43,14 @@ def test_forward_schedule_trials_and_pairings(gpu):
     try:
         r = autotune.tune(512, box=64, nframes=8, fod=1, reps=1)
         assert len(r["fwd_trials"]) == len(autotune.FWD_STREAMS) * 4
-        assert r["fwd_ms"] == min(t["ms"] for t in r["fwd_trials"]) > 0
+        # the fastest trial, or the built-in schedule (4 streams, both passes
+        # paired) when it is within 1 % of the fastest
+        best = min(t["ms"] for t in r["fwd_trials"])
+        chosen = next(t for t in r["fwd_trials"] if (t["fwd_streams"], t["fwd_rows_pairing"], t["fwd_cols_pairing"])
+                      == (r["fwd_streams"], r["fwd_rows_pairing"], r["fwd_cols_pairing"]))
+        assert r["fwd_ms"] == chosen["ms"] > 0
+        assert r["fwd_ms"] == best or ((r["fwd_streams"], r["fwd_rows_pairing"], r["fwd_cols_pairing"]) == (4, 2, 2)
+                                       and r["fwd_ms"] <= 1.01 * best)
         assert api.schedule_get(512)["fwd_streams"] == r["fwd_streams"]
         mv = synth.make_movie(3838, 3710, 3, mean=1.2, seed=71, dtype="u8")
         o = O.forward_spectrum(O.decode_frame(mv.frames[2], 0), 0, 0, 3710, 3710)
