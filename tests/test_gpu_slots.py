@@ -170,6 +170,32 @@ def test_batch_lanes_with_slot_plans(gpu):
         np.testing.assert_array_equal(m["frame_shifts"], g["frame_shifts"])
 
 
+def test_single_graph_batch_rejects_slot_plans(gpu):
+    """The one-graph batch needs every spectrum of a movie in HBM: under a
+    device budget that forces spectrum slots it reports so, and runs again
+    once the budget is lifted."""
+    import torch
+    mv = synth.make_movie(530, 520, 12, mean=2.0, seed=241, dtype="u8", speed=0.6, rw_sigma=0.4)
+    p = api.verify_params(api.Params(crop_nsam=512, CCPeakSearchDim=64), 12)
+    d = torch.from_numpy(np.ascontiguousarray(mv.frames)).cuda()
+    img = torch.zeros((512, 512), dtype=torch.float32, pin_memory=True)
+    movie = {"params": p, "nx": 530, "ny": 520, "nz": 12, "mode": 0, "device_ptr": d.data_ptr(),
+             "image": img.numpy(), "frame_shifts": np.zeros((12, 2))}
+    L = _lib.lib()
+    try:
+        L.mc_debug_device_budget(KEEP_FREE + int(5.5 * _spec_bytes(512)))
+        with api.Batch(0, lanes=1, graph=True) as bt:
+            res = bt.run([movie], check=False)
+    finally:
+        L.mc_debug_device_budget(0)
+    assert res[0]["status"] == -5 and "spectrum slots" in res[0]["message"], res[0]
+    with api.Batch(0, lanes=1, graph=True) as bt:
+        res = bt.run([movie])
+    assert res[0]["status"] == 0
+    ref = api.align(mv.frames, 0, p)
+    np.testing.assert_array_equal(img.numpy(), ref["image"])
+
+
 @pytest.mark.slow
 def test_c4_with_sixteen_slots_equals_resident(gpu):
     """The c4 movie (60 x 4096^2 float32, -itr 3, -ref 1) with 16 of its 60
