@@ -393,9 +393,12 @@ size_t mc_batch_device_bytes(const mc_batch* b);
  * synchronisation; the graph is kept and relaunched while the job list is
  * the same.  Every job must hold device frames (on_device = 1), run
  * device-only (-itr 0, no refinement) and give its image in pinned host or
- * device memory (or NULL); otherwise mc_batch_run returns MC_E_ARG.  The
- * per-movie gpu_ms is 0 and start/end times are the batch's.  No reference
- * counterpart (the reference aligns one movie per process). */
+ * device memory (or NULL); otherwise mc_batch_run returns MC_E_ARG.  A
+ * movie whose plan holds spectrum slots (its spectra did not fit the free
+ * device memory; mc_plan_create_slots) gives MC_E_STATE: run such batches
+ * with lanes.  The per-movie gpu_ms is 0 and start/end times are the
+ * batch's.  No reference counterpart (the reference aligns one movie per
+ * process). */
 int mc_batch_set_graph(mc_batch* b, int on);
 
 /* ---- Stack files (host only; no GPU needed) -------------------------------
