@@ -151,7 +151,9 @@ int mc_plan_set_stretch(mc_plan* plan, float xscale, float yscale);
  * positions [first, first+count) from host memory (pinned or pageable) or
  * from device memory.  Replaces MRC::read2DIm_32bit + GPUMemH2D per frame
  * (DFAlign.cu:713, 770, 795).  Host copies return once the source buffer
- * may be reused; device copies are ordered on the plan stream. */
+ * may be reused; device copies are ordered on the plan stream, which does
+ * not wait for the caller's streams: the frames must be complete when the
+ * call is made (synchronise the stream that wrote them). */
 int mc_plan_load_frames(mc_plan* plan, const void* frames, int first, int count);
 int mc_plan_load_frames_device(mc_plan* plan, const void* d_frames, int first, int count);
 
@@ -330,7 +332,9 @@ int mc_plan_create_slots(const mc_params* p, int nx, int ny, int nz, int mode, i
 /* Reads the run's frames (positions nStart..nEnd, nx*ny pixels each in the
  * plan's MRC mode, back to back) in place from caller device memory on the
  * plan's GPU instead of the plan's own frame buffer; the memory must stay
- * valid and unchanged until the run returns.  NULL unbinds.  A later
+ * valid and unchanged until the run returns, and complete when the run
+ * starts (the plan stream does not wait for the caller's streams).  NULL
+ * unbinds.  A later
  * mc_plan_load_frames* or mc_plan_run_host switches back to the plan's
  * buffer. */
 int mc_plan_bind_frames_device(mc_plan* plan, const void* d_frames);

@@ -127,7 +127,8 @@ def make_movie_torch(nx: int, ny: int, nframes: int, mean: float, seed: int, dty
                      period: float = 20.0, contrast: float = 0.5, device: str = "cuda"):
     """Same signal model generated with torch on ``device`` (fast full-size
     inputs).  Blobs are deposited on integer pixels and blurred in Fourier
-    space.  Returns (frames tensor (nz, ny, nx) uint8|float32 on device, truth)."""
+    space.  Returns (frames tensor (nz, ny, nx) uint8|float32 on device, truth)
+    after the device has finished writing them."""
     import torch
     rng = np.random.Generator(np.random.PCG64(seed))
     truth = drift_track(nframes, rng, kind, speed, rw_sigma, amp, period)
@@ -158,6 +159,10 @@ def make_movie_torch(nx: int, ny: int, nframes: int, mean: float, seed: int, dty
         rate = mean * torch.clamp(1.0 + contrast * img, min=0.0)
         counts = torch.poisson(rate, generator=g)
         out[k] = counts.clamp(max=127).to(out.dtype) if dtype == "u8" else counts.to(out.dtype)
+    # the frames are complete before they are returned: libmc's plans copy or
+    # read them on their own non-blocking streams, which do not wait for
+    # torch's stream
+    torch.cuda.synchronize(out.device)
     return out, truth
 
 
