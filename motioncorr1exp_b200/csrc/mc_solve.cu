@@ -236,11 +236,14 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(SolveArgs a) {
 
 // ---------------------------------------------------------------------------
 // Shared-memory form of the same solve (used when its working set fits):
-// the pair list, the measured shifts, the normal matrix and the residuals
-// live in shared memory; the normal equations are built one frame step per
-// thread in a single pass over the pairs (a histogram of the pair ends per
-// step, then suffix sums), and the per-row residual and compaction loops run
-// in parallel.  Sums run in the same order as the global-memory form.
+// the pair list, the measured shifts, the normal matrix, the residuals, the
+// rank order, the union-find parents and the final step shifts live in
+// shared memory (the one-thread sections, the threshold scan and the
+// union-find pass, then run on shared-memory latency instead of dependent
+// global loads); the normal equations are built one frame step per thread in
+// a single pass over the pairs (a histogram of the pair ends per step, then
+// suffix sums), and the per-row residual and compaction loops run in
+// parallel.  Sums run in the same order as the global-memory form.
 namespace {
 
 struct SolveSmem {
@@ -249,6 +252,8 @@ struct SolveSmem {
   int* mask;       // [P]
   double* ki;      // [P]
   int* hist;       // [nc][nf]
+  int* order;      // [P] rows in ascending ki1 rank
+  int* uf;         // [nf] union-find parents
   double* M;       // [nc][nc]
   double* rx;      // [nc]
   double* ry;      // [nc]
@@ -341,8 +346,8 @@ __device__ double row_residual(const SolveSmem& m, const double* wx, const doubl
 
 size_t solve_smem_bytes(int P, int nf) {
   const size_t nc = nf - 1;
-  return (size_t)P * (sizeof(int2) + sizeof(float2) + sizeof(int) + sizeof(double)) + nc * nf * sizeof(int) +
-         nc * nc * sizeof(double) + 6 * (size_t)nf * sizeof(double) + 64;
+  return (size_t)P * (sizeof(int2) + sizeof(float2) + 2 * sizeof(int) + sizeof(double)) + nc * nf * sizeof(int) +
+         (size_t)nf * sizeof(int) + nc * nc * sizeof(double) + 6 * (size_t)nf * sizeof(double) + 64;
 }
 
 }  // namespace
@@ -361,6 +366,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
   m.pr = reinterpret_cast<int2*>(m.ps + P);
   m.mask = reinterpret_cast<int*>(m.pr + P);
   m.hist = m.mask + P;
+  m.order = m.hist + (size_t)nc * nf;
+  m.uf = m.order + P;
   for (int r = tid; r < P; r += kSolveThreads) {
     m.pr[r] = a.pairs[r];
     m.ps[r] = make_float2(a.pshift[2 * r], a.pshift[2 * r + 1]);
@@ -375,10 +382,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
     const double v = row_residual(m, wx, wy, r);
     m.ki[r] = v;
     a.ki1[r] = v;
+    m.order[r] = r;  // every slot holds a row even if NaN residuals share a rank
   }
   __syncthreads();
   // stable ascending rank of ki1 (OD_Threshold's repeated first-minimum pick)
-  int* order = a.order;
+  int* order = m.order;
   for (int r = tid; r < P; r += kSolveThreads) {
     const double v = m.ki[r];
     int pos = 0;
@@ -394,7 +402,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
     for (i = P - 1; i >= nc; i--)
       if (m.ki[order[i]] < (double)a.kithresh) break;
     int len = i + 1;
-    int* par = a.uf;
+    int* par = m.uf;
     for (int f = 0; f < nf; f++) par[f] = f;
     int comps = nf;
     for (int q = 0; q < P; q++) m.mask[q] = 0;
@@ -461,6 +469,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
       py = ny;
       sx[2 * k] = stx;
       sx[2 * k + 1] = sty;
+      m.rx[k] = stx;  // shared copies for the sums below (no global reads back)
+      m.ry[k] = sty;
       tx += stx;
       ty += sty;
       a.frame_shift[2 * (k + 1)] = tx;
@@ -469,18 +479,18 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_smem(SolveArgs a) {
     double mx = 0.0, my = 0.0;
     if (a.align_to_mid)
       for (int k = 0; k < a.mid_steps; k++) {
-        mx += sx[2 * k];
-        my += sx[2 * k + 1];
+        mx += m.rx[k];
+        my += m.ry[k];
       }
     double Tx = 0.0, Ty = 0.0;
     for (int k = 1; k < a.sum_first + 1; k++) {
-      Tx += sx[2 * (k - 1)];
-      Ty += sx[2 * (k - 1) + 1];
+      Tx += m.rx[k - 1];
+      Ty += m.ry[k - 1];
     }
     for (int k = a.sum_first; k <= a.sum_last; k++) {
       if (k > a.sum_first) {
-        Tx += sx[2 * (k - 1)];
-        Ty += sx[2 * (k - 1) + 1];
+        Tx += m.rx[k - 1];
+        Ty += m.ry[k - 1];
       }
       const int q2 = k - a.sum_first;
       a.sum_shift[q2] = make_double2(-Tx + mx, -Ty + my);
