@@ -181,9 +181,10 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
 // as items (output row m, chunk of at most 16 k1): Horner's rule from the
 // chunk's last term down, acc = acc w + Y with w = W^(y_m) (4 FMAs per term,
 // no twiddle loads; the powers of the rounded w drift by ~1e-6 over a chunk),
-// then one multiply by W^(kb y_m).  A thread runs two items at a time with
-// their chains interleaved (5.85 -> 5.71 ms per c2 movie: with two warps
-// per scheduler the dependent FMAs of one item left issue slots empty).  Consecutive threads take consecutive rows
+// then one multiply by W^(kb y_m).  A thread runs three items at a time with
+// their chains interleaved (one item 5.85, two 5.71, three 5.64 ms per c2
+// movie: with two warps per scheduler the dependent FMAs of one item left
+// issue slots empty).  Consecutive threads take consecutive rows
 // m, so their Y rows (odd stride in float2) fall on different bank pairs and
 // their twiddle loads are contiguous.  The chunk partials meet in shared
 // memory and are added in chunk order.
@@ -247,28 +248,42 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
     }
     team_barrier(1 + tm, T);
     int c = lt / box, m = lt - (lt / box) * box;
-    // two items per pass, their chains interleaved (twice the independent work)
-    for (int it = lt; it < box * C; it += 2 * T) {
+    // three items per pass, their chains interleaved (three times the
+    // independent work)
+    for (int it = lt; it < box * C; it += 3 * T) {
       int c1 = c, m1 = m + T;
       while (m1 >= box) {
         m1 -= box;
         c1++;
       }
-      const bool two = it + T < box * C;
-      if (!two) {
+      int c2 = c1, m2 = m1 + T;
+      while (m2 >= box) {
+        m2 -= box;
+        c2++;
+      }
+      const bool has1 = it + T < box * C, has2 = it + 2 * T < box * C;
+      const int nc_ = c2, nm_ = m2;
+      if (!has1) {
         c1 = c;
         m1 = m;
       }
-      int r0 = ys + m % Q, r1 = ys + m1 % Q;
+      if (!has2) {
+        c2 = c;
+        m2 = m;
+      }
+      int r0 = ys + m % Q, r1 = ys + m1 % Q, r2 = ys + m2 % Q;
       if (r0 >= Q) r0 -= Q;
       if (r1 >= Q) r1 -= Q;
-      const int kb0 = c * L, kb1 = c1 * L;
+      if (r2 >= Q) r2 -= Q;
+      const int kb0 = c * L, kb1 = c1 * L, kb2 = c2 * L;
       const float2* yr0 = Y + PS * r0 + kb0;
       const float2* yr1 = Y + PS * r1 + kb1;
-      const float2 w0 = tws[m], w1 = tws[m1];
-      const float2 v0 = cmul(w0, w0), v1 = cmul(w1, w1);
+      const float2* yr2 = Y + PS * r2 + kb2;
+      const float2 w0 = tws[m], w1 = tws[m1], w2 = tws[m2];
+      const float2 v0 = cmul(w0, w0), v1 = cmul(w1, w1), v2 = cmul(w2, w2);
       float2 ae0 = make_float2(0.f, 0.f), ao0 = make_float2(0.f, 0.f);
       float2 ae1 = make_float2(0.f, 0.f), ao1 = make_float2(0.f, 0.f);
+      float2 ae2 = make_float2(0.f, 0.f), ao2 = make_float2(0.f, 0.f);
 #pragma unroll
       for (int kk = L - 1; kk >= 0; kk--) {
         if (L * C == P || kb0 + kk < P) {
@@ -285,18 +300,29 @@ __global__ void __launch_bounds__(kRegThreads, pair_reg_min_blocks(Q)) k_pair_co
           h.x = fmaf(s.x, v1.x, fmaf(-s.y, v1.y, yv.x));
           h.y = fmaf(s.x, v1.y, fmaf(s.y, v1.x, yv.y));
         }
+        if (L * C == P || kb2 + kk < P) {
+          const float2 yv = yr2[kk];
+          float2& h = (kk & 1) ? ao2 : ae2;
+          const float2 s = h;
+          h.x = fmaf(s.x, v2.x, fmaf(-s.y, v2.y, yv.x));
+          h.y = fmaf(s.x, v2.y, fmaf(s.y, v2.x, yv.y));
+        }
       }
-      float2 acc0, acc1;
+      float2 acc0, acc1, acc2;
       acc0.x = fmaf(ao0.x, w0.x, fmaf(-ao0.y, w0.y, ae0.x));
       acc0.y = fmaf(ao0.x, w0.y, fmaf(ao0.y, w0.x, ae0.y));
       acc1.x = fmaf(ao1.x, w1.x, fmaf(-ao1.y, w1.y, ae1.x));
       acc1.y = fmaf(ao1.x, w1.y, fmaf(ao1.y, w1.x, ae1.y));
+      acc2.x = fmaf(ao2.x, w2.x, fmaf(-ao2.y, w2.y, ae2.x));
+      acc2.y = fmaf(ao2.x, w2.y, fmaf(ao2.y, w2.x, ae2.y));
       if (kb0 < P) acc0 = cmul(acc0, tws[(1 + c) * box + m]);
       if (kb1 < P) acc1 = cmul(acc1, tws[(1 + c1) * box + m1]);
+      if (kb2 < P) acc2 = cmul(acc2, tws[(1 + c2) * box + m2]);
       part[c * box + m] = acc0;
-      if (two) part[c1 * box + m1] = acc1;
-      m = m1 + T;
-      c = c1;
+      if (has1) part[c1 * box + m1] = acc1;
+      if (has2) part[c2 * box + m2] = acc2;
+      m = nm_ + T;
+      c = nc_;
       while (m >= box) {
         m -= box;
         c++;
