@@ -148,7 +148,7 @@ def load(path: Optional[str] = None, gpu: Optional[str] = None) -> int:
                              fwd_cols_pairing=int(r.get("fwd_cols_pairing", 0)))
             count += 1
         except Exception:
-            continue   # an entry this build's kernels no longer take
+            continue   # an entry the compiled kernels of libmc no longer take
     return count
 
 
