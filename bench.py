@@ -542,8 +542,7 @@ def run_ours(args):
             # configuration (32 of them here) the first time they run it.
             r5 = c5_measure(local, args.seed, (1, args.lanes), 2, 3)
             line["batch_c5"] = {"workload": C5_WORKLOAD, "frames_per_batch": r5["frames_per_batch"],
-                                "lanes": {str(k): {kk: vv for kk, vv in v.items() if kk != "clocks"}
-                                          for k, v in r5["lanes"].items()}}
+                                "lanes": {str(k): dict(v) for k, v in r5["lanes"].items()}}
         if world == 1 and not args.no_oracle_check and args.workload in ("c1", "c2", "c3"):
             line["vs_oracle"] = oracle_check(host_np_all, mode, p, g_res, p.NoisePeakSize)
             line["shift_rmse_vs_oracle_px"] = line["vs_oracle"]["shift_rmse_vs_oracle_px"]
